@@ -1,0 +1,339 @@
+"""Benchmark: the acoustic hall, 256³ nodes, 5000 steps per run (FP32 fields, FP64 audits).
+
+One bench step is one full run of the workload: `timesteps` calls of `Hall::step`, each with
+its fused FP64 invariant and on-device audit, over the 256³ grid (16.8 M nodes; 268 MB of f32
+state, larger than the 126 MB L2, so no flush is needed between steps).
+
+  value  node-updates/s with the state resident in HBM, timed with CUDA events on the stream
+         the kernels run on, max over ranks. FP32 chosen form.
+  e2e    the same through the C ABI with host buffers: release from pinned host memory (H2D),
+         the run, the pressure field and the ledger back to the host (D2H), every step.
+  plain_f64  the bit-exact f64 form on the same workload, for the FP32/f64 ratio.
+  roofline   the hall kernel's algorithmic bytes (32 B per FP32 node-update: p, vx, vy, vz read
+             and written once) per launch over its average launch time, against the measured
+             HBM copy bandwidth.
+  cpu_baseline  the reference's CPU path for this workload (the oracle's restatement of
+             `Simulation::advance` over `Hall::step` and its ledger), on a bounded sample.
+
+`--impl reference` times that CPU path alone, on all usable host cores (one independent hall per
+thread, the reference's `Ensemble` pattern), and prints its own line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s (acoustic hall 256^3, FP32 fields + FP64 audit)"
+UNIT = "Gcell-updates/s"
+BYTES_F32 = 32  # per node-update: p, vx, vy, vz, read and written once
+BYTES_F64 = 64
+# dram__bytes_read.sum + dram__bytes_write.sum of one hall_step<float> launch at 256³, from the
+# ncu capture summarised in profiles/hall_step_f32_256.md (None until captured).
+HALL_F32_TRAFFIC = None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.samples = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def summary(self):
+        if not getattr(self, "samples", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for s in self.samples for q in range(4) if s[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def hall_workload(n, timesteps):
+    from pantometry_b200 import workloads as W
+
+    return W.acoustic_hall(n, steps=timesteps)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import workloads as W
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    cfg = hall_workload(args.n, args.timesteps)
+    nodes = args.n ** 3
+    T = args.timesteps
+    stream = torch.cuda.Stream(device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_runs(precision, k, w):
+        hall = W.build_hall(cfg, precision=precision, device=local)
+        hall.set_stream(stream.cuda_stream)
+        hall.set_tolerance(1e-6 if precision == "f32" else 1e-9)
+        for _ in range(w):
+            v = hall.step(cfg["dt"], T)
+            assert v is None, v
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            start.record(stream)
+            for _ in range(k):
+                v = hall.step(cfg["dt"], T)
+                assert v is None, v
+            end.record(stream)
+            torch.cuda.synchronize()
+        ms = start.elapsed_time(end)
+        barrier()
+        return hall, max_over_ranks(ms), clk
+
+    # FP32 chosen form (the headline) and the plain f64 form, device-resident
+    h32, ms32, clk = timed_runs("f32", args.steps, args.warmup)
+    led32 = h32.ledger()
+    p32 = h32.fields()["p"]
+    del h32
+    plain_steps = max(1, args.steps // 2)
+    h64, ms64, _ = timed_runs("f64", plain_steps, max(1, args.warmup // 2))
+    led64 = h64.ledger()
+    del h64
+    # error of the FP32 run against the f64 run after the same number of steps
+    hf, _, _ = timed_runs("f64", 0, 0)
+    hf.step(cfg["dt"], T * (args.steps + args.warmup))
+    p64 = hf.fields()["p"]
+    led_ref = hf.ledger()
+    del hf
+    field_err = float(np.abs(p32 - p64).max())
+    ledger_err = abs(led32["total"] - led_ref["total"]) / max(abs(led_ref["total"]), led_ref["scale"])
+
+    # e2e through the C ABI with host buffers
+    pinned = torch.empty(nodes, dtype=torch.float64, pin_memory=True).numpy()
+    pinned[:] = cfg["pressure"]
+    out = torch.empty(nodes, dtype=torch.float64, pin_memory=True).numpy()
+    hall = W.build_hall(cfg, precision="f32", device=local)
+    hall.set_stream(stream.cuda_stream)
+    hall.set_tolerance(1e-6)
+    for _ in range(args.warmup):
+        hall.release(pinned)
+        hall.step(cfg["dt"], T)
+    barrier()
+    t0 = time.perf_counter()
+    s0 = torch.cuda.Event(enable_timing=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        hall.release(pinned)
+        v = hall.step(cfg["dt"], T)
+        assert v is None, v
+        hall.ledger()
+        hall.download_pressure(out)
+    e0.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    e2e_ms = max_over_ranks(max(s0.elapsed_time(e0), wall_ms))
+    del hall
+
+    peak, peak_kind = peaks()
+    per_launch_ms = ms32 / (args.steps * T)
+    achieved = BYTES_F32 * nodes / (per_launch_ms * 1e-3) / 1e9
+    value = world * nodes * T * args.steps / (ms32 * 1e-3) / 1e9
+    plain = world * nodes * T * plain_steps / (ms64 * 1e-3) / 1e9
+    per_launch64 = ms64 / (plain_steps * T)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms32 / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 fields, f64 audit",
+        "data": "synthetic (seeded Rng::for_index noise + Ricker source)",
+        "config": {"workload": f"acoustic_hall {args.n}^3 nodes, {T} timesteps per step, CFL 0.5, "
+                               "rigid walls, FP64 audit every timestep",
+                   "nodes": nodes, "timesteps_per_step": T, "parallelism": f"replicas x{world}",
+                   "l2": "state 268 MB > 126 MB L2, no flush"},
+        "e2e": {"value": round(world * nodes * T * args.steps / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                "h2d_bytes_per_step": nodes * 8, "d2h_bytes_per_step": nodes * 8 + 8 * 16},
+        "gpu_launches": args.steps * T,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": HALL_F32_TRAFFIC,
+                     "kernel": "hall_step<float>", "bytes_per_launch": BYTES_F32 * nodes,
+                     "peak_source": f"{peak_kind} hbm_gbs"},
+        "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
+                      "roofline_frac": round(BYTES_F64 * nodes / (per_launch64 * 1e-3) / 1e9 / peak, 4),
+                      "fp32_over_f64": round(value / plain, 3)},
+        "error_vs_f64": {"max_abs_pressure_pa": field_err, "ledger_rel": ledger_err,
+                         "after_timesteps": T * (args.steps + args.warmup),
+                         "f64_ledger_drift": abs(led64["total"] - led_ref["total"]) / max(abs(led_ref["total"]), 1e-300)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.n, sample_steps=args.cpu_sample_steps, threads=1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(n, sample_steps=2, threads=1):
+    """The reference's CPU path, restated (the oracle): `Simulation::advance` with one `Hall`:
+    ledger before, `attribute`'s own ledger, `Hall::step`, ledger after, audit — one thread per
+    hall, `threads` independent halls at once (the `Ensemble` pattern)."""
+    import oracle
+    from pantometry_b200 import workloads as W
+
+    cfg = W.acoustic_hall(n, steps=sample_steps + 1)
+    w, h, d = cfg["size"]
+    halls = []
+    for _ in range(threads):
+        o = oracle.Hall(w, h, d, cfg["across"], cfg["speed"], cfg["density"])
+        o.release(cfg["pressure"])
+        o.set_source(cfg["source_node"], cfg["wave"])
+        assert o.advance(cfg["dt"], 1) is None  # warm-up, and the leapfrog's opening half step
+        halls.append(o)
+    times = [0.0] * threads
+
+    def work(q):
+        t0 = time.perf_counter()
+        assert halls[q].advance(cfg["dt"], sample_steps) is None
+        times[q] = time.perf_counter() - t0
+
+    ths = [threading.Thread(target=work, args=(q,)) for q in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    secs = max(times)
+    value = threads * n ** 3 * sample_steps / secs / 1e9
+    return {"value": round(value, 6), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{threads} x {sample_steps} audited Simulation::advance steps of the {n}^3 hall "
+                      f"(after 1 warm-up step), {secs:.2f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    try:
+        import psutil
+
+        avail = psutil.virtual_memory().available
+    except Exception:  # noqa: BLE001
+        avail = 64 << 30
+    per_hall = 6 * (args.n ** 3) * 8
+    threads = max(1, min(ncpu, int(avail * 0.6 // per_hall)))
+    samples = []
+    for _ in range(args.steps):
+        samples.append(cpu_baseline(args.n, sample_steps=args.cpu_sample_steps, threads=threads))
+    value = statistics.median(s["value"] for s in samples)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Rng::for_index noise + Ricker source)",
+        "impl": "reference",
+        "config": {"workload": f"acoustic_hall {args.n}^3 nodes, audited Simulation::advance steps", "nodes": args.n ** 3},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": samples[0]["sample"] + "; the Rust reference cannot be built here (no cargo), "
+                                   "so this is the oracle's C++ restatement of its loops"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--timesteps", type=int, default=5000)
+    ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

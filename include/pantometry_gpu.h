@@ -1,0 +1,226 @@
+/*
+ * pantometry_gpu.h — the C ABI of the B200-native stepping path.
+ *
+ * One library, libpantometry_b200.so, holds sm_100a CUDA kernels and a C++ host runtime for
+ * three of pantometry's `Domain` implementations:
+ *
+ *   pm_heat    ~ Solid3D  (crates/pantometry-thermal/src/solid.rs)
+ *   pm_hall    ~ Hall     (crates/pantometry-acoustic/src/hall.rs)
+ *   pm_cavity  ~ Cavity   (crates/pantometry-em/src/cavity.rs)
+ *
+ * Each handle is the device-side state of one domain and answers the calls a `Domain` answers
+ * (crates/pantometry-core/src/sim.rs:77-252): step, ledger, max_stable_dt, checkpoint, restore.
+ * Every step computes the domain's energy ledger on the device in FP64 with a fixed-order
+ * reduction tree (run-to-run reproducible), and can audit it against the previous step the way
+ * `Simulation::advance` does (sim.rs:947-965, conserved.rs:323-363) without a host round trip.
+ *
+ * Two arithmetic forms per domain (pm_precision):
+ *   PM_PLAIN_F64   IEEE f64, no FMA contraction, the reference's operand order: bit-exact with
+ *                  the reference cell by cell.
+ *   PM_FIELDS_F32  fields stored and updated in f32 (heat stores T − T0); ledgers, audits and
+ *                  the running books stay in f64.
+ *
+ * Conventions: plain pointers and sizes, host memory unless a name says `device`. Every call
+ * returns a pm_status; nothing calls exit() or abort(). pm_last_error() gives the message of
+ * the last failing call on the calling thread. There is no CPU fallback: without a CUDA device
+ * pm_*_create returns PM_NO_DEVICE.
+ */
+#ifndef PANTOMETRY_GPU_H
+#define PANTOMETRY_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Replaces `Result<(), Violation>` (sim.rs:77-252) and
+ * `Unavailable{NoAdapter, NoDevice, NotConducting}` (runtime/gpu/src/lib.rs:99-106). */
+typedef enum pm_status {
+    PM_OK = 0,
+    PM_NO_DEVICE = 1,      /* no CUDA device, or the library's kernels cannot run on it */
+    PM_UNSUPPORTED = 2,    /* a feature the kernels do not implement (e.g. phase change) */
+    PM_VIOLATION = 3,      /* a step was refused or an audit failed; the pm_violation is filled */
+    PM_DEVICE_TIMEOUT = 4, /* reserved: a device-side wait gave up (no kernel here waits) */
+    PM_BAD_ARG = 5,
+    PM_CUDA_ERROR = 6,
+    PM_OUT_OF_MEMORY = 7
+} pm_status;
+
+typedef enum pm_precision { PM_PLAIN_F64 = 0, PM_FIELDS_F32 = 1 } pm_precision;
+
+/* `Violation` (crates/pantometry-core/src/conserved.rs:128-143), plus the step it happened on. */
+typedef struct pm_violation {
+    char quantity[32];
+    char site[96];
+    double before;
+    double after;
+    double scale;
+    double tolerance;
+    long long step; /* 1-based index, within the failing call, of the step that failed */
+} pm_violation;
+
+/* The "energy" `Entry` of a `Ledger` (conserved.rs:37-124): its total and scale, and the
+ * contributions that `Ledger::with` added, in order:
+ *   heat:   stored, lost, -supplied                          (solid.rs:1904-1927)
+ *   hall:   invariant + offset (- source injection)          (hall.rs:532-534)
+ *   cavity: invariant, dissipated (, -source work)           (cavity.rs:1520-1524) */
+typedef struct pm_ledger {
+    double total;
+    double scale;
+    double parts[4];
+    int n_parts;
+    long long steps; /* steps taken since the state was last uploaded or released */
+} pm_ledger;
+
+const char* pm_status_string(pm_status status);
+const char* pm_last_error(void);
+pm_status pm_device_count(int* count);
+const char* pm_version(void);
+
+/* ==================================== Solid3D ====================================== */
+
+typedef struct pm_heat pm_heat;
+
+/* `Substance` with its `ThermalProps` (crates/pantometry-core/src/substance.rs:43-92, 108-123).
+ * thermal == 0 is `thermal: None`, which leaves the block with no diffusivity. */
+typedef struct pm_substance {
+    double density;       /* kg/m^3 */
+    double conductivity;  /* W/m/K */
+    double specific_heat; /* J/kg/K */
+    double emissivity;
+    int thermal;
+} pm_substance;
+
+typedef struct pm_heat_desc {
+    const char* name;
+    int nx, ny, nz;
+    double dx;
+    pm_substance substance;
+    double initial_kelvin; /* also the enthalpy reference stored heat is measured from */
+    int precision;         /* pm_precision */
+    int device;
+} pm_heat_desc;
+
+/* Solid3D::new (solid.rs:377-421). */
+pm_status pm_heat_create(const pm_heat_desc* desc, pm_heat** out);
+/* Solid3D::fill (solid.rs:519-543): cells with mask[c] != 0 take `substance`. */
+pm_status pm_heat_fill(pm_heat* h, const pm_substance* substance, const uint8_t* mask, size_t n);
+/* Solid3D::losing_from (solid.rs:1039-1043). face: 0..5 = XMin, XMax, YMin, YMax, ZMin, ZMax.
+ * `area` is the whole face's area; convection may be +inf (a Dirichlet face). */
+pm_status pm_heat_losing_from(pm_heat* h, int face, double ambient_kelvin,
+                              double convection_w_per_m2_k, double area);
+/* Solid3D::set_temperature over every cell (solid.rs:1346-1361), kelvin, index x + nx(y + ny z). */
+pm_status pm_heat_upload(pm_heat* h, const double* kelvin, size_t n);
+pm_status pm_heat_download(pm_heat* h, double* kelvin, size_t n);
+/* Domain::max_stable_dt (solid.rs:1709-1715). */
+pm_status pm_heat_max_stable_dt(pm_heat* h, double* seconds);
+/* Relative tolerance of the per-step audit (`Simulation::advance`, sim.rs:947-965, and
+ * `attribute`, sim.rs:1169-1223). Negative disables it, leaving plain `Domain::step`. */
+pm_status pm_heat_set_tolerance(pm_heat* h, double tolerance);
+/* `nsteps` calls of Domain::step (solid.rs:1717-1901), each followed by the ledger and, when
+ * enabled, the audit. Stops at the first violation (PM_VIOLATION, *out filled). */
+pm_status pm_heat_step(pm_heat* h, double dt, long long nsteps, pm_violation* out);
+/* Domain::ledger (solid.rs:1904-1927), as of the last step. */
+pm_status pm_heat_ledger(pm_heat* h, pm_ledger* out);
+/* Placeless heat off the bus, spread to a uniform rise (solid.rs:1752-1765). */
+pm_status pm_heat_absorb(pm_heat* h, double joules);
+/* Domain::checkpoint / restore (solid.rs:1935-1950). */
+pm_status pm_heat_checkpoint(pm_heat* h);
+pm_status pm_heat_restore(pm_heat* h);
+/* Run subsequent work on `stream` (a cudaStream_t); NULL restores the handle's own stream. */
+pm_status pm_heat_set_stream(pm_heat* h, void* stream);
+void pm_heat_destroy(pm_heat* h);
+
+/* ===================================== Hall ========================================= */
+
+typedef struct pm_hall pm_hall;
+
+typedef struct pm_hall_desc {
+    const char* name;
+    double width, height, depth; /* metres */
+    int across;                  /* nodes along the width */
+    double speed;                /* m/s */
+    double density;              /* kg/m^3 */
+    int precision;               /* pm_precision */
+    int device;
+} pm_hall_desc;
+
+/* Hall::new (hall.rs:99-134). */
+pm_status pm_hall_create(const pm_hall_desc* desc, pm_hall** out);
+pm_status pm_hall_nodes(pm_hall* h, int* nx, int* ny, int* nz, double* dx);
+/* Hall::released_from (hall.rs:166-184) with the profile sampled at the nodes. */
+pm_status pm_hall_release(pm_hall* h, const double* pressure, size_t n);
+/* Extension (not in the reference): a soft point source adding wave[s] Pa at `node` after the
+ * pressure update of step s (s counted from the release); its work is kept in the ledger. */
+pm_status pm_hall_set_source(pm_hall* h, long long node, const double* wave, size_t n);
+/* Extension (not in the reference): a piecewise-constant sound speed over cubic blocks of
+ * `block` nodes per side, speeds[b] for block index bx + nbx(by + nby bz). The step limit
+ * follows the fastest block. */
+pm_status pm_hall_set_speed_blocks(pm_hall* h, int block, const double* speeds, size_t n);
+pm_status pm_hall_max_stable_dt(pm_hall* h, double* seconds);
+pm_status pm_hall_set_tolerance(pm_hall* h, double tolerance);
+/* `nsteps` calls of Domain::step (hall.rs:408-530), ledger and audit as for pm_heat_step. */
+pm_status pm_hall_step(pm_hall* h, double dt, long long nsteps, pm_violation* out);
+pm_status pm_hall_ledger(pm_hall* h, pm_ledger* out);
+/* Any pointer may be NULL. p_prev is `pressure_prev`. */
+pm_status pm_hall_download(pm_hall* h, double* p, double* p_prev, double* vx, double* vy, double* vz);
+pm_status pm_hall_checkpoint(pm_hall* h);
+pm_status pm_hall_restore(pm_hall* h);
+pm_status pm_hall_set_stream(pm_hall* h, void* stream);
+void pm_hall_destroy(pm_hall* h);
+
+/* ===================================== Cavity ======================================= */
+
+typedef struct pm_cavity pm_cavity;
+
+typedef struct pm_cavity_desc {
+    const char* name;
+    int nx, ny, nz; /* cells */
+    double dx;
+    double eps_r, mu_r, sigma; /* the `Medium` (crates/pantometry-em/src/lib.rs:73-118) */
+    int precision;             /* pm_precision */
+    int device;
+} pm_cavity_desc;
+
+/* Cavity::new (cavity.rs:211-245). All walls conducting. */
+pm_status pm_cavity_create(const pm_cavity_desc* desc, pm_cavity** out);
+/* Cavity::fill once per cell (cavity.rs:250-267): per-cell eps_r, mu_r, sigma (any may be NULL,
+ * keeping the present value), then `refresh_media` (cavity.rs:348-458). */
+pm_status pm_cavity_fill_cells(pm_cavity* c, const double* eps_r, const double* mu_r,
+                               const double* sigma, size_t n);
+/* Cavity::obstruct (cavity.rs:281-295): mask[c] != 0 makes cell c a perfect conductor. */
+pm_status pm_cavity_obstruct(pm_cavity* c, const uint8_t* mask, size_t n);
+/* Cavity::set_boundary (cavity.rs:566-569). wall 0..5 = XLow..ZHigh; kind 0 conducting,
+ * 1 magnetic, 2 open (Mur). */
+pm_status pm_cavity_set_boundary(pm_cavity* c, int wall, int kind);
+/* Cavity::release_mode (cavity.rs:675-732). */
+pm_status pm_cavity_release_mode(pm_cavity* c, int m, int p, double amplitude, double dt);
+/* Set all six components (host arrays in the reference's index order) and `started`. */
+pm_status pm_cavity_upload(pm_cavity* c, const double* ex, const double* ey, const double* ez,
+                           const double* hx, const double* hy, const double* hz, int started);
+pm_status pm_cavity_download(pm_cavity* c, double* ex, double* ey, double* ez, double* hx,
+                             double* hy, double* hz);
+/* Extension (not in the reference): a soft current density current[s] (A/m^2) on the Ez edge
+ * with flat index `edge`, applied in step s's electric update; its work is kept in the ledger. */
+pm_status pm_cavity_set_source(pm_cavity* c, long long edge, const double* current, size_t n);
+/* Cavity::courant_limit (cavity.rs:1035-1037). */
+pm_status pm_cavity_courant_limit(pm_cavity* c, double* seconds);
+pm_status pm_cavity_set_tolerance(pm_cavity* c, double tolerance);
+/* `nsteps` calls of Domain::step (cavity.rs:1468-1501), ledger and audit per step. */
+pm_status pm_cavity_step(pm_cavity* c, double dt, long long nsteps, pm_violation* out);
+/* Domain::ledger (cavity.rs:1520-1524). */
+pm_status pm_cavity_ledger(pm_cavity* c, pm_ledger* out);
+/* Cavity::electric_energy / magnetic_energy (cavity.rs:824-847, 919-940), on the device. */
+pm_status pm_cavity_energies(pm_cavity* c, double* electric, double* magnetic);
+pm_status pm_cavity_checkpoint(pm_cavity* c);
+pm_status pm_cavity_restore(pm_cavity* c);
+pm_status pm_cavity_set_stream(pm_cavity* c, void* stream);
+void pm_cavity_destroy(pm_cavity* c);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PANTOMETRY_GPU_H */

@@ -1,0 +1,589 @@
+// pm_cavity: the device form of `Cavity` (crates/pantometry-em/src/cavity.rs).
+#include <algorithm>
+#include <limits>
+#include <new>
+
+#include "runtime.h"
+
+namespace pm {
+
+namespace {
+constexpr double kEpsilon0 = 8.8541878128e-12;  // crates/pantometry-em/src/lib.rs:67
+constexpr double kMu0 = 1.25663706212e-6;       // crates/pantometry-em/src/lib.rs:69
+constexpr double kCourant3D = 0.5773502691896258;  // cavity.rs:15
+}  // namespace
+
+struct Cavity : Handle {
+    int nx = 1, ny = 1, nz = 1;
+    double dx = 0.0;
+    double eps_r = 1.0, mu_r = 1.0, sigma = 0.0;  // the constructor's `Medium`
+    int boundary[6] = {0, 0, 0, 0, 0, 0};
+    bool started = false;
+    // media (cavity.rs:348-458)
+    bool uniform = true;
+    double eps_u = 0.0, sig_u = 0.0, mu_u = 0.0;
+    std::vector<double> cell_eps, cell_mu, cell_sig;  // per cell, relative ε, μ and σ
+    std::vector<double> eps[3], sig[3], mu[3];
+    DBuf deps[3], dsig[3], dmu[3];
+    std::vector<uint8_t> solid;
+    bool any_solid = false;
+    DBuf dsolid;
+    // fields (in place: no ping-pong)
+    DBuf f[6];  // ex ey ez hx hy hz
+    DBuf keep[3];
+    DBuf stage;
+    DBuf energies;  // 2 doubles
+    // source (extension)
+    long long src = -1;
+    DBuf current;
+    long long ncurrent = 0;
+    // checkpoint (cavity.rs:1566-1590)
+    DBuf sf[6];
+    bool s_started = false;
+    double s_dissipated = 0.0;
+
+    size_t count(int q) const {
+        switch (q) {
+            case 0: return (size_t)nx * (ny + 1) * (nz + 1);
+            case 1: return (size_t)(nx + 1) * ny * (nz + 1);
+            case 2: return (size_t)(nx + 1) * (ny + 1) * nz;
+            case 3: return (size_t)(nx + 1) * ny * nz;
+            case 4: return (size_t)nx * (ny + 1) * nz;
+            default: return (size_t)nx * ny * (nz + 1);
+        }
+    }
+    size_t cells() const { return (size_t)nx * ny * nz; }
+    size_t esize() const { return precision == PM_PLAIN_F64 ? 8 : 4; }
+    double volume() const { return dx * (dx * dx); }  // dx.powi(3)
+    double permittivity() const { return kEpsilon0 * eps_r; }
+    double permeability() const { return kMu0 * mu_r; }
+    double wave_speed() const { return 1.0 / std::sqrt(permittivity() * permeability()); }
+    double courant_limit() const { return kCourant3D * dx / wave_speed(); }
+
+    // cavity.rs:348-458
+    void refresh_media() {
+        auto at = [&](long i, long j, long k) -> size_t {
+            auto c = [](long v, long n) { return (size_t)std::min(std::max(v, 0L), n - 1); };
+            return c(i, nx) + (size_t)nx * (c(j, ny) + (size_t)ny * c(k, nz));
+        };
+        auto perm = [&](size_t c) { return kEpsilon0 * cell_eps[c]; };
+        auto cond = [&](size_t c) { return std::max(cell_sig[c], 0.0); };
+        auto mean4 = [&](const size_t* of, bool conductivity) {
+            double s = -0.0;
+            for (int q = 0; q < 4; ++q) s += conductivity ? cond(of[q]) : perm(of[q]);
+            return s / 4.0;
+        };
+        for (int q = 0; q < 3; ++q) {
+            eps[q].assign(count(q), 0.0);
+            sig[q].assign(count(q), 0.0);
+            mu[q].assign(count(q + 3), 0.0);
+        }
+        for (long k = 0; k <= nz; ++k)
+            for (long j = 0; j <= ny; ++j)
+                for (long i = 0; i <= nx; ++i) {
+                    if (i < nx) {
+                        size_t of[4] = {at(i, j - 1, k - 1), at(i, j, k - 1), at(i, j - 1, k), at(i, j, k)};
+                        size_t idx = i + (size_t)nx * (j + (size_t)(ny + 1) * k);
+                        eps[0][idx] = mean4(of, false);
+                        sig[0][idx] = mean4(of, true);
+                    }
+                    if (j < ny) {
+                        size_t of[4] = {at(i - 1, j, k - 1), at(i, j, k - 1), at(i - 1, j, k), at(i, j, k)};
+                        size_t idx = i + (size_t)(nx + 1) * (j + (size_t)ny * k);
+                        eps[1][idx] = mean4(of, false);
+                        sig[1][idx] = mean4(of, true);
+                    }
+                    if (k < nz) {
+                        size_t of[4] = {at(i - 1, j - 1, k), at(i, j - 1, k), at(i - 1, j, k), at(i, j, k)};
+                        size_t idx = i + (size_t)(nx + 1) * (j + (size_t)(ny + 1) * k);
+                        eps[2][idx] = mean4(of, false);
+                        sig[2][idx] = mean4(of, true);
+                    }
+                }
+        auto mean2 = [&](size_t a, size_t b) {
+            double s = -0.0;
+            s += kMu0 * cell_mu[a];
+            s += kMu0 * cell_mu[b];
+            return s / 2.0;
+        };
+        for (long k = 0; k < nz; ++k)
+            for (long j = 0; j < ny; ++j)
+                for (long i = 0; i < nx; ++i) {
+                    mu[0][i + (size_t)(nx + 1) * (j + (size_t)ny * k)] = mean2(at(i - 1, j, k), at(i, j, k));
+                    mu[1][i + (size_t)nx * (j + (size_t)(ny + 1) * k)] = mean2(at(i, j - 1, k), at(i, j, k));
+                    mu[2][i + (size_t)nx * (j + (size_t)ny * k)] = mean2(at(i, j, k - 1), at(i, j, k));
+                }
+        const double fallback = permeability();
+        for (int q = 0; q < 3; ++q)
+            for (double& v : mu[q])
+                if (v <= 0.0) v = fallback;
+    }
+
+    // The uniform values every edge and face of a one-medium box holds (the same means).
+    void uniform_media() {
+        double s = -0.0;
+        for (int q = 0; q < 4; ++q) s += permittivity();
+        eps_u = s / 4.0;
+        s = -0.0;
+        for (int q = 0; q < 4; ++q) s += std::max(sigma, 0.0);
+        sig_u = s / 4.0;
+        s = -0.0;
+        s += permeability();
+        s += permeability();
+        mu_u = s / 2.0;
+        if (mu_u <= 0.0) mu_u = permeability();
+    }
+
+    template <typename Real>
+    YeeHArgs<Real> hargs(double g, int energy) const {
+        YeeHArgs<Real> a{};
+        a.ex = f[0].as<Real>(); a.ey = f[1].as<Real>(); a.ez = f[2].as<Real>();
+        a.hx = f[3].as<Real>(); a.hy = f[4].as<Real>(); a.hz = f[5].as<Real>();
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        a.g = g;
+        a.uniform = uniform ? 1 : 0;
+        a.ch = (Real)(g / mu_u);  // cavity.rs:1355: g / μ
+        a.mu0 = dmu[0].as<double>(); a.mu1 = dmu[1].as<double>(); a.mu2 = dmu[2].as<double>();
+        a.energy = energy;
+        a.eps_u = eps_u; a.mu_u = mu_u;
+        a.eps0 = deps[0].as<double>(); a.eps1 = deps[1].as<double>(); a.eps2 = deps[2].as<double>();
+        a.volume = volume();
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        a.nblocks = plane_blocks(nx + 1, ny + 1, nz + 1);
+        return a;
+    }
+
+    template <typename Real>
+    YeeEArgs<Real> eargs(double dt) const {
+        YeeEArgs<Real> a{};
+        a.ex = f[0].as<Real>(); a.ey = f[1].as<Real>(); a.ez = f[2].as<Real>();
+        a.hx = f[3].as<Real>(); a.hy = f[4].as<Real>(); a.hz = f[5].as<Real>();
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        a.dt = dt; a.dx = dx; a.volume = volume();
+        a.uniform = uniform ? 1 : 0;
+        // cavity.rs:1391-1397 at the uniform edge ε and σ
+        const double half = sig_u * dt / (2.0 * eps_u);
+        for (int q = 0; q < 3; ++q) {
+            a.decay[q] = (Real)((1.0 - half) / (1.0 + half));
+            a.gain[q] = (Real)((dt / (eps_u * dx)) / (1.0 + half));
+            a.sigma_u[q] = sig_u;
+        }
+        a.eps0 = deps[0].as<double>(); a.eps1 = deps[1].as<double>(); a.eps2 = deps[2].as<double>();
+        a.sig0 = dsig[0].as<double>(); a.sig1 = dsig[1].as<double>(); a.sig2 = dsig[2].as<double>();
+        a.solid = any_solid ? dsolid.as<uint8_t>() : nullptr;
+        a.src = src;
+        a.current = current.as<double>();
+        a.ncurrent = ncurrent;
+        a.with_source = src >= 0 ? 1 : 0;
+        if (src >= 0) {
+            a.eps_src = uniform ? eps_u : eps[2][(size_t)src];
+            a.sig_src = uniform ? sig_u : sig[2][(size_t)src];
+        }
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        a.nblocks = plane_blocks(nx + 1, ny + 1, nz + 1);
+        return a;
+    }
+
+    pm_status launch_h(double g, int energy, cudaStream_t s) const {
+        if (precision == PM_PLAIN_F64) PM_CUDA(launch_yee_h<double>(hargs<double>(g, energy), s));
+        else PM_CUDA(launch_yee_h<float>(hargs<float>(g, energy), s));
+        return PM_OK;
+    }
+
+    pm_status put(int q, const double* src_host) {
+        const size_t n = count(q);
+        if (!src_host) {
+            PM_CUDA(cudaMemsetAsync(f[q].p, 0, n * esize(), stream()));
+            return PM_OK;
+        }
+        if (precision == PM_PLAIN_F64) {
+            PM_CUDA(cudaMemcpyAsync(f[q].p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
+        } else {
+            if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(n * 8));
+            PM_CUDA(cudaMemcpyAsync(stage.p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
+            PM_CUDA(launch_to_f32(stage.as<double>(), f[q].as<float>(), n, stream()));
+            PM_CUDA(cudaStreamSynchronize(stream()));
+        }
+        return PM_OK;
+    }
+    pm_status get(int q, double* dst_host) {
+        if (!dst_host) return PM_OK;
+        const size_t n = count(q);
+        if (precision == PM_PLAIN_F64) {
+            PM_CUDA(cudaMemcpyAsync(dst_host, f[q].p, n * 8, cudaMemcpyDeviceToHost, stream()));
+        } else {
+            if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(n * 8));
+            PM_CUDA(launch_to_f64(f[q].as<float>(), stage.as<double>(), n, stream()));
+            PM_CUDA(cudaMemcpyAsync(dst_host, stage.p, n * 8, cudaMemcpyDeviceToHost, stream()));
+        }
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        return PM_OK;
+    }
+
+    // ½εE² and ½μH² of the present state.
+    pm_status measure_naive(double* electric, double* magnetic) {
+        if (!energies.p) PM_CUDA(energies.alloc(2 * sizeof(double)));
+        if (precision == PM_PLAIN_F64) PM_CUDA(launch_yee_measure<double>(hargs<double>(0.0, 0), energies.as<double>(), stream()));
+        else PM_CUDA(launch_yee_measure<float>(hargs<float>(0.0, 0), energies.as<double>(), stream()));
+        double e2[2];
+        PM_CUDA(cudaMemcpyAsync(e2, energies.p, sizeof(e2), cudaMemcpyDeviceToHost, stream()));
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        if (electric) *electric = e2[0];
+        if (magnetic) *magnetic = e2[1];
+        return PM_OK;
+    }
+
+    // The ledger as `Domain::ledger` reads it now (cavity.rs:1520-1524, 912-917), made the
+    // audit's starting point.
+    pm_status reset_ledger() {
+        pm_status s = read_state();
+        if (s != PM_OK) return s;
+        DevState* st = host_state;
+        double inv = st->invariant;
+        if (!st->has_invariant) {
+            double e = 0.0, m = 0.0;
+            if ((s = measure_naive(&e, &m)) != PM_OK) return s;
+            inv = e + m;
+        }
+        double total = 0.0, scale = 0.0;
+        auto add = [&](double x) { total += x; scale = std::fmax(scale, std::fabs(x)); };  // Ledger::add
+        add(inv);
+        add(st->dissipated);
+        if (src >= 0) add(-st->work);
+        st->total = total;
+        st->scale = scale;
+        st->part[0] = inv;
+        st->part[1] = st->dissipated;
+        st->part[2] = -st->work;
+        st->prev_total = total;
+        st->prev_scale = scale;
+        return write_state();
+    }
+
+    pm_status upload_media() {
+        drop_graphs();
+        if (uniform) return PM_OK;
+        for (int q = 0; q < 3; ++q) {
+            PM_CUDA(deps[q].alloc(eps[q].size() * 8));
+            PM_CUDA(dsig[q].alloc(sig[q].size() * 8));
+            PM_CUDA(dmu[q].alloc(mu[q].size() * 8));
+            PM_CUDA(cudaMemcpy(deps[q].p, eps[q].data(), eps[q].size() * 8, cudaMemcpyHostToDevice));
+            PM_CUDA(cudaMemcpy(dsig[q].p, sig[q].data(), sig[q].size() * 8, cudaMemcpyHostToDevice));
+            PM_CUDA(cudaMemcpy(dmu[q].p, mu[q].data(), mu[q].size() * 8, cudaMemcpyHostToDevice));
+        }
+        return PM_OK;
+    }
+};
+
+}  // namespace pm
+
+using namespace pm;
+
+#define CAV_GUARD(c)                                            \
+    do {                                                        \
+        if (!(c)) return fail(PM_BAD_ARG, "null pm_cavity");     \
+        cudaSetDevice((c)->device);                             \
+    } while (0)
+
+extern "C" {
+
+pm_status pm_cavity_create(const pm_cavity_desc* d, pm_cavity** out) {
+    if (!d || !out) return fail(PM_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (d->precision != PM_PLAIN_F64 && d->precision != PM_FIELDS_F32) return fail(PM_BAD_ARG, "unknown precision");
+    if (!(d->dx > 0.0)) return fail(PM_BAD_ARG, "dx must be positive");
+    Cavity* c = new (std::nothrow) Cavity();
+    if (!c) return fail(PM_OUT_OF_MEMORY, "host allocation");
+    c->name = d->name ? d->name : "cavity";
+    c->precision = d->precision;
+    c->nx = std::max(d->nx, 1); c->ny = std::max(d->ny, 1); c->nz = std::max(d->nz, 1);
+    c->dx = d->dx;
+    c->eps_r = d->eps_r; c->mu_r = d->mu_r; c->sigma = d->sigma;
+    c->uniform_media();
+    pm_status s = c->init(d->device, (size_t)plane_blocks(c->nx + 1, c->ny + 1, c->nz + 1) * 6);
+    if (s != PM_OK) { delete c; return s; }
+    for (int q = 0; q < 6; ++q) {
+        cudaError_t e = c->f[q].alloc(c->count(q) * c->esize());
+        if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMalloc cavity fields"); }
+        cudaMemset(c->f[q].p, 0, c->count(q) * c->esize());
+    }
+    *out = reinterpret_cast<pm_cavity*>(c);
+    s = c->reset_ledger();
+    if (s != PM_OK) { delete c; *out = nullptr; }
+    return s;
+}
+
+pm_status pm_cavity_fill_cells(pm_cavity* cp, const double* eps_r, const double* mu_r, const double* sigma, size_t n) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (n != c->cells()) return fail(PM_BAD_ARG, "fill_cells: one value per cell");
+    if (c->cell_eps.empty()) {
+        c->cell_eps.assign(c->cells(), c->eps_r);
+        c->cell_mu.assign(c->cells(), c->mu_r);
+        c->cell_sig.assign(c->cells(), c->sigma);
+    }
+    for (size_t q = 0; q < n; ++q) {
+        if (eps_r) c->cell_eps[q] = eps_r[q];
+        if (mu_r) c->cell_mu[q] = mu_r[q];
+        if (sigma) c->cell_sig[q] = sigma[q];
+    }
+    c->uniform = false;
+    c->refresh_media();
+    pm_status s = c->upload_media();
+    if (s != PM_OK) return s;
+    return c->reset_ledger();
+}
+
+pm_status pm_cavity_obstruct(pm_cavity* cp, const uint8_t* mask, size_t n) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (!mask || n != c->cells()) return fail(PM_BAD_ARG, "obstruct: one byte per cell");
+    if (c->solid.empty()) c->solid.assign(c->cells(), 0);
+    for (size_t q = 0; q < n; ++q)
+        if (mask[q]) { c->solid[q] = 1; c->any_solid = true; }
+    if (!c->any_solid) return PM_OK;
+    PM_CUDA(c->dsolid.alloc(c->cells()));
+    PM_CUDA(cudaMemcpy(c->dsolid.p, c->solid.data(), c->cells(), cudaMemcpyHostToDevice));
+    c->drop_graphs();
+    // cavity.rs:293 `enforce_solid` now, on the host copy of E
+    std::vector<double> e[3];
+    pm_status s;
+    for (int q = 0; q < 3; ++q) {
+        e[q].resize(c->count(q));
+        if ((s = c->get(q, e[q].data())) != PM_OK) return s;
+    }
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                if (!c->solid[i + (size_t)nx * (j + (size_t)ny * k)]) continue;
+                const int d[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
+                for (auto& q : d) e[0][(i) + (size_t)nx * ((j + q[0]) + (size_t)(ny + 1) * (k + q[1]))] = 0.0;
+                for (auto& q : d) e[1][(i + q[0]) + (size_t)(nx + 1) * (j + (size_t)ny * (k + q[1]))] = 0.0;
+                for (auto& q : d) e[2][(i + q[0]) + (size_t)(nx + 1) * ((j + q[1]) + (size_t)(ny + 1) * k)] = 0.0;
+            }
+    for (int q = 0; q < 3; ++q)
+        if ((s = c->put(q, e[q].data())) != PM_OK) return s;
+    PM_CUDA(cudaStreamSynchronize(c->stream()));
+    return PM_OK;
+}
+
+pm_status pm_cavity_set_boundary(pm_cavity* cp, int wall, int kind) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (wall < 0 || wall > 5 || kind < 0 || kind > 2) return fail(PM_BAD_ARG, "wall 0..5, kind 0..2");
+    c->boundary[wall] = kind;
+    c->drop_graphs();
+    return PM_OK;
+}
+
+pm_status pm_cavity_upload(pm_cavity* cp, const double* ex, const double* ey, const double* ez, const double* hx,
+                           const double* hy, const double* hz, int started) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    const double* src[6] = {ex, ey, ez, hx, hy, hz};
+    pm_status s;
+    for (int q = 0; q < 6; ++q)
+        if ((s = c->put(q, src[q])) != PM_OK) return s;
+    PM_CUDA(cudaStreamSynchronize(c->stream()));
+    c->started = started != 0;
+    if ((s = c->read_state()) != PM_OK) return s;
+    c->host_state->has_invariant = 0;
+    c->host_state->steps = 0;
+    if ((s = c->write_state()) != PM_OK) return s;
+    return c->reset_ledger();
+}
+
+pm_status pm_cavity_download(pm_cavity* cp, double* ex, double* ey, double* ez, double* hx, double* hy, double* hz) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    double* dst[6] = {ex, ey, ez, hx, hy, hz};
+    pm_status s;
+    for (int q = 0; q < 6; ++q)
+        if ((s = c->get(q, dst[q])) != PM_OK) return s;
+    return PM_OK;
+}
+
+pm_status pm_cavity_release_mode(pm_cavity* cp, int m_in, int p_in, double amplitude, double dt) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    // cavity.rs:675-732
+    const double m = (double)std::max(m_in, 1), p = (double)std::max(p_in, 1);
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const double sx = (double)nx * c->dx, sz = (double)nz * c->dx;
+    const double kx = M_PI * m / sx, kz = M_PI * p / sz;
+    std::vector<double> ey(c->count(1), 0.0);
+    for (int k = 0; k <= nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i <= nx; ++i) {
+                const double x = (double)i * c->dx, z = (double)k * c->dx;
+                ey[i + (size_t)(nx + 1) * (j + (size_t)ny * k)] = amplitude * std::sin(kx * x) * std::sin(kz * z);
+            }
+    // enforce_walls (cavity.rs:1296-1343): Ey is tangential to the x and z walls
+    for (int k = 0; k <= nz; ++k)
+        for (int j = 0; j < ny; ++j) {
+            ey[0 + (size_t)(nx + 1) * (j + (size_t)ny * k)] = 0.0;
+            ey[nx + (size_t)(nx + 1) * (j + (size_t)ny * k)] = 0.0;
+        }
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i <= nx; ++i) {
+            ey[i + (size_t)(nx + 1) * (j + (size_t)ny * 0)] = 0.0;
+            ey[i + (size_t)(nx + 1) * (j + (size_t)ny * nz)] = 0.0;
+        }
+    pm_status s;
+    if ((s = c->read_state()) != PM_OK) return s;
+    c->host_state->violated = kRunning;
+    c->host_state->has_invariant = 0;
+    c->host_state->steps = 0;
+    if ((s = c->write_state()) != PM_OK) return s;
+    for (int q = 0; q < 6; ++q)
+        if ((s = c->put(q, q == 1 ? ey.data() : nullptr)) != PM_OK) return s;
+    // H = +(dt/2μ)∇×E with the scheme's own stencil, then the invariant from a trial step
+    if ((s = c->launch_h((-0.5 * dt) / c->dx, 0, c->stream())) != PM_OK) return s;
+    c->started = true;
+    for (int q = 0; q < 3; ++q) {
+        const size_t bytes = c->count(q + 3) * c->esize();
+        if (!c->keep[q].p) PM_CUDA(c->keep[q].alloc(bytes));
+        PM_CUDA(cudaMemcpyAsync(c->keep[q].p, c->f[q + 3].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
+    }
+    if ((s = c->launch_h(dt / c->dx, 1, c->stream())) != PM_OK) return s;
+    for (int q = 0; q < 3; ++q)
+        PM_CUDA(cudaMemcpyAsync(c->f[q + 3].p, c->keep[q].p, c->count(q + 3) * c->esize(), cudaMemcpyDeviceToDevice,
+                                c->stream()));
+    PM_CUDA(cudaStreamSynchronize(c->stream()));
+    return c->reset_ledger();
+}
+
+pm_status pm_cavity_set_source(pm_cavity* cp, long long edge, const double* cur, size_t n) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (edge < 0 || (size_t)edge >= c->count(2) || (!cur && n > 0)) return fail(PM_BAD_ARG, "source edge out of range");
+    c->src = edge;
+    c->ncurrent = (long long)n;
+    if (n > 0) {
+        PM_CUDA(c->current.alloc(n * 8));
+        PM_CUDA(cudaMemcpy(c->current.p, cur, n * 8, cudaMemcpyHostToDevice));
+    }
+    c->drop_graphs();
+    return c->reset_ledger();
+}
+
+pm_status pm_cavity_courant_limit(pm_cavity* cp, double* seconds) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (!seconds) return fail(PM_BAD_ARG, "null output");
+    *seconds = c->courant_limit();
+    return PM_OK;
+}
+
+pm_status pm_cavity_set_tolerance(pm_cavity* cp, double tol) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    c->tolerance = tol;
+    return PM_OK;
+}
+
+pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violation* out) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
+    if (nsteps == 0) return PM_OK;
+    for (int w = 0; w < 6; ++w)
+        if (c->boundary[w] != 0)
+            return fail(PM_UNSUPPORTED, "magnetic and open (Mur) walls are not on the GPU path; conducting walls only");
+    // cavity.rs:1469-1480
+    const double h = dt, limit = c->courant_limit();
+    if (h > limit) {
+        fill_violation(out, "Courant number", c->name, limit, h, limit, 0.0, 1);
+        set_error("Courant limit");
+        return PM_VIOLATION;
+    }
+    pm_status s = c->begin_call();
+    if (s != PM_OK) return s;
+    const long long before = c->host_state->steps;
+    if (!c->started) {  // cavity.rs:1486-1489
+        if ((s = c->launch_h((0.5 * h) / c->dx, 0, c->stream())) != PM_OK) return s;
+        c->started = true;
+    }
+    const double g = h / c->dx;
+    s = c->run_steps(nsteps, dt, false, [c, g, h](int, cudaStream_t st) {
+        cudaError_t e;
+        if (c->precision == PM_PLAIN_F64) {
+            if ((e = launch_yee_h<double>(c->hargs<double>(g, 1), st)) != cudaSuccess) return e;
+            return launch_yee_e<double>(c->eargs<double>(h), st);
+        }
+        if ((e = launch_yee_h<float>(c->hargs<float>(g, 1), st)) != cudaSuccess) return e;
+        return launch_yee_e<float>(c->eargs<float>(h), st);
+    });
+    if (s != PM_OK) return s;
+    return c->finish_call(before, out, "simulation", "simulation", false);
+}
+
+pm_status pm_cavity_ledger(pm_cavity* cp, pm_ledger* out) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (!out) return fail(PM_BAD_ARG, "null output");
+    pm_status s = c->read_state();
+    if (s != PM_OK) return s;
+    std::memset(out, 0, sizeof(*out));
+    const DevState* st = c->host_state;
+    out->total = st->total;
+    out->scale = st->scale;
+    out->n_parts = 3;
+    out->parts[0] = st->part[0];
+    out->parts[1] = st->part[1];
+    out->parts[2] = st->part[2];
+    out->steps = st->steps;
+    return PM_OK;
+}
+
+pm_status pm_cavity_energies(pm_cavity* cp, double* electric, double* magnetic) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    return c->measure_naive(electric, magnetic);
+}
+
+pm_status pm_cavity_checkpoint(pm_cavity* cp) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    for (int q = 0; q < 6; ++q) {
+        const size_t bytes = c->count(q) * c->esize();
+        if (!c->sf[q].p) PM_CUDA(c->sf[q].alloc(bytes));
+        PM_CUDA(cudaMemcpyAsync(c->sf[q].p, c->f[q].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
+    }
+    pm_status s = c->read_state();
+    if (s != PM_OK) return s;
+    c->s_started = c->started;
+    c->s_dissipated = c->host_state->dissipated;
+    c->has_saved = true;
+    return PM_OK;
+}
+
+pm_status pm_cavity_restore(pm_cavity* cp) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (!c->has_saved) return PM_OK;
+    for (int q = 0; q < 6; ++q)
+        PM_CUDA(cudaMemcpyAsync(c->f[q].p, c->sf[q].p, c->count(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
+    pm_status s = c->read_state();
+    if (s != PM_OK) return s;
+    c->started = c->s_started;
+    c->host_state->dissipated = c->s_dissipated;
+    if ((s = c->write_state()) != PM_OK) return s;
+    c->has_saved = false;  // cavity.rs:1580 takes the checkpoint
+    return c->reset_ledger();
+}
+
+pm_status pm_cavity_set_stream(pm_cavity* cp, void* stream) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    PM_CUDA(cudaStreamSynchronize(c->stream()));
+    c->user = static_cast<cudaStream_t>(stream);
+    return PM_OK;
+}
+
+void pm_cavity_destroy(pm_cavity* cp) { delete reinterpret_cast<Cavity*>(cp); }
+
+}  // extern "C"

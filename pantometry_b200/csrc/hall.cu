@@ -1,0 +1,420 @@
+// pm_hall: the device form of `Hall` (crates/pantometry-acoustic/src/hall.rs).
+#include <algorithm>
+#include <limits>
+#include <new>
+
+#include "runtime.h"
+
+namespace pm {
+
+struct Hall : Handle {
+    int nx = 2, ny = 1, nz = 1;
+    double dx = 0.0, speed = 0.0, density = 0.0;
+    bool staggered = false;  // hall.rs:84-85 `velocity_staggered`
+    DBuf p[2], vx[2], vy[2], vz[2];
+    DBuf stage;
+    // point source (extension)
+    long long src = -1;
+    DBuf wave;
+    long long nwave = 0;
+    double wsrc = 0.0;
+    // heterogeneous speed (extension)
+    int block = 0, nbx = 0, nby = 0, nbz = 0;
+    DBuf bscale, bknode;
+    std::vector<double> speeds;
+    double max_speed = 0.0;
+    double bscale_dt = NAN;
+    // checkpoint (hall.rs:536-555)
+    DBuf sp, svx, svy, svz;
+    bool s_staggered = false;
+
+    size_t nodes() const { return (size_t)nx * ny * nz; }
+    size_t nvx() const { return (size_t)(nx - 1) * ny * nz; }
+    size_t nvy() const { return (size_t)nx * (ny - 1) * nz; }
+    size_t nvz() const { return (size_t)nx * ny * (nz - 1); }
+    size_t esize() const { return precision == PM_PLAIN_F64 ? 8 : 4; }
+    double rc2() const { return density * speed * speed; }
+    double volume() const { return dx * dx * dx; }
+
+    template <typename Real>
+    HallArgs<Real> args(int par, double h, bool starting) const {
+        HallArgs<Real> a{};
+        a.p0 = p[par].as<Real>(); a.vx0 = vx[par].as<Real>(); a.vy0 = vy[par].as<Real>(); a.vz0 = vz[par].as<Real>();
+        a.p1 = p[par ^ 1].as<Real>(); a.vx1 = vx[par ^ 1].as<Real>(); a.vy1 = vy[par ^ 1].as<Real>(); a.vz1 = vz[par ^ 1].as<Real>();
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        const double vh = starting ? 0.5 * h : h;  // hall.rs:428
+        a.gain = (Real)(vh / (density * dx));       // hall.rs:433
+        a.scale = (Real)(h * rc2() / dx);           // hall.rs:464
+        if (block > 0) {
+            a.block_scale = bscale.as<Real>();
+            a.block_knode = bknode.as<double>();
+            a.block = block; a.nbx = nbx; a.nby = nby;
+        }
+        a.knode = volume() / (2.0 * rc2());
+        a.kface = 0.5 * density * volume();
+        a.src = src;
+        a.wave = wave.as<double>();
+        a.nwave = nwave;
+        a.wsrc = wsrc;
+        a.starting = starting ? 1 : 0;
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        a.nblocks = plane_blocks(nx, ny, nz);
+        return a;
+    }
+
+    pm_status launch_one(int par, double h, bool starting, cudaStream_t s) const {
+        if (precision == PM_PLAIN_F64) PM_CUDA(launch_hall<double>(args<double>(par, h, starting), s));
+        else PM_CUDA(launch_hall<float>(args<float>(par, h, starting), s));
+        return PM_OK;
+    }
+
+    // Per-block scale h·ρc_b²/dx (in the field type) and invariant weight V/(2ρc_b²).
+    pm_status upload_block_scale(double h) {
+        if (block <= 0 || bscale_dt == h) return PM_OK;
+        const size_t nb = speeds.size();
+        std::vector<double> kn(nb), sc64(nb);
+        std::vector<float> sc32(nb);
+        for (size_t b = 0; b < nb; ++b) {
+            const double r = density * speeds[b] * speeds[b];
+            kn[b] = volume() / (2.0 * r);
+            sc64[b] = h * r / dx;
+            sc32[b] = (float)sc64[b];
+        }
+        if (!bscale.p) PM_CUDA(bscale.alloc(nb * 8));
+        if (!bknode.p) PM_CUDA(bknode.alloc(nb * 8));
+        if (precision == PM_PLAIN_F64) PM_CUDA(cudaMemcpy(bscale.p, sc64.data(), nb * 8, cudaMemcpyHostToDevice));
+        else PM_CUDA(cudaMemcpy(bscale.p, sc32.data(), nb * 4, cudaMemcpyHostToDevice));
+        PM_CUDA(cudaMemcpy(bknode.p, kn.data(), nb * 8, cudaMemcpyHostToDevice));
+        bscale_dt = h;
+        drop_graphs();
+        return PM_OK;
+    }
+
+    // `invariant_si` of the present state (hall.rs:334-384), into host_state->invariant.
+    pm_status measure(int par_p, int par_pp) {
+        if (precision == PM_PLAIN_F64) {
+            HallMeasureArgs<double> m{};
+            m.p = p[par_p].as<double>(); m.pp = p[par_pp].as<double>();
+            m.vx = vx[parity].as<double>(); m.vy = vy[parity].as<double>(); m.vz = vz[parity].as<double>();
+            m.nx = nx; m.ny = ny; m.nz = nz;
+            m.knode = volume() / (2.0 * rc2()); m.kface = 0.5 * density * volume();
+            if (block > 0) { m.block_knode = bknode.as<double>(); m.block = block; m.nbx = nbx; m.nby = nby; }
+            m.st = state.as<DevState>(); m.partials = partials.as<double>(); m.nblocks = plane_blocks(nx, ny, nz);
+            PM_CUDA(launch_hall_measure<double>(m, stream()));
+        } else {
+            HallMeasureArgs<float> m{};
+            m.p = p[par_p].as<float>(); m.pp = p[par_pp].as<float>();
+            m.vx = vx[parity].as<float>(); m.vy = vy[parity].as<float>(); m.vz = vz[parity].as<float>();
+            m.nx = nx; m.ny = ny; m.nz = nz;
+            m.knode = volume() / (2.0 * rc2()); m.kface = 0.5 * density * volume();
+            if (block > 0) { m.block_knode = bknode.as<double>(); m.block = block; m.nbx = nbx; m.nby = nby; }
+            m.st = state.as<DevState>(); m.partials = partials.as<double>(); m.nblocks = plane_blocks(nx, ny, nz);
+            PM_CUDA(launch_hall_measure<float>(m, stream()));
+        }
+        return read_state();
+    }
+
+    // Host f64 → device field (converted to f32 on the device for the chosen form).
+    pm_status put(DBuf& dst, const double* src_host, size_t n) {
+        if (precision == PM_PLAIN_F64) {
+            PM_CUDA(cudaMemcpyAsync(dst.p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
+        } else {
+            if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(std::max<size_t>(n, 1) * 8));
+            PM_CUDA(cudaMemcpyAsync(stage.p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
+            PM_CUDA(launch_to_f32(stage.as<double>(), dst.as<float>(), n, stream()));
+        }
+        return PM_OK;
+    }
+    pm_status get(const DBuf& src_dev, double* dst_host, size_t n) {
+        if (!dst_host) return PM_OK;
+        if (precision == PM_PLAIN_F64) {
+            PM_CUDA(cudaMemcpyAsync(dst_host, src_dev.p, n * 8, cudaMemcpyDeviceToHost, stream()));
+        } else {
+            if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(std::max<size_t>(n, 1) * 8));
+            PM_CUDA(launch_to_f64(src_dev.as<float>(), stage.as<double>(), n, stream()));
+            PM_CUDA(cudaMemcpyAsync(dst_host, stage.p, n * 8, cudaMemcpyDeviceToHost, stream()));
+        }
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        return PM_OK;
+    }
+};
+
+}  // namespace pm
+
+using namespace pm;
+
+#define HALL_GUARD(h)                                          \
+    do {                                                       \
+        if (!(h)) return fail(PM_BAD_ARG, "null pm_hall");      \
+        cudaSetDevice((h)->device);                            \
+    } while (0)
+
+extern "C" {
+
+pm_status pm_hall_create(const pm_hall_desc* d, pm_hall** out) {
+    if (!d || !out) return fail(PM_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (d->precision != PM_PLAIN_F64 && d->precision != PM_FIELDS_F32) return fail(PM_BAD_ARG, "unknown precision");
+    Hall* h = new (std::nothrow) Hall();
+    if (!h) return fail(PM_OUT_OF_MEMORY, "host allocation");
+    h->name = d->name ? d->name : "hall";
+    h->precision = d->precision;
+    // hall.rs:108-114
+    h->nx = std::max(d->across, 2);
+    h->dx = std::max(d->width / (double)(h->nx - 1), std::numeric_limits<double>::min());
+    auto quantise = [&](double l) { return (int)std::max(std::round(l / h->dx), 0.0) + 1; };
+    h->ny = quantise(d->height);
+    h->nz = quantise(d->depth);
+    h->speed = d->speed;
+    h->density = d->density;
+    h->max_speed = d->speed;
+    pm_status s = h->init(d->device, (size_t)plane_blocks(h->nx, h->ny, h->nz) * 3);
+    if (s != PM_OK) { delete h; return s; }
+    for (int q = 0; q < 2; ++q) {
+        cudaError_t e;
+        if ((e = h->p[q].alloc(h->nodes() * h->esize())) != cudaSuccess ||
+            (e = h->vx[q].alloc(h->nvx() * h->esize())) != cudaSuccess ||
+            (e = h->vy[q].alloc(h->nvy() * h->esize())) != cudaSuccess ||
+            (e = h->vz[q].alloc(h->nvz() * h->esize())) != cudaSuccess) {
+            delete h;
+            return cuda_fail(e, "cudaMalloc hall fields");
+        }
+    }
+    *out = reinterpret_cast<pm_hall*>(h);
+    std::vector<double> zero(h->nodes(), 0.0);
+    s = pm_hall_release(*out, zero.data(), zero.size());  // Hall::new is at rest
+    if (s != PM_OK) { delete h; *out = nullptr; }
+    return s;
+}
+
+pm_status pm_hall_nodes(pm_hall* hp, int* nx, int* ny, int* nz, double* dx) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (nx) *nx = h->nx;
+    if (ny) *ny = h->ny;
+    if (nz) *nz = h->nz;
+    if (dx) *dx = h->dx;
+    return PM_OK;
+}
+
+pm_status pm_hall_release(pm_hall* hp, const double* pressure, size_t n) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (!pressure || n != h->nodes()) return fail(PM_BAD_ARG, "release: one pressure per node");
+    // hall.rs:166-184: pressure from the profile, pressure_prev = pressure, v = 0, then the datum
+    h->parity = 0;
+    pm_status s;
+    if ((s = h->put(h->p[0], pressure, n)) != PM_OK) return s;
+    PM_CUDA(cudaMemcpyAsync(h->p[1].p, h->p[0].p, n * h->esize(), cudaMemcpyDeviceToDevice, h->stream()));
+    for (int q = 0; q < 2; ++q) {
+        PM_CUDA(cudaMemsetAsync(h->vx[q].p, 0, h->nvx() * h->esize(), h->stream()));
+        PM_CUDA(cudaMemsetAsync(h->vy[q].p, 0, h->nvy() * h->esize(), h->stream()));
+        PM_CUDA(cudaMemsetAsync(h->vz[q].p, 0, h->nvz() * h->esize(), h->stream()));
+    }
+    h->staggered = false;
+    if ((s = h->measure(0, 1)) != PM_OK) return s;
+    DevState* st = h->host_state;
+    const double datum = st->invariant;
+    std::memset(st, 0, sizeof(DevState));
+    st->tol = h->tolerance;
+    st->datum = datum;
+    st->invariant = datum;
+    st->offset = 0.0;
+    st->total = datum;  // Ledger::new().with(ENERGY, energy()) with energy = invariant + 0
+    st->scale = std::fabs(datum);
+    st->part[0] = datum;
+    st->prev_total = st->total;
+    st->prev_scale = st->scale;
+    return h->write_state();
+}
+
+pm_status pm_hall_set_source(pm_hall* hp, long long node, const double* wave, size_t n) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (node < 0 || (size_t)node >= h->nodes() || (!wave && n > 0)) return fail(PM_BAD_ARG, "source node out of range");
+    h->src = node;
+    h->nwave = (long long)n;
+    if (n > 0) {
+        PM_CUDA(h->wave.alloc(n * 8));
+        PM_CUDA(cudaMemcpy(h->wave.p, wave, n * 8, cudaMemcpyHostToDevice));
+    }
+    const int i = (int)(node % h->nx), j = (int)((node / h->nx) % h->ny), k = (int)(node / ((long long)h->nx * h->ny));
+    auto w = [](int q, int m) { return (q == 0 || q + 1 == m) ? 2.0 : 1.0; };
+    const double share = 1.0 / (w(i, h->nx) * w(j, h->ny) * w(k, h->nz));
+    h->wsrc = share * (h->dx * h->dx * h->dx) / (2.0 * h->rc2());
+    if (h->block > 0) {
+        const double c = h->speeds[(size_t)(i / h->block) + (size_t)h->nbx * ((size_t)(j / h->block) + (size_t)h->nby * (k / h->block))];
+        h->wsrc = share * (h->dx * h->dx * h->dx) / (2.0 * (h->density * c * c));
+    }
+    h->drop_graphs();
+    return PM_OK;
+}
+
+pm_status pm_hall_set_speed_blocks(pm_hall* hp, int block, const double* speeds, size_t n) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (block <= 0 || !speeds) return fail(PM_BAD_ARG, "block must be positive and speeds non-null");
+    const int nbx = (h->nx + block - 1) / block, nby = (h->ny + block - 1) / block, nbz = (h->nz + block - 1) / block;
+    if (n != (size_t)nbx * nby * nbz) return fail(PM_BAD_ARG, "speeds: one per block");
+    h->block = block; h->nbx = nbx; h->nby = nby; h->nbz = nbz;
+    h->speeds.assign(speeds, speeds + n);
+    h->max_speed = *std::max_element(h->speeds.begin(), h->speeds.end());
+    h->bscale_dt = NAN;
+    h->bscale.release();
+    h->bknode.release();
+    h->drop_graphs();
+    pm_status s = h->upload_block_scale(0.0);
+    if (s != PM_OK) return s;
+    h->bscale_dt = NAN;
+    // the datum of the present state under the new weights
+    const int par = h->parity;
+    if ((s = h->measure(par, par ^ 1)) != PM_OK) return s;
+    DevState* st = h->host_state;
+    if (!h->staggered) {
+        st->datum = st->invariant;
+        st->total = st->invariant + st->offset - st->injected;
+        st->scale = std::fabs(st->total);
+        st->prev_total = st->total;
+        st->prev_scale = st->scale;
+    }
+    return h->write_state();
+}
+
+pm_status pm_hall_max_stable_dt(pm_hall* hp, double* seconds) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (!seconds) return fail(PM_BAD_ARG, "null output");
+    // hall.rs:401-406 (with the fastest block when the speed varies)
+    const double c = h->block > 0 ? h->max_speed : h->speed;
+    *seconds = c <= 0.0 ? std::numeric_limits<double>::infinity() : h->dx / (c * std::sqrt(3.0));
+    return PM_OK;
+}
+
+pm_status pm_hall_set_tolerance(pm_hall* hp, double tol) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    h->tolerance = tol;
+    return PM_OK;
+}
+
+pm_status pm_hall_step(pm_hall* hp, double dt, long long nsteps, pm_violation* out) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
+    if (nsteps == 0) return PM_OK;
+    // hall.rs:409-419
+    const double c = h->block > 0 ? h->max_speed : h->speed;
+    const double courant = c * dt * std::sqrt(3.0) / h->dx;
+    if (courant > 1.0 + 1e-12) {
+        fill_violation(out, "Courant number", h->name + " (three-dimensional wave equation)", 1.0, courant, 1.0, 1e-12, 1);
+        set_error("Courant number past the limit");
+        return PM_VIOLATION;
+    }
+    if (dt <= 0.0) return PM_OK;  // hall.rs:421-423
+    pm_status s;
+    if ((s = h->upload_block_scale(dt)) != PM_OK) return s;
+    if ((s = h->begin_call()) != PM_OK) return s;
+    const long long before = h->host_state->steps;
+    long long remaining = nsteps;
+    if (!h->staggered) {
+        if ((s = h->launch_one(h->parity, dt, true, h->stream())) != PM_OK) return s;
+        h->parity ^= 1;
+        h->staggered = true;
+        remaining -= 1;
+    }
+    s = h->run_steps(remaining, dt, true, [h, dt](int par, cudaStream_t st) {
+        return h->precision == PM_PLAIN_F64 ? launch_hall<double>(h->args<double>(par, dt, false), st)
+                                            : launch_hall<float>(h->args<float>(par, dt, false), st);
+    });
+    if (s != PM_OK) return s;
+    return h->finish_call(before, out, h->name + " (its own books, against what it moved on the bus)",
+                          h->name + " (starting the leapfrog)", true);
+}
+
+pm_status pm_hall_ledger(pm_hall* hp, pm_ledger* out) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (!out) return fail(PM_BAD_ARG, "null output");
+    pm_status s = h->read_state();
+    if (s != PM_OK) return s;
+    std::memset(out, 0, sizeof(*out));
+    const DevState* st = h->host_state;
+    out->total = st->total;
+    out->scale = st->scale;
+    out->n_parts = 4;
+    out->parts[0] = st->invariant;
+    out->parts[1] = st->offset;
+    out->parts[2] = -st->injected;
+    out->parts[3] = st->datum;
+    out->steps = st->steps;
+    return PM_OK;
+}
+
+pm_status pm_hall_download(pm_hall* hp, double* pr, double* pp, double* vx, double* vy, double* vz) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    const int par = h->parity;
+    pm_status s;
+    if ((s = h->get(h->p[par], pr, h->nodes())) != PM_OK) return s;
+    if ((s = h->get(h->p[par ^ 1], pp, h->nodes())) != PM_OK) return s;
+    if ((s = h->get(h->vx[par], vx, h->nvx())) != PM_OK) return s;
+    if ((s = h->get(h->vy[par], vy, h->nvy())) != PM_OK) return s;
+    return h->get(h->vz[par], vz, h->nvz());
+}
+
+pm_status pm_hall_checkpoint(pm_hall* hp) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    const int par = h->parity;
+    auto save = [&](DBuf& dst, const DBuf& src, size_t n) -> pm_status {
+        if (!dst.p) PM_CUDA(dst.alloc(std::max<size_t>(n, 1) * h->esize()));
+        PM_CUDA(cudaMemcpyAsync(dst.p, src.p, n * h->esize(), cudaMemcpyDeviceToDevice, h->stream()));
+        return PM_OK;
+    };
+    pm_status s;
+    if ((s = save(h->sp, h->p[par], h->nodes())) != PM_OK) return s;
+    if ((s = save(h->svx, h->vx[par], h->nvx())) != PM_OK) return s;
+    if ((s = save(h->svy, h->vy[par], h->nvy())) != PM_OK) return s;
+    if ((s = save(h->svz, h->vz[par], h->nvz())) != PM_OK) return s;
+    h->s_staggered = h->staggered;
+    h->has_saved = true;
+    PM_CUDA(cudaStreamSynchronize(h->stream()));
+    return PM_OK;
+}
+
+pm_status pm_hall_restore(pm_hall* hp) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (!h->has_saved) return PM_OK;
+    const int par = h->parity;
+    const size_t e = h->esize();
+    // hall.rs:546-555: pressure_prev = pressure = saved
+    PM_CUDA(cudaMemcpyAsync(h->p[par].p, h->sp.p, h->nodes() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->p[par ^ 1].p, h->sp.p, h->nodes() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->vx[par].p, h->svx.p, h->nvx() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->vy[par].p, h->svy.p, h->nvy() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->vz[par].p, h->svz.p, h->nvz() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    h->staggered = h->s_staggered;
+    pm_status s = h->measure(par, par ^ 1);
+    if (s != PM_OK) return s;
+    DevState* st = h->host_state;
+    st->total = st->invariant + st->offset - st->injected;
+    st->scale = std::fabs(st->total);
+    st->part[0] = st->total;
+    st->prev_total = st->total;
+    st->prev_scale = st->scale;
+    return h->write_state();
+}
+
+pm_status pm_hall_set_stream(pm_hall* hp, void* stream) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    PM_CUDA(cudaStreamSynchronize(h->stream()));
+    h->user = static_cast<cudaStream_t>(stream);
+    return PM_OK;
+}
+
+void pm_hall_destroy(pm_hall* hp) { delete reinterpret_cast<Hall*>(hp); }
+
+}  // extern "C"

@@ -1,0 +1,534 @@
+// pm_heat: the device form of `Solid3D` (crates/pantometry-thermal/src/solid.rs).
+#include <algorithm>
+#include <limits>
+#include <new>
+
+#include "runtime.h"
+
+namespace pm {
+
+namespace {
+
+constexpr double kStableFourier3D = 1.0 / 6.0;  // solid.rs:84
+
+double host_series_with_half_cell(double film, double conductivity, double area, double dx) {  // solid.rs:110-122
+    if (film <= 0.0) return 0.0;
+    double half = 2.0 * conductivity * area / dx;
+    if (!std::isfinite(half)) return film;
+    if (half <= 0.0) return 0.0;
+    return 1.0 / (1.0 / film + 1.0 / half);
+}
+
+double rust_max(double a, double b) {  // f64::max
+    if (std::isnan(a)) return b;
+    if (std::isnan(b)) return a;
+    return a > b ? a : b;
+}
+
+}  // namespace
+
+struct Heat : Handle {
+    int nx = 1, ny = 1, nz = 1;
+    double dx = 0.0, reference = 0.0;
+    std::vector<pm_substance> mats;
+    std::vector<uint32_t> which;  // empty while the block is one material
+    HeatFilms films{};
+    double film_conv[6] = {0, 0, 0, 0, 0, 0};
+    // `resolve` products (solid.rs:588-784)
+    bool uniform = true;
+    double kface = 0.0, mobility = 0.0, capacity = 0.0;
+    std::vector<double> kx, ky, kz, mob, cap;
+    double worst_rate = 0.0;
+    double cap_sum = 0.0;
+    // device buffers
+    DBuf field[2];  // f64 kelvin (plain) or f32 deviations
+    DBuf dkx, dky, dkz, dmob, dcap, dwhich, dmatk, dmateps;
+    DBuf saved;
+    DBuf stage;     // f64 staging for uploads/downloads of the f32 form
+    double saved_lost = 0.0, saved_supplied = 0.0;
+
+    size_t n() const { return (size_t)nx * ny * nz; }
+    size_t esize() const { return precision == PM_PLAIN_F64 ? sizeof(double) : sizeof(float); }
+
+    double mat_k(uint32_t m) const { return mats[m].thermal ? mats[m].conductivity : std::numeric_limits<double>::infinity(); }
+    double mat_eps(uint32_t m) const { return mats[m].thermal ? mats[m].emissivity : 0.0; }
+    uint32_t mat_of(size_t c) const { return which.empty() ? 0u : which[c]; }
+
+    // Per-cell (k, C) of a one-phase block (solid.rs:600-702 with φ = 0).
+    void cell_props(size_t c, double& k, double& C) const {
+        const pm_substance& s = mats[mat_of(c)];
+        const double volume = dx * dx * dx;
+        const double ks = s.thermal ? s.conductivity : NAN;
+        const double cs = s.thermal ? (s.density * volume) * s.specific_heat : NAN;
+        const double phi = 0.0;
+        k = ks + phi * (ks - ks);
+        C = cs + phi * (cs - cs);
+    }
+    static double series(double a, double b) {
+        double sum = a + b;
+        return sum > 0.0 ? 2.0 * a * b / sum : 0.0;
+    }
+
+    // Face conductivities of a uniform block: zero on the outer faces, `kface` inside.
+    double face_x(int i) const { return (i > 0 && i < nx) ? kface : 0.0; }
+    double face_y(int j) const { return (j > 0 && j < ny) ? kface : 0.0; }
+    double face_z(int k) const { return (k > 0 && k < nz) ? kface : 0.0; }
+
+    double face_sum_at(int i, int j, int k) const {  // solid.rs:757-762
+        if (uniform)
+            return face_x(i) + face_x(i + 1) + face_y(j) + face_y(j + 1) + face_z(k) + face_z(k + 1);
+        return kx[i + (size_t)(nx + 1) * (j + (size_t)ny * k)] + kx[i + 1 + (size_t)(nx + 1) * (j + (size_t)ny * k)] +
+               ky[i + (size_t)nx * (j + (size_t)(ny + 1) * k)] + ky[i + (size_t)nx * (j + 1 + (size_t)(ny + 1) * k)] +
+               kz[i + (size_t)nx * (j + (size_t)ny * k)] + kz[i + (size_t)nx * (j + (size_t)ny * (k + 1))];
+    }
+    double mob_at(size_t c) const { return uniform ? mobility : mob[c]; }
+
+    // solid.rs:588-784 for a one-phase block with no void.
+    void resolve() {
+        uniform = mats.size() == 1;
+        const size_t N = n();
+        if (uniform) {
+            double k, C;
+            cell_props(0, k, C);
+            kface = series(k, k);
+            capacity = C;
+            mobility = dx / C;
+            kx.clear(); ky.clear(); kz.clear(); mob.clear(); cap.clear();
+            cap_sum = -0.0;
+            for (size_t c = 0; c < N; ++c) cap_sum += C;
+            // The rate is the same within each class of cell (interior, face, edge, corner), so
+            // sampling i, j, k at 0, 1, n-2, n-1 visits every distinct value.
+            worst_rate = 0.0;
+            bool nowhere = false;
+            for (int k3 : {0, 1, nz - 2, nz - 1}) {
+                if (k3 < 0 || k3 >= nz) continue;
+                for (int j3 : {0, 1, ny - 2, ny - 1}) {
+                    if (j3 < 0 || j3 >= ny) continue;
+                    for (int i3 : {0, 1, nx - 2, nx - 1}) {
+                        if (i3 < 0 || i3 >= nx) continue;
+                        double rate = mobility * face_sum_at(i3, j3, k3);
+                        if (std::isnan(rate)) nowhere = true;
+                        else worst_rate = rust_max(worst_rate, rate);
+                    }
+                }
+            }
+            if (nowhere) worst_rate = NAN;
+            return;
+        }
+        std::vector<double> km(N), cm(N);
+        for (size_t c = 0; c < N; ++c) cell_props(c, km[c], cm[c]);
+        kx.assign((size_t)(nx + 1) * ny * nz, 0.0);
+        ky.assign((size_t)nx * (ny + 1) * nz, 0.0);
+        kz.assign((size_t)nx * ny * (nz + 1), 0.0);
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+                    if (i > 0) kx[i + (size_t)(nx + 1) * (j + (size_t)ny * k)] = series(km[c - 1], km[c]);
+                    if (j > 0) ky[i + (size_t)nx * (j + (size_t)(ny + 1) * k)] = series(km[c - nx], km[c]);
+                    if (k > 0) kz[i + (size_t)nx * (j + (size_t)ny * k)] = series(km[c - (size_t)nx * ny], km[c]);
+                }
+        cap.assign(N, 0.0);
+        mob.assign(N, 0.0);
+        worst_rate = 0.0;
+        cap_sum = -0.0;
+        bool nowhere = false;
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+                    cap[c] = cm[c];
+                    mob[c] = dx / cm[c];
+                    cap_sum += cm[c];
+                    double rate = mob[c] * face_sum_at(i, j, k);
+                    if (std::isnan(rate)) nowhere = true;
+                    else worst_rate = rust_max(worst_rate, rate);
+                }
+        if (nowhere) worst_rate = NAN;
+    }
+
+    bool any_radiative_film() const {
+        for (int f = 0; f < 6; ++f)
+            if (((films.exposed >> f) & 1)) {
+                for (uint32_t m = 0; m < mats.size(); ++m)
+                    if (mat_eps(m) != 0.0) return true;
+            }
+        return false;
+    }
+
+    size_t cells_on(int f) const {  // solid.rs:1222-1229
+        return f < 2 ? (size_t)ny * nz : (f < 4 ? (size_t)nx * nz : (size_t)nx * ny);
+    }
+
+    // solid.rs:1269-1288 at a temperature-independent film (emissivity zero).
+    double loss_at(int i, int j, int k, size_t c) const {
+        double total = -0.0;
+        for (int f = 0; f < 6; ++f) {
+            if (!((films.exposed >> f) & 1)) continue;
+            bool holds = f == 0 ? i == 0 : f == 1 ? i + 1 == nx : f == 2 ? j == 0 : f == 3 ? j + 1 == ny : f == 4 ? k == 0 : k + 1 == nz;
+            if (!holds) continue;
+            double share = films.share[f];
+            // h + 4εσ·max(T, T∞)³ with ε = 0 (radiating films are refused before this runs)
+            double h = film_conv[f];
+            total += host_series_with_half_cell(h * share, mat_k(mat_of(c)), share, dx);
+        }
+        return total;
+    }
+
+    // solid.rs:1148-1185
+    double worst_rate_now() const {
+        if (films.exposed == 0 || std::isnan(worst_rate)) return worst_rate;
+        double worst = worst_rate;
+        auto visit = [&](int i, int j, int k) {
+            size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+            double loss = loss_at(i, j, k, c);
+            if (loss == 0.0) return;
+            worst = rust_max(worst, mob_at(c) * (face_sum_at(i, j, k) + loss / dx));
+        };
+        if (uniform) {
+            for (int k3 : {0, 1, nz - 2, nz - 1}) {
+                if (k3 < 0 || k3 >= nz) continue;
+                for (int j3 : {0, 1, ny - 2, ny - 1}) {
+                    if (j3 < 0 || j3 >= ny) continue;
+                    for (int i3 : {0, 1, nx - 2, nx - 1})
+                        if (i3 >= 0 && i3 < nx) visit(i3, j3, k3);
+                }
+            }
+        } else {
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i)
+                        if (i == 0 || i + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz) visit(i, j, k);
+        }
+        return worst;
+    }
+
+    pm_status upload_coefficients() {
+        drop_graphs();
+        if (uniform) return PM_OK;
+        if (precision != PM_PLAIN_F64) return fail(PM_UNSUPPORTED, "a filled (multi-material) block runs in the plain f64 form only");
+        auto put = [&](DBuf& b, const void* src, size_t bytes) -> pm_status {
+            PM_CUDA(b.alloc(bytes));
+            PM_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+            return PM_OK;
+        };
+        pm_status s;
+        if ((s = put(dkx, kx.data(), kx.size() * 8)) != PM_OK) return s;
+        if ((s = put(dky, ky.data(), ky.size() * 8)) != PM_OK) return s;
+        if ((s = put(dkz, kz.data(), kz.size() * 8)) != PM_OK) return s;
+        if ((s = put(dmob, mob.data(), mob.size() * 8)) != PM_OK) return s;
+        if ((s = put(dcap, cap.data(), cap.size() * 8)) != PM_OK) return s;
+        std::vector<uint32_t> w(n(), 0u);
+        for (size_t c = 0; c < n(); ++c) w[c] = mat_of(c);
+        if ((s = put(dwhich, w.data(), w.size() * 4)) != PM_OK) return s;
+        std::vector<double> mk(mats.size()), me(mats.size());
+        for (uint32_t m = 0; m < mats.size(); ++m) { mk[m] = mat_k(m); me[m] = mat_eps(m); }
+        if ((s = put(dmatk, mk.data(), mk.size() * 8)) != PM_OK) return s;
+        if ((s = put(dmateps, me.data(), me.size() * 8)) != PM_OK) return s;
+        return PM_OK;
+    }
+
+    HeatPlainArgs plain_args(int par, double dt) const {
+        HeatPlainArgs a{};
+        a.told = field[par].as<double>();
+        a.tnew = field[par ^ 1].as<double>();
+        a.uniform = uniform ? 1 : 0;
+        if (!uniform) {
+            a.kx = dkx.as<double>(); a.ky = dky.as<double>(); a.kz = dkz.as<double>();
+            a.mob = dmob.as<double>(); a.cap = dcap.as<double>();
+            a.which = dwhich.as<uint32_t>(); a.mat_k = dmatk.as<double>(); a.mat_eps = dmateps.as<double>();
+        }
+        a.kface = kface; a.mobility = mobility; a.capacity = capacity;
+        a.k_cell = mat_k(0); a.eps_cell = mat_eps(0);
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        a.dts = dt; a.dx = dx; a.reference = reference;
+        a.films = films;
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        a.nblocks = plane_blocks(nx, ny, nz);
+        return a;
+    }
+
+    static int zchunk_for(int nz) { return nz >= 64 ? 16 : (nz >= 16 ? 8 : 4); }
+
+    HeatF32Args f32_args(int par, double dt) const {
+        HeatF32Args a{};
+        a.dold = field[par].as<float>();
+        a.dnew = field[par ^ 1].as<float>();
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        const double dm = dt * mobility;
+        a.a = (float)(dm * kface);
+        a.exposed = films.exposed;
+        for (int f = 0; f < 6; ++f) {
+            double g = 0.0;
+            if ((films.exposed >> f) & 1) {
+                // The film's conductance with the half cell in series (solid.rs:1192-1219) at zero
+                // emissivity, which does not depend on the temperature difference.
+                g = host_series_with_half_cell(film_conv[f] * films.share[f], mat_k(0), films.share[f], dx);
+            }
+            a.b[f] = (float)(dm * g / dx);
+            a.off[f] = (float)(reference - films.ambient[f]);
+        }
+        a.capacity = capacity;
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        const int zc = zchunk_for(nz);
+        a.nblocks = ((nx + 31) / 32) * ((ny + 7) / 8) * ((nz + zc - 1) / zc);
+        return a;
+    }
+
+    pm_status measure() {  // the opening ledger of the present state
+        HeatMeasureArgs m{};
+        if (precision == PM_PLAIN_F64) m.t64 = field[parity].as<double>();
+        else m.d32 = field[parity].as<float>();
+        m.cap = uniform ? nullptr : dcap.as<double>();
+        m.capacity = capacity;
+        m.reference = reference;
+        m.n = n();
+        m.st = state.as<DevState>();
+        m.partials = partials.as<double>();
+        m.nblocks = kMeasureBlocks;
+        PM_CUDA(precision == PM_PLAIN_F64 ? launch_heat_measure_plain(m, stream()) : launch_heat_measure_f32(m, stream()));
+        return read_state();
+    }
+};
+
+}  // namespace pm
+
+using namespace pm;
+
+#define HEAT_GUARD(h)                                          \
+    do {                                                       \
+        if (!(h)) return fail(PM_BAD_ARG, "null pm_heat");      \
+        cudaSetDevice((h)->device);                            \
+    } while (0)
+
+extern "C" {
+
+pm_status pm_heat_create(const pm_heat_desc* d, pm_heat** out) {
+    if (!d || !out) return fail(PM_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (d->precision != PM_PLAIN_F64 && d->precision != PM_FIELDS_F32) return fail(PM_BAD_ARG, "unknown precision");
+    if (!(d->dx > 0.0)) return fail(PM_BAD_ARG, "dx must be positive");
+    Heat* h = new (std::nothrow) Heat();
+    if (!h) return fail(PM_OUT_OF_MEMORY, "host allocation");
+    h->name = d->name ? d->name : "block";
+    h->nx = std::max(d->nx, 1); h->ny = std::max(d->ny, 1); h->nz = std::max(d->nz, 1);
+    h->dx = d->dx;
+    h->reference = d->initial_kelvin;
+    h->precision = d->precision;
+    h->mats.push_back(d->substance);
+    h->resolve();
+    const int zc = Heat::zchunk_for(h->nz);
+    size_t nblocks = std::max<size_t>(std::max<size_t>(plane_blocks(h->nx, h->ny, h->nz),
+                                                       (size_t)((h->nx + 31) / 32) * ((h->ny + 7) / 8) * ((h->nz + zc - 1) / zc)),
+                                      kMeasureBlocks);
+    pm_status s = h->init(d->device, nblocks * 2);
+    if (s != PM_OK) { delete h; return s; }
+    for (auto& f : h->field) {
+        cudaError_t e = f.alloc(h->n() * h->esize());
+        if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaMalloc field"); }
+    }
+    // Solid3D::new starts every cell at `initial`.
+    std::vector<double> t(h->n(), d->initial_kelvin);
+    *out = reinterpret_cast<pm_heat*>(h);
+    s = pm_heat_upload(*out, t.data(), t.size());
+    if (s != PM_OK) { delete h; *out = nullptr; return s; }
+    return PM_OK;
+}
+
+pm_status pm_heat_fill(pm_heat* hp, const pm_substance* sub, const uint8_t* mask, size_t n) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!sub || !mask || n != h->n()) return fail(PM_BAD_ARG, "fill: substance, mask and a mask of one byte per cell");
+    // solid.rs:524-530: reuse an equal substance, else append
+    int id = -1;
+    for (size_t q = 0; q < h->mats.size(); ++q) {
+        const pm_substance& o = h->mats[q];
+        if (o.density == sub->density && o.conductivity == sub->conductivity && o.specific_heat == sub->specific_heat &&
+            o.emissivity == sub->emissivity && o.thermal == sub->thermal) { id = (int)q; break; }
+    }
+    if (id < 0) { h->mats.push_back(*sub); id = (int)h->mats.size() - 1; }
+    if (h->which.empty()) h->which.assign(h->n(), 0u);
+    for (size_t c = 0; c < n; ++c)
+        if (mask[c]) h->which[c] = (uint32_t)id;
+    h->resolve();
+    pm_status s = h->upload_coefficients();
+    if (s != PM_OK) return s;
+    return h->measure();
+}
+
+pm_status pm_heat_losing_from(pm_heat* hp, int face, double ambient, double convection, double area) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (face < 0 || face > 5) return fail(PM_BAD_ARG, "face must be 0..5");
+    h->films.exposed |= 1 << face;
+    h->films.ambient[face] = ambient;
+    h->films.convection[face] = convection;
+    h->film_conv[face] = convection;
+    h->films.share[face] = area / (double)std::max<size_t>(h->cells_on(face), 1);  // solid.rs:1203
+    h->resolve();
+    h->drop_graphs();
+    return PM_OK;
+}
+
+pm_status pm_heat_upload(pm_heat* hp, const double* kelvin, size_t n) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!kelvin || n != h->n()) return fail(PM_BAD_ARG, "upload: one value per cell");
+    h->parity = 0;
+    if (h->precision == PM_PLAIN_F64) {
+        PM_CUDA(cudaMemcpyAsync(h->field[0].p, kelvin, n * 8, cudaMemcpyHostToDevice, h->stream()));
+    } else {
+        if (!h->stage.p || h->stage.bytes < n * 8) PM_CUDA(h->stage.alloc(n * 8));
+        PM_CUDA(cudaMemcpyAsync(h->stage.p, kelvin, n * 8, cudaMemcpyHostToDevice, h->stream()));
+        PM_CUDA(launch_heat_convert(h->stage.as<double>(), h->field[0].as<float>(), h->reference, n, 1, nullptr, h->stream()));
+    }
+    return h->measure();
+}
+
+pm_status pm_heat_download(pm_heat* hp, double* kelvin, size_t n) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!kelvin || n != h->n()) return fail(PM_BAD_ARG, "download: one value per cell");
+    if (h->precision == PM_PLAIN_F64) {
+        PM_CUDA(cudaMemcpyAsync(kelvin, h->field[h->parity].p, n * 8, cudaMemcpyDeviceToHost, h->stream()));
+    } else {
+        if (!h->stage.p || h->stage.bytes < n * 8) PM_CUDA(h->stage.alloc(n * 8));
+        PM_CUDA(launch_heat_convert(nullptr, h->field[h->parity].as<float>(), h->reference, n, 0, h->stage.as<double>(), h->stream()));
+        PM_CUDA(cudaMemcpyAsync(kelvin, h->stage.p, n * 8, cudaMemcpyDeviceToHost, h->stream()));
+    }
+    PM_CUDA(cudaStreamSynchronize(h->stream()));
+    return PM_OK;
+}
+
+pm_status pm_heat_max_stable_dt(pm_heat* hp, double* seconds) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!seconds) return fail(PM_BAD_ARG, "null output");
+    if (h->films.exposed && h->any_radiative_film())
+        return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) make the step limit state-dependent; not on the GPU path");
+    double rate = h->worst_rate_now();
+    *seconds = std::isnan(rate) ? std::numeric_limits<double>::infinity() : 1.0 / rate;  // solid.rs:1709-1715
+    return PM_OK;
+}
+
+pm_status pm_heat_set_tolerance(pm_heat* hp, double tol) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    h->tolerance = tol;
+    return PM_OK;
+}
+
+pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* out) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
+    if (nsteps == 0) return PM_OK;
+    if (h->films.exposed && h->any_radiative_film())
+        return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) make the step limit state-dependent; not on the GPU path");
+    // solid.rs:1718-1738: the stability refusal, before anything moves.
+    const double ratio = dt * h->worst_rate_now();
+    if (std::isnan(ratio)) {
+        const double inf = std::numeric_limits<double>::infinity();
+        fill_violation(out, "substance has no diffusivity", h->name, inf, inf, inf, 0.0, 1);
+        set_error("substance has no diffusivity");
+        return PM_VIOLATION;
+    }
+    if (ratio > 1.0 + 6e-12) {
+        fill_violation(out, "Fourier number", h->name + " (explicit 3D conduction)", kStableFourier3D,
+                       ratio * kStableFourier3D, kStableFourier3D, 1e-12, 1);
+        set_error("Fourier number past the explicit limit");
+        return PM_VIOLATION;
+    }
+    pm_status s = h->begin_call();
+    if (s != PM_OK) return s;
+    const long long before = h->host_state->steps;
+    if (h->precision == PM_PLAIN_F64) {
+        s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {
+            return launch_heat_plain(h->plain_args(par, dt), st);
+        });
+    } else {
+        const int zc = Heat::zchunk_for(h->nz);
+        s = h->run_steps(nsteps, dt, true, [h, dt, zc](int par, cudaStream_t st) {
+            return launch_heat_f32(h->f32_args(par, dt), zc, st);
+        });
+    }
+    if (s != PM_OK) return s;
+    return h->finish_call(before, out, h->name + " (its own books, against what it moved on the bus)", h->name, true);
+}
+
+pm_status pm_heat_ledger(pm_heat* hp, pm_ledger* out) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!out) return fail(PM_BAD_ARG, "null output");
+    pm_status s = h->read_state();
+    if (s != PM_OK) return s;
+    std::memset(out, 0, sizeof(*out));
+    out->total = h->host_state->total;
+    out->scale = h->host_state->scale;
+    out->n_parts = 3;
+    for (int q = 0; q < 3; ++q) out->parts[q] = h->host_state->part[q];
+    out->steps = h->host_state->steps;
+    return PM_OK;
+}
+
+pm_status pm_heat_absorb(pm_heat* hp, double joules) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (joules == 0.0) return PM_OK;
+    const double rise = joules / h->cap_sum;  // solid.rs:1755
+    PM_CUDA(launch_heat_rise(h->precision == PM_PLAIN_F64 ? h->field[h->parity].as<double>() : nullptr,
+                             h->precision == PM_PLAIN_F64 ? nullptr : h->field[h->parity].as<float>(), rise, h->n(),
+                             h->stream()));
+    // absorbed heat is bus traffic, not a change of the domain's own books: re-measure stored
+    pm_status s = h->read_state();
+    if (s != PM_OK) return s;
+    double lost = h->host_state->lost, supplied = h->host_state->supplied;
+    s = h->measure();
+    if (s != PM_OK) return s;
+    h->host_state->lost = lost;
+    h->host_state->supplied = supplied;
+    return h->write_state();
+}
+
+pm_status pm_heat_checkpoint(pm_heat* hp) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    const size_t bytes = h->n() * h->esize();
+    if (!h->saved.p) PM_CUDA(h->saved.alloc(bytes));
+    PM_CUDA(cudaMemcpyAsync(h->saved.p, h->field[h->parity].p, bytes, cudaMemcpyDeviceToDevice, h->stream()));
+    pm_status s = h->read_state();
+    if (s != PM_OK) return s;
+    h->saved_lost = h->host_state->lost;
+    h->saved_supplied = h->host_state->supplied;
+    h->has_saved = true;
+    return PM_OK;
+}
+
+pm_status pm_heat_restore(pm_heat* hp) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!h->has_saved) return PM_OK;
+    const size_t bytes = h->n() * h->esize();
+    PM_CUDA(cudaMemcpyAsync(h->field[h->parity].p, h->saved.p, bytes, cudaMemcpyDeviceToDevice, h->stream()));
+    pm_status s = h->read_state();
+    if (s != PM_OK) return s;
+    h->host_state->lost = h->saved_lost;
+    h->host_state->supplied = h->saved_supplied;
+    s = h->write_state();
+    if (s != PM_OK) return s;
+    return h->measure();
+}
+
+pm_status pm_heat_set_stream(pm_heat* hp, void* stream) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    PM_CUDA(cudaStreamSynchronize(h->stream()));
+    h->user = static_cast<cudaStream_t>(stream);
+    return PM_OK;
+}
+
+void pm_heat_destroy(pm_heat* hp) { delete reinterpret_cast<Heat*>(hp); }
+
+}  // extern "C"

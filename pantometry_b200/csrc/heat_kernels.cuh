@@ -1,0 +1,295 @@
+// Solid3D stepping kernels (crates/pantometry-thermal/src/solid.rs:1717-1901).
+//
+// heat_plain_step — IEEE f64, the reference's operand order, compiled with --fmad=false so no
+//   multiply-add is contracted: bit-exact with `Solid3D::step` cell by cell. One thread per
+//   cell, reading the old field and writing the new one (the reference's `old = cells.clone()`
+//   becomes a ping-pong pair). Films (`losing_from`) are evaluated in the same update, from the
+//   old state, exactly as `film_flux` does. Fused: this step's stored heat and shed heat, summed
+//   in FP64 by the fixed-order tree, then the ledger and the audit in the last block.
+//
+// heat_f32_step — the chosen form. The field is stored as the deviation T − T0 in f32, which
+//   keeps the subtraction `T_nb − T` on numbers of order the deviation rather than of 300 K
+//   (the reference's own finding, runtime/gpu/src/lib.rs:37-51). Uniform material; films with
+//   a temperature-independent conductance. Stored heat, shed heat and the ledger stay FP64.
+#pragma once
+
+#include "common.cuh"
+
+namespace pm {
+
+constexpr double kStefanBoltzmann = 5.670374419e-8;  // pantometry-units/src/lib.rs:899
+
+// Rust `powi` with a constant exponent: binary-decomposition multiplies.
+__device__ __forceinline__ double powi4(double x) {
+    double s = x * x;
+    return s * s;
+}
+
+// solid.rs:110-122
+__device__ __forceinline__ double series_with_half_cell(double film, double conductivity, double area,
+                                                        double dx) {
+    if (film <= 0.0) return 0.0;
+    double half = 2.0 * conductivity * area / dx;
+    if (!isfinite(half)) return film;
+    if (half <= 0.0) return 0.0;
+    return 1.0 / (1.0 / film + 1.0 / half);
+}
+
+__device__ __forceinline__ bool face_holds(int f, int i, int j, int k, int nx, int ny, int nz) {
+    switch (f) {
+        case 0: return i == 0;
+        case 1: return i + 1 == nx;
+        case 2: return j == 0;
+        case 3: return j + 1 == ny;
+        case 4: return k == 0;
+        default: return k + 1 == nz;
+    }
+}
+
+struct HeatFilms {
+    int exposed;  // bit f set: face f (XMin, XMax, YMin, YMax, ZMin, ZMax) loses heat
+    double ambient[6];
+    double convection[6];
+    double share[6];  // area / cells_on(face), computed on the host as the reference does
+};
+
+struct HeatPlainArgs {
+    const double* __restrict__ told;
+    double* __restrict__ tnew;
+    // General (filled) blocks: per-face conductivities and per-cell coefficients, as
+    // `resolve` builds them (solid.rs:588-784). Null in uniform mode.
+    const double* __restrict__ kx;
+    const double* __restrict__ ky;
+    const double* __restrict__ kz;
+    const double* __restrict__ mob;
+    const double* __restrict__ cap;
+    const uint32_t* __restrict__ which;  // per-cell material, for the film (general mode)
+    const double* __restrict__ mat_k;    // per-material conductivity (+inf: `thermal: None`)
+    const double* __restrict__ mat_eps;  // per-material emissivity
+    // Uniform blocks: the single values every interior face and cell holds.
+    double kface, mobility, capacity, k_cell, eps_cell;
+    int uniform;
+    int nx, ny, nz;
+    double dts, dx, reference;
+    HeatFilms films;
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+// solid.rs:1192-1219 `film_flux`, read off the old state.
+__device__ __forceinline__ double film_flux(const HeatPlainArgs& a, int i, int j, int k, size_t c,
+                                            double here) {
+    double emissivity, conductivity;
+    if (a.uniform) {
+        emissivity = a.eps_cell;
+        conductivity = a.k_cell;
+    } else {
+        uint32_t m = a.which[c];
+        emissivity = a.mat_eps[m];
+        conductivity = a.mat_k[m];
+    }
+    double out = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (!((a.films.exposed >> f) & 1)) continue;
+        if (!face_holds(f, i, j, k, a.nx, a.ny, a.nz)) continue;
+        double share = a.films.share[f];
+        double ambient = a.films.ambient[f];
+        double gap = here - ambient;
+        if (gap == 0.0) continue;
+        // crates/pantometry-thermal/src/lib.rs:104-110 `Environment::loss_from`, area = share
+        double convective = a.films.convection[f] * share * (here - ambient);
+        double radiative = emissivity * kStefanBoltzmann * share * (powi4(here) - powi4(ambient));
+        double bare = convective + radiative;
+        double g = series_with_half_cell(bare / gap, conductivity, share, a.dx);
+        out += g * gap / a.dx;
+    }
+    return out;
+}
+
+static __global__ void __launch_bounds__(256) heat_plain_step(HeatPlainArgs a) {
+    if (a.st->violated) return;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int k = blockIdx.z;
+    double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
+    if (i < a.nx && j < a.ny) {
+        const int nx = a.nx, ny = a.ny, nz = a.nz;
+        const size_t plane = (size_t)nx * ny;
+        const size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
+        const double t = a.told[c];
+        double flux = 0.0;
+        if (a.uniform) {
+            const double kf = a.kface;
+            if (i > 0) flux += kf * (a.told[c - 1] - t);
+            if (i + 1 < nx) flux += kf * (a.told[c + 1] - t);
+            if (j > 0) flux += kf * (a.told[c - nx] - t);
+            if (j + 1 < ny) flux += kf * (a.told[c + nx] - t);
+            if (k > 0) flux += kf * (a.told[c - plane] - t);
+            if (k + 1 < nz) flux += kf * (a.told[c + plane] - t);
+        } else {
+            const size_t xr = (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
+            const size_t yr = (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
+            if (i > 0) flux += a.kx[i + xr] * (a.told[c - 1] - t);
+            if (i + 1 < nx) flux += a.kx[i + 1 + xr] * (a.told[c + 1] - t);
+            if (j > 0) flux += a.ky[i + yr] * (a.told[c - nx] - t);
+            if (j + 1 < ny) flux += a.ky[i + nx + yr] * (a.told[c + nx] - t);
+            if (k > 0) flux += a.kz[c] * (a.told[c - plane] - t);
+            if (k + 1 < nz) flux += a.kz[c + plane] * (a.told[c + plane] - t);
+        }
+        const double shed = a.films.exposed ? film_flux(a, i, j, k, c, t) : 0.0;
+        const double mob = a.uniform ? a.mobility : a.mob[c];
+        const double capc = a.uniform ? a.capacity : a.cap[c];
+        const double nt = t + a.dts * mob * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
+        a.tnew[c] = nt;
+        acc[0] = capc * (nt - a.reference);                  // solid.rs:1583-1590
+        if (shed != 0.0) acc[1] = a.dts * mob * shed * capc;  // solid.rs:1821-1823
+    }
+    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+        DevState* st = a.st;
+        st->lost += acc[1];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, acc[0]);
+        ledger_add(total, scale, st->lost);
+        ledger_add(total, scale, -st->supplied);
+        st->part[0] = acc[0];
+        st->part[1] = st->lost;
+        st->part[2] = -st->supplied;
+        audit_and_commit(st, total, scale);
+    }
+}
+
+struct HeatF32Args {
+    const float* __restrict__ dold;
+    float* __restrict__ dnew;
+    int nx, ny, nz;
+    float a;         // dt · mobility · k_face
+    int exposed;     // film faces
+    float b[6];      // dt · mobility · g_f / dx per film face
+    float off[6];    // T0 − ambient per film face
+    double capacity; // per cell
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+// Chosen form, z-marching: each thread owns one (i, j) column of a z-chunk and keeps the cell
+// below, the cell and the cell above in registers, so a plane is read from memory once and the
+// in-plane neighbours come from L1/L2.
+static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a, int zchunk) {
+    if (a.st->violated) return;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int k0 = blockIdx.z * zchunk;
+    const int k1 = min(a.nz, k0 + zchunk);
+    double acc[2] = {0.0, 0.0};
+    if (i < a.nx && j < a.ny && k0 < k1) {
+        const int nx = a.nx, ny = a.ny, nz = a.nz;
+        const size_t plane = (size_t)nx * ny;
+        size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+        float below = k0 > 0 ? __ldg(a.dold + c - plane) : 0.0f;
+        float here = __ldg(a.dold + c);
+        const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
+        const bool edge_xy = !(xl && xh && yl && yh);
+        for (int k = k0; k < k1; ++k, c += plane) {
+            const float above = (k + 1 < nz) ? __ldg(a.dold + c + plane) : 0.0f;
+            float s = 0.0f;
+            if (xl) s += __ldg(a.dold + c - 1) - here;
+            if (xh) s += __ldg(a.dold + c + 1) - here;
+            if (yl) s += __ldg(a.dold + c - nx) - here;
+            if (yh) s += __ldg(a.dold + c + nx) - here;
+            if (k > 0) s += below - here;
+            if (k + 1 < nz) s += above - here;
+            float shed = 0.0f;
+            if (a.exposed && (edge_xy || k == 0 || k + 1 == nz)) {
+                if (((a.exposed >> 0) & 1) && !xl) shed += a.b[0] * (here + a.off[0]);
+                if (((a.exposed >> 1) & 1) && !xh) shed += a.b[1] * (here + a.off[1]);
+                if (((a.exposed >> 2) & 1) && !yl) shed += a.b[2] * (here + a.off[2]);
+                if (((a.exposed >> 3) & 1) && !yh) shed += a.b[3] * (here + a.off[3]);
+                if (((a.exposed >> 4) & 1) && k == 0) shed += a.b[4] * (here + a.off[4]);
+                if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += a.b[5] * (here + a.off[5]);
+            }
+            const float nd = here + (a.a * s - shed);
+            a.dnew[c] = nd;
+            acc[0] += (double)nd;
+            acc[1] += (double)shed;
+            below = here;
+            here = above;
+        }
+    }
+    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+        DevState* st = a.st;
+        const double stored = a.capacity * acc[0];
+        st->lost += a.capacity * acc[1];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, stored);
+        ledger_add(total, scale, st->lost);
+        ledger_add(total, scale, -st->supplied);
+        st->part[0] = stored;
+        st->part[1] = st->lost;
+        st->part[2] = -st->supplied;
+        audit_and_commit(st, total, scale);
+    }
+}
+
+// The opening ledger of a freshly uploaded block: stored heat only (lost and supplied are zero
+// until something steps). Plain: Σ C·(T − T_ref); f32: C·Σ dev.
+struct HeatMeasureArgs {
+    const double* t64;
+    const float* d32;
+    const double* cap;  // null: uniform `capacity`
+    double capacity, reference;
+    size_t n;
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+static __global__ void __launch_bounds__(256) heat_measure(HeatMeasureArgs a) {
+    double acc[1] = {0.0};
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += (size_t)gridDim.x * blockDim.x) {
+        if (a.t64) {
+            const double capc = a.cap ? a.cap[c] : a.capacity;
+            acc[0] += capc * (a.t64[c] - a.reference);
+        } else {
+            acc[0] += (double)a.d32[c];
+        }
+    }
+    if (finish_blocks<1>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+        DevState* st = a.st;
+        const double stored = a.t64 ? acc[0] : a.capacity * acc[0];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, stored);
+        ledger_add(total, scale, st->lost);
+        ledger_add(total, scale, -st->supplied);
+        st->part[0] = stored;
+        st->part[1] = st->lost;
+        st->part[2] = -st->supplied;
+        st->total = total;
+        st->scale = scale;
+        st->prev_total = total;
+        st->prev_scale = scale;
+    }
+}
+
+// Conversions between the caller's kelvin (f64) and the f32 deviation store.
+static __global__ void heat_to_deviation(const double* __restrict__ t, float* __restrict__ d, double t0, size_t n) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        d[c] = (float)(t[c] - t0);
+}
+static __global__ void heat_from_deviation(const float* __restrict__ d, double* __restrict__ t, double t0, size_t n) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        t[c] = t0 + (double)d[c];
+}
+// solid.rs:1752-1765 + 1620-1635: a uniform rise over every cell.
+static __global__ void heat_add_rise64(double* __restrict__ t, double rise, size_t n) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        t[c] += rise;
+}
+static __global__ void heat_add_rise32(float* __restrict__ d, float rise, size_t n) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+        d[c] += rise;
+}
+
+}  // namespace pm

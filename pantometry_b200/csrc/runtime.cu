@@ -1,0 +1,164 @@
+// Host runtime: the Handle base (stream, graphs, device state, audit readout) and the C ABI's
+// status and error functions. The three domains live in heat.cu, hall.cu and cavity.cu.
+#include <new>
+
+#include "runtime.h"
+
+namespace pm {
+
+static thread_local std::string g_error;
+
+void set_error(const std::string& msg) { g_error = msg; }
+
+pm_status fail(pm_status s, const std::string& msg) {
+    set_error(msg);
+    return s;
+}
+
+pm_status cuda_fail(cudaError_t e, const char* what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    set_error(msg);
+    if (e == cudaErrorMemoryAllocation) return PM_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+        return PM_NO_DEVICE;
+    return PM_CUDA_ERROR;
+}
+
+void fill_violation(pm_violation* v, const char* quantity, const std::string& site, double before, double after,
+                    double scale, double tol, long long step) {
+    if (!v) return;
+    std::memset(v, 0, sizeof(*v));
+    std::snprintf(v->quantity, sizeof(v->quantity), "%s", quantity);
+    std::snprintf(v->site, sizeof(v->site), "%s", site.c_str());
+    v->before = before;
+    v->after = after;
+    v->scale = scale;
+    v->tolerance = tol;
+    v->step = step;
+}
+
+pm_status Handle::init(int dev, size_t partial_doubles) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(PM_NO_DEVICE, std::string("no CUDA device: ") + (e == cudaSuccess ? "count is 0" : cudaGetErrorString(e)));
+    if (dev < 0 || dev >= count) return fail(PM_BAD_ARG, "device index out of range");
+    device = dev;
+    PM_CUDA(cudaSetDevice(dev));
+    cudaDeviceProp prop;
+    PM_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10)
+        return fail(PM_NO_DEVICE, "the kernels are built for sm_100a (B200); this device is sm_" +
+                                      std::to_string(prop.major) + std::to_string(prop.minor));
+    PM_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    PM_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
+    PM_CUDA(state.alloc(sizeof(DevState)));
+    PM_CUDA(partials.alloc(partial_doubles * sizeof(double)));
+    PM_CUDA(cudaMallocHost((void**)&host_state, sizeof(DevState)));
+    std::memset(host_state, 0, sizeof(DevState));
+    host_state->tol = tolerance;
+    PM_CUDA(cudaMemcpy(state.p, host_state, sizeof(DevState), cudaMemcpyHostToDevice));
+    return PM_OK;
+}
+
+void Handle::drop_graphs() {
+    for (auto& g : graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    graph_dt = NAN;
+    graph_steps = 0;
+}
+
+Handle::~Handle() {
+    if (own || capture) cudaSetDevice(device);
+    drop_graphs();
+    if (own) {
+        cudaStreamSynchronize(own);
+        cudaStreamDestroy(own);
+    }
+    if (user) cudaStreamSynchronize(user);
+    if (capture) cudaStreamDestroy(capture);
+    if (host_state) cudaFreeHost(host_state);
+}
+
+pm_status Handle::read_state() {
+    PM_CUDA(cudaMemcpyAsync(host_state, state.p, sizeof(DevState), cudaMemcpyDeviceToHost, stream()));
+    PM_CUDA(cudaStreamSynchronize(stream()));
+    return PM_OK;
+}
+
+pm_status Handle::write_state() {
+    PM_CUDA(cudaMemcpyAsync(state.p, host_state, sizeof(DevState), cudaMemcpyHostToDevice, stream()));
+    PM_CUDA(cudaStreamSynchronize(stream()));
+    return PM_OK;
+}
+
+pm_status Handle::begin_call() {
+    // Clear the previous call's violation and set the tolerance; the ledger and books stay.
+    PM_CUDA(cudaSetDevice(device));
+    pm_status s = read_state();
+    if (s != PM_OK) return s;
+    host_state->violated = kRunning;
+    host_state->violation_step = 0;
+    host_state->tol = tolerance;
+    host_state->counter = 0u;
+    call_parity = parity;
+    return write_state();
+}
+
+pm_status Handle::finish_call(long long steps_before, pm_violation* out, const std::string& audit_site,
+                              const std::string& startup_site, bool pingpong) {
+    pm_status s = read_state();
+    if (s != PM_OK) return s;
+    PM_CUDA(cudaGetLastError());
+    const long long executed = host_state->steps - steps_before;
+    if (pingpong) parity = call_parity ^ (int)(executed & 1);
+    if (host_state->violated == kRunning) return PM_OK;
+    const long long at = host_state->violation_step - steps_before;
+    if (host_state->violated == kStartupFailed)
+        fill_violation(out, "energy", startup_site, host_state->v_before, host_state->v_after, host_state->v_scale,
+                       host_state->v_tol, at);
+    else
+        fill_violation(out, "energy", audit_site, host_state->v_before, host_state->v_after, host_state->v_scale,
+                       host_state->v_tol, at);
+    set_error("conservation audit failed at " + audit_site);
+    return PM_VIOLATION;
+}
+
+}  // namespace pm
+
+using namespace pm;
+
+extern "C" {
+
+const char* pm_status_string(pm_status s) {
+    switch (s) {
+        case PM_OK: return "ok";
+        case PM_NO_DEVICE: return "no device";
+        case PM_UNSUPPORTED: return "unsupported";
+        case PM_VIOLATION: return "violation";
+        case PM_DEVICE_TIMEOUT: return "device timeout";
+        case PM_BAD_ARG: return "bad argument";
+        case PM_CUDA_ERROR: return "cuda error";
+        case PM_OUT_OF_MEMORY: return "out of memory";
+    }
+    return "unknown";
+}
+
+const char* pm_last_error(void) { return g_error.c_str(); }
+
+pm_status pm_device_count(int* count) {
+    if (!count) return fail(PM_BAD_ARG, "count is null");
+    *count = 0;
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(PM_NO_DEVICE, cudaGetErrorString(e));
+    }
+    return PM_OK;
+}
+
+const char* pm_version(void) { return "pantometry_b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

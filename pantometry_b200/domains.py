@@ -1,0 +1,292 @@
+"""Python face of the C ABI, shaped like pantometry's `Domain` implementations.
+
+`Solid3D`, `Hall` and `Cavity` here hold a device handle each and answer what the Rust types
+answer (crates/pantometry-core/src/sim.rs:77-252): `step` returns `None` or a violation dict
+(the `Result<(), Violation>`), `ledger`, `max_stable_dt`, `checkpoint` and `restore`, plus the
+constructors and setters the reference offers. Arrays are numpy f64 in the reference's index
+order (x fastest). Everything runs on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+FACES = ("XMin", "XMax", "YMin", "YMax", "ZMin", "ZMax")
+WALLS = ("XLow", "XHigh", "YLow", "YHigh", "ZLow", "ZHigh")
+BOUNDARY_KINDS = {"conducting": 0, "magnetic": 1, "open": 2}
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _precision(p):
+    if p in (N.PM_PLAIN_F64, "f64", "plain", "plain_f64"):
+        return N.PM_PLAIN_F64
+    if p in (N.PM_FIELDS_F32, "f32", "fields_f32"):
+        return N.PM_FIELDS_F32
+    raise ValueError(f"unknown precision {p!r}")
+
+
+def _ledger(fn, handle):
+    led = N.Ledger()
+    N.check(fn(handle, C.byref(led)))
+    return {
+        "total": led.total,
+        "scale": led.scale,
+        "parts": [led.parts[q] for q in range(led.n_parts)],
+        "steps": led.steps,
+    }
+
+
+def _step(fn, handle, dt, nsteps):
+    v = N.Violation()
+    st = fn(handle, float(dt), int(nsteps), C.byref(v))
+    if st == N.PM_VIOLATION:
+        return v.as_dict()
+    N.check(st)
+    return None
+
+
+class _Domain:
+    _destroy = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            getattr(N.load(), self._destroy)(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    def set_stream(self, stream):
+        """Run on a CUDA stream given as an integer handle (e.g. `torch.cuda.Stream().cuda_stream`)."""
+        N.check(getattr(self._lib, self._prefix + "set_stream")(self._h, C.c_void_p(stream or 0)))
+
+    def set_tolerance(self, tol):
+        """The per-step audit's relative tolerance; negative turns the audit off."""
+        N.check(getattr(self._lib, self._prefix + "set_tolerance")(self._h, float(tol)))
+
+    def step(self, dt, nsteps=1):
+        return _step(getattr(self._lib, self._prefix + "step"), self._h, dt, nsteps)
+
+    def ledger(self):
+        return _ledger(getattr(self._lib, self._prefix + "ledger"), self._h)
+
+    def checkpoint(self):
+        N.check(getattr(self._lib, self._prefix + "checkpoint")(self._h))
+
+    def restore(self):
+        N.check(getattr(self._lib, self._prefix + "restore")(self._h))
+
+
+class Solid3D(_Domain):
+    """`Solid3D` (crates/pantometry-thermal/src/solid.rs) on the GPU."""
+
+    _destroy = "pm_heat_destroy"
+    _prefix = "pm_heat_"
+
+    def __init__(self, counts, dx, density, conductivity, specific_heat, initial, emissivity=0.0,
+                 thermal=True, precision="f64", name="block", device=0):
+        self._lib = N.load()
+        d = N.HeatDesc()
+        self._name = name.encode()
+        d.name = self._name
+        d.nx, d.ny, d.nz = (max(1, int(c)) for c in counts)
+        d.dx = dx
+        d.substance = N.Substance(density, conductivity, specific_heat, emissivity, int(thermal))
+        d.initial_kelvin = initial
+        d.precision = _precision(precision)
+        d.device = device
+        h = C.c_void_p()
+        N.check(self._lib.pm_heat_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.counts = (d.nx, d.ny, d.nz)
+        self.n = d.nx * d.ny * d.nz
+        self.precision = d.precision
+
+    def losing_from(self, face, ambient, convection, area):
+        f = FACES.index(face) if isinstance(face, str) else int(face)
+        N.check(self._lib.pm_heat_losing_from(self._h, f, ambient, convection, area))
+        return self
+
+    def fill(self, mask, density, conductivity, specific_heat, emissivity=0.0, thermal=True):
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        s = N.Substance(density, conductivity, specific_heat, emissivity, int(thermal))
+        N.check(self._lib.pm_heat_fill(self._h, C.byref(s), m.ctypes.data_as(C.c_void_p), m.size))
+        return self
+
+    @property
+    def cells(self):
+        out = np.empty(self.n, dtype=np.float64)
+        N.check(self._lib.pm_heat_download(self._h, _ptr(out), out.size))
+        return out
+
+    @cells.setter
+    def cells(self, t):
+        t = _f64(t, self.n)
+        N.check(self._lib.pm_heat_upload(self._h, _ptr(t), t.size))
+
+    def max_stable_dt(self):
+        out = C.c_double()
+        N.check(self._lib.pm_heat_max_stable_dt(self._h, C.byref(out)))
+        return out.value
+
+    def absorb(self, joules):
+        N.check(self._lib.pm_heat_absorb(self._h, float(joules)))
+
+
+class Hall(_Domain):
+    """`Hall` (crates/pantometry-acoustic/src/hall.rs) on the GPU."""
+
+    _destroy = "pm_hall_destroy"
+    _prefix = "pm_hall_"
+
+    def __init__(self, width, height, depth, across, speed, density, precision="f64", name="hall", device=0):
+        self._lib = N.load()
+        d = N.HallDesc()
+        self._name = name.encode()
+        d.name = self._name
+        d.width, d.height, d.depth = width, height, depth
+        d.across = across
+        d.speed, d.density = speed, density
+        d.precision = _precision(precision)
+        d.device = device
+        h = C.c_void_p()
+        N.check(self._lib.pm_hall_create(C.byref(d), C.byref(h)))
+        self._h = h
+        nx, ny, nz, dx = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        N.check(self._lib.pm_hall_nodes(h, C.byref(nx), C.byref(ny), C.byref(nz), C.byref(dx)))
+        self.nodes = (nx.value, ny.value, nz.value)
+        self.dx = dx.value
+        self.precision = d.precision
+
+    @property
+    def n(self):
+        nx, ny, nz = self.nodes
+        return nx * ny * nz
+
+    def release(self, pressure):
+        """`released_from` with the profile already sampled at the nodes."""
+        p = _f64(pressure, self.n)
+        N.check(self._lib.pm_hall_release(self._h, _ptr(p), p.size))
+        return self
+
+    def set_source(self, node, wave):
+        w = _f64(wave)
+        N.check(self._lib.pm_hall_set_source(self._h, int(node), _ptr(w), w.size))
+
+    def set_speed_blocks(self, block, speeds):
+        s = _f64(speeds)
+        N.check(self._lib.pm_hall_set_speed_blocks(self._h, int(block), _ptr(s), s.size))
+
+    def max_stable_dt(self):
+        out = C.c_double()
+        N.check(self._lib.pm_hall_max_stable_dt(self._h, C.byref(out)))
+        return out.value
+
+    def download_pressure(self, out):
+        """The pressure field into a caller-owned f64 array (pinned memory makes this a DMA)."""
+        if out.dtype != np.float64 or out.size != self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous f64 array with one value per node")
+        N.check(self._lib.pm_hall_download(self._h, _ptr(out), None, None, None, None))
+        return out
+
+    def fields(self):
+        nx, ny, nz = self.nodes
+        out = {
+            "p": np.empty(self.n), "p_prev": np.empty(self.n),
+            "vx": np.empty((nx - 1) * ny * nz), "vy": np.empty(nx * (ny - 1) * nz), "vz": np.empty(nx * ny * (nz - 1)),
+        }
+        N.check(self._lib.pm_hall_download(self._h, *[_ptr(out[k]) for k in ("p", "p_prev", "vx", "vy", "vz")]))
+        return out
+
+
+class Cavity(_Domain):
+    """`Cavity` (crates/pantometry-em/src/cavity.rs) on the GPU."""
+
+    _destroy = "pm_cavity_destroy"
+    _prefix = "pm_cavity_"
+
+    def __init__(self, counts, dx, eps_r=1.0, mu_r=1.0, sigma=0.0, precision="f64", name="cavity", device=0):
+        self._lib = N.load()
+        d = N.CavityDesc()
+        self._name = name.encode()
+        d.name = self._name
+        d.nx, d.ny, d.nz = (max(1, int(c)) for c in counts)
+        d.dx = dx
+        d.eps_r, d.mu_r, d.sigma = eps_r, mu_r, sigma
+        d.precision = _precision(precision)
+        d.device = device
+        h = C.c_void_p()
+        N.check(self._lib.pm_cavity_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.counts = (d.nx, d.ny, d.nz)
+        self.dx = dx
+        self.precision = d.precision
+
+    def shapes(self):
+        nx, ny, nz = self.counts
+        return {
+            "ex": nx * (ny + 1) * (nz + 1), "ey": (nx + 1) * ny * (nz + 1), "ez": (nx + 1) * (ny + 1) * nz,
+            "hx": (nx + 1) * ny * nz, "hy": nx * (ny + 1) * nz, "hz": nx * ny * (nz + 1),
+        }
+
+    def fill_cells(self, eps_r=None, mu_r=None, sigma=None):
+        n = self.counts[0] * self.counts[1] * self.counts[2]
+        arrs = [None if a is None else _f64(a, n) for a in (eps_r, mu_r, sigma)]
+        N.check(self._lib.pm_cavity_fill_cells(self._h, *[_ptr(a) for a in arrs], n))
+
+    def obstruct(self, mask):
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        N.check(self._lib.pm_cavity_obstruct(self._h, m.ctypes.data_as(C.c_void_p), m.size))
+
+    def set_boundary(self, wall, kind):
+        w = WALLS.index(wall) if isinstance(wall, str) else int(wall)
+        k = BOUNDARY_KINDS[kind] if isinstance(kind, str) else int(kind)
+        N.check(self._lib.pm_cavity_set_boundary(self._h, w, k))
+
+    def release_mode(self, mode, amplitude, dt):
+        N.check(self._lib.pm_cavity_release_mode(self._h, int(mode[0]), int(mode[1]), float(amplitude), float(dt)))
+
+    def set_fields(self, fields, started):
+        s = self.shapes()
+        arrs = [_f64(fields[k], s[k]) for k in ("ex", "ey", "ez", "hx", "hy", "hz")]
+        N.check(self._lib.pm_cavity_upload(self._h, *[_ptr(a) for a in arrs], int(started)))
+
+    def fields(self):
+        s = self.shapes()
+        out = {k: np.empty(v) for k, v in s.items()}
+        N.check(self._lib.pm_cavity_download(self._h, *[_ptr(out[k]) for k in ("ex", "ey", "ez", "hx", "hy", "hz")]))
+        return out
+
+    def set_source(self, edge, current):
+        w = _f64(current)
+        N.check(self._lib.pm_cavity_set_source(self._h, int(edge), _ptr(w), w.size))
+
+    def courant_limit(self):
+        out = C.c_double()
+        N.check(self._lib.pm_cavity_courant_limit(self._h, C.byref(out)))
+        return out.value
+
+    def energies(self):
+        e, m = C.c_double(), C.c_double()
+        N.check(self._lib.pm_cavity_energies(self._h, C.byref(e), C.byref(m)))
+        return e.value, m.value
+
+
+def device_count():
+    n = C.c_int()
+    st = N.load().pm_device_count(C.byref(n))
+    return n.value if st == N.PM_OK else 0
