@@ -571,6 +571,10 @@ struct Cavity {
     std::vector<double> current;
     long long steps_taken = 0;
     double source_work = 0.0;
+    // The invariant of step n is taken before step n's electric update, so the work that
+    // update does belongs against step n+1's invariant: the ledger books the work through the
+    // previous step.
+    double work_booked = 0.0;
 
     size_t iex(int i, int j, int k) const { return i + (size_t)nx * (j + (size_t)(ny + 1) * k); }
     size_t iey(int i, int j, int k) const { return i + (size_t)(nx + 1) * (j + (size_t)ny * k); }
@@ -918,6 +922,7 @@ struct Cavity {
         invariant = electric_energy() + paired_magnetic_energy(bx, by, bz);
         has_invariant = true;
         double j = (source_edge >= 0 && steps_taken < (long long)current.size()) ? current[steps_taken] : 0.0;
+        work_booked = source_work;
         dissipated += advance_electric(h, j);
         apply_boundaries(h);
         enforce_solid();
@@ -929,7 +934,7 @@ struct Cavity {
         or_entry e{0.0, 0.0};
         ledger_add(e, invariant_energy());
         ledger_add(e, dissipated);
-        if (source_edge >= 0) ledger_add(e, -source_work);
+        if (source_edge >= 0) ledger_add(e, -work_booked);
         return e;
     }
 

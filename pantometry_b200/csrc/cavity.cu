@@ -148,9 +148,11 @@ struct Cavity : Handle {
         a.eps_u = eps_u; a.mu_u = mu_u;
         a.eps0 = deps[0].as<double>(); a.eps1 = deps[1].as<double>(); a.eps2 = deps[2].as<double>();
         a.volume = volume();
+        const unsigned w = wave_of(sizeof(Real) == 8 ? kYeeHF64 : kYeeHF32);
+        a.tiles = make_tiles(nx + 1, ny + 1, nz + 1, choose_zc(nx + 1, ny + 1, nz + 1, w));
+        a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
-        a.nblocks = plane_blocks(nx + 1, ny + 1, nz + 1);
         return a;
     }
 
@@ -180,9 +182,11 @@ struct Cavity : Handle {
             a.eps_src = uniform ? eps_u : eps[2][(size_t)src];
             a.sig_src = uniform ? sig_u : sig[2][(size_t)src];
         }
+        const unsigned w = wave_of(sizeof(Real) == 8 ? kYeeEF64 : kYeeEF32);
+        a.tiles = make_tiles(nx + 1, ny + 1, nz + 1, choose_zc(nx + 1, ny + 1, nz + 1, w));
+        a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
-        a.nblocks = plane_blocks(nx + 1, ny + 1, nz + 1);
         return a;
     }
 
@@ -251,12 +255,12 @@ struct Cavity : Handle {
         auto add = [&](double x) { total += x; scale = std::fmax(scale, std::fabs(x)); };  // Ledger::add
         add(inv);
         add(st->dissipated);
-        if (src >= 0) add(-st->work);
+        if (src >= 0) add(-st->work_booked);
         st->total = total;
         st->scale = scale;
         st->part[0] = inv;
         st->part[1] = st->dissipated;
-        st->part[2] = -st->work;
+        st->part[2] = -st->work_booked;
         st->prev_total = total;
         st->prev_scale = scale;
         return write_state();
@@ -302,7 +306,7 @@ pm_status pm_cavity_create(const pm_cavity_desc* d, pm_cavity** out) {
     c->dx = d->dx;
     c->eps_r = d->eps_r; c->mu_r = d->mu_r; c->sigma = d->sigma;
     c->uniform_media();
-    pm_status s = c->init(d->device, (size_t)plane_blocks(c->nx + 1, c->ny + 1, c->nz + 1) * 6);
+    pm_status s = c->init(d->device, 0);
     if (s != PM_OK) { delete c; return s; }
     for (int q = 0; q < 6; ++q) {
         cudaError_t e = c->f[q].alloc(c->count(q) * c->esize());

@@ -15,6 +15,38 @@
 
 namespace pm {
 
+// The tiling every step kernel walks: 32 × 8 columns of cells (one warp row per y), each
+// marched through `zc` planes by its thread. A persistent grid of blocks takes tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... in that fixed order, so every thread's share of a
+// reduction is summed in the same order on every run.
+struct Tiles {
+    int nx, ny, nz, zc;
+    int ntx, nty, ntz;
+    long long ntiles;
+};
+
+__host__ __device__ inline Tiles make_tiles(int nx, int ny, int nz, int zc) {
+    Tiles t;
+    t.nx = nx; t.ny = ny; t.nz = nz; t.zc = zc;
+    t.ntx = (nx + 31) / 32;
+    t.nty = (ny + 7) / 8;
+    t.ntz = (nz + zc - 1) / zc;
+    t.ntiles = (long long)t.ntx * t.nty * t.ntz;
+    return t;
+}
+
+// Asynchronous global → shared copies (cp.async, sm_80 and later): each thread queues element
+// copies for planes ahead of the one it computes, so the bytes in flight are set by the ring of
+// shared-memory stages rather than by registers or thread count.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Why the run stopped, in DevState::violated.
 enum : int { kRunning = 0, kAuditFailed = 1, kStartupFailed = 2 };
 
@@ -37,6 +69,7 @@ struct DevState {
     double datum, offset, injected, last_delta;
     // Cavity books (cavity.rs:161-162) and the source extension
     double invariant, dissipated, work;
+    double work_booked;  // cavity source work already in the ledger: through the previous step
     unsigned int counter;  // arrival ticket for the last-block reduction; always 0 between kernels
     unsigned int pad;
 };

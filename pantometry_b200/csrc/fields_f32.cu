@@ -3,9 +3,8 @@
 
 namespace pm {
 
-cudaError_t launch_heat_f32(const HeatF32Args& a, int zchunk, cudaStream_t s) {
-    dim3 g((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + zchunk - 1) / zchunk);
-    heat_f32_step<<<g, plane_block(), 0, s>>>(a, zchunk);
+cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s) {
+    heat_f32_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -16,27 +15,36 @@ cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s) {
 
 template <>
 cudaError_t launch_hall<float>(const HallArgs<float>& a, cudaStream_t s) {
-    hall_step<float><<<plane_grid(a.nx, a.ny, a.nz), plane_block(), 0, s>>>(a);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
+        cudaFuncSetAttribute(hall_step<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
+        attr = true;
+    }
+    if (a.block_scale)
+        hall_step<float, true><<<a.nblocks, tile_block(), hall_smem_bytes<float>(), s>>>(a);
+    else
+        hall_step<float, false><<<a.nblocks, tile_block(), hall_smem_bytes<float>(), s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_hall_measure<float>(const HallMeasureArgs<float>& a, cudaStream_t s) {
-    hall_measure<float><<<plane_grid(a.nx, a.ny, a.nz), plane_block(), 0, s>>>(a);
+    hall_measure<float><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_yee_h<float>(const YeeHArgs<float>& a, cudaStream_t s) {
-    yee_h<float><<<plane_grid(a.nx + 1, a.ny + 1, a.nz + 1), plane_block(), 0, s>>>(a);
+    yee_h<float><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_yee_e<float>(const YeeEArgs<float>& a, cudaStream_t s) {
-    yee_e<float><<<plane_grid(a.nx + 1, a.ny + 1, a.nz + 1), plane_block(), 0, s>>>(a);
+    yee_e<float><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_yee_measure<float>(const YeeHArgs<float>& a, double* out2, cudaStream_t s) {
-    yee_measure<float><<<plane_grid(a.nx + 1, a.ny + 1, a.nz + 1), plane_block(), 0, s>>>(a, out2);
+    yee_measure<float><<<a.nblocks, tile_block(), 0, s>>>(a, out2);
     return cudaGetLastError();
 }
 
@@ -55,6 +63,23 @@ cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t 
 cudaError_t launch_to_f64(const float* src, double* dst, size_t n, cudaStream_t s) {
     to_f64_kernel<<<kMeasureBlocks, 256, 0, s>>>(src, dst, n);
     return cudaGetLastError();
+}
+
+
+int occupancy_f32(KernelId id) {
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+    switch (id) {
+        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step, 256, 0); break;
+        case kHallF32:
+            cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<float, false>, 256, hall_smem_bytes<float>());
+            break;
+        case kYeeHF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<float>, 256, 0); break;
+        case kYeeEF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<float>, 256, 0); break;
+        default: return -1;
+    }
+    return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 }  // namespace pm

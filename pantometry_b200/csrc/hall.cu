@@ -53,13 +53,21 @@ struct Hall : Handle {
         a.knode = volume() / (2.0 * rc2());
         a.kface = 0.5 * density * volume();
         a.src = src;
+        a.src_i = a.src_j = a.src_k = -1;
+        if (src >= 0) {
+            a.src_i = (int)(src % nx);
+            a.src_j = (int)((src / nx) % ny);
+            a.src_k = (int)(src / ((long long)nx * ny));
+        }
         a.wave = wave.as<double>();
         a.nwave = nwave;
         a.wsrc = wsrc;
         a.starting = starting ? 1 : 0;
+        const unsigned w = wave_of(sizeof(Real) == 8 ? kHallF64 : kHallF32);
+        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
+        a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
-        a.nblocks = plane_blocks(nx, ny, nz);
         return a;
     }
 
@@ -100,7 +108,8 @@ struct Hall : Handle {
             m.nx = nx; m.ny = ny; m.nz = nz;
             m.knode = volume() / (2.0 * rc2()); m.kface = 0.5 * density * volume();
             if (block > 0) { m.block_knode = bknode.as<double>(); m.block = block; m.nbx = nbx; m.nby = nby; }
-            m.st = state.as<DevState>(); m.partials = partials.as<double>(); m.nblocks = plane_blocks(nx, ny, nz);
+            m.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, resident)); m.nblocks = grid_for(m.tiles, resident);
+            m.st = state.as<DevState>(); m.partials = partials.as<double>();
             PM_CUDA(launch_hall_measure<double>(m, stream()));
         } else {
             HallMeasureArgs<float> m{};
@@ -109,7 +118,8 @@ struct Hall : Handle {
             m.nx = nx; m.ny = ny; m.nz = nz;
             m.knode = volume() / (2.0 * rc2()); m.kface = 0.5 * density * volume();
             if (block > 0) { m.block_knode = bknode.as<double>(); m.block = block; m.nbx = nbx; m.nby = nby; }
-            m.st = state.as<DevState>(); m.partials = partials.as<double>(); m.nblocks = plane_blocks(nx, ny, nz);
+            m.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, resident)); m.nblocks = grid_for(m.tiles, resident);
+            m.st = state.as<DevState>(); m.partials = partials.as<double>();
             PM_CUDA(launch_hall_measure<float>(m, stream()));
         }
         return read_state();
@@ -169,7 +179,7 @@ pm_status pm_hall_create(const pm_hall_desc* d, pm_hall** out) {
     h->speed = d->speed;
     h->density = d->density;
     h->max_speed = d->speed;
-    pm_status s = h->init(d->device, (size_t)plane_blocks(h->nx, h->ny, h->nz) * 3);
+    pm_status s = h->init(d->device, 0);
     if (s != PM_OK) { delete h; return s; }
     for (int q = 0; q < 2; ++q) {
         cudaError_t e;

@@ -243,13 +243,13 @@ struct Heat : Handle {
         a.nx = nx; a.ny = ny; a.nz = nz;
         a.dts = dt; a.dx = dx; a.reference = reference;
         a.films = films;
+        const unsigned w = wave_of(kHeatPlain);
+        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
+        a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
-        a.nblocks = plane_blocks(nx, ny, nz);
         return a;
     }
-
-    static int zchunk_for(int nz) { return nz >= 64 ? 16 : (nz >= 16 ? 8 : 4); }
 
     HeatF32Args f32_args(int par, double dt) const {
         HeatF32Args a{};
@@ -270,10 +270,11 @@ struct Heat : Handle {
             a.off[f] = (float)(reference - films.ambient[f]);
         }
         a.capacity = capacity;
+        const unsigned w = wave_of(kHeatF32);
+        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
+        a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
-        const int zc = zchunk_for(nz);
-        a.nblocks = ((nx + 31) / 32) * ((ny + 7) / 8) * ((nz + zc - 1) / zc);
         return a;
     }
 
@@ -319,11 +320,7 @@ pm_status pm_heat_create(const pm_heat_desc* d, pm_heat** out) {
     h->precision = d->precision;
     h->mats.push_back(d->substance);
     h->resolve();
-    const int zc = Heat::zchunk_for(h->nz);
-    size_t nblocks = std::max<size_t>(std::max<size_t>(plane_blocks(h->nx, h->ny, h->nz),
-                                                       (size_t)((h->nx + 31) / 32) * ((h->ny + 7) / 8) * ((h->nz + zc - 1) / zc)),
-                                      kMeasureBlocks);
-    pm_status s = h->init(d->device, nblocks * 2);
+    pm_status s = h->init(d->device, 0);
     if (s != PM_OK) { delete h; return s; }
     for (auto& f : h->field) {
         cudaError_t e = f.alloc(h->n() * h->esize());
@@ -449,9 +446,8 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
             return launch_heat_plain(h->plain_args(par, dt), st);
         });
     } else {
-        const int zc = Heat::zchunk_for(h->nz);
-        s = h->run_steps(nsteps, dt, true, [h, dt, zc](int par, cudaStream_t st) {
-            return launch_heat_f32(h->f32_args(par, dt), zc, st);
+        s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {
+            return launch_heat_f32(h->f32_args(par, dt), st);
         });
     }
     if (s != PM_OK) return s;

@@ -72,9 +72,10 @@ struct HeatPlainArgs {
     int nx, ny, nz;
     double dts, dx, reference;
     HeatFilms films;
+    Tiles tiles;
     DevState* st;
     double* partials;
-    unsigned nblocks;
+    unsigned nblocks;  // the launch's grid: min(tiles, resident blocks)
 };
 
 // solid.rs:1192-1219 `film_flux`, read off the old state.
@@ -108,43 +109,64 @@ __device__ __forceinline__ double film_flux(const HeatPlainArgs& a, int i, int j
     return out;
 }
 
+// Decode tile t of a tiling into the thread's column (i, j) and plane range [k0, k1).
+__device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i, int& j, int& k0, int& k1) {
+    const int tx = (int)(t % T.ntx);
+    const long long r = t / T.ntx;
+    const int ty = (int)(r % T.nty);
+    const int tz = (int)(r / T.nty);
+    i = tx * 32 + threadIdx.x;
+    j = ty * 8 + threadIdx.y;
+    k0 = tz * T.zc;
+    k1 = min(T.nz, k0 + T.zc);
+}
+
+// Plain form. Each thread marches its column through the tile's planes, holding the cell
+// below, the cell and the cell above in registers.
 static __global__ void __launch_bounds__(256) heat_plain_step(HeatPlainArgs a) {
     if (a.st->violated) return;
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k = blockIdx.z;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t plane = (size_t)nx * ny;
     double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
-    if (i < a.nx && j < a.ny) {
-        const int nx = a.nx, ny = a.ny, nz = a.nz;
-        const size_t plane = (size_t)nx * ny;
-        const size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
-        const double t = a.told[c];
-        double flux = 0.0;
-        if (a.uniform) {
-            const double kf = a.kface;
-            if (i > 0) flux += kf * (a.told[c - 1] - t);
-            if (i + 1 < nx) flux += kf * (a.told[c + 1] - t);
-            if (j > 0) flux += kf * (a.told[c - nx] - t);
-            if (j + 1 < ny) flux += kf * (a.told[c + nx] - t);
-            if (k > 0) flux += kf * (a.told[c - plane] - t);
-            if (k + 1 < nz) flux += kf * (a.told[c + plane] - t);
-        } else {
-            const size_t xr = (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
-            const size_t yr = (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
-            if (i > 0) flux += a.kx[i + xr] * (a.told[c - 1] - t);
-            if (i + 1 < nx) flux += a.kx[i + 1 + xr] * (a.told[c + 1] - t);
-            if (j > 0) flux += a.ky[i + yr] * (a.told[c - nx] - t);
-            if (j + 1 < ny) flux += a.ky[i + nx + yr] * (a.told[c + nx] - t);
-            if (k > 0) flux += a.kz[c] * (a.told[c - plane] - t);
-            if (k + 1 < nz) flux += a.kz[c + plane] * (a.told[c + plane] - t);
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        int i, j, k0, k1;
+        tile_column(a.tiles, t, i, j, k0, k1);
+        if (i >= nx || j >= ny) continue;
+        size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+        double below = k0 > 0 ? a.told[c - plane] : 0.0;
+        double here = a.told[c];
+        for (int k = k0; k < k1; ++k, c += plane) {
+            const double above = k + 1 < nz ? a.told[c + plane] : 0.0;
+            const double t0 = here;
+            double flux = 0.0;
+            if (a.uniform) {
+                const double kf = a.kface;
+                if (i > 0) flux += kf * (a.told[c - 1] - t0);
+                if (i + 1 < nx) flux += kf * (a.told[c + 1] - t0);
+                if (j > 0) flux += kf * (a.told[c - nx] - t0);
+                if (j + 1 < ny) flux += kf * (a.told[c + nx] - t0);
+                if (k > 0) flux += kf * (below - t0);
+                if (k + 1 < nz) flux += kf * (above - t0);
+            } else {
+                const size_t xr = (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
+                const size_t yr = (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
+                if (i > 0) flux += a.kx[i + xr] * (a.told[c - 1] - t0);
+                if (i + 1 < nx) flux += a.kx[i + 1 + xr] * (a.told[c + 1] - t0);
+                if (j > 0) flux += a.ky[i + yr] * (a.told[c - nx] - t0);
+                if (j + 1 < ny) flux += a.ky[i + nx + yr] * (a.told[c + nx] - t0);
+                if (k > 0) flux += a.kz[c] * (below - t0);
+                if (k + 1 < nz) flux += a.kz[c + plane] * (above - t0);
+            }
+            const double shed = a.films.exposed ? film_flux(a, i, j, k, c, t0) : 0.0;
+            const double mob = a.uniform ? a.mobility : a.mob[c];
+            const double capc = a.uniform ? a.capacity : a.cap[c];
+            const double nt = t0 + a.dts * mob * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
+            a.tnew[c] = nt;
+            acc[0] += capc * (nt - a.reference);                  // solid.rs:1583-1590
+            if (shed != 0.0) acc[1] += a.dts * mob * shed * capc;  // solid.rs:1821-1823
+            below = here;
+            here = above;
         }
-        const double shed = a.films.exposed ? film_flux(a, i, j, k, c, t) : 0.0;
-        const double mob = a.uniform ? a.mobility : a.mob[c];
-        const double capc = a.uniform ? a.capacity : a.cap[c];
-        const double nt = t + a.dts * mob * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
-        a.tnew[c] = nt;
-        acc[0] = capc * (nt - a.reference);                  // solid.rs:1583-1590
-        if (shed != 0.0) acc[1] = a.dts * mob * shed * capc;  // solid.rs:1821-1823
     }
     if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;
@@ -169,29 +191,28 @@ struct HeatF32Args {
     float b[6];      // dt · mobility · g_f / dx per film face
     float off[6];    // T0 − ambient per film face
     double capacity; // per cell
+    Tiles tiles;
     DevState* st;
     double* partials;
     unsigned nblocks;
 };
 
-// Chosen form, z-marching: each thread owns one (i, j) column of a z-chunk and keeps the cell
-// below, the cell and the cell above in registers, so a plane is read from memory once and the
-// in-plane neighbours come from L1/L2.
-static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a, int zchunk) {
+// Chosen form, z-marching like the plain form; neighbours in the plane come from L1/L2.
+static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
     if (a.st->violated) return;
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k0 = blockIdx.z * zchunk;
-    const int k1 = min(a.nz, k0 + zchunk);
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t plane = (size_t)nx * ny;
     double acc[2] = {0.0, 0.0};
-    if (i < a.nx && j < a.ny && k0 < k1) {
-        const int nx = a.nx, ny = a.ny, nz = a.nz;
-        const size_t plane = (size_t)nx * ny;
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        int i, j, k0, k1;
+        tile_column(a.tiles, t, i, j, k0, k1);
+        if (i >= nx || j >= ny) continue;
         size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
         float below = k0 > 0 ? __ldg(a.dold + c - plane) : 0.0f;
         float here = __ldg(a.dold + c);
         const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
         const bool edge_xy = !(xl && xh && yl && yh);
+        double col_shed = 0.0;
         for (int k = k0; k < k1; ++k, c += plane) {
             const float above = (k + 1 < nz) ? __ldg(a.dold + c + plane) : 0.0f;
             float s = 0.0f;
@@ -209,14 +230,15 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a, int z
                 if (((a.exposed >> 3) & 1) && !yh) shed += a.b[3] * (here + a.off[3]);
                 if (((a.exposed >> 4) & 1) && k == 0) shed += a.b[4] * (here + a.off[4]);
                 if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += a.b[5] * (here + a.off[5]);
+                col_shed += (double)shed;
             }
             const float nd = here + (a.a * s - shed);
             a.dnew[c] = nd;
             acc[0] += (double)nd;
-            acc[1] += (double)shed;
             below = here;
             here = above;
         }
+        acc[1] += col_shed;
     }
     if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;

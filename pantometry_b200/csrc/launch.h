@@ -11,19 +11,45 @@
 
 namespace pm {
 
-// Launch geometry shared by every per-node kernel: 32 × 8 threads per block, one z-plane (or
-// z-chunk) per grid row.
-inline dim3 plane_block() { return dim3(32, 8, 1); }
-inline dim3 plane_grid(int nx, int ny, int nz) { return dim3((nx + 31) / 32, (ny + 7) / 8, nz); }
-inline unsigned plane_blocks(int nx, int ny, int nz) {
-    dim3 g = plane_grid(nx, ny, nz);
-    return g.x * g.y * g.z;
+// Launch geometry: 32 × 8 threads per block; a persistent grid of at most `resident` blocks
+// (8 per SM at 256 threads) walking the tiles of make_tiles().
+inline dim3 tile_block() { return dim3(32, 8, 1); }
+constexpr int kBlocksPerSM = 8;
+constexpr int kMeasureBlocks = 592;  // 4 × 148 SMs, for the flat element-wise kernels
+
+// The z-chunk that spreads the tiles most evenly over `resident` blocks, preferring deeper
+// chunks (fewer re-read planes) when the balance is equal.
+inline int choose_zc(int nx, int ny, int nz, unsigned resident) {
+    int best = 4;
+    double best_score = -1.0;
+    for (int zc : {4, 8, 16, 32}) {
+        if (zc > nz && zc != 4) continue;
+        Tiles t = make_tiles(nx, ny, nz, zc);
+        double per = (double)t.ntiles / resident;
+        double rounds = per < 1.0 ? 1.0 : (double)((t.ntiles + resident - 1) / resident);
+        double balance = per < 1.0 ? per : per / rounds;
+        double score = balance * (1.0 - 1.0 / (2.0 * zc));
+        if (score > best_score + 1e-9) { best_score = score; best = zc; }
+    }
+    return best;
 }
-constexpr int kMeasureBlocks = 592;  // 4 × 148 SMs
+inline unsigned grid_for(const Tiles& t, unsigned resident) {
+    return (unsigned)(t.ntiles < (long long)resident ? t.ntiles : (long long)resident);
+}
+
+// Resident blocks per SM of each step kernel at 256 threads (cudaOccupancyMaxActiveBlocksPer-
+// Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
+enum KernelId : int {
+    kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kKernelCount
+};
+int blocks_per_sm(KernelId id);
+
+template <typename Real>
+inline size_t hall_smem_bytes() { return sizeof(HallStage<Real>) * HallDepth<Real>::stages; }
 
 cudaError_t launch_heat_plain(const HeatPlainArgs& a, cudaStream_t s);
 cudaError_t launch_heat_measure_plain(const HeatMeasureArgs& a, cudaStream_t s);
-cudaError_t launch_heat_f32(const HeatF32Args& a, int zchunk, cudaStream_t s);
+cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s);
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s);
 cudaError_t launch_heat_convert(const double* t, float* d, double t0, size_t n, int to_dev, double* tout,
                                 cudaStream_t s);

@@ -6,7 +6,7 @@
 namespace pm {
 
 cudaError_t launch_heat_plain(const HeatPlainArgs& a, cudaStream_t s) {
-    heat_plain_step<<<plane_grid(a.nx, a.ny, a.nz), plane_block(), 0, s>>>(a);
+    heat_plain_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -34,28 +34,54 @@ cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, cud
 
 template <>
 cudaError_t launch_hall<double>(const HallArgs<double>& a, cudaStream_t s) {
-    hall_step<double><<<plane_grid(a.nx, a.ny, a.nz), plane_block(), 0, s>>>(a);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(hall_step<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
+        cudaFuncSetAttribute(hall_step<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
+        attr = true;
+    }
+    if (a.block_scale)
+        hall_step<double, true><<<a.nblocks, tile_block(), hall_smem_bytes<double>(), s>>>(a);
+    else
+        hall_step<double, false><<<a.nblocks, tile_block(), hall_smem_bytes<double>(), s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_hall_measure<double>(const HallMeasureArgs<double>& a, cudaStream_t s) {
-    hall_measure<double><<<plane_grid(a.nx, a.ny, a.nz), plane_block(), 0, s>>>(a);
+    hall_measure<double><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_yee_h<double>(const YeeHArgs<double>& a, cudaStream_t s) {
-    yee_h<double><<<plane_grid(a.nx + 1, a.ny + 1, a.nz + 1), plane_block(), 0, s>>>(a);
+    yee_h<double><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_yee_e<double>(const YeeEArgs<double>& a, cudaStream_t s) {
-    yee_e<double><<<plane_grid(a.nx + 1, a.ny + 1, a.nz + 1), plane_block(), 0, s>>>(a);
+    yee_e<double><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 template <>
 cudaError_t launch_yee_measure<double>(const YeeHArgs<double>& a, double* out2, cudaStream_t s) {
-    yee_measure<double><<<plane_grid(a.nx + 1, a.ny + 1, a.nz + 1), plane_block(), 0, s>>>(a, out2);
+    yee_measure<double><<<a.nblocks, tile_block(), 0, s>>>(a, out2);
     return cudaGetLastError();
+}
+
+
+int occupancy_f64(KernelId id) {
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+    switch (id) {
+        case kHeatPlain: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_step, 256, 0); break;
+        case kHallF64:
+            cudaFuncSetAttribute(hall_step<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<double, false>, 256, hall_smem_bytes<double>());
+            break;
+        case kYeeHF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<double>, 256, 0); break;
+        case kYeeEF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<double>, 256, 0); break;
+        default: return -1;
+    }
+    return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 }  // namespace pm

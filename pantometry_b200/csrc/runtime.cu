@@ -1,5 +1,6 @@
 // Host runtime: the Handle base (stream, graphs, device state, audit readout) and the C ABI's
 // status and error functions. The three domains live in heat.cu, hall.cu and cavity.cu.
+#include <algorithm>
 #include <new>
 
 #include "runtime.h"
@@ -7,6 +8,20 @@
 namespace pm {
 
 static thread_local std::string g_error;
+
+int occupancy_f64(KernelId id);
+int occupancy_f32(KernelId id);
+
+int blocks_per_sm(KernelId id) {
+    static int cache[kKernelCount] = {0};
+    if (id < 0 || id >= kKernelCount) return 1;
+    if (cache[id] == 0) {
+        int n = occupancy_f64(id);
+        if (n < 0) n = occupancy_f32(id);
+        cache[id] = n < 1 ? 1 : n;
+    }
+    return cache[id];
+}
 
 void set_error(const std::string& msg) { g_error = msg; }
 
@@ -50,6 +65,12 @@ pm_status Handle::init(int dev, size_t partial_doubles) {
     if (prop.major != 10)
         return fail(PM_NO_DEVICE, "the kernels are built for sm_100a (B200); this device is sm_" +
                                       std::to_string(prop.major) + std::to_string(prop.minor));
+    int sms = 0;
+    PM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    sm_count = (unsigned)sms;
+    resident = (unsigned)sms * kBlocksPerSM;
+    if (partial_doubles < (size_t)std::max<unsigned>(resident, kMeasureBlocks) * 6)
+        partial_doubles = (size_t)std::max<unsigned>(resident, kMeasureBlocks) * 6;
     PM_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
     PM_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
     PM_CUDA(state.alloc(sizeof(DevState)));

@@ -61,7 +61,10 @@ struct Handle {
     DBuf state;      // DevState
     DBuf partials;   // per-block partial sums
     DevState* host_state = nullptr;  // pinned mirror
-    double tolerance = 1e-9;         // Tolerances::default (conserved.rs:303-307)
+    double tolerance = -1.0;         // no audit: plain `Domain::step`; set one to audit every step
+    unsigned resident = 148 * kBlocksPerSM;  // upper bound of any persistent grid (partials sizing)
+    unsigned sm_count = 148;
+    unsigned wave_of(KernelId id) const { return sm_count * (unsigned)blocks_per_sm(id); }
     int parity = 0;                  // which buffer of a ping-pong pair holds the state
     int call_parity = 0;             // parity when the present call began
     // graph cache

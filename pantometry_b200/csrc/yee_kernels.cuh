@@ -42,6 +42,7 @@ struct YeeHArgs {
     const double* __restrict__ eps1;
     const double* __restrict__ eps2;
     double volume;                   // dx³
+    Tiles tiles;                     // over the (nx+1) × (ny+1) × (nz+1) node lattice
     DevState* st;
     double* partials;
     unsigned nblocks;
@@ -52,71 +53,82 @@ __device__ __forceinline__ double half_if(bool end) { return end ? 0.5 : 1.0; }
 template <typename Real>
 static __global__ void __launch_bounds__(256) yee_h(YeeHArgs<Real> a) {
     if (a.st->violated) return;
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k = blockIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    // index helpers, cavity.rs:1044-1067
-    auto iex = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)nx * ((size_t)jj + (size_t)(ny + 1) * kk); };
-    auto iey = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)(nx + 1) * ((size_t)jj + (size_t)ny * kk); };
-    auto iez = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)(nx + 1) * ((size_t)jj + (size_t)(ny + 1) * kk); };
-    auto ihx = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)(nx + 1) * ((size_t)jj + (size_t)ny * kk); };
-    auto ihy = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)nx * ((size_t)jj + (size_t)(ny + 1) * kk); };
-    auto ihz = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)nx * ((size_t)jj + (size_t)ny * kk); };
+    // strides of the six arrays (cavity.rs:1044-1067): x fastest, then y, then z
+    const size_t sEx = (size_t)nx * (ny + 1), sEy = (size_t)(nx + 1) * ny, sEz = (size_t)(nx + 1) * (ny + 1);
+    const size_t sHx = (size_t)(nx + 1) * ny, sHy = (size_t)nx * (ny + 1), sHz = (size_t)nx * ny;
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // Σ wεEx², Σ wεEy², Σ wεEz², Σ wμHx⁺Hx⁻, ...
-    if (i <= nx && j <= ny && k <= nz) {
-        if (j < ny && k < nz) {  // hx over (nx+1) × ny × nz
-            const Real curl = (a.ez[iez(i, j + 1, k)] - a.ez[iez(i, j, k)]) - (a.ey[iey(i, j, k + 1)] - a.ey[iey(i, j, k)]);
-            const size_t idx = ihx(i, j, k);
-            const Real was = a.hx[idx];
-            double mu = a.mu_u;
-            Real c = a.ch;
-            if (!a.uniform) { mu = a.mu0[idx]; c = (Real)(a.g / mu); }
-            const Real now = was - c * curl;
-            a.hx[idx] = now;
-            if (a.energy) acc[3] = half_if(i == 0 || i == nx) * mu * (double)now * (double)was;
-        }
-        if (i < nx && k < nz) {  // hy over nx × (ny+1) × nz
-            const Real curl = (a.ex[iex(i, j, k + 1)] - a.ex[iex(i, j, k)]) - (a.ez[iez(i + 1, j, k)] - a.ez[iez(i, j, k)]);
-            const size_t idx = ihy(i, j, k);
-            const Real was = a.hy[idx];
-            double mu = a.mu_u;
-            Real c = a.ch;
-            if (!a.uniform) { mu = a.mu1[idx]; c = (Real)(a.g / mu); }
-            const Real now = was - c * curl;
-            a.hy[idx] = now;
-            if (a.energy) acc[4] = half_if(j == 0 || j == ny) * mu * (double)now * (double)was;
-        }
-        if (i < nx && j < ny) {  // hz over nx × ny × (nz+1)
-            const Real curl = (a.ey[iey(i + 1, j, k)] - a.ey[iey(i, j, k)]) - (a.ex[iex(i, j + 1, k)] - a.ex[iex(i, j, k)]);
-            const size_t idx = ihz(i, j, k);
-            const Real was = a.hz[idx];
-            double mu = a.mu_u;
-            Real c = a.ch;
-            if (!a.uniform) { mu = a.mu2[idx]; c = (Real)(a.g / mu); }
-            const Real now = was - c * curl;
-            a.hz[idx] = now;
-            if (a.energy) acc[5] = half_if(k == 0 || k == nz) * mu * (double)now * (double)was;
-        }
-        if (a.energy) {
-            if (i < nx) {  // ex: cell-centred in x, node-centred in y and z
-                const size_t idx = iex(i, j, k);
-                const double e = a.uniform ? a.eps_u : a.eps0[idx];
-                const double f = (double)a.ex[idx];
-                acc[0] = 1.0 * half_if(j == 0 || j == ny) * half_if(k == 0 || k == nz) * e * f * f;
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        const int tx = (int)(t % a.tiles.ntx);
+        const long long r = t / a.tiles.ntx;
+        const int i = tx * 32 + threadIdx.x;
+        const int j = (int)(r % a.tiles.nty) * 8 + threadIdx.y;
+        const int k0 = (int)(r / a.tiles.nty) * a.tiles.zc;
+        const int k1 = min(nz + 1, k0 + a.tiles.zc);
+        if (i > nx || j > ny) continue;
+        const bool hx_col = j < ny, hy_col = i < nx, hz_col = i < nx && j < ny;
+        const size_t ex0 = (size_t)i + (size_t)nx * j, ey0 = (size_t)i + (size_t)(nx + 1) * j;
+        const size_t ez0 = (size_t)i + (size_t)(nx + 1) * j;
+        const size_t hx0 = (size_t)i + (size_t)(nx + 1) * j, hy0 = (size_t)i + (size_t)nx * j, hz0 = (size_t)i + (size_t)nx * j;
+        // Ey(i, j, k) and Ex(i, j, k) of the present plane, carried from the previous plane's k+1
+        Real ey_k = (j < ny) ? a.ey[ey0 + sEy * k0] : Real(0);
+        Real ex_k = (i < nx) ? a.ex[ex0 + sEx * k0] : Real(0);
+        for (int k = k0; k < k1; ++k) {
+            const bool zin = k < nz;
+            const Real ey_k1 = (j < ny && zin) ? a.ey[ey0 + sEy * (k + 1)] : Real(0);
+            const Real ex_k1 = (i < nx && zin) ? a.ex[ex0 + sEx * (k + 1)] : Real(0);
+            if (hx_col && zin) {  // hx over (nx+1) × ny × nz (cavity.rs:1349-1358)
+                const Real curl = (a.ez[ez0 + (nx + 1) + sEz * k] - a.ez[ez0 + sEz * k]) - (ey_k1 - ey_k);
+                const size_t idx = hx0 + sHx * k;
+                const Real was = a.hx[idx];
+                double mu = a.mu_u;
+                Real c = a.ch;
+                if (!a.uniform) { mu = a.mu0[idx]; c = (Real)(a.g / mu); }
+                const Real now = was - c * curl;
+                a.hx[idx] = now;
+                if (a.energy) acc[3] += half_if(i == 0 || i == nx) * mu * (double)now * (double)was;
             }
-            if (j < ny) {
-                const size_t idx = iey(i, j, k);
-                const double e = a.uniform ? a.eps_u : a.eps1[idx];
-                const double f = (double)a.ey[idx];
-                acc[1] = half_if(i == 0 || i == nx) * 1.0 * half_if(k == 0 || k == nz) * e * f * f;
+            if (hy_col && zin) {  // hy over nx × (ny+1) × nz (cavity.rs:1359-1368)
+                const Real curl = (ex_k1 - ex_k) - (a.ez[ez0 + 1 + sEz * k] - a.ez[ez0 + sEz * k]);
+                const size_t idx = hy0 + sHy * k;
+                const Real was = a.hy[idx];
+                double mu = a.mu_u;
+                Real c = a.ch;
+                if (!a.uniform) { mu = a.mu1[idx]; c = (Real)(a.g / mu); }
+                const Real now = was - c * curl;
+                a.hy[idx] = now;
+                if (a.energy) acc[4] += half_if(j == 0 || j == ny) * mu * (double)now * (double)was;
             }
-            if (k < nz) {
-                const size_t idx = iez(i, j, k);
-                const double e = a.uniform ? a.eps_u : a.eps2[idx];
-                const double f = (double)a.ez[idx];
-                acc[2] = half_if(i == 0 || i == nx) * half_if(j == 0 || j == ny) * 1.0 * e * f * f;
+            if (hz_col) {  // hz over nx × ny × (nz+1) (cavity.rs:1369-1378)
+                const Real curl = (a.ey[ey0 + 1 + sEy * k] - ey_k) - (a.ex[ex0 + nx + sEx * k] - ex_k);
+                const size_t idx = hz0 + sHz * k;
+                const Real was = a.hz[idx];
+                double mu = a.mu_u;
+                Real c = a.ch;
+                if (!a.uniform) { mu = a.mu2[idx]; c = (Real)(a.g / mu); }
+                const Real now = was - c * curl;
+                a.hz[idx] = now;
+                if (a.energy) acc[5] += half_if(k == 0 || k == nz) * mu * (double)now * (double)was;
             }
+            if (a.energy) {
+                if (i < nx) {  // ex: cell-centred in x, node-centred in y and z
+                    const double e = a.uniform ? a.eps_u : a.eps0[ex0 + sEx * k];
+                    const double f = (double)ex_k;
+                    acc[0] += 1.0 * half_if(j == 0 || j == ny) * half_if(k == 0 || k == nz) * e * f * f;
+                }
+                if (j < ny) {
+                    const double e = a.uniform ? a.eps_u : a.eps1[ey0 + sEy * k];
+                    const double f = (double)ey_k;
+                    acc[1] += half_if(i == 0 || i == nx) * 1.0 * half_if(k == 0 || k == nz) * e * f * f;
+                }
+                if (zin) {
+                    const double e = a.uniform ? a.eps_u : a.eps2[ez0 + sEz * k];
+                    const double f = (double)a.ez[ez0 + sEz * k];
+                    acc[2] += half_if(i == 0 || i == nx) * half_if(j == 0 || j == ny) * 1.0 * e * f * f;
+                }
+            }
+            ey_k = ey_k1;
+            ex_k = ex_k1;
         }
     }
     if (!a.energy) return;
@@ -154,6 +166,7 @@ struct YeeEArgs {
     long long ncurrent;
     double eps_src, sig_src;            // ε, σ at the source edge
     int with_source;
+    Tiles tiles;
     DevState* st;
     double* partials;
     unsigned nblocks;
@@ -182,86 +195,103 @@ template <typename Real>
 static __global__ void __launch_bounds__(256) yee_e(YeeEArgs<Real> a) {
     DevState* st = a.st;
     if (st->violated) return;
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k = blockIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    auto iex = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)nx * ((size_t)jj + (size_t)(ny + 1) * kk); };
-    auto iey = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)(nx + 1) * ((size_t)jj + (size_t)ny * kk); };
-    auto iez = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)(nx + 1) * ((size_t)jj + (size_t)(ny + 1) * kk); };
-    auto ihx = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)(nx + 1) * ((size_t)jj + (size_t)ny * kk); };
-    auto ihy = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)nx * ((size_t)jj + (size_t)(ny + 1) * kk); };
-    auto ihz = [&](int ii, int jj, int kk) { return (size_t)ii + (size_t)nx * ((size_t)jj + (size_t)ny * kk); };
+    const size_t sEx = (size_t)nx * (ny + 1), sEy = (size_t)(nx + 1) * ny, sEz = (size_t)(nx + 1) * (ny + 1);
+    const size_t sHx = (size_t)(nx + 1) * ny, sHy = (size_t)nx * (ny + 1), sHz = (size_t)nx * ny;
     const long long step = st->steps;
     const double jsrc = (a.with_source && step < a.ncurrent) ? a.current[step] : 0.0;
     const double dt = a.dt;
     double acc[2] = {0.0, 0.0};  // Joule loss, source work
-    if (i <= nx && j <= ny && k <= nz) {
-        if (i < nx) {  // ex over nx × (ny+1) × (nz+1); interior j in 1..ny-1, k in 1..nz-1
-            const size_t idx = iex(i, j, k);
-            Real v = Real(0);
-            if (j >= 1 && j < ny && k >= 1 && k < nz) {
-                const Real curl = (a.hz[ihz(i, j, k)] - a.hz[ihz(i, j - 1, k)]) - (a.hy[ihy(i, j, k)] - a.hy[ihy(i, j, k - 1)]);
-                Real decay = a.decay[0], gain = a.gain[0];
-                double s = a.sigma_u[0];
-                if (!a.uniform) { s = a.sig0[idx]; coefficients<Real>(a.eps0[idx], s, dt, a.dx, decay, gain); }
-                const Real before = a.ex[idx];
-                v = decay * before + gain * curl;
-                const double mid = 0.5 * ((double)before + (double)v);
-                acc[0] += s * mid * mid * dt * a.volume;
-            }
-            if (a.solid && touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) v = Real(0);
-            a.ex[idx] = v;
-        }
-        if (j < ny) {  // ey over (nx+1) × ny × (nz+1); interior i in 1..nx-1, k in 1..nz-1
-            const size_t idx = iey(i, j, k);
-            Real v = Real(0);
-            if (i >= 1 && i < nx && k >= 1 && k < nz) {
-                const Real curl = (a.hx[ihx(i, j, k)] - a.hx[ihx(i, j, k - 1)]) - (a.hz[ihz(i, j, k)] - a.hz[ihz(i - 1, j, k)]);
-                Real decay = a.decay[1], gain = a.gain[1];
-                double s = a.sigma_u[1];
-                if (!a.uniform) { s = a.sig1[idx]; coefficients<Real>(a.eps1[idx], s, dt, a.dx, decay, gain); }
-                const Real before = a.ey[idx];
-                v = decay * before + gain * curl;
-                const double mid = 0.5 * ((double)before + (double)v);
-                acc[0] += s * mid * mid * dt * a.volume;
-            }
-            if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) v = Real(0);
-            a.ey[idx] = v;
-        }
-        if (k < nz) {  // ez over (nx+1) × (ny+1) × nz; interior i in 1..nx-1, j in 1..ny-1
-            const size_t idx = iez(i, j, k);
-            Real v = Real(0);
-            if (i >= 1 && i < nx && j >= 1 && j < ny) {
-                const Real curl = (a.hy[ihy(i, j, k)] - a.hy[ihy(i - 1, j, k)]) - (a.hx[ihx(i, j, k)] - a.hx[ihx(i, j - 1, k)]);
-                Real decay = a.decay[2], gain = a.gain[2];
-                double s = a.sigma_u[2];
-                if (!a.uniform) { s = a.sig2[idx]; coefficients<Real>(a.eps2[idx], s, dt, a.dx, decay, gain); }
-                const Real before = a.ez[idx];
-                v = decay * before + gain * curl;
-                if ((long long)idx == a.src) {
-                    // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
-                    const double e = a.eps_src, ss = a.sig_src;
-                    v = (Real)((double)v - (dt / e) / (1.0 + (ss * dt / (2.0 * e))) * jsrc);
-                    acc[1] += -(dt * a.volume) * jsrc * (0.5 * ((double)before + (double)v));
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        const int tx = (int)(t % a.tiles.ntx);
+        const long long r = t / a.tiles.ntx;
+        const int i = tx * 32 + threadIdx.x;
+        const int j = (int)(r % a.tiles.nty) * 8 + threadIdx.y;
+        const int k0 = (int)(r / a.tiles.nty) * a.tiles.zc;
+        const int k1 = min(nz + 1, k0 + a.tiles.zc);
+        if (i > nx || j > ny) continue;
+        const size_t ex0 = (size_t)i + (size_t)nx * j, ey0 = (size_t)i + (size_t)(nx + 1) * j;
+        const size_t ez0 = (size_t)i + (size_t)(nx + 1) * j;
+        const size_t hx0 = (size_t)i + (size_t)(nx + 1) * j, hy0 = (size_t)i + (size_t)nx * j, hz0 = (size_t)i + (size_t)nx * j;
+        // hy(i, j, k-1) and hx(i, j, k-1), carried from the previous plane
+        const bool xin = i >= 1 && i < nx, yin = j >= 1 && j < ny;
+        Real hy_km = (k0 >= 1 && i < nx && k0 - 1 < nz) ? a.hy[hy0 + sHy * (k0 - 1)] : Real(0);
+        Real hx_km = (k0 >= 1 && j < ny && k0 - 1 < nz) ? a.hx[hx0 + sHx * (k0 - 1)] : Real(0);
+        for (int k = k0; k < k1; ++k) {
+            const bool zin = k < nz, kint = k >= 1 && k < nz;
+            const Real hy_k = (i < nx && zin) ? a.hy[hy0 + sHy * k] : Real(0);
+            const Real hx_k = (j < ny && zin) ? a.hx[hx0 + sHx * k] : Real(0);
+            if (i < nx) {  // ex over nx × (ny+1) × (nz+1); interior j in 1..ny-1, k in 1..nz-1
+                const size_t idx = ex0 + sEx * k;
+                Real v = Real(0);
+                if (yin && kint) {
+                    const Real curl = (a.hz[hz0 + sHz * k] - a.hz[hz0 - nx + sHz * k]) - (hy_k - hy_km);
+                    Real decay = a.decay[0], gain = a.gain[0];
+                    double s = a.sigma_u[0];
+                    if (!a.uniform) { s = a.sig0[idx]; coefficients<Real>(a.eps0[idx], s, dt, a.dx, decay, gain); }
+                    const Real before = a.ex[idx];
+                    v = decay * before + gain * curl;
+                    const double mid = 0.5 * ((double)before + (double)v);
+                    acc[0] += s * mid * mid * dt * a.volume;
                 }
-                const double mid = 0.5 * ((double)before + (double)v);
-                acc[0] += s * mid * mid * dt * a.volume;
+                if (a.solid && touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) v = Real(0);
+                a.ex[idx] = v;
             }
-            if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) v = Real(0);
-            a.ez[idx] = v;
+            if (j < ny) {  // ey over (nx+1) × ny × (nz+1); interior i in 1..nx-1, k in 1..nz-1
+                const size_t idx = ey0 + sEy * k;
+                Real v = Real(0);
+                if (xin && kint) {
+                    const Real curl = (hx_k - hx_km) - (a.hz[hz0 + sHz * k] - a.hz[hz0 - 1 + sHz * k]);
+                    Real decay = a.decay[1], gain = a.gain[1];
+                    double s = a.sigma_u[1];
+                    if (!a.uniform) { s = a.sig1[idx]; coefficients<Real>(a.eps1[idx], s, dt, a.dx, decay, gain); }
+                    const Real before = a.ey[idx];
+                    v = decay * before + gain * curl;
+                    const double mid = 0.5 * ((double)before + (double)v);
+                    acc[0] += s * mid * mid * dt * a.volume;
+                }
+                if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) v = Real(0);
+                a.ey[idx] = v;
+            }
+            if (zin) {  // ez over (nx+1) × (ny+1) × nz; interior i in 1..nx-1, j in 1..ny-1
+                const size_t idx = ez0 + sEz * k;
+                Real v = Real(0);
+                if (xin && yin) {
+                    const Real curl = (hy_k - a.hy[hy0 - 1 + sHy * k]) - (hx_k - a.hx[hx0 - (nx + 1) + sHx * k]);
+                    Real decay = a.decay[2], gain = a.gain[2];
+                    double s = a.sigma_u[2];
+                    if (!a.uniform) { s = a.sig2[idx]; coefficients<Real>(a.eps2[idx], s, dt, a.dx, decay, gain); }
+                    const Real before = a.ez[idx];
+                    v = decay * before + gain * curl;
+                    if ((long long)idx == a.src) {
+                        // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
+                        const double e = a.eps_src, ss = a.sig_src;
+                        v = (Real)((double)v - (dt / e) / (1.0 + (ss * dt / (2.0 * e))) * jsrc);
+                        acc[1] += -(dt * a.volume) * jsrc * (0.5 * ((double)before + (double)v));
+                    }
+                    const double mid = 0.5 * ((double)before + (double)v);
+                    acc[0] += s * mid * mid * dt * a.volume;
+                }
+                if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) v = Real(0);
+                a.ez[idx] = v;
+            }
+            hy_km = hy_k;
+            hx_km = hx_k;
         }
     }
     if (finish_blocks<2>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
         st->dissipated += fmax(acc[0], 0.0);
+        // The invariant of this step was taken before this step's electric update, so the work
+        // that update did is booked against the next step's invariant.
+        st->work_booked = st->work;
         st->work += acc[1];
         double total = 0.0, scale = 0.0;
         ledger_add(total, scale, st->invariant);
         ledger_add(total, scale, st->dissipated);
-        if (a.with_source) ledger_add(total, scale, -st->work);
+        if (a.with_source) ledger_add(total, scale, -st->work_booked);
         st->part[0] = st->invariant;
         st->part[1] = st->dissipated;
-        st->part[2] = -st->work;
+        st->part[2] = -st->work_booked;
         audit_and_commit(st, total, scale);
     }
 }
@@ -270,41 +300,47 @@ static __global__ void __launch_bounds__(256) yee_e(YeeEArgs<Real> a) {
 // ledger reports before any invariant exists, and what pm_cavity_energies returns.
 template <typename Real>
 static __global__ void __launch_bounds__(256) yee_measure(YeeHArgs<Real> a, double* out2) {
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k = blockIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (i <= nx && j <= ny && k <= nz) {
-        if (i < nx) {
-            const size_t idx = (size_t)i + (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
-            const double f = (double)a.ex[idx];
-            acc[0] = half_if(j == 0 || j == ny) * half_if(k == 0 || k == nz) * (a.uniform ? a.eps_u : a.eps0[idx]) * f * f;
-        }
-        if (j < ny) {
-            const size_t idx = (size_t)i + (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
-            const double f = (double)a.ey[idx];
-            acc[1] = half_if(i == 0 || i == nx) * half_if(k == 0 || k == nz) * (a.uniform ? a.eps_u : a.eps1[idx]) * f * f;
-        }
-        if (k < nz) {
-            const size_t idx = (size_t)i + (size_t)(nx + 1) * ((size_t)j + (size_t)(ny + 1) * k);
-            const double f = (double)a.ez[idx];
-            acc[2] = half_if(i == 0 || i == nx) * half_if(j == 0 || j == ny) * (a.uniform ? a.eps_u : a.eps2[idx]) * f * f;
-        }
-        if (j < ny && k < nz) {
-            const size_t idx = (size_t)i + (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
-            const double f = (double)a.hx[idx];
-            acc[3] = half_if(i == 0 || i == nx) * (a.uniform ? a.mu_u : a.mu0[idx]) * f * f;
-        }
-        if (i < nx && k < nz) {
-            const size_t idx = (size_t)i + (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
-            const double f = (double)a.hy[idx];
-            acc[4] = half_if(j == 0 || j == ny) * (a.uniform ? a.mu_u : a.mu1[idx]) * f * f;
-        }
-        if (i < nx && j < ny) {
-            const size_t idx = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
-            const double f = (double)a.hz[idx];
-            acc[5] = half_if(k == 0 || k == nz) * (a.uniform ? a.mu_u : a.mu2[idx]) * f * f;
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        const int tx = (int)(t % a.tiles.ntx);
+        const long long r = t / a.tiles.ntx;
+        const int i = tx * 32 + threadIdx.x;
+        const int j = (int)(r % a.tiles.nty) * 8 + threadIdx.y;
+        const int k0 = (int)(r / a.tiles.nty) * a.tiles.zc;
+        const int k1 = min(nz + 1, k0 + a.tiles.zc);
+        if (i > nx || j > ny) continue;
+        for (int k = k0; k < k1; ++k) {
+            if (i < nx) {
+                const size_t idx = (size_t)i + (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
+                const double f = (double)a.ex[idx];
+                acc[0] += half_if(j == 0 || j == ny) * half_if(k == 0 || k == nz) * (a.uniform ? a.eps_u : a.eps0[idx]) * f * f;
+            }
+            if (j < ny) {
+                const size_t idx = (size_t)i + (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
+                const double f = (double)a.ey[idx];
+                acc[1] += half_if(i == 0 || i == nx) * half_if(k == 0 || k == nz) * (a.uniform ? a.eps_u : a.eps1[idx]) * f * f;
+            }
+            if (k < nz) {
+                const size_t idx = (size_t)i + (size_t)(nx + 1) * ((size_t)j + (size_t)(ny + 1) * k);
+                const double f = (double)a.ez[idx];
+                acc[2] += half_if(i == 0 || i == nx) * half_if(j == 0 || j == ny) * (a.uniform ? a.eps_u : a.eps2[idx]) * f * f;
+            }
+            if (j < ny && k < nz) {
+                const size_t idx = (size_t)i + (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
+                const double f = (double)a.hx[idx];
+                acc[3] += half_if(i == 0 || i == nx) * (a.uniform ? a.mu_u : a.mu0[idx]) * f * f;
+            }
+            if (i < nx && k < nz) {
+                const size_t idx = (size_t)i + (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
+                const double f = (double)a.hy[idx];
+                acc[4] += half_if(j == 0 || j == ny) * (a.uniform ? a.mu_u : a.mu1[idx]) * f * f;
+            }
+            if (i < nx && j < ny) {
+                const size_t idx = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
+                const double f = (double)a.hz[idx];
+                acc[5] += half_if(k == 0 || k == nz) * (a.uniform ? a.mu_u : a.mu2[idx]) * f * f;
+            }
         }
     }
     if (finish_blocks<6>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {

@@ -212,3 +212,29 @@ def test_audit_semantics():
     assert v["quantity"] == "energy" and v["site"] == "thermal"
     assert abs(abs(v["after"] - v["before"]) / v["scale"] - 0.4) < 1e-12
     assert oracle.audit_energy("s", (0.0, 0.0), (0.0, 0.0), 0.0) is None
+
+
+def test_extension_sources_keep_the_books_balanced():
+    """The point-source (Hall) and dipole-current (Cavity) extensions carry their work in the
+    ledger, so an audited run with the source on stays within the reference's 1e-9 tolerance."""
+    from pantometry_b200 import workloads as W
+
+    h = W.acoustic_hall(20, steps=200)
+    w, ht, d = h["size"]
+    o = oracle.Hall(w, ht, d, h["across"], h["speed"], h["density"])
+    o.release(h["pressure"])
+    o.set_source(h["source_node"], h["wave"])
+    assert o.advance(h["dt"], 200, tol=1e-9) is None
+    led = o.ledger()
+    assert abs(led["injected"]) > 1e-3 * abs(led["invariant"])  # the source really did work
+
+    counts, dx = (12, 10, 9), 1e-3
+    c = oracle.Yee(counts, dx)
+    dt = 0.9 * c.courant_limit()
+    t = (np.arange(300) + 0.5) * dt
+    cur = 1e6 * np.exp(-((t - 60 * dt) / (15 * dt)) ** 2) * np.sin(2 * math.pi * t / (20 * dt))
+    edge = 6 + (counts[0] + 1) * (5 + (counts[1] + 1) * 4)
+    c.set_source(edge, cur)
+    assert c.advance(dt, 300, tol=1e-9) is None
+    led = c.ledger()
+    assert led["invariant"] > 0.0 and abs(led["work"]) > 0.5 * led["invariant"]
