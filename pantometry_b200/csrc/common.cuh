@@ -43,6 +43,15 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
 }
+// The same copy to a shared address given as a 32-bit offset, issued only where `pred` holds
+// (a predicated instruction: no branch, no divergence).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_if(unsigned saddr, const void* gmem, bool pred) {
+    asm volatile(
+        "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q cp.async.ca.shared.global [%0], [%1], %3;\n}\n" ::"r"(saddr),
+        "l"(gmem), "r"((int)pred), "n"(BYTES)
+        : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }

@@ -54,50 +54,54 @@ struct HallArgs {
 __device__ __forceinline__ double wall_weight(int k, int n) { return (k == 0 || k + 1 == n) ? 2.0 : 1.0; }
 
 // The walk. Block b takes tiles b, b + G, b + 2G, ... (a tile is a 32 × 8 column of nodes over a
-// z-chunk) and steps through each tile's planes; neighbouring blocks hold neighbouring tiles at
-// the same time, so a tile's x and y halos come out of L2.
+// z-chunk) and steps through each tile's planes two at a time; neighbouring blocks hold
+// neighbouring tiles at the same time, so a tile's x and y halos come out of L2.
 //
-// Staging. Each plane of a tile — the pressures with a one-node halo in x and y, the pressures
-// of the plane above, the face velocities on both sides of the nodes — is copied into a ring of
-// kStages shared-memory stages with cp.async, up to kStages − 1 planes ahead of the plane being
-// computed, and the copies run on across tile boundaries. Every thread copies its own node's
-// five values plus at most one fixed halo value, so a plane costs a handful of instructions and
-// one barrier.
+// Staging. Each pair of planes of a tile — the pressures of both planes with a one-node halo in
+// x and y, the pressures of the plane above the pair, and the face velocities — is copied into a
+// ring of HallDepth::stages shared-memory stages with cp.async, running ahead of the pair being
+// computed and on across tile boundaries. Every thread copies its own nodes' values plus at most
+// one fixed halo value per plane, so a pair costs a handful of copy instructions and one barrier.
 template <typename Real> struct HallDepth;
-template <> struct HallDepth<float> { static constexpr int stages = 6, min_blocks = 4; };
-template <> struct HallDepth<double> { static constexpr int stages = 4, min_blocks = 3; };
+template <> struct HallDepth<float> { static constexpr int stages = 4, min_blocks = 3; };
+template <> struct HallDepth<double> { static constexpr int stages = 3, min_blocks = 2; };
 
 template <typename Real>
 struct HallStage {
-    Real p[10][34];  // p(x0-1 .. x0+32, y0-1 .. y0+8, k)
-    Real pa[8][32];  // p(x0 .. x0+31, y0 .. y0+7, k+1)
-    Real vx[8][33];  // x faces x0-1 .. x0+31
-    Real vy[9][32];  // y faces y0-1 .. y0+7
-    Real vz[8][32];  // z faces at k
+    Real p[2][10][34];  // p(x0-1 .. x0+32, y0-1 .. y0+8, k + h), h = 0, 1
+    Real pa[8][32];     // p(x0 .. x0+31, y0 .. y0+7, k+2)
+    Real vx[2][8][33];  // x faces x0-1 .. x0+31
+    Real vy[2][9][32];  // y faces y0-1 .. y0+7
+    Real vz[2][8][32];  // z faces at k + h
 };
 
 struct HallCursor {
-    long long t;
+    unsigned t;
     int x0, y0, k, k0, k1;
     bool valid;
 };
 
-__device__ __forceinline__ void hall_cursor_at(HallCursor& c, const Tiles& T, long long t) {
+// Tile t of the tiling (fewer than 2^32 tiles): 32-bit divisions only, once per tile.
+__device__ __forceinline__ void hall_cursor_at(HallCursor& c, const Tiles& T, unsigned t) {
     c.t = t;
-    c.valid = t < T.ntiles;
+    c.valid = t < (unsigned)T.ntiles;
     if (!c.valid) return;
-    const int tx = (int)(t % T.ntx);
-    const long long r = t / T.ntx;
-    c.x0 = tx * 32;
-    c.y0 = (int)(r % T.nty) * 8;
-    c.k0 = c.k = (int)(r / T.nty) * T.zc;
+    const unsigned r = t / (unsigned)T.ntx;
+    const unsigned tz = r / (unsigned)T.nty;
+    c.x0 = (int)(t - r * (unsigned)T.ntx) * 32;
+    c.y0 = (int)(r - tz * (unsigned)T.nty) * 8;
+    c.k0 = c.k = (int)tz * T.zc;
     c.k1 = min(T.nz, c.k + T.zc);
 }
-__device__ __forceinline__ void hall_cursor_next(HallCursor& c, const Tiles& T) {
-    if (++c.k >= c.k1) hall_cursor_at(c, T, c.t + gridDim.x);
+// to the next pair of planes; returns whether a new tile began
+__device__ __forceinline__ bool hall_cursor_next(HallCursor& c, const Tiles& T) {
+    c.k += 2;
+    if (c.k < c.k1) return false;
+    hall_cursor_at(c, T, c.t + gridDim.x);
+    return true;
 }
 
-// The one halo value thread `tid` copies, as (row, column) in the stage's p tile (kind 0), the
+// The one halo value thread `tid` copies per plane, as (row, column) in the p tile (kind 0), the
 // x-face column (kind 1) or the y-face row (kind 2); kind -1 for none.
 struct HallHalo {
     int kind, r, c;
@@ -113,67 +117,105 @@ __device__ __forceinline__ HallHalo hall_halo(int tid) {
     return h;
 }
 
-// A thread's offsets into the four arrays for its node of one tile, at the tile's first plane,
-// and the per-plane strides. Every array here has fewer than 2^32 elements.
-struct HallOffsets {
-    unsigned p, fx, fy;  // p and vz share the node index
-    unsigned halo;       // the thread's halo value, if any
+// What a thread copies for one tile: the global offsets of its node at plane k (every array here
+// has fewer than 2^32 elements), whether each value exists, and its halo value's array, offset and
+// plane stride, chosen once per tile so that the copies themselves never branch.
+struct HallCopy {
+    unsigned p, fx, fy;      // p and vz share the node index
+    unsigned halo, hstride;  // the halo value's offset and per-plane stride
+    unsigned hplane;         // bytes from the halo value's slot in the pair's first plane to its second
     bool live, xh, yh, halo_live;
 };
 
-__device__ __forceinline__ HallOffsets hall_offsets(const HallCursor& c, int nx, int ny, const HallHalo& h) {
-    HallOffsets o;
+template <typename Real>
+__device__ __forceinline__ HallCopy hall_copy_at(const HallCursor& c, const HallArgs<Real>& a, const HallHalo& h,
+                                                 unsigned sp, unsigned sx, unsigned sy) {
+    HallCopy o;
+    const int nx = a.nx, ny = a.ny;
     const int i = c.x0 + threadIdx.x, j = c.y0 + threadIdx.y, k = c.k;
     o.live = i < nx && j < ny;
-    o.xh = i + 1 < nx;
-    o.yh = j + 1 < ny;
+    o.xh = o.live && i + 1 < nx;
+    o.yh = o.live && j + 1 < ny;
     o.p = (unsigned)i + (unsigned)nx * ((unsigned)j + (unsigned)ny * (unsigned)k);
     o.fx = (unsigned)i + (unsigned)(nx - 1) * ((unsigned)j + (unsigned)ny * (unsigned)k);
     o.fy = (unsigned)i + (unsigned)nx * ((unsigned)j + (unsigned)(ny - 1) * (unsigned)k);
     o.halo = 0;
+    o.hstride = 0;
+    o.hplane = 0;
     o.halo_live = false;
     if (h.kind == 0) {
         const int gi = c.x0 - 1 + h.c, gj = c.y0 - 1 + h.r;
         o.halo_live = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
         o.halo = (unsigned)gi + (unsigned)nx * ((unsigned)gj + (unsigned)ny * (unsigned)k);
+        o.hstride = sp;
+        o.hplane = sizeof(Real) * 10 * 34;
     } else if (h.kind == 1) {
         const int fi = c.x0 - 1, gj = c.y0 + h.r;
         o.halo_live = fi >= 0 && gj < ny;
         o.halo = (unsigned)fi + (unsigned)(nx - 1) * ((unsigned)gj + (unsigned)ny * (unsigned)k);
+        o.hstride = sx;
+        o.hplane = sizeof(Real) * 8 * 33;
     } else if (h.kind == 2) {
         const int gi = c.x0 + h.c, fj = c.y0 - 1;
         o.halo_live = gi < nx && fj >= 0;
         o.halo = (unsigned)gi + (unsigned)nx * ((unsigned)fj + (unsigned)(ny - 1) * (unsigned)k);
+        o.hstride = sy;
+        o.hplane = sizeof(Real) * 9 * 32;
     }
     return o;
 }
 
-template <typename Real>
-__device__ __forceinline__ void hall_stage(HallStage<Real>& st, const HallArgs<Real>& a, const HallOffsets& o,
-                                           bool zh, const HallHalo& h) {
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    if (o.live) {
-        cp_async<sizeof(Real)>(&st.p[ty + 1][tx + 1], a.p0 + o.p);
-        if (zh) {
-            cp_async<sizeof(Real)>(&st.pa[ty][tx], a.p0 + o.p + (unsigned)a.nx * (unsigned)a.ny);
-            cp_async<sizeof(Real)>(&st.vz[ty][tx], a.vz0 + o.p);
-        }
-        if (o.xh) cp_async<sizeof(Real)>(&st.vx[ty][tx + 1], a.vx0 + o.fx);
-        if (o.yh) cp_async<sizeof(Real)>(&st.vy[ty + 1][tx], a.vy0 + o.fy);
-    }
-    if (o.halo_live) {
-        if (h.kind == 0) cp_async<sizeof(Real)>(&st.p[h.r][h.c], a.p0 + o.halo);
-        else if (h.kind == 1) cp_async<sizeof(Real)>(&st.vx[h.r][0], a.vx0 + o.halo);
-        else cp_async<sizeof(Real)>(&st.vy[0][h.c], a.vy0 + o.halo);
-    }
+__device__ __forceinline__ void hall_copy_next(HallCopy& o, unsigned sp, unsigned sx, unsigned sy) {
+    o.p += 2 * sp;
+    o.fx += 2 * sx;
+    o.fy += 2 * sy;
+    o.halo += 2 * o.hstride;
 }
 
-__device__ __forceinline__ void hall_offsets_next(HallOffsets& o, const HallHalo& h, unsigned sp, unsigned sx,
-                                                  unsigned sy) {
-    o.p += sp;
-    o.fx += sx;
-    o.fy += sy;
-    o.halo += h.kind == 0 ? sp : (h.kind == 1 ? sx : sy);
+// Byte offset within a stage of one of this thread's values.
+template <typename Real>
+__device__ __forceinline__ unsigned hall_at(const Real* q) {
+    return (unsigned)((const char*)q - (const char*)static_cast<const HallStage<Real>*>(nullptr));
+}
+
+// Byte offset within a stage of this thread's halo value (plane h).
+template <typename Real>
+__device__ __forceinline__ unsigned hall_halo_at(const HallHalo& h, int plane) {
+    const HallStage<Real>* z = nullptr;
+    if (h.kind == 0) return hall_at<Real>(&z->p[plane][h.r][h.c]);
+    if (h.kind == 1) return hall_at<Real>(&z->vx[plane][h.r][0]);
+    return hall_at<Real>(&z->vy[plane][0][h.c < 32 ? h.c : 0]);
+}
+
+// Queue the copies of the pair (k, k+1) of cursor c into the stage at shared address `base`.
+template <typename Real>
+__device__ __forceinline__ void hall_stage(unsigned base, unsigned halo_at, const HallArgs<Real>& a,
+                                           const HallCursor& c, const HallCopy& o, const Real* hsrc, unsigned sp,
+                                           unsigned sx, unsigned sy) {
+    constexpr int B = sizeof(Real);
+    constexpr unsigned PLANE_P = sizeof(Real) * 10 * 34, PLANE_VX = sizeof(Real) * 8 * 33, PLANE_VY = sizeof(Real) * 9 * 32,
+                       PLANE_VZ = sizeof(Real) * 8 * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const HallStage<Real>* z = nullptr;
+    const unsigned sp0 = base + hall_at<Real>(&z->p[0][ty + 1][tx + 1]);
+    const unsigned svx = base + hall_at<Real>(&z->vx[0][ty][tx + 1]);
+    const unsigned svy = base + hall_at<Real>(&z->vy[0][ty + 1][tx]);
+    const unsigned svz = base + hall_at<Real>(&z->vz[0][ty][tx]);
+    const unsigned spa = base + hall_at<Real>(&z->pa[ty][tx]);
+    const int nz = a.nz, k = c.k;
+    const bool two = k + 1 < c.k1;  // the pair's second plane is computed here
+    const bool z1 = o.live && k + 1 < nz, z2 = o.live && two && k + 2 < nz;
+    cp_async_if<B>(sp0, a.p0 + o.p, o.live);
+    cp_async_if<B>(sp0 + PLANE_P, a.p0 + o.p + sp, z1);
+    cp_async_if<B>(svz, a.vz0 + o.p, z1);
+    cp_async_if<B>(svx, a.vx0 + o.fx, o.xh);
+    cp_async_if<B>(svy, a.vy0 + o.fy, o.yh);
+    cp_async_if<B>(spa, a.p0 + o.p + 2 * sp, z2);
+    cp_async_if<B>(svz + PLANE_VZ, a.vz0 + o.p + sp, z2);
+    cp_async_if<B>(svx + PLANE_VX, a.vx0 + o.fx + sx, o.xh && two);
+    cp_async_if<B>(svy + PLANE_VY, a.vy0 + o.fy + sy, o.yh && two);
+    cp_async_if<B>(base + halo_at, hsrc + o.halo, o.halo_live);
+    cp_async_if<B>(base + halo_at + o.hplane, hsrc + o.halo + o.hstride, o.halo_live && two);
 }
 
 template <typename Real, bool HET>
@@ -181,8 +223,10 @@ static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_
     DevState* st = a.st;
     if (st->violated) return;
     constexpr int S = HallDepth<Real>::stages;
+    constexpr unsigned STAGE = sizeof(HallStage<Real>);
     extern __shared__ __align__(16) unsigned char hall_smem[];
     HallStage<Real>* ring = reinterpret_cast<HallStage<Real>*>(hall_smem);
+    const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(hall_smem));
     const long long step = st->steps;
     const double delta = (a.src_i >= 0 && step < a.nwave) ? a.wave[step] : 0.0;
     const double last_delta = st->last_delta;
@@ -195,43 +239,42 @@ static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_
     const Real gain = a.gain;
     const Tiles T = a.tiles;
     const HallHalo halo = hall_halo(tx + 32 * ty);
+    const unsigned halo_at = hall_halo_at<Real>(halo, 0);
+    const Real* hsrc = halo.kind == 1 ? a.vx0 : (halo.kind == 2 ? a.vy0 : a.p0);
 
     HallCursor pf, cc;
     hall_cursor_at(pf, T, blockIdx.x);
     hall_cursor_at(cc, T, blockIdx.x);
-    HallOffsets po = hall_offsets(pf, nx, ny, halo);
+    HallCopy po = hall_copy_at<Real>(pf, a, halo, sp, sx, sy);
     for (int d = 0; d < S - 1; ++d) {
-        if (pf.valid) hall_stage<Real>(ring[d], a, po, pf.k + 1 < nz, halo);
+        if (pf.valid) hall_stage<Real>(ring_base + d * STAGE, halo_at, a, pf, po, hsrc, sp, sx, sy);
         cp_async_commit();
-        const long long t = pf.t;
-        hall_cursor_next(pf, T);
-        if (pf.t != t) po = hall_offsets(pf, nx, ny, halo);
-        else hall_offsets_next(po, halo, sp, sx, sy);
+        if (hall_cursor_next(pf, T)) po = hall_copy_at<Real>(pf, a, halo, sp, sx, sy);
+        else hall_copy_next(po, sp, sx, sy);
     }
     // per tile: this thread's node offsets and its invariant weights
-    HallOffsets co = hall_offsets(cc, nx, ny, halo);
+    HallCopy co = hall_copy_at<Real>(cc, a, halo, sp, sx, sy);
+    bool fresh = true;
     double cn = 0.0, cxf = 0.0, cyf = 0.0, czf = 0.0;  // node, x-face, y-face, z-face weights
     Real wi = Real(1), wj = Real(1);
     bool xl = false, yl = false, src_col = false;
     Real sc = a.scale;
     double kn = a.knode;
     Real lz = Real(0);
-    long long tile = -1;
     int slot = 0;
     while (cc.valid) {
-        cp_async_wait<S - 2>();  // this thread's copies of the plane have landed
-        __syncthreads();         // ... and everyone's; and everyone is done with the previous plane
-        if (pf.valid) hall_stage<Real>(ring[(slot + S - 1) % S], a, po, pf.k + 1 < nz, halo);
-        cp_async_commit();
+        cp_async_wait<S - 2>();  // this thread's copies of the pair have landed
+        __syncthreads();         // ... and everyone's; and everyone is done with the previous pair
         {
-            const long long t = pf.t;
-            hall_cursor_next(pf, T);
-            if (pf.t != t) po = hall_offsets(pf, nx, ny, halo);
-            else hall_offsets_next(po, halo, sp, sx, sy);
+            const int fill = slot == 0 ? S - 1 : slot - 1;
+            if (pf.valid) hall_stage<Real>(ring_base + fill * STAGE, halo_at, a, pf, po, hsrc, sp, sx, sy);
+            cp_async_commit();
+            if (hall_cursor_next(pf, T)) po = hall_copy_at<Real>(pf, a, halo, sp, sx, sy);
+            else hall_copy_next(po, sp, sx, sy);
         }
-        const int i = cc.x0 + tx, j = cc.y0 + ty, k = cc.k;
-        if (cc.t != tile) {  // a new tile: the weights that are constant over a column
-            tile = cc.t;
+        const int i = cc.x0 + tx, j = cc.y0 + ty;
+        if (fresh) {  // a new tile: the weights that are constant over a column
+            fresh = false;
             xl = i > 0;
             yl = j > 0;
             // hall.rs:675-681: weight 2 on a wall, 1 inside; the share 1/w is an exact power of two
@@ -239,11 +282,6 @@ static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_
             wj = (yl && co.yh) ? Real(1) : Real(2);
             const double si = (xl && co.xh) ? 1.0 : 0.5, sj = (yl && co.yh) ? 1.0 : 0.5;
             src_col = i == a.src_i && j == a.src_j;
-            if (HET) {
-                const int b = i / a.block + a.nbx * (j / a.block + a.nby * (k / a.block));
-                sc = a.block_scale[b];
-                kn = a.block_knode[b];
-            }
             cn = si * sj * kn;
             cxf = a.kface * sj;
             cyf = a.kface * si;
@@ -252,59 +290,67 @@ static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_
                 // the low z face of the tile's first node, from the old state:
                 // vz(k-1) − gain·(p(k) − p(k-1))
                 lz = Real(0);
-                if (k > 0) lz = a.vz0[co.p - sp] - gain * (a.p0[co.p] - a.p0[co.p - sp]);
+                if (cc.k > 0) lz = a.vz0[co.p - sp] - gain * (a.p0[co.p] - a.p0[co.p - sp]);
             }
         }
         const HallStage<Real>& c = ring[slot];
         if (co.live) {
-            if (HET && (k % a.block) == 0) {
-                const int b = i / a.block + a.nbx * (j / a.block + a.nby * (k / a.block));
-                sc = a.block_scale[b];
-                kn = a.block_knode[b];
-                cn = (((xl && co.xh) ? 1.0 : 0.5) * ((yl && co.yh) ? 1.0 : 0.5)) * kn;
+            unsigned op = co.p, ofx = co.fx, ofy = co.fy;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = cc.k + h;
+                if (h == 1 && k >= cc.k1) break;
+                if (HET && (h == 0 || (k % a.block) == 0)) {
+                    const int b = i / a.block + a.nbx * (j / a.block + a.nby * (k / a.block));
+                    sc = a.block_scale[b];
+                    kn = a.block_knode[b];
+                    cn = (((xl && co.xh) ? 1.0 : 0.5) * ((yl && co.yh) ? 1.0 : 0.5)) * kn;
+                }
+                // Every staged read is in bounds; a value with no face behind it is computed
+                // and then replaced by the reference's 0.0.
+                const Real pc = c.p[h][ty + 1][tx + 1];
+                const bool zh = k + 1 < nz;
+                const Real above = h == 0 ? c.p[1][ty + 1][tx + 1] : c.pa[ty][tx];
+                const Real hx0 = c.vx[h][ty][tx + 1] - gain * (c.p[h][ty + 1][tx + 2] - pc);
+                const Real lx0 = c.vx[h][ty][tx] - gain * (pc - c.p[h][ty + 1][tx]);
+                const Real hy0 = c.vy[h][ty + 1][tx] - gain * (c.p[h][ty + 2][tx + 1] - pc);
+                const Real ly0 = c.vy[h][ty][tx] - gain * (pc - c.p[h][ty][tx + 1]);
+                const Real hz0 = c.vz[h][ty][tx] - gain * (above - pc);
+                const Real hx = co.xh ? hx0 : Real(0), lx = xl ? lx0 : Real(0);
+                const Real hy = co.yh ? hy0 : Real(0), ly = yl ? ly0 : Real(0);
+                const Real hz = zh ? hz0 : Real(0);
+                if (co.xh) a.vx1[ofx] = hx;
+                if (co.yh) a.vy1[ofy] = hy;
+                if (zh) a.vz1[op] = hz;
+                const bool zin = k > 0 && zh;
+                const Real wk = zin ? Real(1) : Real(2);
+                // hall.rs:499-502
+                Real np = pc - sc * (wi * (hx - lx) + wj * (hy - ly) + wk * (hz - lz));
+                if (src_col && k == a.src_k) {
+                    // deferred term of the previous injection, then this one's
+                    acc[2] += a.wsrc * (last_delta + delta) * (double)pc;
+                    acc[1] += a.wsrc * delta * (double)pc;
+                    np = (Real)((double)np + delta);
+                }
+                a.p1[op] = np;
+                // hall.rs:345-349 (share · p · p_prev / 2ρc² · V) and 356-382 (share · ½ρv² · V
+                // on the node's own high faces)
+                const double dhx = (double)hx, dhy = (double)hy, dhz = (double)hz;
+                const double sk = zin ? 1.0 : 0.5;
+                acc[0] += sk * (cn * (double)np * (double)pc + cxf * dhx * dhx + cyf * dhy * dhy) + czf * dhz * dhz;
+                lz = hz;
+                op += sp;
+                ofx += sx;
+                ofy += sy;
             }
-            const Real pc = c.p[ty + 1][tx + 1];
-            const bool zh = k + 1 < nz;
-            Real hx = Real(0), lx = Real(0), hy = Real(0), ly = Real(0), hz = Real(0);
-            if (co.xh) {
-                hx = c.vx[ty][tx + 1] - gain * (c.p[ty + 1][tx + 2] - pc);
-                a.vx1[co.fx] = hx;
-            }
-            if (xl) lx = c.vx[ty][tx] - gain * (pc - c.p[ty + 1][tx]);
-            if (co.yh) {
-                hy = c.vy[ty + 1][tx] - gain * (c.p[ty + 2][tx + 1] - pc);
-                a.vy1[co.fy] = hy;
-            }
-            if (yl) ly = c.vy[ty][tx] - gain * (pc - c.p[ty][tx + 1]);
-            if (zh) {
-                hz = c.vz[ty][tx] - gain * (c.pa[ty][tx] - pc);
-                a.vz1[co.p] = hz;
-            }
-            const bool zin = k > 0 && zh;
-            const Real wk = zin ? Real(1) : Real(2);
-            // hall.rs:499-502
-            Real np = pc - sc * (wi * (hx - lx) + wj * (hy - ly) + wk * (hz - lz));
-            if (src_col && k == a.src_k) {
-                // deferred term of the previous injection, then this one's
-                acc[2] += a.wsrc * (last_delta + delta) * (double)pc;
-                acc[1] += a.wsrc * delta * (double)pc;
-                np = (Real)((double)np + delta);
-            }
-            a.p1[co.p] = np;
-            // hall.rs:345-349 (share · p · p_prev / 2ρc² · V) and 356-382 (share · ½ρv² · V on
-            // the node's own high faces)
-            const double dhx = (double)hx, dhy = (double)hy, dhz = (double)hz;
-            const double sk = zin ? 1.0 : 0.5;
-            acc[0] += sk * (cn * (double)np * (double)pc + cxf * dhx * dhx + cyf * dhy * dhy) + czf * dhz * dhz;
-            lz = hz;
         }
-        {
-            const long long t = cc.t;
-            hall_cursor_next(cc, T);
-            if (cc.t != t) co = hall_offsets(cc, nx, ny, halo);
-            else hall_offsets_next(co, halo, sp, sx, sy);
+        if (hall_cursor_next(cc, T)) {
+            co = hall_copy_at<Real>(cc, a, halo, sp, sx, sy);
+            fresh = true;
+        } else {
+            hall_copy_next(co, sp, sx, sy);
         }
-        slot = (slot + 1) % S;
+        slot = slot + 1 == S ? 0 : slot + 1;
     }
     cp_async_wait<0>();
     if (finish_blocks<3>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
