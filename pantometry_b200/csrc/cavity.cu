@@ -28,8 +28,8 @@ struct Cavity : Handle {
     std::vector<uint8_t> solid;
     bool any_solid = false;
     DBuf dsolid;
-    // fields (in place: no ping-pong)
-    DBuf f[6];  // ex ey ez hx hy hz
+    // fields: ping-pong pairs, f[parity] holds the state
+    DBuf f[2][6];  // ex ey ez hx hy hz
     DBuf keep[3];
     DBuf stage;
     DBuf energies;  // 2 doubles
@@ -137,8 +137,9 @@ struct Cavity : Handle {
     template <typename Real>
     YeeHArgs<Real> hargs(double g, int energy) const {
         YeeHArgs<Real> a{};
-        a.ex = f[0].as<Real>(); a.ey = f[1].as<Real>(); a.ez = f[2].as<Real>();
-        a.hx = f[3].as<Real>(); a.hy = f[4].as<Real>(); a.hz = f[5].as<Real>();
+        const DBuf* c = f[parity];
+        a.ex = c[0].as<Real>(); a.ey = c[1].as<Real>(); a.ez = c[2].as<Real>();
+        a.hx = c[3].as<Real>(); a.hy = c[4].as<Real>(); a.hz = c[5].as<Real>();
         a.nx = nx; a.ny = ny; a.nz = nz;
         a.g = g;
         a.uniform = uniform ? 1 : 0;
@@ -159,8 +160,9 @@ struct Cavity : Handle {
     template <typename Real>
     YeeEArgs<Real> eargs(double dt) const {
         YeeEArgs<Real> a{};
-        a.ex = f[0].as<Real>(); a.ey = f[1].as<Real>(); a.ez = f[2].as<Real>();
-        a.hx = f[3].as<Real>(); a.hy = f[4].as<Real>(); a.hz = f[5].as<Real>();
+        const DBuf* c = f[parity];
+        a.ex = c[0].as<Real>(); a.ey = c[1].as<Real>(); a.ez = c[2].as<Real>();
+        a.hx = c[3].as<Real>(); a.hy = c[4].as<Real>(); a.hz = c[5].as<Real>();
         a.nx = nx; a.ny = ny; a.nz = nz;
         a.dt = dt; a.dx = dx; a.volume = volume();
         a.uniform = uniform ? 1 : 0;
@@ -190,6 +192,54 @@ struct Cavity : Handle {
         return a;
     }
 
+    // The fused step from buffer set `par` into `par ^ 1`.
+    template <typename Real>
+    YeeStepArgs<Real> sargs(int par, double dt) const {
+        YeeStepArgs<Real> a{};
+        for (int q = 0; q < 6; ++q) {
+            a.old[q] = f[par][q].as<Real>();
+            a.neu[q] = f[par ^ 1][q].as<Real>();
+        }
+        a.pstride[0] = (unsigned)nx * (unsigned)(ny + 1);
+        a.pstride[1] = (unsigned)(nx + 1) * (unsigned)ny;
+        a.pstride[2] = (unsigned)(nx + 1) * (unsigned)(ny + 1);
+        a.pstride[3] = (unsigned)(nx + 1) * (unsigned)ny;
+        a.pstride[4] = (unsigned)nx * (unsigned)(ny + 1);
+        a.pstride[5] = (unsigned)nx * (unsigned)ny;
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        a.g = dt / dx;
+        a.uniform = uniform ? 1 : 0;
+        a.ch = (Real)(a.g / mu_u);  // cavity.rs:1355: g / μ
+        a.mu0 = dmu[0].as<double>(); a.mu1 = dmu[1].as<double>(); a.mu2 = dmu[2].as<double>();
+        a.mu_u = mu_u; a.eps_u = eps_u;
+        a.dt = dt; a.dx = dx; a.volume = volume();
+        const double half = sig_u * dt / (2.0 * eps_u);  // cavity.rs:1391-1397
+        for (int q = 0; q < 3; ++q) {
+            a.decay[q] = (Real)((1.0 - half) / (1.0 + half));
+            a.gain[q] = (Real)((dt / (eps_u * dx)) / (1.0 + half));
+            a.sigma_u[q] = sig_u;
+        }
+        a.eps0 = deps[0].as<double>(); a.eps1 = deps[1].as<double>(); a.eps2 = deps[2].as<double>();
+        a.sig0 = dsig[0].as<double>(); a.sig1 = dsig[1].as<double>(); a.sig2 = dsig[2].as<double>();
+        a.solid = any_solid ? dsolid.as<uint8_t>() : nullptr;
+        a.src_i = a.src_j = a.src_k = -1;
+        if (src >= 0) {
+            a.src_i = (int)(src % (nx + 1));
+            a.src_j = (int)((src / (nx + 1)) % (ny + 1));
+            a.src_k = (int)(src / ((long long)(nx + 1) * (ny + 1)));
+            a.eps_src = uniform ? eps_u : eps[2][(size_t)src];
+            a.sig_src = uniform ? sig_u : sig[2][(size_t)src];
+        }
+        a.current = current.as<double>();
+        a.ncurrent = ncurrent;
+        const unsigned w = wave_of(sizeof(Real) == 8 ? kYeeStepF64 : kYeeStepF32);
+        a.tiles = make_tiles(nx + 1, ny + 1, nz + 1, choose_zc(nx + 1, ny + 1, nz + 1, w));
+        a.nblocks = grid_for(a.tiles, w);
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        return a;
+    }
+
     pm_status launch_h(double g, int energy, cudaStream_t s) const {
         if (precision == PM_PLAIN_F64) PM_CUDA(launch_yee_h<double>(hargs<double>(g, energy), s));
         else PM_CUDA(launch_yee_h<float>(hargs<float>(g, energy), s));
@@ -199,15 +249,15 @@ struct Cavity : Handle {
     pm_status put(int q, const double* src_host) {
         const size_t n = count(q);
         if (!src_host) {
-            PM_CUDA(cudaMemsetAsync(f[q].p, 0, n * esize(), stream()));
+            PM_CUDA(cudaMemsetAsync(f[parity][q].p, 0, n * esize(), stream()));
             return PM_OK;
         }
         if (precision == PM_PLAIN_F64) {
-            PM_CUDA(cudaMemcpyAsync(f[q].p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
+            PM_CUDA(cudaMemcpyAsync(f[parity][q].p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
         } else {
             if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(n * 8));
             PM_CUDA(cudaMemcpyAsync(stage.p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
-            PM_CUDA(launch_to_f32(stage.as<double>(), f[q].as<float>(), n, stream()));
+            PM_CUDA(launch_to_f32(stage.as<double>(), f[parity][q].as<float>(), n, stream()));
             PM_CUDA(cudaStreamSynchronize(stream()));
         }
         return PM_OK;
@@ -216,10 +266,10 @@ struct Cavity : Handle {
         if (!dst_host) return PM_OK;
         const size_t n = count(q);
         if (precision == PM_PLAIN_F64) {
-            PM_CUDA(cudaMemcpyAsync(dst_host, f[q].p, n * 8, cudaMemcpyDeviceToHost, stream()));
+            PM_CUDA(cudaMemcpyAsync(dst_host, f[parity][q].p, n * 8, cudaMemcpyDeviceToHost, stream()));
         } else {
             if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(n * 8));
-            PM_CUDA(launch_to_f64(f[q].as<float>(), stage.as<double>(), n, stream()));
+            PM_CUDA(launch_to_f64(f[parity][q].as<float>(), stage.as<double>(), n, stream()));
             PM_CUDA(cudaMemcpyAsync(dst_host, stage.p, n * 8, cudaMemcpyDeviceToHost, stream()));
         }
         PM_CUDA(cudaStreamSynchronize(stream()));
@@ -308,11 +358,12 @@ pm_status pm_cavity_create(const pm_cavity_desc* d, pm_cavity** out) {
     c->uniform_media();
     pm_status s = c->init(d->device, 0);
     if (s != PM_OK) { delete c; return s; }
-    for (int q = 0; q < 6; ++q) {
-        cudaError_t e = c->f[q].alloc(c->count(q) * c->esize());
-        if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMalloc cavity fields"); }
-        cudaMemset(c->f[q].p, 0, c->count(q) * c->esize());
-    }
+    for (int par = 0; par < 2; ++par)
+        for (int q = 0; q < 6; ++q) {
+            cudaError_t e = c->f[par][q].alloc(c->count(q) * c->esize());
+            if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMalloc cavity fields"); }
+            cudaMemset(c->f[par][q].p, 0, c->count(q) * c->esize());
+        }
     *out = reinterpret_cast<pm_cavity*>(c);
     s = c->reset_ledger();
     if (s != PM_OK) { delete c; *out = nullptr; }
@@ -388,6 +439,7 @@ pm_status pm_cavity_upload(pm_cavity* cp, const double* ex, const double* ey, co
     Cavity* c = reinterpret_cast<Cavity*>(cp);
     CAV_GUARD(c);
     const double* src[6] = {ex, ey, ez, hx, hy, hz};
+    c->parity = 0;
     pm_status s;
     for (int q = 0; q < 6; ++q)
         if ((s = c->put(q, src[q])) != PM_OK) return s;
@@ -450,11 +502,11 @@ pm_status pm_cavity_release_mode(pm_cavity* cp, int m_in, int p_in, double ampli
     for (int q = 0; q < 3; ++q) {
         const size_t bytes = c->count(q + 3) * c->esize();
         if (!c->keep[q].p) PM_CUDA(c->keep[q].alloc(bytes));
-        PM_CUDA(cudaMemcpyAsync(c->keep[q].p, c->f[q + 3].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
+        PM_CUDA(cudaMemcpyAsync(c->keep[q].p, c->f[c->parity][q + 3].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
     }
     if ((s = c->launch_h(dt / c->dx, 1, c->stream())) != PM_OK) return s;
     for (int q = 0; q < 3; ++q)
-        PM_CUDA(cudaMemcpyAsync(c->f[q + 3].p, c->keep[q].p, c->count(q + 3) * c->esize(), cudaMemcpyDeviceToDevice,
+        PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q + 3].p, c->keep[q].p, c->count(q + 3) * c->esize(), cudaMemcpyDeviceToDevice,
                                 c->stream()));
     PM_CUDA(cudaStreamSynchronize(c->stream()));
     return c->reset_ledger();
@@ -511,18 +563,12 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
         if ((s = c->launch_h((0.5 * h) / c->dx, 0, c->stream())) != PM_OK) return s;
         c->started = true;
     }
-    const double g = h / c->dx;
-    s = c->run_steps(nsteps, dt, false, [c, g, h](int, cudaStream_t st) {
-        cudaError_t e;
-        if (c->precision == PM_PLAIN_F64) {
-            if ((e = launch_yee_h<double>(c->hargs<double>(g, 1), st)) != cudaSuccess) return e;
-            return launch_yee_e<double>(c->eargs<double>(h), st);
-        }
-        if ((e = launch_yee_h<float>(c->hargs<float>(g, 1), st)) != cudaSuccess) return e;
-        return launch_yee_e<float>(c->eargs<float>(h), st);
+    s = c->run_steps(nsteps, dt, true, [c, h](int par, cudaStream_t st) {
+        if (c->precision == PM_PLAIN_F64) return launch_yee_step<double>(c->sargs<double>(par, h), st);
+        return launch_yee_step<float>(c->sargs<float>(par, h), st);
     });
     if (s != PM_OK) return s;
-    return c->finish_call(before, out, "simulation", "simulation", false);
+    return c->finish_call(before, out, "simulation", "simulation", true);
 }
 
 pm_status pm_cavity_ledger(pm_cavity* cp, pm_ledger* out) {
@@ -555,7 +601,7 @@ pm_status pm_cavity_checkpoint(pm_cavity* cp) {
     for (int q = 0; q < 6; ++q) {
         const size_t bytes = c->count(q) * c->esize();
         if (!c->sf[q].p) PM_CUDA(c->sf[q].alloc(bytes));
-        PM_CUDA(cudaMemcpyAsync(c->sf[q].p, c->f[q].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
+        PM_CUDA(cudaMemcpyAsync(c->sf[q].p, c->f[c->parity][q].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
     }
     pm_status s = c->read_state();
     if (s != PM_OK) return s;
@@ -570,7 +616,7 @@ pm_status pm_cavity_restore(pm_cavity* cp) {
     CAV_GUARD(c);
     if (!c->has_saved) return PM_OK;
     for (int q = 0; q < 6; ++q)
-        PM_CUDA(cudaMemcpyAsync(c->f[q].p, c->sf[q].p, c->count(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
+        PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q].p, c->sf[q].p, c->count(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
     pm_status s = c->read_state();
     if (s != PM_OK) return s;
     c->started = c->s_started;

@@ -4,7 +4,7 @@
 namespace pm {
 
 cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s) {
-    heat_f32_step<<<a.nblocks, tile_block(), 0, s>>>(a);
+    heat_f32_step<<<a.nblocks, tile_block(), sizeof(HeatStage) * kHeatStages, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -43,6 +43,16 @@ cudaError_t launch_yee_e<float>(const YeeEArgs<float>& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 template <>
+cudaError_t launch_yee_step<float>(const YeeStepArgs<float>& a, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(yee_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
+        attr = true;
+    }
+    yee_step<float><<<a.nblocks, tile_block(), yee_smem_bytes<float>(), s>>>(a);
+    return cudaGetLastError();
+}
+template <>
 cudaError_t launch_yee_measure<float>(const YeeHArgs<float>& a, double* out2, cudaStream_t s) {
     yee_measure<float><<<a.nblocks, tile_block(), 0, s>>>(a, out2);
     return cudaGetLastError();
@@ -70,13 +80,17 @@ int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
     switch (id) {
-        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step, 256, 0); break;
+        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step, 256, sizeof(HeatStage) * kHeatStages); break;
         case kHallF32:
             cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<float, false>, 256, hall_smem_bytes<float>());
             break;
         case kYeeHF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<float>, 256, 0); break;
         case kYeeEF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<float>, 256, 0); break;
+        case kYeeStepF32:
+            cudaFuncSetAttribute(yee_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float>, 256, yee_smem_bytes<float>());
+            break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -73,6 +73,8 @@ struct HallStage {
     Real vx[2][8][33];  // x faces x0-1 .. x0+31
     Real vy[2][9][32];  // y faces y0-1 .. y0+7
     Real vz[2][8][32];  // z faces at k + h
+    Real pb[8][32];     // p(.., k-1) and vz(.., k-1): the plane below, at a tile's first pair only
+    Real vzb[8][32];
 };
 
 struct HallCursor {
@@ -214,6 +216,10 @@ __device__ __forceinline__ void hall_stage(unsigned base, unsigned halo_at, cons
     cp_async_if<B>(svz + PLANE_VZ, a.vz0 + o.p + sp, z2);
     cp_async_if<B>(svx + PLANE_VX, a.vx0 + o.fx + sx, o.xh && two);
     cp_async_if<B>(svy + PLANE_VY, a.vy0 + o.fy + sy, o.yh && two);
+    // the plane below a tile's first pair, for the low z face of its first node
+    const bool below = o.live && k == c.k0 && k > 0;
+    cp_async_if<B>(base + hall_at<Real>(&z->pb[ty][tx]), a.p0 + (below ? o.p - sp : o.p), below);
+    cp_async_if<B>(base + hall_at<Real>(&z->vzb[ty][tx]), a.vz0 + (below ? o.p - sp : o.p), below);
     cp_async_if<B>(base + halo_at, hsrc + o.halo, o.halo_live);
     cp_async_if<B>(base + halo_at + o.hplane, hsrc + o.halo + o.hstride, o.halo_live && two);
 }
@@ -286,14 +292,13 @@ static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_
             cxf = a.kface * sj;
             cyf = a.kface * si;
             czf = a.kface * si * sj;
-            if (co.live) {
-                // the low z face of the tile's first node, from the old state:
-                // vz(k-1) − gain·(p(k) − p(k-1))
-                lz = Real(0);
-                if (cc.k > 0) lz = a.vz0[co.p - sp] - gain * (a.p0[co.p] - a.p0[co.p - sp]);
-            }
         }
         const HallStage<Real>& c = ring[slot];
+        if (cc.k == cc.k0) {
+            // the low z face of the tile's first node, from the old state staged with the pair:
+            // vz(k-1) − gain·(p(k) − p(k-1))
+            lz = cc.k > 0 ? c.vzb[ty][tx] - gain * (c.p[0][ty + 1][tx + 1] - c.pb[ty][tx]) : Real(0);
+        }
         if (co.live) {
             unsigned op = co.p, ofx = co.fx, ofy = co.fy;
 #pragma unroll

@@ -40,10 +40,13 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Resident blocks per SM of each step kernel at 256 threads (cudaOccupancyMaxActiveBlocksPer-
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
-    kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kKernelCount
+    kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
+    kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
+template <typename Real>
+inline size_t yee_smem_bytes() { return sizeof(YeeStage<Real>) * YeeDepth<Real>::stages + sizeof(YeeHp<Real>); }
 template <typename Real>
 inline size_t hall_smem_bytes() { return sizeof(HallStage<Real>) * HallDepth<Real>::stages; }
 
@@ -59,6 +62,7 @@ template <typename Real> cudaError_t launch_hall(const HallArgs<Real>& a, cudaSt
 template <typename Real> cudaError_t launch_hall_measure(const HallMeasureArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_h(const YeeHArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_e(const YeeEArgs<Real>& a, cudaStream_t s);
+template <typename Real> cudaError_t launch_yee_step(const YeeStepArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_measure(const YeeHArgs<Real>& a, double* out2, cudaStream_t s);
 
 // Element-wise conversions between the caller's f64 arrays and an f32 store.

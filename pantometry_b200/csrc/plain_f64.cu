@@ -62,6 +62,16 @@ cudaError_t launch_yee_e<double>(const YeeEArgs<double>& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 template <>
+cudaError_t launch_yee_step<double>(const YeeStepArgs<double>& a, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(yee_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
+        attr = true;
+    }
+    yee_step<double><<<a.nblocks, tile_block(), yee_smem_bytes<double>(), s>>>(a);
+    return cudaGetLastError();
+}
+template <>
 cudaError_t launch_yee_measure<double>(const YeeHArgs<double>& a, double* out2, cudaStream_t s) {
     yee_measure<double><<<a.nblocks, tile_block(), 0, s>>>(a, out2);
     return cudaGetLastError();
@@ -79,6 +89,10 @@ int occupancy_f64(KernelId id) {
             break;
         case kYeeHF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<double>, 256, 0); break;
         case kYeeEF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<double>, 256, 0); break;
+        case kYeeStepF64:
+            cudaFuncSetAttribute(yee_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double>, 256, yee_smem_bytes<double>());
+            break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -296,6 +296,452 @@ static __global__ void __launch_bounds__(256) yee_e(YeeEArgs<Real> a) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The fused step. One pass per step over ping-pong copies of E and H: H⁺ from Eⁿ, the invariant
+// ½ε|Eⁿ|² + ½μ H⁻·H⁺, then Eⁿ⁺¹ from H⁺ — the reference's order inside `Cavity::step`
+// (cavity.rs:1490-1500), with nothing written in place.
+//
+// Block b walks tiles b, b + G, ... of the (nx+1) × (ny+1) lattice (32 × 8 columns over a
+// z-chunk), streaming planes k0 − 1 .. k1 through a ring of kYeeStages shared-memory stages with
+// cp.async. A stage holds one plane of all six old components over the tile and a one-cell halo
+// (289 halo values, at most two per thread). Per plane:
+//   1. H⁺ on the tile's own faces and on the halo faces its edges need (the x0 − 1 column and
+//      the y0 − 1 row — a neighbouring block computes those too, from the same old values, and
+//      gets the same bits), into shared memory; the tile's own H⁺ to the new buffer; the
+//      invariant's terms for the tile's own edges and faces.
+//   2. one barrier, then Eⁿ⁺¹ on the tile's own edges: interior edges by the semi-implicit
+//      update (cavity.rs:1383-1452), conducting walls 0, edges touching a solid cell 0. H⁺ of the
+//      plane below comes from registers carried up the column (at a tile's first plane, from
+//      the extra plane k0 − 1 the tile streams first).
+// ---------------------------------------------------------------------------------------------
+constexpr int kYeeHalo = 289;
+
+template <typename Real> struct YeeDepth;
+template <> struct YeeDepth<float> { static constexpr int stages = 6, min_blocks = 2; };
+template <> struct YeeDepth<double> { static constexpr int stages = 3, min_blocks = 2; };
+
+template <typename Real>
+struct YeeStage {
+    Real ex[10][33];  // lattice (x0-1 .. x0+31, y0-1 .. y0+8)
+    Real ey[9][34];   // (x0-1 .. x0+32, y0-1 .. y0+7)
+    Real ez[10][34];  // (x0-1 .. x0+32, y0-1 .. y0+8)
+    Real hx[9][32];   // (x0 .. x0+31, y0-1 .. y0+7)
+    Real hy[8][33];   // (x0-1 .. x0+31, y0 .. y0+7)
+    Real hz[9][33];   // (x0-1 .. x0+31, y0-1 .. y0+7)
+};
+
+template <typename Real>
+struct YeeHp {        // H⁺ of the present plane over the tile and its halo
+    Real hx[9][32];
+    Real hy[8][33];
+    Real hz[9][33];
+};
+
+template <typename Real>
+struct YeeStepArgs {
+    const Real* old[6];  // ex ey ez hx hy hz at step n (H at n − ½)
+    Real* neu[6];        // at n + 1 (H at n + ½)
+    unsigned pstride[6]; // elements per plane of each component
+    int nx, ny, nz;
+    double g;            // dt / dx
+    int uniform;
+    Real ch;             // uniform: g / μ
+    const double* __restrict__ mu0;
+    const double* __restrict__ mu1;
+    const double* __restrict__ mu2;
+    double mu_u, eps_u;
+    double dt, dx, volume;
+    Real decay[3], gain[3];
+    double sigma_u[3];
+    const double* __restrict__ eps0;
+    const double* __restrict__ eps1;
+    const double* __restrict__ eps2;
+    const double* __restrict__ sig0;
+    const double* __restrict__ sig1;
+    const double* __restrict__ sig2;
+    const uint8_t* __restrict__ solid;
+    int src_i, src_j, src_k;  // the Ez edge with a soft current (extension); src_i < 0: none
+    const double* __restrict__ current;
+    long long ncurrent;
+    double eps_src, sig_src;
+    Tiles tiles;              // over the (nx+1) × (ny+1) × (nz+1) lattice
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+// Halo value e (0 .. 288) of a stage: component, row, column.
+__device__ __forceinline__ void yee_halo_elem(int e, int& q, int& r, int& c) {
+    // ex [10][33]: column 0 (10), rows 0 and 9 of columns 1..32 (64)
+    if (e < 74) { q = 0; if (e < 10) { r = e; c = 0; } else { e -= 10; r = e < 32 ? 0 : 9; c = 1 + (e & 31); } return; }
+    e -= 74;
+    // ey [9][34]: columns 0 and 33 (18), row 0 of columns 1..32 (32)
+    if (e < 50) { q = 1; if (e < 18) { r = e % 9; c = e < 9 ? 0 : 33; } else { r = 0; c = 1 + (e - 18); } return; }
+    e -= 50;
+    // ez [10][34]: columns 0 and 33 (20), rows 0 and 9 of columns 1..32 (64)
+    if (e < 84) { q = 2; if (e < 20) { r = e % 10; c = e < 10 ? 0 : 33; } else { e -= 20; r = e < 32 ? 0 : 9; c = 1 + (e & 31); } return; }
+    e -= 84;
+    // hx [9][32]: row 0 (32)
+    if (e < 32) { q = 3; r = 0; c = e; return; }
+    e -= 32;
+    // hy [8][33]: column 0 (8)
+    if (e < 8) { q = 4; r = e; c = 0; return; }
+    e -= 8;
+    // hz [9][33]: column 0 (9), row 0 of columns 1..32 (32)
+    q = 5;
+    if (e < 9) { r = e; c = 0; } else { r = 0; c = 1 + (e - 9); }
+}
+
+// Lattice origin (column 0, row 0) of each component's stage array relative to (x0, y0), and
+// its row width; the component's own extents.
+__device__ __forceinline__ void yee_geom(int q, int nx, int ny, int nz, int& ox, int& oy, int& W, int& ext_x, int& ext_y,
+                                         int& ext_z) {
+    switch (q) {
+        case 0: ox = -1; oy = -1; W = 33; ext_x = nx; ext_y = ny + 1; ext_z = nz + 1; break;
+        case 1: ox = -1; oy = -1; W = 34; ext_x = nx + 1; ext_y = ny; ext_z = nz + 1; break;
+        case 2: ox = -1; oy = -1; W = 34; ext_x = nx + 1; ext_y = ny + 1; ext_z = nz; break;
+        case 3: ox = 0; oy = -1; W = 32; ext_x = nx + 1; ext_y = ny; ext_z = nz; break;
+        case 4: ox = -1; oy = 0; W = 33; ext_x = nx; ext_y = ny + 1; ext_z = nz; break;
+        default: ox = -1; oy = -1; W = 33; ext_x = nx; ext_y = ny; ext_z = nz + 1; break;
+    }
+}
+
+__device__ __forceinline__ unsigned yee_stage_offset(int q, int r, int c, unsigned esize) {
+    // element offsets of the six arrays inside YeeStage, in order
+    const unsigned start[6] = {0u, 330u, 330u + 306u, 330u + 306u + 340u, 330u + 306u + 340u + 288u,
+                               330u + 306u + 340u + 288u + 264u};
+    const unsigned W[6] = {33u, 34u, 34u, 32u, 33u, 33u};
+    return (start[q] + (unsigned)r * W[q] + (unsigned)c) * esize;
+}
+
+struct YeeWalk {
+    unsigned t;
+    int x0, y0, k0, k1, k, first, last;
+    bool valid;
+};
+
+__device__ __forceinline__ void yee_walk_at(YeeWalk& w, const Tiles& T, unsigned t, int nz) {
+    w.t = t;
+    w.valid = t < (unsigned)T.ntiles;
+    if (!w.valid) return;
+    const unsigned r = t / (unsigned)T.ntx;
+    const unsigned tz = r / (unsigned)T.nty;
+    w.x0 = (int)(t - r * (unsigned)T.ntx) * 32;
+    w.y0 = (int)(r - tz * (unsigned)T.nty) * 8;
+    w.k0 = (int)tz * T.zc;
+    w.k1 = min(T.nz, w.k0 + T.zc);  // T.nz = nz + 1 lattice planes
+    w.first = w.k0 > 0 ? w.k0 - 1 : 0;
+    w.last = min(w.k1, nz);
+    w.k = w.first;
+}
+__device__ __forceinline__ void yee_walk_next(YeeWalk& w, const Tiles& T, int nz) {
+    if (++w.k > w.last) yee_walk_at(w, T, w.t + gridDim.x, nz);
+}
+
+// Per-tile copy state of one thread: its own lattice position's six offsets at the tile's first
+// streamed plane and their validity, and its (up to two) halo values'.
+struct YeeCopy {
+    unsigned own[6];
+    unsigned hoff[2];
+    unsigned ownmask, hmask;  // bit q: own value q exists (in x, y); bit h: halo value h exists
+};
+
+template <typename Real>
+__device__ __forceinline__ YeeCopy yee_copy_at(const YeeStepArgs<Real>& a, const YeeWalk& w, const int (&hq)[2],
+                                               const int (&hr)[2], const int (&hc)[2]) {
+    YeeCopy o;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    o.ownmask = 0;
+    for (int q = 0; q < 6; ++q) {
+        int ox, oy, W, ex, ey, ez;
+        yee_geom(q, nx, ny, nz, ox, oy, W, ex, ey, ez);
+        const int i = w.x0 + tx, j = w.y0 + ty;
+        if (i < ex && j < ey) o.ownmask |= 1u << q;
+        o.own[q] = (unsigned)(i < ex ? i : 0) + (unsigned)ex * ((unsigned)(j < ey ? j : 0) + (unsigned)ey * (unsigned)w.k);
+    }
+    o.hmask = 0;
+    for (int h = 0; h < 2; ++h) {
+        o.hoff[h] = 0;
+        if (hq[h] < 0) continue;
+        int ox, oy, W, ex, ey, ez;
+        yee_geom(hq[h], nx, ny, nz, ox, oy, W, ex, ey, ez);
+        const int gi = w.x0 + ox + hc[h], gj = w.y0 + oy + hr[h];
+        if (gi >= 0 && gi < ex && gj >= 0 && gj < ey) {
+            o.hmask |= 1u << h;
+            o.hoff[h] = (unsigned)gi + (unsigned)ex * ((unsigned)gj + (unsigned)ey * (unsigned)w.k);
+        }
+    }
+    return o;
+}
+
+template <typename Real>
+__device__ __forceinline__ void yee_copy_next(YeeCopy& o, const YeeStepArgs<Real>& a, const int (&hq)[2]) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o.own[q] += a.pstride[q];
+    if (hq[0] >= 0) o.hoff[0] += a.pstride[hq[0]];
+    if (hq[1] >= 0) o.hoff[1] += a.pstride[hq[1]];
+}
+
+// Queue the copies of plane w.k into the stage at shared address `base`.
+template <typename Real>
+__device__ __forceinline__ void yee_stage(unsigned base, const YeeStepArgs<Real>& a, const YeeWalk& w, const YeeCopy& o,
+                                          const int (&hq)[2], const unsigned (&hs)[2]) {
+    constexpr int B = sizeof(Real);
+    const int tx = threadIdx.x, ty = threadIdx.y, nz = a.nz, k = w.k;
+    const YeeStage<Real>* z = nullptr;
+    auto at = [&](const Real* q) { return base + (unsigned)((const char*)q - (const char*)z); };
+    const bool zin = k < nz;  // components with nz planes (ez, hx, hy) exist at this plane
+    cp_async_if<B>(at(&z->ex[ty + 1][tx + 1]), a.old[0] + o.own[0], (o.ownmask >> 0) & 1);
+    cp_async_if<B>(at(&z->ey[ty + 1][tx + 1]), a.old[1] + o.own[1], (o.ownmask >> 1) & 1);
+    cp_async_if<B>(at(&z->ez[ty + 1][tx + 1]), a.old[2] + o.own[2], ((o.ownmask >> 2) & 1) && zin);
+    cp_async_if<B>(at(&z->hx[ty + 1][tx]), a.old[3] + o.own[3], ((o.ownmask >> 3) & 1) && zin);
+    cp_async_if<B>(at(&z->hy[ty][tx + 1]), a.old[4] + o.own[4], ((o.ownmask >> 4) & 1) && zin);
+    cp_async_if<B>(at(&z->hz[ty + 1][tx + 1]), a.old[5] + o.own[5], (o.ownmask >> 5) & 1);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        if (hq[h] < 0) continue;
+        const bool planar = hq[h] == 0 || hq[h] == 1 || hq[h] == 5;  // nz + 1 planes
+        cp_async_if<B>(base + hs[h], a.old[hq[h]] + o.hoff[h], ((o.hmask >> h) & 1) && (planar || zin));
+    }
+}
+
+template <typename Real>
+static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_step(YeeStepArgs<Real> a) {
+    DevState* st = a.st;
+    if (st->violated) return;
+    constexpr int S = YeeDepth<Real>::stages;
+    constexpr unsigned STAGE = sizeof(YeeStage<Real>);
+    extern __shared__ __align__(16) unsigned char yee_smem[];
+    const YeeStage<Real>* ring = reinterpret_cast<const YeeStage<Real>*>(yee_smem);
+    YeeHp<Real>* hp = reinterpret_cast<YeeHp<Real>*>(yee_smem + S * STAGE);
+    const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(yee_smem));
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
+    const Tiles T = a.tiles;
+    const long long step = st->steps;
+    const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
+    const double dt = a.dt;
+    // acc: Σ wεEx², Σ wεEy², Σ wεEz², Σ wμHx⁺Hx⁻, Σ wμHy⁺Hy⁻, Σ wμHz⁺Hz⁻, Joule loss, source work
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+
+    int hq[2], hr[2], hc[2];
+    unsigned hs[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int e = tid + 256 * h;
+        hq[h] = -1; hr[h] = 0; hc[h] = 0; hs[h] = 0;
+        if (e < kYeeHalo) {
+            yee_halo_elem(e, hq[h], hr[h], hc[h]);
+            hs[h] = yee_stage_offset(hq[h], hr[h], hc[h], sizeof(Real));
+        }
+    }
+
+    YeeWalk pf, cw;
+    yee_walk_at(pf, T, blockIdx.x, nz);
+    yee_walk_at(cw, T, blockIdx.x, nz);
+    YeeCopy po = yee_copy_at<Real>(a, pf, hq, hr, hc);
+    for (int d = 0; d < S - 1; ++d) {
+        if (pf.valid) yee_stage<Real>(ring_base + d * STAGE, a, pf, po, hq, hs);
+        cp_async_commit();
+        const unsigned t = pf.t;
+        yee_walk_next(pf, T, nz);
+        if (pf.t != t) po = yee_copy_at<Real>(a, pf, hq, hr, hc);
+        else yee_copy_next<Real>(po, a, hq);
+    }
+    Real hx_below = Real(0), hy_below = Real(0);  // H⁺ of this column at the plane below
+    unsigned own_h[6];                            // this thread's offsets at the computed plane
+    {
+        YeeCopy co = yee_copy_at<Real>(a, cw, hq, hr, hc);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) own_h[q] = co.own[q];
+    }
+    int slot = 0;
+    while (cw.valid) {
+        cp_async_wait<S - 2>();  // this thread's copies of this plane and the next have landed
+        __syncthreads();         // ... and everyone's; and everyone is done with the oldest stage and H⁺
+        {
+            const int fill = slot == 0 ? S - 1 : slot - 1;
+            if (pf.valid) yee_stage<Real>(ring_base + fill * STAGE, a, pf, po, hq, hs);
+            cp_async_commit();
+            const unsigned t = pf.t;
+            yee_walk_next(pf, T, nz);
+            if (pf.t != t) po = yee_copy_at<Real>(a, pf, hq, hr, hc);
+            else yee_copy_next<Real>(po, a, hq);
+        }
+        const YeeStage<Real>& S0 = ring[slot];
+        const YeeStage<Real>& S1 = ring[slot + 1 == S ? 0 : slot + 1];
+        const int k = cw.k;
+        const int i = cw.x0 + tx, j = cw.y0 + ty;
+        const bool compute = k >= cw.k0 && k < cw.k1;  // else the extra plane below or above the chunk
+        const bool zin = k < nz;
+        const bool in_x = i <= nx, in_y = j <= ny;
+        // ---- 1. H⁺ (cavity.rs:1346-1379) on own faces, into shared memory and the new buffer
+        Real hxn = Real(0), hyn = Real(0), hzn = Real(0);
+        {
+            double mux = a.mu_u, muy = a.mu_u, muz = a.mu_u;
+            Real cx = a.ch, cy = a.ch, cz = a.ch;
+            const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
+            if (!a.uniform) {
+                if (fx) { mux = a.mu0[own_h[3]]; cx = (Real)(a.g / mux); }
+                if (fy) { muy = a.mu1[own_h[4]]; cy = (Real)(a.g / muy); }
+                if (fz) { muz = a.mu2[own_h[5]]; cz = (Real)(a.g / muz); }
+            }
+            const Real wx = S0.hx[ty + 1][tx], wy = S0.hy[ty][tx + 1], wz = S0.hz[ty + 1][tx + 1];
+            const Real curlx = (S0.ez[ty + 2][tx + 1] - S0.ez[ty + 1][tx + 1]) - (S1.ey[ty + 1][tx + 1] - S0.ey[ty + 1][tx + 1]);
+            const Real curly = (S1.ex[ty + 1][tx + 1] - S0.ex[ty + 1][tx + 1]) - (S0.ez[ty + 1][tx + 2] - S0.ez[ty + 1][tx + 1]);
+            const Real curlz = (S0.ey[ty + 1][tx + 2] - S0.ey[ty + 1][tx + 1]) - (S0.ex[ty + 2][tx + 1] - S0.ex[ty + 1][tx + 1]);
+            hxn = wx - cx * curlx;
+            hyn = wy - cy * curly;
+            hzn = wz - cz * curlz;
+            if (compute) {
+                if (fx) {
+                    a.neu[3][own_h[3]] = hxn;
+                    acc[3] += ((i == 0 || i == nx) ? 0.5 : 1.0) * mux * (double)hxn * (double)wx;
+                }
+                if (fy) {
+                    a.neu[4][own_h[4]] = hyn;
+                    acc[4] += ((j == 0 || j == ny) ? 0.5 : 1.0) * muy * (double)hyn * (double)wy;
+                }
+                if (fz) {
+                    a.neu[5][own_h[5]] = hzn;
+                    acc[5] += ((k == 0 || k == nz) ? 0.5 : 1.0) * muz * (double)hzn * (double)wz;
+                }
+                // ½εEⁿ² on own edges (cavity.rs:776-847)
+                if (i < nx && in_y) {
+                    const double e = a.uniform ? a.eps_u : a.eps0[own_h[0]];
+                    const double f = (double)S0.ex[ty + 1][tx + 1];
+                    acc[0] += ((j == 0 || j == ny) ? 0.5 : 1.0) * ((k == 0 || k == nz) ? 0.5 : 1.0) * e * f * f;
+                }
+                if (in_x && j < ny) {
+                    const double e = a.uniform ? a.eps_u : a.eps1[own_h[1]];
+                    const double f = (double)S0.ey[ty + 1][tx + 1];
+                    acc[1] += ((i == 0 || i == nx) ? 0.5 : 1.0) * ((k == 0 || k == nz) ? 0.5 : 1.0) * e * f * f;
+                }
+                if (in_x && in_y && zin) {
+                    const double e = a.uniform ? a.eps_u : a.eps2[own_h[2]];
+                    const double f = (double)S0.ez[ty + 1][tx + 1];
+                    acc[2] += ((i == 0 || i == nx) ? 0.5 : 1.0) * ((j == 0 || j == ny) ? 0.5 : 1.0) * e * f * f;
+                }
+            }
+            hp->hx[ty + 1][tx] = hxn;
+            hp->hy[ty][tx + 1] = hyn;
+            hp->hz[ty + 1][tx + 1] = hzn;
+        }
+        // halo faces: the y0 − 1 row (hx, hz) by warp 7, the x0 − 1 column (hy, hz) by warp 6
+        if (compute && ty == 7) {
+            const int ii = cw.x0 + tx, jj = cw.y0 - 1;
+            Real c = a.ch;
+            if (!a.uniform && jj >= 0 && ii <= nx && zin) c = (Real)(a.g / a.mu0[(unsigned)ii + (unsigned)(nx + 1) * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+            hp->hx[0][tx] = S0.hx[0][tx] - c * ((S0.ez[1][tx + 1] - S0.ez[0][tx + 1]) - (S1.ey[0][tx + 1] - S0.ey[0][tx + 1]));
+            c = a.ch;
+            if (!a.uniform && jj >= 0 && ii < nx) c = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+            hp->hz[0][tx + 1] = S0.hz[0][tx + 1] - c * ((S0.ey[0][tx + 2] - S0.ey[0][tx + 1]) - (S0.ex[1][tx + 1] - S0.ex[0][tx + 1]));
+        }
+        if (compute && ty == 6 && tx < 9) {
+            // column x0 − 1, rows y0 − 1 .. y0 + 7 (row index r = tx)
+            const int r = tx, ii = cw.x0 - 1, jj = cw.y0 - 1 + r;
+            if (r >= 1) {
+                Real c = a.ch;
+                if (!a.uniform && ii >= 0 && jj <= ny && zin) c = (Real)(a.g / a.mu1[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)]);
+                hp->hy[r - 1][0] = S0.hy[r - 1][0] - c * ((S1.ex[r][0] - S0.ex[r][0]) - (S0.ez[r][1] - S0.ez[r][0]));
+            }
+            Real c = a.ch;
+            if (!a.uniform && ii >= 0 && jj >= 0 && jj < ny) c = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+            hp->hz[r][0] = S0.hz[r][0] - c * ((S0.ey[r][1] - S0.ey[r][0]) - (S0.ex[r + 1][0] - S0.ex[r][0]));
+        }
+        __syncthreads();
+        // ---- 2. Eⁿ⁺¹ on own edges (cavity.rs:1383-1452), walls (1239-1293), solids (304-331)
+        if (compute) {
+            if (i < nx && in_y) {  // ex
+                Real v = Real(0);
+                if (j >= 1 && j < ny && k >= 1 && k < nz) {
+                    const Real curl = (hp->hz[ty + 1][tx + 1] - hp->hz[ty][tx + 1]) - (hyn - hy_below);
+                    Real decay = a.decay[0], gain = a.gain[0];
+                    double s = a.sigma_u[0];
+                    if (!a.uniform) { s = a.sig0[own_h[0]]; coefficients<Real>(a.eps0[own_h[0]], s, dt, a.dx, decay, gain); }
+                    const Real before = S0.ex[ty + 1][tx + 1];
+                    v = decay * before + gain * curl;
+                    const double mid = 0.5 * ((double)before + (double)v);
+                    acc[6] += s * mid * mid * dt * a.volume;
+                }
+                if (a.solid && touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) v = Real(0);
+                a.neu[0][own_h[0]] = v;
+            }
+            if (in_x && j < ny) {  // ey
+                Real v = Real(0);
+                if (i >= 1 && i < nx && k >= 1 && k < nz) {
+                    const Real curl = (hxn - hx_below) - (hp->hz[ty + 1][tx + 1] - hp->hz[ty + 1][tx]);
+                    Real decay = a.decay[1], gain = a.gain[1];
+                    double s = a.sigma_u[1];
+                    if (!a.uniform) { s = a.sig1[own_h[1]]; coefficients<Real>(a.eps1[own_h[1]], s, dt, a.dx, decay, gain); }
+                    const Real before = S0.ey[ty + 1][tx + 1];
+                    v = decay * before + gain * curl;
+                    const double mid = 0.5 * ((double)before + (double)v);
+                    acc[6] += s * mid * mid * dt * a.volume;
+                }
+                if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) v = Real(0);
+                a.neu[1][own_h[1]] = v;
+            }
+            if (in_x && in_y && zin) {  // ez
+                Real v = Real(0);
+                if (i >= 1 && i < nx && j >= 1 && j < ny) {
+                    const Real curl = (hyn - hp->hy[ty][tx]) - (hxn - hp->hx[ty][tx]);
+                    Real decay = a.decay[2], gain = a.gain[2];
+                    double s = a.sigma_u[2];
+                    if (!a.uniform) { s = a.sig2[own_h[2]]; coefficients<Real>(a.eps2[own_h[2]], s, dt, a.dx, decay, gain); }
+                    const Real before = S0.ez[ty + 1][tx + 1];
+                    v = decay * before + gain * curl;
+                    if (i == a.src_i && j == a.src_j && k == a.src_k) {
+                        // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
+                        const double e = a.eps_src, ss = a.sig_src;
+                        v = (Real)((double)v - (dt / e) / (1.0 + (ss * dt / (2.0 * e))) * jsrc);
+                        acc[7] += -(dt * a.volume) * jsrc * (0.5 * ((double)before + (double)v));
+                    }
+                    const double mid = 0.5 * ((double)before + (double)v);
+                    acc[6] += s * mid * mid * dt * a.volume;
+                }
+                if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) v = Real(0);
+                a.neu[2][own_h[2]] = v;
+            }
+        }
+        hx_below = hxn;
+        hy_below = hyn;
+        {
+            const unsigned t = cw.t;
+            yee_walk_next(cw, T, nz);
+            if (cw.t != t) {
+                YeeCopy co = yee_copy_at<Real>(a, cw, hq, hr, hc);
+#pragma unroll
+                for (int q = 0; q < 6; ++q) own_h[q] = co.own[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 6; ++q) own_h[q] += a.pstride[q];
+            }
+        }
+        slot = slot + 1 == S ? 0 : slot + 1;
+    }
+    cp_async_wait<0>();
+    if (finish_blocks<8>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
+        const double v = a.volume;
+        const double electric = 0.5 * ((acc[0] + acc[1]) + acc[2]) * v;   // cavity.rs:846
+        const double paired = 0.5 * v * ((acc[3] + acc[4]) + acc[5]);      // cavity.rs:885-904
+        st->invariant = electric + paired;
+        st->has_invariant = 1;
+        st->dissipated += fmax(acc[6], 0.0);
+        st->work_booked = st->work;
+        st->work += acc[7];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, st->invariant);
+        ledger_add(total, scale, st->dissipated);
+        if (a.src_i >= 0) ledger_add(total, scale, -st->work_booked);
+        st->part[0] = st->invariant;
+        st->part[1] = st->dissipated;
+        st->part[2] = -st->work_booked;
+        audit_and_commit(st, total, scale);
+    }
+}
+
 // ½εE² and ½μH² of the present state (cavity.rs:824-847, 919-940): the naive energy the
 // ledger reports before any invariant exists, and what pm_cavity_energies returns.
 template <typename Real>
