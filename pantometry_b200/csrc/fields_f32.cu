@@ -4,7 +4,7 @@
 namespace pm {
 
 cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s) {
-    heat_f32_step<<<a.nblocks, tile_block(), sizeof(HeatStage) * kHeatStages, s>>>(a);
+    heat_f32_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -45,11 +45,21 @@ cudaError_t launch_yee_e<float>(const YeeEArgs<float>& a, cudaStream_t s) {
 template <>
 cudaError_t launch_yee_step<float>(const YeeStepArgs<float>& a, cudaStream_t s) {
     static bool attr = false;
+    const int smem = (int)yee_smem_bytes<float>();
     if (!attr) {
-        cudaFuncSetAttribute(yee_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
+        cudaFuncSetAttribute(yee_step<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_step<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_step<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_step<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    yee_step<float><<<a.nblocks, tile_block(), yee_smem_bytes<float>(), s>>>(a);
+    if (a.uniform) {
+        if (a.solid) yee_step<float, true, true><<<a.nblocks, tile_block(), smem, s>>>(a);
+        else yee_step<float, true, false><<<a.nblocks, tile_block(), smem, s>>>(a);
+    } else {
+        if (a.solid) yee_step<float, false, true><<<a.nblocks, tile_block(), smem, s>>>(a);
+        else yee_step<float, false, false><<<a.nblocks, tile_block(), smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 template <>
@@ -80,7 +90,7 @@ int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
     switch (id) {
-        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step, 256, sizeof(HeatStage) * kHeatStages); break;
+        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step, 256, 0); break;
         case kHallF32:
             cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<float, false>, 256, hall_smem_bytes<float>());
@@ -88,8 +98,8 @@ int occupancy_f32(KernelId id) {
         case kYeeHF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<float>, 256, 0); break;
         case kYeeEF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<float>, 256, 0); break;
         case kYeeStepF32:
-            cudaFuncSetAttribute(yee_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float>, 256, yee_smem_bytes<float>());
+            cudaFuncSetAttribute(yee_step<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
         default: return -1;
     }

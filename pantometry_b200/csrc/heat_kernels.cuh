@@ -197,138 +197,49 @@ struct HeatF32Args {
     unsigned nblocks;
 };
 
-// Chosen form. Block b walks tiles b, b + G, ... (32 × 8 columns over a z-chunk). For each tile
-// it streams the planes k0 − 1 .. k1 (the chunk plus the plane below and above it, where they
-// exist) through a ring of kHeatStages shared-memory stages with cp.async, each plane with a
-// one-cell halo in x and y, running ahead of the plane being computed and on across tile
-// boundaries; every thread copies its own cell plus at most one halo cell. The cell below comes
-// from a register, the rest from the stage; one barrier per plane.
-constexpr int kHeatStages = 16;
-
-struct HeatStage {
-    float d[10][34];  // deviations T − T0 of (x0-1 .. x0+32, y0-1 .. y0+8) at one plane
-};
-
-struct HeatWalk {
-    unsigned t;      // tile
-    int x0, y0, k0, k1;
-    int k;           // the plane this position streams
-    int first, last; // the tile's streamed planes: k0 - 1 (or k0) .. k1 (or k1 - 1)
-    bool valid;
-};
-
-__device__ __forceinline__ void heat_walk_at(HeatWalk& w, const Tiles& T, unsigned t) {
-    w.t = t;
-    w.valid = t < (unsigned)T.ntiles;
-    if (!w.valid) return;
-    const unsigned r = t / (unsigned)T.ntx;
-    const unsigned tz = r / (unsigned)T.nty;
-    w.x0 = (int)(t - r * (unsigned)T.ntx) * 32;
-    w.y0 = (int)(r - tz * (unsigned)T.nty) * 8;
-    w.k0 = (int)tz * T.zc;
-    w.k1 = min(T.nz, w.k0 + T.zc);
-    w.first = w.k0 > 0 ? w.k0 - 1 : w.k0;
-    w.last = w.k1 < T.nz ? w.k1 : w.k1 - 1;
-    w.k = w.first;
-}
-__device__ __forceinline__ void heat_walk_next(HeatWalk& w, const Tiles& T) {
-    if (++w.k > w.last) heat_walk_at(w, T, w.t + gridDim.x);
-}
-
-struct HeatHalo {
-    int r, c;  // row and column in the stage, r < 0: none
-};
-__device__ __forceinline__ HeatHalo heat_halo(int tid) {
-    if (tid < 34) return HeatHalo{0, tid};
-    if (tid < 68) return HeatHalo{9, tid - 34};
-    if (tid < 76) return HeatHalo{tid - 68 + 1, 0};
-    if (tid < 84) return HeatHalo{tid - 76 + 1, 33};
-    return HeatHalo{-1, 0};
-}
-
-__device__ __forceinline__ void heat_stage(unsigned base, const HeatF32Args& a, const HeatWalk& w, const HeatHalo& h) {
-    if (!w.valid) return;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int nx = a.nx, ny = a.ny;
-    const unsigned plane = (unsigned)nx * (unsigned)ny * (unsigned)w.k;
-    const int i = w.x0 + tx, j = w.y0 + ty;
-    const HeatStage* z = nullptr;
-    const unsigned own = base + (unsigned)((const char*)&z->d[ty + 1][tx + 1] - (const char*)z);
-    cp_async_if<4>(own, a.dold + plane + (unsigned)i + (unsigned)nx * (unsigned)j, i < nx && j < ny);
-    if (h.r >= 0) {
-        const int gi = w.x0 - 1 + h.c, gj = w.y0 - 1 + h.r;
-        const unsigned hs = base + (unsigned)((const char*)&z->d[h.r][h.c] - (const char*)z);
-        const bool in = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
-        cp_async_if<4>(hs, a.dold + plane + (unsigned)(in ? gi : 0) + (unsigned)nx * (unsigned)(in ? gj : 0), in);
-    }
-}
-
+// Chosen form, z-marching like the plain form; neighbours in the plane come from L1/L2.
 static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
     if (a.st->violated) return;
-    extern __shared__ __align__(16) unsigned char heat_smem[];
-    const HeatStage* ring = reinterpret_cast<const HeatStage*>(heat_smem);
-    const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(heat_smem));
-    constexpr int S = kHeatStages;
-    constexpr unsigned STAGE = sizeof(HeatStage);
     const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const Tiles T = a.tiles;
-    const HeatHalo halo = heat_halo(tx + 32 * ty);
+    const size_t plane = (size_t)nx * ny;
     double acc[2] = {0.0, 0.0};
-
-    HeatWalk pf, cw;
-    heat_walk_at(pf, T, blockIdx.x);
-    heat_walk_at(cw, T, blockIdx.x);
-    for (int d = 0; d < S - 1; ++d) {
-        heat_stage(ring_base + d * STAGE, a, pf, halo);
-        cp_async_commit();
-        heat_walk_next(pf, T);
-    }
-    float below = 0.0f;
-    int slot = 0;
-    while (cw.valid) {
-        cp_async_wait<S - 2>();  // this thread's copies of this plane and the next have landed
-        __syncthreads();         // ... and everyone's; and everyone is done with the oldest stage
-        {
-            const int fill = slot == 0 ? S - 1 : slot - 1;
-            heat_stage(ring_base + fill * STAGE, a, pf, halo);
-            cp_async_commit();
-            heat_walk_next(pf, T);
-        }
-        const int k = cw.k;
-        const int i = cw.x0 + tx, j = cw.y0 + ty;
-        const HeatStage& c = ring[slot];
-        const float here = c.d[ty + 1][tx + 1];
-        if (k >= cw.k0 && k < cw.k1 && i < nx && j < ny) {
-            const HeatStage& n = ring[slot + 1 == S ? 0 : slot + 1];
-            const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny, zl = k > 0, zh = k + 1 < nz;
-            const float above = n.d[ty + 1][tx + 1];
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        int i, j, k0, k1;
+        tile_column(a.tiles, t, i, j, k0, k1);
+        if (i >= nx || j >= ny) continue;
+        size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+        float below = k0 > 0 ? __ldg(a.dold + c - plane) : 0.0f;
+        float here = __ldg(a.dold + c);
+        const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
+        const bool edge_xy = !(xl && xh && yl && yh);
+        double col_shed = 0.0;
+        for (int k = k0; k < k1; ++k, c += plane) {
+            const float above = (k + 1 < nz) ? __ldg(a.dold + c + plane) : 0.0f;
             float s = 0.0f;
-            s += xl ? c.d[ty + 1][tx] - here : 0.0f;
-            s += xh ? c.d[ty + 1][tx + 2] - here : 0.0f;
-            s += yl ? c.d[ty][tx + 1] - here : 0.0f;
-            s += yh ? c.d[ty + 2][tx + 1] - here : 0.0f;
-            s += zl ? below - here : 0.0f;
-            s += zh ? above - here : 0.0f;
+            if (xl) s += __ldg(a.dold + c - 1) - here;
+            if (xh) s += __ldg(a.dold + c + 1) - here;
+            if (yl) s += __ldg(a.dold + c - nx) - here;
+            if (yh) s += __ldg(a.dold + c + nx) - here;
+            if (k > 0) s += below - here;
+            if (k + 1 < nz) s += above - here;
             float shed = 0.0f;
-            if (a.exposed && !(xl && xh && yl && yh && zl && zh)) {
+            if (a.exposed && (edge_xy || k == 0 || k + 1 == nz)) {
                 if (((a.exposed >> 0) & 1) && !xl) shed += a.b[0] * (here + a.off[0]);
                 if (((a.exposed >> 1) & 1) && !xh) shed += a.b[1] * (here + a.off[1]);
                 if (((a.exposed >> 2) & 1) && !yl) shed += a.b[2] * (here + a.off[2]);
                 if (((a.exposed >> 3) & 1) && !yh) shed += a.b[3] * (here + a.off[3]);
-                if (((a.exposed >> 4) & 1) && !zl) shed += a.b[4] * (here + a.off[4]);
-                if (((a.exposed >> 5) & 1) && !zh) shed += a.b[5] * (here + a.off[5]);
-                acc[1] += (double)shed;
+                if (((a.exposed >> 4) & 1) && k == 0) shed += a.b[4] * (here + a.off[4]);
+                if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += a.b[5] * (here + a.off[5]);
+                col_shed += (double)shed;
             }
             const float nd = here + (a.a * s - shed);
-            a.dnew[(unsigned)i + (unsigned)nx * ((unsigned)j + (unsigned)ny * (unsigned)k)] = nd;
+            a.dnew[c] = nd;
             acc[0] += (double)nd;
+            below = here;
+            here = above;
         }
-        below = here;
-        heat_walk_next(cw, T);
-        slot = slot + 1 == S ? 0 : slot + 1;
+        acc[1] += col_shed;
     }
-    cp_async_wait<0>();
     if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;
         const double stored = a.capacity * acc[0];

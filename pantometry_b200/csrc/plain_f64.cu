@@ -64,11 +64,21 @@ cudaError_t launch_yee_e<double>(const YeeEArgs<double>& a, cudaStream_t s) {
 template <>
 cudaError_t launch_yee_step<double>(const YeeStepArgs<double>& a, cudaStream_t s) {
     static bool attr = false;
+    const int smem = (int)yee_smem_bytes<double>();
     if (!attr) {
-        cudaFuncSetAttribute(yee_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
+        cudaFuncSetAttribute(yee_step<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_step<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_step<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_step<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    yee_step<double><<<a.nblocks, tile_block(), yee_smem_bytes<double>(), s>>>(a);
+    if (a.uniform) {
+        if (a.solid) yee_step<double, true, true><<<a.nblocks, tile_block(), smem, s>>>(a);
+        else yee_step<double, true, false><<<a.nblocks, tile_block(), smem, s>>>(a);
+    } else {
+        if (a.solid) yee_step<double, false, true><<<a.nblocks, tile_block(), smem, s>>>(a);
+        else yee_step<double, false, false><<<a.nblocks, tile_block(), smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 template <>
@@ -90,8 +100,8 @@ int occupancy_f64(KernelId id) {
         case kYeeHF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<double>, 256, 0); break;
         case kYeeEF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<double>, 256, 0); break;
         case kYeeStepF64:
-            cudaFuncSetAttribute(yee_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double>, 256, yee_smem_bytes<double>());
+            cudaFuncSetAttribute(yee_step<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double, false, true>, 256, yee_smem_bytes<double>());
             break;
         default: return -1;
     }

@@ -506,7 +506,8 @@ __device__ __forceinline__ void yee_stage(unsigned base, const YeeStepArgs<Real>
     }
 }
 
-template <typename Real>
+// UNIFORM: one medium everywhere (no media arrays read); SOLID: some cells are obstacles.
+template <typename Real, bool UNIFORM, bool SOLID>
 static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_step(YeeStepArgs<Real> a) {
     DevState* st = a.st;
     if (st->violated) return;
@@ -522,8 +523,9 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
     const long long step = st->steps;
     const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
     const double dt = a.dt;
-    // acc: Σ wεEx², Σ wεEy², Σ wεEz², Σ wμHx⁺Hx⁻, Σ wμHy⁺Hy⁻, Σ wμHz⁺Hz⁻, Joule loss, source work
-    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const bool lossy = !UNIFORM || a.sigma_u[0] != 0.0;
+    // Σ wεE², Σ wμH⁺H⁻ (each already weighted), Joule loss, source work
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
     int hq[2], hr[2], hc[2];
     unsigned hs[2];
@@ -556,6 +558,8 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
 #pragma unroll
         for (int q = 0; q < 6; ++q) own_h[q] = co.own[q];
     }
+    const Real ch = a.ch;
+    const Real dec0 = a.decay[0], gain0 = a.gain[0];
     int slot = 0;
     while (cw.valid) {
         cp_async_wait<S - 2>();  // this thread's copies of this plane and the next have landed
@@ -576,134 +580,114 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
         const bool compute = k >= cw.k0 && k < cw.k1;  // else the extra plane below or above the chunk
         const bool zin = k < nz;
         const bool in_x = i <= nx, in_y = j <= ny;
+        // node-centred half weights of the boundary samples (cavity.rs:766-772)
+        const double hi = (i == 0 || i == nx) ? 0.5 : 1.0, hj = (j == 0 || j == ny) ? 0.5 : 1.0,
+                     hk = (k == 0 || k == nz) ? 0.5 : 1.0;
         // ---- 1. H⁺ (cavity.rs:1346-1379) on own faces, into shared memory and the new buffer
-        Real hxn = Real(0), hyn = Real(0), hzn = Real(0);
-        {
-            double mux = a.mu_u, muy = a.mu_u, muz = a.mu_u;
-            Real cx = a.ch, cy = a.ch, cz = a.ch;
-            const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
-            if (!a.uniform) {
-                if (fx) { mux = a.mu0[own_h[3]]; cx = (Real)(a.g / mux); }
-                if (fy) { muy = a.mu1[own_h[4]]; cy = (Real)(a.g / muy); }
-                if (fz) { muz = a.mu2[own_h[5]]; cz = (Real)(a.g / muz); }
+        const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
+        const Real wx = S0.hx[ty + 1][tx], wy = S0.hy[ty][tx + 1], wz = S0.hz[ty + 1][tx + 1];
+        const Real ex0 = S0.ex[ty + 1][tx + 1], ey0 = S0.ey[ty + 1][tx + 1], ez0 = S0.ez[ty + 1][tx + 1];
+        Real cx = ch, cy = ch, cz = ch;
+        double mux = a.mu_u, muy = a.mu_u, muz = a.mu_u;
+        if constexpr (!UNIFORM) {
+            if (fx) { mux = a.mu0[own_h[3]]; cx = (Real)(a.g / mux); }
+            if (fy) { muy = a.mu1[own_h[4]]; cy = (Real)(a.g / muy); }
+            if (fz) { muz = a.mu2[own_h[5]]; cz = (Real)(a.g / muz); }
+        }
+        const Real hxn = wx - cx * ((S0.ez[ty + 2][tx + 1] - ez0) - (S1.ey[ty + 1][tx + 1] - ey0));
+        const Real hyn = wy - cy * ((S1.ex[ty + 1][tx + 1] - ex0) - (S0.ez[ty + 1][tx + 2] - ez0));
+        const Real hzn = wz - cz * ((S0.ey[ty + 1][tx + 2] - ey0) - (S0.ex[ty + 2][tx + 1] - ex0));
+        hp->hx[ty + 1][tx] = hxn;
+        hp->hy[ty][tx + 1] = hyn;
+        hp->hz[ty + 1][tx + 1] = hzn;
+        if (compute) {
+            if (fx) a.neu[3][own_h[3]] = hxn;
+            if (fy) a.neu[4][own_h[4]] = hyn;
+            if (fz) a.neu[5][own_h[5]] = hzn;
+            // ½μ H⁻·H⁺ (cavity.rs:854-905) and ½εEⁿ² (cavity.rs:776-847) on own faces and edges
+            double m = 0.0, e = 0.0;
+            m += fx ? hi * mux * (double)hxn * (double)wx : 0.0;
+            m += fy ? hj * muy * (double)hyn * (double)wy : 0.0;
+            m += fz ? hk * muz * (double)hzn * (double)wz : 0.0;
+            double epx = a.eps_u, epy = a.eps_u, epz = a.eps_u;
+            if constexpr (!UNIFORM) {
+                if (i < nx && in_y) epx = a.eps0[own_h[0]];
+                if (in_x && j < ny) epy = a.eps1[own_h[1]];
+                if (in_x && in_y && zin) epz = a.eps2[own_h[2]];
             }
-            const Real wx = S0.hx[ty + 1][tx], wy = S0.hy[ty][tx + 1], wz = S0.hz[ty + 1][tx + 1];
-            const Real curlx = (S0.ez[ty + 2][tx + 1] - S0.ez[ty + 1][tx + 1]) - (S1.ey[ty + 1][tx + 1] - S0.ey[ty + 1][tx + 1]);
-            const Real curly = (S1.ex[ty + 1][tx + 1] - S0.ex[ty + 1][tx + 1]) - (S0.ez[ty + 1][tx + 2] - S0.ez[ty + 1][tx + 1]);
-            const Real curlz = (S0.ey[ty + 1][tx + 2] - S0.ey[ty + 1][tx + 1]) - (S0.ex[ty + 2][tx + 1] - S0.ex[ty + 1][tx + 1]);
-            hxn = wx - cx * curlx;
-            hyn = wy - cy * curly;
-            hzn = wz - cz * curlz;
-            if (compute) {
-                if (fx) {
-                    a.neu[3][own_h[3]] = hxn;
-                    acc[3] += ((i == 0 || i == nx) ? 0.5 : 1.0) * mux * (double)hxn * (double)wx;
-                }
-                if (fy) {
-                    a.neu[4][own_h[4]] = hyn;
-                    acc[4] += ((j == 0 || j == ny) ? 0.5 : 1.0) * muy * (double)hyn * (double)wy;
-                }
-                if (fz) {
-                    a.neu[5][own_h[5]] = hzn;
-                    acc[5] += ((k == 0 || k == nz) ? 0.5 : 1.0) * muz * (double)hzn * (double)wz;
-                }
-                // ½εEⁿ² on own edges (cavity.rs:776-847)
-                if (i < nx && in_y) {
-                    const double e = a.uniform ? a.eps_u : a.eps0[own_h[0]];
-                    const double f = (double)S0.ex[ty + 1][tx + 1];
-                    acc[0] += ((j == 0 || j == ny) ? 0.5 : 1.0) * ((k == 0 || k == nz) ? 0.5 : 1.0) * e * f * f;
-                }
-                if (in_x && j < ny) {
-                    const double e = a.uniform ? a.eps_u : a.eps1[own_h[1]];
-                    const double f = (double)S0.ey[ty + 1][tx + 1];
-                    acc[1] += ((i == 0 || i == nx) ? 0.5 : 1.0) * ((k == 0 || k == nz) ? 0.5 : 1.0) * e * f * f;
-                }
-                if (in_x && in_y && zin) {
-                    const double e = a.uniform ? a.eps_u : a.eps2[own_h[2]];
-                    const double f = (double)S0.ez[ty + 1][tx + 1];
-                    acc[2] += ((i == 0 || i == nx) ? 0.5 : 1.0) * ((j == 0 || j == ny) ? 0.5 : 1.0) * e * f * f;
-                }
-            }
-            hp->hx[ty + 1][tx] = hxn;
-            hp->hy[ty][tx + 1] = hyn;
-            hp->hz[ty + 1][tx + 1] = hzn;
+            const double dex = (double)ex0, dey = (double)ey0, dez = (double)ez0;
+            e += (i < nx && in_y) ? hj * hk * epx * dex * dex : 0.0;
+            e += (in_x && j < ny) ? hi * hk * epy * dey * dey : 0.0;
+            e += (in_x && in_y && zin) ? hi * hj * epz * dez * dez : 0.0;
+            acc[0] += e;
+            acc[1] += m;
         }
         // halo faces: the y0 − 1 row (hx, hz) by warp 7, the x0 − 1 column (hy, hz) by warp 6
         if (compute && ty == 7) {
-            const int ii = cw.x0 + tx, jj = cw.y0 - 1;
-            Real c = a.ch;
-            if (!a.uniform && jj >= 0 && ii <= nx && zin) c = (Real)(a.g / a.mu0[(unsigned)ii + (unsigned)(nx + 1) * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
-            hp->hx[0][tx] = S0.hx[0][tx] - c * ((S0.ez[1][tx + 1] - S0.ez[0][tx + 1]) - (S1.ey[0][tx + 1] - S0.ey[0][tx + 1]));
-            c = a.ch;
-            if (!a.uniform && jj >= 0 && ii < nx) c = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
-            hp->hz[0][tx + 1] = S0.hz[0][tx + 1] - c * ((S0.ey[0][tx + 2] - S0.ey[0][tx + 1]) - (S0.ex[1][tx + 1] - S0.ex[0][tx + 1]));
+            Real c1 = ch, c2 = ch;
+            if constexpr (!UNIFORM) {
+                const int ii = cw.x0 + tx, jj = cw.y0 - 1;
+                if (jj >= 0 && ii <= nx && zin) c1 = (Real)(a.g / a.mu0[(unsigned)ii + (unsigned)(nx + 1) * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+                if (jj >= 0 && ii < nx) c2 = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+            }
+            hp->hx[0][tx] = S0.hx[0][tx] - c1 * ((S0.ez[1][tx + 1] - S0.ez[0][tx + 1]) - (S1.ey[0][tx + 1] - S0.ey[0][tx + 1]));
+            hp->hz[0][tx + 1] = S0.hz[0][tx + 1] - c2 * ((S0.ey[0][tx + 2] - S0.ey[0][tx + 1]) - (S0.ex[1][tx + 1] - S0.ex[0][tx + 1]));
         }
         if (compute && ty == 6 && tx < 9) {
             // column x0 − 1, rows y0 − 1 .. y0 + 7 (row index r = tx)
-            const int r = tx, ii = cw.x0 - 1, jj = cw.y0 - 1 + r;
-            if (r >= 1) {
-                Real c = a.ch;
-                if (!a.uniform && ii >= 0 && jj <= ny && zin) c = (Real)(a.g / a.mu1[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)]);
-                hp->hy[r - 1][0] = S0.hy[r - 1][0] - c * ((S1.ex[r][0] - S0.ex[r][0]) - (S0.ez[r][1] - S0.ez[r][0]));
+            const int r = tx;
+            Real c1 = ch, c2 = ch;
+            if constexpr (!UNIFORM) {
+                const int ii = cw.x0 - 1, jj = cw.y0 - 1 + r;
+                if (ii >= 0 && jj <= ny && zin) c1 = (Real)(a.g / a.mu1[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)]);
+                if (ii >= 0 && jj >= 0 && jj < ny) c2 = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
             }
-            Real c = a.ch;
-            if (!a.uniform && ii >= 0 && jj >= 0 && jj < ny) c = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
-            hp->hz[r][0] = S0.hz[r][0] - c * ((S0.ey[r][1] - S0.ey[r][0]) - (S0.ex[r + 1][0] - S0.ex[r][0]));
+            if (r >= 1) hp->hy[r - 1][0] = S0.hy[r - 1][0] - c1 * ((S1.ex[r][0] - S0.ex[r][0]) - (S0.ez[r][1] - S0.ez[r][0]));
+            hp->hz[r][0] = S0.hz[r][0] - c2 * ((S0.ey[r][1] - S0.ey[r][0]) - (S0.ex[r + 1][0] - S0.ex[r][0]));
         }
         __syncthreads();
-        // ---- 2. Eⁿ⁺¹ on own edges (cavity.rs:1383-1452), walls (1239-1293), solids (304-331)
+        // ---- 2. Eⁿ⁺¹ on own edges (cavity.rs:1383-1452): interior by the semi-implicit update,
+        // conducting walls 0 (cavity.rs:1239-1293), edges touching a solid cell 0 (cavity.rs:304-331)
         if (compute) {
-            if (i < nx && in_y) {  // ex
-                Real v = Real(0);
-                if (j >= 1 && j < ny && k >= 1 && k < nz) {
-                    const Real curl = (hp->hz[ty + 1][tx + 1] - hp->hz[ty][tx + 1]) - (hyn - hy_below);
-                    Real decay = a.decay[0], gain = a.gain[0];
-                    double s = a.sigma_u[0];
-                    if (!a.uniform) { s = a.sig0[own_h[0]]; coefficients<Real>(a.eps0[own_h[0]], s, dt, a.dx, decay, gain); }
-                    const Real before = S0.ex[ty + 1][tx + 1];
-                    v = decay * before + gain * curl;
-                    const double mid = 0.5 * ((double)before + (double)v);
-                    acc[6] += s * mid * mid * dt * a.volume;
-                }
-                if (a.solid && touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) v = Real(0);
-                a.neu[0][own_h[0]] = v;
+            const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
+            const Real cex = (hp->hz[ty + 1][tx + 1] - hp->hz[ty][tx + 1]) - (hyn - hy_below);
+            const Real cey = (hxn - hx_below) - (hp->hz[ty + 1][tx + 1] - hp->hz[ty + 1][tx]);
+            const Real cez = (hyn - hp->hy[ty][tx]) - (hxn - hp->hx[ty][tx]);
+            Real d0 = dec0, g0 = gain0, d1 = dec0, g1 = gain0, d2 = dec0, g2 = gain0;
+            double s0 = a.sigma_u[0], s1 = s0, s2 = s0;
+            if constexpr (!UNIFORM) {
+                if (i < nx && in_y && iy && iz) { s0 = a.sig0[own_h[0]]; coefficients<Real>(a.eps0[own_h[0]], s0, dt, a.dx, d0, g0); }
+                if (in_x && j < ny && ix && iz) { s1 = a.sig1[own_h[1]]; coefficients<Real>(a.eps1[own_h[1]], s1, dt, a.dx, d1, g1); }
+                if (in_x && in_y && zin && ix && iy) { s2 = a.sig2[own_h[2]]; coefficients<Real>(a.eps2[own_h[2]], s2, dt, a.dx, d2, g2); }
             }
-            if (in_x && j < ny) {  // ey
-                Real v = Real(0);
-                if (i >= 1 && i < nx && k >= 1 && k < nz) {
-                    const Real curl = (hxn - hx_below) - (hp->hz[ty + 1][tx + 1] - hp->hz[ty + 1][tx]);
-                    Real decay = a.decay[1], gain = a.gain[1];
-                    double s = a.sigma_u[1];
-                    if (!a.uniform) { s = a.sig1[own_h[1]]; coefficients<Real>(a.eps1[own_h[1]], s, dt, a.dx, decay, gain); }
-                    const Real before = S0.ey[ty + 1][tx + 1];
-                    v = decay * before + gain * curl;
-                    const double mid = 0.5 * ((double)before + (double)v);
-                    acc[6] += s * mid * mid * dt * a.volume;
-                }
-                if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) v = Real(0);
-                a.neu[1][own_h[1]] = v;
+            Real vx = d0 * ex0 + g0 * cex;
+            Real vy = d1 * ey0 + g1 * cey;
+            Real vz = d2 * ez0 + g2 * cez;
+            if (i == a.src_i && j == a.src_j && k == a.src_k) {
+                // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
+                const double e = a.eps_src, ss = a.sig_src;
+                vz = (Real)((double)vz - (dt / e) / (1.0 + (ss * dt / (2.0 * e))) * jsrc);
+                acc[3] += -(dt * a.volume) * jsrc * (0.5 * ((double)ez0 + (double)vz));
             }
-            if (in_x && in_y && zin) {  // ez
-                Real v = Real(0);
-                if (i >= 1 && i < nx && j >= 1 && j < ny) {
-                    const Real curl = (hyn - hp->hy[ty][tx]) - (hxn - hp->hx[ty][tx]);
-                    Real decay = a.decay[2], gain = a.gain[2];
-                    double s = a.sigma_u[2];
-                    if (!a.uniform) { s = a.sig2[own_h[2]]; coefficients<Real>(a.eps2[own_h[2]], s, dt, a.dx, decay, gain); }
-                    const Real before = S0.ez[ty + 1][tx + 1];
-                    v = decay * before + gain * curl;
-                    if (i == a.src_i && j == a.src_j && k == a.src_k) {
-                        // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
-                        const double e = a.eps_src, ss = a.sig_src;
-                        v = (Real)((double)v - (dt / e) / (1.0 + (ss * dt / (2.0 * e))) * jsrc);
-                        acc[7] += -(dt * a.volume) * jsrc * (0.5 * ((double)before + (double)v));
-                    }
-                    const double mid = 0.5 * ((double)before + (double)v);
-                    acc[6] += s * mid * mid * dt * a.volume;
-                }
-                if (a.solid && touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) v = Real(0);
-                a.neu[2][own_h[2]] = v;
+            const bool lx = iy && iz, ly = ix && iz, lz = ix && iy;  // interior edges
+            vx = lx ? vx : Real(0);
+            vy = ly ? vy : Real(0);
+            vz = lz ? vz : Real(0);
+            if (lossy) {
+                const double mx = 0.5 * ((double)ex0 + (double)vx), my = 0.5 * ((double)ey0 + (double)vy),
+                             mz = 0.5 * ((double)ez0 + (double)vz);
+                acc[2] += (lx && i < nx && in_y) ? s0 * mx * mx * dt * a.volume : 0.0;
+                acc[2] += (ly && in_x && j < ny) ? s1 * my * my * dt * a.volume : 0.0;
+                acc[2] += (lz && in_x && in_y && zin) ? s2 * mz * mz * dt * a.volume : 0.0;
             }
+            if constexpr (SOLID) {
+                if (touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) vx = Real(0);
+                if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) vy = Real(0);
+                if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) vz = Real(0);
+            }
+            if (i < nx && in_y) a.neu[0][own_h[0]] = vx;
+            if (in_x && j < ny) a.neu[1][own_h[1]] = vy;
+            if (in_x && in_y && zin) a.neu[2][own_h[2]] = vz;
         }
         hx_below = hxn;
         hy_below = hyn;
@@ -722,15 +706,15 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
         slot = slot + 1 == S ? 0 : slot + 1;
     }
     cp_async_wait<0>();
-    if (finish_blocks<8>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
+    if (finish_blocks<4>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
         const double v = a.volume;
-        const double electric = 0.5 * ((acc[0] + acc[1]) + acc[2]) * v;   // cavity.rs:846
-        const double paired = 0.5 * v * ((acc[3] + acc[4]) + acc[5]);      // cavity.rs:885-904
+        const double electric = 0.5 * acc[0] * v;   // cavity.rs:846
+        const double paired = 0.5 * v * acc[1];     // cavity.rs:885-904
         st->invariant = electric + paired;
         st->has_invariant = 1;
-        st->dissipated += fmax(acc[6], 0.0);
+        st->dissipated += fmax(acc[2], 0.0);
         st->work_booked = st->work;
-        st->work += acc[7];
+        st->work += acc[3];
         double total = 0.0, scale = 0.0;
         ledger_add(total, scale, st->invariant);
         ledger_add(total, scale, st->dissipated);
