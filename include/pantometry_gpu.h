@@ -219,6 +219,32 @@ pm_status pm_cavity_restore(pm_cavity* c);
 pm_status pm_cavity_set_stream(pm_cavity* c, void* stream);
 void pm_cavity_destroy(pm_cavity* c);
 
+/* ============================ Without allocation ==================================== */
+
+/* No counterpart in the reference. One Hall step (f32 fields, f64 invariant) on device buffers the
+ * caller owns, for callers that cannot allocate device memory themselves or through this library —
+ * a host that owns every device allocation through its own pool and forbids other allocators, a
+ * plugin running inside such a host, or code that must not trigger the device-wide
+ * synchronisation cudaMalloc and cudaFree can cause. The kernel is pm_hall_step's; its scratch (a
+ * state block and one FP64 partial sum per block) lives in a fixed 64 KiB device array of this
+ * library, which every GPU that loads the library holds until the process exits. Grids whose
+ * scratch would exceed it are refused with PM_BAD_ARG and a message. Nothing is allocated: no
+ * cudaMalloc, no cudaFree, no allocating library call.
+ *   Fields are in the reference's index order, nx*ny*nz nodes and (nx-1)*ny*nz, nx*(ny-1)*nz,
+ *   nx*ny*(nz-1) faces, as `Hall` lays them out (hall.rs:67-77); the old state is read from
+ *   p0/vx0/vy0/vz0 and the new one written to p1/vx1/vy1/vz1 (distinct buffers). first_step != 0
+ *   gives the velocities the half step the leapfrog opens with (hall.rs:427-430). *invariant
+ *   receives `invariant_si` of the new state (hall.rs:334-384); the startup offset and the audit
+ *   stay with the caller.
+ *   The first call on a device looks up the scratch array's device address (cudaGetSymbolAddress,
+ *   with that device current); make that first call before any stream capture. Every call shares
+ *   the array and leaves its contents behind; each call clears what must start at zero. Calls that
+ *   overlap on the GPU (other streams, other threads) race on the array: do not overlap them. */
+pm_status pm_hall_step_f32_noalloc(int nx, int ny, int nz, double dx, double speed, double density, double dt,
+                                   int first_step, const float* p0, const float* vx0, const float* vy0,
+                                   const float* vz0, float* p1, float* vx1, float* vy1, float* vz1, void* stream,
+                                   double* invariant);
+
 #ifdef __cplusplus
 }
 #endif

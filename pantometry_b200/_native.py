@@ -166,6 +166,8 @@ SIGNATURES = {
     "pm_cavity_restore": (_st, [_p]),
     "pm_cavity_set_stream": (_st, [_p, _p]),
     "pm_cavity_destroy": (None, [_p]),
+    # Without allocation
+    "pm_hall_step_f32_noalloc": (_st, [_i, _i, _i, _d, _d, _d, _d, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _dp]),
 }
 
 OPTIONAL_SIGNATURES = {
