@@ -37,9 +37,9 @@ METRIC = "Gcell-updates/s (acoustic hall 256^3, FP32 fields + FP64 audit)"
 UNIT = "Gcell-updates/s"
 BYTES_F32 = 32  # per node-update: p, vx, vy, vz, read and written once
 BYTES_F64 = 64
-# dram__bytes_read.sum + dram__bytes_write.sum of one hall_step<float> launch at 256³, from the
-# ncu capture summarised in profiles/hall_step_f32_256.md (None until captured).
-HALL_F32_TRAFFIC = None
+# dram__bytes_read.sum + dram__bytes_write.sum of one hall_step<float> launch at 256³ (277.8 MB
+# read + 222.9 MB written), from the ncu capture summarised in profiles/hall_step_f32_256.md.
+HALL_F32_TRAFFIC = 500773632
 
 
 def peaks():
