@@ -318,18 +318,261 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+ENS_METRIC = "Gcell-updates/s (heat ensemble, 512 uneven grids of 16..128 cells per axis, FP32 fields + FP64 audit)"
+
+
+def init_dist(local):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return dist
+
+
+def run_ensemble(args):
+    """Config 4: every grid its own `Solid3D` with Dirichlet 300 K films and dt at 0.9 of its own
+    limit; one bench step = `timesteps` steps of every grid (one persistent brick-list kernel
+    launch per timestep, graphs of 64), FP64 ledger and audit per grid every timestep."""
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import sharding
+    from pantometry_b200 import workloads as W
+    from pantometry_b200.domains import Ensemble
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = init_dist(local) if world > 1 else None
+    cfg = W.heat_ensemble(count=args.grids, steps=args.timesteps)
+    all_grids = W.ensemble_grids(cfg)
+    sizes = [int(np.prod(g["counts"])) for g in all_grids]
+    share = sharding.partition(sizes, world)[rank]
+    grids = [all_grids[g] for g in share]
+    cells = np.concatenate([W.ensemble_cells(cfg["grids"][g]) for g in share])
+    total_cells = sum(sizes)
+    T = args.timesteps
+    stream = torch.cuda.Stream(device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def build(precision):
+        e = Ensemble(grids, precision=precision, device=local)
+        e.set_stream(stream.cuda_stream)
+        e.upload(cells)
+        return e
+
+    def timed(e, k, w, tol):
+        e.set_tolerance(tol)
+        for _ in range(w):
+            v = e.step(T)
+            assert v is None, v
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            start.record(stream)
+            for _ in range(k):
+                v = e.step(T)
+                assert v is None, v
+            end.record(stream)
+            torch.cuda.synchronize()
+        ms = start.elapsed_time(end)
+        barrier()
+        return max_over_ranks(ms), clk
+
+    e32 = build("f32")
+    shape32 = e32.autotune(trial_steps=10)
+    ms32, clk = timed(e32, args.steps, args.warmup, 1e-6)
+    plain_steps = max(1, args.steps // 2)
+    e64 = build("f64")
+    shape64 = e64.autotune(trial_steps=5)
+    ms64, _ = timed(e64, plain_steps, max(1, args.warmup // 2), 1e-9)
+    # error of FP32 against the f64 form after one bench step from the same start
+    e32.upload(cells)
+    e64.upload(cells)
+    assert e32.step(T) is None and e64.step(T) is None
+    field_err = float(np.abs(e32.download() - e64.download()).max())
+    led32, led64 = e32.ledgers(), e64.ledgers()
+    ledger_err = max(abs(a["total"] - b["total"]) / max(abs(b["total"]), b["scale"], 1e-300) for a, b in zip(led32, led64))
+    del e64
+
+    # e2e through the C ABI with host buffers: upload from pinned memory, run, ledgers back
+    pinned = torch.empty(cells.size, dtype=torch.float64, pin_memory=True).numpy()
+    pinned[:] = cells
+    for _ in range(args.warmup):
+        e32.upload(pinned)
+        e32.step(T)
+    barrier()
+    t0 = time.perf_counter()
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        e32.upload(pinned)
+        v = e32.step(T)
+        assert v is None, v
+        ledgers = sharding.gather_ledgers(e32.ledgers(), share, len(all_grids), dist)
+    e0.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    e2e_ms = max_over_ranks(max(s0.elapsed_time(e0), wall_ms))
+    del e32
+    assert len(ledgers) == len(all_grids)
+
+    peak, peak_kind = peaks()
+    local_cells = int(cells.size)
+    per_launch_ms = ms32 / (args.steps * T)
+    achieved = 8 * local_cells / (per_launch_ms * 1e-3) / 1e9
+    value = total_cells * T * args.steps / (ms32 * 1e-3) / 1e9
+    plain = total_cells * T * plain_steps / (ms64 * 1e-3) / 1e9
+    line = {
+        "metric": ENS_METRIC,
+        "value": round(value, 3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms32 / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak" if world == 1 else "strong",
+        "vs_baseline": None,
+        "dtype": "f32 fields, f64 audit",
+        "data": "synthetic (seeded Rng::for_index sizes, diffusivities and hot spots)",
+        "config": {"workload": f"heat ensemble: {len(all_grids)} grids, 16..128 cells per axis, {total_cells} cells, "
+                               f"{T} timesteps per step, Dirichlet 300 K faces, dt 0.9 x each grid's limit, "
+                               "FP64 audit per grid every timestep",
+                   "grids": len(all_grids), "cells": total_cells, "timesteps_per_step": T,
+                   "parallelism": f"grids sharded over {world} rank(s)", "brick_f32": list(shape32),
+                   "brick_f64": list(shape64), "l2": f"state {8 * total_cells / 1e9:.2f} GB > 126 MB L2, no flush",
+                   "grids_per_s": round(len(all_grids) * args.steps / (ms32 * 1e-3), 3)},
+        "e2e": {"value": round(total_cells * T * args.steps / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                "h2d_bytes_per_step": local_cells * 8, "d2h_bytes_per_step": len(grids) * 56},
+        "gpu_launches": args.steps * T,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "kernel": "ens_step<float>",
+                     "bytes_per_launch": 8 * local_cells, "peak_source": f"{peak_kind} hbm_gbs"},
+        "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
+                      "roofline_frac": round(16 * local_cells / (ms64 / (plain_steps * T) * 1e-3) / 1e9 / peak, 4),
+                      "fp32_over_f64": round(value / plain, 3)},
+        "error_vs_f64": {"max_abs_kelvin": field_err, "ledger_rel_max_over_grids": ledger_err, "after_timesteps": T},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_ensemble(cfg, all_grids, sample_steps=args.cpu_sample_steps, threads=1,
+                                                     sample_grids=48)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline_ensemble(cfg, grids, sample_steps=2, threads=1, sample_grids=16):
+    """`Ensemble::run` over `Solid3D` samples, restated (the oracle): the first `sample_grids`
+    grids, each with its own audited `Simulation::advance` steps, `threads` grids at a time."""
+    import queue
+
+    import oracle
+    from pantometry_b200 import workloads as W
+
+    blocks = []
+    for g in range(min(sample_grids, len(grids))):
+        d = grids[g]
+        nx, ny, nz = d["counts"]
+        dx, s = d["dx"], d["substance"]
+        o = oracle.Heat((nx, ny, nz), dx, s["density"], s["conductivity"], s["specific_heat"], d["initial"])
+        areas = [(ny * dx) * (nz * dx)] * 2 + [(nx * dx) * (nz * dx)] * 2 + [(nx * dx) * (ny * dx)] * 2
+        for f in range(6):
+            o.losing_from(f, d["initial"], d["convection"], areas[f])
+        o.cells = W.ensemble_cells(cfg["grids"][g])
+        assert o.advance(d["dt"], 1) is None  # warm-up
+        blocks.append((o, d["dt"], nx * ny * nz))
+    work = queue.Queue()
+    for b in blocks:
+        work.put(b)
+
+    def worker():
+        while True:
+            try:
+                o, dt, _ = work.get_nowait()
+            except queue.Empty:
+                return
+            assert o.advance(dt, sample_steps) is None
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker) for _ in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    secs = time.perf_counter() - t0
+    ncells = sum(b[2] for b in blocks)
+    return {"value": round(ncells * sample_steps / secs / 1e9, 6), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(blocks)} grids ({ncells} cells) x {sample_steps} audited Simulation::advance steps "
+                      f"(after 1 warm-up step), {threads} thread(s), {secs:.2f} s"}
+
+
+def run_reference_ensemble(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    from pantometry_b200 import workloads as W
+
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    cfg = W.heat_ensemble(count=args.grids, steps=args.timesteps)
+    grids = W.ensemble_grids(cfg)
+    samples = [cpu_baseline_ensemble(cfg, grids, sample_steps=args.cpu_sample_steps, threads=ncpu,
+                                     sample_grids=max(16, 2 * ncpu)) for _ in range(args.steps)]
+    value = statistics.median(s["value"] for s in samples)
+    line = {
+        "metric": ENS_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Rng::for_index sizes, diffusivities and hot spots)",
+        "impl": "reference",
+        "config": {"workload": f"heat ensemble: {len(grids)} grids, audited Simulation::advance steps per grid"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncpu, "kind": "port",
+                         "sample": samples[0]["sample"] + "; the Rust reference cannot be built here (no cargo), "
+                                   "so this is the oracle's C++ restatement of its loops"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble"],
+                    help="hall: the acoustic hall 256^3 (the headline); ensemble: 512 uneven heat grids")
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--timesteps", type=int, default=5000)
-    ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    ap.add_argument("--grids", type=int, default=512)
+    ap.add_argument("--timesteps", type=int, default=None, help="timesteps per bench step (hall 5000, ensemble 2000)")
+    ap.add_argument("--cpu-sample-steps", type=int, default=None,
+                    help="audited steps per CPU sample (hall 16, ensemble 8): about 10 s of one core")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.timesteps is None:
+        args.timesteps = 5000 if args.workload == "hall" else 2000
+    if args.cpu_sample_steps is None:
+        args.cpu_sample_steps = 16 if args.workload == "hall" else 8
+    if args.workload == "ensemble":
+        if args.impl == "reference":
+            run_reference_ensemble(args)
+        else:
+            run_ensemble(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -219,6 +219,54 @@ pm_status pm_cavity_restore(pm_cavity* c);
 pm_status pm_cavity_set_stream(pm_cavity* c, void* stream);
 void pm_cavity_destroy(pm_cavity* c);
 
+/* ============================= Solid3D ensembles (batched) ========================== */
+
+/* Many independent one-material `Solid3D` blocks of uneven sizes, each with its own substance,
+ * step and films, advanced together: one persistent kernel per step walks a list of bricks of
+ * every block, and runs of 64 steps replay a CUDA graph. It replaces `Ensemble::run` over
+ * `Solid3D` samples (crates/pantometry-core/src/ensemble.rs:102-140), each sample driven by
+ * `Solid3D::step` (crates/pantometry-thermal/src/solid.rs:1717-1901) with its own ledger
+ * (solid.rs:1904-1927). Cells are concatenated block by block, each block in the reference's
+ * order i + nx*(j + ny*k). PM_PLAIN_F64 gives each block the bit-exact `Solid3D::step`;
+ * PM_FIELDS_F32 stores T - T0 in f32 with FP64 books. */
+typedef struct pm_ensemble pm_ensemble;
+
+typedef struct pm_ensemble_grid {
+    int nx, ny, nz;
+    double dx;
+    pm_substance substance;        /* the block's one material (solid.rs:377-421) */
+    double initial_kelvin;         /* T0: the start, the ledger's reference and the films' ambient */
+    double convection_w_per_m2_k;  /* film on each of the six faces over its whole area
+                                      (`losing_from`, solid.rs:1269-1288); 0 = insulated,
+                                      +inf = held at T0 (Dirichlet). Emissivity must be 0 with films. */
+    double dt;                     /* the block's own step */
+} pm_ensemble_grid;
+
+/* `max_stable_dt` of each described block (solid.rs:1709-1715), without a device. */
+pm_status pm_ensemble_max_stable_dt(const pm_ensemble_grid* grids, int count, double* seconds);
+/* Every block starts at its T0; the brick shape starts at 32 x 8 x 16. */
+pm_status pm_ensemble_create(const pm_ensemble_grid* grids, int count, int precision, int device,
+                             pm_ensemble** out);
+/* kelvin: every block's cells, concatenated in block order. Upload starts fresh books. */
+pm_status pm_ensemble_upload(pm_ensemble* e, const double* kelvin, size_t n);
+pm_status pm_ensemble_download(pm_ensemble* e, double* kelvin, size_t n);
+pm_status pm_ensemble_set_tolerance(pm_ensemble* e, double tol);
+/* nsteps steps of every block. Refused before anything moves if a block's dt is past its
+ * limit (PM_VIOLATION, "Fourier number"). With a tolerance set, a block whose audit fails stops
+ * where it failed (the others go on) and the call returns PM_VIOLATION for the lowest such
+ * block, its `site` naming it. */
+pm_status pm_ensemble_step(pm_ensemble* e, long long nsteps, pm_violation* out);
+/* One pm_ledger per block, in block order (parts: stored, lost, -supplied). */
+pm_status pm_ensemble_ledgers(pm_ensemble* e, pm_ledger* out, int count);
+/* Brick shape: x extent 16, 32 or 64 (y = 256 / x) and 8, 16, 32 or 64 planes. */
+pm_status pm_ensemble_set_shape(pm_ensemble* e, int brick_x, int planes);
+pm_status pm_ensemble_shape(pm_ensemble* e, int* brick_x, int* brick_y, int* planes);
+/* Time `trial_steps` steps of every brick shape on the present state, keep the fastest, and put
+ * the state and books back as they were. */
+pm_status pm_ensemble_autotune(pm_ensemble* e, int trial_steps, int* brick_x, int* planes);
+pm_status pm_ensemble_set_stream(pm_ensemble* e, void* stream);
+void pm_ensemble_destroy(pm_ensemble* e);
+
 /* ============================ Without allocation ==================================== */
 
 /* No counterpart in the reference. One Hall step (f32 fields, f64 invariant) on device buffers the

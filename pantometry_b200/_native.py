@@ -166,21 +166,24 @@ SIGNATURES = {
     "pm_cavity_restore": (_st, [_p]),
     "pm_cavity_set_stream": (_st, [_p, _p]),
     "pm_cavity_destroy": (None, [_p]),
+    # Ensembles
+    "pm_ensemble_max_stable_dt": (_st, [C.POINTER(EnsembleGrid), _i, _dp]),
+    "pm_ensemble_create": (_st, [C.POINTER(EnsembleGrid), _i, _i, _i, C.POINTER(_p)]),
+    "pm_ensemble_upload": (_st, [_p, _dp, _sz]),
+    "pm_ensemble_download": (_st, [_p, _dp, _sz]),
+    "pm_ensemble_set_tolerance": (_st, [_p, _d]),
+    "pm_ensemble_step": (_st, [_p, _ll, _vp]),
+    "pm_ensemble_ledgers": (_st, [_p, _lp, _i]),
+    "pm_ensemble_set_shape": (_st, [_p, _i, _i]),
+    "pm_ensemble_shape": (_st, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "pm_ensemble_autotune": (_st, [_p, _i, C.POINTER(_i), C.POINTER(_i)]),
+    "pm_ensemble_set_stream": (_st, [_p, _p]),
+    "pm_ensemble_destroy": (None, [_p]),
     # Without allocation
     "pm_hall_step_f32_noalloc": (_st, [_i, _i, _i, _d, _d, _d, _d, _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _dp]),
 }
 
-OPTIONAL_SIGNATURES = {
-    # Ensembles
-    "pm_ensemble_create": (_st, [C.POINTER(EnsembleGrid), _i, _i, C.POINTER(_p)]),
-    "pm_ensemble_upload": (_st, [_p, _dp, _sz]),
-    "pm_ensemble_download": (_st, [_p, _dp, _sz]),
-    "pm_ensemble_step": (_st, [_p, _ll]),
-    "pm_ensemble_ledgers": (_st, [_p, _lp, _i]),
-    "pm_ensemble_autotune": (_st, [_p, C.POINTER(_i)]),
-    "pm_ensemble_set_stream": (_st, [_p, _p]),
-    "pm_ensemble_destroy": (None, [_p]),
-}
+OPTIONAL_SIGNATURES = {}
 
 _lib = None
 

@@ -323,9 +323,9 @@ struct Cavity : Handle {
             PM_CUDA(deps[q].alloc(eps[q].size() * 8));
             PM_CUDA(dsig[q].alloc(sig[q].size() * 8));
             PM_CUDA(dmu[q].alloc(mu[q].size() * 8));
-            PM_CUDA(cudaMemcpy(deps[q].p, eps[q].data(), eps[q].size() * 8, cudaMemcpyHostToDevice));
-            PM_CUDA(cudaMemcpy(dsig[q].p, sig[q].data(), sig[q].size() * 8, cudaMemcpyHostToDevice));
-            PM_CUDA(cudaMemcpy(dmu[q].p, mu[q].data(), mu[q].size() * 8, cudaMemcpyHostToDevice));
+            PM_CUDA(put_sync(deps[q].p, eps[q].data(), eps[q].size() * 8));
+            PM_CUDA(put_sync(dsig[q].p, sig[q].data(), sig[q].size() * 8));
+            PM_CUDA(put_sync(dmu[q].p, mu[q].data(), mu[q].size() * 8));
         }
         return PM_OK;
     }
@@ -400,7 +400,7 @@ pm_status pm_cavity_obstruct(pm_cavity* cp, const uint8_t* mask, size_t n) {
         if (mask[q]) { c->solid[q] = 1; c->any_solid = true; }
     if (!c->any_solid) return PM_OK;
     PM_CUDA(c->dsolid.alloc(c->cells()));
-    PM_CUDA(cudaMemcpy(c->dsolid.p, c->solid.data(), c->cells(), cudaMemcpyHostToDevice));
+    PM_CUDA(c->put_sync(c->dsolid.p, c->solid.data(), c->cells()));
     c->drop_graphs();
     // cavity.rs:293 `enforce_solid` now, on the host copy of E
     std::vector<double> e[3];
@@ -520,7 +520,7 @@ pm_status pm_cavity_set_source(pm_cavity* cp, long long edge, const double* cur,
     c->ncurrent = (long long)n;
     if (n > 0) {
         PM_CUDA(c->current.alloc(n * 8));
-        PM_CUDA(cudaMemcpy(c->current.p, cur, n * 8, cudaMemcpyHostToDevice));
+        PM_CUDA(c->put_sync(c->current.p, cur, n * 8));
     }
     c->drop_graphs();
     return c->reset_ledger();

@@ -1,0 +1,236 @@
+// Batched Solid3D stepping: many independent uneven blocks advanced by one persistent kernel per
+// step that walks a list of bricks (the GPU form of `Ensemble::run` over `Solid3D` samples,
+// crates/pantometry-core/src/ensemble.rs:102-140, with each sample's own `Solid3D::step`,
+// crates/pantometry-thermal/src/solid.rs:1717-1901).
+//
+// Layout. The blocks' cells are concatenated in block order, each block in the reference's
+// index order i + nx·(j + ny·k). A brick is a bx × by × zc box of one block (bx·by = 256
+// threads, each marching one column of zc planes); the brick list holds every brick of every
+// block, block by block, and a persistent grid of thread blocks takes bricks blockIdx.x,
+// blockIdx.x + gridDim.x, ... in that fixed order. Brick shapes are chosen at run time (the
+// autotuner times each candidate on the real state).
+//
+// Per-cell arithmetic. The f64 form is heat_plain_step's uniform path (the reference's operand
+// order, compiled with --fmad=false: bit-exact with `Solid3D::step` for each block on its own).
+// The f32 form is heat_f32_step's (deviations T − T0, temperature-independent films).
+//
+// Ledgers. Every brick leaves one FP64 partial per quantity (fixed thread order, fixed tree).
+// The last brick of a block to finish — found with the block's own atomic ticket — sums that
+// block's partials in fixed order and runs the block's ledger and audit. The sums therefore do
+// not depend on which thread block ran which brick, only on the brick shape.
+#pragma once
+
+#include "heat_kernels.cuh"
+
+namespace pm {
+
+// One block of the ensemble, as the kernel reads it.
+struct EnsGrid {
+    int nx, ny, nz;
+    unsigned nbricks;
+    unsigned long long offset;  // first cell in the concatenated field
+    unsigned first_brick;
+    int exposed;                // film faces (bit f: XMin, XMax, YMin, YMax, ZMin, ZMax)
+    // plain f64 coefficients (`resolve` of a one-material block, solid.rs:588-784)
+    double kface, mobility, capacity, k_cell, eps_cell;
+    double dts, dx, reference;
+    double share[6], ambient[6], convection[6];
+    // f32 coefficients
+    float a;      // dt · mobility · k_face
+    float b[6];   // dt · mobility · g_f / dx per film face
+    float off[6]; // T0 − ambient per film face
+    float pad;
+};
+
+struct EnsBrick {
+    unsigned grid;
+    unsigned short x0, y0, z0, z1;
+    unsigned pad;
+};
+
+template <typename Real>
+struct EnsArgs {
+    const Real* __restrict__ old;
+    Real* __restrict__ nu;
+    const EnsGrid* __restrict__ grids;
+    const EnsBrick* __restrict__ bricks;
+    unsigned nbricks;
+    int bxs;             // log2 of the brick's x extent (4, 5 or 6)
+    DevState* states;    // one per block: its books, ledger and audit
+    double* partials;    // two per brick
+};
+
+// `film_flux` (solid.rs:1192-1219) of a block's cell, read off the old state.
+__device__ __forceinline__ double ens_film_flux(const EnsGrid& g, int i, int j, int k, double here) {
+    double out = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (!((g.exposed >> f) & 1)) continue;
+        if (!face_holds(f, i, j, k, g.nx, g.ny, g.nz)) continue;
+        const double share = g.share[f];
+        const double ambient = g.ambient[f];
+        const double gap = here - ambient;
+        if (gap == 0.0) continue;
+        // crates/pantometry-thermal/src/lib.rs:104-110 `Environment::loss_from`, area = share
+        const double convective = g.convection[f] * share * (here - ambient);
+        const double radiative = g.eps_cell * kStefanBoltzmann * share * (powi4(here) - powi4(ambient));
+        const double bare = convective + radiative;
+        const double cond = series_with_half_cell(bare / gap, g.k_cell, share, g.dx);
+        out += cond * gap / g.dx;
+    }
+    return out;
+}
+
+// One step of every live block (MEASURE = false), or the opening ledger of the present state
+// (MEASURE = true: nothing is written, stored heat is summed and committed without an audit).
+template <typename Real, bool MEASURE>
+__device__ __forceinline__ void ens_brick(const EnsArgs<Real>& a, const EnsGrid& g, const EnsBrick& br,
+                                          double (&acc)[2]) {
+    const int tid = threadIdx.x;
+    const int bx = 1 << a.bxs;
+    const int i = br.x0 + (tid & (bx - 1));
+    const int j = br.y0 + (tid >> a.bxs);
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const size_t plane = (size_t)nx * ny;
+    const Real* __restrict__ told = a.old + g.offset;
+    Real* __restrict__ tnew = a.nu + g.offset;
+    const int k0 = br.z0, k1 = br.z1;
+    size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+    if (MEASURE) {
+        for (int k = k0; k < k1; ++k, c += plane) {
+            if constexpr (sizeof(Real) == 8) acc[0] += g.capacity * ((double)told[c] - g.reference);  // solid.rs:1583-1590
+            else acc[0] += (double)told[c];
+        }
+        return;
+    }
+    if constexpr (sizeof(Real) == 8) {
+        // heat_plain_step, uniform block: the reference's order of the six face terms
+        double below = k0 > 0 ? told[c - plane] : 0.0;
+        double here = told[c];
+        const double kf = g.kface;
+        for (int k = k0; k < k1; ++k, c += plane) {
+            const double above = k + 1 < nz ? told[c + plane] : 0.0;
+            const double t0 = here;
+            double flux = 0.0;
+            if (i > 0) flux += kf * (told[c - 1] - t0);
+            if (i + 1 < nx) flux += kf * (told[c + 1] - t0);
+            if (j > 0) flux += kf * (told[c - nx] - t0);
+            if (j + 1 < ny) flux += kf * (told[c + nx] - t0);
+            if (k > 0) flux += kf * (below - t0);
+            if (k + 1 < nz) flux += kf * (above - t0);
+            const double shed = g.exposed ? ens_film_flux(g, i, j, k, t0) : 0.0;
+            const double nt = t0 + g.dts * g.mobility * (flux - shed);  // add_kelvin (solid.rs:1620-1635)
+            tnew[c] = nt;
+            acc[0] += g.capacity * (nt - g.reference);
+            if (shed != 0.0) acc[1] += g.dts * g.mobility * shed * g.capacity;  // solid.rs:1821-1823
+            below = here;
+            here = above;
+        }
+    } else {
+        // heat_f32_step on deviations
+        float below = k0 > 0 ? __ldg(told + c - plane) : 0.0f;
+        float here = __ldg(told + c);
+        const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
+        const bool edge_xy = !(xl && xh && yl && yh);
+        const float ga = g.a;
+        double col_shed = 0.0;
+        for (int k = k0; k < k1; ++k, c += plane) {
+            const float above = (k + 1 < nz) ? __ldg(told + c + plane) : 0.0f;
+            float s = 0.0f;
+            if (xl) s += __ldg(told + c - 1) - here;
+            if (xh) s += __ldg(told + c + 1) - here;
+            if (yl) s += __ldg(told + c - nx) - here;
+            if (yh) s += __ldg(told + c + nx) - here;
+            if (k > 0) s += below - here;
+            if (k + 1 < nz) s += above - here;
+            float shed = 0.0f;
+            if (g.exposed && (edge_xy || k == 0 || k + 1 == nz)) {
+                if (((g.exposed >> 0) & 1) && !xl) shed += g.b[0] * (here + g.off[0]);
+                if (((g.exposed >> 1) & 1) && !xh) shed += g.b[1] * (here + g.off[1]);
+                if (((g.exposed >> 2) & 1) && !yl) shed += g.b[2] * (here + g.off[2]);
+                if (((g.exposed >> 3) & 1) && !yh) shed += g.b[3] * (here + g.off[3]);
+                if (((g.exposed >> 4) & 1) && k == 0) shed += g.b[4] * (here + g.off[4]);
+                if (((g.exposed >> 5) & 1) && k + 1 == nz) shed += g.b[5] * (here + g.off[5]);
+                col_shed += (double)shed;
+            }
+            const float nd = here + (ga * s - shed);
+            tnew[c] = nd;
+            acc[0] += (double)nd;
+            below = here;
+            here = above;
+        }
+        acc[1] += col_shed;
+    }
+}
+
+// A block whose audit failed keeps its state: its bricks copy old to new, so the ping-pong
+// parity stays the same for every block of the ensemble.
+template <typename Real>
+__device__ __forceinline__ void ens_hold(const EnsArgs<Real>& a, const EnsGrid& g, const EnsBrick& br) {
+    const int tid = threadIdx.x;
+    const int i = br.x0 + (tid & ((1 << a.bxs) - 1));
+    const int j = br.y0 + (tid >> a.bxs);
+    if (i >= g.nx || j >= g.ny) return;
+    const size_t plane = (size_t)g.nx * g.ny;
+    size_t c = g.offset + (size_t)i + (size_t)g.nx * ((size_t)j + (size_t)g.ny * br.z0);
+    for (int k = br.z0; k < br.z1; ++k, c += plane) a.nu[c] = a.old[c];
+}
+
+template <typename Real, bool MEASURE>
+static __global__ void __launch_bounds__(256) ens_step(EnsArgs<Real> a) {
+    __shared__ double red[32 * 2];
+    __shared__ int last;
+    const int tid = threadIdx.x;
+    for (unsigned b = blockIdx.x; b < a.nbricks; b += gridDim.x) {
+        const EnsBrick br = a.bricks[b];
+        const EnsGrid& g = a.grids[br.grid];
+        DevState* st = a.states + br.grid;
+        if (!MEASURE && st->violated) {  // block-uniform: every thread reads the same word
+            ens_hold<Real>(a, g, br);
+            continue;
+        }
+        double acc[2] = {0.0, 0.0};
+        ens_brick<Real, MEASURE>(a, g, br, acc);
+        block_sum<2>(acc, red);
+        if (tid == 0) {
+            a.partials[2 * (size_t)b] = acc[0];
+            a.partials[2 * (size_t)b + 1] = acc[1];
+            __threadfence();
+            const unsigned ticket = atomicAdd(&st->counter, 1u);
+            last = ticket == g.nbricks - 1 ? 1 : 0;
+        }
+        __syncthreads();
+        if (!last) continue;
+        // The block's last brick: its partials in fixed order, then the ledger and the audit.
+        __threadfence();
+        double v[2] = {0.0, 0.0};
+        for (unsigned q = tid; q < g.nbricks; q += blockDim.x) {
+            v[0] += __ldcg(&a.partials[2 * (size_t)(g.first_brick + q)]);
+            v[1] += __ldcg(&a.partials[2 * (size_t)(g.first_brick + q) + 1]);
+        }
+        block_sum<2>(v, red);
+        if (tid == 0) {
+            st->counter = 0u;
+            const double stored = sizeof(Real) == 8 ? v[0] : g.capacity * v[0];
+            if (!MEASURE) st->lost += sizeof(Real) == 8 ? v[1] : g.capacity * v[1];
+            double total = 0.0, scale = 0.0;
+            ledger_add(total, scale, stored);
+            ledger_add(total, scale, st->lost);
+            ledger_add(total, scale, -st->supplied);
+            st->part[0] = stored;
+            st->part[1] = st->lost;
+            st->part[2] = -st->supplied;
+            if (MEASURE) {
+                st->total = total;
+                st->scale = scale;
+                st->prev_total = total;
+                st->prev_scale = scale;
+            } else {
+                audit_and_commit(st, total, scale);
+            }
+        }
+    }
+}
+
+}  // namespace pm

@@ -86,6 +86,13 @@ cudaError_t launch_to_f64(const float* src, double* dst, size_t n, cudaStream_t 
 }
 
 
+template <>
+cudaError_t launch_ens<float>(const EnsArgs<float>& a, bool measure, unsigned nblocks, cudaStream_t s) {
+    if (measure) ens_step<float, true><<<nblocks, 256, 0, s>>>(a);
+    else ens_step<float, false><<<nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -101,6 +108,7 @@ int occupancy_f32(KernelId id) {
             cudaFuncSetAttribute(yee_step<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
+        case kEnsF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

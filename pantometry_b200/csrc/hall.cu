@@ -91,9 +91,9 @@ struct Hall : Handle {
         }
         if (!bscale.p) PM_CUDA(bscale.alloc(nb * 8));
         if (!bknode.p) PM_CUDA(bknode.alloc(nb * 8));
-        if (precision == PM_PLAIN_F64) PM_CUDA(cudaMemcpy(bscale.p, sc64.data(), nb * 8, cudaMemcpyHostToDevice));
-        else PM_CUDA(cudaMemcpy(bscale.p, sc32.data(), nb * 4, cudaMemcpyHostToDevice));
-        PM_CUDA(cudaMemcpy(bknode.p, kn.data(), nb * 8, cudaMemcpyHostToDevice));
+        if (precision == PM_PLAIN_F64) PM_CUDA(put_sync(bscale.p, sc64.data(), nb * 8));
+        else PM_CUDA(put_sync(bscale.p, sc32.data(), nb * 4));
+        PM_CUDA(put_sync(bknode.p, kn.data(), nb * 8));
         bscale_dt = h;
         drop_graphs();
         return PM_OK;
@@ -247,7 +247,7 @@ pm_status pm_hall_set_source(pm_hall* hp, long long node, const double* wave, si
     h->nwave = (long long)n;
     if (n > 0) {
         PM_CUDA(h->wave.alloc(n * 8));
-        PM_CUDA(cudaMemcpy(h->wave.p, wave, n * 8, cudaMemcpyHostToDevice));
+        PM_CUDA(h->put_sync(h->wave.p, wave, n * 8));
     }
     const int i = (int)(node % h->nx), j = (int)((node / h->nx) % h->ny), k = (int)(node / ((long long)h->nx * h->ny));
     auto w = [](int q, int m) { return (q == 0 || q + 1 == m) ? 2.0 : 1.0; };

@@ -209,7 +209,7 @@ struct Heat : Handle {
         if (precision != PM_PLAIN_F64) return fail(PM_UNSUPPORTED, "a filled (multi-material) block runs in the plain f64 form only");
         auto put = [&](DBuf& b, const void* src, size_t bytes) -> pm_status {
             PM_CUDA(b.alloc(bytes));
-            PM_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+            PM_CUDA(put_sync(b.p, src, bytes));
             return PM_OK;
         };
         pm_status s;

@@ -8,6 +8,7 @@
 #include "heat_kernels.cuh"
 #include "hall_kernels.cuh"
 #include "yee_kernels.cuh"
+#include "ensemble_kernels.cuh"
 
 namespace pm {
 
@@ -41,7 +42,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kKernelCount
+    kEnsF64, kEnsF32, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -64,6 +65,8 @@ template <typename Real> cudaError_t launch_yee_h(const YeeHArgs<Real>& a, cudaS
 template <typename Real> cudaError_t launch_yee_e(const YeeEArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_step(const YeeStepArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_measure(const YeeHArgs<Real>& a, double* out2, cudaStream_t s);
+// One ensemble step (measure = false) or the opening ledgers (measure = true) over the brick list.
+template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool measure, unsigned nblocks, cudaStream_t s);
 
 // Element-wise conversions between the caller's f64 arrays and an f32 store.
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);

@@ -86,7 +86,12 @@ cudaError_t launch_yee_measure<double>(const YeeHArgs<double>& a, double* out2, 
     yee_measure<double><<<a.nblocks, tile_block(), 0, s>>>(a, out2);
     return cudaGetLastError();
 }
-
+template <>
+cudaError_t launch_ens<double>(const EnsArgs<double>& a, bool measure, unsigned nblocks, cudaStream_t s) {
+    if (measure) ens_step<double, true><<<nblocks, 256, 0, s>>>(a);
+    else ens_step<double, false><<<nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
 
 int occupancy_f64(KernelId id) {
     int n = 0;
@@ -103,6 +108,7 @@ int occupancy_f64(KernelId id) {
             cudaFuncSetAttribute(yee_step<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double, false, true>, 256, yee_smem_bytes<double>());
             break;
+        case kEnsF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

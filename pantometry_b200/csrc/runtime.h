@@ -82,6 +82,13 @@ struct Handle {
     void drop_graphs();
     ~Handle();
 
+    // Host → device copy ordered on the handle's stream and complete on return, so the source
+    // may be freed at once and every later launch on the stream sees the bytes.
+    cudaError_t put_sync(void* dst, const void* src, size_t bytes) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream());
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream());
+        return e;
+    }
     pm_status read_state();                    // device → host_state, synchronising
     pm_status write_state();                   // host_state → device
     pm_status begin_call();                    // clear the previous call's violation

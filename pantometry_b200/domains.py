@@ -286,6 +286,109 @@ class Cavity(_Domain):
         return e.value, m.value
 
 
+class Ensemble:
+    """Many independent one-material `Solid3D` blocks of uneven sizes advanced together by one
+    persistent brick-list kernel per step — the GPU form of `Ensemble::run` over `Solid3D`
+    samples (crates/pantometry-core/src/ensemble.rs:102-140). Each block has its own substance,
+    step, films (on all six faces at its own T0: 0 insulated, +inf Dirichlet) and FP64 books.
+
+    `grids` is a list of dicts: counts, dx, substance (density, conductivity, specific_heat,
+    emissivity), initial (T0, kelvin), convection (W/m²K) and dt (seconds)."""
+
+    def __init__(self, grids, precision="f32", device=0):
+        self._lib = N.load()
+        self._desc = self.describe(grids)
+        self.counts = [tuple(int(c) for c in g["counts"]) for g in grids]
+        self.sizes = np.array([nx * ny * nz for nx, ny, nz in self.counts], dtype=np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+        self.n = int(self.offsets[-1])
+        self.precision = _precision(precision)
+        h = C.c_void_p()
+        N.check(self._lib.pm_ensemble_create(self._desc, len(grids), self.precision, device, C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def describe(grids):
+        arr = (N.EnsembleGrid * len(grids))()
+        for d, g in zip(arr, grids):
+            d.nx, d.ny, d.nz = (int(c) for c in g["counts"])
+            d.dx = g["dx"]
+            s = g["substance"]
+            d.substance = N.Substance(s["density"], s["conductivity"], s["specific_heat"], s.get("emissivity", 0.0), 1)
+            d.initial_kelvin = g["initial"]
+            d.convection_w_per_m2_k = g.get("convection", 0.0)
+            d.dt = g.get("dt", 1.0)
+        return arr
+
+    @staticmethod
+    def max_stable_dt(grids):
+        """Each block's `max_stable_dt` (solid.rs:1709-1715), computed on the host."""
+        desc = Ensemble.describe(grids)
+        out = np.empty(len(grids))
+        N.check(N.load().pm_ensemble_max_stable_dt(desc, len(grids), _ptr(out)))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.load().pm_ensemble_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    def upload(self, kelvin):
+        """Every block's cells, concatenated in block order; starts fresh books."""
+        t = _f64(kelvin, self.n)
+        N.check(self._lib.pm_ensemble_upload(self._h, _ptr(t), t.size))
+
+    def download(self, out=None):
+        if out is None:
+            out = np.empty(self.n)
+        if out.dtype != np.float64 or out.size != self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous f64 array with one value per cell")
+        N.check(self._lib.pm_ensemble_download(self._h, _ptr(out), out.size))
+        return out
+
+    def block(self, cells, g):
+        """Block g's cells out of a concatenated array."""
+        return cells[self.offsets[g]:self.offsets[g + 1]]
+
+    def set_tolerance(self, tol):
+        N.check(self._lib.pm_ensemble_set_tolerance(self._h, float(tol)))
+
+    def set_stream(self, stream):
+        N.check(self._lib.pm_ensemble_set_stream(self._h, C.c_void_p(stream or 0)))
+
+    def step(self, nsteps=1):
+        v = N.Violation()
+        st = self._lib.pm_ensemble_step(self._h, int(nsteps), C.byref(v))
+        if st == N.PM_VIOLATION:
+            return v.as_dict()
+        N.check(st)
+        return None
+
+    def ledgers(self):
+        out = (N.Ledger * len(self.counts))()
+        N.check(self._lib.pm_ensemble_ledgers(self._h, out, len(self.counts)))
+        return [{"total": l.total, "scale": l.scale, "parts": [l.parts[q] for q in range(l.n_parts)], "steps": l.steps}
+                for l in out]
+
+    def set_shape(self, brick_x, planes):
+        N.check(self._lib.pm_ensemble_set_shape(self._h, int(brick_x), int(planes)))
+
+    def shape(self):
+        bx, by, zc = C.c_int(), C.c_int(), C.c_int()
+        N.check(self._lib.pm_ensemble_shape(self._h, C.byref(bx), C.byref(by), C.byref(zc)))
+        return bx.value, by.value, zc.value
+
+    def autotune(self, trial_steps=10):
+        """Time every brick shape on the present state, keep the fastest; the state is put back."""
+        bx, zc = C.c_int(), C.c_int()
+        N.check(self._lib.pm_ensemble_autotune(self._h, int(trial_steps), C.byref(bx), C.byref(zc)))
+        return bx.value, zc.value
+
+
 def device_count():
     n = C.c_int()
     st = N.load().pm_device_count(C.byref(n))

@@ -195,3 +195,23 @@ def heat_ensemble(count=512, seed=SEED, lo=16, hi=128, steps=2000):
 
 def ensemble_cells(grid):
     return hot_spot(grid["counts"], grid["centre"], sigma=grid["sigma"])
+
+
+def ensemble_grids(cfg, dt_fraction=0.9):
+    """The ensemble's block descriptors: Dirichlet (h = +inf) films at 300 K on every face and
+    each block's dt at `dt_fraction` of its own stability limit."""
+    from .domains import Ensemble
+
+    grids = [{"counts": g["counts"], "dx": g["dx"], "substance": g["substance"], "initial": g["initial"],
+              "convection": math.inf} for g in cfg["grids"]]
+    for g, limit in zip(grids, Ensemble.max_stable_dt(grids)):
+        g["dt"] = dt_fraction * limit
+    return grids
+
+
+def build_ensemble(cfg, precision="f32", device=0, cells=None):
+    from .domains import Ensemble
+
+    e = Ensemble(ensemble_grids(cfg), precision=precision, device=device)
+    e.upload(np.concatenate([ensemble_cells(g) for g in cfg["grids"]]) if cells is None else cells)
+    return e
