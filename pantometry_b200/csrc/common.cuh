@@ -57,13 +57,14 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Why the run stopped, in DevState::violated.
-enum : int { kRunning = 0, kAuditFailed = 1, kStartupFailed = 2 };
+// kDeviceTimeout: a bounded wait inside a kernel ran out (the kernel gave up and returned).
+enum : int { kRunning = 0, kAuditFailed = 1, kStartupFailed = 2, kDeviceTimeout = 3 };
 
 // One per handle, in device memory. Written only by the last block of a step kernel (and by
 // the host between calls), read by every block of the next kernel: stream order is the only
 // synchronisation, nothing ever spins.
 struct DevState {
-    int violated;       // kRunning / kAuditFailed / kStartupFailed
+    int violated;       // kRunning / kAuditFailed / kStartupFailed / kDeviceTimeout
     int has_invariant;  // cavity: an invariant exists (after release_mode or a first step)
     long long steps;    // steps completed since the state was uploaded or released
     long long violation_step;

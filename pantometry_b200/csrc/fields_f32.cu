@@ -1,4 +1,6 @@
 // The f32-field forms (the chosen precision): fields in f32, ledgers and audits in f64.
+#include <cudaTypedefs.h>
+
 #include "launch.h"
 
 namespace pm {
@@ -93,6 +95,41 @@ cudaError_t launch_ens<float>(const EnsArgs<float>& a, bool measure, unsigned nb
     return cudaGetLastError();
 }
 
+cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s) {
+    constexpr int P = kHallTmaPlanes, S = kHallTmaStages;
+    static bool attr = false;
+    const int smem = (int)hall_tma_smem_bytes();
+    if (!attr) {
+        cudaFuncSetAttribute(hall_tma_step<P, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(hall_tma_step<P, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    if (a.block_scale)
+        hall_tma_step<P, S, true><<<a.nblocks, tile_block(), smem, s>>>(a, m);
+    else
+        hall_tma_step<P, S, false><<<a.nblocks, tile_block(), smem, s>>>(a, m);
+    return cudaGetLastError();
+}
+
+bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
+    const cuuint32_t box[3] = {bx, by, bz};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -109,6 +146,12 @@ int occupancy_f32(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
         case kEnsF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false>, 256, 0); break;
+        case kHallTma:
+            cudaFuncSetAttribute(hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_tma_smem_bytes());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>, 256,
+                                                              hall_tma_smem_bytes());
+            break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -27,11 +27,19 @@ struct Hall : Handle {
     // checkpoint (hall.rs:536-555)
     DBuf sp, svx, svy, svz;
     bool s_staggered = false;
+    // FP32 halls whose x extent is a multiple of 4 keep the face arrays padded to the node grid
+    // and step with the TMA-staged kernel (hall_tma.cuh); maps[par] describe the fields of parity par
+    bool tma = false;
+    HallMaps maps[2];
 
     size_t nodes() const { return (size_t)nx * ny * nz; }
     size_t nvx() const { return (size_t)(nx - 1) * ny * nz; }
     size_t nvy() const { return (size_t)nx * (ny - 1) * nz; }
     size_t nvz() const { return (size_t)nx * ny * (nz - 1); }
+    // elements held on the device per face array (the padded layout keeps one per node)
+    size_t dvx() const { return tma ? nodes() : nvx(); }
+    size_t dvy() const { return tma ? nodes() : nvy(); }
+    size_t dvz() const { return tma ? nodes() : nvz(); }
     size_t esize() const { return precision == PM_PLAIN_F64 ? 8 : 4; }
     double rc2() const { return density * speed * speed; }
     double volume() const { return dx * dx * dx; }
@@ -63,7 +71,7 @@ struct Hall : Handle {
         a.nwave = nwave;
         a.wsrc = wsrc;
         a.starting = starting ? 1 : 0;
-        const unsigned w = wave_of(sizeof(Real) == 8 ? kHallF64 : kHallF32);
+        const unsigned w = wave_of(sizeof(Real) == 8 ? kHallF64 : (tma ? kHallTma : kHallF32));
         a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
         a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
@@ -71,9 +79,26 @@ struct Hall : Handle {
         return a;
     }
 
+    cudaError_t launch(int par, double h, bool starting, cudaStream_t s) const {
+        if (precision == PM_PLAIN_F64) return launch_hall<double>(args<double>(par, h, starting), s);
+        if (tma) return launch_hall_tma(args<float>(par, h, starting), maps[par], s);
+        return launch_hall<float>(args<float>(par, h, starting), s);
+    }
     pm_status launch_one(int par, double h, bool starting, cudaStream_t s) const {
-        if (precision == PM_PLAIN_F64) PM_CUDA(launch_hall<double>(args<double>(par, h, starting), s));
-        else PM_CUDA(launch_hall<float>(args<float>(par, h, starting), s));
+        PM_CUDA(launch(par, h, starting, s));
+        return PM_OK;
+    }
+
+    // Tensor maps of both parities' fields, with the boxes hall_tma_step loads.
+    pm_status build_maps() {
+        constexpr unsigned P = kHallTmaPlanes;
+        for (int q = 0; q < 2; ++q) {
+            if (!hall_tma_map(&maps[q].p, p[q].p, nx, ny, nz, 40, 10, P + 2) ||
+                !hall_tma_map(&maps[q].vx, vx[q].p, nx, ny, nz, 36, 8, P) ||
+                !hall_tma_map(&maps[q].vy, vy[q].p, nx, ny, nz, 32, 9, P) ||
+                !hall_tma_map(&maps[q].vz, vz[q].p, nx, ny, nz, 32, 8, P + 1))
+                return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a hall field");
+        }
         return PM_OK;
     }
 
@@ -118,6 +143,7 @@ struct Hall : Handle {
             m.nx = nx; m.ny = ny; m.nz = nz;
             m.knode = volume() / (2.0 * rc2()); m.kface = 0.5 * density * volume();
             if (block > 0) { m.block_knode = bknode.as<double>(); m.block = block; m.nbx = nbx; m.nby = nby; }
+            m.padded = tma ? 1 : 0;
             m.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, resident)); m.nblocks = grid_for(m.tiles, resident);
             m.st = state.as<DevState>(); m.partials = partials.as<double>();
             PM_CUDA(launch_hall_measure<float>(m, stream()));
@@ -134,6 +160,27 @@ struct Hall : Handle {
             PM_CUDA(cudaMemcpyAsync(stage.p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
             PM_CUDA(launch_to_f32(stage.as<double>(), dst.as<float>(), n, stream()));
         }
+        return PM_OK;
+    }
+    // A face array to the host in the reference's layout (hall.rs:67-77): the padded layout
+    // drops the high column (x), row (y) or plane (z) of each array.
+    pm_status get_face(int axis, const DBuf& src_dev, double* dst_host) {
+        if (!dst_host) return PM_OK;
+        const size_t n = axis == 0 ? nvx() : axis == 1 ? nvy() : nvz();
+        if (!tma) return get(src_dev, dst_host, n);
+        if (n == 0) return PM_OK;
+        if (!stage.p || stage.bytes < nodes() * 8) PM_CUDA(stage.alloc(nodes() * 8));
+        PM_CUDA(launch_to_f64(src_dev.as<float>(), stage.as<double>(), nodes(), stream()));
+        const size_t row = (size_t)nx * 8;
+        if (axis == 0)
+            PM_CUDA(cudaMemcpy2DAsync(dst_host, (nx - 1) * 8, stage.p, row, (nx - 1) * 8, (size_t)ny * nz,
+                                      cudaMemcpyDeviceToHost, stream()));
+        else if (axis == 1)
+            PM_CUDA(cudaMemcpy2DAsync(dst_host, row * (ny - 1), stage.p, row * ny, row * (ny - 1), nz,
+                                      cudaMemcpyDeviceToHost, stream()));
+        else
+            PM_CUDA(cudaMemcpyAsync(dst_host, stage.p, n * 8, cudaMemcpyDeviceToHost, stream()));
+        PM_CUDA(cudaStreamSynchronize(stream()));
         return PM_OK;
     }
     pm_status get(const DBuf& src_dev, double* dst_host, size_t n) {
@@ -181,15 +228,21 @@ pm_status pm_hall_create(const pm_hall_desc* d, pm_hall** out) {
     h->max_speed = d->speed;
     pm_status s = h->init(d->device, 0);
     if (s != PM_OK) { delete h; return s; }
-    for (int q = 0; q < 2; ++q) {
-        cudaError_t e;
-        if ((e = h->p[q].alloc(h->nodes() * h->esize())) != cudaSuccess ||
-            (e = h->vx[q].alloc(h->nvx() * h->esize())) != cudaSuccess ||
-            (e = h->vy[q].alloc(h->nvy() * h->esize())) != cudaSuccess ||
-            (e = h->vz[q].alloc(h->nvz() * h->esize())) != cudaSuccess) {
-            delete h;
-            return cuda_fail(e, "cudaMalloc hall fields");
+    h->tma = h->precision == PM_FIELDS_F32 && h->nx % 4 == 0 && h->nodes() < (1ull << 32);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        for (int q = 0; q < 2; ++q) {
+            cudaError_t e;
+            if ((e = h->p[q].alloc(h->nodes() * h->esize())) != cudaSuccess ||
+                (e = h->vx[q].alloc(h->dvx() * h->esize())) != cudaSuccess ||
+                (e = h->vy[q].alloc(h->dvy() * h->esize())) != cudaSuccess ||
+                (e = h->vz[q].alloc(h->dvz() * h->esize())) != cudaSuccess) {
+                delete h;
+                return cuda_fail(e, "cudaMalloc hall fields");
+            }
         }
+        // a shape the driver will not tile steps with the cp.async kernel on the reference layout
+        if (!h->tma || h->build_maps() == PM_OK) break;
+        h->tma = false;
     }
     *out = reinterpret_cast<pm_hall*>(h);
     std::vector<double> zero(h->nodes(), 0.0);
@@ -218,9 +271,9 @@ pm_status pm_hall_release(pm_hall* hp, const double* pressure, size_t n) {
     if ((s = h->put(h->p[0], pressure, n)) != PM_OK) return s;
     PM_CUDA(cudaMemcpyAsync(h->p[1].p, h->p[0].p, n * h->esize(), cudaMemcpyDeviceToDevice, h->stream()));
     for (int q = 0; q < 2; ++q) {
-        PM_CUDA(cudaMemsetAsync(h->vx[q].p, 0, h->nvx() * h->esize(), h->stream()));
-        PM_CUDA(cudaMemsetAsync(h->vy[q].p, 0, h->nvy() * h->esize(), h->stream()));
-        PM_CUDA(cudaMemsetAsync(h->vz[q].p, 0, h->nvz() * h->esize(), h->stream()));
+        PM_CUDA(cudaMemsetAsync(h->vx[q].p, 0, h->dvx() * h->esize(), h->stream()));
+        PM_CUDA(cudaMemsetAsync(h->vy[q].p, 0, h->dvy() * h->esize(), h->stream()));
+        PM_CUDA(cudaMemsetAsync(h->vz[q].p, 0, h->dvz() * h->esize(), h->stream()));
     }
     h->staggered = false;
     if ((s = h->measure(0, 1)) != PM_OK) return s;
@@ -333,10 +386,7 @@ pm_status pm_hall_step(pm_hall* hp, double dt, long long nsteps, pm_violation* o
         h->staggered = true;
         remaining -= 1;
     }
-    s = h->run_steps(remaining, dt, true, [h, dt](int par, cudaStream_t st) {
-        return h->precision == PM_PLAIN_F64 ? launch_hall<double>(h->args<double>(par, dt, false), st)
-                                            : launch_hall<float>(h->args<float>(par, dt, false), st);
-    });
+    s = h->run_steps(remaining, dt, true, [h, dt](int par, cudaStream_t st) { return h->launch(par, dt, false, st); });
     if (s != PM_OK) return s;
     return h->finish_call(before, out, h->name + " (its own books, against what it moved on the bus)",
                           h->name + " (starting the leapfrog)", true);
@@ -368,9 +418,9 @@ pm_status pm_hall_download(pm_hall* hp, double* pr, double* pp, double* vx, doub
     pm_status s;
     if ((s = h->get(h->p[par], pr, h->nodes())) != PM_OK) return s;
     if ((s = h->get(h->p[par ^ 1], pp, h->nodes())) != PM_OK) return s;
-    if ((s = h->get(h->vx[par], vx, h->nvx())) != PM_OK) return s;
-    if ((s = h->get(h->vy[par], vy, h->nvy())) != PM_OK) return s;
-    return h->get(h->vz[par], vz, h->nvz());
+    if ((s = h->get_face(0, h->vx[par], vx)) != PM_OK) return s;
+    if ((s = h->get_face(1, h->vy[par], vy)) != PM_OK) return s;
+    return h->get_face(2, h->vz[par], vz);
 }
 
 pm_status pm_hall_checkpoint(pm_hall* hp) {
@@ -384,9 +434,9 @@ pm_status pm_hall_checkpoint(pm_hall* hp) {
     };
     pm_status s;
     if ((s = save(h->sp, h->p[par], h->nodes())) != PM_OK) return s;
-    if ((s = save(h->svx, h->vx[par], h->nvx())) != PM_OK) return s;
-    if ((s = save(h->svy, h->vy[par], h->nvy())) != PM_OK) return s;
-    if ((s = save(h->svz, h->vz[par], h->nvz())) != PM_OK) return s;
+    if ((s = save(h->svx, h->vx[par], h->dvx())) != PM_OK) return s;
+    if ((s = save(h->svy, h->vy[par], h->dvy())) != PM_OK) return s;
+    if ((s = save(h->svz, h->vz[par], h->dvz())) != PM_OK) return s;
     h->s_staggered = h->staggered;
     h->has_saved = true;
     PM_CUDA(cudaStreamSynchronize(h->stream()));
@@ -402,9 +452,9 @@ pm_status pm_hall_restore(pm_hall* hp) {
     // hall.rs:546-555: pressure_prev = pressure = saved
     PM_CUDA(cudaMemcpyAsync(h->p[par].p, h->sp.p, h->nodes() * e, cudaMemcpyDeviceToDevice, h->stream()));
     PM_CUDA(cudaMemcpyAsync(h->p[par ^ 1].p, h->sp.p, h->nodes() * e, cudaMemcpyDeviceToDevice, h->stream()));
-    PM_CUDA(cudaMemcpyAsync(h->vx[par].p, h->svx.p, h->nvx() * e, cudaMemcpyDeviceToDevice, h->stream()));
-    PM_CUDA(cudaMemcpyAsync(h->vy[par].p, h->svy.p, h->nvy() * e, cudaMemcpyDeviceToDevice, h->stream()));
-    PM_CUDA(cudaMemcpyAsync(h->vz[par].p, h->svz.p, h->nvz() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->vx[par].p, h->svx.p, h->dvx() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->vy[par].p, h->svy.p, h->dvy() * e, cudaMemcpyDeviceToDevice, h->stream()));
+    PM_CUDA(cudaMemcpyAsync(h->vz[par].p, h->svz.p, h->dvz() * e, cudaMemcpyDeviceToDevice, h->stream()));
     h->staggered = h->s_staggered;
     pm_status s = h->measure(par, par ^ 1);
     if (s != PM_OK) return s;

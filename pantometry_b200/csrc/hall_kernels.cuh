@@ -224,6 +224,40 @@ __device__ __forceinline__ void hall_stage(unsigned base, unsigned halo_at, cons
     cp_async_if<B>(base + halo_at + o.hplane, hsrc + o.halo + o.hstride, o.halo_live && two);
 }
 
+// The step's ledger, in the last block: the invariant of the new state, the source's injected
+// work, the startup offset on the first step (hall.rs:513-528) and the audit.
+template <typename Real>
+__device__ __forceinline__ void hall_finish(const HallArgs<Real>& a, double (&acc)[3], double delta) {
+    DevState* st = a.st;
+    if (finish_blocks<3>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
+        const double plus = acc[0];
+        st->injected += acc[2];
+        st->last_delta = delta;
+        if (a.starting) {
+            // hall.rs:513-528, with the invariant taken before this step's injection
+            const double invariant = plus - acc[1];
+            const double off = st->datum - invariant;
+            const double sc = rmax(fabs(st->datum), fabs(invariant));
+            if (sc > 0.0 && fabs(off) / sc > 0.25) {
+                st->violated = kStartupFailed;
+                st->violation_step = st->steps + 1;
+                st->v_before = st->datum;
+                st->v_after = invariant;
+                st->v_scale = sc;
+                st->v_tol = 0.25;
+            } else {
+                st->offset = off;
+            }
+        }
+        double total = 0.0, scale = 0.0;
+        const double energy = plus + st->offset - st->injected;
+        ledger_add(total, scale, energy);
+        st->part[0] = energy;
+        st->invariant = plus;
+        audit_and_commit(st, total, scale);
+    }
+}
+
 template <typename Real, bool HET>
 static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_step(HallArgs<Real> a) {
     DevState* st = a.st;
@@ -358,33 +392,7 @@ static __global__ void __launch_bounds__(256, HallDepth<Real>::min_blocks) hall_
         slot = slot + 1 == S ? 0 : slot + 1;
     }
     cp_async_wait<0>();
-    if (finish_blocks<3>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
-        const double plus = acc[0];
-        st->injected += acc[2];
-        st->last_delta = delta;
-        if (a.starting) {
-            // hall.rs:513-528, with the invariant taken before this step's injection
-            const double invariant = plus - acc[1];
-            const double off = st->datum - invariant;
-            const double sc = rmax(fabs(st->datum), fabs(invariant));
-            if (sc > 0.0 && fabs(off) / sc > 0.25) {
-                st->violated = kStartupFailed;
-                st->violation_step = st->steps + 1;
-                st->v_before = st->datum;
-                st->v_after = invariant;
-                st->v_scale = sc;
-                st->v_tol = 0.25;
-            } else {
-                st->offset = off;
-            }
-        }
-        double total = 0.0, scale = 0.0;
-        const double energy = plus + st->offset - st->injected;
-        ledger_add(total, scale, energy);
-        st->part[0] = energy;
-        st->invariant = plus;
-        audit_and_commit(st, total, scale);
-    }
+    hall_finish<Real>(a, acc, delta);
 }
 
 // `invariant_si` of an uploaded state (hall.rs:334-384), for `released_from`'s datum.
@@ -399,6 +407,7 @@ struct HallMeasureArgs {
     double knode, kface;
     const double* __restrict__ block_knode;
     int block, nbx, nby;
+    int padded;  // face arrays laid out like the nodes (nx·ny·nz each), as the TMA form keeps them
     Tiles tiles;
     DevState* st;
     double* partials;
@@ -424,11 +433,11 @@ static __global__ void __launch_bounds__(256) hall_measure(HallMeasureArgs<Real>
             if (a.block_knode) kn = a.block_knode[i / a.block + a.nbx * (j / a.block + a.nby * (k / a.block))];
             double inv = (1.0 / (wi * wj * wk)) * (double)a.p[idx] * (double)a.pp[idx] * kn;
             if (i + 1 < nx) {
-                const double v = a.vx[(size_t)i + (size_t)(nx - 1) * ((size_t)j + (size_t)ny * k)];
+                const double v = a.vx[a.padded ? idx : (size_t)i + (size_t)(nx - 1) * ((size_t)j + (size_t)ny * k)];
                 inv += (1.0 / (wj * wk)) * a.kface * v * v;
             }
             if (j + 1 < ny) {
-                const double v = a.vy[(size_t)i + (size_t)nx * ((size_t)j + (size_t)(ny - 1) * k)];
+                const double v = a.vy[a.padded ? idx : (size_t)i + (size_t)nx * ((size_t)j + (size_t)(ny - 1) * k)];
                 inv += (1.0 / (wi * wk)) * a.kface * v * v;
             }
             if (k + 1 < nz) {

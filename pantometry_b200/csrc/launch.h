@@ -9,6 +9,7 @@
 #include "hall_kernels.cuh"
 #include "yee_kernels.cuh"
 #include "ensemble_kernels.cuh"
+#include "hall_tma.cuh"
 
 namespace pm {
 
@@ -42,7 +43,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -65,6 +66,14 @@ template <typename Real> cudaError_t launch_yee_h(const YeeHArgs<Real>& a, cudaS
 template <typename Real> cudaError_t launch_yee_e(const YeeEArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_step(const YeeStepArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_measure(const YeeHArgs<Real>& a, double* out2, cudaStream_t s);
+// The FP32 Hall step staged by TMA (padded face layout, nx a multiple of 4).
+cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s);
+inline size_t hall_tma_smem_bytes() {
+    return sizeof(HallTmaStage<kHallTmaPlanes>) * kHallTmaStages + 8 * kHallTmaStages;
+}
+// Encode the tensor map of one f32 field of an nx × ny × nz hall (row pitch nx·4 bytes) with the
+// given box; false if the driver refuses it.
+bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz);
 // One ensemble step (measure = false) or the opening ledgers (measure = true) over the brick list.
 template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool measure, unsigned nblocks, cudaStream_t s);
 

@@ -136,6 +136,8 @@ pm_status Handle::finish_call(long long steps_before, pm_violation* out, const s
     const long long executed = host_state->steps - steps_before;
     if (pingpong) parity = call_parity ^ (int)(executed & 1);
     if (host_state->violated == kRunning) return PM_OK;
+    if (host_state->violated == kDeviceTimeout)
+        return fail(PM_DEVICE_TIMEOUT, "a bounded wait inside a " + name + " kernel ran out; the call stopped");
     const long long at = host_state->violation_step - steps_before;
     if (host_state->violated == kStartupFailed)
         fill_violation(out, "energy", startup_site, host_state->v_before, host_state->v_after, host_state->v_scale,
