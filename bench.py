@@ -37,9 +37,9 @@ METRIC = "Gcell-updates/s (acoustic hall 256^3, FP32 fields + FP64 audit)"
 UNIT = "Gcell-updates/s"
 BYTES_F32 = 32  # per node-update: p, vx, vy, vz, read and written once
 BYTES_F64 = 64
-# dram__bytes_read.sum + dram__bytes_write.sum of one hall_step<float> launch at 256³ (277.8 MB
-# read + 222.9 MB written), from the ncu capture summarised in profiles/hall_step_f32_256.md.
-HALL_F32_TRAFFIC = 500773632
+# dram__bytes_read.sum + dram__bytes_write.sum of one hall_tma_step launch at 256³ (270.4 MB read
+# + 219.5 MB written), from the ncu capture summarised in profiles/hall_tma_step_f32_256.md.
+HALL_F32_TRAFFIC = 489971968
 
 
 def peaks():
@@ -233,7 +233,7 @@ def run_ours(args):
         "gpu_launches": args.steps * T,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": HALL_F32_TRAFFIC,
-                     "kernel": "hall_step<float>", "bytes_per_launch": BYTES_F32 * nodes,
+                     "kernel": "hall_tma_step (FP32, TMA-staged)", "bytes_per_launch": BYTES_F32 * nodes,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
                       "roofline_frac": round(BYTES_F64 * nodes / (per_launch64 * 1e-3) / 1e9 / peak, 4),

@@ -72,7 +72,7 @@ struct Hall : Handle {
         a.wsrc = wsrc;
         a.starting = starting ? 1 : 0;
         const unsigned w = wave_of(sizeof(Real) == 8 ? kHallF64 : (tma ? kHallTma : kHallF32));
-        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
+        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w, (sizeof(Real) == 4 && tma) ? kHallTmaPlanes : 4));
         a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();

@@ -43,12 +43,17 @@ struct HallTmaStage {
     float vz[P + 1][8][32];
 };
 
-// Planes per stage and stages in the ring.
+// Planes per stage, stages in the ring and resident blocks per SM: 8 planes in each of 2 stages
+// (87 KB of shared memory, two blocks per SM) measured fastest on B200 at 256³ among 2-8 planes
+// and 2-5 stages.
 #ifndef PM_HALL_TMA_PLANES
-#define PM_HALL_TMA_PLANES 2
+#define PM_HALL_TMA_PLANES 8
 #endif
 #ifndef PM_HALL_TMA_STAGES
-#define PM_HALL_TMA_STAGES 4
+#define PM_HALL_TMA_STAGES 2
+#endif
+#ifndef PM_HALL_TMA_MIN_BLOCKS
+#define PM_HALL_TMA_MIN_BLOCKS 2
 #endif
 constexpr int kHallTmaPlanes = PM_HALL_TMA_PLANES;
 constexpr int kHallTmaStages = PM_HALL_TMA_STAGES;
@@ -103,7 +108,7 @@ __device__ __forceinline__ void hall_tma_issue(const HallMaps& m, unsigned stage
 }
 
 template <int P, int S, bool HET>
-static __global__ void __launch_bounds__(256, 3) hall_tma_step(HallArgs<float> a, const __grid_constant__ HallMaps m) {
+static __global__ void __launch_bounds__(256, PM_HALL_TMA_MIN_BLOCKS) hall_tma_step(HallArgs<float> a, const __grid_constant__ HallMaps m) {
     DevState* st = a.st;
     if (st->violated) return;
     using St = HallTmaStage<P>;

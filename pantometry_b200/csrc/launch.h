@@ -21,11 +21,12 @@ constexpr int kMeasureBlocks = 592;  // 4 × 148 SMs, for the flat element-wise 
 
 // The z-chunk that spreads the tiles most evenly over `resident` blocks, preferring deeper
 // chunks (fewer re-read planes) when the balance is equal.
-inline int choose_zc(int nx, int ny, int nz, unsigned resident) {
-    int best = 4;
+// `lo`: the smallest chunk a kernel takes (a multiple of the planes it streams per stage).
+inline int choose_zc(int nx, int ny, int nz, unsigned resident, int lo = 4) {
+    int best = lo;
     double best_score = -1.0;
     for (int zc : {4, 8, 16, 32}) {
-        if (zc > nz && zc != 4) continue;
+        if (zc < lo || (zc > nz && zc != lo)) continue;
         Tiles t = make_tiles(nx, ny, nz, zc);
         double per = (double)t.ntiles / resident;
         double rounds = per < 1.0 ? 1.0 : (double)((t.ntiles + resident - 1) / resident);
