@@ -118,6 +118,7 @@ def _declare(L):
         "or_hall_get": (None, [p, dp, dp, dp, dp, dp]),
         "or_hall_ledger": (None, [p, dp, dp, dp, dp, dp]),
         "or_hall_max_stable_dt": (d, [p]),
+        "or_hall_set_speed_blocks": (None, [p, C.c_int, dp, ll]),
         "or_hall_checkpoint": (None, [p]),
         "or_hall_restore": (None, [p]),
         "or_yee_new": (p, [C.c_char_p, i, i, i, d, d, d, d]),
@@ -288,6 +289,12 @@ class Hall(_Box):
         w = np.ascontiguousarray(wave, dtype=np.float64)
         self._wave = w
         lib().or_hall_set_source(self._h, node, _dp(w), w.size)
+
+    def set_speed_blocks(self, block, speeds):
+        """Extension: one sound speed per cubic block of `block` nodes a side (x-fastest)."""
+        s = np.ascontiguousarray(speeds, dtype=np.float64)
+        self._speeds = s
+        lib().or_hall_set_speed_blocks(self._h, int(block), _dp(s), s.size)
 
     def max_stable_dt(self):
         return lib().or_hall_max_stable_dt(self._h)

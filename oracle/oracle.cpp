@@ -397,20 +397,37 @@ struct Hall {
     long long steps_taken = 0;
     double injected = 0.0;
     double last_delta = 0.0;
+    // Extension: a sound speed per cubic block of `block` nodes a side (the heterogeneous
+    // medium of the 1024³ configuration); `Hall` itself has one speed (hall.rs:82-83).
+    int block = 0, nbx = 0, nby = 0;
+    std::vector<double> speeds;
 
     size_t at(int i, int j, int k) const { return i + (size_t)nx * (j + (size_t)ny * k); }
+    double speed_at(int i, int j, int k) const {
+        if (block <= 0) return speed;
+        return speeds[(size_t)(i / block) + (size_t)nbx * ((size_t)(j / block) + (size_t)nby * (k / block))];
+    }
+    double max_speed() const {
+        double c = speed;
+        if (block > 0) { c = speeds[0]; for (double v : speeds) c = v > c ? v : c; }
+        return c;
+    }
 
     // hall.rs:334-384
     double invariant_si() const {
         double volume = dx * dx * dx;
         double rc2 = density * speed * speed;
-        if (rc2 <= 0.0) return 0.0;
+        if (block <= 0 && rc2 <= 0.0) return 0.0;
         double total = 0.0;
         for (int k = 0; k < nz; ++k)
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < nx; ++i) {
                     double share = 1.0 / (wall_weight(i, nx) * wall_weight(j, ny) * wall_weight(k, nz));
                     size_t idx = at(i, j, k);
+                    if (block > 0) {
+                        double c = speed_at(i, j, k);
+                        rc2 = density * c * c;
+                    }
                     total += share * p[idx] * pp[idx] / (2.0 * rc2) * volume;
                 }
         double half_rho = 0.5 * density;
@@ -438,7 +455,7 @@ struct Hall {
         return total;
     }
 
-    double courant(double dt) const { return speed * dt * std::sqrt(3.0) / dx; }  // hall.rs:319
+    double courant(double dt) const { return max_speed() * dt * std::sqrt(3.0) / dx; }  // hall.rs:319
 
     // Source bookkeeping: adding δ at node s after the pressure update moves the discrete
     // invariant by share·δ·p_prev·V/(2ρc²) at once, and by share·δ·p·V/(2ρc²) one step later
@@ -447,7 +464,8 @@ struct Hall {
     double node_weight(size_t idx) const {
         int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((size_t)nx * ny));
         double share = 1.0 / (wall_weight(i, nx) * wall_weight(j, ny) * wall_weight(k, nz));
-        double rc2 = density * speed * speed;
+        double c = speed_at(i, j, k);
+        double rc2 = density * c * c;
         return share * (dx * dx * dx) / (2.0 * rc2);
     }
 
@@ -496,6 +514,10 @@ struct Hall {
                     double lo_z = k > 0 ? vz[i + (size_t)nx * (j + (size_t)ny * (k - 1))] : 0.0;
                     double hi_z = k + 1 < nz ? vz[i + (size_t)nx * (j + (size_t)ny * k)] : 0.0;
                     size_t idx = at(i, j, k);
+                    if (block > 0) {
+                        double c = speed_at(i, j, k);
+                        scale = h * (density * c * c) / dx;
+                    }
                     p[idx] -= scale * (wall_weight(i, nx) * (hi_x - lo_x) +
                                        wall_weight(j, ny) * (hi_y - lo_y) +
                                        wall_weight(k, nz) * (hi_z - lo_z));
@@ -1203,8 +1225,19 @@ void or_hall_ledger(void* p, double* total, double* scale, double* invariant, do
 }
 double or_hall_max_stable_dt(void* p) {
     Hall* h = (Hall*)p;
-    if (h->speed <= 0.0) return INF;
-    return h->dx / (h->speed * std::sqrt(3.0));
+    const double c = h->max_speed();
+    if (c <= 0.0) return INF;
+    return h->dx / (c * std::sqrt(3.0));
+}
+// Extension: one speed per cubic block of `block` nodes a side, blocks in x-fastest order; the
+// datum of the present state is re-taken under the new weights.
+void or_hall_set_speed_blocks(void* p, int block, const double* speeds, long long n) {
+    Hall* h = (Hall*)p;
+    h->block = block;
+    h->nbx = (h->nx + block - 1) / block;
+    h->nby = (h->ny + block - 1) / block;
+    h->speeds.assign(speeds, speeds + n);
+    if (!h->staggered) h->datum = h->invariant_si();
 }
 void or_hall_checkpoint(void* p) {
     Hall* h = (Hall*)p;
