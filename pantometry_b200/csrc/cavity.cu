@@ -41,6 +41,11 @@ struct Cavity : Handle {
     DBuf sf[6];
     bool s_started = false;
     double s_dissipated = 0.0;
+    // FP32 cavities of one medium keep all six components on the padded lattice (row pitch L)
+    // and step with the TMA-staged kernel (yee_tma.cuh); maps[par] describe parity par's fields
+    bool tma = false;
+    unsigned L = 0;
+    YeeMaps maps[2];
 
     size_t count(int q) const {
         switch (q) {
@@ -53,6 +58,14 @@ struct Cavity : Handle {
         }
     }
     size_t cells() const { return (size_t)nx * ny * nz; }
+    // elements held on the device per component
+    size_t lattice() const { return (size_t)L * (ny + 1) * (nz + 1); }
+    size_t dcount(int q) const { return tma ? lattice() : count(q); }
+    void extents(int q, int& ex, int& ey, int& ez) const {
+        ex = (q == 0 || q == 4 || q == 5) ? nx : nx + 1;
+        ey = (q == 1 || q == 3 || q == 5) ? ny : ny + 1;
+        ez = (q == 2 || q == 3 || q == 4) ? nz : nz + 1;
+    }
     size_t esize() const { return precision == PM_PLAIN_F64 ? 8 : 4; }
     double volume() const { return dx * (dx * dx); }  // dx.powi(3)
     double permittivity() const { return kEpsilon0 * eps_r; }
@@ -248,6 +261,17 @@ struct Cavity : Handle {
 
     pm_status put(int q, const double* src_host) {
         const size_t n = count(q);
+        if (tma) {  // into the padded lattice, padding zero
+            PM_CUDA(cudaMemsetAsync(f[parity][q].p, 0, lattice() * 4, stream()));
+            if (!src_host) return PM_OK;
+            if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(n * 8));
+            PM_CUDA(cudaMemcpyAsync(stage.p, src_host, n * 8, cudaMemcpyHostToDevice, stream()));
+            int ex, ey, ez;
+            extents(q, ex, ey, ez);
+            PM_CUDA(launch_yee_relayout(stage.p, true, f[parity][q].p, false, ex, ey, ez, L, ny + 1, 1, stream()));
+            PM_CUDA(cudaStreamSynchronize(stream()));
+            return PM_OK;
+        }
         if (!src_host) {
             PM_CUDA(cudaMemsetAsync(f[parity][q].p, 0, n * esize(), stream()));
             return PM_OK;
@@ -265,6 +289,15 @@ struct Cavity : Handle {
     pm_status get(int q, double* dst_host) {
         if (!dst_host) return PM_OK;
         const size_t n = count(q);
+        if (tma) {
+            if (!stage.p || stage.bytes < n * 8) PM_CUDA(stage.alloc(n * 8));
+            int ex, ey, ez;
+            extents(q, ex, ey, ez);
+            PM_CUDA(launch_yee_relayout(f[parity][q].p, false, stage.p, true, ex, ey, ez, L, ny + 1, 0, stream()));
+            PM_CUDA(cudaMemcpyAsync(dst_host, stage.p, n * 8, cudaMemcpyDeviceToHost, stream()));
+            PM_CUDA(cudaStreamSynchronize(stream()));
+            return PM_OK;
+        }
         if (precision == PM_PLAIN_F64) {
             PM_CUDA(cudaMemcpyAsync(dst_host, f[parity][q].p, n * 8, cudaMemcpyDeviceToHost, stream()));
         } else {
@@ -276,8 +309,100 @@ struct Cavity : Handle {
         return PM_OK;
     }
 
+    // Run `fn` on the present state in the reference layout. On a padded cavity the state is
+    // gathered into the other ping-pong set (free between steps), `fn` sees that set as the
+    // present one, and when `writes` the result is scattered back.
+    template <typename F>
+    pm_status with_reference_layout(bool writes, F fn) {
+        if (!tma) return fn();
+        const int home = parity;
+        for (int q = 0; q < 6; ++q) {
+            int ex, ey, ez;
+            extents(q, ex, ey, ez);
+            PM_CUDA(launch_yee_relayout(f[home][q].p, false, f[home ^ 1][q].p, false, ex, ey, ez, L, ny + 1, 0, stream()));
+        }
+        parity = home ^ 1;
+        tma = false;
+        pm_status s = fn();
+        tma = true;
+        parity = home;
+        if (s != PM_OK) return s;
+        if (writes) {
+            for (int q = 0; q < 6; ++q) {
+                int ex, ey, ez;
+                extents(q, ex, ey, ez);
+                PM_CUDA(cudaMemsetAsync(f[home][q].p, 0, lattice() * 4, stream()));
+                PM_CUDA(launch_yee_relayout(f[home ^ 1][q].p, false, f[home][q].p, false, ex, ey, ez, L, ny + 1, 1, stream()));
+            }
+        }
+        for (int q = 0; q < 6; ++q)  // the other set back to a zero-padded lattice
+            PM_CUDA(cudaMemsetAsync(f[home ^ 1][q].p, 0, lattice() * 4, stream()));
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        return PM_OK;
+    }
+
+    // Tensor maps of both parities' six components over the padded lattice.
+    pm_status build_maps() {
+        constexpr unsigned P = kYeeTmaPlanes;
+        for (int q = 0; q < 2; ++q) {
+            const int d0 = (int)L, d1 = ny + 1, d2 = nz + 1;
+            if (!hall_tma_map(&maps[q].ex, f[q][0].p, d0, d1, d2, 36, 10, P + 1) ||
+                !hall_tma_map(&maps[q].ey, f[q][1].p, d0, d1, d2, 40, 9, P + 1) ||
+                !hall_tma_map(&maps[q].ez, f[q][2].p, d0, d1, d2, 40, 10, P) ||
+                !hall_tma_map(&maps[q].hx, f[q][3].p, d0, d1, d2, 32, 9, P) ||
+                !hall_tma_map(&maps[q].hy, f[q][4].p, d0, d1, d2, 36, 8, P) ||
+                !hall_tma_map(&maps[q].hz, f[q][5].p, d0, d1, d2, 36, 9, P))
+                return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a cavity field");
+        }
+        return PM_OK;
+    }
+
+    // The padded cavity back to the reference layout (before per-cell media, which only the
+    // cp.async kernel reads). The state goes through the host once; a checkpoint taken in the
+    // other layout is dropped.
+    pm_status leave_tma() {
+        if (!tma) return PM_OK;
+        std::vector<double> v[6];
+        pm_status s;
+        for (int q = 0; q < 6; ++q) {
+            v[q].resize(count(q));
+            if ((s = get(q, v[q].data())) != PM_OK) return s;
+        }
+        tma = false;
+        drop_graphs();
+        has_saved = false;
+        for (int q = 0; q < 6; ++q)
+            if ((s = put(q, v[q].data())) != PM_OK) return s;
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        return PM_OK;
+    }
+
+    // Step arguments of the TMA kernel: the cp.async kernel's, with its own tiling (chunks of
+    // P·m − 1 planes, so a chunk and the plane below it fill whole stages).
+    YeeStepArgs<float> targs(int par, double dt) const {
+        YeeStepArgs<float> a = sargs<float>(par, dt);
+        const unsigned w = wave_of(kYeeTma);
+        const int X = nx + 1, Y = ny + 1, Z = nz + 1;
+        int best = 2 * kYeeTmaPlanes - 1;
+        double best_score = -1.0;
+        for (int mlt : {2, 4, 8, 16}) {
+            const int zc = kYeeTmaPlanes * mlt - 1;
+            if (zc > Z && zc != 2 * kYeeTmaPlanes - 1) continue;
+            const Tiles t = make_tiles(X, Y, Z, zc);
+            const double per = (double)t.ntiles / w;
+            const double rounds = per < 1.0 ? 1.0 : (double)((t.ntiles + w - 1) / w);
+            const double balance = per < 1.0 ? per : per / rounds;
+            const double score = balance * (1.0 - 1.0 / (2.0 * zc));
+            if (score > best_score + 1e-9) { best_score = score; best = zc; }
+        }
+        a.tiles = make_tiles(X, Y, Z, best);
+        a.nblocks = grid_for(a.tiles, w);
+        return a;
+    }
+
     // ½εE² and ½μH² of the present state.
     pm_status measure_naive(double* electric, double* magnetic) {
+        if (tma) return with_reference_layout(false, [&]() { return measure_naive(electric, magnetic); });
         if (!energies.p) PM_CUDA(energies.alloc(2 * sizeof(double)));
         if (precision == PM_PLAIN_F64) PM_CUDA(launch_yee_measure<double>(hargs<double>(0.0, 0), energies.as<double>(), stream()));
         else PM_CUDA(launch_yee_measure<float>(hargs<float>(0.0, 0), energies.as<double>(), stream()));
@@ -358,12 +483,19 @@ pm_status pm_cavity_create(const pm_cavity_desc* d, pm_cavity** out) {
     c->uniform_media();
     pm_status s = c->init(d->device, 0);
     if (s != PM_OK) { delete c; return s; }
-    for (int par = 0; par < 2; ++par)
-        for (int q = 0; q < 6; ++q) {
-            cudaError_t e = c->f[par][q].alloc(c->count(q) * c->esize());
-            if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMalloc cavity fields"); }
-            cudaMemset(c->f[par][q].p, 0, c->count(q) * c->esize());
-        }
+    c->L = (unsigned)((c->nx + 1 + 3) & ~3);
+    c->tma = c->precision == PM_FIELDS_F32 && c->lattice() < (1ull << 32);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        for (int par = 0; par < 2; ++par)
+            for (int q = 0; q < 6; ++q) {
+                cudaError_t e = c->f[par][q].alloc(c->dcount(q) * c->esize());
+                if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMalloc cavity fields"); }
+                cudaMemset(c->f[par][q].p, 0, c->dcount(q) * c->esize());
+            }
+        // a shape the driver will not tile steps with the cp.async kernel on the reference layout
+        if (!c->tma || c->build_maps() == PM_OK) break;
+        c->tma = false;
+    }
     *out = reinterpret_cast<pm_cavity*>(c);
     s = c->reset_ledger();
     if (s != PM_OK) { delete c; *out = nullptr; }
@@ -384,6 +516,8 @@ pm_status pm_cavity_fill_cells(pm_cavity* cp, const double* eps_r, const double*
         if (mu_r) c->cell_mu[q] = mu_r[q];
         if (sigma) c->cell_sig[q] = sigma[q];
     }
+    pm_status ls = c->leave_tma();
+    if (ls != PM_OK) return ls;
     c->uniform = false;
     c->refresh_media();
     pm_status s = c->upload_media();
@@ -494,21 +628,26 @@ pm_status pm_cavity_release_mode(pm_cavity* cp, int m_in, int p_in, double ampli
     c->host_state->has_invariant = 0;
     c->host_state->steps = 0;
     if ((s = c->write_state()) != PM_OK) return s;
-    for (int q = 0; q < 6; ++q)
-        if ((s = c->put(q, q == 1 ? ey.data() : nullptr)) != PM_OK) return s;
-    // H = +(dt/2μ)∇×E with the scheme's own stencil, then the invariant from a trial step
-    if ((s = c->launch_h((-0.5 * dt) / c->dx, 0, c->stream())) != PM_OK) return s;
+    s = c->with_reference_layout(true, [&]() -> pm_status {
+        pm_status r;
+        for (int q = 0; q < 6; ++q)
+            if ((r = c->put(q, q == 1 ? ey.data() : nullptr)) != PM_OK) return r;
+        // H = +(dt/2μ)∇×E with the scheme's own stencil, then the invariant from a trial step
+        if ((r = c->launch_h((-0.5 * dt) / c->dx, 0, c->stream())) != PM_OK) return r;
+        for (int q = 0; q < 3; ++q) {
+            const size_t bytes = c->count(q + 3) * c->esize();
+            if (!c->keep[q].p) PM_CUDA(c->keep[q].alloc(bytes));
+            PM_CUDA(cudaMemcpyAsync(c->keep[q].p, c->f[c->parity][q + 3].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
+        }
+        if ((r = c->launch_h(dt / c->dx, 1, c->stream())) != PM_OK) return r;
+        for (int q = 0; q < 3; ++q)
+            PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q + 3].p, c->keep[q].p, c->count(q + 3) * c->esize(),
+                                    cudaMemcpyDeviceToDevice, c->stream()));
+        PM_CUDA(cudaStreamSynchronize(c->stream()));
+        return PM_OK;
+    });
+    if (s != PM_OK) return s;
     c->started = true;
-    for (int q = 0; q < 3; ++q) {
-        const size_t bytes = c->count(q + 3) * c->esize();
-        if (!c->keep[q].p) PM_CUDA(c->keep[q].alloc(bytes));
-        PM_CUDA(cudaMemcpyAsync(c->keep[q].p, c->f[c->parity][q + 3].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
-    }
-    if ((s = c->launch_h(dt / c->dx, 1, c->stream())) != PM_OK) return s;
-    for (int q = 0; q < 3; ++q)
-        PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q + 3].p, c->keep[q].p, c->count(q + 3) * c->esize(), cudaMemcpyDeviceToDevice,
-                                c->stream()));
-    PM_CUDA(cudaStreamSynchronize(c->stream()));
     return c->reset_ledger();
 }
 
@@ -560,11 +699,13 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
     if (s != PM_OK) return s;
     const long long before = c->host_state->steps;
     if (!c->started) {  // cavity.rs:1486-1489
-        if ((s = c->launch_h((0.5 * h) / c->dx, 0, c->stream())) != PM_OK) return s;
+        s = c->with_reference_layout(true, [&]() { return c->launch_h((0.5 * h) / c->dx, 0, c->stream()); });
+        if (s != PM_OK) return s;
         c->started = true;
     }
     s = c->run_steps(nsteps, dt, true, [c, h](int par, cudaStream_t st) {
         if (c->precision == PM_PLAIN_F64) return launch_yee_step<double>(c->sargs<double>(par, h), st);
+        if (c->tma) return launch_yee_tma(c->targs(par, h), c->L, c->maps[par], st);
         return launch_yee_step<float>(c->sargs<float>(par, h), st);
     });
     if (s != PM_OK) return s;
@@ -599,8 +740,8 @@ pm_status pm_cavity_checkpoint(pm_cavity* cp) {
     Cavity* c = reinterpret_cast<Cavity*>(cp);
     CAV_GUARD(c);
     for (int q = 0; q < 6; ++q) {
-        const size_t bytes = c->count(q) * c->esize();
-        if (!c->sf[q].p) PM_CUDA(c->sf[q].alloc(bytes));
+        const size_t bytes = c->dcount(q) * c->esize();
+        if (!c->sf[q].p || c->sf[q].bytes < bytes) PM_CUDA(c->sf[q].alloc(bytes));
         PM_CUDA(cudaMemcpyAsync(c->sf[q].p, c->f[c->parity][q].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
     }
     pm_status s = c->read_state();
@@ -616,7 +757,7 @@ pm_status pm_cavity_restore(pm_cavity* cp) {
     CAV_GUARD(c);
     if (!c->has_saved) return PM_OK;
     for (int q = 0; q < 6; ++q)
-        PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q].p, c->sf[q].p, c->count(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
+        PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q].p, c->sf[q].p, c->dcount(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
     pm_status s = c->read_state();
     if (s != PM_OK) return s;
     c->started = c->s_started;

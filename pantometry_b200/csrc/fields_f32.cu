@@ -130,6 +130,38 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
+    constexpr int P = kYeeTmaPlanes, S = kYeeTmaStages;
+    static bool attr = false;
+    const int smem = (int)yee_tma_smem_bytes();
+    if (!attr) {
+        cudaFuncSetAttribute(yee_tma_step<P, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(yee_tma_step<P, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    if (a.solid)
+        yee_tma_step<P, S, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+    else
+        yee_tma_step<P, S, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,
+                                unsigned L, unsigned ny1, int to_padded, cudaStream_t s) {
+    if (src_f64 && !dst_f64)
+        yee_relayout<double, float><<<kMeasureBlocks, 256, 0, s>>>(static_cast<const double*>(src), static_cast<float*>(dst), ex, ey,
+                                                                   ez, L, ny1, to_padded);
+    else if (!src_f64 && dst_f64)
+        yee_relayout<float, double><<<kMeasureBlocks, 256, 0, s>>>(static_cast<const float*>(src), static_cast<double*>(dst), ex, ey,
+                                                                   ez, L, ny1, to_padded);
+    else if (!src_f64 && !dst_f64)
+        yee_relayout<float, float><<<kMeasureBlocks, 256, 0, s>>>(static_cast<const float*>(src), static_cast<float*>(dst), ex, ey,
+                                                                  ez, L, ny1, to_padded);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -146,6 +178,12 @@ int occupancy_f32(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
         case kEnsF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false>, 256, 0); break;
+        case kYeeTma:
+            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false>, 256,
+                                                              yee_tma_smem_bytes());
+            break;
         case kHallTma:
             cudaFuncSetAttribute(hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_tma_smem_bytes());

@@ -10,6 +10,7 @@
 #include "yee_kernels.cuh"
 #include "ensemble_kernels.cuh"
 #include "hall_tma.cuh"
+#include "yee_tma.cuh"
 
 namespace pm {
 
@@ -44,7 +45,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -75,6 +76,13 @@ inline size_t hall_tma_smem_bytes() {
 // Encode the tensor map of one f32 field of an nx × ny × nz hall (row pitch nx·4 bytes) with the
 // given box; false if the driver refuses it.
 bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz);
+// The FP32 uniform-medium cavity step staged by TMA (padded lattice of row pitch L).
+cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s);
+inline size_t yee_tma_smem_bytes() { return yee_tma_smem_bytes_for<kYeeTmaPlanes>(kYeeTmaStages); }
+// One component between the reference layout and the padded lattice (see yee_relayout);
+// src_f64 / dst_f64 select double or float for each side.
+cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,
+                                unsigned L, unsigned ny1, int to_padded, cudaStream_t s);
 // One ensemble step (measure = false) or the opening ledgers (measure = true) over the brick list.
 template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool measure, unsigned nblocks, cudaStream_t s);
 

@@ -1,0 +1,297 @@
+// Cavity step, FP32 form for one uniform medium (with or without obstacles), staged by the Tensor
+// Memory Accelerator. The arithmetic per edge and face is yee_step's for a uniform medium
+// (cavity.rs:1346-1501): H⁺ from Eⁿ, the invariant ½ε|Eⁿ|² + ½μ H⁻·H⁺, then Eⁿ⁺¹ from H⁺.
+//
+// Layout. The handle keeps all six components on the (nx+1) × (ny+1) × (nz+1) node lattice with
+// one index n = i + L·(j + (ny+1)·k), L = nx+1 rounded up to a multiple of 4 (so every row pitch
+// is a multiple of 16 bytes, as TMA requires). A component's lattice positions outside its own
+// extent (cavity.rs:112-123) are padding: zero, never written.
+//
+// Walk. Tiles are 32 × 8 columns of the lattice over a z-chunk, taken by a persistent grid in
+// order; a tile's chunk of planes k0 .. k1−1 is streamed from k0 − 1 (whose H⁺ the first plane's
+// Eⁿ⁺¹ needs) P planes at a time. For a stage of planes kb .. kb+P−1 one thread issues six tiled
+// TMA loads into a ring of S shared-memory stages (boxes start at x0 − 4 or x0, 16-byte aligned;
+// the hardware fills outside the lattice with zeros):
+//   ex  x0−4 .. x0+31, y0−1 .. y0+8, kb .. kb+P      ey  x0−4 .. x0+35, y0−1 .. y0+7, kb .. kb+P
+//   ez  x0−4 .. x0+35, y0−1 .. y0+8, kb .. kb+P−1    hx  x0   .. x0+31, y0−1 .. y0+7, kb .. kb+P−1
+//   hy  x0−4 .. x0+31, y0   .. y0+7, kb .. kb+P−1    hz  x0−4 .. x0+31, y0−1 .. y0+7, kb .. kb+P−1
+// Per plane: H⁺ on the tile's own faces and on the x0−1 column / y0−1 row its edges need, into a
+// double-buffered shared plane; one barrier; Eⁿ⁺¹ on the tile's own edges, with H⁺ of the plane
+// below carried in registers. Completion of each stage is one mbarrier; every wait is bounded.
+#pragma once
+
+#include <cuda.h>
+
+#include "hall_tma.cuh"
+#include "yee_kernels.cuh"
+
+namespace pm {
+
+struct YeeMaps {
+    CUtensorMap ex, ey, ez, hx, hy, hz;
+};
+
+#ifndef PM_YEE_TMA_PLANES
+#define PM_YEE_TMA_PLANES 4
+#endif
+#ifndef PM_YEE_TMA_STAGES
+#define PM_YEE_TMA_STAGES 2
+#endif
+constexpr int kYeeTmaPlanes = PM_YEE_TMA_PLANES;
+constexpr int kYeeTmaStages = PM_YEE_TMA_STAGES;
+
+constexpr unsigned round128(unsigned b) { return (b + 127u) & ~127u; }
+
+// Byte offsets of the six boxes inside one stage (each 128-byte aligned).
+template <int P>
+struct YeeTmaLayout {
+    static constexpr unsigned EX_B = (P + 1) * 10 * 36 * 4, EY_B = (P + 1) * 9 * 40 * 4, EZ_B = P * 10 * 40 * 4,
+                              HX_B = P * 9 * 32 * 4, HY_B = P * 8 * 36 * 4, HZ_B = P * 9 * 36 * 4;
+    static constexpr unsigned EX = 0, EY = round128(EX + EX_B), EZ = round128(EY + EY_B), HX = round128(EZ + EZ_B),
+                              HY = round128(HX + HX_B), HZ = round128(HY + HY_B), BYTES = round128(HZ + HZ_B);
+    static constexpr unsigned TX = EX_B + EY_B + EZ_B + HX_B + HY_B + HZ_B;  // bytes the six loads deliver
+};
+
+template <int P>
+inline size_t yee_tma_smem_bytes_for(int S) {
+    return (size_t)S * YeeTmaLayout<P>::BYTES + 2 * sizeof(YeeHp<float>) + 8 * (size_t)S;
+}
+
+struct YeeTmaCursor {
+    unsigned t;
+    int x0, y0, k0, k1, kb;
+    bool valid;
+};
+__device__ __forceinline__ void yee_tma_at(YeeTmaCursor& c, const Tiles& T, unsigned t) {
+    c.t = t;
+    c.valid = t < (unsigned)T.ntiles;
+    if (!c.valid) return;
+    const unsigned r = t / (unsigned)T.ntx;
+    const unsigned tz = r / (unsigned)T.nty;
+    c.x0 = (int)(t - r * (unsigned)T.ntx) * 32;
+    c.y0 = (int)(r - tz * (unsigned)T.nty) * 8;
+    c.k0 = (int)tz * T.zc;
+    c.k1 = min(T.nz, c.k0 + T.zc);  // T.nz = nz + 1 lattice planes
+    c.kb = c.k0 > 0 ? c.k0 - 1 : 0;
+}
+__device__ __forceinline__ void yee_tma_next(YeeTmaCursor& c, const Tiles& T, int planes) {
+    c.kb += planes;
+    if (c.kb >= c.k1) yee_tma_at(c, T, c.t + gridDim.x);
+}
+
+template <int P>
+__device__ __forceinline__ void yee_tma_issue(const YeeMaps& m, unsigned stage, unsigned bar, const YeeTmaCursor& c) {
+    using Lay = YeeTmaLayout<P>;
+    mbar_expect_tx(bar, Lay::TX);
+    tma_load_3d(stage + Lay::EX, &m.ex, c.x0 - 4, c.y0 - 1, c.kb, bar);
+    tma_load_3d(stage + Lay::EY, &m.ey, c.x0 - 4, c.y0 - 1, c.kb, bar);
+    tma_load_3d(stage + Lay::EZ, &m.ez, c.x0 - 4, c.y0 - 1, c.kb, bar);
+    tma_load_3d(stage + Lay::HX, &m.hx, c.x0, c.y0 - 1, c.kb, bar);
+    tma_load_3d(stage + Lay::HY, &m.hy, c.x0 - 4, c.y0, c.kb, bar);
+    tma_load_3d(stage + Lay::HZ, &m.hz, c.x0 - 4, c.y0 - 1, c.kb, bar);
+}
+
+template <int P, int S, bool SOLID>
+static __global__ void __launch_bounds__(256, 2) yee_tma_step(YeeStepArgs<float> a, unsigned L,
+                                                             const __grid_constant__ YeeMaps m) {
+    DevState* st = a.st;
+    if (st->violated) return;
+    using Lay = YeeTmaLayout<P>;
+    extern __shared__ __align__(128) unsigned char yee_tma_smem[];
+    const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(yee_tma_smem));
+    YeeHp<float>* hp = reinterpret_cast<YeeHp<float>*>(yee_tma_smem + S * Lay::BYTES);
+    const unsigned bar_base = ring_base + S * Lay::BYTES + 2 * (unsigned)sizeof(YeeHp<float>);
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
+    const Tiles T = a.tiles;
+    const long long step = st->steps;
+    const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
+    const double dt = a.dt;
+    const bool lossy = a.sigma_u[0] != 0.0;
+    // Σ w|Eⁿ|², Σ w H⁺·H⁻ (the uniform ε and μ applied at the end), Joule loss, source work
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(bar_base + 8 * s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    YeeTmaCursor pf, cc;
+    yee_tma_at(cc, T, blockIdx.x);
+    int issued = 0;
+    if (tid == 0) {
+        yee_tma_at(pf, T, blockIdx.x);
+        for (; issued < S - 1 && pf.valid; ++issued) {
+            yee_tma_issue<P>(m, ring_base + issued * Lay::BYTES, bar_base + 8 * issued, pf);
+            yee_tma_next(pf, T, P);
+        }
+    }
+    const float ch = a.ch;
+    const float dec0 = a.decay[0], gain0 = a.gain[0];
+    const double sig0 = a.sigma_u[0];
+    const unsigned ny1 = (unsigned)ny + 1;
+    float hx_below = 0.0f, hy_below = 0.0f;  // H⁺ of this column at the plane below
+    int hpar = 0;                            // which H⁺ plane buffer the present plane fills
+    bool timed_out = false;
+    int it = 0;
+    while (cc.valid) {
+        const int slot = it % S;
+        const bool got = mbar_wait(bar_base + 8 * slot, (unsigned)((it / S) & 1));
+        if (!__syncthreads_and(got)) {
+            timed_out = true;
+            break;
+        }
+        if (tid == 0 && pf.valid) {
+            const int fill = (it + S - 1) % S;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            yee_tma_issue<P>(m, ring_base + fill * Lay::BYTES, bar_base + 8 * fill, pf);
+            yee_tma_next(pf, T, P);
+            ++issued;
+        }
+        const unsigned char* sb = yee_tma_smem + slot * Lay::BYTES;
+        const float(*EX)[10][36] = reinterpret_cast<const float(*)[10][36]>(sb + Lay::EX);
+        const float(*EY)[9][40] = reinterpret_cast<const float(*)[9][40]>(sb + Lay::EY);
+        const float(*EZ)[10][40] = reinterpret_cast<const float(*)[10][40]>(sb + Lay::EZ);
+        const float(*HX)[9][32] = reinterpret_cast<const float(*)[9][32]>(sb + Lay::HX);
+        const float(*HY)[8][36] = reinterpret_cast<const float(*)[8][36]>(sb + Lay::HY);
+        const float(*HZ)[9][36] = reinterpret_cast<const float(*)[9][36]>(sb + Lay::HZ);
+        const int i = cc.x0 + tx, j = cc.y0 + ty;
+        const bool in_x = i <= nx, in_y = j <= ny;
+        // node-centred half weights of the boundary samples (cavity.rs:766-772)
+        const double hi = (i == 0 || i == nx) ? 0.5 : 1.0, hj = (j == 0 || j == ny) ? 0.5 : 1.0;
+#pragma unroll 1
+        for (int h = 0; h < P; ++h) {
+            const int k = cc.kb + h;
+            if (k >= cc.k1) break;
+            const bool compute = k >= cc.k0;  // else the plane below the chunk: H⁺ only
+            const bool zin = k < nz;
+            const double hk = (k == 0 || k == nz) ? 0.5 : 1.0;
+            YeeHp<float>* hq = hp + hpar;
+            // ---- 1. H⁺ (cavity.rs:1346-1379) on own faces
+            const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
+            const float wx = HX[h][ty + 1][tx], wy = HY[h][ty][tx + 4], wz = HZ[h][ty + 1][tx + 4];
+            const float ex0 = EX[h][ty + 1][tx + 4], ey0 = EY[h][ty + 1][tx + 4], ez0 = EZ[h][ty + 1][tx + 4];
+            const float hxn = wx - ch * ((EZ[h][ty + 2][tx + 4] - ez0) - (EY[h + 1][ty + 1][tx + 4] - ey0));
+            const float hyn = wy - ch * ((EX[h + 1][ty + 1][tx + 4] - ex0) - (EZ[h][ty + 1][tx + 5] - ez0));
+            const float hzn = wz - ch * ((EY[h][ty + 1][tx + 5] - ey0) - (EX[h][ty + 2][tx + 4] - ex0));
+            hq->hx[ty + 1][tx] = hxn;
+            hq->hy[ty][tx + 1] = hyn;
+            hq->hz[ty + 1][tx + 1] = hzn;
+            const unsigned n = (unsigned)i + L * ((unsigned)j + ny1 * (unsigned)k);
+            if (compute) {
+                if (fx) a.neu[3][n] = hxn;
+                if (fy) a.neu[4][n] = hyn;
+                if (fz) a.neu[5][n] = hzn;
+                // ½μ H⁻·H⁺ (cavity.rs:854-905) and ½εEⁿ² (cavity.rs:776-847), weights only
+                double mm = 0.0, e = 0.0;
+                mm += fx ? hi * (double)hxn * (double)wx : 0.0;
+                mm += fy ? hj * (double)hyn * (double)wy : 0.0;
+                mm += fz ? hk * (double)hzn * (double)wz : 0.0;
+                const double dex = (double)ex0, dey = (double)ey0, dez = (double)ez0;
+                e += (i < nx && in_y) ? hj * hk * dex * dex : 0.0;
+                e += (in_x && j < ny) ? hi * hk * dey * dey : 0.0;
+                e += (in_x && in_y && zin) ? hi * hj * dez * dez : 0.0;
+                acc[0] += e;
+                acc[1] += mm;
+                // halo faces: the y0 − 1 row (hx, hz) by warp 7, the x0 − 1 column (hy, hz) by warp 6
+                if (ty == 7) {
+                    hq->hx[0][tx] = HX[h][0][tx] - ch * ((EZ[h][1][tx + 4] - EZ[h][0][tx + 4]) - (EY[h + 1][0][tx + 4] - EY[h][0][tx + 4]));
+                    hq->hz[0][tx + 1] = HZ[h][0][tx + 4] - ch * ((EY[h][0][tx + 5] - EY[h][0][tx + 4]) - (EX[h][1][tx + 4] - EX[h][0][tx + 4]));
+                }
+                if (ty == 6 && tx < 9) {
+                    const int r = tx;  // column x0 − 1, rows y0 − 1 .. y0 + 7
+                    if (r >= 1) hq->hy[r - 1][0] = HY[h][r - 1][3] - ch * ((EX[h + 1][r][3] - EX[h][r][3]) - (EZ[h][r][4] - EZ[h][r][3]));
+                    hq->hz[r][0] = HZ[h][r][3] - ch * ((EY[h][r][4] - EY[h][r][3]) - (EX[h][r + 1][3] - EX[h][r][3]));
+                }
+            }
+            __syncthreads();
+            // ---- 2. Eⁿ⁺¹ on own edges (cavity.rs:1383-1452): interior by the semi-implicit update,
+            // conducting walls 0 (cavity.rs:1239-1293), edges touching a solid cell 0 (cavity.rs:304-331)
+            if (compute) {
+                const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
+                const float cex = (hq->hz[ty + 1][tx + 1] - hq->hz[ty][tx + 1]) - (hyn - hy_below);
+                const float cey = (hxn - hx_below) - (hq->hz[ty + 1][tx + 1] - hq->hz[ty + 1][tx]);
+                const float cez = (hyn - hq->hy[ty][tx]) - (hxn - hq->hx[ty][tx]);
+                float vx = dec0 * ex0 + gain0 * cex;
+                float vy = dec0 * ey0 + gain0 * cey;
+                float vz = dec0 * ez0 + gain0 * cez;
+                if (i == a.src_i && j == a.src_j && k == a.src_k) {
+                    // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
+                    const double e = a.eps_src, ss = a.sig_src;
+                    vz = (float)((double)vz - (dt / e) / (1.0 + (ss * dt / (2.0 * e))) * jsrc);
+                    acc[3] += -(dt * a.volume) * jsrc * (0.5 * ((double)ez0 + (double)vz));
+                }
+                const bool lx = iy && iz, ly = ix && iz, lz = ix && iy;  // interior edges
+                vx = lx ? vx : 0.0f;
+                vy = ly ? vy : 0.0f;
+                vz = lz ? vz : 0.0f;
+                if (lossy) {
+                    const double mx = 0.5 * ((double)ex0 + (double)vx), my = 0.5 * ((double)ey0 + (double)vy),
+                                 mz = 0.5 * ((double)ez0 + (double)vz);
+                    acc[2] += (lx && i < nx && in_y) ? sig0 * mx * mx * dt * a.volume : 0.0;
+                    acc[2] += (ly && in_x && j < ny) ? sig0 * my * my * dt * a.volume : 0.0;
+                    acc[2] += (lz && in_x && in_y && zin) ? sig0 * mz * mz * dt * a.volume : 0.0;
+                }
+                if constexpr (SOLID) {
+                    if (touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) vx = 0.0f;
+                    if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) vy = 0.0f;
+                    if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) vz = 0.0f;
+                }
+                if (i < nx && in_y) a.neu[0][n] = vx;
+                if (in_x && j < ny) a.neu[1][n] = vy;
+                if (in_x && in_y && zin) a.neu[2][n] = vz;
+            }
+            hx_below = hxn;
+            hy_below = hyn;
+            hpar ^= 1;
+        }
+        yee_tma_next(cc, T, P);
+        ++it;
+    }
+    if (timed_out) {
+        // stop every later kernel of the call, and let the copies still in flight land before
+        // the block's shared memory is given up
+        if (tid == 0) {
+            st->violated = kDeviceTimeout;
+            for (int q = it; q < issued; ++q) mbar_wait(bar_base + 8 * (q % S), (unsigned)((q / S) & 1));
+        }
+        return;
+    }
+    if (finish_blocks<4>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
+        const double v = a.volume;
+        const double electric = 0.5 * (a.eps_u * acc[0]) * v;  // cavity.rs:846
+        const double paired = 0.5 * v * (a.mu_u * acc[1]);     // cavity.rs:885-904
+        st->invariant = electric + paired;
+        st->has_invariant = 1;
+        st->dissipated += fmax(acc[2], 0.0);
+        st->work_booked = st->work;
+        st->work += acc[3];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, st->invariant);
+        ledger_add(total, scale, st->dissipated);
+        if (a.src_i >= 0) ledger_add(total, scale, -st->work_booked);
+        st->part[0] = st->invariant;
+        st->part[1] = st->dissipated;
+        st->part[2] = -st->work_booked;
+        audit_and_commit(st, total, scale);
+    }
+}
+
+// Between the reference layout of one component (extents ex × ey × ez, x fastest) and the
+// padded lattice (row pitch L, ny1 rows per plane): to_padded = 1 scatters into the lattice
+// (whose padding the caller has zeroed), 0 gathers back.
+template <typename S, typename D>
+static __global__ void yee_relayout(const S* __restrict__ src, D* __restrict__ dst, int ex, int ey, int ez, unsigned L,
+                                    unsigned ny1, int to_padded) {
+    const size_t n = (size_t)ex * ey * ez;
+    for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = r % (size_t)ex, rest = r / (size_t)ex;
+        const size_t j = rest % (size_t)ey, k = rest / (size_t)ey;
+        const size_t p = i + (size_t)L * (j + (size_t)ny1 * k);
+        if (to_padded) dst[p] = (D)src[r];
+        else dst[r] = (D)src[p];
+    }
+}
+
+}  // namespace pm

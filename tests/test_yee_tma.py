@@ -1,0 +1,91 @@
+"""The FP32 cavity form staged by TMA (one uniform medium, with or without obstacles).
+
+Those cavities keep all six components on a padded node lattice and step with `yee_tma_step`;
+release, the starting half step and the naive energies run the reference-layout kernels on a
+relaid copy, and per-cell media (`fill_cells`) move the cavity back to the reference layout and
+the cp.async kernel. Checked against the f64 oracle with the f32 bounds of the other f32 tests
+through each of those paths.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import cavity_pair, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def field_err(fo, fg):
+    worst = 0.0
+    for k in fo:
+        assert fg[k].shape == fo[k].shape, k
+        scale = max(np.abs(fo[k]).max(), 1e-30)
+        worst = max(worst, np.abs(fg[k] - fo[k]).max() / scale)
+    return worst
+
+
+@pytest.mark.parametrize("counts", [(24, 20, 22), (13, 9, 7), (33, 5, 40), (4, 4, 4)])
+def test_yee_tma_mode_error_and_invariant(counts):
+    o, g = cavity_pair(counts, 1e-3, precision="f32")
+    dt = 0.99 * o.courant_limit()
+    o.release_mode((1, 1), 1.0, dt)
+    g.release_mode((1, 1), 1.0, dt)
+    l0 = g.ledger()["total"]
+    assert rel(l0, o.ledger()["total"]) < 1e-6
+    assert o.step(dt, 300) is None
+    assert g.step(dt, 300) is None  # a graph of 64 steps and single launches
+    assert field_err(o.fields(), g.fields()) < 1e-4
+    assert rel(g.ledger()["total"], o.ledger()["total"]) < 1e-5
+    assert rel(g.ledger()["total"], l0) < 1e-5
+    eo, go = o.energies(), g.energies()
+    assert rel(go[0], eo[0]) < 1e-4 and rel(go[1], eo[1]) < 1e-4
+
+
+def test_yee_tma_obstacle_and_source_audited():
+    counts, dx = (20, 17, 15), 1e-3
+    solid = np.zeros(counts[::-1], dtype=np.uint8)
+    solid[3:6, 4:7, 12:15] = 1
+    nx, ny, nz = counts
+    edge = 8 + (nx + 1) * (8 + (ny + 1) * 7)
+    o0 = oracle.Yee(counts, dx)
+    dt = 0.9 * o0.courant_limit()
+    t = (np.arange(400) + 0.5) * dt
+    cur = 1e6 * np.exp(-((t - 60 * dt) / (15 * dt)) ** 2) * np.sin(2 * math.pi * t / (20 * dt))
+    o, g = cavity_pair(counts, dx, solid=solid.reshape(-1), source=(edge, cur), precision="f32")
+    assert o.advance(dt, 400, tol=1e-9) is None
+    g.set_tolerance(1e-5)
+    assert g.step(dt, 400) is None
+    assert field_err(o.fields(), g.fields()) < 1e-4
+    lo, lg = o.ledger(), g.ledger()
+    assert abs(lg["total"] - lo["total"]) <= 1e-5 * lo["scale"]
+
+
+def test_yee_tma_checkpoint_restore():
+    _, g = cavity_pair((18, 12, 10), 1e-3, precision="f32")
+    dt = 0.9 * g.courant_limit()
+    g.release_mode((1, 1), 1.0, dt)
+    g.step(dt, 5)
+    g.checkpoint()
+    f0 = g.fields()
+    g.step(dt, 70)
+    g.restore()
+    f1 = g.fields()
+    for k in f0:
+        assert np.array_equal(f1[k], f0[k]), k
+
+
+def test_yee_fill_cells_leaves_the_padded_layout():
+    """Per-cell media after a few padded steps: the state carries over to the reference layout."""
+    counts, dx = (16, 12, 10), 1e-3
+    eps = np.where(np.arange(np.prod(counts)) % 7 == 0, 2.5, 1.0)
+    o, g = cavity_pair(counts, dx, precision="f32")
+    dt = 0.5 * o.courant_limit()
+    o.release_mode((1, 1), 1.0, dt)
+    g.release_mode((1, 1), 1.0, dt)
+    assert o.step(dt, 20) is None and g.step(dt, 20) is None
+    o.set_cells(eps_r=eps)
+    g.fill_cells(eps_r=eps)
+    assert o.step(dt, 100) is None and g.step(dt, 100) is None
+    assert field_err(o.fields(), g.fields()) < 1e-4
