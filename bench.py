@@ -477,6 +477,137 @@ def run_ensemble(args):
         dist.destroy_process_group()
 
 
+CAV_METRIC = "Gcell-updates/s (Yee cavity 384^3, FP32 fields + FP64 audit)"
+
+
+def run_cavity(args):
+    """Config 3: a vacuum cavity of n³ cells with conducting walls, Courant 0.99/√3, and the soft
+    z-current on the centre Ez edge; one bench step = `timesteps` steps, each with the fused FP64
+    invariant and the audit (tolerance 1e-5, FP32)."""
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import workloads as W
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = init_dist(local) if world > 1 else None
+    n, T = args.n, args.timesteps
+    cfg = W.yee_cavity(n, steps=T * (args.steps + args.warmup + 1))
+    cells = n ** 3
+    stream = torch.cuda.Stream(device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(precision, k, w, tol):
+        c = W.build_cavity(cfg, precision=precision, device=local)
+        c.set_stream(stream.cuda_stream)
+        c.set_tolerance(tol)
+        for _ in range(w):
+            v = c.step(cfg["dt"], T)
+            assert v is None, v
+        barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            start.record(stream)
+            for _ in range(k):
+                v = c.step(cfg["dt"], T)
+                assert v is None, v
+            end.record(stream)
+            torch.cuda.synchronize()
+        ms = start.elapsed_time(end)
+        barrier()
+        return c, max_over_ranks(ms), clk
+
+    c32, ms32, clk = timed("f32", args.steps, args.warmup, 1e-5)
+    del c32
+    plain_steps = max(1, args.steps // 2)
+    c64, ms64, _ = timed("f64", plain_steps, max(1, args.warmup // 2), 1e-9)
+    del c64
+    # FP32 against f64 after one bench step from the same start
+    a32, _, _ = timed("f32", 0, 1, 1e-5)
+    a64, _, _ = timed("f64", 0, 1, 1e-9)
+    f32f, f64f = a32.fields(), a64.fields()
+    # max |FP32 − f64| over E (and over H), relative to the largest |f64| value of that field
+    e_scale = max(float(np.abs(f64f[q]).max()) for q in ("ex", "ey", "ez"))
+    h_scale = max(float(np.abs(f64f[q]).max()) for q in ("hx", "hy", "hz"))
+    field_err = max(max(float(np.abs(f32f[q] - f64f[q]).max()) for q in ("ex", "ey", "ez")) / max(e_scale, 1e-300),
+                    max(float(np.abs(f32f[q] - f64f[q]).max()) for q in ("hx", "hy", "hz")) / max(h_scale, 1e-300))
+    l32, l64 = a32.ledger(), a64.ledger()
+    ledger_err = abs(l32["total"] - l64["total"]) / max(abs(l64["total"]), l64["scale"], 1e-300)
+    del a32, a64, f32f, f64f
+
+    # e2e through the C ABI with host buffers: the six fields from pinned memory, the run, the
+    # ledger and Ez back every bench step
+    c = W.build_cavity(cfg, precision="f32", device=local)
+    c.set_stream(stream.cuda_stream)
+    c.set_tolerance(1e-5)
+    shapes = c.shapes()
+    pinned = {q: torch.zeros(m, dtype=torch.float64, pin_memory=True).numpy() for q, m in shapes.items()}
+    ez_out = torch.empty(shapes["ez"], dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(args.warmup):
+        c.set_fields(pinned, started=False)
+        c.step(cfg["dt"], T)
+    barrier()
+    t0 = time.perf_counter()
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        c.set_fields(pinned, started=False)
+        v = c.step(cfg["dt"], T)
+        assert v is None, v
+        c.ledger()
+        c.download_component("ez", ez_out)
+    e0.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    e2e_ms = max_over_ranks(max(s0.elapsed_time(e0), wall_ms))
+    del c
+
+    peak, peak_kind = peaks()
+    per_launch_ms = ms32 / (args.steps * T)
+    achieved = 48 * cells / (per_launch_ms * 1e-3) / 1e9
+    value = world * cells * T * args.steps / (ms32 * 1e-3) / 1e9
+    plain = world * cells * T * plain_steps / (ms64 * 1e-3) / 1e9
+    h2d = sum(m for m in shapes.values()) * 8
+    line = {
+        "metric": CAV_METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms32 / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 audit",
+        "data": "synthetic (zero fields, Gaussian-modulated dipole current)",
+        "config": {"workload": f"yee_cavity {n}^3 cells, vacuum, conducting walls, Courant 0.99/sqrt(3), "
+                               f"{T} timesteps per step, soft z-current at the centre Ez edge, FP64 audit every timestep",
+                   "cells": cells, "timesteps_per_step": T, "parallelism": f"replicas x{world}",
+                   "l2": f"state {48 * cells / 2 / 1e9:.2f} GB > 126 MB L2, no flush"},
+        "e2e": {"value": round(world * cells * T * args.steps / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": shapes["ez"] * 8 + 64},
+        "gpu_launches": args.steps * T,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "kernel": "yee_tma_step (FP32, TMA-staged)",
+                     "bytes_per_launch": 48 * cells, "peak_source": f"{peak_kind} hbm_gbs"},
+        "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
+                      "roofline_frac": round(96 * cells / (ms64 / (plain_steps * T) * 1e-3) / 1e9 / peak, 4),
+                      "fp32_over_f64": round(value / plain, 3)},
+        "error_vs_f64": {"max_rel_field": field_err, "ledger_rel": ledger_err, "after_timesteps": T},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def cpu_baseline_ensemble(cfg, grids, sample_steps=2, threads=1, sample_grids=16):
     """`Ensemble::run` over `Solid3D` samples, restated (the oracle): the first `sample_grids`
     grids, each with its own audited `Simulation::advance` steps, `threads` grids at a time."""
@@ -554,8 +685,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble"],
-                    help="hall: the acoustic hall 256^3 (the headline); ensemble: 512 uneven heat grids")
+    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble", "cavity"],
+                    help="hall: the acoustic hall 256^3 (the headline); ensemble: 512 uneven heat grids; "
+                         "cavity: the Yee cavity 384^3")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--grids", type=int, default=512)
     ap.add_argument("--timesteps", type=int, default=None, help="timesteps per bench step (hall 5000, ensemble 2000)")
@@ -563,10 +695,20 @@ def main():
                     help="audited steps per CPU sample (hall 16, ensemble 8): about 10 s of one core")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload == "cavity" and args.n == 256:
+        args.n = 384
     if args.timesteps is None:
         args.timesteps = 5000 if args.workload == "hall" else 2000
     if args.cpu_sample_steps is None:
         args.cpu_sample_steps = 16 if args.workload == "hall" else 8
+    if args.workload == "cavity":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "workload": "cavity",
+                              "unavailable": "the reference arm times the headline hall and the ensemble; "
+                                             "the cavity's CPU path is timed in the tests' oracle only"}))
+        else:
+            run_cavity(args)
+        return
     if args.workload == "ensemble":
         if args.impl == "reference":
             run_reference_ensemble(args)

@@ -317,8 +317,10 @@ static __global__ void __launch_bounds__(256) yee_e(YeeEArgs<Real> a) {
 constexpr int kYeeHalo = 289;
 
 template <typename Real> struct YeeDepth;
+// At least 3: the plane computed, the plane above it, and one in flight.
 template <> struct YeeDepth<float> { static constexpr int stages = 6, min_blocks = 2; };
-template <> struct YeeDepth<double> { static constexpr int stages = 3, min_blocks = 2; };
+template <> struct YeeDepth<double> { static constexpr int stages = 4, min_blocks = 2; };
+static_assert(YeeDepth<float>::stages >= 3 && YeeDepth<double>::stages >= 3, "the ring holds two planes being read");
 
 template <typename Real>
 struct YeeStage {
@@ -562,8 +564,10 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
     const Real dec0 = a.decay[0], gain0 = a.gain[0];
     int slot = 0;
     while (cw.valid) {
-        cp_async_wait<S - 2>();  // this thread's copies of this plane and the next have landed
-        __syncthreads();         // ... and everyone's; and everyone is done with the oldest stage and H⁺
+        // This plane (slot) and the next (slot + 1, whose ex and ey the H⁺ update reads) must have
+        // landed: of the S − 1 + n groups committed before plane n, all but the newest S − 3.
+        cp_async_wait<S - 3>();
+        __syncthreads();  // ... everyone's; and everyone is done with the oldest stage and H⁺
         {
             const int fill = slot == 0 ? S - 1 : slot - 1;
             if (pf.valid) yee_stage<Real>(ring_base + fill * STAGE, a, pf, po, hq, hs);
@@ -639,7 +643,7 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
             Real c1 = ch, c2 = ch;
             if constexpr (!UNIFORM) {
                 const int ii = cw.x0 - 1, jj = cw.y0 - 1 + r;
-                if (ii >= 0 && jj <= ny && zin) c1 = (Real)(a.g / a.mu1[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)]);
+                if (ii >= 0 && jj >= 0 && jj <= ny && zin) c1 = (Real)(a.g / a.mu1[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)]);
                 if (ii >= 0 && jj >= 0 && jj < ny) c2 = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
             }
             if (r >= 1) hp->hy[r - 1][0] = S0.hy[r - 1][0] - c1 * ((S1.ex[r][0] - S0.ex[r][0]) - (S0.ez[r][1] - S0.ez[r][0]));

@@ -37,6 +37,9 @@ struct YeeMaps {
 #ifndef PM_YEE_TMA_STAGES
 #define PM_YEE_TMA_STAGES 2
 #endif
+#ifndef PM_YEE_TMA_MIN_BLOCKS
+#define PM_YEE_TMA_MIN_BLOCKS 2
+#endif
 constexpr int kYeeTmaPlanes = PM_YEE_TMA_PLANES;
 constexpr int kYeeTmaStages = PM_YEE_TMA_STAGES;
 
@@ -92,7 +95,7 @@ __device__ __forceinline__ void yee_tma_issue(const YeeMaps& m, unsigned stage, 
 }
 
 template <int P, int S, bool SOLID>
-static __global__ void __launch_bounds__(256, 2) yee_tma_step(YeeStepArgs<float> a, unsigned L,
+static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m) {
     DevState* st = a.st;
     if (st->violated) return;

@@ -271,6 +271,15 @@ class Cavity(_Domain):
         N.check(self._lib.pm_cavity_download(self._h, *[_ptr(out[k]) for k in ("ex", "ey", "ez", "hx", "hy", "hz")]))
         return out
 
+    def download_component(self, name, out):
+        """One component into a caller-owned f64 array (pinned memory makes this a DMA)."""
+        size = self.shapes()[name]
+        if out.dtype != np.float64 or out.size != size or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous f64 array of {size} values")
+        ptrs = [_ptr(out) if k == name else None for k in ("ex", "ey", "ez", "hx", "hy", "hz")]
+        N.check(self._lib.pm_cavity_download(self._h, *ptrs))
+        return out
+
     def set_source(self, edge, current):
         w = _f64(current)
         N.check(self._lib.pm_cavity_set_source(self._h, int(edge), _ptr(w), w.size))

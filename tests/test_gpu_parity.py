@@ -293,3 +293,49 @@ def test_ledger_is_reproducible_run_to_run():
         g.step(cfg["dt"], 100)
         totals.append(g.ledger()["total"])
     assert totals[0] == totals[1]
+
+
+def test_cavity_plain_bitexact_at_128_repeated():
+    """The source-driven vacuum cavity at 128³: large enough that the staged copies of the plane
+    above take longer than a plane's work, which is where a missing wait would read stale data.
+    Three fresh runs, each bit for bit against the oracle."""
+    from pantometry_b200 import workloads as W
+
+    n = 128
+    cfg = W.yee_cavity(n, steps=40)
+    o = oracle.Yee((n, n, n), cfg["dx"])
+    o.set_source(cfg["edge"], cfg["current"])
+    assert o.advance(cfg["dt"], 6, tol=1e-9) is None
+    fo = o.fields()
+    for _ in range(3):
+        g = W.build_cavity(cfg, precision="f64")
+        g.set_tolerance(1e-9)
+        assert g.step(cfg["dt"], 6) is None
+        fg = g.fields()
+        for k in fo:
+            assert_bitexact(k, fg[k], fo[k])
+
+
+def test_cavity_f32_media_at_96_repeated():
+    """The FP32 cp.async form (per-cell media) at 96³, three fresh runs against the oracle."""
+    from pantometry_b200 import workloads as W
+
+    n = 96
+    cfg = W.yee_cavity(n, steps=40)
+    eps = np.where(np.arange(n ** 3) % 11 == 0, 3.0, 1.0)
+    o = oracle.Yee((n, n, n), cfg["dx"])
+    o.set_cells(eps_r=eps)
+    o.set_source(cfg["edge"], cfg["current"])
+    assert o.step(cfg["dt"], 8) is None
+    fo = o.fields()
+    for _ in range(3):
+        from pantometry_b200.domains import Cavity
+
+        g = Cavity((n, n, n), cfg["dx"], precision="f32")
+        g.fill_cells(eps_r=eps)
+        g.set_source(cfg["edge"], cfg["current"])
+        assert g.step(cfg["dt"], 8) is None
+        fg = g.fields()
+        for k in fo:
+            scale = max(np.abs(fo[k]).max(), 1e-300)
+            assert np.abs(fg[k] - fo[k]).max() < 1e-5 * scale, k
