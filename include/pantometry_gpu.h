@@ -197,7 +197,9 @@ pm_status pm_cavity_obstruct(pm_cavity* c, const uint8_t* mask, size_t n);
 pm_status pm_cavity_set_boundary(pm_cavity* c, int wall, int kind);
 /* Cavity::release_mode (cavity.rs:675-732). */
 pm_status pm_cavity_release_mode(pm_cavity* c, int m, int p, double amplitude, double dt);
-/* Set all six components (host arrays in the reference's index order) and `started`. */
+/* Set all six components (host arrays in the reference's index order) and `started`. A new state
+ * starts fresh books: nothing dissipated, no source work, the source's clock back at step 0, and
+ * the ledger taken from the uploaded fields (the reference has no such setter). */
 pm_status pm_cavity_upload(pm_cavity* c, const double* ex, const double* ey, const double* ez,
                            const double* hx, const double* hy, const double* hz, int started);
 pm_status pm_cavity_download(pm_cavity* c, double* ex, double* ey, double* ez, double* hx,

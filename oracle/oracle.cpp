@@ -1328,6 +1328,12 @@ void or_yee_set(void* p, const double* ex, const double* ey, const double* ez, c
     if (hy) std::memcpy(c->hy.data(), hy, c->hy.size() * 8);
     if (hz) std::memcpy(c->hz.data(), hz, c->hz.size() * 8);
     c->started = started != 0;
+    // a new state starts fresh books and the source's clock (the reference has no setter)
+    c->has_invariant = false;
+    c->steps_taken = 0;
+    c->dissipated = 0.0;
+    c->source_work = 0.0;
+    c->work_booked = 0.0;
 }
 void or_yee_get_media(void* p, double* eps, double* sigma, double* mu) {
     Cavity* c = (Cavity*)p;

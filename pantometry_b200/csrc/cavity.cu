@@ -580,8 +580,13 @@ pm_status pm_cavity_upload(pm_cavity* cp, const double* ex, const double* ey, co
     PM_CUDA(cudaStreamSynchronize(c->stream()));
     c->started = started != 0;
     if ((s = c->read_state()) != PM_OK) return s;
+    // fresh books for a new state
     c->host_state->has_invariant = 0;
     c->host_state->steps = 0;
+    c->host_state->violated = kRunning;
+    c->host_state->dissipated = 0.0;
+    c->host_state->work = 0.0;
+    c->host_state->work_booked = 0.0;
     if ((s = c->write_state()) != PM_OK) return s;
     return c->reset_ledger();
 }
