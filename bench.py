@@ -688,15 +688,15 @@ def main():
     ap.add_argument("--workload", default="hall", choices=["hall", "ensemble", "cavity"],
                     help="hall: the acoustic hall 256^3 (the headline); ensemble: 512 uneven heat grids; "
                          "cavity: the Yee cavity 384^3")
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--n", type=int, default=None, help="grid size: hall 256 nodes, cavity 384 cells per axis")
     ap.add_argument("--grids", type=int, default=512)
     ap.add_argument("--timesteps", type=int, default=None, help="timesteps per bench step (hall 5000, ensemble 2000)")
     ap.add_argument("--cpu-sample-steps", type=int, default=None,
                     help="audited steps per CPU sample (hall 16, ensemble 8): about 10 s of one core")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    if args.workload == "cavity" and args.n == 256:
-        args.n = 384
+    if args.n is None:
+        args.n = 384 if args.workload == "cavity" else 256
     if args.timesteps is None:
         args.timesteps = 5000 if args.workload == "hall" else 2000
     if args.cpu_sample_steps is None:

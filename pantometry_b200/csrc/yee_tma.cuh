@@ -111,7 +111,9 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
     const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
     const double dt = a.dt;
     const bool lossy = a.sigma_u[0] != 0.0;
-    // Σ w|Eⁿ|², Σ w H⁺·H⁻ (the uniform ε and μ applied at the end), Joule loss, source work
+    // Σ w|Eⁿ|², Σ w H⁺·H⁻ (the uniform ε and μ applied at the end), Joule loss, source work.
+    // Each thread forms its cells' energy terms in f32 and sums them over a stage's planes; the
+    // stage sums, the reduction over the grid and the ledger are FP64.
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
     if (tid == 0) {
@@ -162,14 +164,15 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
         const int i = cc.x0 + tx, j = cc.y0 + ty;
         const bool in_x = i <= nx, in_y = j <= ny;
         // node-centred half weights of the boundary samples (cavity.rs:766-772)
-        const double hi = (i == 0 || i == nx) ? 0.5 : 1.0, hj = (j == 0 || j == ny) ? 0.5 : 1.0;
+        const float hi = (i == 0 || i == nx) ? 0.5f : 1.0f, hj = (j == 0 || j == ny) ? 0.5f : 1.0f;
+        float es = 0.0f, ms = 0.0f;  // this stage's w|E|² and w H⁺·H⁻ of the thread's cells
 #pragma unroll 1
         for (int h = 0; h < P; ++h) {
             const int k = cc.kb + h;
             if (k >= cc.k1) break;
             const bool compute = k >= cc.k0;  // else the plane below the chunk: H⁺ only
             const bool zin = k < nz;
-            const double hk = (k == 0 || k == nz) ? 0.5 : 1.0;
+            const float hk = (k == 0 || k == nz) ? 0.5f : 1.0f;
             YeeHp<float>* hq = hp + hpar;
             // ---- 1. H⁺ (cavity.rs:1346-1379) on own faces
             const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
@@ -186,17 +189,12 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
                 if (fx) a.neu[3][n] = hxn;
                 if (fy) a.neu[4][n] = hyn;
                 if (fz) a.neu[5][n] = hzn;
-                // ½μ H⁻·H⁺ (cavity.rs:854-905) and ½εEⁿ² (cavity.rs:776-847), weights only
-                double mm = 0.0, e = 0.0;
-                mm += fx ? hi * (double)hxn * (double)wx : 0.0;
-                mm += fy ? hj * (double)hyn * (double)wy : 0.0;
-                mm += fz ? hk * (double)hzn * (double)wz : 0.0;
-                const double dex = (double)ex0, dey = (double)ey0, dez = (double)ez0;
-                e += (i < nx && in_y) ? hj * hk * dex * dex : 0.0;
-                e += (in_x && j < ny) ? hi * hk * dey * dey : 0.0;
-                e += (in_x && in_y && zin) ? hi * hj * dez * dez : 0.0;
-                acc[0] += e;
-                acc[1] += mm;
+                // ½μ H⁻·H⁺ (cavity.rs:854-905) and ½εEⁿ² (cavity.rs:776-847), weights only. No
+                // mask is needed: at a lattice position a component does not have, its old value
+                // (padding, or the fill outside the lattice) is exactly zero, so its E term and
+                // its H⁻·H⁺ term are zero.
+                ms += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
+                es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
                 // halo faces: the y0 − 1 row (hx, hz) by warp 7, the x0 − 1 column (hy, hz) by warp 6
                 if (ty == 7) {
                     hq->hx[0][tx] = HX[h][0][tx] - ch * ((EZ[h][1][tx + 4] - EZ[h][0][tx + 4]) - (EY[h + 1][0][tx + 4] - EY[h][0][tx + 4]));
@@ -249,6 +247,8 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
             hy_below = hyn;
             hpar ^= 1;
         }
+        acc[0] += (double)es;
+        acc[1] += (double)ms;
         yee_tma_next(cc, T, P);
         ++it;
     }
