@@ -195,15 +195,19 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
                 // its H⁻·H⁺ term are zero.
                 ms += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
                 es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
-                // halo faces: the y0 − 1 row (hx, hz) by warp 7, the x0 − 1 column (hy, hz) by warp 6
+                // halo faces, one line per warp so the barrier waits on no warp doing twice the
+                // work: the y0 − 1 row of hx (warp 7) and of hz (warp 6), the x0 − 1 column of hz
+                // (warp 5, rows y0 − 1 .. y0 + 7) and of hy (warp 4, rows y0 .. y0 + 7)
                 if (ty == 7) {
                     hq->hx[0][tx] = HX[h][0][tx] - ch * ((EZ[h][1][tx + 4] - EZ[h][0][tx + 4]) - (EY[h + 1][0][tx + 4] - EY[h][0][tx + 4]));
+                } else if (ty == 6) {
                     hq->hz[0][tx + 1] = HZ[h][0][tx + 4] - ch * ((EY[h][0][tx + 5] - EY[h][0][tx + 4]) - (EX[h][1][tx + 4] - EX[h][0][tx + 4]));
-                }
-                if (ty == 6 && tx < 9) {
-                    const int r = tx;  // column x0 − 1, rows y0 − 1 .. y0 + 7
-                    if (r >= 1) hq->hy[r - 1][0] = HY[h][r - 1][3] - ch * ((EX[h + 1][r][3] - EX[h][r][3]) - (EZ[h][r][4] - EZ[h][r][3]));
+                } else if (ty == 5 && tx < 9) {
+                    const int r = tx;
                     hq->hz[r][0] = HZ[h][r][3] - ch * ((EY[h][r][4] - EY[h][r][3]) - (EX[h][r + 1][3] - EX[h][r][3]));
+                } else if (ty == 4 && tx >= 1 && tx < 9) {
+                    const int r = tx;
+                    hq->hy[r - 1][0] = HY[h][r - 1][3] - ch * ((EX[h + 1][r][3] - EX[h][r][3]) - (EZ[h][r][4] - EZ[h][r][3]));
                 }
             }
             __syncthreads();
