@@ -1,0 +1,302 @@
+// Batched Solid3D stepping, FP32 form, staged by the Tensor Memory Accelerator: the brick list of
+// ensemble_kernels.cuh walked by a persistent grid, each 32 × 8-column brick streamed P planes at
+// a time through a ring of S shared-memory stages. For a stage of planes kb .. kb+P−1 of block g
+// one thread issues one tiled TMA load of the block's deviations
+//   x0−4 .. x0+35, y0−1 .. y0+8, kb−1 .. kb+P
+// (rows padded to a multiple of 4 elements, so every row starts on 16 bytes; the hardware fills
+// outside the block with zeros) through block g's own tensor map. The per-cell arithmetic is
+// heat_f32_step's, the per-brick FP64 partials and the per-block ticket reduction are ens_step's.
+// Every wait on a stage's mbarrier is bounded; a wait that runs out stops the kernel with
+// kDeviceTimeout in every block's books.
+#pragma once
+
+#include "ensemble_kernels.cuh"
+#include "hall_tma.cuh"
+
+namespace pm {
+
+#ifndef PM_ENS_TMA_PLANES
+#define PM_ENS_TMA_PLANES 8
+#endif
+#ifndef PM_ENS_TMA_STAGES
+#define PM_ENS_TMA_STAGES 3
+#endif
+constexpr int kEnsTmaPlanes = PM_ENS_TMA_PLANES;
+constexpr int kEnsTmaStages = PM_ENS_TMA_STAGES;
+
+template <int P>
+struct EnsTmaStage {
+    float t[P + 2][10][40];
+};
+
+inline size_t ens_tma_smem_bytes() { return sizeof(EnsTmaStage<kEnsTmaPlanes>) * kEnsTmaStages + 16 * kEnsTmaStages; }
+
+// Everything a stage's consumers need about its brick, one 128-byte record per brick built on the
+// host; the producer bulk-copies it into the stage's slot with the stage's tile, on the same
+// mbarrier, so neither side ever waits on a dependent chain of global loads.
+struct alignas(16) EnsBrickInfo {
+    unsigned long long offset;
+    unsigned grid;
+    int x0, y0, nx, ny, nz, pitch, exposed;
+    float a, b[6], off[6];
+    unsigned pad[9];
+};
+static_assert(sizeof(EnsBrickInfo) == 128, "one record is one 128-byte bulk copy");
+
+constexpr unsigned kEnsHoldBlocks = 16384;  // blocks whose stop flags fit the shared bitmask
+
+struct EnsTmaArgs {
+    EnsArgs<float> e;
+    const CUtensorMap* maps;    // per block: the old field's map (this launch's parity)
+    const EnsBrickInfo* infos;  // per brick
+};
+
+__device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// The 256 consumer threads only (named barrier 1): a barrier, and a barrier that ANDs a predicate.
+constexpr int kEnsConsumers = 256;
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ bool consumers_and(bool p) {
+    unsigned r;
+    asm volatile("{\n .reg .pred a, b;\n setp.ne.u32 a, %1, 0;\n bar.red.and.pred b, 1, 256, a;\n selp.u32 %0, 1, 0, b;\n}\n"
+                 : "=r"(r)
+                 : "r"((unsigned)p)
+                 : "memory");
+    return r != 0;
+}
+// block_sum over the consumers (result in consumer thread 0).
+template <int NV>
+__device__ __forceinline__ void consumers_sum(double (&v)[NV], double* smem, int tid) {
+    const int lane = tid & 31, warp = tid >> 5;
+    warp_sum<NV>(v);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) smem[warp * NV + q] = v[q];
+    }
+    consumers_sync();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) v[q] = lane < kEnsConsumers / 32 ? smem[lane * NV + q] : 0.0;
+        warp_sum<NV>(v);
+    }
+    consumers_sync();
+}
+
+// Warps 0-7 consume (the cells of a 32 × 8 brick column each); warp 8 produces: it walks the
+// bricks (blockIdx.x, blockIdx.x + gridDim.x, ...), the next brick's entry fetched a brick ahead,
+// and for every stage issues the brick's record and the tile, S − 1 stages ahead. Slots are handed
+// back and forth with a full and an empty mbarrier each; every wait is bounded.
+template <int P, int S>
+static __global__ void __launch_bounds__(kEnsConsumers + 32, 3) ens_tma_step(const EnsTmaArgs t) {
+    using St = EnsTmaStage<P>;
+    const EnsArgs<float>& a = t.e;
+    extern __shared__ __align__(128) unsigned char ens_tma_smem[];
+    __shared__ double red[32 * 2];
+    __shared__ int last;
+    __shared__ EnsBrickInfo info[S];
+    __shared__ unsigned stage_brick[S];
+    __shared__ int stage_kb[S], stage_z1[S];  // stage_z1 < 0: the walk is over
+    __shared__ unsigned holdmask[kEnsHoldBlocks / 32];
+    const St* ring = reinterpret_cast<const St*>(ens_tma_smem);
+    const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(ens_tma_smem));
+    const unsigned full_base = ring_base + S * (unsigned)sizeof(St), empty_base = full_base + 8 * S;
+    const unsigned info_base = static_cast<unsigned>(__cvta_generic_to_shared(info));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // A block's flag changes only after all its bricks of a launch are done, so the flags read
+    // at the start hold for the whole launch (the host keeps this path to ≤ kEnsHoldBlocks blocks).
+    for (unsigned w = tid; w < (a.ngrids + 31) / 32; w += blockDim.x) {
+        unsigned bits = 0;
+        for (unsigned q = 0; q < 32 && 32 * w + q < a.ngrids; ++q)
+            if (a.states[32 * w + q].violated) bits |= 1u << q;
+        holdmask[w] = bits;
+    }
+    if (tid == 0) {
+        for (int q = 0; q < S; ++q) {
+            mbar_init(full_base + 8 * q, 1);
+            mbar_init(empty_base + 8 * q, kEnsConsumers / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == kEnsConsumers / 32) {  // the producer
+        if (lane != 0) return;
+        unsigned b = blockIdx.x;
+        EnsBrick br{}, nbr{};
+        if (b < a.nbricks) br = a.bricks[b];
+        if (b + gridDim.x < a.nbricks) nbr = a.bricks[b + gridDim.x];
+        int kb = br.z0;
+        int q = 0;
+        bool ok = true;
+        for (;; ++q) {
+            const int slot = q % S;
+            if (q >= S && !mbar_wait(empty_base + 8 * slot, (unsigned)(((q / S) - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            if (b >= a.nbricks) {  // the end of the walk, released with a plain arrive
+                stage_z1[slot] = -1;
+                mbar_arrive(full_base + 8 * slot);
+                break;
+            }
+            stage_brick[slot] = b;
+            stage_kb[slot] = kb;
+            stage_z1[slot] = br.z1;
+            const unsigned full = full_base + 8 * slot;
+            mbar_expect_tx(full, (unsigned)sizeof(St) + (unsigned)sizeof(EnsBrickInfo));
+            bulk_load(info_base + slot * (unsigned)sizeof(EnsBrickInfo), t.infos + b, sizeof(EnsBrickInfo), full);
+            tma_load_3d(ring_base + slot * (unsigned)sizeof(St), t.maps + br.grid, (int)br.x0 - 4, (int)br.y0 - 1, kb - 1,
+                        full);
+            kb += P;
+            if (kb >= br.z1) {  // to the next brick, and fetch the one after it
+                b += gridDim.x;
+                br = nbr;
+                kb = br.z0;
+                if (b + gridDim.x < a.nbricks) nbr = a.bricks[b + gridDim.x];
+            }
+        }
+        if (!ok) {
+            for (unsigned g = 0; g < a.ngrids; ++g) a.states[g].violated = kDeviceTimeout;
+        }
+        // the last use of each slot: its copies land before this thread (and the block) is done
+        for (int u = (q >= S ? q - S + 1 : 0); u < q; ++u) mbar_wait(full_base + 8 * (u % S), (unsigned)((u / S) & 1));
+        return;
+    }
+    const int tx = lane, ty = warp;
+    double acc[2] = {0.0, 0.0};  // the brick's Σ deviation of the new state, Σ heat shed
+    for (int it = 0;; ++it) {
+        const int slot = it % S;
+        const bool got = mbar_wait(full_base + 8 * slot, (unsigned)((it / S) & 1));
+        if (!consumers_and(got)) {
+            if (tid == 0)
+                for (unsigned g = 0; g < a.ngrids; ++g) a.states[g].violated = kDeviceTimeout;
+            return;
+        }
+        const int z1 = stage_z1[slot];
+        if (z1 < 0) return;  // the walk is over (every consumer reads the same word)
+        const EnsBrickInfo& m = info[slot];
+        const St& s = ring[slot];
+        const int kb = stage_kb[slot];
+        const unsigned brick = stage_brick[slot], gi = m.grid;
+        const int nx = m.nx, ny = m.ny, nz = m.nz, pitch = m.pitch;
+        const bool hold = (holdmask[gi >> 5] >> (gi & 31)) & 1u;
+        const int i = m.x0 + tx, j = m.y0 + ty;
+        if (i < nx && j < ny) {
+            const size_t plane = (size_t)pitch * ny;
+            float* __restrict__ tnew = a.nu + m.offset;
+            size_t c = (size_t)i + (size_t)pitch * ((size_t)j + (size_t)ny * kb);
+            const int hn = min(P, z1 - kb);  // planes of this stage in the brick
+            if (hold) {
+                for (int h = 0; h < hn; ++h, c += plane) tnew[c] = s.t[h + 1][ty + 1][tx + 4];
+            } else {
+                const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
+                const bool edge_xy = !(xl && xh && yl && yh);
+                const float ga = m.a;
+                const int exposed = m.exposed;
+                double col_shed = 0.0;
+#pragma unroll
+                for (int h = 0; h < P; ++h) {
+                    if (h >= hn) break;
+                    const int k = kb + h;
+                    const float here = s.t[h + 1][ty + 1][tx + 4];
+                    const float below = s.t[h][ty + 1][tx + 4], above = s.t[h + 2][ty + 1][tx + 4];
+                    const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+                    const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
+                    float nd;
+                    if (!edge_xy && k > 0 && k + 1 < nz) {
+                        // interior: all six neighbours, no film; heat_f32_step's order
+                        const float sum = (((((xm - here) + (xp - here)) + (ym - here)) + (yp - here)) + (below - here)) + (above - here);
+                        // the general path's two roundings, ga·sum − 0 then here + that, spelled out so
+                        // that the compiler cannot fold them into one fused multiply-add
+                        nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
+                    } else {
+                        float sum = 0.0f;  // the neighbours present, in the reference's order
+                        if (xl) sum += xm - here;
+                        if (xh) sum += xp - here;
+                        if (yl) sum += ym - here;
+                        if (yh) sum += yp - here;
+                        if (k > 0) sum += below - here;
+                        if (k + 1 < nz) sum += above - here;
+                        float shed = 0.0f;
+                        if (exposed) {
+                            if (((exposed >> 0) & 1) && !xl) shed += m.b[0] * (here + m.off[0]);
+                            if (((exposed >> 1) & 1) && !xh) shed += m.b[1] * (here + m.off[1]);
+                            if (((exposed >> 2) & 1) && !yl) shed += m.b[2] * (here + m.off[2]);
+                            if (((exposed >> 3) & 1) && !yh) shed += m.b[3] * (here + m.off[3]);
+                            if (((exposed >> 4) & 1) && k == 0) shed += m.b[4] * (here + m.off[4]);
+                            if (((exposed >> 5) & 1) && k + 1 == nz) shed += m.b[5] * (here + m.off[5]);
+                            col_shed += (double)shed;
+                        }
+                        nd = here + (ga * sum - shed);
+                    }
+                    tnew[c] = nd;
+                    acc[0] += (double)nd;
+                    c += plane;
+                }
+                acc[1] += col_shed;
+            }
+        }
+        const bool brick_done = kb + P >= z1;
+        // this warp is done with the slot (the tile and the record)
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty_base + 8 * slot);
+        if (brick_done && !hold) {
+            // the brick's partials, then the block's ticket; the last brick of the block reduces
+            // the block's partials in fixed order, then its ledger and audit
+            const EnsGrid& g = a.grids[gi];
+            DevState* st = a.states + gi;
+            consumers_sum<2>(acc, red, tid);
+            if (tid == 0) {
+                a.partials[2 * (size_t)brick] = acc[0];
+                a.partials[2 * (size_t)brick + 1] = acc[1];
+                __threadfence();
+                const unsigned ticket = atomicAdd(&st->counter, 1u);
+                last = ticket == g.nbricks - 1 ? 1 : 0;
+            }
+            consumers_sync();
+            if (last) {
+                __threadfence();
+                double v[2] = {0.0, 0.0};
+                for (unsigned q = tid; q < g.nbricks; q += kEnsConsumers) {
+                    v[0] += __ldcg(&a.partials[2 * (size_t)(g.first_brick + q)]);
+                    v[1] += __ldcg(&a.partials[2 * (size_t)(g.first_brick + q) + 1]);
+                }
+                consumers_sum<2>(v, red, tid);
+                if (tid == 0) {
+                    st->counter = 0u;
+                    const double stored = g.capacity * v[0];
+                    st->lost += g.capacity * v[1];
+                    double total = 0.0, scale = 0.0;
+                    ledger_add(total, scale, stored);
+                    ledger_add(total, scale, st->lost);
+                    ledger_add(total, scale, -st->supplied);
+                    st->part[0] = stored;
+                    st->part[1] = st->lost;
+                    st->part[2] = -st->supplied;
+                    audit_and_commit(st, total, scale);
+                }
+            }
+        }
+        if (brick_done) acc[0] = acc[1] = 0.0;
+    }
+}
+
+// One block's cells between the caller's kelvin (x fastest, rows of nx) and the device's f32
+// deviations T − T0 on rows of `pitch` (to_dev = 1; the padding zeroed by the caller), and back.
+static __global__ void ens_relayout(const double* __restrict__ kelvin, float* __restrict__ dev, double* __restrict__ out,
+                                    int nx, int ny, int nz, int pitch, double t0, int to_dev) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = r % (size_t)nx, rest = r / (size_t)nx;
+        const size_t p = i + (size_t)pitch * rest;  // rest = j + ny·k
+        if (to_dev) dev[p] = (float)(kelvin[r] - t0);
+        else out[r] = (double)dev[p] + t0;
+    }
+}
+
+}  // namespace pm

@@ -136,7 +136,13 @@ struct Ensemble : Handle {
     std::vector<EnsGrid> grids;
     std::vector<EnsBrick> bricks;
     std::vector<DevState> states;  // host mirror of the per-block books
-    size_t cells = 0;
+    size_t cells = 0;                     // cells of every block, in the caller's layout
+    size_t dcells = 0;                    // elements on the device (f32 rows padded to a multiple of 4)
+    std::vector<size_t> ref_offset;       // each block's first cell in the caller's layout
+    // FP32: bricks 32 wide step with the TMA-staged kernel; maps[par * blocks + g] is block g's map
+    bool tma = false;
+    std::vector<CUtensorMap> maps;
+    DBuf dmaps, dinfos;
     int shape = 0;
     long long generation = 0;  // bumped when the brick list changes (the graph cache key)
     DBuf field[2], stage, dgrids, dbricks, dstates, bpartials, saved, saved_states;
@@ -166,6 +172,23 @@ struct Ensemble : Handle {
             e.nbricks = (unsigned)bricks.size() - e.first_brick;
         }
         if (bricks.size() >= (size_t)UINT32_MAX) return fail(PM_BAD_ARG, "too many bricks");
+        if (tma) {  // the per-brick records the TMA kernel copies with each stage
+            std::vector<EnsBrickInfo> infos(bricks.size());
+            for (size_t q = 0; q < bricks.size(); ++q) {
+                const EnsGrid& g = grids[bricks[q].grid];
+                EnsBrickInfo& f = infos[q];
+                std::memset(&f, 0, sizeof(f));
+                f.offset = g.offset;
+                f.grid = bricks[q].grid;
+                f.x0 = bricks[q].x0; f.y0 = bricks[q].y0;
+                f.nx = g.nx; f.ny = g.ny; f.nz = g.nz; f.pitch = g.pitch; f.exposed = g.exposed;
+                f.a = g.a;
+                for (int k = 0; k < 6; ++k) { f.b[k] = g.b[k]; f.off[k] = g.off[k]; }
+            }
+            PM_CUDA(cudaStreamSynchronize(stream()));
+            if (dinfos.bytes < infos.size() * sizeof(EnsBrickInfo)) PM_CUDA(dinfos.alloc(infos.size() * sizeof(EnsBrickInfo)));
+            PM_CUDA(put_sync(dinfos.p, infos.data(), infos.size() * sizeof(EnsBrickInfo)));
+        }
         drop_graphs();
         PM_CUDA(cudaStreamSynchronize(stream()));
         if (dbricks.bytes < bricks.size() * sizeof(EnsBrick)) PM_CUDA(dbricks.alloc(bricks.size() * sizeof(EnsBrick)));
@@ -185,6 +208,7 @@ struct Ensemble : Handle {
         a.grids = dgrids.as<EnsGrid>();
         a.bricks = dbricks.as<EnsBrick>();
         a.nbricks = (unsigned)bricks.size();
+        a.ngrids = (unsigned)grids.size();
         a.bxs = kEnsShapes[shape].bxs;
         a.states = dstates.as<DevState>();
         a.partials = bpartials.as<double>();
@@ -194,7 +218,31 @@ struct Ensemble : Handle {
 
     cudaError_t launch(int par, bool measure, cudaStream_t s) const {
         if (precision == PM_PLAIN_F64) return launch_ens<double>(args<double>(par), measure, nblocks(), s);
+        if (!measure && tma && kEnsShapes[shape].bxs == 5) {
+            EnsTmaArgs t{};
+            t.e = args<float>(par);
+            t.maps = dmaps.as<CUtensorMap>() + (size_t)par * grids.size();
+            t.infos = dinfos.as<EnsBrickInfo>();
+            const unsigned w = wave_of(kEnsTma);
+            return launch_ens_tma(t, std::min<unsigned>(w, (unsigned)std::max<size_t>(bricks.size(), 1)), s);
+        }
         return launch_ens<float>(args<float>(par), measure, nblocks(), s);
+    }
+
+    // Tensor maps of every block's field in both parities (box 40 × 10 × (P + 2), x from x0 − 4).
+    pm_status build_maps() {
+        const size_t G = grids.size();
+        maps.assign(2 * G, CUtensorMap{});
+        for (int par = 0; par < 2; ++par)
+            for (size_t g = 0; g < G; ++g) {
+                const EnsGrid& q = grids[g];
+                if (!hall_tma_map(&maps[par * G + g], field[par].as<float>() + q.offset, q.pitch, q.ny, q.nz, 40, 10,
+                                  kEnsTmaPlanes + 2))
+                    return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused an ensemble block");
+            }
+        PM_CUDA(dmaps.alloc(maps.size() * sizeof(CUtensorMap)));
+        PM_CUDA(put_sync(dmaps.p, maps.data(), maps.size() * sizeof(CUtensorMap)));
+        return PM_OK;
     }
 
     pm_status read_states() {
@@ -267,8 +315,9 @@ pm_status pm_ensemble_create(const pm_ensemble_grid* grids, int count, int preci
         EnsGrid& q = e->grids[g];
         std::memset(&q, 0, sizeof(q));
         q.nx = d.nx; q.ny = d.ny; q.nz = d.nz;
+        q.pitch = precision == PM_PLAIN_F64 ? d.nx : (d.nx + 3) & ~3;
         q.offset = offset;
-        offset += (size_t)d.nx * d.ny * d.nz;
+        offset += (size_t)q.pitch * d.ny * d.nz;
         q.exposed = d.convection_w_per_m2_k != 0.0 ? 0x3f : 0;
         q.kface = u.kface; q.mobility = u.mobility; q.capacity = u.capacity;
         q.k_cell = u.k_cell; q.eps_cell = d.substance.emissivity;
@@ -284,12 +333,19 @@ pm_status pm_ensemble_create(const pm_ensemble_grid* grids, int count, int preci
             q.off[f] = 0.0f;  // the films' ambient is the block's own T0
         }
     }
-    e->cells = offset;
+    e->dcells = offset;
+    e->ref_offset.resize(count);
+    e->cells = 0;
+    for (int g = 0; g < count; ++g) {
+        e->ref_offset[g] = e->cells;
+        e->cells += (size_t)grids[g].nx * grids[g].ny * grids[g].nz;
+    }
     pm_status s = e->init(device, 0);
     if (s != PM_OK) { delete e; return s; }
     auto bail = [&](pm_status st) { delete e; return st; };
     for (auto& f : e->field) {
-        cudaError_t ce = f.alloc(e->cells * e->esize());
+        cudaError_t ce = f.alloc(e->dcells * e->esize());
+        if (ce == cudaSuccess) ce = cudaMemset(f.p, 0, e->dcells * e->esize());
         if (ce != cudaSuccess) return bail(cuda_fail(ce, "cudaMalloc ensemble field"));
     }
     cudaError_t ce = e->dgrids.alloc(count * sizeof(EnsGrid));
@@ -299,11 +355,13 @@ pm_status pm_ensemble_create(const pm_ensemble_grid* grids, int count, int preci
     e->states.assign(count, DevState{});
     for (auto& st : e->states) st.tol = e->tolerance;
     if ((s = e->write_states()) != PM_OK) return bail(s);
+    // FP32 bricks 32 wide step with the TMA kernel when the driver tiles every block
+    if (precision == PM_FIELDS_F32 && count <= (int)kEnsHoldBlocks) e->tma = e->build_maps() == PM_OK;
     if ((s = e->set_shape(0)) != PM_OK) return bail(s);
     // every block starts at its own T0 (Solid3D::new)
     std::vector<double> t(e->cells);
     for (int g = 0; g < count; ++g)
-        std::fill(t.begin() + e->grids[g].offset, t.begin() + e->grids[g].offset + (size_t)grids[g].nx * grids[g].ny * grids[g].nz,
+        std::fill(t.begin() + e->ref_offset[g], t.begin() + e->ref_offset[g] + (size_t)grids[g].nx * grids[g].ny * grids[g].nz,
                   grids[g].initial_kelvin);
     *out = reinterpret_cast<pm_ensemble*>(e);
     s = pm_ensemble_upload(*out, t.data(), t.size());
@@ -323,9 +381,8 @@ pm_status pm_ensemble_upload(pm_ensemble* ep, const double* kelvin, size_t n) {
         PM_CUDA(cudaMemcpyAsync(e->stage.p, kelvin, n * 8, cudaMemcpyHostToDevice, e->stream()));
         for (size_t g = 0; g < e->grids.size(); ++g) {
             const EnsGrid& q = e->grids[g];
-            const size_t m = (size_t)q.nx * q.ny * q.nz;
-            PM_CUDA(launch_heat_convert(e->stage.as<double>() + q.offset, e->field[0].as<float>() + q.offset, q.reference, m, 1,
-                                        nullptr, e->stream()));
+            PM_CUDA(launch_ens_relayout(e->stage.as<double>() + e->ref_offset[g], e->field[0].as<float>() + q.offset, nullptr,
+                                        q.nx, q.ny, q.nz, q.pitch, q.reference, 1, e->stream()));
         }
     }
     // fresh books: nothing lost or supplied, no audit history
@@ -348,9 +405,9 @@ pm_status pm_ensemble_download(pm_ensemble* ep, double* kelvin, size_t n) {
         if (e->stage.bytes < n * 8) PM_CUDA(e->stage.alloc(n * 8));
         for (size_t g = 0; g < e->grids.size(); ++g) {
             const EnsGrid& q = e->grids[g];
-            const size_t m = (size_t)q.nx * q.ny * q.nz;
-            PM_CUDA(launch_heat_convert(nullptr, e->field[e->parity].as<float>() + q.offset, q.reference, m, 0,
-                                        e->stage.as<double>() + q.offset, e->stream()));
+            PM_CUDA(launch_ens_relayout(nullptr, e->field[e->parity].as<float>() + q.offset,
+                                        e->stage.as<double>() + e->ref_offset[g], q.nx, q.ny, q.nz, q.pitch, q.reference, 0,
+                                        e->stream()));
         }
         PM_CUDA(cudaMemcpyAsync(kelvin, e->stage.p, n * 8, cudaMemcpyDeviceToHost, e->stream()));
     }
@@ -454,7 +511,7 @@ pm_status pm_ensemble_autotune(pm_ensemble* ep, int trial_steps, int* brick_x, i
     ENS_GUARD(e);
     if (trial_steps < 1) return fail(PM_BAD_ARG, "trial_steps must be >= 1");
     // keep the present state and books; every trial runs on a copy of them and is undone
-    const size_t bytes = e->cells * e->esize();
+    const size_t bytes = e->dcells * e->esize();
     if (e->saved.bytes < bytes) PM_CUDA(e->saved.alloc(bytes));
     PM_CUDA(cudaMemcpyAsync(e->saved.p, e->field[e->parity].p, bytes, cudaMemcpyDeviceToDevice, e->stream()));
     pm_status s = e->read_states();

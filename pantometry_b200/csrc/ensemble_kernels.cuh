@@ -4,7 +4,8 @@
 // crates/pantometry-thermal/src/solid.rs:1717-1901).
 //
 // Layout. The blocks' cells are concatenated in block order, each block in the reference's
-// index order i + nx·(j + ny·k). A brick is a bx × by × zc box of one block (bx·by = 256
+// index order i + pitch·(j + ny·k) (pitch = nx for f64; nx rounded up to 4 for f32, the padding
+// columns zero, so that TMA can tile each block). A brick is a bx × by × zc box of one block (bx·by = 256
 // threads, each marching one column of zc planes); the brick list holds every brick of every
 // block, block by block, and a persistent grid of thread blocks takes bricks blockIdx.x,
 // blockIdx.x + gridDim.x, ... in that fixed order. Brick shapes are chosen at run time (the
@@ -29,6 +30,8 @@ struct EnsGrid {
     int nx, ny, nz;
     unsigned nbricks;
     unsigned long long offset;  // first cell in the concatenated field
+    int pitch;                  // elements per row: nx (f64), nx rounded up to 4 (f32, for TMA)
+    int pad0;
     unsigned first_brick;
     int exposed;                // film faces (bit f: XMin, XMax, YMin, YMax, ZMin, ZMax)
     // plain f64 coefficients (`resolve` of a one-material block, solid.rs:588-784)
@@ -55,6 +58,7 @@ struct EnsArgs {
     const EnsGrid* __restrict__ grids;
     const EnsBrick* __restrict__ bricks;
     unsigned nbricks;
+    unsigned ngrids;
     int bxs;             // log2 of the brick's x extent (4, 5 or 6)
     DevState* states;    // one per block: its books, ledger and audit
     double* partials;    // two per brick
@@ -92,11 +96,12 @@ __device__ __forceinline__ void ens_brick(const EnsArgs<Real>& a, const EnsGrid&
     const int j = br.y0 + (tid >> a.bxs);
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i >= nx || j >= ny) return;
-    const size_t plane = (size_t)nx * ny;
+    const int pitch = g.pitch;
+    const size_t plane = (size_t)pitch * ny;
     const Real* __restrict__ told = a.old + g.offset;
     Real* __restrict__ tnew = a.nu + g.offset;
     const int k0 = br.z0, k1 = br.z1;
-    size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+    size_t c = (size_t)i + (size_t)pitch * ((size_t)j + (size_t)ny * k0);
     if (MEASURE) {
         for (int k = k0; k < k1; ++k, c += plane) {
             if constexpr (sizeof(Real) == 8) acc[0] += g.capacity * ((double)told[c] - g.reference);  // solid.rs:1583-1590
@@ -115,8 +120,8 @@ __device__ __forceinline__ void ens_brick(const EnsArgs<Real>& a, const EnsGrid&
             double flux = 0.0;
             if (i > 0) flux += kf * (told[c - 1] - t0);
             if (i + 1 < nx) flux += kf * (told[c + 1] - t0);
-            if (j > 0) flux += kf * (told[c - nx] - t0);
-            if (j + 1 < ny) flux += kf * (told[c + nx] - t0);
+            if (j > 0) flux += kf * (told[c - pitch] - t0);
+            if (j + 1 < ny) flux += kf * (told[c + pitch] - t0);
             if (k > 0) flux += kf * (below - t0);
             if (k + 1 < nz) flux += kf * (above - t0);
             const double shed = g.exposed ? ens_film_flux(g, i, j, k, t0) : 0.0;
@@ -140,8 +145,8 @@ __device__ __forceinline__ void ens_brick(const EnsArgs<Real>& a, const EnsGrid&
             float s = 0.0f;
             if (xl) s += __ldg(told + c - 1) - here;
             if (xh) s += __ldg(told + c + 1) - here;
-            if (yl) s += __ldg(told + c - nx) - here;
-            if (yh) s += __ldg(told + c + nx) - here;
+            if (yl) s += __ldg(told + c - pitch) - here;
+            if (yh) s += __ldg(told + c + pitch) - here;
             if (k > 0) s += below - here;
             if (k + 1 < nz) s += above - here;
             float shed = 0.0f;
@@ -172,8 +177,8 @@ __device__ __forceinline__ void ens_hold(const EnsArgs<Real>& a, const EnsGrid& 
     const int i = br.x0 + (tid & ((1 << a.bxs) - 1));
     const int j = br.y0 + (tid >> a.bxs);
     if (i >= g.nx || j >= g.ny) return;
-    const size_t plane = (size_t)g.nx * g.ny;
-    size_t c = g.offset + (size_t)i + (size_t)g.nx * ((size_t)j + (size_t)g.ny * br.z0);
+    const size_t plane = (size_t)g.pitch * g.ny;
+    size_t c = g.offset + (size_t)i + (size_t)g.pitch * ((size_t)j + (size_t)g.ny * br.z0);
     for (int k = br.z0; k < br.z1; ++k, c += plane) a.nu[c] = a.old[c];
 }
 

@@ -162,6 +162,23 @@ cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool d
     return cudaGetLastError();
 }
 
+cudaError_t launch_ens_tma(const EnsTmaArgs& t, unsigned nblocks, cudaStream_t s) {
+    static bool attr = false;
+    const int smem = (int)ens_tma_smem_bytes();
+    if (!attr) {
+        cudaFuncSetAttribute(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    ens_tma_step<kEnsTmaPlanes, kEnsTmaStages><<<nblocks, kEnsConsumers + 32, smem, s>>>(t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, int nx, int ny, int nz, int pitch,
+                                double t0, int to_dev, cudaStream_t s) {
+    ens_relayout<<<kMeasureBlocks, 256, 0, s>>>(kelvin, dev, out, nx, ny, nz, pitch, t0, to_dev);
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -178,6 +195,12 @@ int occupancy_f32(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
         case kEnsF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false>, 256, 0); break;
+        case kEnsTma:
+            cudaFuncSetAttribute(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ens_tma_smem_bytes());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>,
+                                                              kEnsConsumers + 32, ens_tma_smem_bytes());
+            break;
         case kYeeTma:
             cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes());

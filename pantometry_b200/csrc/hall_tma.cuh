@@ -74,10 +74,17 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Wait for phase `parity` of the barrier to complete, at most kMbarSpinLimit rounds.
+// Wait for phase `parity` of the barrier to complete, at most kMbarSpinLimit rounds. After the
+// first few rounds each failed round sleeps, so waiting warps leave the issue slots to the warps
+// of other blocks that have work (about a second in all before the wait gives up).
+#ifndef PM_MBAR_SLEEP_NS
+#define PM_MBAR_SLEEP_NS 64
+#endif
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-    for (unsigned n = 0; n < kMbarSpinLimit; ++n)
+    for (unsigned n = 0; n < kMbarSpinLimit; ++n) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (PM_MBAR_SLEEP_NS > 0 && n >= 4) __nanosleep(PM_MBAR_SLEEP_NS);
+    }
     return false;
 }
 __device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int x, int y, int z, unsigned bar) {

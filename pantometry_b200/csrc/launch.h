@@ -11,6 +11,7 @@
 #include "ensemble_kernels.cuh"
 #include "hall_tma.cuh"
 #include "yee_tma.cuh"
+#include "ens_tma.cuh"
 
 namespace pm {
 
@@ -45,7 +46,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kEnsTma, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -83,6 +84,11 @@ inline size_t yee_tma_smem_bytes() { return yee_tma_smem_bytes_for<kYeeTmaPlanes
 // src_f64 / dst_f64 select double or float for each side.
 cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,
                                 unsigned L, unsigned ny1, int to_padded, cudaStream_t s);
+// One FP32 ensemble step over 32 × 8-column bricks, staged by TMA.
+cudaError_t launch_ens_tma(const EnsTmaArgs& t, unsigned nblocks, cudaStream_t s);
+// One block between kelvin on the host's layout and f32 deviations on padded rows.
+cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, int nx, int ny, int nz, int pitch,
+                                double t0, int to_dev, cudaStream_t s);
 // One ensemble step (measure = false) or the opening ledgers (measure = true) over the brick list.
 template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool measure, unsigned nblocks, cudaStream_t s);
 

@@ -167,3 +167,21 @@ def test_ensemble_refusals_and_audit_name_the_block():
     e.set_tolerance(-1.0)
     assert e.step(3) is None  # a new call clears the stop; every block steps again
     assert all(s1 == s0 + 3 for s0, s1 in zip(steps, (led["steps"] for led in e.ledgers())))
+
+
+@pytest.mark.gpu
+def test_ensemble_f32_tma_and_brick_kernels_agree():
+    """32-wide bricks step with the TMA-staged kernel, 16- and 64-wide with the plain brick kernel;
+    both do heat_f32_step's arithmetic on the same padded rows, so the fields agree bit for bit."""
+    from pantometry_b200.domains import Ensemble
+
+    grids, cells = small_grids(count=10, seed=0xA11)
+    runs = []
+    for bx, planes in ((32, 16), (16, 8), (64, 32), (32, 64)):
+        e = Ensemble(grids, precision="f32")
+        e.set_shape(bx, planes)
+        e.upload(np.concatenate(cells))
+        assert e.step(STEPS) is None
+        runs.append(e.download())
+    for r in runs[1:]:
+        assert np.array_equal(r, runs[0])
