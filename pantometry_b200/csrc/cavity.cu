@@ -46,6 +46,11 @@ struct Cavity : Handle {
     bool tma = false;
     unsigned L = 0;
     YeeMaps maps[2];
+    // Mur's history (cavity.rs:141): E after the last step's walls. Normally the old buffer of the
+    // ping-pong pair; after something rewrote E between steps it is a snapshot taken before that.
+    bool has_prev = false;   // a step has run (cavity.rs:1087)
+    bool use_stale = false;  // the next step's history is `stale`
+    DBuf stale[3];
 
     size_t count(int q) const {
         switch (q) {
@@ -341,6 +346,64 @@ struct Cavity : Handle {
         return PM_OK;
     }
 
+    bool open_or_magnetic() const {
+        for (int w = 0; w < 6; ++w)
+            if (boundary[w] != 0) return true;
+        return false;
+    }
+    // Before E is rewritten between steps: keep the history the next step's open walls need.
+    pm_status keep_history() {
+        if (!has_prev || use_stale) return PM_OK;
+        for (int q = 0; q < 3; ++q) {
+            const size_t bytes = dcount(q) * esize();
+            if (stale[q].bytes < bytes) PM_CUDA(stale[q].alloc(bytes));
+            PM_CUDA(cudaMemcpyAsync(stale[q].p, f[parity][q].p, bytes, cudaMemcpyDeviceToDevice, stream()));
+        }
+        use_stale = true;
+        return PM_OK;
+    }
+    // The walls after the step from `par` into `par ^ 1` (cavity.rs:1074-1164): magnetic mirrors,
+    // then open walls by Mur (or held at zero before any history exists), one wall at a time.
+    template <typename Real>
+    cudaError_t walls(int par, bool prev, bool stale_history, double dt, cudaStream_t s) const {
+        YeeWallArgs<Real> a{};
+        for (int q = 0; q < 3; ++q) {
+            a.e[q] = f[par ^ 1][q].as<Real>();
+            a.pe[q] = stale_history ? stale[q].as<Real>() : f[par][q].as<Real>();
+            int ex, ey, ez;
+            extents(q, ex, ey, ez);
+            a.rx[q] = tma ? L : (unsigned)ex;
+            a.ry[q] = tma ? (unsigned)(ny + 1) : (unsigned)ey;
+        }
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        const double c_dt = wave_speed() * dt;
+        a.k = (Real)((c_dt - dx) / (c_dt + dx));  // cavity.rs:1075-1078
+        for (int w = 0; w < 6; ++w) {
+            if (boundary[w] != 1) continue;
+            a.wall = w;
+            a.kind = 1;
+            cudaError_t e = launch_yee_walls<Real>(a, s);
+            if (e != cudaSuccess) return e;
+        }
+        for (int w = 0; w < 6; ++w) {
+            if (boundary[w] != 2) continue;
+            a.wall = w;
+            a.kind = prev ? 2 : 3;
+            cudaError_t e = launch_yee_walls<Real>(a, s);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    // One step from `par`, its walls included.
+    cudaError_t step_once(int par, double h, bool prev, bool stale_history, cudaStream_t s) const {
+        cudaError_t e;
+        if (precision == PM_PLAIN_F64) e = launch_yee_step<double>(sargs<double>(par, h), s);
+        else if (tma) e = launch_yee_tma(targs(par, h), L, maps[par], s);
+        else e = launch_yee_step<float>(sargs<float>(par, h), s);
+        if (e != cudaSuccess || !open_or_magnetic()) return e;
+        return precision == PM_PLAIN_F64 ? walls<double>(par, prev, stale_history, h, s) : walls<float>(par, prev, stale_history, h, s);
+    }
+
     // Tensor maps of both parities' six components over the padded lattice.
     pm_status build_maps() {
         constexpr unsigned P = kYeeTmaPlanes;
@@ -533,6 +596,8 @@ pm_status pm_cavity_obstruct(pm_cavity* cp, const uint8_t* mask, size_t n) {
     for (size_t q = 0; q < n; ++q)
         if (mask[q]) { c->solid[q] = 1; c->any_solid = true; }
     if (!c->any_solid) return PM_OK;
+    pm_status hs = c->keep_history();  // the edges it zeroes change E between steps
+    if (hs != PM_OK) return hs;
     PM_CUDA(c->dsolid.alloc(c->cells()));
     PM_CUDA(c->put_sync(c->dsolid.p, c->solid.data(), c->cells()));
     c->drop_graphs();
@@ -573,8 +638,9 @@ pm_status pm_cavity_upload(pm_cavity* cp, const double* ex, const double* ey, co
     Cavity* c = reinterpret_cast<Cavity*>(cp);
     CAV_GUARD(c);
     const double* src[6] = {ex, ey, ez, hx, hy, hz};
+    pm_status s = c->keep_history();  // the next step's open walls use the E of before the upload
+    if (s != PM_OK) return s;
     c->parity = 0;
-    pm_status s;
     for (int q = 0; q < 6; ++q)
         if ((s = c->put(q, src[q])) != PM_OK) return s;
     PM_CUDA(cudaStreamSynchronize(c->stream()));
@@ -604,7 +670,9 @@ pm_status pm_cavity_download(pm_cavity* cp, double* ex, double* ey, double* ez, 
 pm_status pm_cavity_release_mode(pm_cavity* cp, int m_in, int p_in, double amplitude, double dt) {
     Cavity* c = reinterpret_cast<Cavity*>(cp);
     CAV_GUARD(c);
-    // cavity.rs:675-732
+    // cavity.rs:675-732; the next step's open walls keep the history of before the release
+    pm_status hs = c->keep_history();
+    if (hs != PM_OK) return hs;
     const double m = (double)std::max(m_in, 1), p = (double)std::max(p_in, 1);
     const int nx = c->nx, ny = c->ny, nz = c->nz;
     const double sx = (double)nx * c->dx, sz = (double)nz * c->dx;
@@ -690,9 +758,9 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
     CAV_GUARD(c);
     if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
     if (nsteps == 0) return PM_OK;
-    for (int w = 0; w < 6; ++w)
-        if (c->boundary[w] != 0)
-            return fail(PM_UNSUPPORTED, "magnetic and open (Mur) walls are not on the GPU path; conducting walls only");
+    if (c->open_or_magnetic() && c->any_solid)
+        return fail(PM_UNSUPPORTED, "obstacles together with magnetic or open walls are not on the GPU path (the reference zeroes "
+                                    "obstacle edges after the walls)");
     // cavity.rs:1469-1480
     const double h = dt, limit = c->courant_limit();
     if (h > limit) {
@@ -708,11 +776,17 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
         if (s != PM_OK) return s;
         c->started = true;
     }
-    s = c->run_steps(nsteps, dt, true, [c, h](int par, cudaStream_t st) {
-        if (c->precision == PM_PLAIN_F64) return launch_yee_step<double>(c->sargs<double>(par, h), st);
-        if (c->tma) return launch_yee_tma(c->targs(par, h), c->L, c->maps[par], st);
-        return launch_yee_step<float>(c->sargs<float>(par, h), st);
-    });
+    long long remaining = nsteps;
+    if (!c->has_prev || c->use_stale) {
+        // the first step after creation holds open walls at zero; the first after E was rewritten
+        // takes its history from the snapshot: both run on their own, outside any graph
+        PM_CUDA(c->step_once(c->parity, h, c->has_prev, c->use_stale, c->stream()));
+        c->parity ^= 1;
+        c->has_prev = true;
+        c->use_stale = false;
+        remaining -= 1;
+    }
+    s = c->run_steps(remaining, dt, true, [c, h](int par, cudaStream_t st) { return c->step_once(par, h, true, false, st); });
     if (s != PM_OK) return s;
     return c->finish_call(before, out, "simulation", "simulation", true);
 }
@@ -761,6 +835,8 @@ pm_status pm_cavity_restore(pm_cavity* cp) {
     Cavity* c = reinterpret_cast<Cavity*>(cp);
     CAV_GUARD(c);
     if (!c->has_saved) return PM_OK;
+    pm_status hs = c->keep_history();  // Mur's history is not part of the checkpoint (cavity.rs:1566-1590)
+    if (hs != PM_OK) return hs;
     for (int q = 0; q < 6; ++q)
         PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q].p, c->sf[q].p, c->dcount(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
     pm_status s = c->read_state();

@@ -21,6 +21,9 @@ namespace pm {
 #ifndef PM_ENS_TMA_STAGES
 #define PM_ENS_TMA_STAGES 3
 #endif
+#ifndef PM_ENS_TMA_MIN_BLOCKS
+#define PM_ENS_TMA_MIN_BLOCKS 4
+#endif
 constexpr int kEnsTmaPlanes = PM_ENS_TMA_PLANES;
 constexpr int kEnsTmaStages = PM_ENS_TMA_STAGES;
 
@@ -93,7 +96,7 @@ __device__ __forceinline__ void consumers_sum(double (&v)[NV], double* smem, int
 // and for every stage issues the brick's record and the tile, S − 1 stages ahead. Slots are handed
 // back and forth with a full and an empty mbarrier each; every wait is bounded.
 template <int P, int S>
-static __global__ void __launch_bounds__(kEnsConsumers + 32, 3) ens_tma_step(const EnsTmaArgs t) {
+static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOCKS) ens_tma_step(const EnsTmaArgs t) {
     using St = EnsTmaStage<P>;
     const EnsArgs<float>& a = t.e;
     extern __shared__ __align__(128) unsigned char ens_tma_smem[];

@@ -179,6 +179,12 @@ cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, i
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_yee_walls<float>(const YeeWallArgs<float>& a, cudaStream_t s) {
+    yee_walls<float><<<kMeasureBlocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;

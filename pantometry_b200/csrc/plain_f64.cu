@@ -93,6 +93,12 @@ cudaError_t launch_ens<double>(const EnsArgs<double>& a, bool measure, unsigned 
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_yee_walls<double>(const YeeWallArgs<double>& a, cudaStream_t s) {
+    yee_walls<double><<<kMeasureBlocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f64(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;

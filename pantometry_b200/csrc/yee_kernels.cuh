@@ -730,6 +730,52 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
     }
 }
 
+// Magnetic and open walls (cavity.rs:1074-1236), applied to the new E after a step, one wall at a
+// time in the reference's order, so edges shared by two walls end as they do there. Any layout:
+// component q's edge (i, j, k) is at i + rx[q]·(j + ry[q]·k).
+template <typename Real>
+struct YeeWallArgs {
+    Real* e[3];         // the new ex, ey, ez
+    const Real* pe[3];  // the previous step's E after its walls (Mur's history)
+    int nx, ny, nz;
+    unsigned rx[3], ry[3];
+    int wall;           // 0..5: XLow, XHigh, YLow, YHigh, ZLow, ZHigh
+    int kind;           // 1 mirror (magnetic), 2 Mur (open), 3 zero (open, no history yet)
+    Real k;             // Mur's coefficient (cΔt − Δ)/(cΔt + Δ)
+};
+
+template <typename Real>
+static __global__ void yee_walls(YeeWallArgs<Real> a) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz, w = a.wall;
+    // the wall's two tangential components (cavity.rs:1096-1157): x walls ey, ez; y walls ex, ez;
+    // z walls ex, ey; each over (u, v) = its two in-plane lattice coordinates
+    const int q0 = w < 2 ? 1 : 0, q1 = w < 4 ? 2 : 1;
+    int n0u, n0v, n1u, n1v;  // extents of (u, v) for each component
+    if (w < 2) { n0u = ny; n0v = nz + 1; n1u = ny + 1; n1v = nz; }
+    else if (w < 4) { n0u = nx; n0v = nz + 1; n1u = nx + 1; n1v = nz; }
+    else { n0u = nx; n0v = ny + 1; n1u = nx + 1; n1v = ny; }
+    const int edge = (w & 1) ? (w < 2 ? nx : w < 4 ? ny : nz) : 0;
+    const int inner = (w & 1) ? edge - 1 : 1;
+    const size_t c0 = (size_t)n0u * n0v, total = c0 + (size_t)n1u * n1v;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const bool first = t < c0;
+        const int q = first ? q0 : q1;
+        const size_t r = first ? t : t - c0;
+        const int nu = first ? n0u : n1u;
+        const int u = (int)(r % (size_t)nu), v = (int)(r / (size_t)nu);
+        int ia, ja, ka, ib, jb, kb;
+        if (w < 2) { ia = edge; ib = inner; ja = jb = u; ka = kb = v; }
+        else if (w < 4) { ja = edge; jb = inner; ia = ib = u; ka = kb = v; }
+        else { ka = edge; kb = inner; ia = ib = u; ja = jb = v; }
+        const size_t ai = (size_t)ia + (size_t)a.rx[q] * ((size_t)ja + (size_t)a.ry[q] * ka);
+        const size_t bi = (size_t)ib + (size_t)a.rx[q] * ((size_t)jb + (size_t)a.ry[q] * kb);
+        Real* e = a.e[q];
+        if (a.kind == 1) e[ai] = e[bi];                                        // cavity.rs:1170-1236
+        else if (a.kind == 2) e[ai] = a.pe[q][bi] + a.k * (e[bi] - a.pe[q][ai]);  // cavity.rs:1096-1157
+        else e[ai] = Real(0);                                                  // cavity.rs:1087-1089
+    }
+}
+
 // ½εE² and ½μH² of the present state (cavity.rs:824-847, 919-940): the naive energy the
 // ledger reports before any invariant exists, and what pm_cavity_energies returns.
 template <typename Real>
