@@ -51,3 +51,13 @@ def test_status_strings_without_a_device(lib):
     assert lib.pm_status_string(3) == b"violation"
     lib.pm_version.restype = ctypes.c_char_p
     assert b"sm_100a" in lib.pm_version()
+
+
+def test_entry_build_in_a_fresh_interpreter():
+    """build() as the driver calls it: a new process, nothing imported beforehand."""
+    import subprocess
+    import sys
+
+    r = subprocess.run([sys.executable, "-c", "import __graft_entry__ as g; g.build()"], cwd=ROOT,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
