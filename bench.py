@@ -608,6 +608,297 @@ def run_cavity(args):
         dist.destroy_process_group()
 
 
+MIX_METRIC = "Gcell-updates/s (1024^3 heterogeneous acoustic hall + 64 Yee 128^3 dielectric cavities, FP32 fields + FP64 audit)"
+
+
+class CavityBatch:
+    """The 64 cavities of the mixed workload, each its own handle, spread over `lanes` CUDA streams
+    with one host thread per stream (a step call returns once its stream has finished)."""
+
+    def __init__(self, cfg, precision, device, lanes=8):
+        import torch
+
+        from pantometry_b200 import workloads as W
+
+        self.cfg = cfg
+        self.cavs = [W.build_dielectric_cavity(cfg, g, precision=precision, device=device)
+                     for g in range(len(cfg["cavities"]))]
+        self.streams = [torch.cuda.Stream(device=device) for _ in range(min(lanes, len(self.cavs)))]
+        for g, c in enumerate(self.cavs):
+            c.set_stream(self.streams[g % len(self.streams)].cuda_stream)
+
+    def set_tolerance(self, tol):
+        for c in self.cavs:
+            c.set_tolerance(tol)
+
+    def run(self, dt, T, before=None, each=None):
+        """Every cavity `T` steps; `before(g, c)` / `each(g, c)` around each cavity's run."""
+        L = len(self.streams)
+        errors = []
+
+        def lane(q):
+            try:
+                for g in range(q, len(self.cavs), L):
+                    c = self.cavs[g]
+                    if before:
+                        before(g, c)
+                    v = c.step(dt, T)
+                    assert v is None, v
+                    if each:
+                        each(g, c)
+            except BaseException as e:  # noqa: BLE001
+                errors.append(e)
+
+        ths = [threading.Thread(target=lane, args=(q,)) for q in range(L)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        if errors:
+            raise errors[0]
+
+    def timed(self, dt, T, k, start_stream, **kw):
+        """`k` runs between two events on `start_stream`; every lane waits on the start event and
+        the end event waits on every lane."""
+        import torch
+
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(start_stream)
+        for s in self.streams:
+            s.wait_event(start)
+        for _ in range(k):
+            self.run(dt, T, **kw)
+        for s in self.streams:
+            e = torch.cuda.Event()
+            e.record(s)
+            start_stream.wait_event(e)
+        end.record(start_stream)
+        return start, end
+
+    def close(self):
+        for c in self.cavs:
+            c.close()
+        self.cavs = []
+
+
+def cpu_baseline_mix(hall_cells, cav_cells, n_sample=128, sample_steps=32):
+    """The reference's CPU path (the oracle) on a bounded sample of the mixed workload: a hall of
+    `n_sample`³ nodes over the same 32³ speed blocks and one dielectric cavity of `n_sample`³
+    cells, `sample_steps` audited steps each on one core; the rate is the mix's: its cell-updates
+    over the time the per-cell costs give for its hall and cavity cells."""
+    import oracle
+    from pantometry_b200 import workloads as W
+
+    h = W.hetero_hall(n_sample, steps=sample_steps + 1)
+    w, ht, d = h["size"]
+    o = oracle.Hall(w, ht, d, h["across"], h["speed"], h["density"])
+    o.release(h["pressure"])
+    o.set_speed_blocks(h["block"], h["speeds"])
+    o.set_source(h["source_node"], h["wave"])
+    assert o.advance(h["dt"], 1) is None
+    t0 = time.perf_counter()
+    assert o.advance(h["dt"], sample_steps) is None
+    t_hall = (time.perf_counter() - t0) / (n_sample ** 3 * sample_steps)
+    del o
+    c = W.dielectric_cavities(1, n_sample, steps=sample_steps + 1)
+    y = oracle.Yee(c["counts"], c["dx"])
+    y.set_cells(eps_r=c["cavities"][0]["eps"])
+    y.set_source(c["edge"], c["current"])
+    assert y.advance(c["dt"], 1) is None
+    t0 = time.perf_counter()
+    assert y.advance(c["dt"], sample_steps) is None
+    t_cav = (time.perf_counter() - t0) / (n_sample ** 3 * sample_steps)
+    value = (hall_cells + cav_cells) / (t_hall * hall_cells + t_cav * cav_cells) / 1e9
+    return {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{sample_steps} audited Simulation::advance steps of a {n_sample}^3 speed-block hall "
+                      f"({t_hall * 1e9:.1f} ns per node-update) and of a {n_sample}^3 dielectric cavity "
+                      f"({t_cav * 1e9:.1f} ns per cell-update), weighted by the mix's cells"}
+
+
+def run_mix(args):
+    """Config 5 on one GPU: the 1024³ acoustic hall in FP32 over a medium of 32³-node blocks with c
+    uniform in [300, 1500] m/s (CFL 0.5 of the fastest block, 1 Pa Ricker at the centre, ±1 mPa
+    noise), then 64 Yee cavities of 128³ cells in FP32 with ε_r uniform in [1, 4] in 10% of the
+    cells (Courant 0.99/√3, the dipole current at the centre edge); every timestep of both audited
+    in FP64. One bench step = `timesteps` steps of the hall followed by `timesteps` steps of every
+    cavity."""
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import workloads as W
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = init_dist(local) if world > 1 else None
+    n, T, K, Wm = args.n, args.timesteps, args.steps, args.warmup
+    total_steps = T * (K + Wm + 2)
+    hcfg = W.hetero_hall(n, steps=total_steps)
+    ccfg = W.dielectric_cavities(args.grids, args.cavity_n, steps=total_steps)
+    hall_cells = n ** 3
+    cav_cells = len(ccfg["cavities"]) * args.cavity_n ** 3
+    stream = torch.cuda.Stream(device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def hall_run(h, k):
+        for _ in range(k):
+            v = h.step(hcfg["dt"], T)
+            assert v is None, v
+
+    # ---- FP32, device-resident: K bench steps after Wm warm-up steps
+    hall = W.build_hetero_hall(hcfg, precision="f32", device=local)
+    hall.set_stream(stream.cuda_stream)
+    hall.set_tolerance(1e-5)
+    cavs = CavityBatch(ccfg, "f32", local)
+    cavs.set_tolerance(1e-5)
+    for _ in range(Wm):
+        hall_run(hall, 1)
+        cavs.run(ccfg["dt"], T)
+    barrier()
+    with Clocks(local) as clk:
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms_hall = ms_cav = 0.0
+        for _ in range(K):
+            h0.record(stream)
+            hall_run(hall, 1)
+            h1.record(stream)
+            c0, c1 = cavs.timed(ccfg["dt"], T, 1, stream)
+            torch.cuda.synchronize()
+            ms_hall += h0.elapsed_time(h1)
+            ms_cav += c0.elapsed_time(c1)
+    barrier()
+    ms_hall, ms_cav = max_over_ranks(ms_hall), max_over_ranks(ms_cav)
+    ms32 = max_over_ranks(ms_hall + ms_cav)
+
+    # ---- e2e through the C ABI with host buffers: the hall's pressure and every cavity's six
+    # fields from pinned memory, the runs, the hall's pressure and every ledger back, each step
+    p_pin = torch.empty(hall_cells, dtype=torch.float64, pin_memory=True).numpy()
+    p_pin[:] = hcfg["pressure"]
+    p_out = torch.empty(hall_cells, dtype=torch.float64, pin_memory=True).numpy()
+    shapes = cavs.cavs[0].shapes()
+    zero = {q: torch.zeros(m, dtype=torch.float64, pin_memory=True).numpy() for q, m in shapes.items()}
+    barrier()
+    t0 = time.perf_counter()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(K):
+        hall.release(p_pin)
+        hall_run(hall, 1)
+        hall.ledger()
+        hall.download_pressure(p_out)
+        cavs.run(ccfg["dt"], T, before=lambda g, c: c.set_fields(zero, started=False), each=lambda g, c: c.ledger())
+    s1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(max(s0.elapsed_time(s1), (time.perf_counter() - t0) * 1e3))
+    hall.close()
+    cavs.close()
+    del hall, cavs, p_pin, p_out
+
+    # ---- drift against the f64 form (bit-exact with the oracle): one bench step of each from the
+    # same start; the plain f64 rate from the same runs
+    def one(precision, tol):
+        h = W.build_hetero_hall(hcfg, precision=precision, device=local)
+        h.set_stream(stream.cuda_stream)
+        h.set_tolerance(tol)
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        hall_run(h, 1)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        out = np.empty(hall_cells, dtype=np.float64)
+        h.download_pressure(out)
+        led = h.ledger()
+        h.close()
+        return out, led, ms
+
+    p32, l32, _ = one("f32", 1e-5)
+    p64, l64, ms64_hall = one("f64", 1e-9)
+    scale = float(np.abs(p64).max())
+    hall_err = float(np.abs(p32 - p64).max()) / max(scale, 1e-300)
+    hall_drift = abs(l32["total"] - l64["total"]) / max(abs(l64["total"]), l64["scale"], 1e-300)
+    del p32, p64
+
+    def cav_fields(precision, tol):
+        b = CavityBatch(ccfg, precision, local)
+        b.set_tolerance(tol)
+        barrier()
+        c0, c1 = b.timed(ccfg["dt"], T, 1, stream)
+        torch.cuda.synchronize()
+        ms = c0.elapsed_time(c1)
+        got = [(c.fields(), c.ledger()) for c in b.cavs[:4]]
+        b.close()
+        return got, ms
+
+    f32c, _ = cav_fields("f32", 1e-5)
+    f64c, ms64_cav = cav_fields("f64", 1e-9)
+    cav_err = cav_drift = 0.0
+    for (fa, la), (fb, lb) in zip(f32c, f64c):
+        for fam in (("ex", "ey", "ez"), ("hx", "hy", "hz")):
+            sc = max(float(np.abs(fb[q]).max()) for q in fam)
+            cav_err = max(cav_err, max(float(np.abs(fa[q] - fb[q]).max()) for q in fam) / max(sc, 1e-300))
+        cav_drift = max(cav_drift, abs(la["total"] - lb["total"]) / max(abs(lb["total"]), lb["scale"], 1e-300))
+    ms64 = max_over_ranks(ms64_hall + ms64_cav)
+
+    peak, peak_kind = peaks()
+    updates = hall_cells * T + cav_cells * T
+    value = world * updates * K / (ms32 * 1e-3) / 1e9
+    plain = world * updates / (ms64 * 1e-3) / 1e9
+    hall_rate = hall_cells * T * K / (ms_hall * 1e-3) / 1e9
+    cav_rate = cav_cells * T * K / (ms_cav * 1e-3) / 1e9
+    per_launch_ms = ms_hall / (K * T)
+    achieved = BYTES_F32 * hall_cells / (per_launch_ms * 1e-3) / 1e9
+    # whole-step algorithmic bytes: 32 B per hall node-update; per cavity cell-update 48 B of fields,
+    # 12 B of per-edge gain (f32) and 24 B of per-edge ε (f64, the audit's weights)
+    step_bytes = T * (BYTES_F32 * hall_cells + 84 * cav_cells)
+    h2d = hall_cells * 8 + len(ccfg["cavities"]) * sum(shapes.values()) * 8
+    d2h = hall_cells * 8 + 64 * (1 + len(ccfg["cavities"]))
+    line = {
+        "metric": MIX_METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": round(ms32 / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 fields, f64 audit",
+        "data": "synthetic (seeded Rng::for_index block speeds, noise, inclusions and eps_r; Ricker and dipole sources)",
+        "config": {"workload": f"hetero acoustic_hall {n}^3 nodes (c per 32^3 block in [300, 1500] m/s, CFL 0.5) "
+                               f"+ {len(ccfg['cavities'])} yee_cavity {args.cavity_n}^3 cells (eps_r in [1, 4] in 10% of "
+                               f"cells), {T} timesteps of each per step, FP64 audit every timestep",
+                   "cells": hall_cells + cav_cells, "timesteps_per_step": T, "parallelism": f"replicas x{world}",
+                   "l2": f"state {(16 * hall_cells + 24 * cav_cells) / 1e9:.1f} GB > 126 MB L2, no flush"},
+        "e2e": {"value": round(world * updates * K / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": K * T * (1 + len(ccfg["cavities"])),
+        "parts": {"hall": {"value": round(hall_rate, 3), "ms_per_step": round(ms_hall / K, 3)},
+                  "cavities": {"value": round(cav_rate, 3), "ms_per_step": round(ms_cav / K, 3)}},
+        "hbm_frac_whole_step": round(step_bytes / (ms32 / K * 1e-3) / 1e9 / peak, 4),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "kernel": "hall_tma_step (FP32, TMA-staged, speed blocks)",
+                     "bytes_per_launch": BYTES_F32 * hall_cells, "peak_source": f"{peak_kind} hbm_gbs"},
+        "plain_f64": {"value": round(plain, 3), "unit": UNIT, "fp32_over_f64": round(value / plain, 3)},
+        "error_vs_f64": {"hall_max_rel_pressure": hall_err, "hall_ledger_rel": hall_drift,
+                         "cavity_max_rel_field": cav_err, "cavity_ledger_rel": cav_drift, "after_timesteps": T,
+                         "cavities_compared": len(f32c)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_mix(hall_cells, cav_cells)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def cpu_baseline_ensemble(cfg, grids, sample_steps=2, threads=1, sample_grids=16):
     """`Ensemble::run` over `Solid3D` samples, restated (the oracle): the first `sample_grids`
     grids, each with its own audited `Simulation::advance` steps, `threads` grids at a time."""
@@ -685,22 +976,34 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble", "cavity"],
+    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble", "cavity", "mix"],
                     help="hall: the acoustic hall 256^3 (the headline); ensemble: 512 uneven heat grids; "
-                         "cavity: the Yee cavity 384^3")
+                         "cavity: the Yee cavity 384^3; mix: the 1024^3 heterogeneous hall and 64 Yee 128^3 "
+                         "dielectric cavities")
+    ap.add_argument("--cavity-n", type=int, default=128, help="mix: cells per axis of each cavity")
     ap.add_argument("--n", type=int, default=None, help="grid size: hall 256 nodes, cavity 384 cells per axis")
-    ap.add_argument("--grids", type=int, default=512)
+    ap.add_argument("--grids", type=int, default=None, help="ensemble: 512 heat grids; mix: 64 cavities")
     ap.add_argument("--timesteps", type=int, default=None, help="timesteps per bench step (hall 5000, ensemble 2000)")
     ap.add_argument("--cpu-sample-steps", type=int, default=None,
                     help="audited steps per CPU sample (hall 16, ensemble 8): about 10 s of one core")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.n is None:
-        args.n = 384 if args.workload == "cavity" else 256
+        args.n = {"cavity": 384, "mix": 1024}.get(args.workload, 256)
+    if args.grids is None:
+        args.grids = 64 if args.workload == "mix" else 512
     if args.timesteps is None:
         args.timesteps = 5000 if args.workload == "hall" else 2000
     if args.cpu_sample_steps is None:
         args.cpu_sample_steps = 16 if args.workload == "hall" else 8
+    if args.workload == "mix":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "workload": "mix",
+                              "unavailable": "the reference arm times the headline hall and the ensemble; "
+                                             "the mix's parts are timed per cell in the hall and cavity arms"}))
+        else:
+            run_mix(args)
+        return
     if args.workload == "cavity":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "workload": "cavity",

@@ -549,9 +549,13 @@ struct Hall {
 
     double energy() const { return invariant_si() + offset; }  // hall.rs:249-251
 
-    or_entry ledger() const {  // hall.rs:532-534 (+ the source term, when a source is set)
+    // hall.rs:532-534, plus the source's injected work as an entry of its own, the way the
+    // cavity books its source work (cavity.rs:1520-1524): the audit's scale then covers what the
+    // source moved, not only the small net left after it.
+    or_entry ledger() const {
         or_entry e{0.0, 0.0};
-        ledger_add(e, energy() - injected);
+        ledger_add(e, energy());
+        if (source_node >= 0) ledger_add(e, -injected);
         return e;
     }
 };

@@ -25,6 +25,13 @@ struct Cavity : Handle {
     std::vector<double> cell_eps, cell_mu, cell_sig;  // per cell, relative ε, μ and σ
     std::vector<double> eps[3], sig[3], mu[3];
     DBuf deps[3], dsig[3], dmu[3];
+    // mixed media: the per-edge gain and decay and per-face g/μ of the step size coef_dt (in the
+    // field type), and what the media leave uniform: σ = 0 on every edge (lossless, no decay
+    // array) and one μ on every face (mu_one, no g/μ array)
+    DBuf dgain[3], ddecay[3], dch[3];
+    double coef_dt = NAN;
+    bool lossless = true, mu_var = false;
+    double mu_one = 0.0;
     std::vector<uint8_t> solid;
     bool any_solid = false;
     DBuf dsolid;
@@ -135,6 +142,13 @@ struct Cavity : Handle {
         for (int q = 0; q < 3; ++q)
             for (double& v : mu[q])
                 if (v <= 0.0) v = fallback;
+        lossless = true;
+        for (int q = 0; q < 3; ++q)
+            for (double v : sig[q]) lossless = lossless && v == 0.0;
+        mu_one = mu[0].empty() ? permeability() : mu[0][0];
+        mu_var = false;
+        for (int q = 0; q < 3; ++q)
+            for (double v : mu[q]) mu_var = mu_var || v != mu_one;
     }
 
     // The uniform values every edge and face of a one-medium box holds (the same means).
@@ -239,6 +253,17 @@ struct Cavity : Handle {
         }
         a.eps0 = deps[0].as<double>(); a.eps1 = deps[1].as<double>(); a.eps2 = deps[2].as<double>();
         a.sig0 = dsig[0].as<double>(); a.sig1 = dsig[1].as<double>(); a.sig2 = dsig[2].as<double>();
+        if (!uniform) {
+            for (int q = 0; q < 3; ++q) {
+                a.cgain[q] = dgain[q].as<Real>();
+                a.cdecay[q] = lossless ? nullptr : ddecay[q].as<Real>();
+                a.cch[q] = mu_var ? dch[q].as<Real>() : nullptr;
+                if (lossless) { a.decay[q] = Real(1); a.sigma_u[q] = 0.0; }  // (1 − 0)/(1 + 0)
+            }
+            a.lossless = lossless ? 1 : 0;
+            a.mu_var = mu_var ? 1 : 0;
+            if (!mu_var) { a.mu_u = mu_one; a.ch = (Real)(a.g / mu_one); }
+        }
         a.solid = any_solid ? dsolid.as<uint8_t>() : nullptr;
         a.src_i = a.src_j = a.src_k = -1;
         if (src >= 0) {
@@ -514,7 +539,38 @@ struct Cavity : Handle {
             PM_CUDA(put_sync(deps[q].p, eps[q].data(), eps[q].size() * 8));
             PM_CUDA(put_sync(dsig[q].p, sig[q].data(), sig[q].size() * 8));
             PM_CUDA(put_sync(dmu[q].p, mu[q].data(), mu[q].size() * 8));
+            PM_CUDA(dgain[q].alloc(eps[q].size() * esize()));
+            if (lossless) ddecay[q].release();
+            else PM_CUDA(ddecay[q].alloc(eps[q].size() * esize()));
+            if (mu_var) PM_CUDA(dch[q].alloc(mu[q].size() * esize()));
+            else dch[q].release();
         }
+        coef_dt = NAN;
+        return PM_OK;
+    }
+
+    // The mixed media's coefficients for step size h, once per change of h (or of the media).
+    template <typename Real>
+    YeeCoefArgs<Real> cargs(double h) const {
+        YeeCoefArgs<Real> a{};
+        for (int q = 0; q < 3; ++q) {
+            a.eps[q] = deps[q].as<double>();
+            a.sig[q] = dsig[q].as<double>();
+            a.mu[q] = dmu[q].as<double>();
+            a.gain[q] = dgain[q].as<Real>();
+            a.decay[q] = lossless ? nullptr : ddecay[q].as<Real>();
+            a.ch[q] = mu_var ? dch[q].as<Real>() : nullptr;
+            a.ne[q] = count(q);
+            a.nf[q] = count(q + 3);
+        }
+        a.dt = h; a.dx = dx; a.g = h / dx;
+        return a;
+    }
+    pm_status prepare_coefs(double h) {
+        if (uniform || coef_dt == h) return PM_OK;
+        if (precision == PM_PLAIN_F64) PM_CUDA(launch_yee_coefs<double>(cargs<double>(h), stream()));
+        else PM_CUDA(launch_yee_coefs<float>(cargs<float>(h), stream()));
+        coef_dt = h;
         return PM_OK;
     }
 };
@@ -770,6 +826,7 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
     }
     pm_status s = c->begin_call();
     if (s != PM_OK) return s;
+    if ((s = c->prepare_coefs(h)) != PM_OK) return s;
     const long long before = c->host_state->steps;
     if (!c->started) {  // cavity.rs:1486-1489
         s = c->with_reference_layout(true, [&]() { return c->launch_h((0.5 * h) / c->dx, 0, c->stream()); });

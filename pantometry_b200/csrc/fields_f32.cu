@@ -184,6 +184,11 @@ cudaError_t launch_yee_walls<float>(const YeeWallArgs<float>& a, cudaStream_t s)
     yee_walls<float><<<kMeasureBlocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
+template <>
+cudaError_t launch_yee_coefs<float>(const YeeCoefArgs<float>& a, cudaStream_t s) {
+    yee_coefs<float><<<kMeasureBlocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
 
 int occupancy_f32(KernelId id) {
     int n = 0;

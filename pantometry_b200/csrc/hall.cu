@@ -102,6 +102,31 @@ struct Hall : Handle {
         return PM_OK;
     }
 
+    // The ledger of the state in host_state: the energy, then the source's injected work as an
+    // entry of its own, the same two entries the step kernel books.
+    void book_totals() {
+        DevState* st = host_state;
+        const double energy = st->invariant + st->offset;
+        st->total = energy - st->injected;
+        st->scale = std::fmax(std::fabs(energy), std::fabs(st->injected));
+        st->part[0] = st->total;
+    }
+
+    // The source node's share of the invariant, share · V/(2ρc²), at the speed of the source's
+    // own block when the medium has blocks (whichever of the source and the blocks came first).
+    void weigh_source() {
+        if (src < 0) return;
+        const int i = (int)(src % nx), j = (int)((src / nx) % ny), k = (int)(src / ((long long)nx * ny));
+        auto w = [](int q, int m) { return (q == 0 || q + 1 == m) ? 2.0 : 1.0; };
+        const double share = 1.0 / (w(i, nx) * w(j, ny) * w(k, nz));
+        double r = rc2();
+        if (block > 0) {
+            const double c = speeds[(size_t)(i / block) + (size_t)nbx * ((size_t)(j / block) + (size_t)nby * (k / block))];
+            r = density * c * c;
+        }
+        wsrc = share * (dx * dx * dx) / (2.0 * r);
+    }
+
     // Per-block scale h·ρc_b²/dx (in the field type) and invariant weight V/(2ρc_b²).
     pm_status upload_block_scale(double h) {
         if (block <= 0 || bscale_dt == h) return PM_OK;
@@ -302,14 +327,7 @@ pm_status pm_hall_set_source(pm_hall* hp, long long node, const double* wave, si
         PM_CUDA(h->wave.alloc(n * 8));
         PM_CUDA(h->put_sync(h->wave.p, wave, n * 8));
     }
-    const int i = (int)(node % h->nx), j = (int)((node / h->nx) % h->ny), k = (int)(node / ((long long)h->nx * h->ny));
-    auto w = [](int q, int m) { return (q == 0 || q + 1 == m) ? 2.0 : 1.0; };
-    const double share = 1.0 / (w(i, h->nx) * w(j, h->ny) * w(k, h->nz));
-    h->wsrc = share * (h->dx * h->dx * h->dx) / (2.0 * h->rc2());
-    if (h->block > 0) {
-        const double c = h->speeds[(size_t)(i / h->block) + (size_t)h->nbx * ((size_t)(j / h->block) + (size_t)h->nby * (k / h->block))];
-        h->wsrc = share * (h->dx * h->dx * h->dx) / (2.0 * (h->density * c * c));
-    }
+    h->weigh_source();
     h->drop_graphs();
     return PM_OK;
 }
@@ -323,6 +341,7 @@ pm_status pm_hall_set_speed_blocks(pm_hall* hp, int block, const double* speeds,
     h->block = block; h->nbx = nbx; h->nby = nby; h->nbz = nbz;
     h->speeds.assign(speeds, speeds + n);
     h->max_speed = *std::max_element(h->speeds.begin(), h->speeds.end());
+    h->weigh_source();
     h->bscale_dt = NAN;
     h->bscale.release();
     h->bknode.release();
@@ -336,8 +355,7 @@ pm_status pm_hall_set_speed_blocks(pm_hall* hp, int block, const double* speeds,
     DevState* st = h->host_state;
     if (!h->staggered) {
         st->datum = st->invariant;
-        st->total = st->invariant + st->offset - st->injected;
-        st->scale = std::fabs(st->total);
+        h->book_totals();
         st->prev_total = st->total;
         st->prev_scale = st->scale;
     }
@@ -459,9 +477,7 @@ pm_status pm_hall_restore(pm_hall* hp) {
     pm_status s = h->measure(par, par ^ 1);
     if (s != PM_OK) return s;
     DevState* st = h->host_state;
-    st->total = st->invariant + st->offset - st->injected;
-    st->scale = std::fabs(st->total);
-    st->part[0] = st->total;
+    h->book_totals();
     st->prev_total = st->total;
     st->prev_scale = st->scale;
     return h->write_state();

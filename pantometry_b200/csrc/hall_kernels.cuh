@@ -249,10 +249,12 @@ __device__ __forceinline__ void hall_finish(const HallArgs<Real>& a, double (&ac
                 st->offset = off;
             }
         }
+        // the energy, then the source's injected work as an entry of its own (zero without a
+        // source): the total is the same sum, and the scale covers what the source moved
         double total = 0.0, scale = 0.0;
-        const double energy = plus + st->offset - st->injected;
-        ledger_add(total, scale, energy);
-        st->part[0] = energy;
+        ledger_add(total, scale, plus + st->offset);
+        ledger_add(total, scale, -st->injected);
+        st->part[0] = total;
         st->invariant = plus;
         audit_and_commit(st, total, scale);
     }

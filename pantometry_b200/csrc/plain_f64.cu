@@ -98,6 +98,11 @@ cudaError_t launch_yee_walls<double>(const YeeWallArgs<double>& a, cudaStream_t 
     yee_walls<double><<<kMeasureBlocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
+template <>
+cudaError_t launch_yee_coefs<double>(const YeeCoefArgs<double>& a, cudaStream_t s) {
+    yee_coefs<double><<<kMeasureBlocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
 
 int occupancy_f64(KernelId id) {
     int n = 0;

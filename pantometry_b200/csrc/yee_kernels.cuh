@@ -370,7 +370,46 @@ struct YeeStepArgs {
     DevState* st;
     double* partials;
     unsigned nblocks;
+    // Mixed media, the coefficients of this dt computed once by yee_coefs: gain and decay per
+    // edge component, g/μ per face component. lossless: σ is 0 on every edge (decay 1, no Joule
+    // term; cdecay and σ never read). mu_var: μ differs between faces (otherwise every face holds
+    // mu_u and its coefficient ch; cch and μ never read).
+    const Real* __restrict__ cgain[3];
+    const Real* __restrict__ cdecay[3];
+    const Real* __restrict__ cch[3];
+    int lossless, mu_var;
 };
+
+// The per-edge and per-face coefficients of one dt for a cavity of mixed media, exactly the values
+// the update would otherwise form at every edge and face of every step (cavity.rs:1355 and
+// 1391-1397): gain and decay from ε and σ, g/μ from μ.
+template <typename Real>
+struct YeeCoefArgs {
+    const double* eps[3];
+    const double* sig[3];
+    const double* mu[3];
+    Real* gain[3];
+    Real* decay[3];  // null: lossless
+    Real* ch[3];     // null: one μ
+    size_t ne[3], nf[3];
+    double dt, dx, g;
+};
+
+template <typename Real>
+static __global__ void yee_coefs(YeeCoefArgs<Real> a) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (int q = 0; q < 3; ++q) {
+        for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.ne[q]; c += stride) {
+            Real d, g;
+            coefficients<Real>(a.eps[q][c], a.sig[q][c], a.dt, a.dx, d, g);
+            a.gain[q][c] = g;
+            if (a.decay[q]) a.decay[q][c] = d;
+        }
+        if (a.ch[q])
+            for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.nf[q]; c += stride)
+                a.ch[q][c] = (Real)(a.g / a.mu[q][c]);
+    }
+}
 
 // Halo value e (0 .. 288) of a stage: component, row, column.
 __device__ __forceinline__ void yee_halo_elem(int e, int& q, int& r, int& c) {
@@ -525,7 +564,7 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
     const long long step = st->steps;
     const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
     const double dt = a.dt;
-    const bool lossy = !UNIFORM || a.sigma_u[0] != 0.0;
+    const bool lossy = UNIFORM ? a.sigma_u[0] != 0.0 : !a.lossless;
     // Σ wεE², Σ wμH⁺H⁻ (each already weighted), Joule loss, source work
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
 
@@ -594,9 +633,11 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
         Real cx = ch, cy = ch, cz = ch;
         double mux = a.mu_u, muy = a.mu_u, muz = a.mu_u;
         if constexpr (!UNIFORM) {
-            if (fx) { mux = a.mu0[own_h[3]]; cx = (Real)(a.g / mux); }
-            if (fy) { muy = a.mu1[own_h[4]]; cy = (Real)(a.g / muy); }
-            if (fz) { muz = a.mu2[own_h[5]]; cz = (Real)(a.g / muz); }
+            if (a.mu_var) {
+                if (fx) { mux = a.mu0[own_h[3]]; cx = a.cch[0][own_h[3]]; }
+                if (fy) { muy = a.mu1[own_h[4]]; cy = a.cch[1][own_h[4]]; }
+                if (fz) { muz = a.mu2[own_h[5]]; cz = a.cch[2][own_h[5]]; }
+            }
         }
         const Real hxn = wx - cx * ((S0.ez[ty + 2][tx + 1] - ez0) - (S1.ey[ty + 1][tx + 1] - ey0));
         const Real hyn = wy - cy * ((S1.ex[ty + 1][tx + 1] - ex0) - (S0.ez[ty + 1][tx + 2] - ez0));
@@ -631,8 +672,8 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
             Real c1 = ch, c2 = ch;
             if constexpr (!UNIFORM) {
                 const int ii = cw.x0 + tx, jj = cw.y0 - 1;
-                if (jj >= 0 && ii <= nx && zin) c1 = (Real)(a.g / a.mu0[(unsigned)ii + (unsigned)(nx + 1) * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
-                if (jj >= 0 && ii < nx) c2 = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+                if (a.mu_var && jj >= 0 && ii <= nx && zin) c1 = a.cch[0][(unsigned)ii + (unsigned)(nx + 1) * ((unsigned)jj + (unsigned)ny * (unsigned)k)];
+                if (a.mu_var && jj >= 0 && ii < nx) c2 = a.cch[2][(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)];
             }
             hp->hx[0][tx] = S0.hx[0][tx] - c1 * ((S0.ez[1][tx + 1] - S0.ez[0][tx + 1]) - (S1.ey[0][tx + 1] - S0.ey[0][tx + 1]));
             hp->hz[0][tx + 1] = S0.hz[0][tx + 1] - c2 * ((S0.ey[0][tx + 2] - S0.ey[0][tx + 1]) - (S0.ex[1][tx + 1] - S0.ex[0][tx + 1]));
@@ -643,8 +684,8 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
             Real c1 = ch, c2 = ch;
             if constexpr (!UNIFORM) {
                 const int ii = cw.x0 - 1, jj = cw.y0 - 1 + r;
-                if (ii >= 0 && jj >= 0 && jj <= ny && zin) c1 = (Real)(a.g / a.mu1[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)]);
-                if (ii >= 0 && jj >= 0 && jj < ny) c2 = (Real)(a.g / a.mu2[(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)]);
+                if (a.mu_var && ii >= 0 && jj >= 0 && jj <= ny && zin) c1 = a.cch[1][(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)(ny + 1) * (unsigned)k)];
+                if (a.mu_var && ii >= 0 && jj >= 0 && jj < ny) c2 = a.cch[2][(unsigned)ii + (unsigned)nx * ((unsigned)jj + (unsigned)ny * (unsigned)k)];
             }
             if (r >= 1) hp->hy[r - 1][0] = S0.hy[r - 1][0] - c1 * ((S1.ex[r][0] - S0.ex[r][0]) - (S0.ez[r][1] - S0.ez[r][0]));
             hp->hz[r][0] = S0.hz[r][0] - c2 * ((S0.ey[r][1] - S0.ey[r][0]) - (S0.ex[r + 1][0] - S0.ex[r][0]));
@@ -660,9 +701,16 @@ static __global__ void __launch_bounds__(256, YeeDepth<Real>::min_blocks) yee_st
             Real d0 = dec0, g0 = gain0, d1 = dec0, g1 = gain0, d2 = dec0, g2 = gain0;
             double s0 = a.sigma_u[0], s1 = s0, s2 = s0;
             if constexpr (!UNIFORM) {
-                if (i < nx && in_y && iy && iz) { s0 = a.sig0[own_h[0]]; coefficients<Real>(a.eps0[own_h[0]], s0, dt, a.dx, d0, g0); }
-                if (in_x && j < ny && ix && iz) { s1 = a.sig1[own_h[1]]; coefficients<Real>(a.eps1[own_h[1]], s1, dt, a.dx, d1, g1); }
-                if (in_x && in_y && zin && ix && iy) { s2 = a.sig2[own_h[2]]; coefficients<Real>(a.eps2[own_h[2]], s2, dt, a.dx, d2, g2); }
+                const bool e0 = i < nx && in_y && iy && iz, e1 = in_x && j < ny && ix && iz,
+                           e2 = in_x && in_y && zin && ix && iy;
+                if (e0) g0 = a.cgain[0][own_h[0]];
+                if (e1) g1 = a.cgain[1][own_h[1]];
+                if (e2) g2 = a.cgain[2][own_h[2]];
+                if (!a.lossless) {
+                    if (e0) { s0 = a.sig0[own_h[0]]; d0 = a.cdecay[0][own_h[0]]; }
+                    if (e1) { s1 = a.sig1[own_h[1]]; d1 = a.cdecay[1][own_h[1]]; }
+                    if (e2) { s2 = a.sig2[own_h[2]]; d2 = a.cdecay[2][own_h[2]]; }
+                }
             }
             Real vx = d0 * ex0 + g0 * cex;
             Real vy = d1 * ey0 + g1 * cey;

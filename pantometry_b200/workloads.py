@@ -15,6 +15,7 @@ Configurations (sizes, media and sources as the benchmark names them):
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
@@ -56,6 +57,25 @@ class Streams:
 
     def range(self, lo, hi):
         return lo + (hi - lo) * self.unit()
+
+
+def uniform_noise(seed, count, lo, hi, out=None, chunk=1 << 22):
+    """`Rng::for_index(seed, i).range(lo, hi)` for i in 0..count, drawn in chunks so that a
+    10⁹-node field needs no more host memory than its own array (`out`, if given, e.g. pinned)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    out = np.empty(count, dtype=np.float64) if out is None else out
+
+    def fill(a):
+        b = min(count, a + chunk)
+        out[a:b] = Streams(seed, np.arange(a, b, dtype=np.uint64)).range(lo, hi)
+
+    if count <= chunk:
+        fill(0)
+        return out
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as pool:  # numpy drops the GIL
+        list(pool.map(fill, range(0, count, chunk)))
+    return out
 
 
 # ------------------------------------------------------------------------------------------
@@ -112,7 +132,7 @@ def ricker(t, f):
 def acoustic_hall(n=256, seed=SEED, steps=5000, dx=5e-3, speed=343.0, density=1.2, source=True):
     width = (n - 1) * dx
     nodes = n * n * n
-    p = Streams(seed, np.arange(nodes, dtype=np.uint64)).range(-1e-3, 1e-3)
+    p = uniform_noise(seed, nodes, -1e-3, 1e-3)
     dx_eff = max(width / (n - 1), np.finfo(np.float64).tiny)  # Hall::new (hall.rs:109)
     dt = 0.5 * dx_eff / (speed * math.sqrt(3.0))
     c = n // 2
@@ -168,6 +188,51 @@ def build_cavity(cfg, precision="f64", device=0):
     cav = Cavity(cfg["counts"], cfg["dx"], precision=precision, device=device)
     if "current" in cfg:
         cav.set_source(cfg["edge"], cfg["current"])
+    return cav
+
+
+# ------------------------------------------------------------------------------------------
+# config 5: a 1024³ hall in a medium of 32³-node blocks (c uniform in [300, 1500] m/s per block)
+# and 64 Yee cavities of 128³ cells with dielectric inclusions (ε_r uniform in [1, 4] in 10% of
+# cells)
+# ------------------------------------------------------------------------------------------
+def hetero_hall(n=1024, block=32, seed=SEED, steps=2000, dx=5e-3, density=1.2, lo=300.0, hi=1500.0):
+    cfg = acoustic_hall(n, seed=seed, steps=steps, dx=dx, density=density, source=True)
+    nb = -(-n // block)
+    speeds = Streams(seed ^ 0x5EED, np.arange(nb ** 3, dtype=np.uint64)).range(lo, hi)
+    cfg["block"] = block
+    cfg["speeds"] = speeds
+    cfg["speed"] = float(speeds.max())  # the descriptor's speed: the limit follows the fastest block
+    cfg["dt"] = 0.5 * dx / (cfg["speed"] * math.sqrt(3.0))  # CFL 0.5 of the fastest block
+    return cfg
+
+
+def build_hetero_hall(cfg, precision="f32", device=0):
+    hall = build_hall(cfg, precision=precision, device=device)
+    hall.set_speed_blocks(cfg["block"], cfg["speeds"])
+    return hall
+
+
+def dielectric_cavities(count=64, n=128, seed=SEED, steps=2000, dx=1e-3, fraction=0.1, lo=1.0, hi=4.0):
+    """Per cavity g: a Bernoulli(fraction) draw per cell from Rng::for_index(seed + g, cell) picks the
+    inclusions, a second draw their ε_r; the dipole current of yee_cavity at the centre edge."""
+    base = yee_cavity(n, steps=steps, dx=dx)
+    cavities = []
+    for g in range(count):
+        r = Streams(seed + 1 + g, np.arange(n ** 3, dtype=np.uint64))
+        pick = r.unit() < fraction
+        eps = np.where(pick, r.range(lo, hi), 1.0)
+        cavities.append({"eps": eps})
+    return {"counts": (n, n, n), "dx": dx, "dt": base["dt"], "edge": base["edge"], "current": base["current"],
+            "cavities": cavities, "steps": steps}
+
+
+def build_dielectric_cavity(cfg, g, precision="f32", device=0):
+    from .domains import Cavity
+
+    cav = Cavity(cfg["counts"], cfg["dx"], precision=precision, device=device)
+    cav.fill_cells(eps_r=cfg["cavities"][g]["eps"])
+    cav.set_source(cfg["edge"], cfg["current"])
     return cav
 
 

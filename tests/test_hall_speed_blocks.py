@@ -65,4 +65,71 @@ def test_speed_blocks_f32(across):
         scale = max(np.abs(fo[k]).max(), 1e-30)
         assert np.abs(fg[k] - fo[k]).max() < 1e-4 * scale, k
     lo, lg = o.ledger(), g.ledger()
-    assert abs(lg["total"] - lo["total"]) < 1e-5 * abs(lo["total"])
+    assert abs(lg["total"] - lo["total"]) < 1e-5 * lo["scale"]
+
+
+
+def _sourced(order, precision, across):
+    """A hall with a Ricker source at an off-centre node, the blocks set before or after the
+    source (the source's share of the invariant follows its own block either way); `precision`
+    None builds the oracle alone."""
+    from pantometry_b200 import workloads as W
+
+    o = oracle.Hall(0.115, 0.115, 0.115, across, 343.0, 1.2)
+    doms = [o]
+    if precision is not None:
+        from pantometry_b200.domains import Hall
+
+        doms.append(Hall(0.115, 0.115, 0.115, across, 343.0, 1.2, precision=precision))
+    noise = W.Streams(11, np.arange(o.n, dtype=np.uint64)).range(-1e-3, 1e-3)
+    sp = speeds(blocks_for(o.nodes, 8), seed=3)
+    node = 5 + across * (6 + across * 9)
+    dt = 0.5 * (0.115 / (across - 1)) / (float(sp.max()) * 3 ** 0.5)
+    wave = W.ricker((np.arange(400) + 1.0) * dt, 2.0 / (40 * dt))
+    for d in doms:
+        d.release(noise)
+        if order == "blocks_first":
+            d.set_speed_blocks(8, sp)
+            d.set_source(node, wave)
+        else:
+            d.set_source(node, wave)
+            d.set_speed_blocks(8, sp)
+    return doms, dt
+
+
+@pytest.mark.parametrize("order", ["blocks_first", "source_first"])
+def test_speed_blocks_with_source_conserve_in_the_oracle(order):
+    (o,), dt = _sourced(order, None, 24)
+    assert o.advance(dt, 300, tol=1e-9) is None
+    led = o.ledger()
+    # the injected work is booked as an entry of its own, so the scale covers it (here the net
+    # total is the noise's energy, some 600 times smaller than what the source moved)
+    assert led["scale"] >= abs(led["injected"]) > 100 * abs(led["total"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", ["blocks_first", "source_first"])
+def test_speed_blocks_with_source_plain_bitexact(order):
+    (o, g), dt = _sourced(order, "f64", 24)
+    g.set_tolerance(1e-9)
+    assert o.advance(dt, 300, tol=1e-9) is None
+    assert g.step(dt, 300) is None
+    fo, fg = o.fields(), g.fields()
+    for k in ("p", "p_prev", "vx", "vy", "vz"):
+        assert_bitexact(k, fg[k], fo[k])
+    lo, lg = o.ledger(), g.ledger()
+    # the source's injected work is an entry of the ledger: its scale covers it
+    assert abs(lg["scale"] - lo["scale"]) <= 1e-12 * lo["scale"]
+    assert abs(lg["total"] - lo["total"]) <= 1e-12 * lo["scale"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", ["blocks_first", "source_first"])
+@pytest.mark.parametrize("across", [24, 23])
+def test_speed_blocks_with_source_f32_audited(order, across):
+    (o, g), dt = _sourced(order, "f32", across)
+    g.set_tolerance(1e-5)
+    assert o.advance(dt, 300, tol=1e-9) is None
+    assert g.step(dt, 300) is None  # audited every step in FP64
+    lo, lg = o.ledger(), g.ledger()
+    assert abs(lg["total"] - lo["total"]) < 1e-5 * lo["scale"]
