@@ -26,8 +26,9 @@ struct Cavity : Handle {
     std::vector<double> eps[3], sig[3], mu[3];
     DBuf deps[3], dsig[3], dmu[3];
     // mixed media: the per-edge gain and decay and per-face g/μ of the step size coef_dt (in the
-    // field type), and what the media leave uniform: σ = 0 on every edge (lossless, no decay
-    // array) and one μ on every face (mu_one, no g/μ array)
+    // field type; the gains on the padded lattice when the cavity is TMA-staged), and what the
+    // media leave uniform: σ = 0 on every edge (lossless, no decay array) and one μ on every face
+    // (mu_one, no g/μ array)
     DBuf dgain[3], ddecay[3], dch[3];
     double coef_dt = NAN;
     bool lossless = true, mu_var = false;
@@ -445,9 +446,9 @@ struct Cavity : Handle {
         return PM_OK;
     }
 
-    // The padded cavity back to the reference layout (before per-cell media, which only the
-    // cp.async kernel reads). The state goes through the host once; a checkpoint taken in the
-    // other layout is dropped.
+    // The padded cavity back to the reference layout (before media with conductivity or per-cell
+    // μ, which only the cp.async kernel reads). The state goes through the host once; a
+    // checkpoint taken in the other layout is dropped.
     pm_status leave_tma() {
         if (!tma) return PM_OK;
         std::vector<double> v[6];
@@ -539,11 +540,20 @@ struct Cavity : Handle {
             PM_CUDA(put_sync(deps[q].p, eps[q].data(), eps[q].size() * 8));
             PM_CUDA(put_sync(dsig[q].p, sig[q].data(), sig[q].size() * 8));
             PM_CUDA(put_sync(dmu[q].p, mu[q].data(), mu[q].size() * 8));
-            PM_CUDA(dgain[q].alloc(eps[q].size() * esize()));
+            PM_CUDA(dgain[q].alloc((tma ? dcount(q) : eps[q].size()) * esize()));
             if (lossless) ddecay[q].release();
             else PM_CUDA(ddecay[q].alloc(eps[q].size() * esize()));
             if (mu_var) PM_CUDA(dch[q].alloc(mu[q].size() * esize()));
             else dch[q].release();
+        }
+        if (tma) {
+            // the gains' boxes: the tile's own edges, 32 × 8 × P (both parities share the arrays)
+            for (int par = 0; par < 2; ++par)
+                for (int q = 0; q < 3; ++q) {
+                    CUtensorMap* m = q == 0 ? &maps[par].gx : q == 1 ? &maps[par].gy : &maps[par].gz;
+                    if (!hall_tma_map(m, dgain[q].p, (int)L, ny + 1, nz + 1, 32, 8, kYeeTmaPlanes))
+                        return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a cavity gain array");
+                }
         }
         coef_dt = NAN;
         return PM_OK;
@@ -564,6 +574,16 @@ struct Cavity : Handle {
             a.nf[q] = count(q + 3);
         }
         a.dt = h; a.dx = dx; a.g = h / dx;
+        if (tma) {
+            a.L = L;
+            a.ny1 = (unsigned)ny + 1;
+            for (int q = 0; q < 3; ++q) {
+                int ex, ey, ez;
+                extents(q, ex, ey, ez);
+                a.ext[q][0] = ex;
+                a.ext[q][1] = ey;
+            }
+        }
         return a;
     }
     pm_status prepare_coefs(double h) {
@@ -635,10 +655,14 @@ pm_status pm_cavity_fill_cells(pm_cavity* cp, const double* eps_r, const double*
         if (mu_r) c->cell_mu[q] = mu_r[q];
         if (sigma) c->cell_sig[q] = sigma[q];
     }
-    pm_status ls = c->leave_tma();
-    if (ls != PM_OK) return ls;
     c->uniform = false;
     c->refresh_media();
+    // the TMA-staged kernel steps per-cell ε with no conductivity and one μ on the padded layout;
+    // other media go back to the reference layout and the cp.async kernel
+    if (!(c->lossless && !c->mu_var)) {
+        pm_status ls = c->leave_tma();
+        if (ls != PM_OK) return ls;
+    }
     pm_status s = c->upload_media();
     if (s != PM_OK) return s;
     return c->reset_ledger();

@@ -133,16 +133,23 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
 cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
     constexpr int P = kYeeTmaPlanes, S = kYeeTmaStages;
     static bool attr = false;
-    const int smem = (int)yee_tma_smem_bytes();
+    const bool media = !a.uniform;
+    const int smem = (int)yee_tma_smem_bytes(media);
     if (!attr) {
-        cudaFuncSetAttribute(yee_tma_step<P, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_tma_step<P, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        const int s0 = (int)yee_tma_smem_bytes(false), s1 = (int)yee_tma_smem_bytes(true);
+        cudaFuncSetAttribute(yee_tma_step<P, S, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
+        cudaFuncSetAttribute(yee_tma_step<P, S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
+        cudaFuncSetAttribute(yee_tma_step<P, S, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
+        cudaFuncSetAttribute(yee_tma_step<P, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
         attr = true;
     }
-    if (a.solid)
-        yee_tma_step<P, S, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-    else
-        yee_tma_step<P, S, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+    if (a.solid) {
+        if (media) yee_tma_step<P, S, true, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+        else yee_tma_step<P, S, true, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+    } else {
+        if (media) yee_tma_step<P, S, false, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+        else yee_tma_step<P, S, false, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+    }
     return cudaGetLastError();
 }
 
@@ -213,9 +220,9 @@ int occupancy_f32(KernelId id) {
                                                               kEnsConsumers + 32, ens_tma_smem_bytes());
             break;
         case kYeeTma:
-            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false>,
+            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes());
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false>, 256,
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false, false>, 256,
                                                               yee_tma_smem_bytes());
             break;
         case kHallTma:

@@ -81,7 +81,10 @@ inline size_t hall_tma_smem_bytes() {
 bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz);
 // The FP32 uniform-medium cavity step staged by TMA (padded lattice of row pitch L).
 cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s);
-inline size_t yee_tma_smem_bytes() { return yee_tma_smem_bytes_for<kYeeTmaPlanes>(kYeeTmaStages); }
+inline size_t yee_tma_smem_bytes(bool media = false) {
+    return media ? yee_tma_smem_bytes_for<kYeeTmaPlanes, true>(kYeeTmaStages)
+                 : yee_tma_smem_bytes_for<kYeeTmaPlanes, false>(kYeeTmaStages);
+}
 // One component between the reference layout and the padded lattice (see yee_relayout);
 // src_f64 / dst_f64 select double or float for each side.
 cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,

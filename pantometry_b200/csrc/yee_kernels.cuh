@@ -393,6 +393,10 @@ struct YeeCoefArgs {
     Real* ch[3];     // null: one μ
     size_t ne[3], nf[3];
     double dt, dx, g;
+    // L > 0: gain and decay go to the padded lattice (row pitch L, ny1 rows per plane) of a
+    // TMA-staged cavity; ext[q] = the x and y extents of edge component q
+    unsigned L, ny1;
+    int ext[3][2];
 };
 
 template <typename Real>
@@ -402,8 +406,13 @@ static __global__ void yee_coefs(YeeCoefArgs<Real> a) {
         for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.ne[q]; c += stride) {
             Real d, g;
             coefficients<Real>(a.eps[q][c], a.sig[q][c], a.dt, a.dx, d, g);
-            a.gain[q][c] = g;
-            if (a.decay[q]) a.decay[q][c] = d;
+            size_t p = c;
+            if (a.L) {
+                const size_t i = c % (size_t)a.ext[q][0], r = c / (size_t)a.ext[q][0];
+                p = i + (size_t)a.L * (r % (size_t)a.ext[q][1] + (size_t)a.ny1 * (r / (size_t)a.ext[q][1]));
+            }
+            a.gain[q][p] = g;
+            if (a.decay[q]) a.decay[q][p] = d;
         }
         if (a.ch[q])
             for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.nf[q]; c += stride)

@@ -1,6 +1,10 @@
-// Cavity step, FP32 form for one uniform medium (with or without obstacles), staged by the Tensor
-// Memory Accelerator. The arithmetic per edge and face is yee_step's for a uniform medium
-// (cavity.rs:1346-1501): H⁺ from Eⁿ, the invariant ½ε|Eⁿ|² + ½μ H⁻·H⁺, then Eⁿ⁺¹ from H⁺.
+// Cavity step, FP32 form for one uniform medium, or (MEDIA) for per-cell ε with no conductivity
+// and one μ, with or without obstacles, staged by the Tensor Memory Accelerator. The arithmetic
+// per edge and face is yee_step's (cavity.rs:1346-1501): H⁺ from Eⁿ, the invariant
+// ½ε|Eⁿ|² + ½μ H⁻·H⁺, then Eⁿ⁺¹ from H⁺. With MEDIA the stage also holds the gains
+// g = Δt/(ε Δx) of the tile's own edges (yee_coefs, on the padded lattice), and each thread weighs
+// its electric terms by 1/g, so the energy it books is ½ (Δt/Δx) Σ w E²/g V: ½ Σ w ε E² V with
+// the ε the update itself used.
 //
 // Layout. The handle keeps all six components on the (nx+1) × (ny+1) × (nz+1) node lattice with
 // one index n = i + L·(j + (ny+1)·k), L = nx+1 rounded up to a multiple of 4 (so every row pitch
@@ -29,6 +33,7 @@ namespace pm {
 
 struct YeeMaps {
     CUtensorMap ex, ey, ez, hx, hy, hz;
+    CUtensorMap gx, gy, gz;  // per-edge gains of a cavity of mixed ε (MEDIA)
 };
 
 #ifndef PM_YEE_TMA_PLANES
@@ -45,19 +50,23 @@ constexpr int kYeeTmaStages = PM_YEE_TMA_STAGES;
 
 constexpr unsigned round128(unsigned b) { return (b + 127u) & ~127u; }
 
-// Byte offsets of the six boxes inside one stage (each 128-byte aligned).
-template <int P>
+// Byte offsets of the six boxes inside one stage (each 128-byte aligned), and with MEDIA the
+// three gain boxes of the tile's own edges, x0 .. x0+31, y0 .. y0+7, kb .. kb+P−1.
+template <int P, bool MEDIA = false>
 struct YeeTmaLayout {
     static constexpr unsigned EX_B = (P + 1) * 10 * 36 * 4, EY_B = (P + 1) * 9 * 40 * 4, EZ_B = P * 10 * 40 * 4,
-                              HX_B = P * 9 * 32 * 4, HY_B = P * 8 * 36 * 4, HZ_B = P * 9 * 36 * 4;
+                              HX_B = P * 9 * 32 * 4, HY_B = P * 8 * 36 * 4, HZ_B = P * 9 * 36 * 4,
+                              G_B = MEDIA ? P * 8 * 32 * 4 : 0;
     static constexpr unsigned EX = 0, EY = round128(EX + EX_B), EZ = round128(EY + EY_B), HX = round128(EZ + EZ_B),
-                              HY = round128(HX + HX_B), HZ = round128(HY + HY_B), BYTES = round128(HZ + HZ_B);
-    static constexpr unsigned TX = EX_B + EY_B + EZ_B + HX_B + HY_B + HZ_B;  // bytes the six loads deliver
+                              HY = round128(HX + HX_B), HZ = round128(HY + HY_B), GX = round128(HZ + HZ_B),
+                              GY = round128(GX + G_B), GZ = round128(GY + G_B), BYTES = round128(GZ + G_B);
+    // bytes the loads of one stage deliver
+    static constexpr unsigned TX = EX_B + EY_B + EZ_B + HX_B + HY_B + HZ_B + 3 * G_B;
 };
 
-template <int P>
+template <int P, bool MEDIA = false>
 inline size_t yee_tma_smem_bytes_for(int S) {
-    return (size_t)S * YeeTmaLayout<P>::BYTES + 2 * sizeof(YeeHp<float>) + 8 * (size_t)S;
+    return (size_t)S * YeeTmaLayout<P, MEDIA>::BYTES + 2 * sizeof(YeeHp<float>) + 8 * (size_t)S;
 }
 
 struct YeeTmaCursor {
@@ -82,9 +91,9 @@ __device__ __forceinline__ void yee_tma_next(YeeTmaCursor& c, const Tiles& T, in
     if (c.kb >= c.k1) yee_tma_at(c, T, c.t + gridDim.x);
 }
 
-template <int P>
+template <int P, bool MEDIA>
 __device__ __forceinline__ void yee_tma_issue(const YeeMaps& m, unsigned stage, unsigned bar, const YeeTmaCursor& c) {
-    using Lay = YeeTmaLayout<P>;
+    using Lay = YeeTmaLayout<P, MEDIA>;
     mbar_expect_tx(bar, Lay::TX);
     tma_load_3d(stage + Lay::EX, &m.ex, c.x0 - 4, c.y0 - 1, c.kb, bar);
     tma_load_3d(stage + Lay::EY, &m.ey, c.x0 - 4, c.y0 - 1, c.kb, bar);
@@ -92,14 +101,19 @@ __device__ __forceinline__ void yee_tma_issue(const YeeMaps& m, unsigned stage, 
     tma_load_3d(stage + Lay::HX, &m.hx, c.x0, c.y0 - 1, c.kb, bar);
     tma_load_3d(stage + Lay::HY, &m.hy, c.x0 - 4, c.y0, c.kb, bar);
     tma_load_3d(stage + Lay::HZ, &m.hz, c.x0 - 4, c.y0 - 1, c.kb, bar);
+    if constexpr (MEDIA) {
+        tma_load_3d(stage + Lay::GX, &m.gx, c.x0, c.y0, c.kb, bar);
+        tma_load_3d(stage + Lay::GY, &m.gy, c.x0, c.y0, c.kb, bar);
+        tma_load_3d(stage + Lay::GZ, &m.gz, c.x0, c.y0, c.kb, bar);
+    }
 }
 
-template <int P, int S, bool SOLID>
+template <int P, int S, bool SOLID, bool MEDIA>
 static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m) {
     DevState* st = a.st;
     if (st->violated) return;
-    using Lay = YeeTmaLayout<P>;
+    using Lay = YeeTmaLayout<P, MEDIA>;
     extern __shared__ __align__(128) unsigned char yee_tma_smem[];
     const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(yee_tma_smem));
     YeeHp<float>* hp = reinterpret_cast<YeeHp<float>*>(yee_tma_smem + S * Lay::BYTES);
@@ -128,7 +142,7 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
     if (tid == 0) {
         yee_tma_at(pf, T, blockIdx.x);
         for (; issued < S - 1 && pf.valid; ++issued) {
-            yee_tma_issue<P>(m, ring_base + issued * Lay::BYTES, bar_base + 8 * issued, pf);
+            yee_tma_issue<P, MEDIA>(m, ring_base + issued * Lay::BYTES, bar_base + 8 * issued, pf);
             yee_tma_next(pf, T, P);
         }
     }
@@ -150,7 +164,7 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
         if (tid == 0 && pf.valid) {
             const int fill = (it + S - 1) % S;
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            yee_tma_issue<P>(m, ring_base + fill * Lay::BYTES, bar_base + 8 * fill, pf);
+            yee_tma_issue<P, MEDIA>(m, ring_base + fill * Lay::BYTES, bar_base + 8 * fill, pf);
             yee_tma_next(pf, T, P);
             ++issued;
         }
@@ -161,6 +175,9 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
         const float(*HX)[9][32] = reinterpret_cast<const float(*)[9][32]>(sb + Lay::HX);
         const float(*HY)[8][36] = reinterpret_cast<const float(*)[8][36]>(sb + Lay::HY);
         const float(*HZ)[9][36] = reinterpret_cast<const float(*)[9][36]>(sb + Lay::HZ);
+        const float(*GX)[8][32] = reinterpret_cast<const float(*)[8][32]>(sb + Lay::GX);
+        const float(*GY)[8][32] = reinterpret_cast<const float(*)[8][32]>(sb + Lay::GY);
+        const float(*GZ)[8][32] = reinterpret_cast<const float(*)[8][32]>(sb + Lay::GZ);
         const int i = cc.x0 + tx, j = cc.y0 + ty;
         const bool in_x = i <= nx, in_y = j <= ny;
         // node-centred half weights of the boundary samples (cavity.rs:766-772)
@@ -173,6 +190,15 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
             const bool compute = k >= cc.k0;  // else the plane below the chunk: H⁺ only
             const bool zin = k < nz;
             const float hk = (k == 0 || k == nz) ? 0.5f : 1.0f;
+            const unsigned n = (unsigned)i + L * ((unsigned)j + ny1 * (unsigned)k);
+            // the gains of the thread's own edges; at a position the component does not have (the
+            // padding, or the fill outside the lattice) the uniform gain, never read as a value
+            float gx = gain0, gy = gain0, gz = gain0;
+            if constexpr (MEDIA) {
+                gx = (i < nx && in_y) ? GX[h][ty][tx] : gain0;
+                gy = (in_x && j < ny) ? GY[h][ty][tx] : gain0;
+                gz = (in_x && in_y && zin) ? GZ[h][ty][tx] : gain0;
+            }
             YeeHp<float>* hq = hp + hpar;
             // ---- 1. H⁺ (cavity.rs:1346-1379) on own faces
             const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
@@ -184,7 +210,6 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
             hq->hx[ty + 1][tx] = hxn;
             hq->hy[ty][tx + 1] = hyn;
             hq->hz[ty + 1][tx + 1] = hzn;
-            const unsigned n = (unsigned)i + L * ((unsigned)j + ny1 * (unsigned)k);
             if (compute) {
                 if (fx) a.neu[3][n] = hxn;
                 if (fy) a.neu[4][n] = hyn;
@@ -194,7 +219,11 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
                 // (padding, or the fill outside the lattice) is exactly zero, so its E term and
                 // its H⁻·H⁺ term are zero.
                 ms += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
-                es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+                if constexpr (MEDIA)  // 1/g to within 2 ulp: the terms are f32 roundings already
+                    es += __fdividef((hj * hk) * (ex0 * ex0), gx) + __fdividef((hi * hk) * (ey0 * ey0), gy) +
+                          __fdividef((hi * hj) * (ez0 * ez0), gz);
+                else
+                    es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
                 // halo faces, one line per warp so the barrier waits on no warp doing twice the
                 // work: the y0 − 1 row of hx (warp 7) and of hz (warp 6), the x0 − 1 column of hz
                 // (warp 5, rows y0 − 1 .. y0 + 7) and of hy (warp 4, rows y0 .. y0 + 7)
@@ -218,9 +247,9 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
                 const float cex = (hq->hz[ty + 1][tx + 1] - hq->hz[ty][tx + 1]) - (hyn - hy_below);
                 const float cey = (hxn - hx_below) - (hq->hz[ty + 1][tx + 1] - hq->hz[ty + 1][tx]);
                 const float cez = (hyn - hq->hy[ty][tx]) - (hxn - hq->hx[ty][tx]);
-                float vx = dec0 * ex0 + gain0 * cex;
-                float vy = dec0 * ey0 + gain0 * cey;
-                float vz = dec0 * ez0 + gain0 * cez;
+                float vx = dec0 * ex0 + gx * cex;
+                float vy = dec0 * ey0 + gy * cey;
+                float vz = dec0 * ez0 + gz * cez;
                 if (i == a.src_i && j == a.src_j && k == a.src_k) {
                     // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
                     const double e = a.eps_src, ss = a.sig_src;
@@ -267,7 +296,8 @@ static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_ste
     }
     if (finish_blocks<4>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
         const double v = a.volume;
-        const double electric = 0.5 * (a.eps_u * acc[0]) * v;  // cavity.rs:846
+        // cavity.rs:846; with MEDIA the terms are already weighted by 1/g = ε Δx/Δt
+        const double electric = MEDIA ? 0.5 * (a.g * acc[0]) * v : 0.5 * (a.eps_u * acc[0]) * v;
         const double paired = 0.5 * v * (a.mu_u * acc[1]);     // cavity.rs:885-904
         st->invariant = electric + paired;
         st->has_invariant = 1;
