@@ -859,9 +859,9 @@ def run_mix(args):
     cav_rate = cav_cells * T * K / (ms_cav * 1e-3) / 1e9
     per_launch_ms = ms_hall / (K * T)
     achieved = BYTES_F32 * hall_cells / (per_launch_ms * 1e-3) / 1e9
-    # whole-step algorithmic bytes: 32 B per hall node-update; per cavity cell-update 48 B of fields,
-    # 12 B of per-edge gain (f32) and 24 B of per-edge ε (f64, the audit's weights)
-    step_bytes = T * (BYTES_F32 * hall_cells + 84 * cav_cells)
+    # whole-step algorithmic bytes: 32 B per hall node-update; per cavity cell-update 48 B of fields
+    # and 12 B of per-edge gains (f32, which also weigh the audit's electric terms)
+    step_bytes = T * (BYTES_F32 * hall_cells + 60 * cav_cells)
     h2d = hall_cells * 8 + len(ccfg["cavities"]) * sum(shapes.values()) * 8
     d2h = hall_cells * 8 + 64 * (1 + len(ccfg["cavities"]))
     line = {
