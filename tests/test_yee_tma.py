@@ -143,3 +143,40 @@ def test_yee_upload_starts_fresh_books(precision):
             assert np.array_equal(fo[k].view(np.uint64), runs[1][0][k].view(np.uint64)), k
         else:
             assert np.abs(fo[k] - runs[1][0][k]).max() <= 1e-4 * scale[k[0]], k
+
+
+def test_yee_f32_books_hold_after_the_source():
+    """The FP32 cavity's books against the soft current: f32 storage rounds the field at the source
+    edge and its neighbours while the pulse pumps energy in and out there, which leaves the ledger a
+    few 1e-6 of the injected energy off (an f32 emulation of the scheme gives the same; f32
+    coefficients alone give 2e-8). Once the pulse has passed the books must hold: no drift."""
+    from pantometry_b200 import workloads as W
+    from pantometry_b200.domains import Cavity
+
+    n = 48
+    cfg = W.yee_cavity(n, steps=1600)
+    g = Cavity((n, n, n), cfg["dx"], precision="f32")
+    g.set_source(cfg["edge"], cfg["current"])
+    g.set_tolerance(1e-5)
+    assert g.step(cfg["dt"], 300) is None  # the pulse is over by about step 180
+    a = g.ledger()
+    assert g.step(cfg["dt"], 1200) is None
+    b = g.ledger()
+    assert abs(a["total"]) < 5e-5 * a["scale"]
+    assert abs(b["total"] - a["total"]) < 2e-7 * b["scale"]
+
+
+def test_yee_f32_invariant_against_f64_over_2000_steps():
+    """A source-free mode at 48³: the FP32 run's invariant stays within 1e-6 of the f64 run's."""
+    from pantometry_b200.domains import Cavity
+
+    n = 48
+    runs = {}
+    for prec in ("f32", "f64"):
+        g = Cavity((n, n, n), 1e-3, precision=prec)
+        dt = 0.99 * g.courant_limit()
+        g.release_mode((1, 1), 1.0, dt)
+        g.set_tolerance(1e-5 if prec == "f32" else 1e-9)
+        assert g.step(dt, 2000) is None
+        runs[prec] = g.ledger()
+    assert abs(runs["f32"]["total"] - runs["f64"]["total"]) < 1e-6 * runs["f64"]["scale"]
