@@ -202,9 +202,29 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                 const float ga = m.a;
                 const int exposed = m.exposed;
                 double col_shed = 0.0;
+                bool done = false;  // the stage went through the interior fast path
+                if (!edge_xy && hn == P && kb > 0 && kb + P < nz) {
+                    // a whole stage of interior cells: no film, no bound, the planes below and
+                    // above carried in registers; the same arithmetic as the interior case below
+                    float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
+#pragma unroll
+                    for (int h = 0; h < P; ++h) {
+                        const float above = s.t[h + 2][ty + 1][tx + 4];
+                        const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+                        const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
+                        const float sum = (((((xm - here) + (xp - here)) + (ym - here)) + (yp - here)) + (below - here)) + (above - here);
+                        const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
+                        tnew[c] = nd;
+                        acc[0] += (double)nd;
+                        c += plane;
+                        below = here;
+                        here = above;
+                    }
+                    done = true;
+                }
 #pragma unroll
                 for (int h = 0; h < P; ++h) {
-                    if (h >= hn) break;
+                    if (done || h >= hn) break;
                     const int k = kb + h;
                     const float here = s.t[h + 1][ty + 1][tx + 4];
                     const float below = s.t[h][ty + 1][tx + 4], above = s.t[h + 2][ty + 1][tx + 4];
