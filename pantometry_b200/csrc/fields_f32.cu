@@ -6,7 +6,8 @@
 namespace pm {
 
 cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s) {
-    heat_f32_step<<<a.nblocks, tile_block(), 0, s>>>(a);
+    if (a.kx) heat_f32_step<true><<<a.nblocks, tile_block(), 0, s>>>(a);
+    else heat_f32_step<false><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -201,7 +202,7 @@ int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
     switch (id) {
-        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step, 256, 0); break;
+        case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step<false>, 256, 0); break;
         case kHallF32:
             cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<float, false>, 256, hall_smem_bytes<float>());

@@ -43,6 +43,11 @@ struct Heat : Handle {
     // device buffers
     DBuf field[2];  // f64 kelvin (plain) or f32 deviations
     DBuf dkx, dky, dkz, dmob, dcap, dwhich, dmatk, dmateps;
+    // the FP32 form of a filled block: face conductivities and film conductances in f32, and
+    // dt·mobility per cell for the step size m_dt
+    DBuf dkx32, dky32, dkz32, dm32, dfilm32;
+    size_t film_off[6] = {0, 0, 0, 0, 0, 0};
+    double m_dt = NAN;
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
     double saved_lost = 0.0, saved_supplied = 0.0;
@@ -203,15 +208,71 @@ struct Heat : Handle {
         return worst;
     }
 
+    pm_status put_buf(DBuf& b, const void* src, size_t bytes) {
+        PM_CUDA(b.alloc(bytes));
+        PM_CUDA(put_sync(b.p, src, bytes));
+        return PM_OK;
+    }
+
+    // A filled block in the FP32 form: the face conductivities rounded to f32, the capacities in
+    // f64 for the stored heat, the film conductances; dt·mobility follows with the step size.
+    pm_status upload_coefficients_f32() {
+        auto put32 = [&](DBuf& b, const std::vector<double>& v) -> pm_status {
+            std::vector<float> f(v.size());
+            for (size_t q = 0; q < v.size(); ++q) f[q] = (float)v[q];
+            return put_buf(b, f.data(), f.size() * 4);
+        };
+        pm_status s;
+        if ((s = put32(dkx32, kx)) != PM_OK) return s;
+        if ((s = put32(dky32, ky)) != PM_OK) return s;
+        if ((s = put32(dkz32, kz)) != PM_OK) return s;
+        if ((s = put_buf(dcap, cap.data(), cap.size() * 8)) != PM_OK) return s;
+        m_dt = NAN;
+        return upload_films_f32();
+    }
+
+    // Per exposed face, each cell's film conductance g/dx with the half cell of its own material
+    // in series (solid.rs:1192-1219 at zero emissivity, where g does not depend on the gap).
+    pm_status upload_films_f32() {
+        if (uniform || precision == PM_PLAIN_F64) return PM_OK;
+        drop_graphs();
+        std::vector<float> v;
+        for (int f = 0; f < 6; ++f) {
+            film_off[f] = v.size();
+            if (!((films.exposed >> f) & 1)) continue;
+            const double share = films.share[f];
+            const int a1 = f < 2 ? ny : nx, a2 = f < 4 ? nz : ny;  // the plane's two extents
+            for (int q2 = 0; q2 < a2; ++q2)
+                for (int q1 = 0; q1 < a1; ++q1) {
+                    int i, j, k;
+                    if (f < 2) { i = f == 0 ? 0 : nx - 1; j = q1; k = q2; }
+                    else if (f < 4) { i = q1; j = f == 2 ? 0 : ny - 1; k = q2; }
+                    else { i = q1; j = q2; k = f == 4 ? 0 : nz - 1; }
+                    const size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+                    const double g = host_series_with_half_cell(film_conv[f] * share, mat_k(mat_of(c)), share, dx);
+                    v.push_back((float)(g / dx));
+                }
+        }
+        if (v.empty()) v.push_back(0.0f);
+        return put_buf(dfilm32, v.data(), v.size() * 4);
+    }
+
+    // dt·mobility per cell for step size dt, once per change of dt or of the block.
+    pm_status prepare_f32(double dt) {
+        if (uniform || precision == PM_PLAIN_F64 || m_dt == dt) return PM_OK;
+        std::vector<float> m(n());
+        for (size_t c = 0; c < n(); ++c) m[c] = (float)(dt * mob[c]);
+        if (!dm32.p || dm32.bytes < n() * 4) PM_CUDA(dm32.alloc(n() * 4));
+        PM_CUDA(put_sync(dm32.p, m.data(), n() * 4));
+        m_dt = dt;
+        return PM_OK;
+    }
+
     pm_status upload_coefficients() {
         drop_graphs();
         if (uniform) return PM_OK;
-        if (precision != PM_PLAIN_F64) return fail(PM_UNSUPPORTED, "a filled (multi-material) block runs in the plain f64 form only");
-        auto put = [&](DBuf& b, const void* src, size_t bytes) -> pm_status {
-            PM_CUDA(b.alloc(bytes));
-            PM_CUDA(put_sync(b.p, src, bytes));
-            return PM_OK;
-        };
+        if (precision != PM_PLAIN_F64) return upload_coefficients_f32();
+        auto put = [&](DBuf& b, const void* src, size_t bytes) -> pm_status { return put_buf(b, src, bytes); };
         pm_status s;
         if ((s = put(dkx, kx.data(), kx.size() * 8)) != PM_OK) return s;
         if ((s = put(dky, ky.data(), ky.size() * 8)) != PM_OK) return s;
@@ -270,6 +331,11 @@ struct Heat : Handle {
             a.off[f] = (float)(reference - films.ambient[f]);
         }
         a.capacity = capacity;
+        if (!uniform) {
+            a.kx = dkx32.as<float>(); a.ky = dky32.as<float>(); a.kz = dkz32.as<float>();
+            a.m = dm32.as<float>(); a.cap = dcap.as<double>();
+            for (int f = 0; f < 6; ++f) a.film[f] = dfilm32.as<float>() + film_off[f];
+        }
         const unsigned w = wave_of(kHeatF32);
         a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
         a.nblocks = grid_for(a.tiles, w);
@@ -366,7 +432,7 @@ pm_status pm_heat_losing_from(pm_heat* hp, int face, double ambient, double conv
     h->films.share[face] = area / (double)std::max<size_t>(h->cells_on(face), 1);  // solid.rs:1203
     h->resolve();
     h->drop_graphs();
-    return PM_OK;
+    return h->upload_films_f32();
 }
 
 pm_status pm_heat_upload(pm_heat* hp, const double* kelvin, size_t n) {
@@ -446,6 +512,7 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
             return launch_heat_plain(h->plain_args(par, dt), st);
         });
     } else {
+        if ((s = h->prepare_f32(dt)) != PM_OK) return s;
         s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {
             return launch_heat_f32(h->f32_args(par, dt), st);
         });

@@ -9,8 +9,11 @@
 //
 // heat_f32_step — the chosen form. The field is stored as the deviation T − T0 in f32, which
 //   keeps the subtraction `T_nb − T` on numbers of order the deviation rather than of 300 K
-//   (the reference's own finding, runtime/gpu/src/lib.rs:37-51). Uniform material; films with
-//   a temperature-independent conductance. Stored heat, shed heat and the ledger stay FP64.
+//   (the reference's own finding, runtime/gpu/src/lib.rs:37-51). Films with a temperature-
+//   independent conductance. A uniform block folds dt·mobility·k into one coefficient; a filled
+//   block (FILLED) reads its per-face conductivities in f32, each cell's dt·mobility (formed once
+//   per step size) and each boundary cell's film conductance, with `Solid3D::step`'s arithmetic
+//   in f32. Stored heat, shed heat and the ledger stay FP64 (per-cell capacities in f64).
 #pragma once
 
 #include "common.cuh"
@@ -191,6 +194,15 @@ struct HeatF32Args {
     float b[6];      // dt · mobility · g_f / dx per film face
     float off[6];    // T0 − ambient per film face
     double capacity; // per cell
+    // Filled blocks (null otherwise): per-face conductivities (solid.rs:686-713), dt · mobility
+    // per cell, capacity per cell, and per exposed face f the film conductance g/dx of each cell
+    // on it (film[f] indexed j + ny·k on the x faces, i + nx·k on the y faces, i + nx·j on z)
+    const float* __restrict__ kx;
+    const float* __restrict__ ky;
+    const float* __restrict__ kz;
+    const float* __restrict__ m;
+    const double* __restrict__ cap;
+    const float* film[6];
     Tiles tiles;
     DevState* st;
     double* partials;
@@ -198,6 +210,7 @@ struct HeatF32Args {
 };
 
 // Chosen form, z-marching like the plain form; neighbours in the plane come from L1/L2.
+template <bool FILLED>
 static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
     if (a.st->violated) return;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
@@ -216,25 +229,58 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
         for (int k = k0; k < k1; ++k, c += plane) {
             const float above = (k + 1 < nz) ? __ldg(a.dold + c + plane) : 0.0f;
             float s = 0.0f;
-            if (xl) s += __ldg(a.dold + c - 1) - here;
-            if (xh) s += __ldg(a.dold + c + 1) - here;
-            if (yl) s += __ldg(a.dold + c - nx) - here;
-            if (yh) s += __ldg(a.dold + c + nx) - here;
-            if (k > 0) s += below - here;
-            if (k + 1 < nz) s += above - here;
+            if constexpr (FILLED) {
+                // solid.rs:1773-1826 in the reference's arm order, each face's own conductivity
+                const size_t xr = (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
+                const size_t yr = (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
+                if (xl) s += __ldg(a.kx + i + xr) * (__ldg(a.dold + c - 1) - here);
+                if (xh) s += __ldg(a.kx + i + 1 + xr) * (__ldg(a.dold + c + 1) - here);
+                if (yl) s += __ldg(a.ky + i + yr) * (__ldg(a.dold + c - nx) - here);
+                if (yh) s += __ldg(a.ky + i + nx + yr) * (__ldg(a.dold + c + nx) - here);
+                if (k > 0) s += __ldg(a.kz + c) * (below - here);
+                if (k + 1 < nz) s += __ldg(a.kz + c + plane) * (above - here);
+            } else {
+                if (xl) s += __ldg(a.dold + c - 1) - here;
+                if (xh) s += __ldg(a.dold + c + 1) - here;
+                if (yl) s += __ldg(a.dold + c - nx) - here;
+                if (yh) s += __ldg(a.dold + c + nx) - here;
+                if (k > 0) s += below - here;
+                if (k + 1 < nz) s += above - here;
+            }
             float shed = 0.0f;
             if (a.exposed && (edge_xy || k == 0 || k + 1 == nz)) {
-                if (((a.exposed >> 0) & 1) && !xl) shed += a.b[0] * (here + a.off[0]);
-                if (((a.exposed >> 1) & 1) && !xh) shed += a.b[1] * (here + a.off[1]);
-                if (((a.exposed >> 2) & 1) && !yl) shed += a.b[2] * (here + a.off[2]);
-                if (((a.exposed >> 3) & 1) && !yh) shed += a.b[3] * (here + a.off[3]);
-                if (((a.exposed >> 4) & 1) && k == 0) shed += a.b[4] * (here + a.off[4]);
-                if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += a.b[5] * (here + a.off[5]);
-                col_shed += (double)shed;
+                if constexpr (FILLED) {
+                    const unsigned px = (unsigned)j + (unsigned)ny * (unsigned)k, py = (unsigned)i + (unsigned)nx * (unsigned)k,
+                                   pz = (unsigned)i + (unsigned)nx * (unsigned)j;
+                    if (((a.exposed >> 0) & 1) && !xl) shed += __ldg(a.film[0] + px) * (here + a.off[0]);
+                    if (((a.exposed >> 1) & 1) && !xh) shed += __ldg(a.film[1] + px) * (here + a.off[1]);
+                    if (((a.exposed >> 2) & 1) && !yl) shed += __ldg(a.film[2] + py) * (here + a.off[2]);
+                    if (((a.exposed >> 3) & 1) && !yh) shed += __ldg(a.film[3] + py) * (here + a.off[3]);
+                    if (((a.exposed >> 4) & 1) && k == 0) shed += __ldg(a.film[4] + pz) * (here + a.off[4]);
+                    if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += __ldg(a.film[5] + pz) * (here + a.off[5]);
+                } else {
+                    if (((a.exposed >> 0) & 1) && !xl) shed += a.b[0] * (here + a.off[0]);
+                    if (((a.exposed >> 1) & 1) && !xh) shed += a.b[1] * (here + a.off[1]);
+                    if (((a.exposed >> 2) & 1) && !yl) shed += a.b[2] * (here + a.off[2]);
+                    if (((a.exposed >> 3) & 1) && !yh) shed += a.b[3] * (here + a.off[3]);
+                    if (((a.exposed >> 4) & 1) && k == 0) shed += a.b[4] * (here + a.off[4]);
+                    if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += a.b[5] * (here + a.off[5]);
+                    col_shed += (double)shed;
+                }
             }
-            const float nd = here + (a.a * s - shed);
+            float nd;
+            if constexpr (FILLED) {
+                // add_kelvin (solid.rs:1620-1635); stored heat C·dev and shed heat C·dt·mob·shed
+                const float mc = __ldg(a.m + c);
+                nd = here + mc * (s - shed);
+                const double capc = __ldg(a.cap + c);
+                acc[0] += capc * (double)nd;
+                if (shed != 0.0f) acc[1] += capc * (double)(mc * shed);
+            } else {
+                nd = here + (a.a * s - shed);
+                acc[0] += (double)nd;
+            }
             a.dnew[c] = nd;
-            acc[0] += (double)nd;
             below = here;
             here = above;
         }
@@ -242,8 +288,8 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
     }
     if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;
-        const double stored = a.capacity * acc[0];
-        st->lost += a.capacity * acc[1];
+        const double stored = FILLED ? acc[0] : a.capacity * acc[0];
+        st->lost += FILLED ? acc[1] : a.capacity * acc[1];
         double total = 0.0, scale = 0.0;
         ledger_add(total, scale, stored);
         ledger_add(total, scale, st->lost);
@@ -275,12 +321,12 @@ static __global__ void __launch_bounds__(256) heat_measure(HeatMeasureArgs a) {
             const double capc = a.cap ? a.cap[c] : a.capacity;
             acc[0] += capc * (a.t64[c] - a.reference);
         } else {
-            acc[0] += (double)a.d32[c];
+            acc[0] += a.cap ? a.cap[c] * (double)a.d32[c] : (double)a.d32[c];
         }
     }
     if (finish_blocks<1>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;
-        const double stored = a.t64 ? acc[0] : a.capacity * acc[0];
+        const double stored = (a.t64 || a.cap) ? acc[0] : a.capacity * acc[0];
         double total = 0.0, scale = 0.0;
         ledger_add(total, scale, stored);
         ledger_add(total, scale, st->lost);
