@@ -121,6 +121,17 @@ def _declare(L):
         "or_hall_set_speed_blocks": (None, [p, C.c_int, dp, ll]),
         "or_hall_checkpoint": (None, [p]),
         "or_hall_restore": (None, [p]),
+        "or_room_new": (p, [C.c_char_p, d, d, i, d, d, d]),
+        "or_room_free": (None, [p]),
+        "or_room_cells": (None, [p, C.POINTER(i), C.POINTER(i), dp]),
+        "or_room_release": (None, [p, dp]),
+        "or_room_step": (i, [p, d, i, vp]),
+        "or_room_advance": (i, [p, d, i, d, vp]),
+        "or_room_get": (None, [p, dp, dp, dp, dp]),
+        "or_room_ledger": (None, [p, dp, dp, dp, dp]),
+        "or_room_max_stable_dt": (d, [p]),
+        "or_room_checkpoint": (None, [p]),
+        "or_room_restore": (None, [p]),
         "or_yee_new": (p, [C.c_char_p, i, i, i, d, d, d, d]),
         "or_yee_free": (None, [p]),
         "or_yee_set_cells": (None, [p, dp, dp, dp]),
@@ -325,6 +336,76 @@ class Hall(_Box):
 
     def restore(self):
         lib().or_hall_restore(self._h)
+
+
+class Room(_Box):
+    """`Room` restated (crates/pantometry-acoustic/src/room.rs): `new`, `released_from`, `step`,
+    `ledger`, `checkpoint`/`restore`. Pressure row-major (i + nx·j); vx (nx−1)·ny, vy nx·(ny−1)."""
+
+    def __init__(self, width, height, across, depth=1.0, density=1.204, speed=343.0, name="room"):
+        L = lib()
+        self._h = L.or_room_new(name.encode(), width, height, across, depth, density, speed)
+        nx, ny, dx = C.c_int(), C.c_int(), C.c_double()
+        L.or_room_cells(self._h, C.byref(nx), C.byref(ny), C.byref(dx))
+        self.cells = (nx.value, ny.value)
+        self.dx = dx.value
+        self.speed, self.density, self.depth = speed, density, depth
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().or_room_free(self._h)
+            self._h = None
+
+    @property
+    def n(self):
+        return self.cells[0] * self.cells[1]
+
+    def release(self, pressure):
+        p = np.ascontiguousarray(pressure, dtype=np.float64).reshape(-1)
+        assert p.size == self.n
+        lib().or_room_release(self._h, _dp(p))
+        return self
+
+    def mode_profile(self, mx, my, amplitude):
+        """`released_in_mode`'s profile (room.rs:166-183), sampled at the nodes."""
+        nx, ny = self.cells
+        lx, ly = (nx - 1) * self.dx, (ny - 1) * self.dx
+        x = np.arange(nx) * self.dx
+        y = np.arange(ny) * self.dx
+        px = np.cos(mx * np.pi * x / lx) if lx > 0 else np.ones(nx)
+        py = np.cos(my * np.pi * y / ly) if ly > 0 else np.ones(ny)
+        return (amplitude * px[None, :] * py[:, None]).reshape(-1)
+
+    def max_stable_dt(self):
+        return lib().or_room_max_stable_dt(self._h)
+
+    def step(self, dt, nsteps=1):
+        v = Violation()
+        rc = lib().or_room_step(self._h, dt, nsteps, C.byref(v))
+        return None if rc == 0 else v.as_dict()
+
+    def advance(self, dt, nsteps=1, tol=1e-9):
+        v = Violation()
+        rc = lib().or_room_advance(self._h, dt, nsteps, tol, C.byref(v))
+        return None if rc == 0 else v.as_dict()
+
+    def fields(self):
+        nx, ny = self.cells
+        p, pp, vx, vy = _out(self.n), _out(self.n), _out((nx - 1) * ny), _out(nx * (ny - 1))
+        lib().or_room_get(self._h, _dp(p), _dp(pp), _dp(vx), _dp(vy))
+        return {"p": p, "p_prev": pp, "vx": vx, "vy": vy}
+
+    def ledger(self):
+        vals = [C.c_double() for _ in range(4)]
+        lib().or_room_ledger(self._h, *[C.byref(v) for v in vals])
+        total, scale, inv, off = (v.value for v in vals)
+        return {"total": total, "scale": scale, "invariant": inv, "offset": off}
+
+    def checkpoint(self):
+        lib().or_room_checkpoint(self._h)
+
+    def restore(self):
+        lib().or_room_restore(self._h)
 
 
 # --------------------------------------------------------------------------------------------

@@ -561,6 +561,101 @@ struct Hall {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Room — pantometry-acoustic/src/room.rs: the two-dimensional staggered scheme (pressure at the
+// nodes, velocities on the faces between them, rigid walls, a depth for the volume).
+// ---------------------------------------------------------------------------------------------
+
+struct Room {
+    std::string name;
+    int nx, ny;
+    double dx, speed, density, depth;
+    std::vector<double> p, pp, vx, vy;
+    bool staggered = false;
+    double offset = 0.0, datum = 0.0;
+    bool has_saved = false;  // room.rs:489-505
+    std::vector<double> sp, svx, svy;
+    bool s_staggered = false;
+
+    // room.rs:243-281
+    double invariant_si() const {
+        double volume = dx * dx * depth;
+        double rc2 = density * speed * speed;
+        if (rc2 <= 0.0) return 0.0;
+        double potential = 0.0;
+        for (size_t k = 0; k < p.size(); ++k) {
+            int i = (int)(k % nx), j = (int)(k / nx);
+            double share = 1.0 / (wall_weight(i, nx) * wall_weight(j, ny));
+            potential += share * p[k] * pp[k] / (2.0 * rc2) * volume;
+        }
+        double kinetic_x = 0.0;
+        for (size_t k = 0; k < vx.size(); ++k) {
+            double u = vx[k];
+            kinetic_x += density * u * u / 2.0 * volume / wall_weight((int)(k / (nx - 1)), ny);
+        }
+        double kinetic_y = 0.0;
+        for (size_t k = 0; k < vy.size(); ++k) {
+            double u = vy[k];
+            kinetic_y += density * u * u / 2.0 * volume / wall_weight((int)(k % nx), nx);
+        }
+        return potential + kinetic_x + kinetic_y;
+    }
+
+    double courant(double dt) const { return speed * dt * std::sqrt(2.0) / dx; }  // room.rs:336-338
+
+    // room.rs:368-478
+    bool step(double dt, or_violation* out) {
+        double c = courant(dt);
+        if (c > 1.0 + 1e-12) {
+            set_violation(out, "Courant number", name + " (two-dimensional wave equation)", 1.0, c, 1.0, 1e-12);
+            return false;
+        }
+        double h = dt;
+        if (h <= 0.0) return true;
+        double rc2 = density * speed * speed;
+        double vh = staggered ? h : 0.5 * h;
+        bool starting = !staggered;
+        staggered = true;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx - 1; ++i) {
+                size_t face = (size_t)j * (nx - 1) + i;
+                vx[face] -= vh / (density * dx) * (p[(size_t)j * nx + i + 1] - p[(size_t)j * nx + i]);
+            }
+        for (int j = 0; j < ny - 1; ++j)
+            for (int i = 0; i < nx; ++i) {
+                size_t face = (size_t)j * nx + i;
+                vy[face] -= vh / (density * dx) * (p[(size_t)(j + 1) * nx + i] - p[(size_t)j * nx + i]);
+            }
+        pp = p;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                double left = i == 0 ? 0.0 : vx[(size_t)j * (nx - 1) + i - 1];
+                double right = i == nx - 1 ? 0.0 : vx[(size_t)j * (nx - 1) + i];
+                double below = j == 0 ? 0.0 : vy[(size_t)(j - 1) * nx + i];
+                double above = j == ny - 1 ? 0.0 : vy[(size_t)j * nx + i];
+                p[(size_t)j * nx + i] -= h * rc2 / dx * (wall_weight(i, nx) * (right - left) + wall_weight(j, ny) * (above - below));
+            }
+        if (starting) {
+            double invariant = invariant_si();
+            double off = datum - invariant;
+            double sc = rmax(std::fabs(datum), std::fabs(invariant));
+            if (sc > 0.0 && std::fabs(off) / sc > 0.25) {
+                set_violation(out, "energy", name + " (starting the leapfrog)", datum, invariant, sc, 0.25);
+                return false;
+            }
+            offset = off;
+        }
+        return true;
+    }
+
+    double energy() const { return invariant_si() + offset; }  // room.rs:226-228
+    or_entry ledger() const {                                  // room.rs:480-482
+        or_entry e{0.0, 0.0};
+        ledger_add(e, energy());
+        return e;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
 // Cavity — pantometry-em/src/cavity.rs (PEC / Magnetic / Open walls, per-cell media,
 // obstruct), plus the soft dipole-current extension on one Ez edge.
 // ---------------------------------------------------------------------------------------------
@@ -1251,6 +1346,85 @@ void or_hall_restore(void* p) {
     Hall* h = (Hall*)p;
     if (!h->has_saved) return;
     h->pp = h->sp; h->p = h->sp; h->vx = h->svx; h->vy = h->svy; h->vz = h->svz; h->staggered = h->s_staggered;
+}
+
+// ---- Room ----
+// room.rs:90-120: nx = max(across, 3), dx from the width, ny from the height, at least 3
+void* or_room_new(const char* name, double width, double height, int across, double depth, double density,
+                  double speed) {
+    Room* r = new Room();
+    r->name = name ? name : "room";
+    r->nx = std::max(across, 3);
+    r->dx = width / (double)(r->nx - 1);
+    r->ny = std::max((int)std::round(height / r->dx) + 1, 3);
+    r->speed = speed; r->density = density; r->depth = depth;
+    size_t n = (size_t)r->nx * r->ny;
+    r->p.assign(n, 0.0); r->pp.assign(n, 0.0);
+    r->vx.assign((size_t)(r->nx - 1) * r->ny, 0.0);
+    r->vy.assign((size_t)r->nx * (r->ny - 1), 0.0);
+    return r;
+}
+void or_room_free(void* p) { delete (Room*)p; }
+void or_room_cells(void* p, int* nx, int* ny, double* dx) {
+    Room* r = (Room*)p; *nx = r->nx; *ny = r->ny; *dx = r->dx;
+}
+// room.rs:140-160 `released_from`, with the profile already sampled at the nodes.
+void or_room_release(void* p, const double* pressure) {
+    Room* r = (Room*)p;
+    std::memcpy(r->p.data(), pressure, r->p.size() * 8);
+    r->pp = r->p;
+    std::fill(r->vx.begin(), r->vx.end(), 0.0);
+    std::fill(r->vy.begin(), r->vy.end(), 0.0);
+    r->staggered = false;
+    r->offset = 0.0;
+    r->datum = r->invariant_si();
+}
+int or_room_step(void* p, double dt, int nsteps, or_violation* out) {
+    Room* r = (Room*)p;
+    for (int s = 0; s < nsteps; ++s)
+        if (!r->step(dt, out)) return 1;
+    return 0;
+}
+int or_room_advance(void* p, double dt, int nsteps, double tol, or_violation* out) {
+    Room* r = (Room*)p;
+    for (int s = 0; s < nsteps; ++s) {
+        or_entry before = r->ledger();
+        or_entry books = r->ledger();
+        if (!r->step(dt, out)) return 1;
+        if (!attribute_energy(r->name, books, r->ledger(), tol, out)) return 1;
+        or_entry after = r->ledger();
+        if (!audit_energy("simulation", before, after, tol, out)) return 1;
+    }
+    return 0;
+}
+void or_room_get(void* p, double* pr, double* pp, double* vx, double* vy) {
+    Room* r = (Room*)p;
+    if (pr) std::memcpy(pr, r->p.data(), r->p.size() * 8);
+    if (pp) std::memcpy(pp, r->pp.data(), r->pp.size() * 8);
+    if (vx) std::memcpy(vx, r->vx.data(), r->vx.size() * 8);
+    if (vy) std::memcpy(vy, r->vy.data(), r->vy.size() * 8);
+}
+void or_room_ledger(void* p, double* total, double* scale, double* invariant, double* offset) {
+    Room* r = (Room*)p;
+    or_entry e = r->ledger();
+    if (total) *total = e.total;
+    if (scale) *scale = e.scale;
+    if (invariant) *invariant = r->invariant_si();
+    if (offset) *offset = r->offset;
+}
+double or_room_max_stable_dt(void* p) {  // room.rs:361-366
+    Room* r = (Room*)p;
+    if (r->speed <= 0.0) return INF;
+    return r->dx / (r->speed * std::sqrt(2.0));
+}
+void or_room_checkpoint(void* p) {
+    Room* r = (Room*)p;
+    r->has_saved = true; r->sp = r->p; r->svx = r->vx; r->svy = r->vy; r->s_staggered = r->staggered;
+}
+void or_room_restore(void* p) {  // room.rs:495-503: pressure_prev is set to the saved pressure
+    Room* r = (Room*)p;
+    if (!r->has_saved) return;
+    r->pp = r->sp; r->p = r->sp; r->vx = r->svx; r->vy = r->svy; r->staggered = r->s_staggered;
 }
 
 // ---- Cavity ----
