@@ -6,6 +6,7 @@
  *
  *   pm_heat    ~ Solid3D  (crates/pantometry-thermal/src/solid.rs)
  *   pm_hall    ~ Hall     (crates/pantometry-acoustic/src/hall.rs)
+ *   pm_room    ~ Room     (crates/pantometry-acoustic/src/room.rs)
  *   pm_cavity  ~ Cavity   (crates/pantometry-em/src/cavity.rs)
  *
  * Each handle is the device-side state of one domain and answers the calls a `Domain` answers
@@ -170,6 +171,42 @@ pm_status pm_hall_checkpoint(pm_hall* h);
 pm_status pm_hall_restore(pm_hall* h);
 pm_status pm_hall_set_stream(pm_hall* h, void* stream);
 void pm_hall_destroy(pm_hall* h);
+
+/* ====================================== Room ======================================== */
+
+typedef struct pm_room pm_room;
+
+typedef struct pm_room_desc {
+    const char* name;
+    double width, height; /* metres */
+    int across;           /* nodes along the width (at least 3) */
+    double depth;         /* metres: the volume a 2D node stands for */
+    double density;       /* kg/m^3 */
+    double speed;         /* m/s */
+    int precision;        /* pm_precision */
+    int device;
+} pm_room_desc;
+
+/* Room::new (room.rs:90-120): nx = max(across, 3), dx = width/(nx-1), ny = max(round(height/dx)+1, 3). */
+pm_status pm_room_create(const pm_room_desc* desc, pm_room** out);
+pm_status pm_room_cells(pm_room* r, int* nx, int* ny, double* dx);
+/* Room::released_from (room.rs:140-160) with the profile sampled at the nodes (i + nx j). */
+pm_status pm_room_release(pm_room* r, const double* pressure, size_t n);
+/* Domain::max_stable_dt (room.rs:361-366): dx/(c sqrt 2), infinite at c = 0. */
+pm_status pm_room_max_stable_dt(pm_room* r, double* seconds);
+pm_status pm_room_set_tolerance(pm_room* r, double tolerance);
+/* `nsteps` calls of Domain::step (room.rs:368-478): the Courant refusal, the half-step start,
+ * the startup offset; ledger and audit as for pm_heat_step. */
+pm_status pm_room_step(pm_room* r, double dt, long long nsteps, pm_violation* out);
+/* total = energy (invariant + startup offset, room.rs:480-482); parts: invariant, offset, datum. */
+pm_status pm_room_ledger(pm_room* r, pm_ledger* out);
+/* Any pointer may be NULL: p (nx ny), p_prev (nx ny), vx ((nx-1) ny), vy (nx (ny-1)). */
+pm_status pm_room_download(pm_room* r, double* p, double* p_prev, double* vx, double* vy);
+/* Domain::checkpoint / restore (room.rs:484-505). */
+pm_status pm_room_checkpoint(pm_room* r);
+pm_status pm_room_restore(pm_room* r);
+pm_status pm_room_set_stream(pm_room* r, void* stream);
+void pm_room_destroy(pm_room* r);
 
 /* ===================================== Cavity ======================================= */
 

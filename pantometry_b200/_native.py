@@ -85,6 +85,19 @@ class HallDesc(C.Structure):
     ]
 
 
+class RoomDesc(C.Structure):
+    _fields_ = [
+        ("name", C.c_char_p),
+        ("width", C.c_double), ("height", C.c_double),
+        ("across", C.c_int),
+        ("depth", C.c_double),
+        ("density", C.c_double),
+        ("speed", C.c_double),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
 class CavityDesc(C.Structure):
     _fields_ = [
         ("name", C.c_char_p),
@@ -148,6 +161,18 @@ SIGNATURES = {
     "pm_hall_restore": (_st, [_p]),
     "pm_hall_set_stream": (_st, [_p, _p]),
     "pm_hall_destroy": (None, [_p]),
+    "pm_room_create": (_st, [C.POINTER(RoomDesc), C.POINTER(_p)]),
+    "pm_room_cells": (_st, [_p, C.POINTER(_i), C.POINTER(_i), _dp]),
+    "pm_room_release": (_st, [_p, _dp, _sz]),
+    "pm_room_max_stable_dt": (_st, [_p, _dp]),
+    "pm_room_set_tolerance": (_st, [_p, _d]),
+    "pm_room_step": (_st, [_p, _d, _ll, _vp]),
+    "pm_room_ledger": (_st, [_p, _lp]),
+    "pm_room_download": (_st, [_p, _dp, _dp, _dp, _dp]),
+    "pm_room_checkpoint": (_st, [_p]),
+    "pm_room_restore": (_st, [_p]),
+    "pm_room_set_stream": (_st, [_p, _p]),
+    "pm_room_destroy": (None, [_p]),
     # Cavity
     "pm_cavity_create": (_st, [C.POINTER(CavityDesc), C.POINTER(_p)]),
     "pm_cavity_fill_cells": (_st, [_p, _dp, _dp, _dp, _sz]),

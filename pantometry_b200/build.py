@@ -23,6 +23,7 @@ UNITS = {
     "runtime.cu": [],
     "heat.cu": [],
     "hall.cu": [],
+    "room.cu": [],
     "cavity.cu": [],
     "ensemble.cu": [],
     "noalloc.cu": [],

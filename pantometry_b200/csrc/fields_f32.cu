@@ -198,6 +198,17 @@ cudaError_t launch_yee_coefs<float>(const YeeCoefArgs<float>& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_room<float>(const RoomArgs<float>& a, cudaStream_t s) {
+    room_step<float><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <>
+cudaError_t launch_room_measure<float>(const RoomMeasureArgs<float>& a, cudaStream_t s) {
+    room_measure<float><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -232,6 +243,7 @@ int occupancy_f32(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>, 256,
                                                               hall_tma_smem_bytes());
             break;
+        case kRoomF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<float>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -11,6 +11,7 @@
 #include "ensemble_kernels.cuh"
 #include "hall_tma.cuh"
 #include "yee_tma.cuh"
+#include "room_kernels.cuh"
 #include "ens_tma.cuh"
 
 namespace pm {
@@ -46,7 +47,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kEnsTma, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kEnsTma, kRoomF64, kRoomF32, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -98,6 +99,8 @@ cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, i
 template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool measure, unsigned nblocks, cudaStream_t s);
 
 // Element-wise conversions between the caller's f64 arrays and an f32 store.
+template <typename Real> cudaError_t launch_room(const RoomArgs<Real>& a, cudaStream_t s);
+template <typename Real> cudaError_t launch_room_measure(const RoomMeasureArgs<Real>& a, cudaStream_t s);
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
 cudaError_t launch_to_f64(const float* src, double* dst, size_t n, cudaStream_t s);
 

@@ -104,6 +104,17 @@ cudaError_t launch_yee_coefs<double>(const YeeCoefArgs<double>& a, cudaStream_t 
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_room<double>(const RoomArgs<double>& a, cudaStream_t s) {
+    room_step<double><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <>
+cudaError_t launch_room_measure<double>(const RoomMeasureArgs<double>& a, cudaStream_t s) {
+    room_measure<double><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f64(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -120,6 +131,7 @@ int occupancy_f64(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double, false, true>, 256, yee_smem_bytes<double>());
             break;
         case kEnsF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false>, 256, 0); break;
+        case kRoomF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<double>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -213,6 +213,54 @@ class Hall(_Domain):
         return out
 
 
+class Room(_Domain):
+    """`Room` (crates/pantometry-acoustic/src/room.rs) on the GPU: the two-dimensional hall."""
+
+    _destroy = "pm_room_destroy"
+    _prefix = "pm_room_"
+
+    def __init__(self, width, height, across, depth=1.0, density=1.204, speed=343.0, precision="f64", name="room",
+                 device=0):
+        self._lib = N.load()
+        d = N.RoomDesc()
+        self._name = name.encode()
+        d.name = self._name
+        d.width, d.height, d.across = width, height, across
+        d.depth, d.density, d.speed = depth, density, speed
+        d.precision = _precision(precision)
+        d.device = device
+        h = C.c_void_p()
+        N.check(self._lib.pm_room_create(C.byref(d), C.byref(h)))
+        self._h = h
+        nx, ny, dx = C.c_int(), C.c_int(), C.c_double()
+        N.check(self._lib.pm_room_cells(h, C.byref(nx), C.byref(ny), C.byref(dx)))
+        self.cells = (nx.value, ny.value)
+        self.dx = dx.value
+        self.precision = d.precision
+
+    @property
+    def n(self):
+        return self.cells[0] * self.cells[1]
+
+    def release(self, pressure):
+        """`released_from` with the profile already sampled at the nodes (i + nx·j)."""
+        p = _f64(pressure, self.n)
+        N.check(self._lib.pm_room_release(self._h, _ptr(p), p.size))
+        return self
+
+    def max_stable_dt(self):
+        out = C.c_double()
+        N.check(self._lib.pm_room_max_stable_dt(self._h, C.byref(out)))
+        return out.value
+
+    def fields(self):
+        nx, ny = self.cells
+        out = {"p": np.empty(self.n), "p_prev": np.empty(self.n), "vx": np.empty((nx - 1) * ny),
+               "vy": np.empty(nx * (ny - 1))}
+        N.check(self._lib.pm_room_download(self._h, *[_ptr(out[k]) for k in ("p", "p_prev", "vx", "vy")]))
+        return out
+
+
 class Cavity(_Domain):
     """`Cavity` (crates/pantometry-em/src/cavity.rs) on the GPU."""
 
