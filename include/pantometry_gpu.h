@@ -7,6 +7,7 @@
  *   pm_heat    ~ Solid3D  (crates/pantometry-thermal/src/solid.rs)
  *   pm_hall    ~ Hall     (crates/pantometry-acoustic/src/hall.rs)
  *   pm_room    ~ Room     (crates/pantometry-acoustic/src/room.rs)
+ *   pm_tube    ~ Tube     (crates/pantometry-acoustic/src/lib.rs:107-560)
  *   pm_cavity  ~ Cavity   (crates/pantometry-em/src/cavity.rs)
  *
  * Each handle is the device-side state of one domain and answers the calls a `Domain` answers
@@ -207,6 +208,46 @@ pm_status pm_room_checkpoint(pm_room* r);
 pm_status pm_room_restore(pm_room* r);
 pm_status pm_room_set_stream(pm_room* r, void* stream);
 void pm_room_destroy(pm_room* r);
+
+/* ====================================== Tube ======================================== */
+
+typedef struct pm_tube pm_tube;
+
+typedef struct pm_tube_desc {
+    const char* name;
+    double length; /* metres */
+    int cells;     /* pressure samples along it (at least 3) */
+    double area;   /* m^2 */
+    double density;
+    double speed;
+    int precision; /* pm_precision */
+    int device;
+} pm_tube_desc;
+
+/* Tube::new (lib.rs:167-193): n = max(cells, 3), dx = length/(n-1), both ends closed. */
+pm_status pm_tube_create(const pm_tube_desc* desc, pm_tube** out);
+pm_status pm_tube_cells(pm_tube* t, int* n, double* dx);
+/* Tube::with_ends (lib.rs:211-215, `End` lib.rs:107-116): kind 0 closed, 1 open, 2 matched to
+ * the impedance z (z <= 0: the tube's own, rho c). */
+pm_status pm_tube_set_ends(pm_tube* t, int left, double z_left, int right, double z_right);
+/* Tube::released_from (lib.rs:226-235) with the profile sampled at the n cells. */
+pm_status pm_tube_release(pm_tube* t, const double* pressure, size_t n);
+/* Domain::max_stable_dt (lib.rs:495-514): dx/c, and dx Z/(2 rho c^2) for an absorbing end. */
+pm_status pm_tube_max_stable_dt(pm_tube* t, double* seconds);
+/* The per-step audit holds the tube's own books against what its ends published (the
+ * `attribute` check of sim.rs:1169-1223): energy plus the published total. */
+pm_status pm_tube_set_tolerance(pm_tube* t, double tolerance);
+/* `nsteps` calls of Domain::step (lib.rs:516-533, advance lib.rs:386-463). */
+pm_status pm_tube_step(pm_tube* t, double dt, long long nsteps, pm_violation* out);
+/* total = energy (lib.rs:535-537); parts: energy, published total (`radiated_energy`), datum. */
+pm_status pm_tube_ledger(pm_tube* t, pm_ledger* out);
+/* Any pointer may be NULL: p (n), p_prev (n), v (n - 1). */
+pm_status pm_tube_download(pm_tube* t, double* p, double* p_prev, double* v);
+/* Domain::checkpoint / restore (lib.rs:539-554). */
+pm_status pm_tube_checkpoint(pm_tube* t);
+pm_status pm_tube_restore(pm_tube* t);
+pm_status pm_tube_set_stream(pm_tube* t, void* stream);
+void pm_tube_destroy(pm_tube* t);
 
 /* ===================================== Cavity ======================================= */
 

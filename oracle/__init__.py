@@ -132,6 +132,19 @@ def _declare(L):
         "or_room_max_stable_dt": (d, [p]),
         "or_room_checkpoint": (None, [p]),
         "or_room_restore": (None, [p]),
+        "or_tube_new": (p, [C.c_char_p, d, i, d, d, d]),
+        "or_tube_free": (None, [p]),
+        "or_tube_dx": (d, [p]),
+        "or_tube_cells": (i, [p]),
+        "or_tube_set_ends": (None, [p, i, d, i, d]),
+        "or_tube_release": (None, [p, dp]),
+        "or_tube_step": (i, [p, d, i, vp]),
+        "or_tube_advance": (i, [p, d, i, d, vp]),
+        "or_tube_get": (None, [p, dp, dp, dp]),
+        "or_tube_ledger": (None, [p, dp, dp, dp, dp, dp]),
+        "or_tube_max_stable_dt": (d, [p]),
+        "or_tube_checkpoint": (None, [p]),
+        "or_tube_restore": (None, [p]),
         "or_yee_new": (p, [C.c_char_p, i, i, i, d, d, d, d]),
         "or_yee_free": (None, [p]),
         "or_yee_set_cells": (None, [p, dp, dp, dp]),
@@ -406,6 +419,66 @@ class Room(_Box):
 
     def restore(self):
         lib().or_room_restore(self._h)
+
+
+END_KINDS = {"closed": 0, "open": 1, "matched": 2}
+
+
+class Tube(_Box):
+    """`Tube` restated (crates/pantometry-acoustic/src/lib.rs:107-560): `new`, `with_ends`,
+    `released_from`, `step`, `ledger`, `checkpoint`/`restore`. Ends: ("closed" | "open" |
+    "matched", z), z <= 0 meaning the tube's own impedance."""
+
+    def __init__(self, length, cells, area=1e-4, density=1.204, speed=343.0, name="tube"):
+        L = lib()
+        self._h = L.or_tube_new(name.encode(), length, cells, area, density, speed)
+        self.n = L.or_tube_cells(self._h)
+        self.dx = L.or_tube_dx(self._h)
+        self.speed, self.density, self.area = speed, density, area
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().or_tube_free(self._h)
+            self._h = None
+
+    def set_ends(self, left, right):
+        (lk, lz), (rk, rz) = left, right
+        lib().or_tube_set_ends(self._h, END_KINDS[lk], lz, END_KINDS[rk], rz)
+        return self
+
+    def release(self, pressure):
+        p = np.ascontiguousarray(pressure, dtype=np.float64).reshape(-1)
+        assert p.size == self.n
+        lib().or_tube_release(self._h, _dp(p))
+        return self
+
+    def max_stable_dt(self):
+        return lib().or_tube_max_stable_dt(self._h)
+
+    def step(self, dt, nsteps=1):
+        v = Violation()
+        rc = lib().or_tube_step(self._h, dt, nsteps, C.byref(v))
+        return None if rc == 0 else v.as_dict()
+
+    def advance(self, dt, nsteps=1, tol=1e-9):
+        v = Violation()
+        rc = lib().or_tube_advance(self._h, dt, nsteps, tol, C.byref(v))
+        return None if rc == 0 else v.as_dict()
+
+    def fields(self):
+        p, pp, v = _out(self.n), _out(self.n), _out(self.n - 1)
+        lib().or_tube_get(self._h, _dp(p), _dp(pp), _dp(v))
+        return {"p": p, "p_prev": pp, "v": v}
+
+    def ledger(self):
+        total, scale, inv, off, rad = self._ledger5(lib().or_tube_ledger)
+        return {"total": total, "scale": scale, "invariant": inv, "offset": off, "radiated": rad}
+
+    def checkpoint(self):
+        lib().or_tube_checkpoint(self._h)
+
+    def restore(self):
+        lib().or_tube_restore(self._h)
 
 
 # --------------------------------------------------------------------------------------------

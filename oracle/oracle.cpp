@@ -656,6 +656,98 @@ struct Room {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Tube — pantometry-acoustic/src/lib.rs:107-560: the one-dimensional staggered scheme, pressure
+// at the n samples, velocity on the n−1 faces, each end closed, open or matched to an impedance.
+// ---------------------------------------------------------------------------------------------
+
+struct Tube {
+    std::string name;
+    int n;
+    double dx, speed, density, area;
+    int end_kind[2] = {0, 0};  // 0 closed, 1 open, 2 matched (lib.rs:107-116)
+    double end_z[2] = {0.0, 0.0};
+    std::vector<double> p, pp, v;
+    bool staggered = false;
+    double offset = 0.0, datum = 0.0, radiated = 0.0;
+    bool has_saved = false;  // lib.rs:539-556
+    std::vector<double> sp, sv;
+    bool s_staggered = false;
+
+    double impedance() const { return density * speed; }  // lib.rs:255-257
+    // lib.rs:301-327
+    double invariant_si() const {
+        double volume = area * dx;
+        double rc2 = density * speed * speed;
+        if (rc2 <= 0.0) return 0.0;
+        int last = n - 1;
+        double potential = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double share = (i == 0 || i == last) ? 0.5 : 1.0;
+            potential += share * p[i] * pp[i] / (2.0 * rc2) * volume;
+        }
+        double kinetic = 0.0;
+        for (double u : v) kinetic += density * u * u / 2.0 * volume;
+        return potential + kinetic;
+    }
+    // lib.rs:368-382
+    double wall_velocity(int end, double boundary_pressure, double outward) const {
+        if (end_kind[end] == 0) return 0.0;
+        if (end_kind[end] == 1) return outward * boundary_pressure / impedance();
+        double zz = end_z[end];
+        if (zz <= 0.0) return outward * boundary_pressure / impedance();
+        return outward * boundary_pressure / zz;
+    }
+    double courant(double dt) const { return speed * dt / dx; }  // lib.rs:358-360
+    // lib.rs:386-463; returns the energy the ends published this step
+    double advance(double dt) {
+        double rc2 = density * speed * speed;
+        double vh = staggered ? dt : 0.5 * dt;
+        bool starting = !staggered;
+        staggered = true;
+        for (size_t i = 0; i < v.size(); ++i) v[i] -= vh / (density * dx) * (p[i + 1] - p[i]);
+        double left_wall = wall_velocity(0, p[0], -1.0);
+        double right_wall = wall_velocity(1, p[n - 1], 1.0);
+        pp = p;
+        double absorbed = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double inflow = i == 0 ? left_wall : v[i - 1];
+            double outflow = i == n - 1 ? right_wall : v[i];
+            double share = (i == 0 || i == n - 1) ? 2.0 : 1.0;
+            p[i] -= dt * rc2 / dx * share * (outflow - inflow);
+        }
+        absorbed += std::fabs(p[0] * left_wall) * area * dt;
+        absorbed += std::fabs(p[n - 1] * right_wall) * area * dt;
+        if (absorbed > 0.0) radiated += absorbed;
+        if (starting) {
+            double invariant = invariant_si();
+            double off = datum - invariant;
+            double sc = rmax(std::fabs(datum), std::fabs(invariant));
+            if (sc > 0.0 && std::fabs(off) / sc <= 0.25) offset = off;
+        }
+        return absorbed > 0.0 ? absorbed : 0.0;
+    }
+    // lib.rs:516-533
+    bool step(double dt, or_violation* out, double* published) {
+        if (published) *published = 0.0;
+        double c = courant(dt);
+        if (c > 1.0 + 1e-12) {
+            set_violation(out, "Courant number", name + " (explicit wave equation)", 1.0, c, 1.0, 1e-12);
+            return false;
+        }
+        if (dt <= 0.0) return true;
+        double pub = advance(dt);
+        if (published) *published = pub;
+        return true;
+    }
+    double energy() const { return invariant_si() + offset; }  // lib.rs:288-290
+    or_entry ledger() const {                                  // lib.rs:535-537
+        or_entry e{0.0, 0.0};
+        ledger_add(e, energy());
+        return e;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
 // Cavity — pantometry-em/src/cavity.rs (PEC / Magnetic / Open walls, per-cell media,
 // obstruct), plus the soft dipole-current extension on one Ez edge.
 // ---------------------------------------------------------------------------------------------
@@ -1425,6 +1517,101 @@ void or_room_restore(void* p) {  // room.rs:495-503: pressure_prev is set to the
     Room* r = (Room*)p;
     if (!r->has_saved) return;
     r->pp = r->sp; r->p = r->sp; r->vx = r->svx; r->vy = r->svy; r->staggered = r->s_staggered;
+}
+
+// ---- Tube ----
+// lib.rs:167-193: cells = max(cells, 3), dx = length/(cells-1), both ends closed
+void* or_tube_new(const char* name, double length, int cells, double area, double density, double speed) {
+    Tube* t = new Tube();
+    t->name = name ? name : "tube";
+    t->n = std::max(cells, 3);
+    t->dx = length / (double)(t->n - 1);
+    t->speed = speed; t->density = density; t->area = area;
+    t->p.assign(t->n, 0.0); t->pp.assign(t->n, 0.0); t->v.assign(t->n - 1, 0.0);
+    return t;
+}
+void or_tube_free(void* p) { delete (Tube*)p; }
+double or_tube_dx(void* p) { return ((Tube*)p)->dx; }
+int or_tube_cells(void* p) { return ((Tube*)p)->n; }
+// lib.rs:211-215 `with_ends`: kind 0 closed, 1 open, 2 matched to z (z <= 0: the tube's own)
+void or_tube_set_ends(void* p, int left, double zl, int right, double zr) {
+    Tube* t = (Tube*)p;
+    t->end_kind[0] = left; t->end_z[0] = zl; t->end_kind[1] = right; t->end_z[1] = zr;
+}
+// lib.rs:226-235 `released_from`, the profile sampled at the cells
+void or_tube_release(void* p, const double* pressure) {
+    Tube* t = (Tube*)p;
+    std::memcpy(t->p.data(), pressure, t->p.size() * 8);
+    t->pp = t->p;
+    std::fill(t->v.begin(), t->v.end(), 0.0);
+    t->staggered = false;
+    t->offset = 0.0;
+    t->datum = t->invariant_si();
+}
+int or_tube_step(void* p, double dt, int nsteps, or_violation* out) {
+    Tube* t = (Tube*)p;
+    for (int s = 0; s < nsteps; ++s)
+        if (!t->step(dt, out, nullptr)) return 1;
+    return 0;
+}
+// Simulation::advance over one tube with its books held against what it published
+// (sim.rs:1169-1223, `attribute`): the energy plus the published total must hold.
+int or_tube_advance(void* p, double dt, int nsteps, double tol, or_violation* out) {
+    Tube* t = (Tube*)p;
+    for (int s = 0; s < nsteps; ++s) {
+        or_entry before = t->ledger();
+        double published = 0.0;
+        if (!t->step(dt, out, &published)) return 1;
+        or_entry after = t->ledger();
+        double expected = -published;
+        double discrepancy = (after.total - before.total) - expected;
+        double scale = rmax(rmax(rmax(rmax(std::fabs(before.total), std::fabs(after.total)), before.scale), after.scale),
+                            std::fabs(expected));
+        if (scale >= 1e-300 && std::fabs(discrepancy) / scale > tol) {
+            set_violation(out, "energy", t->name + " (its own books, against what it moved on the bus)",
+                          before.total + expected, after.total, scale, tol);
+            return 1;
+        }
+    }
+    return 0;
+}
+void or_tube_get(void* p, double* pr, double* pp, double* v) {
+    Tube* t = (Tube*)p;
+    if (pr) std::memcpy(pr, t->p.data(), t->p.size() * 8);
+    if (pp) std::memcpy(pp, t->pp.data(), t->pp.size() * 8);
+    if (v) std::memcpy(v, t->v.data(), t->v.size() * 8);
+}
+void or_tube_ledger(void* p, double* total, double* scale, double* invariant, double* offset, double* radiated) {
+    Tube* t = (Tube*)p;
+    or_entry e = t->ledger();
+    if (total) *total = e.total;
+    if (scale) *scale = e.scale;
+    if (invariant) *invariant = t->invariant_si();
+    if (offset) *offset = t->offset;
+    if (radiated) *radiated = t->radiated;
+}
+// lib.rs:495-514
+double or_tube_max_stable_dt(void* p) {
+    Tube* t = (Tube*)p;
+    if (t->speed <= 0.0) return INF;
+    double wave = t->dx / t->speed;
+    double rc2 = t->density * t->speed * t->speed;
+    auto drain = [&](int e) {
+        if (t->end_kind[e] == 0) return INF;
+        if (t->end_kind[e] == 1) return t->dx * t->impedance() / (2.0 * rc2);
+        double zz = t->end_z[e] > 0.0 ? t->end_z[e] : t->impedance();
+        return t->dx * zz / (2.0 * rc2);
+    };
+    return std::min(std::min(wave, drain(0)), drain(1));
+}
+void or_tube_checkpoint(void* p) {
+    Tube* t = (Tube*)p;
+    t->has_saved = true; t->sp = t->p; t->sv = t->v; t->s_staggered = t->staggered;
+}
+void or_tube_restore(void* p) {  // lib.rs:547-554: pressure_prev is set to the saved pressure
+    Tube* t = (Tube*)p;
+    if (!t->has_saved) return;
+    t->pp = t->sp; t->p = t->sp; t->v = t->sv; t->staggered = t->s_staggered;
 }
 
 // ---- Cavity ----

@@ -98,6 +98,19 @@ class RoomDesc(C.Structure):
     ]
 
 
+class TubeDesc(C.Structure):
+    _fields_ = [
+        ("name", C.c_char_p),
+        ("length", C.c_double),
+        ("cells", C.c_int),
+        ("area", C.c_double),
+        ("density", C.c_double),
+        ("speed", C.c_double),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
 class CavityDesc(C.Structure):
     _fields_ = [
         ("name", C.c_char_p),
@@ -173,6 +186,19 @@ SIGNATURES = {
     "pm_room_restore": (_st, [_p]),
     "pm_room_set_stream": (_st, [_p, _p]),
     "pm_room_destroy": (None, [_p]),
+    "pm_tube_create": (_st, [C.POINTER(TubeDesc), C.POINTER(_p)]),
+    "pm_tube_cells": (_st, [_p, C.POINTER(_i), _dp]),
+    "pm_tube_set_ends": (_st, [_p, _i, _d, _i, _d]),
+    "pm_tube_release": (_st, [_p, _dp, _sz]),
+    "pm_tube_max_stable_dt": (_st, [_p, _dp]),
+    "pm_tube_set_tolerance": (_st, [_p, _d]),
+    "pm_tube_step": (_st, [_p, _d, _ll, _vp]),
+    "pm_tube_ledger": (_st, [_p, _lp]),
+    "pm_tube_download": (_st, [_p, _dp, _dp, _dp]),
+    "pm_tube_checkpoint": (_st, [_p]),
+    "pm_tube_restore": (_st, [_p]),
+    "pm_tube_set_stream": (_st, [_p, _p]),
+    "pm_tube_destroy": (None, [_p]),
     # Cavity
     "pm_cavity_create": (_st, [C.POINTER(CavityDesc), C.POINTER(_p)]),
     "pm_cavity_fill_cells": (_st, [_p, _dp, _dp, _dp, _sz]),

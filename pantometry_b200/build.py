@@ -24,6 +24,7 @@ UNITS = {
     "heat.cu": [],
     "hall.cu": [],
     "room.cu": [],
+    "tube.cu": [],
     "cavity.cu": [],
     "ensemble.cu": [],
     "noalloc.cu": [],

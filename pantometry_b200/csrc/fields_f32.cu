@@ -209,6 +209,17 @@ cudaError_t launch_room_measure<float>(const RoomMeasureArgs<float>& a, cudaStre
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_tube<float>(const TubeArgs<float>& a, cudaStream_t s) {
+    tube_step<float><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <>
+cudaError_t launch_tube_measure<float>(const TubeMeasureArgs<float>& a, cudaStream_t s) {
+    tube_measure<float><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -244,6 +255,7 @@ int occupancy_f32(KernelId id) {
                                                               hall_tma_smem_bytes());
             break;
         case kRoomF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<float>, 256, 0); break;
+        case kTubeF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tube_step<float>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -115,6 +115,17 @@ cudaError_t launch_room_measure<double>(const RoomMeasureArgs<double>& a, cudaSt
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_tube<double>(const TubeArgs<double>& a, cudaStream_t s) {
+    tube_step<double><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <>
+cudaError_t launch_tube_measure<double>(const TubeMeasureArgs<double>& a, cudaStream_t s) {
+    tube_measure<double><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 int occupancy_f64(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -132,6 +143,7 @@ int occupancy_f64(KernelId id) {
             break;
         case kEnsF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false>, 256, 0); break;
         case kRoomF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<double>, 256, 0); break;
+        case kTubeF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tube_step<double>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -120,4 +120,102 @@ static __global__ void __launch_bounds__(256) room_measure(RoomMeasureArgs<Real>
     if (finish_blocks<1>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) a.st->invariant = acc[0];
 }
 
+// ---------------------------------------------------------------------------------------------
+// Tube (crates/pantometry-acoustic/src/lib.rs:107-560): the same scheme in one dimension, n
+// pressure samples, n−1 faces, and ends that are closed, open or matched to an impedance.
+//
+// tube_step — one thread per sample. Its faces come from the old pressure with the reference's
+//   expression (lib.rs:402-405); an end sample's outer face is the wall's velocity from its own
+//   old pressure (lib.rs:368-382, 411-412). The new pressure follows lib.rs:424-433. Fused: the
+//   FP64 invariant (lib.rs:301-327), the work the moving ends publish, |p u| A dt with the new
+//   pressure (lib.rs:441-450), the startup offset (lib.rs:457-462: taken only within 25%, never
+//   refused), and the audit of the tube's books: its energy plus what it has published.
+// ---------------------------------------------------------------------------------------------
+template <typename Real>
+struct TubeArgs {
+    const Real* __restrict__ p0;
+    const Real* __restrict__ v0;
+    Real* __restrict__ p1;
+    Real* __restrict__ v1;
+    int n;
+    Real gain;       // vh/(ρ·dx)
+    Real coef;       // dt·ρc²/dx
+    double outward[2];  // end k's outward sign (−1 left, +1 right), 0 when closed
+    double z[2];        // the impedance end k's wall velocity divides by (lib.rs:368-382)
+    double knode;       // V/(2ρc²), V = area·dx; 0 with ρc² ≤ 0
+    double kface;       // ρ/2·V; 0 with ρc² ≤ 0
+    double area, dt;    // for the published work
+    int starting;
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+template <typename Real>
+static __global__ void __launch_bounds__(256) tube_step(TubeArgs<Real> a) {
+    DevState* st = a.st;
+    if (st->violated) return;
+    const int n = a.n;
+    const Real gain = a.gain;
+    double acc[2] = {0.0, 0.0};  // the invariant of the new state, the work published this step
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Real pc = a.p0[i];
+        Real inflow, outflow;
+        // u = outward·p/Z at an open or matched end, 0 at a closed one
+        if (i == 0) inflow = a.outward[0] == 0.0 ? Real(0) : (Real)(a.outward[0] * (double)pc / a.z[0]);
+        else inflow = a.v0[i - 1] - gain * (pc - a.p0[i - 1]);
+        if (i == n - 1) outflow = a.outward[1] == 0.0 ? Real(0) : (Real)(a.outward[1] * (double)pc / a.z[1]);
+        else outflow = a.v0[i] - gain * (a.p0[i + 1] - pc);
+        if (i < n - 1) a.v1[i] = outflow;
+        const bool end = i == 0 || i == n - 1;
+        const Real share = end ? Real(2) : Real(1);
+        const Real np = pc - a.coef * share * (outflow - inflow);
+        a.p1[i] = np;
+        const double dn = (double)np, dof = (double)outflow;
+        acc[0] += (end ? 0.5 : 1.0) * a.knode * dn * (double)pc + (i < n - 1 ? a.kface * (dof * dof) : 0.0);
+        if (i == 0) acc[1] += fabs(dn * (double)inflow) * a.area * a.dt;
+        if (i == n - 1) acc[1] += fabs(dn * (double)outflow) * a.area * a.dt;
+    }
+    if (finish_blocks<2>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
+        const double invariant = acc[0];
+        if (a.starting) {
+            const double off = st->datum - invariant;
+            const double sc = rmax(fabs(st->datum), fabs(invariant));
+            if (sc > 0.0 && fabs(off) / sc <= 0.25) st->offset = off;
+        }
+        st->injected += acc[1];  // the published total
+        const double energy = invariant + st->offset;
+        double total = 0.0, scale_l = 0.0;
+        ledger_add(total, scale_l, energy);
+        ledger_add(total, scale_l, st->injected);
+        st->part[0] = energy;
+        st->part[1] = st->injected;
+        st->invariant = invariant;
+        audit_and_commit(st, total, scale_l);
+    }
+}
+
+template <typename Real>
+struct TubeMeasureArgs {
+    const Real* p;
+    const Real* pp;
+    const Real* v;
+    int n;
+    double knode, kface;
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+template <typename Real>
+static __global__ void __launch_bounds__(256) tube_measure(TubeMeasureArgs<Real> a) {
+    const int n = a.n;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double u = i < n - 1 ? (double)a.v[i] : 0.0;
+        acc[0] += ((i == 0 || i == n - 1) ? 0.5 : 1.0) * a.knode * (double)a.p[i] * (double)a.pp[i] + a.kface * (u * u);
+    }
+    if (finish_blocks<1>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) a.st->invariant = acc[0];
+}
+
 }  // namespace pm

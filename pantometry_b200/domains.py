@@ -261,6 +261,55 @@ class Room(_Domain):
         return out
 
 
+END_KINDS = {"closed": 0, "open": 1, "matched": 2}
+
+
+class Tube(_Domain):
+    """`Tube` (crates/pantometry-acoustic/src/lib.rs:107-560) on the GPU: the one-dimensional hall,
+    its ends closed, open or matched to an impedance."""
+
+    _destroy = "pm_tube_destroy"
+    _prefix = "pm_tube_"
+
+    def __init__(self, length, cells, area=1e-4, density=1.204, speed=343.0, precision="f64", name="tube", device=0):
+        self._lib = N.load()
+        d = N.TubeDesc()
+        self._name = name.encode()
+        d.name = self._name
+        d.length, d.cells, d.area = length, cells, area
+        d.density, d.speed = density, speed
+        d.precision = _precision(precision)
+        d.device = device
+        h = C.c_void_p()
+        N.check(self._lib.pm_tube_create(C.byref(d), C.byref(h)))
+        self._h = h
+        n, dx = C.c_int(), C.c_double()
+        N.check(self._lib.pm_tube_cells(h, C.byref(n), C.byref(dx)))
+        self.n, self.dx = n.value, dx.value
+        self.precision = d.precision
+
+    def set_ends(self, left, right):
+        """Each end ("closed" | "open" | "matched", z); z <= 0 is the tube's own impedance."""
+        (lk, lz), (rk, rz) = left, right
+        N.check(self._lib.pm_tube_set_ends(self._h, END_KINDS[lk], float(lz), END_KINDS[rk], float(rz)))
+        return self
+
+    def release(self, pressure):
+        p = _f64(pressure, self.n)
+        N.check(self._lib.pm_tube_release(self._h, _ptr(p), p.size))
+        return self
+
+    def max_stable_dt(self):
+        out = C.c_double()
+        N.check(self._lib.pm_tube_max_stable_dt(self._h, C.byref(out)))
+        return out.value
+
+    def fields(self):
+        out = {"p": np.empty(self.n), "p_prev": np.empty(self.n), "v": np.empty(self.n - 1)}
+        N.check(self._lib.pm_tube_download(self._h, *[_ptr(out[k]) for k in ("p", "p_prev", "v")]))
+        return out
+
+
 class Cavity(_Domain):
     """`Cavity` (crates/pantometry-em/src/cavity.rs) on the GPU."""
 
