@@ -8,6 +8,7 @@
  *   pm_hall    ~ Hall     (crates/pantometry-acoustic/src/hall.rs)
  *   pm_room    ~ Room     (crates/pantometry-acoustic/src/room.rs)
  *   pm_tube    ~ Tube     (crates/pantometry-acoustic/src/lib.rs:107-560)
+ *   pm_bar     ~ Bar1D    (crates/pantometry-thermal/src/lib.rs:425-660)
  *   pm_cavity  ~ Cavity   (crates/pantometry-em/src/cavity.rs)
  *
  * Each handle is the device-side state of one domain and answers the calls a `Domain` answers
@@ -248,6 +249,47 @@ pm_status pm_tube_checkpoint(pm_tube* t);
 pm_status pm_tube_restore(pm_tube* t);
 pm_status pm_tube_set_stream(pm_tube* t, void* stream);
 void pm_tube_destroy(pm_tube* t);
+
+/* ===================================== Bar1D ======================================== */
+
+typedef struct pm_bar pm_bar;
+
+typedef struct pm_bar_desc {
+    const char* name;
+    int cells;              /* at least 2 */
+    double dx;              /* metres per cell */
+    double area;            /* cross-section, m^2 */
+    pm_substance substance; /* density, conductivity, specific heat, thermal (emissivity unused) */
+    double initial_kelvin;  /* every cell, and the temperature the stored heat is measured from */
+    int precision;          /* pm_precision */
+    int device;
+} pm_bar_desc;
+
+/* Bar1D::new (lib.rs:443-464). */
+pm_status pm_bar_create(const pm_bar_desc* desc, pm_bar** out);
+/* Set / read every cell's temperature (kelvin). An upload re-takes the books from the new state. */
+pm_status pm_bar_upload(pm_bar* b, const double* kelvin, size_t n);
+pm_status pm_bar_download(pm_bar* b, double* kelvin, size_t n);
+/* The heat the next step takes from the bus, handed in by the caller (lib.rs:590-606): lumped
+ * joules into the first cell (`take_share` of HEAT), joules per cell (a flux over `exposing`'s
+ * faces). Both are booked as taken from the bus. */
+pm_status pm_bar_absorb(pm_bar* b, double joules);
+pm_status pm_bar_deposit(pm_bar* b, const double* joules, size_t n);
+/* Domain::max_stable_dt (lib.rs:564-569): dx^2/(2 alpha). */
+pm_status pm_bar_max_stable_dt(pm_bar* b, double* seconds);
+/* The per-step audit holds the bar's books (books_balance, lib.rs:555-557): stored heat minus
+ * what it took from the bus, the `attribute` check of sim.rs:1169-1223. */
+pm_status pm_bar_set_tolerance(pm_bar* b, double tolerance);
+/* `nsteps` calls of Domain::step (lib.rs:571-627): the Fourier refusal, the heat handed in (first
+ * step only), insulated conduction. */
+pm_status pm_bar_step(pm_bar* b, double dt, long long nsteps, pm_violation* out);
+/* total = stored heat C sum(T - T_ref) (lib.rs:629-631); parts: stored, absorbed. */
+pm_status pm_bar_ledger(pm_bar* b, pm_ledger* out);
+/* Domain::checkpoint / restore (lib.rs:633-639): the cells. */
+pm_status pm_bar_checkpoint(pm_bar* b);
+pm_status pm_bar_restore(pm_bar* b);
+pm_status pm_bar_set_stream(pm_bar* b, void* stream);
+void pm_bar_destroy(pm_bar* b);
 
 /* ===================================== Cavity ======================================= */
 

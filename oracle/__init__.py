@@ -145,6 +145,20 @@ def _declare(L):
         "or_tube_max_stable_dt": (d, [p]),
         "or_tube_checkpoint": (None, [p]),
         "or_tube_restore": (None, [p]),
+        "or_bar_new": (p, [C.c_char_p, i, d, d, d, d, d, i, d]),
+        "or_bar_free": (None, [p]),
+        "or_bar_cells": (i, [p]),
+        "or_bar_set": (None, [p, dp]),
+        "or_bar_get": (None, [p, dp]),
+        "or_bar_absorb": (None, [p, d]),
+        "or_bar_deposit": (None, [p, dp]),
+        "or_bar_max_stable_dt": (d, [p]),
+        "or_bar_fourier_number": (d, [p, d]),
+        "or_bar_step": (i, [p, d, i, vp]),
+        "or_bar_advance": (i, [p, d, i, d, vp]),
+        "or_bar_ledger": (None, [p, dp, dp, dp]),
+        "or_bar_checkpoint": (None, [p]),
+        "or_bar_restore": (None, [p]),
         "or_yee_new": (p, [C.c_char_p, i, i, i, d, d, d, d]),
         "or_yee_free": (None, [p]),
         "or_yee_set_cells": (None, [p, dp, dp, dp]),
@@ -479,6 +493,71 @@ class Tube(_Box):
 
     def restore(self):
         lib().or_tube_restore(self._h)
+
+
+class Bar(_Box):
+    """`Bar1D` restated (crates/pantometry-thermal/src/lib.rs:425-660): insulated explicit
+    conduction; the heat a step takes from the bus is handed in first (`absorb`: lumped, into
+    the first cell; `deposit`: per cell)."""
+
+    def __init__(self, cells, dx, area, density, conductivity, specific_heat, initial, thermal=True, name="bar"):
+        L = lib()
+        self._h = L.or_bar_new(name.encode(), cells, dx, area, density, conductivity, specific_heat, int(thermal),
+                               initial)
+        self.n = L.or_bar_cells(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().or_bar_free(self._h)
+            self._h = None
+
+    @property
+    def cells(self):
+        out = _out(self.n)
+        lib().or_bar_get(self._h, _dp(out))
+        return out
+
+    @cells.setter
+    def cells(self, t):
+        t = np.ascontiguousarray(t, dtype=np.float64).reshape(-1)
+        assert t.size == self.n
+        lib().or_bar_set(self._h, _dp(t))
+
+    def absorb(self, joules):
+        lib().or_bar_absorb(self._h, joules)
+
+    def deposit(self, joules):
+        j = np.ascontiguousarray(joules, dtype=np.float64).reshape(-1)
+        assert j.size == self.n
+        lib().or_bar_deposit(self._h, _dp(j))
+
+    def max_stable_dt(self):
+        return lib().or_bar_max_stable_dt(self._h)
+
+    def fourier_number(self, dt):
+        return lib().or_bar_fourier_number(self._h, dt)
+
+    def step(self, dt, nsteps=1):
+        v = Violation()
+        rc = lib().or_bar_step(self._h, dt, nsteps, C.byref(v))
+        return None if rc == 0 else v.as_dict()
+
+    def advance(self, dt, nsteps=1, tol=1e-9):
+        v = Violation()
+        rc = lib().or_bar_advance(self._h, dt, nsteps, tol, C.byref(v))
+        return None if rc == 0 else v.as_dict()
+
+    def ledger(self):
+        vals = [C.c_double() for _ in range(3)]
+        lib().or_bar_ledger(self._h, *[C.byref(v) for v in vals])
+        total, scale, absorbed = (v.value for v in vals)
+        return {"total": total, "scale": scale, "absorbed": absorbed}
+
+    def checkpoint(self):
+        lib().or_bar_checkpoint(self._h)
+
+    def restore(self):
+        lib().or_bar_restore(self._h)
 
 
 # --------------------------------------------------------------------------------------------

@@ -748,6 +748,83 @@ struct Tube {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Bar1D — pantometry-thermal/src/lib.rs:425-660: explicit conduction along a bar with insulated
+// ends. The heat its step takes from the bus (lumped into the first cell, lib.rs:590-593; per
+// cell over its exposed side, lib.rs:598-606) is handed in by the caller before the step.
+// ---------------------------------------------------------------------------------------------
+
+struct Bar {
+    std::string name;
+    int n;
+    double dx, area, reference;
+    double density, conductivity, specific_heat;
+    int thermal;
+    std::vector<double> cells, saved;
+    double absorbed = 0.0;
+    double lumped = 0.0;             // the next step's share of placeless heat
+    std::vector<double> per_cell;    // the next step's heat per cell, empty: none
+
+    // substance.rs:211-222 (mass_of: density·volume, substance.rs:237-239)
+    double diffusivity() const { return thermal ? conductivity / (density * specific_heat) : NAN; }
+    double cell_capacity() const {  // lib.rs:514-520
+        double volume = area * dx;
+        return thermal ? (density * volume) * specific_heat : INF;
+    }
+    double fourier_number(double dt) const {  // lib.rs:546-551
+        if (!thermal) return INF;
+        return diffusivity() * dt / (dx * dx);
+    }
+    double stored_heat() const {  // lib.rs:536-538
+        double s = 0.0;
+        for (double t : cells) s += t - reference;
+        return cell_capacity() * s;
+    }
+    // lib.rs:571-627; `published` is what the step took from the bus
+    bool step(double dt, or_violation* out, double* taken) {
+        if (taken) *taken = 0.0;
+        double f = fourier_number(dt);
+        if (!std::isfinite(f)) {  // Violation::at (conserved.rs:149-158)
+            set_violation(out, "substance has no diffusivity", name, f, f, std::fabs(f), 0.0);
+            return false;
+        }
+        if (f > 0.5 + 1e-12) {
+            set_violation(out, "Fourier number", name + " (explicit conduction)", 0.5, f, 0.5, 1e-12);
+            return false;
+        }
+        double capacity = cell_capacity();
+        double gained = lumped;
+        lumped = 0.0;
+        absorbed += gained;
+        cells[0] += gained / capacity;
+        double got = gained;
+        if (!per_cell.empty()) {
+            double total = 0.0;
+            for (int i = 0; i < n; ++i) {
+                cells[i] += per_cell[i] / capacity;
+                total += per_cell[i];
+            }
+            absorbed += total;
+            got += total;
+            per_cell.clear();
+        }
+        std::vector<double> previous = cells;
+        int last = n - 1;
+        for (int i = 0; i <= last; ++i) {
+            double left = previous[i > 0 ? i - 1 : 0];
+            double right = previous[i + 1 < last ? i + 1 : last];
+            cells[i] = previous[i] + f * (left - 2.0 * previous[i] + right);
+        }
+        if (taken) *taken = got;
+        return true;
+    }
+    or_entry ledger() const {  // lib.rs:629-631
+        or_entry e{0.0, 0.0};
+        ledger_add(e, stored_heat());
+        return e;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
 // Cavity — pantometry-em/src/cavity.rs (PEC / Magnetic / Open walls, per-cell media,
 // obstruct), plus the soft dipole-current extension on one Ez edge.
 // ---------------------------------------------------------------------------------------------
@@ -1613,6 +1690,72 @@ void or_tube_restore(void* p) {  // lib.rs:547-554: pressure_prev is set to the 
     if (!t->has_saved) return;
     t->pp = t->sp; t->p = t->sp; t->v = t->sv; t->staggered = t->s_staggered;
 }
+
+// ---- Bar1D ----
+// lib.rs:443-464: cells = max(cells, 2), every cell at `initial`, which is also the reference
+void* or_bar_new(const char* name, int cells, double dx, double area, double density, double conductivity,
+                 double specific_heat, int thermal, double initial) {
+    Bar* b = new Bar();
+    b->name = name ? name : "bar";
+    b->n = std::max(cells, 2);
+    b->dx = dx; b->area = area; b->reference = initial;
+    b->density = density; b->conductivity = conductivity; b->specific_heat = specific_heat; b->thermal = thermal;
+    b->cells.assign(b->n, initial);
+    b->saved = b->cells;
+    return b;
+}
+void or_bar_free(void* p) { delete (Bar*)p; }
+int or_bar_cells(void* p) { return ((Bar*)p)->n; }
+void or_bar_set(void* p, const double* t) { Bar* b = (Bar*)p; std::memcpy(b->cells.data(), t, b->cells.size() * 8); }
+void or_bar_get(void* p, double* t) { Bar* b = (Bar*)p; std::memcpy(t, b->cells.data(), b->cells.size() * 8); }
+// The bus's part: lumped heat for the next step's first cell, and heat per cell
+void or_bar_absorb(void* p, double joules) { ((Bar*)p)->lumped += joules; }
+void or_bar_deposit(void* p, const double* joules) {
+    Bar* b = (Bar*)p;
+    if (b->per_cell.empty()) b->per_cell.assign(b->n, 0.0);
+    for (int i = 0; i < b->n; ++i) b->per_cell[i] += joules[i];
+}
+double or_bar_max_stable_dt(void* p) {  // lib.rs:564-569
+    Bar* b = (Bar*)p;
+    if (!b->thermal) return INF;
+    return b->dx * b->dx / (2.0 * b->diffusivity());
+}
+double or_bar_fourier_number(void* p, double dt) { return ((Bar*)p)->fourier_number(dt); }
+int or_bar_step(void* p, double dt, int nsteps, or_violation* out) {
+    Bar* b = (Bar*)p;
+    for (int s = 0; s < nsteps; ++s)
+        if (!b->step(dt, out, nullptr)) return 1;
+    return 0;
+}
+// Simulation::advance over one bar (books_balance, lib.rs:555-557): `attribute`
+// (sim.rs:1169-1223) with the heat taken from the bus as the expected change.
+int or_bar_advance(void* p, double dt, int nsteps, double tol, or_violation* out) {
+    Bar* b = (Bar*)p;
+    for (int s = 0; s < nsteps; ++s) {
+        or_entry before = b->ledger();
+        double taken = 0.0;
+        if (!b->step(dt, out, &taken)) return 1;
+        or_entry after = b->ledger();
+        double discrepancy = (after.total - before.total) - taken;
+        double scale = rmax(rmax(rmax(rmax(std::fabs(before.total), std::fabs(after.total)), before.scale), after.scale),
+                            std::fabs(taken));
+        if (scale >= 1e-300 && std::fabs(discrepancy) / scale > tol) {
+            set_violation(out, "energy", b->name + " (its own books, against what it moved on the bus)",
+                          before.total + taken, after.total, scale, tol);
+            return 1;
+        }
+    }
+    return 0;
+}
+void or_bar_ledger(void* p, double* total, double* scale, double* absorbed) {
+    Bar* b = (Bar*)p;
+    or_entry e = b->ledger();
+    if (total) *total = e.total;
+    if (scale) *scale = e.scale;
+    if (absorbed) *absorbed = b->absorbed;
+}
+void or_bar_checkpoint(void* p) { Bar* b = (Bar*)p; b->saved = b->cells; }  // lib.rs:633-639
+void or_bar_restore(void* p) { Bar* b = (Bar*)p; b->cells = b->saved; }
 
 // ---- Cavity ----
 void* or_yee_new(const char* name, int nx, int ny, int nz, double dx, double eps_r, double mu_r, double sigma) {

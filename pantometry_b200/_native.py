@@ -111,6 +111,19 @@ class TubeDesc(C.Structure):
     ]
 
 
+class BarDesc(C.Structure):
+    _fields_ = [
+        ("name", C.c_char_p),
+        ("cells", C.c_int),
+        ("dx", C.c_double),
+        ("area", C.c_double),
+        ("substance", Substance),
+        ("initial_kelvin", C.c_double),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
 class CavityDesc(C.Structure):
     _fields_ = [
         ("name", C.c_char_p),
@@ -199,6 +212,19 @@ SIGNATURES = {
     "pm_tube_restore": (_st, [_p]),
     "pm_tube_set_stream": (_st, [_p, _p]),
     "pm_tube_destroy": (None, [_p]),
+    "pm_bar_create": (_st, [C.POINTER(BarDesc), C.POINTER(_p)]),
+    "pm_bar_upload": (_st, [_p, _dp, _sz]),
+    "pm_bar_download": (_st, [_p, _dp, _sz]),
+    "pm_bar_absorb": (_st, [_p, _d]),
+    "pm_bar_deposit": (_st, [_p, _dp, _sz]),
+    "pm_bar_max_stable_dt": (_st, [_p, _dp]),
+    "pm_bar_set_tolerance": (_st, [_p, _d]),
+    "pm_bar_step": (_st, [_p, _d, _ll, _vp]),
+    "pm_bar_ledger": (_st, [_p, _lp]),
+    "pm_bar_checkpoint": (_st, [_p]),
+    "pm_bar_restore": (_st, [_p]),
+    "pm_bar_set_stream": (_st, [_p, _p]),
+    "pm_bar_destroy": (None, [_p]),
     # Cavity
     "pm_cavity_create": (_st, [C.POINTER(CavityDesc), C.POINTER(_p)]),
     "pm_cavity_fill_cells": (_st, [_p, _dp, _dp, _dp, _sz]),

@@ -25,6 +25,7 @@ UNITS = {
     "hall.cu": [],
     "room.cu": [],
     "tube.cu": [],
+    "bar.cu": [],
     "cavity.cu": [],
     "ensemble.cu": [],
     "noalloc.cu": [],

@@ -1,4 +1,5 @@
 // The f32-field forms (the chosen precision): fields in f32, ledgers and audits in f64.
+#include <algorithm>
 #include <cudaTypedefs.h>
 
 #include "launch.h"
@@ -220,6 +221,17 @@ cudaError_t launch_tube_measure<float>(const TubeMeasureArgs<float>& a, cudaStre
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_bar<float>(const BarArgs<float>& a, cudaStream_t s) {
+    bar_step<float><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <>
+cudaError_t launch_bar_deposit<float>(float* t, const double* per_cell, double lumped, double capacity, int n, cudaStream_t s) {
+    bar_deposit<float><<<(unsigned)std::min(592, (n + 255) / 256), 256, 0, s>>>(t, per_cell, lumped, capacity, n);
+    return cudaGetLastError();
+}
+
 int occupancy_f32(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -256,6 +268,7 @@ int occupancy_f32(KernelId id) {
             break;
         case kRoomF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<float>, 256, 0); break;
         case kTubeF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tube_step<float>, 256, 0); break;
+        case kBarF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bar_step<float>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

@@ -360,4 +360,64 @@ static __global__ void heat_add_rise32(float* __restrict__ d, float rise, size_t
         d[c] += rise;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Bar1D (crates/pantometry-thermal/src/lib.rs:425-660): explicit conduction along a bar with
+// insulated ends, `prev + f·(left − 2·prev + right)` with the end cells' missing neighbour their
+// own value (lib.rs:614-620). One thread per cell; the plain f64 form (built with --fmad=false)
+// is bit-exact with `Bar1D::step`, the FP32 form keeps T − T_ref. Fused: the stored heat
+// C·Σ(T − T_ref) (lib.rs:536-538) and the audit of the bar's books against the heat it took from
+// the bus (its `attribute` check, books_balance at lib.rs:555-557).
+//
+// bar_deposit — the heat a step takes from the bus before it conducts (lib.rs:590-606): lumped
+// joules into the first cell, then joules per cell, each divided by the cell's capacity.
+// ---------------------------------------------------------------------------------------------
+template <typename Real>
+struct BarArgs {
+    const Real* __restrict__ told;
+    Real* __restrict__ tnew;
+    int n;
+    Real f;            // α·dt/dx² (lib.rs:546-551)
+    double capacity;   // (ρ·area·dx)·c (lib.rs:514-520)
+    double reference;  // T_ref in the plain form; 0 for the FP32 deviations
+    DevState* st;
+    double* partials;
+    unsigned nblocks;
+};
+
+template <typename Real>
+static __global__ void __launch_bounds__(256) bar_step(BarArgs<Real> a) {
+    DevState* st = a.st;
+    if (st->violated) return;
+    const int n = a.n, last = n - 1;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Real prev = a.told[i];
+        const Real left = a.told[i > 0 ? i - 1 : 0];
+        const Real right = a.told[i + 1 < last ? i + 1 : last];
+        const Real nt = prev + a.f * (left - Real(2) * prev + right);
+        a.tnew[i] = nt;
+        acc[0] += (double)nt - a.reference;
+    }
+    if (finish_blocks<1>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
+        const double stored = a.capacity * acc[0];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, stored);
+        ledger_add(total, scale, -st->injected);  // what it has taken from the bus
+        st->part[0] = stored;
+        st->part[1] = st->injected;
+        audit_and_commit(st, total, scale);
+    }
+}
+
+template <typename Real>
+static __global__ void bar_deposit(Real* __restrict__ t, const double* __restrict__ per_cell, double lumped,
+                                   double capacity, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Real v = t[i];
+        if (i == 0 && lumped != 0.0) v = (Real)((double)v + lumped / capacity);
+        if (per_cell) v = (Real)((double)v + per_cell[i] / capacity);
+        t[i] = v;
+    }
+}
+
 }  // namespace pm

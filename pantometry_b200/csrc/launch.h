@@ -47,7 +47,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -102,6 +102,9 @@ template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool mea
 template <typename Real> cudaError_t launch_room(const RoomArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_room_measure(const RoomMeasureArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_tube(const TubeArgs<Real>& a, cudaStream_t s);
+template <typename Real> cudaError_t launch_bar(const BarArgs<Real>& a, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_bar_deposit(Real* t, const double* per_cell, double lumped, double capacity, int n, cudaStream_t s);
 template <typename Real> cudaError_t launch_tube_measure(const TubeMeasureArgs<Real>& a, cudaStream_t s);
 cudaError_t launch_to_f32(const double* src, float* dst, size_t n, cudaStream_t s);
 cudaError_t launch_to_f64(const float* src, double* dst, size_t n, cudaStream_t s);

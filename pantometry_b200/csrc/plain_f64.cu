@@ -1,6 +1,7 @@
 // The plain f64 forms. This translation unit is compiled with --fmad=false: no multiply-add is
 // contracted, so every value is formed by the reference's own expression, rounded per operation
 // as rustc's f64 arithmetic rounds it.
+#include <algorithm>
 #include "launch.h"
 
 namespace pm {
@@ -126,6 +127,17 @@ cudaError_t launch_tube_measure<double>(const TubeMeasureArgs<double>& a, cudaSt
     return cudaGetLastError();
 }
 
+template <>
+cudaError_t launch_bar<double>(const BarArgs<double>& a, cudaStream_t s) {
+    bar_step<double><<<a.nblocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template <>
+cudaError_t launch_bar_deposit<double>(double* t, const double* per_cell, double lumped, double capacity, int n, cudaStream_t s) {
+    bar_deposit<double><<<(unsigned)std::min(592, (n + 255) / 256), 256, 0, s>>>(t, per_cell, lumped, capacity, n);
+    return cudaGetLastError();
+}
+
 int occupancy_f64(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;
@@ -144,6 +156,7 @@ int occupancy_f64(KernelId id) {
         case kEnsF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false>, 256, 0); break;
         case kRoomF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<double>, 256, 0); break;
         case kTubeF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tube_step<double>, 256, 0); break;
+        case kBarF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bar_step<double>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;

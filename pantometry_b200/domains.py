@@ -147,6 +147,55 @@ class Solid3D(_Domain):
         N.check(self._lib.pm_heat_absorb(self._h, float(joules)))
 
 
+class Bar(_Domain):
+    """`Bar1D` (crates/pantometry-thermal/src/lib.rs:425-660) on the GPU: insulated conduction along a
+    bar. `absorb` (lumped, into the first cell) and `deposit` (per cell) hand it the heat its next
+    step takes from the bus."""
+
+    _destroy = "pm_bar_destroy"
+    _prefix = "pm_bar_"
+
+    def __init__(self, cells, dx, area, density, conductivity, specific_heat, initial, thermal=True,
+                 precision="f64", name="bar", device=0):
+        self._lib = N.load()
+        d = N.BarDesc()
+        self._name = name.encode()
+        d.name = self._name
+        d.cells, d.dx, d.area = int(cells), dx, area
+        d.substance = N.Substance(density, conductivity, specific_heat, 0.0, int(thermal))
+        d.initial_kelvin = initial
+        d.precision = _precision(precision)
+        d.device = device
+        h = C.c_void_p()
+        N.check(self._lib.pm_bar_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.n = max(2, int(cells))
+        self.precision = d.precision
+
+    @property
+    def cells(self):
+        out = np.empty(self.n, dtype=np.float64)
+        N.check(self._lib.pm_bar_download(self._h, _ptr(out), out.size))
+        return out
+
+    @cells.setter
+    def cells(self, t):
+        t = _f64(t, self.n)
+        N.check(self._lib.pm_bar_upload(self._h, _ptr(t), t.size))
+
+    def absorb(self, joules):
+        N.check(self._lib.pm_bar_absorb(self._h, float(joules)))
+
+    def deposit(self, joules):
+        j = _f64(joules, self.n)
+        N.check(self._lib.pm_bar_deposit(self._h, _ptr(j), j.size))
+
+    def max_stable_dt(self):
+        out = C.c_double()
+        N.check(self._lib.pm_bar_max_stable_dt(self._h, C.byref(out)))
+        return out.value
+
+
 class Hall(_Domain):
     """`Hall` (crates/pantometry-acoustic/src/hall.rs) on the GPU."""
 

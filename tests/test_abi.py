@@ -28,7 +28,7 @@ def lib():
 
 def test_header_declares_the_domain_surface():
     names = declared_functions()
-    for prefix in ("pm_heat_", "pm_hall_", "pm_room_", "pm_tube_", "pm_cavity_"):
+    for prefix in ("pm_heat_", "pm_hall_", "pm_room_", "pm_tube_", "pm_bar_", "pm_cavity_"):
         for verb in ("create", "step", "ledger", "checkpoint", "restore", "destroy", "set_tolerance"):
             assert prefix + verb in names, prefix + verb
 
