@@ -278,8 +278,8 @@ def load():
         return _lib
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python pantometry_b200/build.py` "
-            "(or __graft_entry__.build()). pantometry_b200 has no CPU fallback."
+            f"{LIB_PATH} is missing: build it with `python pantometry_b200/build.py`. "
+            "pantometry_b200 has no CPU fallback."
         )
     lib = C.CDLL(LIB_PATH)
     for table, required in ((SIGNATURES, True), (OPTIONAL_SIGNATURES, False)):

@@ -432,7 +432,7 @@ struct Cavity : Handle {
 
     // Tensor maps of both parities' six components over the padded lattice.
     pm_status build_maps() {
-        constexpr unsigned P = kYeeTmaPlanes;
+        const unsigned P = (unsigned)yee_tma_planes(!uniform);
         for (int q = 0; q < 2; ++q) {
             const int d0 = (int)L, d1 = ny + 1, d2 = nz + 1;
             if (!hall_tma_map(&maps[q].ex, f[q][0].p, d0, d1, d2, 36, 10, P + 1) ||
@@ -470,13 +470,14 @@ struct Cavity : Handle {
     // P·m − 1 planes, so a chunk and the plane below it fill whole stages).
     YeeStepArgs<float> targs(int par, double dt) const {
         YeeStepArgs<float> a = sargs<float>(par, dt);
-        const unsigned w = wave_of(kYeeTma);
+        const unsigned w = wave_of(uniform ? kYeeTma : kYeeTmaMedia);
+        const int P = yee_tma_planes(!uniform);
         const int X = nx + 1, Y = ny + 1, Z = nz + 1;
-        int best = 2 * kYeeTmaPlanes - 1;
+        int best = 2 * P - 1;
         double best_score = -1.0;
         for (int mlt : {2, 4, 8, 16}) {
-            const int zc = kYeeTmaPlanes * mlt - 1;
-            if (zc > Z && zc != 2 * kYeeTmaPlanes - 1) continue;
+            const int zc = P * mlt - 1;
+            if (zc > Z && zc != 2 * P - 1) continue;
             const Tiles t = make_tiles(X, Y, Z, zc);
             const double per = (double)t.ntiles / w;
             const double rounds = per < 1.0 ? 1.0 : (double)((t.ntiles + w - 1) / w);
@@ -547,11 +548,14 @@ struct Cavity : Handle {
             else dch[q].release();
         }
         if (tma) {
-            // the gains' boxes: the tile's own edges, 32 × 8 × P (both parities share the arrays)
+            // the mixed-ε form stages more planes: the field boxes again, then the gains' boxes,
+            // the tile's own edges, 32 × 8 × P (both parities share the arrays)
+            pm_status ms = build_maps();
+            if (ms != PM_OK) return ms;
             for (int par = 0; par < 2; ++par)
                 for (int q = 0; q < 3; ++q) {
                     CUtensorMap* m = q == 0 ? &maps[par].gx : q == 1 ? &maps[par].gy : &maps[par].gz;
-                    if (!hall_tma_map(m, dgain[q].p, (int)L, ny + 1, nz + 1, 32, 8, kYeeTmaPlanes))
+                    if (!hall_tma_map(m, dgain[q].p, (int)L, ny + 1, nz + 1, 32, 8, kYeeTmaPlanesMedia))
                         return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a cavity gain array");
                 }
         }

@@ -133,24 +133,24 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
 }
 
 cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
-    constexpr int P = kYeeTmaPlanes, S = kYeeTmaStages;
+    constexpr int S = kYeeTmaStages, PU = kYeeTmaPlanesUniform, PM = kYeeTmaPlanesMedia;
     static bool attr = false;
     const bool media = !a.uniform;
     const int smem = (int)yee_tma_smem_bytes(media);
     if (!attr) {
         const int s0 = (int)yee_tma_smem_bytes(false), s1 = (int)yee_tma_smem_bytes(true);
-        cudaFuncSetAttribute(yee_tma_step<P, S, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
-        cudaFuncSetAttribute(yee_tma_step<P, S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
-        cudaFuncSetAttribute(yee_tma_step<P, S, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
-        cudaFuncSetAttribute(yee_tma_step<P, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
+        cudaFuncSetAttribute(yee_tma_step<PU, S, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
+        cudaFuncSetAttribute(yee_tma_step<PU, S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
+        cudaFuncSetAttribute(yee_tma_step<PM, S, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
+        cudaFuncSetAttribute(yee_tma_step<PM, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
         attr = true;
     }
     if (a.solid) {
-        if (media) yee_tma_step<P, S, true, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-        else yee_tma_step<P, S, true, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+        if (media) yee_tma_step<PM, S, true, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+        else yee_tma_step<PU, S, true, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
     } else {
-        if (media) yee_tma_step<P, S, false, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-        else yee_tma_step<P, S, false, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+        if (media) yee_tma_step<PM, S, false, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
+        else yee_tma_step<PU, S, false, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
     }
     return cudaGetLastError();
 }
@@ -255,10 +255,16 @@ int occupancy_f32(KernelId id) {
                                                               kEnsConsumers + 32, ens_tma_smem_bytes());
             break;
         case kYeeTma:
-            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes());
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanes, kYeeTmaStages, false, false>, 256,
-                                                              yee_tma_smem_bytes());
+            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes(false));
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>,
+                                                              256, yee_tma_smem_bytes(false));
+            break;
+        case kYeeTmaMedia:
+            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes(true));
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>,
+                                                              256, yee_tma_smem_bytes(true));
             break;
         case kHallTma:
             cudaFuncSetAttribute(hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>,

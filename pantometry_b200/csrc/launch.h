@@ -47,7 +47,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -83,8 +83,8 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
 // The FP32 uniform-medium cavity step staged by TMA (padded lattice of row pitch L).
 cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s);
 inline size_t yee_tma_smem_bytes(bool media = false) {
-    return media ? yee_tma_smem_bytes_for<kYeeTmaPlanes, true>(kYeeTmaStages)
-                 : yee_tma_smem_bytes_for<kYeeTmaPlanes, false>(kYeeTmaStages);
+    return media ? yee_tma_smem_bytes_for<kYeeTmaPlanesMedia, true>(kYeeTmaStages)
+                 : yee_tma_smem_bytes_for<kYeeTmaPlanesUniform, false>(kYeeTmaStages);
 }
 // One component between the reference layout and the padded lattice (see yee_relayout);
 // src_f64 / dst_f64 select double or float for each side.

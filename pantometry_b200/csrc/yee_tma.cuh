@@ -36,17 +36,13 @@ struct YeeMaps {
     CUtensorMap gx, gy, gz;  // per-edge gains of a cavity of mixed ε (MEDIA)
 };
 
-#ifndef PM_YEE_TMA_PLANES
-#define PM_YEE_TMA_PLANES 4
-#endif
-#ifndef PM_YEE_TMA_STAGES
-#define PM_YEE_TMA_STAGES 2
-#endif
-#ifndef PM_YEE_TMA_MIN_BLOCKS
-#define PM_YEE_TMA_MIN_BLOCKS 2
-#endif
-constexpr int kYeeTmaPlanes = PM_YEE_TMA_PLANES;
-constexpr int kYeeTmaStages = PM_YEE_TMA_STAGES;
+// Planes per stage and resident blocks per SM of each form, both with 2 stages in the ring: one
+// medium 3 planes at three blocks per SM (61 KB of shared memory a block), mixed ε 4 planes at two
+// (95 KB with its gain boxes). Measured on B200 at 384³: one medium 100 Gcell/s at 3 planes and
+// three blocks against 95 at 4 planes and two; mixed ε 85 at 4 planes and two against 60 at 3.
+constexpr int kYeeTmaStages = 2;
+constexpr int kYeeTmaPlanesUniform = 3, kYeeTmaPlanesMedia = 4;
+constexpr int yee_tma_planes(bool media) { return media ? kYeeTmaPlanesMedia : kYeeTmaPlanesUniform; }
 
 constexpr unsigned round128(unsigned b) { return (b + 127u) & ~127u; }
 
@@ -109,7 +105,7 @@ __device__ __forceinline__ void yee_tma_issue(const YeeMaps& m, unsigned stage, 
 }
 
 template <int P, int S, bool SOLID, bool MEDIA>
-static __global__ void __launch_bounds__(256, PM_YEE_TMA_MIN_BLOCKS) yee_tma_step(YeeStepArgs<float> a, unsigned L,
+static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m) {
     DevState* st = a.st;
     if (st->violated) return;
