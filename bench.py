@@ -212,7 +212,7 @@ def run_ours(args):
     plain = world * nodes * T * plain_steps / (ms64 * 1e-3) / 1e9
     per_launch64 = ms64 / (plain_steps * T)
     line = {
-        "metric": METRIC,
+        "metric": METRIC.replace("256^3", f"{args.n}^3"),
         "value": round(value, 3),
         "unit": UNIT,
         "n_gpus": world,
@@ -305,7 +305,7 @@ def run_reference(args):
         samples.append(cpu_baseline(args.n, sample_steps=args.cpu_sample_steps, threads=threads))
     value = statistics.median(s["value"] for s in samples)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC.replace("256^3", f"{args.n}^3"), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded Rng::for_index noise + Ricker source)",
         "impl": "reference",
@@ -581,7 +581,7 @@ def run_cavity(args):
     plain = world * cells * T * plain_steps / (ms64 * 1e-3) / 1e9
     h2d = sum(m for m in shapes.values()) * 8
     line = {
-        "metric": CAV_METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": CAV_METRIC.replace("384^3", f"{n}^3"), "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms32 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 audit",
         "data": "synthetic (zero fields, Gaussian-modulated dipole current)",
@@ -865,7 +865,8 @@ def run_mix(args):
     h2d = hall_cells * 8 + len(ccfg["cavities"]) * sum(shapes.values()) * 8
     d2h = hall_cells * 8 + 64 * (1 + len(ccfg["cavities"]))
     line = {
-        "metric": MIX_METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
+        "metric": MIX_METRIC.replace("1024^3", f"{n}^3").replace("64 Yee 128^3", f"{len(ccfg['cavities'])} Yee {args.cavity_n}^3"),
+        "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": round(ms32 / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 fields, f64 audit",
         "data": "synthetic (seeded Rng::for_index block speeds, noise, inclusions and eps_r; Ricker and dipole sources)",

@@ -45,7 +45,8 @@ struct HallTmaStage {
 
 // Planes per stage, stages in the ring and resident blocks per SM: 8 planes in each of 2 stages
 // (87 KB of shared memory, two blocks per SM) measured fastest on B200 at 256³ among 2-8 planes
-// and 2-5 stages.
+// and 2-5 stages, and against three blocks per SM (6 planes × 2 stages: 166 Gcell/s; 4 × 3: 141;
+// this one: 176).
 #ifndef PM_HALL_TMA_PLANES
 #define PM_HALL_TMA_PLANES 8
 #endif
