@@ -40,6 +40,10 @@ BYTES_F64 = 64
 # dram__bytes_read.sum + dram__bytes_write.sum of one hall_tma_step launch at 256³ (270.4 MB read
 # + 219.5 MB written), from the ncu capture summarised in profiles/hall_tma_step_f32_256.md.
 HALL_F32_TRAFFIC = 489971968
+# dram__bytes_read.sum + dram__bytes_write.sum of one yee_tma_step launch at 256³ cells (432.4 MB
+# read + 366.6 MB written, profiles/yee_tma_step_f32_256.md), per cell; a launch at another size
+# moves that many bytes per cell (the kernel reads and writes each cell's six values once)
+YEE_F32_TRAFFIC_PER_CELL = (432385024 + 366586112) / 256 ** 3
 
 
 def peaks():
@@ -593,7 +597,8 @@ def run_cavity(args):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": shapes["ez"] * 8 + 64},
         "gpu_launches": args.steps * T,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "kernel": "yee_tma_step (FP32, TMA-staged)",
+                     "frac": round(achieved / peak, 4), "traffic": round(YEE_F32_TRAFFIC_PER_CELL * cells),
+                     "traffic_source": "ncu capture at 256^3, scaled by cells", "kernel": "yee_tma_step (FP32, TMA-staged)",
                      "bytes_per_launch": 48 * cells, "peak_source": f"{peak_kind} hbm_gbs"},
         "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
                       "roofline_frac": round(96 * cells / (ms64 / (plain_steps * T) * 1e-3) / 1e9 / peak, 4),
