@@ -46,6 +46,11 @@ struct alignas(16) EnsBrickInfo {
 };
 static_assert(sizeof(EnsBrickInfo) == 128, "one record is one 128-byte bulk copy");
 
+template <bool B>
+struct Flag {
+    static constexpr bool value = B;
+};
+
 constexpr unsigned kEnsHoldBlocks = 16384;  // blocks whose stop flags fit the shared bitmask
 
 struct EnsTmaArgs {
@@ -172,9 +177,10 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
     }
     const int tx = lane, ty = warp;
     double acc[2] = {0.0, 0.0};  // the brick's Σ deviation of the new state, Σ heat shed
-    for (int it = 0;; ++it) {
-        const int slot = it % S;
-        const bool got = mbar_wait(full_base + 8 * slot, (unsigned)((it / S) & 1));
+    int slot = 0;
+    unsigned phase = 0;  // of the slot's full barrier: flips each time the ring wraps
+    for (;; slot = slot + 1 == S ? 0 : slot + 1, phase ^= slot == 0 ? 1u : 0u) {
+        const bool got = mbar_wait(full_base + 8 * slot, phase);
         if (!consumers_and(got)) {
             if (tid == 0)
                 for (unsigned g = 0; g < a.ngrids; ++g) a.states[g].violated = kDeviceTimeout;
@@ -191,21 +197,18 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
         const int i = m.x0 + tx, j = m.y0 + ty;
         if (i < nx && j < ny) {
             const size_t plane = (size_t)pitch * ny;
-            float* __restrict__ tnew = a.nu + m.offset;
-            size_t c = (size_t)i + (size_t)pitch * ((size_t)j + (size_t)ny * kb);
+            // this lane's cell of the stage's first plane; each plane's store steps it by a plane
+            float* __restrict__ out = a.nu + m.offset + ((size_t)i + (size_t)pitch * ((size_t)j + (size_t)ny * kb));
             const int hn = min(P, z1 - kb);  // planes of this stage in the brick
             if (hold) {
-                for (int h = 0; h < hn; ++h, c += plane) tnew[c] = s.t[h + 1][ty + 1][tx + 4];
+                for (int h = 0; h < hn; ++h, out += plane) *out = s.t[h + 1][ty + 1][tx + 4];
             } else {
                 const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
-                const bool edge_xy = !(xl && xh && yl && yh);
+                const bool xedge = m.x0 == 0 || m.x0 + 32 >= nx;  // the brick holds an x face
                 const float ga = m.a;
-                const int exposed = m.exposed;
-                double col_shed = 0.0;
-                bool done = false;  // the stage went through the interior fast path
-                if (!edge_xy && hn == P && kb > 0 && kb + P < nz) {
+                if (!xedge && yl && yh && hn == P && kb > 0 && kb + P < nz) {
                     // a whole stage of interior cells: no film, no bound, the planes below and
-                    // above carried in registers; the same arithmetic as the interior case below
+                    // above carried in registers; the general form's arithmetic without its zeros
                     float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
 #pragma unroll
                     for (int h = 0; h < P; ++h) {
@@ -214,54 +217,80 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                         const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
                         const float sum = (((((xm - here) + (xp - here)) + (ym - here)) + (yp - here)) + (below - here)) + (above - here);
                         const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
-                        tnew[c] = nd;
+                        *out = nd;
+                        out += plane;
                         acc[0] += (double)nd;
-                        c += plane;
                         below = here;
                         here = above;
                     }
-                    done = true;
-                }
+                } else {
+                    // The general form, taken by the whole warp: its row (y) and each plane (z) are
+                    // the same for every lane, so those tests are uniform, and a lane on an x face
+                    // selects its terms rather than diverging. The sums start at +0 and so are never
+                    // −0, which makes adding +0 for an absent neighbour or film exact; the film terms
+                    // are the fused b·(here + off) + shed that the plain `shed += ...` contracts to.
+                    const int exposed = m.exposed;
+                    const bool ex0 = xedge && ((exposed >> 0) & 1), ex1 = xedge && ((exposed >> 1) & 1);
+                    const bool ey0 = ((exposed >> 2) & 1) && !yl, ey1 = ((exposed >> 3) & 1) && !yh;
+                    const bool ez0 = ((exposed >> 4) & 1) && kb == 0;  // plane 0 of the stage is the z− face
+                    const bool ez1 = (exposed >> 5) & 1;
+                    const int zlast = nz - 1 - kb;  // the stage's plane on the z+ face, if below P
+                    // the y and z films are taken only by stages on a face row or a face plane
+                    const bool faces = ey0 || ey1 || ez0 || (ez1 && zlast < hn);
+                    // the x faces' film coefficients, used by every cell of the stage, in registers
+                    const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
+                    double col_shed = 0.0;
+                    auto run = [&](auto faces_tag, auto full_tag) {
+                        constexpr bool FACES = decltype(faces_tag)::value, FULL = decltype(full_tag)::value;
+                        float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
 #pragma unroll
-                for (int h = 0; h < P; ++h) {
-                    if (done || h >= hn) break;
-                    const int k = kb + h;
-                    const float here = s.t[h + 1][ty + 1][tx + 4];
-                    const float below = s.t[h][ty + 1][tx + 4], above = s.t[h + 2][ty + 1][tx + 4];
-                    const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
-                    const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
-                    float nd;
-                    if (!edge_xy && k > 0 && k + 1 < nz) {
-                        // interior: all six neighbours, no film; heat_f32_step's order
-                        const float sum = (((((xm - here) + (xp - here)) + (ym - here)) + (yp - here)) + (below - here)) + (above - here);
-                        // the general path's two roundings, ga·sum − 0 then here + that, spelled out so
-                        // that the compiler cannot fold them into one fused multiply-add
-                        nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
-                    } else {
-                        float sum = 0.0f;  // the neighbours present, in the reference's order
-                        if (xl) sum += xm - here;
-                        if (xh) sum += xp - here;
-                        if (yl) sum += ym - here;
-                        if (yh) sum += yp - here;
-                        if (k > 0) sum += below - here;
-                        if (k + 1 < nz) sum += above - here;
-                        float shed = 0.0f;
-                        if (exposed) {
-                            if (((exposed >> 0) & 1) && !xl) shed += m.b[0] * (here + m.off[0]);
-                            if (((exposed >> 1) & 1) && !xh) shed += m.b[1] * (here + m.off[1]);
-                            if (((exposed >> 2) & 1) && !yl) shed += m.b[2] * (here + m.off[2]);
-                            if (((exposed >> 3) & 1) && !yh) shed += m.b[3] * (here + m.off[3]);
-                            if (((exposed >> 4) & 1) && k == 0) shed += m.b[4] * (here + m.off[4]);
-                            if (((exposed >> 5) & 1) && k + 1 == nz) shed += m.b[5] * (here + m.off[5]);
-                            col_shed += (double)shed;
+                        for (int h = 0; h < P; ++h) {
+                            if (!FULL && h >= hn) break;
+                            const bool zl = h > 0 || kb > 0, zh = h < zlast;
+                            const float above = s.t[h + 2][ty + 1][tx + 4];
+                            const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+                            float sum = 0.0f;  // the neighbours present, in the reference's order
+                            sum += xl ? xm - here : 0.0f;
+                            sum += xh ? xp - here : 0.0f;
+                            if (yl) sum += s.t[h + 1][ty][tx + 4] - here;
+                            if (yh) sum += s.t[h + 1][ty + 2][tx + 4] - here;
+                            if (zl) sum += below - here;
+                            if (zh) sum += above - here;
+                            float shed = 0.0f;
+                            if (exposed) {
+                                if (ex0) {
+                                    const float v = __fmaf_rn(b0, here + o0, shed);
+                                    shed = xl ? shed : v;
+                                }
+                                if (ex1) {
+                                    const float v = __fmaf_rn(b1, here + o1, shed);
+                                    shed = xh ? shed : v;
+                                }
+                                if constexpr (FACES) {
+                                    if (ey0) shed = __fmaf_rn(m.b[2], here + m.off[2], shed);
+                                    if (ey1) shed = __fmaf_rn(m.b[3], here + m.off[3], shed);
+                                    if (ez0 && h == 0) shed = __fmaf_rn(m.b[4], here + m.off[4], shed);
+                                    if (ez1 && !zh) shed = __fmaf_rn(m.b[5], here + m.off[5], shed);
+                                }
+                                col_shed += (double)shed;
+                            }
+                            const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
+                            *out = nd;
+                            out += plane;
+                            acc[0] += (double)nd;
+                            below = here;
+                            here = above;
                         }
-                        nd = here + (ga * sum - shed);
+                    };
+                    if (faces) {
+                        if (hn == P) run(Flag<true>{}, Flag<true>{});
+                        else run(Flag<true>{}, Flag<false>{});
+                    } else {
+                        if (hn == P) run(Flag<false>{}, Flag<true>{});
+                        else run(Flag<false>{}, Flag<false>{});
                     }
-                    tnew[c] = nd;
-                    acc[0] += (double)nd;
-                    c += plane;
+                    acc[1] += col_shed;
                 }
-                acc[1] += col_shed;
             }
         }
         const bool brick_done = kb + P >= z1;

@@ -20,12 +20,12 @@ from pantometry_b200 import workloads as W
 STEPS = 70  # one graph of 64 steps, then six single launches
 
 
-def small_grids(count=9, seed=0x5EED):
-    """Uneven blocks of 3..21 cells per axis with the benchmark's draws; films cycle through
-    insulated, Dirichlet (h = +inf) and a finite h, so all three film paths are covered."""
+def small_grids(count=9, seed=0x5EED, lo=3, hi=21):
+    """Uneven blocks of lo..hi (3..21) cells per axis with the benchmark's draws; films cycle
+    through insulated, Dirichlet (h = +inf) and a finite h, so all three film paths are covered."""
     from pantometry_b200.domains import Ensemble
 
-    cfg = W.heat_ensemble(count=count, seed=seed, lo=3, hi=21)
+    cfg = W.heat_ensemble(count=count, seed=seed, lo=lo, hi=hi)
     grids = []
     for g, src in enumerate(cfg["grids"]):
         grids.append({"counts": src["counts"], "dx": src["dx"], "substance": src["substance"],
@@ -182,6 +182,25 @@ def test_ensemble_f32_tma_and_brick_kernels_agree():
         e.set_shape(bx, planes)
         e.upload(np.concatenate(cells))
         assert e.step(STEPS) is None
+        runs.append(e.download())
+    for r in runs[1:]:
+        assert np.array_equal(r, runs[0])
+
+
+@pytest.mark.gpu
+def test_ensemble_f32_tma_interior_and_face_bricks_agree():
+    """Blocks of 65..99 cells per axis: the TMA kernel's 32-wide bricks include ones clear of every
+    x face (the whole-stage interior form) beside ones holding a face (the general form, one x face
+    selected per lane), with and without films; the plain brick kernel agrees bit for bit."""
+    from pantometry_b200.domains import Ensemble
+
+    grids, cells = small_grids(count=3, seed=0xB16, lo=65, hi=99)
+    runs = []
+    for bx, planes in ((32, 16), (16, 8), (32, 64)):
+        e = Ensemble(grids, precision="f32")
+        e.set_shape(bx, planes)
+        e.upload(np.concatenate(cells))
+        assert e.step(12) is None
         runs.append(e.download())
     for r in runs[1:]:
         assert np.array_equal(r, runs[0])
