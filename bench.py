@@ -44,6 +44,10 @@ HALL_F32_TRAFFIC = 489971968
 # read + 366.6 MB written, profiles/yee_tma_step_f32_256.md), per cell; a launch at another size
 # moves that many bytes per cell (the kernel reads and writes each cell's six values once)
 YEE_F32_TRAFFIC_PER_CELL = (432385024 + 366586112) / 256 ** 3
+# dram__bytes_read.sum + dram__bytes_write.sum of one ens_tma_step launch over the 512-grid heat
+# ensemble (1.149 GB read + 785.9 MB written for 187,991,031 cells,
+# profiles/ens_tma_step_f32_ensemble512.md), per cell
+ENS_F32_TRAFFIC_PER_CELL = (1149139000 + 785889024) / 187991031
 
 
 def peaks():
@@ -463,7 +467,10 @@ def run_ensemble(args):
                 "h2d_bytes_per_step": local_cells * 8, "d2h_bytes_per_step": len(grids) * 56},
         "gpu_launches": args.steps * T,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "kernel": "ens_step<float>",
+                     "frac": round(achieved / peak, 4),
+                     "traffic": round(ENS_F32_TRAFFIC_PER_CELL * local_cells) if shape32[0] == 32 else None,
+                     "traffic_source": "ncu capture of the 512-grid ensemble, per cell",
+                     "kernel": "ens_tma_step (FP32, TMA-staged)" if shape32[0] == 32 else "ens_step<float>",
                      "bytes_per_launch": 8 * local_cells, "peak_source": f"{peak_kind} hbm_gbs"},
         "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
                       "roofline_frac": round(16 * local_cells / (ms64 / (plain_steps * T) * 1e-3) / 1e9 / peak, 4),
