@@ -170,6 +170,7 @@ SIGNATURES = {
     "pm_heat_absorb": (_st, [_p, _d]),
     "pm_heat_checkpoint": (_st, [_p]),
     "pm_heat_restore": (_st, [_p]),
+    "pm_heat_set_cells_per_thread": (_st, [_p, _i]),
     "pm_heat_set_stream": (_st, [_p, _p]),
     "pm_heat_destroy": (None, [_p]),
     # Hall

@@ -8,6 +8,7 @@ namespace pm {
 
 cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s) {
     if (a.kx) heat_f32_step<true><<<a.nblocks, tile_block(), 0, s>>>(a);
+    else if (a.quads) heat_f32_quad_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     else heat_f32_step<false><<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -237,6 +238,7 @@ int occupancy_f32(KernelId id) {
     cudaError_t e = cudaSuccess;
     switch (id) {
         case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step<false>, 256, 0); break;
+        case kHeatF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_step, 256, 0); break;
         case kHallF32:
             cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<float, false>, 256, hall_smem_bytes<float>());

@@ -48,6 +48,9 @@ struct Heat : Handle {
     DBuf dkx32, dky32, dkz32, dm32, dfilm32;
     size_t film_off[6] = {0, 0, 0, 0, 0, 0};
     double m_dt = NAN;
+    // cells of a row per thread in the FP32 form: 4 (heat_f32_quad_step) where the block is uniform
+    // and its rows hold a multiple of 4 cells, else 1 (heat_f32_step); 1 forces the latter
+    int cells_per_thread = 4;
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
     double saved_lost = 0.0, saved_supplied = 0.0;
@@ -336,8 +339,10 @@ struct Heat : Handle {
             a.m = dm32.as<float>(); a.cap = dcap.as<double>();
             for (int f = 0; f < 6; ++f) a.film[f] = dfilm32.as<float>() + film_off[f];
         }
-        const unsigned w = wave_of(kHeatF32);
-        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
+        a.quads = uniform && nx % 4 == 0 && cells_per_thread == 4 ? 1 : 0;
+        const unsigned w = wave_of(a.quads ? kHeatF32Quad : kHeatF32);
+        const int tx = a.quads ? nx / 4 : nx;  // the threads along a row
+        a.tiles = make_tiles(tx, ny, nz, choose_zc(tx, ny, nz, w));
         a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
@@ -582,6 +587,18 @@ pm_status pm_heat_restore(pm_heat* hp) {
     s = h->write_state();
     if (s != PM_OK) return s;
     return h->measure();
+}
+
+pm_status pm_heat_set_cells_per_thread(pm_heat* hp, int cells) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (cells != 1 && cells != 4) return fail(PM_BAD_ARG, "cells per thread: 1 or 4");
+    if (cells != h->cells_per_thread) {
+        PM_CUDA(cudaStreamSynchronize(h->stream()));
+        h->drop_graphs();  // the captured launches hold the old tiling
+        h->cells_per_thread = cells;
+    }
+    return PM_OK;
 }
 
 pm_status pm_heat_set_stream(pm_heat* hp, void* stream) {

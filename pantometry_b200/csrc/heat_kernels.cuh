@@ -203,11 +203,30 @@ struct HeatF32Args {
     const float* __restrict__ m;
     const double* __restrict__ cap;
     const float* film[6];
+    int quads;  // uniform blocks with rows of a multiple of 4: heat_f32_quad_step, tiles of quads
     Tiles tiles;
     DevState* st;
     double* partials;
     unsigned nblocks;
 };
+
+// The books of an FP32 step, after its cells: the block's partials reduced in fixed order by the
+// last block to finish, then the ledger and the audit.
+__device__ __forceinline__ void heat_f32_books(const HeatF32Args& a, double (&acc)[2], bool filled) {
+    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+        DevState* st = a.st;
+        const double stored = filled ? acc[0] : a.capacity * acc[0];
+        st->lost += filled ? acc[1] : a.capacity * acc[1];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, stored);
+        ledger_add(total, scale, st->lost);
+        ledger_add(total, scale, -st->supplied);
+        st->part[0] = stored;
+        st->part[1] = st->lost;
+        st->part[2] = -st->supplied;
+        audit_and_commit(st, total, scale);
+    }
+}
 
 // Chosen form, z-marching like the plain form; neighbours in the plane come from L1/L2.
 template <bool FILLED>
@@ -286,19 +305,75 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
         }
         acc[1] += col_shed;
     }
-    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
-        DevState* st = a.st;
-        const double stored = FILLED ? acc[0] : a.capacity * acc[0];
-        st->lost += FILLED ? acc[1] : a.capacity * acc[1];
-        double total = 0.0, scale = 0.0;
-        ledger_add(total, scale, stored);
-        ledger_add(total, scale, st->lost);
-        ledger_add(total, scale, -st->supplied);
-        st->part[0] = stored;
-        st->part[1] = st->lost;
-        st->part[2] = -st->supplied;
-        audit_and_commit(st, total, scale);
+    heat_f32_books(a, acc, FILLED);
+}
+
+// The uniform FP32 form with four adjacent cells of a row per thread (rows of a multiple of 4
+// cells, so every quad starts on 16 bytes): per plane one 16-byte load each for the plane above
+// and the rows either side, two scalar loads for the cells left and right of the quad, one 16-byte
+// store. Each cell's arithmetic is heat_f32_step's uniform case in the same order and roundings
+// (the sums from +0 with the neighbours present, the films as the fused b·(here + off) + shed,
+// then here + (a·sum − shed) as a fused multiply-add and an add), so the fields agree with it bit
+// for bit; only the order of the FP64 sums within a block differs.
+static __global__ void __launch_bounds__(256) heat_f32_quad_step(HeatF32Args a) {
+    if (a.st->violated) return;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t plane = (size_t)nx * ny;
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    double acc[2] = {0.0, 0.0};
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        int q, j, k0, k1;
+        tile_column(a.tiles, t, q, j, k0, k1);  // q: the quad's place along the row
+        const int i = 4 * q;
+        if (i >= nx || j >= ny) continue;
+        const size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+        const float* p = a.dold + c;
+        float* o = a.dnew + c;
+        const bool xl = i > 0, xh = i + 4 < nx, yl = j > 0, yh = j + 1 < ny;
+        float4 below = k0 > 0 ? __ldg(reinterpret_cast<const float4*>(p - plane)) : zero;
+        float4 here = __ldg(reinterpret_cast<const float4*>(p));
+        double col_shed = 0.0;
+        for (int k = k0; k < k1; ++k, p += plane, o += plane) {
+            const bool zl = k > 0, zh = k + 1 < nz;
+            const float4 above = zh ? __ldg(reinterpret_cast<const float4*>(p + plane)) : zero;
+            const float4 ym = yl ? __ldg(reinterpret_cast<const float4*>(p - nx)) : zero;
+            const float4 yp = yh ? __ldg(reinterpret_cast<const float4*>(p + nx)) : zero;
+            const float xm = xl ? __ldg(p - 1) : 0.0f, xp = xh ? __ldg(p + 4) : 0.0f;
+            const float hv[4] = {here.x, here.y, here.z, here.w}, bv[4] = {below.x, below.y, below.z, below.w};
+            const float av[4] = {above.x, above.y, above.z, above.w};
+            const float mv[4] = {ym.x, ym.y, ym.z, ym.w}, pv[4] = {yp.x, yp.y, yp.z, yp.w};
+            float nd[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float h = hv[e];
+                const bool l = e > 0 || xl, r = e < 3 || xh;  // the cell's x neighbours are in the block
+                float s = 0.0f;
+                if (l) s += (e == 0 ? xm : hv[e - 1]) - h;
+                if (r) s += (e == 3 ? xp : hv[e + 1]) - h;
+                if (yl) s += mv[e] - h;
+                if (yh) s += pv[e] - h;
+                if (zl) s += bv[e] - h;
+                if (zh) s += av[e] - h;
+                float shed = 0.0f;
+                if (a.exposed && (!(l && r && yl && yh) || !zl || !zh)) {
+                    if (((a.exposed >> 0) & 1) && !l) shed = __fmaf_rn(a.b[0], h + a.off[0], shed);
+                    if (((a.exposed >> 1) & 1) && !r) shed = __fmaf_rn(a.b[1], h + a.off[1], shed);
+                    if (((a.exposed >> 2) & 1) && !yl) shed = __fmaf_rn(a.b[2], h + a.off[2], shed);
+                    if (((a.exposed >> 3) & 1) && !yh) shed = __fmaf_rn(a.b[3], h + a.off[3], shed);
+                    if (((a.exposed >> 4) & 1) && !zl) shed = __fmaf_rn(a.b[4], h + a.off[4], shed);
+                    if (((a.exposed >> 5) & 1) && !zh) shed = __fmaf_rn(a.b[5], h + a.off[5], shed);
+                    col_shed += (double)shed;
+                }
+                nd[e] = __fadd_rn(h, __fmaf_rn(a.a, s, -shed));
+                acc[0] += (double)nd[e];
+            }
+            *reinterpret_cast<float4*>(o) = make_float4(nd[0], nd[1], nd[2], nd[3]);
+            below = here;
+            here = above;
+        }
+        acc[1] += col_shed;
     }
+    heat_f32_books(a, acc, false);
 }
 
 // The opening ledger of a freshly uploaded block: stored heat only (lost and supplied are zero

@@ -121,6 +121,11 @@ class Solid3D(_Domain):
         N.check(self._lib.pm_heat_losing_from(self._h, f, ambient, convection, area))
         return self
 
+    def set_cells_per_thread(self, cells):
+        """Cells of a row per thread in the FP32 form: 4 (the default, where the block is one
+        material and its rows hold a multiple of 4 cells) or 1; the fields agree bit for bit."""
+        N.check(self._lib.pm_heat_set_cells_per_thread(self._h, int(cells)))
+
     def fill(self, mask, density, conductivity, specific_heat, emissivity=0.0, thermal=True):
         m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
         s = N.Substance(density, conductivity, specific_heat, emissivity, int(thermal))

@@ -1,0 +1,57 @@
+"""The FP32 `Solid3D` step with four adjacent cells of a row per thread (heat_f32_quad_step, taken
+by blocks of one material whose rows hold a multiple of 4 cells) against one cell per thread
+(heat_f32_step) on the same block. Both do `Solid3D::step`'s arithmetic in f32
+(crates/pantometry-thermal/src/solid.rs:1773-1826) in the same order and roundings, so the fields
+agree bit for bit under insulated faces, Dirichlet films (h = +inf) and films of finite h on some
+faces; the books, summed in another order, agree to 1e-12 of the ledger's scale. Both stay within
+the oracle's FP32 bounds, audited every step.
+"""
+import numpy as np
+import pytest
+
+from helpers import dirichlet_films, heat_pair
+
+pytestmark = pytest.mark.gpu
+
+ALUMINIUM = dict(density=2700.0, conductivity=167.0, specific_heat=896.0, emissivity=0.0)
+
+
+def films_of(kind, counts, dx):
+    nx, ny, nz = counts
+    areas = [(ny * dx) * (nz * dx)] * 2 + [(nx * dx) * (nz * dx)] * 2 + [(nx * dx) * (ny * dx)] * 2
+    if kind == "insulated":
+        return []
+    if kind == "dirichlet":
+        return dirichlet_films(counts, dx, 300.0)
+    return [(0, 280.0, 50.0, areas[0]), (1, 320.0, 2000.0, areas[1]), (3, 290.0, 10.0, areas[3]),
+            (4, 310.0, 500.0, areas[4])]
+
+
+@pytest.mark.parametrize("counts", [(4, 3, 5), (8, 8, 8), (64, 20, 17), (100, 9, 33)])
+@pytest.mark.parametrize("kind", ["insulated", "dirichlet", "finite"])
+def test_quads_and_single_cells_agree(counts, kind):
+    dx = 1e-3
+    cells = 300.0 + 30.0 * np.random.default_rng(sum(counts)).random(int(np.prod(counts)))
+    films = films_of(kind, counts, dx)
+    runs = []
+    for per_thread in (4, 1):
+        o, g = heat_pair(counts, dx, ALUMINIUM, 300.0, films, cells, precision="f32")
+        g.set_cells_per_thread(per_thread)
+        g.set_tolerance(1e-6)
+        dt = 0.9 * g.max_stable_dt()
+        assert g.step(dt, 70) is None  # a captured graph of 64, then six single launches
+        runs.append((g.cells, g.ledger()))
+    assert o.step(dt, 70) is None
+    (quad, lq), (single, ls) = runs
+    bad = np.flatnonzero(quad.view(np.uint64) != single.view(np.uint64))
+    assert bad.size == 0, f"{bad.size} cells differ, first at {bad[0]}"
+    assert abs(lq["total"] - ls["total"]) <= 1e-12 * max(ls["scale"], 1e-300)
+    assert np.abs(quad - o.cells).max() < 1e-4  # kelvin, on a 30 K spread
+
+
+def test_cells_per_thread_is_one_or_four():
+    _, g = heat_pair((8, 4, 4), 1e-3, ALUMINIUM, 300.0, precision="f32")
+    with pytest.raises(Exception):
+        g.set_cells_per_thread(2)
+    g.set_cells_per_thread(1)
+    g.set_cells_per_thread(4)
