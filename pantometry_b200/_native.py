@@ -253,6 +253,7 @@ SIGNATURES = {
     "pm_ensemble_step": (_st, [_p, _ll, _vp]),
     "pm_ensemble_ledgers": (_st, [_p, _lp, _i]),
     "pm_ensemble_set_shape": (_st, [_p, _i, _i]),
+    "pm_ensemble_set_brick": (_st, [_p, _i, _i, _i]),
     "pm_ensemble_shape": (_st, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
     "pm_ensemble_autotune": (_st, [_p, _i, C.POINTER(_i), C.POINTER(_i)]),
     "pm_ensemble_set_stream": (_st, [_p, _p]),

@@ -28,13 +28,18 @@ double ens_rust_max(double a, double b) {  // f64::max
     return a > b ? a : b;
 }
 
-// The brick shapes the autotuner chooses among: log2 of the x extent (y = 256 / x) and the
-// number of planes each column marches.
+// The brick shapes the autotuner chooses among: log2 of the threads along x (256 threads, so
+// y = 256 >> bxs rows), the planes each thread marches, and the cells of its row each thread takes
+// (1, or 4 for the f32 quad shapes). Every shape has its own x and y extents in cells.
 struct EnsShape {
-    int bxs, zc;
+    int bxs, zc, cells;
+    int x() const { return cells << bxs; }
+    int y() const { return 256 >> bxs; }
 };
-constexpr EnsShape kEnsShapes[] = {{5, 16}, {5, 8}, {5, 32}, {5, 64}, {4, 8}, {4, 16},
-                                   {4, 32}, {4, 64}, {6, 8}, {6, 16}, {6, 32}, {6, 64}};
+constexpr EnsShape kEnsShapes[] = {{5, 16, 1}, {5, 8, 1},  {5, 32, 1}, {5, 64, 1}, {4, 8, 1},  {4, 16, 1},
+                                   {4, 32, 1}, {4, 64, 1}, {6, 8, 1},  {6, 16, 1}, {6, 32, 1}, {6, 64, 1},
+                                   {2, 32, 4}, {2, 64, 4}, {3, 32, 4}, {3, 64, 4}, {4, 32, 4}, {4, 64, 4},
+                                   {5, 32, 4}, {5, 64, 4}};
 constexpr int kEnsShapeCount = sizeof(kEnsShapes) / sizeof(kEnsShapes[0]);
 
 // What `Solid3D::resolve` and `worst_rate_now` give for one uniform block with films on all six
@@ -148,12 +153,15 @@ struct Ensemble : Handle {
     DBuf field[2], stage, dgrids, dbricks, dstates, bpartials, saved, saved_states;
 
     size_t esize() const { return precision == PM_PLAIN_F64 ? sizeof(double) : sizeof(float); }
-    unsigned wave() const { return wave_of(precision == PM_PLAIN_F64 ? kEnsF64 : kEnsF32); }
+    unsigned wave() const {
+        return wave_of(precision == PM_PLAIN_F64 ? kEnsF64 : kEnsShapes[shape].cells == 4 ? kEnsF32Quad : kEnsF32);
+    }
 
     // Brick list and block table for a shape; uploads both.
     pm_status set_shape(int sh) {
         const EnsShape s = kEnsShapes[sh];
-        const int bx = 1 << s.bxs, by = 256 >> s.bxs;
+        if (s.cells != 1 && precision == PM_PLAIN_F64) return fail(PM_BAD_ARG, "quad brick shapes are f32 only");
+        const int bx = s.x(), by = s.y();
         bricks.clear();
         for (size_t g = 0; g < grids.size(); ++g) {
             EnsGrid& e = grids[g];
@@ -210,6 +218,7 @@ struct Ensemble : Handle {
         a.nbricks = (unsigned)bricks.size();
         a.ngrids = (unsigned)grids.size();
         a.bxs = kEnsShapes[shape].bxs;
+        a.quads = kEnsShapes[shape].cells == 4 ? 1 : 0;
         a.states = dstates.as<DevState>();
         a.partials = bpartials.as<double>();
         return a;
@@ -218,7 +227,7 @@ struct Ensemble : Handle {
 
     cudaError_t launch(int par, bool measure, cudaStream_t s) const {
         if (precision == PM_PLAIN_F64) return launch_ens<double>(args<double>(par), measure, nblocks(), s);
-        if (!measure && tma && kEnsShapes[shape].bxs == 5) {
+        if (!measure && tma && kEnsShapes[shape].bxs == 5 && kEnsShapes[shape].cells == 1) {
             EnsTmaArgs t{};
             t.e = args<float>(par);
             t.maps = dmaps.as<CUtensorMap>() + (size_t)par * grids.size();
@@ -492,16 +501,24 @@ pm_status pm_ensemble_set_shape(pm_ensemble* ep, int brick_x, int planes) {
     Ensemble* e = reinterpret_cast<Ensemble*>(ep);
     ENS_GUARD(e);
     for (int q = 0; q < kEnsShapeCount; ++q)
-        if ((1 << kEnsShapes[q].bxs) == brick_x && kEnsShapes[q].zc == planes) return e->set_shape(q);
+        if (kEnsShapes[q].cells == 1 && kEnsShapes[q].x() == brick_x && kEnsShapes[q].zc == planes) return e->set_shape(q);
     return fail(PM_BAD_ARG, "brick shape: x extent 16, 32 or 64 and 8, 16, 32 or 64 planes");
+}
+
+pm_status pm_ensemble_set_brick(pm_ensemble* ep, int brick_x, int brick_y, int planes) {
+    Ensemble* e = reinterpret_cast<Ensemble*>(ep);
+    ENS_GUARD(e);
+    for (int q = 0; q < kEnsShapeCount; ++q)
+        if (kEnsShapes[q].x() == brick_x && kEnsShapes[q].y() == brick_y && kEnsShapes[q].zc == planes) return e->set_shape(q);
+    return fail(PM_BAD_ARG, "brick: one of the listed shapes (x × y × planes)");
 }
 
 pm_status pm_ensemble_shape(pm_ensemble* ep, int* brick_x, int* brick_y, int* planes) {
     Ensemble* e = reinterpret_cast<Ensemble*>(ep);
     ENS_GUARD(e);
     const EnsShape s = kEnsShapes[e->shape];
-    if (brick_x) *brick_x = 1 << s.bxs;
-    if (brick_y) *brick_y = 256 >> s.bxs;
+    if (brick_x) *brick_x = s.x();
+    if (brick_y) *brick_y = s.y();
     if (planes) *planes = s.zc;
     return PM_OK;
 }
@@ -527,6 +544,7 @@ pm_status pm_ensemble_autotune(pm_ensemble* ep, int trial_steps, int* brick_x, i
     float best_ms = std::numeric_limits<float>::infinity();
     pm_status result = PM_OK;
     for (int q = 0; q < kEnsShapeCount && result == PM_OK; ++q) {
+        if (kEnsShapes[q].cells != 1 && e->precision == PM_PLAIN_F64) continue;  // the quads are f32 only
         if ((result = e->set_shape(q)) != PM_OK) break;
         cudaError_t ce = cudaSuccess;
         for (int w = 0; w < 2 && ce == cudaSuccess; ++w) { ce = e->launch(e->parity, false, e->stream()); e->parity ^= 1; }
@@ -555,7 +573,7 @@ pm_status pm_ensemble_autotune(pm_ensemble* ep, int trial_steps, int* brick_x, i
         e->states[g].tol = books[g].tol;
     }
     if ((s = e->write_states()) != PM_OK) return s;
-    if (brick_x) *brick_x = 1 << kEnsShapes[best].bxs;
+    if (brick_x) *brick_x = kEnsShapes[best].x();
     if (planes) *planes = kEnsShapes[best].zc;
     return PM_OK;
 }

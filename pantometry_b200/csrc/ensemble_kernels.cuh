@@ -59,7 +59,8 @@ struct EnsArgs {
     const EnsBrick* __restrict__ bricks;
     unsigned nbricks;
     unsigned ngrids;
-    int bxs;             // log2 of the brick's x extent (4, 5 or 6)
+    int bxs;             // log2 of the threads along the brick's x extent (2 to 6)
+    int quads;           // f32 only: each thread takes four adjacent cells of its row
     DevState* states;    // one per block: its books, ledger and audit
     double* partials;    // two per brick
 };
@@ -169,20 +170,103 @@ __device__ __forceinline__ void ens_brick(const EnsArgs<Real>& a, const EnsGrid&
     }
 }
 
-// A block whose audit failed keeps its state: its bricks copy old to new, so the ping-pong
-// parity stays the same for every block of the ensemble.
-template <typename Real>
-__device__ __forceinline__ void ens_hold(const EnsArgs<Real>& a, const EnsGrid& g, const EnsBrick& br) {
+// Four adjacent cells of a row per thread (the f32 quad shapes): heat_f32_quad_step's arithmetic
+// on a brick of one block, which is ens_brick's f32 arithmetic cell for cell (the same order and
+// roundings), so the fields agree with every other brick shape bit for bit. Rows are padded to a
+// multiple of 4 cells, so every quad starts on 16 bytes; cells of a quad past the block's last
+// column (the padding) are neither used as neighbours nor written nor summed.
+template <bool MEASURE>
+__device__ __forceinline__ void ens_brick_quad(const EnsArgs<float>& a, const EnsGrid& g, const EnsBrick& br,
+                                               double (&acc)[2]) {
     const int tid = threadIdx.x;
-    const int i = br.x0 + (tid & ((1 << a.bxs) - 1));
+    const int i = br.x0 + 4 * (tid & ((1 << a.bxs) - 1));
     const int j = br.y0 + (tid >> a.bxs);
-    if (i >= g.nx || j >= g.ny) return;
-    const size_t plane = (size_t)g.pitch * g.ny;
-    size_t c = g.offset + (size_t)i + (size_t)g.pitch * ((size_t)j + (size_t)g.ny * br.z0);
-    for (int k = br.z0; k < br.z1; ++k, c += plane) a.nu[c] = a.old[c];
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const int pitch = g.pitch;
+    const size_t plane = (size_t)pitch * ny;
+    const int k0 = br.z0, k1 = br.z1;
+    const size_t c = g.offset + (size_t)i + (size_t)pitch * ((size_t)j + (size_t)ny * k0);
+    const float* p = a.old + c;
+    float* o = a.nu + c;
+    const int valid = min(4, nx - i);  // cells of the quad inside the block
+    if (MEASURE) {
+        for (int k = k0; k < k1; ++k, p += plane) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+            acc[0] += (double)v.x;
+            if (valid > 1) acc[0] += (double)v.y;
+            if (valid > 2) acc[0] += (double)v.z;
+            if (valid > 3) acc[0] += (double)v.w;
+        }
+        return;
+    }
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const bool xl = i > 0, xh = i + 4 < nx, yl = j > 0, yh = j + 1 < ny;
+    const float ga = g.a;
+    float4 below = k0 > 0 ? __ldg(reinterpret_cast<const float4*>(p - plane)) : zero;
+    float4 here = __ldg(reinterpret_cast<const float4*>(p));
+    double col_shed = 0.0;
+    for (int k = k0; k < k1; ++k, p += plane, o += plane) {
+        const bool zl = k > 0, zh = k + 1 < nz;
+        const float4 above = zh ? __ldg(reinterpret_cast<const float4*>(p + plane)) : zero;
+        const float4 ym = yl ? __ldg(reinterpret_cast<const float4*>(p - pitch)) : zero;
+        const float4 yp = yh ? __ldg(reinterpret_cast<const float4*>(p + pitch)) : zero;
+        const float xm = xl ? __ldg(p - 1) : 0.0f, xp = xh ? __ldg(p + 4) : 0.0f;
+        const float hv[4] = {here.x, here.y, here.z, here.w}, bv[4] = {below.x, below.y, below.z, below.w};
+        const float av[4] = {above.x, above.y, above.z, above.w};
+        const float mv[4] = {ym.x, ym.y, ym.z, ym.w}, pv[4] = {yp.x, yp.y, yp.z, yp.w};
+        float nd[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float h = hv[e];
+            const bool l = e > 0 || xl, r = e < 3 ? i + e + 1 < nx : xh;  // x neighbours in the block
+            float sum = 0.0f;
+            if (l) sum += (e == 0 ? xm : hv[e - 1]) - h;
+            if (r) sum += (e == 3 ? xp : hv[e + 1]) - h;
+            if (yl) sum += mv[e] - h;
+            if (yh) sum += pv[e] - h;
+            if (zl) sum += bv[e] - h;
+            if (zh) sum += av[e] - h;
+            float shed = 0.0f;
+            if (g.exposed && (!(l && r && yl && yh) || !zl || !zh)) {
+                if (((g.exposed >> 0) & 1) && !l) shed = __fmaf_rn(g.b[0], h + g.off[0], shed);
+                if (((g.exposed >> 1) & 1) && !r) shed = __fmaf_rn(g.b[1], h + g.off[1], shed);
+                if (((g.exposed >> 2) & 1) && !yl) shed = __fmaf_rn(g.b[2], h + g.off[2], shed);
+                if (((g.exposed >> 3) & 1) && !yh) shed = __fmaf_rn(g.b[3], h + g.off[3], shed);
+                if (((g.exposed >> 4) & 1) && !zl) shed = __fmaf_rn(g.b[4], h + g.off[4], shed);
+                if (((g.exposed >> 5) & 1) && !zh) shed = __fmaf_rn(g.b[5], h + g.off[5], shed);
+                if (e < valid) col_shed += (double)shed;
+            }
+            nd[e] = __fadd_rn(h, __fmaf_rn(ga, sum, -shed));
+            if (e < valid) acc[0] += (double)nd[e];
+        }
+        if (valid == 4) {
+            *reinterpret_cast<float4*>(o) = make_float4(nd[0], nd[1], nd[2], nd[3]);
+        } else {
+            for (int e = 0; e < valid; ++e) o[e] = nd[e];
+        }
+        below = here;
+        here = above;
+    }
+    acc[1] += col_shed;
 }
 
-template <typename Real, bool MEASURE>
+// A block whose audit failed keeps its state: its bricks copy old to new, so the ping-pong
+// parity stays the same for every block of the ensemble.
+template <typename Real, bool QUAD>
+__device__ __forceinline__ void ens_hold(const EnsArgs<Real>& a, const EnsGrid& g, const EnsBrick& br) {
+    const int tid = threadIdx.x;
+    const int i = br.x0 + (QUAD ? 4 : 1) * (tid & ((1 << a.bxs) - 1));
+    const int j = br.y0 + (tid >> a.bxs);
+    if (i >= g.nx || j >= g.ny) return;
+    const int cells = QUAD ? min(4, g.nx - i) : 1;
+    const size_t plane = (size_t)g.pitch * g.ny;
+    size_t c = g.offset + (size_t)i + (size_t)g.pitch * ((size_t)j + (size_t)g.ny * br.z0);
+    for (int k = br.z0; k < br.z1; ++k, c += plane)
+        for (int e = 0; e < cells; ++e) a.nu[c + e] = a.old[c + e];
+}
+
+template <typename Real, bool MEASURE, bool QUAD = false>
 static __global__ void __launch_bounds__(256) ens_step(EnsArgs<Real> a) {
     __shared__ double red[32 * 2];
     __shared__ int last;
@@ -192,11 +276,12 @@ static __global__ void __launch_bounds__(256) ens_step(EnsArgs<Real> a) {
         const EnsGrid& g = a.grids[br.grid];
         DevState* st = a.states + br.grid;
         if (!MEASURE && st->violated) {  // block-uniform: every thread reads the same word
-            ens_hold<Real>(a, g, br);
+            ens_hold<Real, QUAD>(a, g, br);
             continue;
         }
         double acc[2] = {0.0, 0.0};
-        ens_brick<Real, MEASURE>(a, g, br, acc);
+        if constexpr (QUAD) ens_brick_quad<MEASURE>(a, g, br, acc);
+        else ens_brick<Real, MEASURE>(a, g, br, acc);
         block_sum<2>(acc, red);
         if (tid == 0) {
             a.partials[2 * (size_t)b] = acc[0];

@@ -93,8 +93,13 @@ cudaError_t launch_to_f64(const float* src, double* dst, size_t n, cudaStream_t 
 
 template <>
 cudaError_t launch_ens<float>(const EnsArgs<float>& a, bool measure, unsigned nblocks, cudaStream_t s) {
-    if (measure) ens_step<float, true><<<nblocks, 256, 0, s>>>(a);
-    else ens_step<float, false><<<nblocks, 256, 0, s>>>(a);
+    if (a.quads) {
+        if (measure) ens_step<float, true, true><<<nblocks, 256, 0, s>>>(a);
+        else ens_step<float, false, true><<<nblocks, 256, 0, s>>>(a);
+    } else {
+        if (measure) ens_step<float, true><<<nblocks, 256, 0, s>>>(a);
+        else ens_step<float, false><<<nblocks, 256, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -250,6 +255,7 @@ int occupancy_f32(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
         case kEnsF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false>, 256, 0); break;
+        case kEnsF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false, true>, 256, 0); break;
         case kEnsTma:
             cudaFuncSetAttribute(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ens_tma_smem_bytes());

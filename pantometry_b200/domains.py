@@ -534,8 +534,13 @@ class Ensemble:
         return [{"total": l.total, "scale": l.scale, "parts": [l.parts[q] for q in range(l.n_parts)], "steps": l.steps}
                 for l in out]
 
-    def set_shape(self, brick_x, planes):
-        N.check(self._lib.pm_ensemble_set_shape(self._h, int(brick_x), int(planes)))
+    def set_shape(self, brick_x, planes, brick_y=None):
+        """The brick shape: x extent and planes (one cell per thread, y = 256 / x), or with
+        `brick_y` any listed shape, the f32 quad shapes (16 × 64, 32 × 32, 64 × 16, 128 × 8) among them."""
+        if brick_y is None:
+            N.check(self._lib.pm_ensemble_set_shape(self._h, int(brick_x), int(planes)))
+        else:
+            N.check(self._lib.pm_ensemble_set_brick(self._h, int(brick_x), int(brick_y), int(planes)))
 
     def shape(self):
         bx, by, zc = C.c_int(), C.c_int(), C.c_int()

@@ -171,15 +171,17 @@ def test_ensemble_refusals_and_audit_name_the_block():
 
 @pytest.mark.gpu
 def test_ensemble_f32_tma_and_brick_kernels_agree():
-    """32-wide bricks step with the TMA-staged kernel, 16- and 64-wide with the plain brick kernel;
-    both do heat_f32_step's arithmetic on the same padded rows, so the fields agree bit for bit."""
+    """32-wide bricks step with the TMA-staged kernel, 16- and 64-wide with the plain brick kernel,
+    the quad shapes with four cells of a row per thread; all do heat_f32_step's arithmetic on the
+    same padded rows, so the fields agree bit for bit."""
     from pantometry_b200.domains import Ensemble
 
     grids, cells = small_grids(count=10, seed=0xA11)
     runs = []
-    for bx, planes in ((32, 16), (16, 8), (64, 32), (32, 64)):
+    # one cell per thread (x, planes), then the quad shapes (x, planes, y)
+    for shape in ((32, 16), (16, 8), (64, 32), (32, 64), (16, 32, 64), (32, 64, 32), (128, 32, 8)):
         e = Ensemble(grids, precision="f32")
-        e.set_shape(bx, planes)
+        e.set_shape(*shape)
         e.upload(np.concatenate(cells))
         assert e.step(STEPS) is None
         runs.append(e.download())
@@ -191,16 +193,29 @@ def test_ensemble_f32_tma_and_brick_kernels_agree():
 def test_ensemble_f32_tma_interior_and_face_bricks_agree():
     """Blocks of 65..99 cells per axis: the TMA kernel's 32-wide bricks include ones clear of every
     x face (the whole-stage interior form) beside ones holding a face (the general form, one x face
-    selected per lane), with and without films; the plain brick kernel agrees bit for bit."""
+    selected per lane), with and without films; the plain brick kernel and the quad shapes agree
+    bit for bit."""
     from pantometry_b200.domains import Ensemble
 
     grids, cells = small_grids(count=3, seed=0xB16, lo=65, hi=99)
     runs = []
-    for bx, planes in ((32, 16), (16, 8), (32, 64)):
+    for shape in ((32, 16), (16, 8), (32, 64), (64, 64, 16), (128, 32, 8)):
         e = Ensemble(grids, precision="f32")
-        e.set_shape(bx, planes)
+        e.set_shape(*shape)
         e.upload(np.concatenate(cells))
         assert e.step(12) is None
         runs.append(e.download())
     for r in runs[1:]:
         assert np.array_equal(r, runs[0])
+
+
+@pytest.mark.gpu
+def test_ensemble_quad_shapes_are_f32_only():
+    from pantometry_b200.domains import Ensemble
+
+    grids, cells = small_grids(count=2)
+    e = Ensemble(grids, precision="f64")
+    with pytest.raises(Exception):
+        e.set_shape(32, 32, 32)
+    e.set_shape(32, 32, 8)  # the one-cell 32 × 8 shape by its extents
+    assert e.shape() == (32, 8, 32)
