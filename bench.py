@@ -488,6 +488,165 @@ def run_ensemble(args):
         dist.destroy_process_group()
 
 
+HEAT_METRIC = "Gcell-updates/s (heat block 64^3, plain f64, energy audit every step)"
+
+
+def run_heat(args):
+    """Config 1: a 64³ block (or `--n`) of the heat substance with Dirichlet 300 K films on every
+    face and a 50 K Gaussian hot spot at a seed-jittered point, dt at 0.9 of the limit; one bench
+    step = `timesteps` audited steps. `value` is the plain f64 form the config names; the FP32
+    form (four cells per thread where the rows allow) is reported beside it. The 64³ state fits
+    in L2, so L2 is flushed before every bench step, outside the events that time it."""
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import workloads as W
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = init_dist(local) if world > 1 else None
+    n, T = args.n, args.timesteps
+    cfg = W.heat_block(n, steps=T)
+    cells = n ** 3
+    stream = torch.cuda.Stream(device=local)
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device=local)  # 256 MB, twice the L2
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(precision, k, w, tol):
+        b = W.build_heat(cfg, precision=precision, device=local)
+        b.set_stream(stream.cuda_stream)
+        b.set_tolerance(tol)
+        dt = cfg["dt_fraction"] * b.max_stable_dt()
+        for _ in range(w):
+            v = b.step(dt, T)
+            assert v is None, v
+        barrier()
+        ms = 0.0
+        with Clocks(local) as clk:
+            for _ in range(k):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                v = b.step(dt, T)
+                assert v is None, v
+                end.record(stream)
+                torch.cuda.synchronize()
+                ms += start.elapsed_time(end)
+        barrier()
+        return b, dt, max_over_ranks(ms), clk
+
+    b64, dt, ms64, clk = timed("f64", args.steps, args.warmup, 1e-9)
+    field64, led64 = b64.cells, b64.ledger()
+    del b64
+    b32, _, ms32, _ = timed("f32", args.steps, args.warmup, 1e-6)
+    del b32
+    # FP32 against f64 after the same steps from the same start
+    a32, _, _, _ = timed("f32", 0, args.warmup + args.steps, 1e-6)
+    field_err = float(np.abs(a32.cells - field64).max())
+    l32 = a32.ledger()
+    ledger_err = abs(l32["total"] - led64["total"]) / max(abs(led64["total"]), led64["scale"], 1e-300)
+    del a32
+
+    # e2e through the C ABI with host buffers: the block's kelvin from pinned memory, the run, the
+    # ledger back, every bench step
+    b = W.build_heat(cfg, precision="f64", device=local)
+    b.set_stream(stream.cuda_stream)
+    b.set_tolerance(1e-9)
+    pinned = torch.empty(cells, dtype=torch.float64, pin_memory=True).numpy()
+    pinned[:] = cfg["cells"]
+    for _ in range(args.warmup):
+        b.cells = pinned
+        b.step(dt, T)
+    barrier()
+    t0 = time.perf_counter()
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        b.cells = pinned
+        v = b.step(dt, T)
+        assert v is None, v
+        b.ledger()
+    e0.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    e2e_ms = max_over_ranks(max(s0.elapsed_time(e0), wall_ms))
+    del b
+
+    peak, peak_kind = peaks()
+    value = world * cells * T * args.steps / (ms64 * 1e-3) / 1e9
+    fp32 = world * cells * T * args.steps / (ms32 * 1e-3) / 1e9
+    quads = n % 4 == 0
+    line = {
+        "metric": HEAT_METRIC.replace("64^3", f"{n}^3"), "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms64 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (300 K block, 50 K Gaussian hot spot, sigma 8 cells, seed-jittered centre)",
+        "config": {"workload": f"heat_block {n}^3 cells, diffusivity 1e-4 m^2/s, dx 1 mm, dt 0.9 x the limit, "
+                               f"Dirichlet 300 K faces, {T} timesteps per step, energy audit every timestep",
+                   "cells": cells, "timesteps_per_step": T, "parallelism": f"replicas x{world}",
+                   "l2": f"state {16 * cells / 1e6:.1f} MB (f64, both parities); L2 flushed before every bench step, "
+                         "outside the timed events"},
+        "e2e": {"value": round(world * cells * T * args.steps / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * cells, "d2h_bytes_per_step": 64},
+        "gpu_launches": args.steps * T,
+        "roofline": {"bound": "hbm", "achieved": round(16 * cells * T * args.steps / (ms64 * 1e-3) / 1e9, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(16 * cells * T * args.steps / (ms64 * 1e-3) / 1e9 / peak, 4), "traffic": None,
+                     "kernel": "heat_plain_step (f64)", "bytes_per_launch": 16 * cells,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "note": "L2-resident within a bench step at 64^3" if 16 * cells < 126e6 else "state larger than L2"},
+        "fp32": {"value": round(fp32, 3), "unit": UNIT, "ms_per_step": round(ms32 / args.steps, 3),
+                 "kernel": "heat_f32_quad_step (four cells per thread)" if quads else "heat_f32_step",
+                 "roofline_frac": round(8 * cells * T * args.steps / (ms32 * 1e-3) / 1e9 / peak, 4),
+                 "fp32_over_f64": round(fp32 / value, 3)},
+        "error_vs_f64": {"max_abs_kelvin": field_err, "ledger_rel": ledger_err,
+                         "after_timesteps": T * (args.warmup + args.steps)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_heat(cfg, T if n <= 64 else args.cpu_sample_steps)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline_heat(cfg, sample_steps):
+    """`Simulation::advance` over the block's `Solid3D::step` and its ledger, restated (the
+    oracle), one core."""
+    import oracle
+
+    nx, ny, nz = cfg["counts"]
+    s = cfg["substance"]
+    o = oracle.Heat(cfg["counts"], cfg["dx"], s["density"], s["conductivity"], s["specific_heat"], cfg["initial"],
+                    emissivity=s["emissivity"])
+    for f, amb, h, area in cfg["films"]:
+        o.losing_from(f, amb, h, area)
+    o.cells = cfg["cells"]
+    dt = cfg["dt_fraction"] * o.max_stable_dt()
+    assert o.advance(dt, 1, tol=1e-9) is None  # warm-up
+    t0 = time.perf_counter()
+    assert o.advance(dt, sample_steps, tol=1e-9) is None
+    secs = time.perf_counter() - t0
+    cells = nx * ny * nz
+    return {"value": round(cells * sample_steps / secs / 1e9, 6), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"the {nx}x{ny}x{nz} block, {sample_steps} audited Simulation::advance steps "
+                      f"(after 1 warm-up step), 1 thread, {secs:.2f} s"}
+
+
 CAV_METRIC = "Gcell-updates/s (Yee cavity 384^3, FP32 fields + FP64 audit)"
 
 
@@ -989,12 +1148,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble", "cavity", "mix"],
+    ap.add_argument("--workload", default="hall", choices=["hall", "ensemble", "cavity", "mix", "heat"],
                     help="hall: the acoustic hall 256^3 (the headline); ensemble: 512 uneven heat grids; "
                          "cavity: the Yee cavity 384^3; mix: the 1024^3 heterogeneous hall and 64 Yee 128^3 "
-                         "dielectric cavities")
+                         "dielectric cavities; heat: the 64^3 heat block, plain f64 and FP32")
     ap.add_argument("--cavity-n", type=int, default=128, help="mix: cells per axis of each cavity")
-    ap.add_argument("--n", type=int, default=None, help="grid size: hall 256 nodes, cavity 384 cells per axis")
+    ap.add_argument("--n", type=int, default=None, help="grid size: hall 256 nodes, cavity 384, heat 64 cells per axis")
     ap.add_argument("--grids", type=int, default=None, help="ensemble: 512 heat grids; mix: 64 cavities")
     ap.add_argument("--timesteps", type=int, default=None, help="timesteps per bench step (hall 5000, ensemble 2000)")
     ap.add_argument("--cpu-sample-steps", type=int, default=None,
@@ -1002,11 +1161,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.n is None:
-        args.n = {"cavity": 384, "mix": 1024}.get(args.workload, 256)
+        args.n = {"cavity": 384, "mix": 1024, "heat": 64}.get(args.workload, 256)
     if args.grids is None:
         args.grids = 64 if args.workload == "mix" else 512
     if args.timesteps is None:
-        args.timesteps = 5000 if args.workload == "hall" else 2000
+        args.timesteps = {"hall": 5000, "heat": 1000}.get(args.workload, 2000)
     if args.cpu_sample_steps is None:
         args.cpu_sample_steps = 16 if args.workload == "hall" else 8
     if args.workload == "mix":
@@ -1016,6 +1175,14 @@ def main():
                                              "the mix's parts are timed per cell in the hall and cavity arms"}))
         else:
             run_mix(args)
+        return
+    if args.workload == "heat":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "workload": "heat",
+                              "unavailable": "the reference arm times the headline hall and the ensemble; "
+                                             "the heat block's CPU path is the cpu_baseline of this line"}))
+        else:
+            run_heat(args)
         return
     if args.workload == "cavity":
         if args.impl == "reference":
