@@ -132,10 +132,11 @@ pm_status pm_heat_absorb(pm_heat* h, double joules);
 /* Domain::checkpoint / restore (solid.rs:1935-1950). */
 pm_status pm_heat_checkpoint(pm_heat* h);
 pm_status pm_heat_restore(pm_heat* h);
-/* Cells of a row per thread in the FP32 form (no reference counterpart: a launch shape, like the
- * ensemble's brick shape). 4, the default, takes four adjacent cells per thread where the block
- * is one material and its rows hold a multiple of 4 cells; 1 takes one cell per thread. The
- * fields are the same bit for bit either way. */
+/* Cells of a row per thread (no reference counterpart: a launch shape, like the ensemble's brick
+ * shape). The default is the precision's wide form where the block is one material and its rows
+ * allow: 2 adjacent cells per thread in the plain f64 form (rows of an even number of cells), 4 in
+ * the FP32 form (rows of a multiple of 4). 1 takes one cell per thread; the other accepted value
+ * is the precision's width (2 or 4). The fields are the same bit for bit either way. */
 pm_status pm_heat_set_cells_per_thread(pm_heat* h, int cells);
 /* Run subsequent work on `stream` (a cudaStream_t); NULL restores the handle's own stream. */
 pm_status pm_heat_set_stream(pm_heat* h, void* stream);

@@ -48,9 +48,10 @@ struct Heat : Handle {
     DBuf dkx32, dky32, dkz32, dm32, dfilm32;
     size_t film_off[6] = {0, 0, 0, 0, 0, 0};
     double m_dt = NAN;
-    // cells of a row per thread in the FP32 form: 4 (heat_f32_quad_step) where the block is uniform
-    // and its rows hold a multiple of 4 cells, else 1 (heat_f32_step); 1 forces the latter
-    int cells_per_thread = 4;
+    // the wide forms, where the block is uniform and its rows allow: two cells of a row per thread
+    // in the plain form (heat_plain_pair_step, even rows), four in the FP32 form
+    // (heat_f32_quad_step, rows of a multiple of 4); false: one cell per thread throughout
+    bool wide = true;
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
     double saved_lost = 0.0, saved_supplied = 0.0;
@@ -307,8 +308,10 @@ struct Heat : Handle {
         a.nx = nx; a.ny = ny; a.nz = nz;
         a.dts = dt; a.dx = dx; a.reference = reference;
         a.films = films;
-        const unsigned w = wave_of(kHeatPlain);
-        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w));
+        a.pairs = uniform && nx % 2 == 0 && wide ? 1 : 0;
+        const unsigned w = wave_of(a.pairs ? kHeatPlainPair : kHeatPlain);
+        const int tx = a.pairs ? nx / 2 : nx;  // the threads along a row
+        a.tiles = make_tiles(tx, ny, nz, choose_zc(tx, ny, nz, w));
         a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
@@ -339,7 +342,7 @@ struct Heat : Handle {
             a.m = dm32.as<float>(); a.cap = dcap.as<double>();
             for (int f = 0; f < 6; ++f) a.film[f] = dfilm32.as<float>() + film_off[f];
         }
-        a.quads = uniform && nx % 4 == 0 && cells_per_thread == 4 ? 1 : 0;
+        a.quads = uniform && nx % 4 == 0 && wide ? 1 : 0;
         const unsigned w = wave_of(a.quads ? kHeatF32Quad : kHeatF32);
         const int tx = a.quads ? nx / 4 : nx;  // the threads along a row
         a.tiles = make_tiles(tx, ny, nz, choose_zc(tx, ny, nz, w));
@@ -592,11 +595,13 @@ pm_status pm_heat_restore(pm_heat* hp) {
 pm_status pm_heat_set_cells_per_thread(pm_heat* hp, int cells) {
     Heat* h = reinterpret_cast<Heat*>(hp);
     HEAT_GUARD(h);
-    if (cells != 1 && cells != 4) return fail(PM_BAD_ARG, "cells per thread: 1 or 4");
-    if (cells != h->cells_per_thread) {
+    const int width = h->precision == PM_PLAIN_F64 ? 2 : 4;
+    if (cells != 1 && cells != width)
+        return fail(PM_BAD_ARG, width == 2 ? "cells per thread (plain f64): 1 or 2" : "cells per thread (FP32): 1 or 4");
+    if ((cells != 1) != h->wide) {
         PM_CUDA(cudaStreamSynchronize(h->stream()));
         h->drop_graphs();  // the captured launches hold the old tiling
-        h->cells_per_thread = cells;
+        h->wide = cells != 1;
     }
     return PM_OK;
 }

@@ -75,6 +75,7 @@ struct HeatPlainArgs {
     int nx, ny, nz;
     double dts, dx, reference;
     HeatFilms films;
+    int pairs;  // uniform blocks with rows of an even number of cells: heat_plain_pair_step
     Tiles tiles;
     DevState* st;
     double* partials;
@@ -124,6 +125,23 @@ __device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i,
     k1 = min(T.nz, k0 + T.zc);
 }
 
+// The books of a plain step, after its cells: the blocks' partials reduced in fixed order by the
+// last block to finish, then the ledger and the audit.
+__device__ __forceinline__ void heat_plain_books(const HeatPlainArgs& a, double (&acc)[2]) {
+    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+        DevState* st = a.st;
+        st->lost += acc[1];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, acc[0]);
+        ledger_add(total, scale, st->lost);
+        ledger_add(total, scale, -st->supplied);
+        st->part[0] = acc[0];
+        st->part[1] = st->lost;
+        st->part[2] = -st->supplied;
+        audit_and_commit(st, total, scale);
+    }
+}
+
 // Plain form. Each thread marches its column through the tile's planes, holding the cell
 // below, the cell and the cell above in registers.
 static __global__ void __launch_bounds__(256) heat_plain_step(HeatPlainArgs a) {
@@ -171,18 +189,69 @@ static __global__ void __launch_bounds__(256) heat_plain_step(HeatPlainArgs a) {
             here = above;
         }
     }
-    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
-        DevState* st = a.st;
-        st->lost += acc[1];
-        double total = 0.0, scale = 0.0;
-        ledger_add(total, scale, acc[0]);
-        ledger_add(total, scale, st->lost);
-        ledger_add(total, scale, -st->supplied);
-        st->part[0] = acc[0];
-        st->part[1] = st->lost;
-        st->part[2] = -st->supplied;
-        audit_and_commit(st, total, scale);
+    heat_plain_books(a, acc);
+}
+
+// The plain form of a uniform block with two adjacent cells of a row per thread (rows of an even
+// number of cells, so every pair starts on 16 bytes): per plane one 16-byte load each for the
+// plane above and the rows either side, two scalar loads for the cells left and right of the
+// pair, one 16-byte store. Each cell's arithmetic is heat_plain_step's uniform path, expression
+// for expression (the reference's operand order, no contraction in the plain unit), so the fields
+// agree with it, and with the reference, bit for bit; only the order of the FP64 sums within a
+// block differs.
+// Four blocks of 256 per SM (64 registers, a few bytes spilled) ran 164.8 Gcell/s on a 256³ block,
+// against 143.0 at three (80 registers) and 114.4 at two (98 registers, the compiler's own choice).
+#ifndef PM_HEAT_PAIR_MIN_BLOCKS
+#define PM_HEAT_PAIR_MIN_BLOCKS 4
+#endif
+static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_step(HeatPlainArgs a) {
+    if (a.st->violated) return;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t plane = (size_t)nx * ny;
+    const double2 zero = make_double2(0.0, 0.0);
+    const double kf = a.kface;
+    double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
+        int q, j, k0, k1;
+        tile_column(a.tiles, t, q, j, k0, k1);  // q: the pair's place along the row
+        const int i = 2 * q;
+        if (i >= nx || j >= ny) continue;
+        const size_t c0 = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+        const double* p = a.told + c0;
+        double* o = a.tnew + c0;
+        const bool xl = i > 0, xh = i + 2 < nx, yl = j > 0, yh = j + 1 < ny;
+        double2 below = k0 > 0 ? *reinterpret_cast<const double2*>(p - plane) : zero;
+        double2 here = *reinterpret_cast<const double2*>(p);
+        size_t c = c0;
+        for (int k = k0; k < k1; ++k, p += plane, o += plane, c += plane) {
+            const double2 above = k + 1 < nz ? *reinterpret_cast<const double2*>(p + plane) : zero;
+            const double2 ym = yl ? *reinterpret_cast<const double2*>(p - nx) : zero;
+            const double2 yp = yh ? *reinterpret_cast<const double2*>(p + nx) : zero;
+            const double xm = xl ? p[-1] : 0.0, xp = xh ? p[2] : 0.0;
+            const double hv[2] = {here.x, here.y}, bv[2] = {below.x, below.y}, av[2] = {above.x, above.y};
+            const double mv[2] = {ym.x, ym.y}, pv[2] = {yp.x, yp.y};
+            double nt[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const double t0 = hv[e];
+                double flux = 0.0;
+                if (e > 0 || xl) flux += kf * ((e == 0 ? xm : hv[0]) - t0);
+                if (e < 1 || xh) flux += kf * ((e == 1 ? xp : hv[1]) - t0);
+                if (yl) flux += kf * (mv[e] - t0);
+                if (yh) flux += kf * (pv[e] - t0);
+                if (k > 0) flux += kf * (bv[e] - t0);
+                if (k + 1 < nz) flux += kf * (av[e] - t0);
+                const double shed = a.films.exposed ? film_flux(a, i + e, j, k, c + e, t0) : 0.0;
+                nt[e] = t0 + a.dts * a.mobility * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
+                acc[0] += a.capacity * (nt[e] - a.reference);     // solid.rs:1583-1590
+                if (shed != 0.0) acc[1] += a.dts * a.mobility * shed * a.capacity;  // solid.rs:1821-1823
+            }
+            *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);
+            below = here;
+            here = above;
+        }
     }
+    heat_plain_books(a, acc);
 }
 
 struct HeatF32Args {

@@ -7,7 +7,8 @@
 namespace pm {
 
 cudaError_t launch_heat_plain(const HeatPlainArgs& a, cudaStream_t s) {
-    heat_plain_step<<<a.nblocks, tile_block(), 0, s>>>(a);
+    if (a.pairs) heat_plain_pair_step<<<a.nblocks, tile_block(), 0, s>>>(a);
+    else heat_plain_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -143,6 +144,7 @@ int occupancy_f64(KernelId id) {
     cudaError_t e = cudaSuccess;
     switch (id) {
         case kHeatPlain: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_step, 256, 0); break;
+        case kHeatPlainPair: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_step, 256, 0); break;
         case kHallF64:
             cudaFuncSetAttribute(hall_step<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<double, false>, 256, hall_smem_bytes<double>());

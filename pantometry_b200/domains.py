@@ -122,8 +122,9 @@ class Solid3D(_Domain):
         return self
 
     def set_cells_per_thread(self, cells):
-        """Cells of a row per thread in the FP32 form: 4 (the default, where the block is one
-        material and its rows hold a multiple of 4 cells) or 1; the fields agree bit for bit."""
+        """Cells of a row per thread: 1, or the precision's wide form (the default where the block
+        is one material and its rows allow): 2 for plain f64, 4 for FP32. The fields agree bit for
+        bit."""
         N.check(self._lib.pm_heat_set_cells_per_thread(self._h, int(cells)))
 
     def fill(self, mask, density, conductivity, specific_heat, emissivity=0.0, thermal=True):

@@ -1,10 +1,11 @@
-"""The FP32 `Solid3D` step with four adjacent cells of a row per thread (heat_f32_quad_step, taken
-by blocks of one material whose rows hold a multiple of 4 cells) against one cell per thread
-(heat_f32_step) on the same block. Both do `Solid3D::step`'s arithmetic in f32
-(crates/pantometry-thermal/src/solid.rs:1773-1826) in the same order and roundings, so the fields
-agree bit for bit under insulated faces, Dirichlet films (h = +inf) and films of finite h on some
-faces; the books, summed in another order, agree to 1e-12 of the ledger's scale. Both stay within
-the oracle's FP32 bounds, audited every step.
+"""The wide `Solid3D` steps against one cell per thread on the same block: four adjacent cells of a
+row per thread in the FP32 form (heat_f32_quad_step, rows of a multiple of 4 cells) and two in the
+plain f64 form (heat_plain_pair_step, even rows), both for blocks of one material. Each does
+`Solid3D::step`'s arithmetic (crates/pantometry-thermal/src/solid.rs:1773-1826) in the same order and
+roundings as the one-cell kernel, so the fields agree bit for bit under insulated faces, Dirichlet
+films (h = +inf) and films of finite h on some faces; the books, summed in another order, agree to
+1e-12 of the ledger's scale. The plain form is also bit for bit with the oracle, the FP32 form
+within its bounds, both audited every step.
 """
 import numpy as np
 import pytest
@@ -27,31 +28,42 @@ def films_of(kind, counts, dx):
             (4, 310.0, 500.0, areas[4])]
 
 
-@pytest.mark.parametrize("counts", [(4, 3, 5), (8, 8, 8), (64, 20, 17), (100, 9, 33)])
+@pytest.mark.parametrize("counts", [(4, 3, 5), (8, 8, 8), (64, 20, 17), (100, 9, 33), (6, 7, 4)])
 @pytest.mark.parametrize("kind", ["insulated", "dirichlet", "finite"])
-def test_quads_and_single_cells_agree(counts, kind):
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_wide_and_single_cells_agree(counts, kind, precision):
     dx = 1e-3
     cells = 300.0 + 30.0 * np.random.default_rng(sum(counts)).random(int(np.prod(counts)))
     films = films_of(kind, counts, dx)
     runs = []
-    for per_thread in (4, 1):
-        o, g = heat_pair(counts, dx, ALUMINIUM, 300.0, films, cells, precision="f32")
+    for per_thread in (4 if precision == "f32" else 2, 1):
+        o, g = heat_pair(counts, dx, ALUMINIUM, 300.0, films, cells, precision=precision)
         g.set_cells_per_thread(per_thread)
-        g.set_tolerance(1e-6)
+        g.set_tolerance(1e-6 if precision == "f32" else 1e-9)
         dt = 0.9 * g.max_stable_dt()
         assert g.step(dt, 70) is None  # a captured graph of 64, then six single launches
         runs.append((g.cells, g.ledger()))
     assert o.step(dt, 70) is None
-    (quad, lq), (single, ls) = runs
-    bad = np.flatnonzero(quad.view(np.uint64) != single.view(np.uint64))
+    (wide, lw), (single, ls) = runs
+    bad = np.flatnonzero(wide.view(np.uint64) != single.view(np.uint64))
     assert bad.size == 0, f"{bad.size} cells differ, first at {bad[0]}"
-    assert abs(lq["total"] - ls["total"]) <= 1e-12 * max(ls["scale"], 1e-300)
-    assert np.abs(quad - o.cells).max() < 1e-4  # kelvin, on a 30 K spread
+    assert abs(lw["total"] - ls["total"]) <= 1e-12 * max(ls["scale"], 1e-300)
+    if precision == "f64":  # the plain form is the reference's arithmetic: bit for bit with the oracle
+        assert np.array_equal(wide.view(np.uint64), o.cells.view(np.uint64))
+        lo = o.ledger()
+        assert abs(lw["total"] - lo["total"]) <= 1e-12 * max(lo["scale"], 1e-300)
+    else:
+        assert np.abs(wide - o.cells).max() < 1e-4  # kelvin, on a 30 K spread
 
 
-def test_cells_per_thread_is_one_or_four():
+def test_cells_per_thread_is_one_or_the_width():
     _, g = heat_pair((8, 4, 4), 1e-3, ALUMINIUM, 300.0, precision="f32")
     with pytest.raises(Exception):
         g.set_cells_per_thread(2)
     g.set_cells_per_thread(1)
     g.set_cells_per_thread(4)
+    _, g = heat_pair((8, 4, 4), 1e-3, ALUMINIUM, 300.0, precision="f64")
+    with pytest.raises(Exception):
+        g.set_cells_per_thread(4)
+    g.set_cells_per_thread(1)
+    g.set_cells_per_thread(2)
