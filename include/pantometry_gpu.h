@@ -389,9 +389,10 @@ pm_status pm_ensemble_ledgers(pm_ensemble* e, pm_ledger* out, int count);
 /* Brick shape with one cell per thread: x extent 16, 32 or 64 (y = 256 / x) and 8, 16, 32 or 64
  * planes. */
 pm_status pm_ensemble_set_shape(pm_ensemble* e, int brick_x, int planes);
-/* Any brick shape by its extents in cells: the one-cell shapes above, or (f32 only) the shapes
- * whose threads take four adjacent cells of a row each: 16 × 64, 32 × 32, 64 × 16 or 128 × 8,
- * with 32 or 64 planes. The fields agree bit for bit under every shape. */
+/* Any brick shape by its extents in cells: the one-cell shapes above; (f32 only) the shapes whose
+ * threads take four adjacent cells of a row each, 16 × 64, 32 × 32, 64 × 16 or 128 × 8; or (plain
+ * f64 only) two cells each, 16 × 32, 32 × 16 or 64 × 8; these with 32 or 64 planes. The fields
+ * agree bit for bit under every shape. */
 pm_status pm_ensemble_set_brick(pm_ensemble* e, int brick_x, int brick_y, int planes);
 pm_status pm_ensemble_shape(pm_ensemble* e, int* brick_x, int* brick_y, int* planes);
 /* Time `trial_steps` steps of every brick shape on the present state, keep the fastest, and put

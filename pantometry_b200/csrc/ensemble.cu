@@ -30,7 +30,8 @@ double ens_rust_max(double a, double b) {  // f64::max
 
 // The brick shapes the autotuner chooses among: log2 of the threads along x (256 threads, so
 // y = 256 >> bxs rows), the planes each thread marches, and the cells of its row each thread takes
-// (1, or 4 for the f32 quad shapes). Every shape has its own x and y extents in cells.
+// (1; 4 for the f32 quad shapes; 2 for the f64 pair shapes). Every shape has its own x and y
+// extents in cells.
 struct EnsShape {
     int bxs, zc, cells;
     int x() const { return cells << bxs; }
@@ -39,7 +40,12 @@ struct EnsShape {
 constexpr EnsShape kEnsShapes[] = {{5, 16, 1}, {5, 8, 1},  {5, 32, 1}, {5, 64, 1}, {4, 8, 1},  {4, 16, 1},
                                    {4, 32, 1}, {4, 64, 1}, {6, 8, 1},  {6, 16, 1}, {6, 32, 1}, {6, 64, 1},
                                    {2, 32, 4}, {2, 64, 4}, {3, 32, 4}, {3, 64, 4}, {4, 32, 4}, {4, 64, 4},
-                                   {5, 32, 4}, {5, 64, 4}};
+                                   {5, 32, 4}, {5, 64, 4}, {3, 32, 2}, {3, 64, 2}, {4, 32, 2}, {4, 64, 2},
+                                   {5, 32, 2}, {5, 64, 2}};
+// whether a shape runs at this precision: the quads are f32 only, the pairs f64 only
+inline bool ens_shape_fits(const EnsShape& s, int p) {
+    return s.cells == 1 || (s.cells == 4) == (p != PM_PLAIN_F64);
+}
 constexpr int kEnsShapeCount = sizeof(kEnsShapes) / sizeof(kEnsShapes[0]);
 
 // What `Solid3D::resolve` and `worst_rate_now` give for one uniform block with films on all six
@@ -154,13 +160,15 @@ struct Ensemble : Handle {
 
     size_t esize() const { return precision == PM_PLAIN_F64 ? sizeof(double) : sizeof(float); }
     unsigned wave() const {
-        return wave_of(precision == PM_PLAIN_F64 ? kEnsF64 : kEnsShapes[shape].cells == 4 ? kEnsF32Quad : kEnsF32);
+        const bool wide = kEnsShapes[shape].cells != 1;
+        return wave_of(precision == PM_PLAIN_F64 ? (wide ? kEnsF64Pair : kEnsF64) : (wide ? kEnsF32Quad : kEnsF32));
     }
 
     // Brick list and block table for a shape; uploads both.
     pm_status set_shape(int sh) {
         const EnsShape s = kEnsShapes[sh];
-        if (s.cells != 1 && precision == PM_PLAIN_F64) return fail(PM_BAD_ARG, "quad brick shapes are f32 only");
+        if (!ens_shape_fits(s, precision))
+            return fail(PM_BAD_ARG, s.cells == 4 ? "quad brick shapes are f32 only" : "pair brick shapes are f64 only");
         const int bx = s.x(), by = s.y();
         bricks.clear();
         for (size_t g = 0; g < grids.size(); ++g) {
@@ -218,7 +226,7 @@ struct Ensemble : Handle {
         a.nbricks = (unsigned)bricks.size();
         a.ngrids = (unsigned)grids.size();
         a.bxs = kEnsShapes[shape].bxs;
-        a.quads = kEnsShapes[shape].cells == 4 ? 1 : 0;
+        a.wide = kEnsShapes[shape].cells != 1 ? 1 : 0;
         a.states = dstates.as<DevState>();
         a.partials = bpartials.as<double>();
         return a;
@@ -324,7 +332,7 @@ pm_status pm_ensemble_create(const pm_ensemble_grid* grids, int count, int preci
         EnsGrid& q = e->grids[g];
         std::memset(&q, 0, sizeof(q));
         q.nx = d.nx; q.ny = d.ny; q.nz = d.nz;
-        q.pitch = precision == PM_PLAIN_F64 ? d.nx : (d.nx + 3) & ~3;
+        q.pitch = precision == PM_PLAIN_F64 ? (d.nx + 1) & ~1 : (d.nx + 3) & ~3;
         q.offset = offset;
         offset += (size_t)q.pitch * d.ny * d.nz;
         q.exposed = d.convection_w_per_m2_k != 0.0 ? 0x3f : 0;
@@ -384,7 +392,15 @@ pm_status pm_ensemble_upload(pm_ensemble* ep, const double* kelvin, size_t n) {
     if (!kelvin || n != e->cells) return fail(PM_BAD_ARG, "upload: one value per cell of every block, in block order");
     e->parity = 0;
     if (e->precision == PM_PLAIN_F64) {
-        PM_CUDA(cudaMemcpyAsync(e->field[0].p, kelvin, n * 8, cudaMemcpyHostToDevice, e->stream()));
+        // rows padded to an even length: the caller's dense blocks moved onto them, the padding zero
+        if (e->stage.bytes < n * 8) PM_CUDA(e->stage.alloc(n * 8));
+        PM_CUDA(cudaMemcpyAsync(e->stage.p, kelvin, n * 8, cudaMemcpyHostToDevice, e->stream()));
+        for (int par = 0; par < 2; ++par) PM_CUDA(cudaMemsetAsync(e->field[par].p, 0, e->dcells * 8, e->stream()));
+        for (size_t g = 0; g < e->grids.size(); ++g) {
+            const EnsGrid& q = e->grids[g];
+            PM_CUDA(launch_ens_relayout64(e->stage.as<double>() + e->ref_offset[g], e->field[0].as<double>() + q.offset,
+                                          nullptr, q.nx, q.ny, q.nz, q.pitch, 1, e->stream()));
+        }
     } else {
         if (e->stage.bytes < n * 8) PM_CUDA(e->stage.alloc(n * 8));
         PM_CUDA(cudaMemcpyAsync(e->stage.p, kelvin, n * 8, cudaMemcpyHostToDevice, e->stream()));
@@ -409,7 +425,14 @@ pm_status pm_ensemble_download(pm_ensemble* ep, double* kelvin, size_t n) {
     ENS_GUARD(e);
     if (!kelvin || n != e->cells) return fail(PM_BAD_ARG, "download: one value per cell of every block, in block order");
     if (e->precision == PM_PLAIN_F64) {
-        PM_CUDA(cudaMemcpyAsync(kelvin, e->field[e->parity].p, n * 8, cudaMemcpyDeviceToHost, e->stream()));
+        if (e->stage.bytes < n * 8) PM_CUDA(e->stage.alloc(n * 8));
+        for (size_t g = 0; g < e->grids.size(); ++g) {
+            const EnsGrid& q = e->grids[g];
+            PM_CUDA(launch_ens_relayout64(nullptr, e->field[e->parity].as<double>() + q.offset,
+                                          e->stage.as<double>() + e->ref_offset[g], q.nx, q.ny, q.nz, q.pitch, 0,
+                                          e->stream()));
+        }
+        PM_CUDA(cudaMemcpyAsync(kelvin, e->stage.p, n * 8, cudaMemcpyDeviceToHost, e->stream()));
     } else {
         if (e->stage.bytes < n * 8) PM_CUDA(e->stage.alloc(n * 8));
         for (size_t g = 0; g < e->grids.size(); ++g) {
@@ -544,7 +567,7 @@ pm_status pm_ensemble_autotune(pm_ensemble* ep, int trial_steps, int* brick_x, i
     float best_ms = std::numeric_limits<float>::infinity();
     pm_status result = PM_OK;
     for (int q = 0; q < kEnsShapeCount && result == PM_OK; ++q) {
-        if (kEnsShapes[q].cells != 1 && e->precision == PM_PLAIN_F64) continue;  // the quads are f32 only
+        if (!ens_shape_fits(kEnsShapes[q], e->precision)) continue;  // quads are f32 only, pairs f64 only
         if ((result = e->set_shape(q)) != PM_OK) break;
         cudaError_t ce = cudaSuccess;
         for (int w = 0; w < 2 && ce == cudaSuccess; ++w) { ce = e->launch(e->parity, false, e->stream()); e->parity ^= 1; }

@@ -4,8 +4,9 @@
 // crates/pantometry-thermal/src/solid.rs:1717-1901).
 //
 // Layout. The blocks' cells are concatenated in block order, each block in the reference's
-// index order i + pitch·(j + ny·k) (pitch = nx for f64; nx rounded up to 4 for f32, the padding
-// columns zero, so that TMA can tile each block). A brick is a bx × by × zc box of one block (bx·by = 256
+// index order i + pitch·(j + ny·k) (pitch = nx rounded up to 2 for f64 and to 4 for f32, the
+// padding columns zero, so that every pair or quad of a row starts on 16 bytes and TMA can tile
+// each f32 block). A brick is a bx × by × zc box of one block (bx·by = 256
 // threads, each marching one column of zc planes); the brick list holds every brick of every
 // block, block by block, and a persistent grid of thread blocks takes bricks blockIdx.x,
 // blockIdx.x + gridDim.x, ... in that fixed order. Brick shapes are chosen at run time (the
@@ -30,7 +31,7 @@ struct EnsGrid {
     int nx, ny, nz;
     unsigned nbricks;
     unsigned long long offset;  // first cell in the concatenated field
-    int pitch;                  // elements per row: nx (f64), nx rounded up to 4 (f32, for TMA)
+    int pitch;                  // elements per row: nx rounded up to 2 (f64) or 4 (f32)
     int pad0;
     unsigned first_brick;
     int exposed;                // film faces (bit f: XMin, XMax, YMin, YMax, ZMin, ZMax)
@@ -60,7 +61,7 @@ struct EnsArgs {
     unsigned nbricks;
     unsigned ngrids;
     int bxs;             // log2 of the threads along the brick's x extent (2 to 6)
-    int quads;           // f32 only: each thread takes four adjacent cells of its row
+    int wide;            // each thread takes adjacent cells of its row: four (f32) or two (f64)
     DevState* states;    // one per block: its books, ledger and audit
     double* partials;    // two per brick
 };
@@ -251,23 +252,95 @@ __device__ __forceinline__ void ens_brick_quad(const EnsArgs<float>& a, const En
     acc[1] += col_shed;
 }
 
+// Two adjacent cells of a row per thread (the f64 pair shapes): ens_brick's f64 arithmetic for each
+// cell, expression for expression (the reference's operand order, compiled without contraction),
+// with 16-byte loads of the pair, the plane above and the rows either side and one 16-byte store,
+// so the fields agree with the one-cell shapes, and with the reference, bit for bit. Rows are
+// padded to an even length; a pair's second cell past the block's last column (the padding) is
+// neither used as a neighbour nor written nor summed.
+template <bool MEASURE>
+__device__ __forceinline__ void ens_brick_pair(const EnsArgs<double>& a, const EnsGrid& g, const EnsBrick& br,
+                                               double (&acc)[2]) {
+    const int tid = threadIdx.x;
+    const int i = br.x0 + 2 * (tid & ((1 << a.bxs) - 1));
+    const int j = br.y0 + (tid >> a.bxs);
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const int pitch = g.pitch;
+    const size_t plane = (size_t)pitch * ny;
+    const int k0 = br.z0, k1 = br.z1;
+    const double* p = a.old + g.offset + ((size_t)i + (size_t)pitch * ((size_t)j + (size_t)ny * k0));
+    double* o = a.nu + (p - a.old);
+    const bool two = i + 1 < nx;  // the pair's second cell is in the block
+    if (MEASURE) {
+        for (int k = k0; k < k1; ++k, p += plane) {
+            const double2 v = *reinterpret_cast<const double2*>(p);
+            acc[0] += g.capacity * (v.x - g.reference);  // solid.rs:1583-1590
+            if (two) acc[0] += g.capacity * (v.y - g.reference);
+        }
+        return;
+    }
+    const double2 zero = make_double2(0.0, 0.0);
+    const double kf = g.kface;
+    const bool xl = i > 0, xh = i + 2 < nx, yl = j > 0, yh = j + 1 < ny;
+    double2 below = k0 > 0 ? *reinterpret_cast<const double2*>(p - plane) : zero;
+    double2 here = *reinterpret_cast<const double2*>(p);
+    for (int k = k0; k < k1; ++k, p += plane, o += plane) {
+        const double2 above = k + 1 < nz ? *reinterpret_cast<const double2*>(p + plane) : zero;
+        const double2 ym = yl ? *reinterpret_cast<const double2*>(p - pitch) : zero;
+        const double2 yp = yh ? *reinterpret_cast<const double2*>(p + pitch) : zero;
+        const double xm = xl ? p[-1] : 0.0, xp = xh ? p[2] : 0.0;
+        const double hv[2] = {here.x, here.y}, bv[2] = {below.x, below.y}, av[2] = {above.x, above.y};
+        const double mv[2] = {ym.x, ym.y}, pv[2] = {yp.x, yp.y};
+        double nt[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const double t0 = hv[e];
+            double flux = 0.0;  // heat_plain_step's uniform path: the reference's order of the six face terms
+            if (e > 0 || xl) flux += kf * ((e == 0 ? xm : hv[0]) - t0);
+            if (e == 0 ? two : xh) flux += kf * ((e == 1 ? xp : hv[1]) - t0);
+            if (yl) flux += kf * (mv[e] - t0);
+            if (yh) flux += kf * (pv[e] - t0);
+            if (k > 0) flux += kf * (bv[e] - t0);
+            if (k + 1 < nz) flux += kf * (av[e] - t0);
+            const double shed = g.exposed ? ens_film_flux(g, i + e, j, k, t0) : 0.0;
+            nt[e] = t0 + g.dts * g.mobility * (flux - shed);  // add_kelvin (solid.rs:1620-1635)
+            if (e == 0 || two) {
+                acc[0] += g.capacity * (nt[e] - g.reference);
+                if (shed != 0.0) acc[1] += g.dts * g.mobility * shed * g.capacity;  // solid.rs:1821-1823
+            }
+        }
+        if (two) *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);
+        else o[0] = nt[0];
+        below = here;
+        here = above;
+    }
+}
+
 // A block whose audit failed keeps its state: its bricks copy old to new, so the ping-pong
 // parity stays the same for every block of the ensemble.
-template <typename Real, bool QUAD>
+template <typename Real, bool WIDE>
 __device__ __forceinline__ void ens_hold(const EnsArgs<Real>& a, const EnsGrid& g, const EnsBrick& br) {
+    constexpr int kWidth = WIDE ? (sizeof(Real) == 8 ? 2 : 4) : 1;
     const int tid = threadIdx.x;
-    const int i = br.x0 + (QUAD ? 4 : 1) * (tid & ((1 << a.bxs) - 1));
+    const int i = br.x0 + kWidth * (tid & ((1 << a.bxs) - 1));
     const int j = br.y0 + (tid >> a.bxs);
     if (i >= g.nx || j >= g.ny) return;
-    const int cells = QUAD ? min(4, g.nx - i) : 1;
+    const int cells = min(kWidth, g.nx - i);
     const size_t plane = (size_t)g.pitch * g.ny;
     size_t c = g.offset + (size_t)i + (size_t)g.pitch * ((size_t)j + (size_t)g.ny * br.z0);
     for (int k = br.z0; k < br.z1; ++k, c += plane)
         for (int e = 0; e < cells; ++e) a.nu[c + e] = a.old[c + e];
 }
 
-template <typename Real, bool MEASURE, bool QUAD = false>
-static __global__ void __launch_bounds__(256) ens_step(EnsArgs<Real> a) {
+// WIDE: four cells of a row per thread (f32) or two (f64, held to PM_ENS_PAIR_MIN_BLOCKS blocks per
+// SM: occupancy sets the speed of the f64 wide forms, as for heat_plain_pair_step).
+#ifndef PM_ENS_PAIR_MIN_BLOCKS
+#define PM_ENS_PAIR_MIN_BLOCKS 4
+#endif
+template <typename Real, bool MEASURE, bool WIDE = false>
+static __global__ void __launch_bounds__(256, (WIDE && sizeof(Real) == 8) ? PM_ENS_PAIR_MIN_BLOCKS : 1)
+    ens_step(EnsArgs<Real> a) {
     __shared__ double red[32 * 2];
     __shared__ int last;
     const int tid = threadIdx.x;
@@ -276,11 +349,12 @@ static __global__ void __launch_bounds__(256) ens_step(EnsArgs<Real> a) {
         const EnsGrid& g = a.grids[br.grid];
         DevState* st = a.states + br.grid;
         if (!MEASURE && st->violated) {  // block-uniform: every thread reads the same word
-            ens_hold<Real, QUAD>(a, g, br);
+            ens_hold<Real, WIDE>(a, g, br);
             continue;
         }
         double acc[2] = {0.0, 0.0};
-        if constexpr (QUAD) ens_brick_quad<MEASURE>(a, g, br, acc);
+        if constexpr (WIDE && sizeof(Real) == 4) ens_brick_quad<MEASURE>(a, g, br, acc);
+        else if constexpr (WIDE) ens_brick_pair<MEASURE>(a, g, br, acc);
         else ens_brick<Real, MEASURE>(a, g, br, acc);
         block_sum<2>(acc, red);
         if (tid == 0) {
@@ -320,6 +394,19 @@ static __global__ void __launch_bounds__(256) ens_step(EnsArgs<Real> a) {
                 audit_and_commit(st, total, scale);
             }
         }
+    }
+}
+
+// One f64 block between the caller's dense layout (x fastest, rows of nx) and the device's rows
+// of `pitch` (to_dev = 1; the padding zeroed by the caller), and back.
+static __global__ void ens_relayout64(const double* __restrict__ dense, double* __restrict__ padded,
+                                      double* __restrict__ out, int nx, int ny, int nz, int pitch, int to_dev) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = r % (size_t)nx, rest = r / (size_t)nx;
+        const size_t q = i + (size_t)pitch * rest;  // rest = j + ny·k
+        if (to_dev) padded[q] = dense[r];
+        else out[r] = padded[q];
     }
 }
 

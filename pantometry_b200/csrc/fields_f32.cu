@@ -93,7 +93,7 @@ cudaError_t launch_to_f64(const float* src, double* dst, size_t n, cudaStream_t 
 
 template <>
 cudaError_t launch_ens<float>(const EnsArgs<float>& a, bool measure, unsigned nblocks, cudaStream_t s) {
-    if (a.quads) {
+    if (a.wide) {
         if (measure) ens_step<float, true, true><<<nblocks, 256, 0, s>>>(a);
         else ens_step<float, false, true><<<nblocks, 256, 0, s>>>(a);
     } else {

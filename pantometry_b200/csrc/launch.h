@@ -47,7 +47,7 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
 // Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -95,6 +95,9 @@ cudaError_t launch_ens_tma(const EnsTmaArgs& t, unsigned nblocks, cudaStream_t s
 // One block between kelvin on the host's layout and f32 deviations on padded rows.
 cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, int nx, int ny, int nz, int pitch,
                                 double t0, int to_dev, cudaStream_t s);
+// One f64 block between the caller's dense layout and the device's rows of `pitch`.
+cudaError_t launch_ens_relayout64(const double* dense, double* padded, double* out, int nx, int ny, int nz, int pitch,
+                                  int to_dev, cudaStream_t s);
 // One ensemble step (measure = false) or the opening ledgers (measure = true) over the brick list.
 template <typename Real> cudaError_t launch_ens(const EnsArgs<Real>& a, bool measure, unsigned nblocks, cudaStream_t s);
 

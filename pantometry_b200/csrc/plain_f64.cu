@@ -90,8 +90,13 @@ cudaError_t launch_yee_measure<double>(const YeeHArgs<double>& a, double* out2, 
 }
 template <>
 cudaError_t launch_ens<double>(const EnsArgs<double>& a, bool measure, unsigned nblocks, cudaStream_t s) {
-    if (measure) ens_step<double, true><<<nblocks, 256, 0, s>>>(a);
-    else ens_step<double, false><<<nblocks, 256, 0, s>>>(a);
+    if (a.wide) {
+        if (measure) ens_step<double, true, true><<<nblocks, 256, 0, s>>>(a);
+        else ens_step<double, false, true><<<nblocks, 256, 0, s>>>(a);
+    } else {
+        if (measure) ens_step<double, true><<<nblocks, 256, 0, s>>>(a);
+        else ens_step<double, false><<<nblocks, 256, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -156,12 +161,19 @@ int occupancy_f64(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double, false, true>, 256, yee_smem_bytes<double>());
             break;
         case kEnsF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false>, 256, 0); break;
+        case kEnsF64Pair: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false, true>, 256, 0); break;
         case kRoomF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<double>, 256, 0); break;
         case kTubeF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tube_step<double>, 256, 0); break;
         case kBarF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bar_step<double>, 256, 0); break;
         default: return -1;
     }
     return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+cudaError_t launch_ens_relayout64(const double* dense, double* padded, double* out, int nx, int ny, int nz, int pitch,
+                                  int to_dev, cudaStream_t s) {
+    ens_relayout64<<<kMeasureBlocks, 256, 0, s>>>(dense, padded, out, nx, ny, nz, pitch, to_dev);
+    return cudaGetLastError();
 }
 
 }  // namespace pm

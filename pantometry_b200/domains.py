@@ -537,7 +537,8 @@ class Ensemble:
 
     def set_shape(self, brick_x, planes, brick_y=None):
         """The brick shape: x extent and planes (one cell per thread, y = 256 / x), or with
-        `brick_y` any listed shape, the f32 quad shapes (16 × 64, 32 × 32, 64 × 16, 128 × 8) among them."""
+        `brick_y` any listed shape, among them the f32 quad shapes (16 × 64, 32 × 32, 64 × 16,
+        128 × 8) and the f64 pair shapes (16 × 32, 32 × 16, 64 × 8)."""
         if brick_y is None:
             N.check(self._lib.pm_ensemble_set_shape(self._h, int(brick_x), int(planes)))
         else:

@@ -80,13 +80,14 @@ def test_ensemble_f64_is_bit_exact_per_block_under_every_shape():
         want.append(o.cells)
         books.append(o.ledger())
     e = Ensemble(grids, precision="f64")
-    for bx, planes in ((32, 16), (16, 8), (64, 64), (32, 8)):
-        e.set_shape(bx, planes)
+    # one cell per thread (x, planes), then the pair shapes (x, planes, y)
+    for shape in ((32, 16), (16, 8), (64, 64), (32, 8), (16, 32, 32), (32, 64, 16), (64, 32, 8)):
+        e.set_shape(*shape)
         e.upload(np.concatenate(cells))
         assert e.step(STEPS) is None
         got = e.download()
         for g in range(len(grids)):
-            assert np.array_equal(e.block(got, g).view(np.uint64), want[g].view(np.uint64)), (bx, planes, g)
+            assert np.array_equal(e.block(got, g).view(np.uint64), want[g].view(np.uint64)), (shape, g)
         for led, o in zip(e.ledgers(), books):
             assert abs(led["total"] - o["total"]) <= 1e-12 * max(o["scale"], 1e-300), (led, o)
             assert abs(led["parts"][1] - o["lost"]) <= 1e-12 * max(o["scale"], 1e-300)
@@ -210,7 +211,7 @@ def test_ensemble_f32_tma_interior_and_face_bricks_agree():
 
 
 @pytest.mark.gpu
-def test_ensemble_quad_shapes_are_f32_only():
+def test_ensemble_quads_are_f32_only_and_pairs_f64_only():
     from pantometry_b200.domains import Ensemble
 
     grids, cells = small_grids(count=2)
@@ -219,3 +220,8 @@ def test_ensemble_quad_shapes_are_f32_only():
         e.set_shape(32, 32, 32)
     e.set_shape(32, 32, 8)  # the one-cell 32 × 8 shape by its extents
     assert e.shape() == (32, 8, 32)
+    e.set_shape(32, 64, 16)
+    assert e.shape() == (32, 16, 64)
+    f = Ensemble(grids, precision="f32")
+    with pytest.raises(Exception):
+        f.set_shape(32, 64, 16)
