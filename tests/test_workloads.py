@@ -21,3 +21,15 @@ def test_workload_shapes():
     assert h["pressure"].shape == (16 ** 3,) and np.abs(h["pressure"]).max() <= 1e-3
     e = W.heat_ensemble(8)
     assert all(16 <= n <= 128 for g in e["grids"] for n in g["counts"])
+
+
+def test_heat_block_baseline_holds_its_audit():
+    """Config 1's CPU baseline leg (bench.py --workload heat): the oracle's audited
+    `Simulation::advance` over the heat block at 0.9 of its limit keeps the books at 1e-9, and the
+    record carries the keys of a bench line's cpu_baseline."""
+    import bench
+
+    cfg = W.heat_block(16, steps=20)
+    out = bench.cpu_baseline_heat(cfg, 20)  # asserts the audit held on every step
+    assert out["value"] > 0.0 and out["cores"] == 1 and out["kind"] == "port"
+    assert out["unit"] == bench.UNIT and "20 audited" in out["sample"]
