@@ -144,7 +144,11 @@ __device__ __forceinline__ void heat_plain_books(const HeatPlainArgs& a, double 
 
 // Plain form. Each thread marches its column through the tile's planes, holding the cell
 // below, the cell and the cell above in registers.
-static __global__ void __launch_bounds__(256) heat_plain_step(HeatPlainArgs a) {
+// Held to four blocks of 256 per SM (64 registers, no spill; 90 and two blocks unbounded).
+#ifndef PM_HEAT_PLAIN_MIN_BLOCKS
+#define PM_HEAT_PLAIN_MIN_BLOCKS 4
+#endif
+static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_plain_step(HeatPlainArgs a) {
     if (a.st->violated) return;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
