@@ -443,6 +443,7 @@ def run_ensemble(args):
     achieved = 8 * local_cells / (per_launch_ms * 1e-3) / 1e9
     value = total_cells * T * args.steps / (ms32 * 1e-3) / 1e9
     plain = total_cells * T * plain_steps / (ms64 * 1e-3) / 1e9
+    tma = tuple(shape32[:2]) == (32, 8)  # the 32 × 8 bricks run the TMA-staged kernel
     line = {
         "metric": ENS_METRIC,
         "value": round(value, 3),
@@ -468,9 +469,10 @@ def run_ensemble(args):
         "gpu_launches": args.steps * T,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
-                     "traffic": round(ENS_F32_TRAFFIC_PER_CELL * local_cells) if shape32[0] == 32 else None,
+                     "traffic": round(ENS_F32_TRAFFIC_PER_CELL * local_cells) if tma else None,
                      "traffic_source": "ncu capture of the 512-grid ensemble, per cell",
-                     "kernel": "ens_tma_step (FP32, TMA-staged)" if shape32[0] == 32 else "ens_step<float>",
+                     "kernel": "ens_tma_step (FP32, TMA-staged)" if tma else
+                               "ens_step<float> (four cells per thread)" if shape32[0] * shape32[1] == 1024 else "ens_step<float>",
                      "bytes_per_launch": 8 * local_cells, "peak_source": f"{peak_kind} hbm_gbs"},
         "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
                       "roofline_frac": round(16 * local_cells / (ms64 / (plain_steps * T) * 1e-3) / 1e9 / peak, 4),

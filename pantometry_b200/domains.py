@@ -550,10 +550,11 @@ class Ensemble:
         return bx.value, by.value, zc.value
 
     def autotune(self, trial_steps=10):
-        """Time every brick shape on the present state, keep the fastest; the state is put back."""
+        """Time every brick shape on the present state, keep the fastest; the state is put back.
+        Returns the chosen shape as `shape()` gives it: (x, y, planes) in cells."""
         bx, zc = C.c_int(), C.c_int()
         N.check(self._lib.pm_ensemble_autotune(self._h, int(trial_steps), C.byref(bx), C.byref(zc)))
-        return bx.value, zc.value
+        return self.shape()
 
 
 def device_count():
