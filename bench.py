@@ -1118,6 +1118,72 @@ def cpu_baseline_ensemble(cfg, grids, sample_steps=2, threads=1, sample_grids=16
                       f"(after 1 warm-up step), {threads} thread(s), {secs:.2f} s"}
 
 
+def run_reference_heat(args):
+    """The reference's CPU path for the heat block (the oracle's restatement of `Simulation::advance`
+    over `Solid3D::step` and its ledger, audited at 1e-9), on every usable host core: one
+    independent copy of the block per thread (the reference's `Ensemble` pattern), each bench step
+    a sample of `sample_steps` audited steps of every copy."""
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    import oracle
+    from pantometry_b200 import workloads as W
+
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    n, T = args.n, args.timesteps
+    cfg = W.heat_block(n, steps=T)
+    cells = n ** 3
+    copies = max(1, min(ncpu, int(8e9 // (16 * cells))))  # at most 8 GB of host state
+    sample_steps = min(T, 100 if n <= 64 else args.cpu_sample_steps)
+    s = cfg["substance"]
+    blocks = []
+    for _ in range(copies):
+        o = oracle.Heat(cfg["counts"], cfg["dx"], s["density"], s["conductivity"], s["specific_heat"],
+                        cfg["initial"], emissivity=s["emissivity"])
+        for f, amb, h, area in cfg["films"]:
+            o.losing_from(f, amb, h, area)
+        o.cells = cfg["cells"]
+        blocks.append(o)
+    dt = cfg["dt_fraction"] * blocks[0].max_stable_dt()
+
+    def sample(steps):
+        refused = []
+
+        def work(o):
+            v = o.advance(dt, steps, tol=1e-9)
+            if v is not None:
+                refused.append(v)
+
+        ths = [threading.Thread(target=work, args=(o,)) for o in blocks]
+        t0 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        secs = time.perf_counter() - t0
+        assert not refused, refused[0]
+        return copies * cells * steps / secs / 1e9, secs
+
+    sample(1)  # warm-up
+    runs = [sample(sample_steps) for _ in range(args.steps)]
+    value = statistics.median(r[0] for r in runs)
+    line = {
+        "metric": HEAT_METRIC.replace("64^3", f"{n}^3"), "value": round(value, 6), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (300 K block, 50 K Gaussian hot spot, sigma 8 cells, seed-jittered centre)",
+        "impl": "reference",
+        "config": {"workload": f"heat_block {n}^3 cells, Dirichlet 300 K faces, dt 0.9 x the limit, audited "
+                               "Simulation::advance steps", "cells": cells, "copies": copies},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": copies, "kind": "port",
+                         "sample": f"{copies} independent copies of the {n}^3 block, one per thread, "
+                                   f"{sample_steps} audited steps each per bench step (median of {args.steps}, "
+                                   f"{runs[0][1]:.2f} s for the first); the Rust reference cannot be built here "
+                                   "(no cargo), so this is the oracle's C++ restatement of its loops"},
+        "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_ensemble(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -1180,9 +1246,7 @@ def main():
         return
     if args.workload == "heat":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "workload": "heat",
-                              "unavailable": "the reference arm times the headline hall and the ensemble; "
-                                             "the heat block's CPU path is the cpu_baseline of this line"}))
+            run_reference_heat(args)
         else:
             run_heat(args)
         return

@@ -33,3 +33,22 @@ def test_heat_block_baseline_holds_its_audit():
     out = bench.cpu_baseline_heat(cfg, 20)  # asserts the audit held on every step
     assert out["value"] > 0.0 and out["cores"] == 1 and out["kind"] == "port"
     assert out["unit"] == bench.UNIT and "20 audited" in out["sample"]
+
+
+def test_heat_reference_arm_prints_its_line():
+    """`bench.py --workload heat --impl reference` runs the oracle's audited steps of the heat block
+    on the host cores and prints one line with the reference arm's keys."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--workload", "heat", "--impl", "reference",
+                          "--n", "16", "--timesteps", "10", "--steps", "1"],
+                         capture_output=True, text=True, timeout=300, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0.0 and line["dtype"] == "f64"
+    assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
