@@ -52,3 +52,14 @@ def test_heat_reference_arm_prints_its_line():
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_cavity_sample_holds_its_audit():
+    """The cavity's CPU baseline and reference arm (bench.py): the oracle's audited steps of the
+    vacuum cavity with its soft source, on independent copies, one per thread."""
+    import bench
+
+    rate, secs = bench.cavity_sample(16, 5, copies=2)  # asserts every step's audit held
+    assert rate > 0.0 and secs > 0.0
+    out = bench.cpu_baseline_cavity(16, 5)
+    assert out["cores"] == 1 and out["kind"] == "port" and out["value"] > 0.0
