@@ -924,38 +924,89 @@ class CavityBatch:
         self.cavs = []
 
 
-def cpu_baseline_mix(hall_cells, cav_cells, n_sample=128, sample_steps=32):
-    """The reference's CPU path (the oracle) on a bounded sample of the mixed workload: a hall of
-    `n_sample`³ nodes over the same 32³ speed blocks and one dielectric cavity of `n_sample`³
-    cells, `sample_steps` audited steps each on one core; the rate is the mix's: its cell-updates
-    over the time the per-cell costs give for its hall and cavity cells."""
+def mix_sample(hall_cells, cav_cells, n_sample=128, sample_steps=32, copies=1):
+    """The reference's CPU path (the oracle) on a bounded sample of the mixed workload: `copies`
+    independent pairs of an `n_sample`³ hall over the same 32³ speed blocks and an `n_sample`³
+    dielectric cavity, one pair per thread, `sample_steps` audited steps of every hall and then of
+    every cavity, each phase timed by the wall clock. Returns the mix's rate (its cell-updates over
+    the time the measured costs per cell give for its hall and cavity cells) and those costs."""
     import oracle
     from pantometry_b200 import workloads as W
 
     h = W.hetero_hall(n_sample, steps=sample_steps + 1)
-    w, ht, d = h["size"]
-    o = oracle.Hall(w, ht, d, h["across"], h["speed"], h["density"])
-    o.release(h["pressure"])
-    o.set_speed_blocks(h["block"], h["speeds"])
-    o.set_source(h["source_node"], h["wave"])
-    assert o.advance(h["dt"], 1) is None
-    t0 = time.perf_counter()
-    assert o.advance(h["dt"], sample_steps) is None
-    t_hall = (time.perf_counter() - t0) / (n_sample ** 3 * sample_steps)
-    del o
     c = W.dielectric_cavities(1, n_sample, steps=sample_steps + 1)
-    y = oracle.Yee(c["counts"], c["dx"])
-    y.set_cells(eps_r=c["cavities"][0]["eps"])
-    y.set_source(c["edge"], c["current"])
-    assert y.advance(c["dt"], 1) is None
-    t0 = time.perf_counter()
-    assert y.advance(c["dt"], sample_steps) is None
-    t_cav = (time.perf_counter() - t0) / (n_sample ** 3 * sample_steps)
+    w, ht, d = h["size"]
+    halls, cavs = [], []
+    for _ in range(copies):
+        o = oracle.Hall(w, ht, d, h["across"], h["speed"], h["density"])
+        o.release(h["pressure"])
+        o.set_speed_blocks(h["block"], h["speeds"])
+        o.set_source(h["source_node"], h["wave"])
+        assert o.advance(h["dt"], 1) is None
+        halls.append(o)
+        y = oracle.Yee(c["counts"], c["dx"])
+        y.set_cells(eps_r=c["cavities"][0]["eps"])
+        y.set_source(c["edge"], c["current"])
+        assert y.advance(c["dt"], 1) is None
+        cavs.append(y)
+
+    def phase(objs, dt):
+        refused = []
+
+        def work(o):
+            v = o.advance(dt, sample_steps)
+            if v is not None:
+                refused.append(v)
+
+        ths = [threading.Thread(target=work, args=(o,)) for o in objs]
+        t0 = time.perf_counter()
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        assert not refused, refused[0]
+        return (time.perf_counter() - t0) / (copies * n_sample ** 3 * sample_steps)
+
+    t_hall = phase(halls, h["dt"])
+    t_cav = phase(cavs, c["dt"])
     value = (hall_cells + cav_cells) / (t_hall * hall_cells + t_cav * cav_cells) / 1e9
+    return value, t_hall, t_cav
+
+
+def cpu_baseline_mix(hall_cells, cav_cells, n_sample=128, sample_steps=32):
+    value, t_hall, t_cav = mix_sample(hall_cells, cav_cells, n_sample, sample_steps)
     return {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{sample_steps} audited Simulation::advance steps of a {n_sample}^3 speed-block hall "
                       f"({t_hall * 1e9:.1f} ns per node-update) and of a {n_sample}^3 dielectric cavity "
                       f"({t_cav * 1e9:.1f} ns per cell-update), weighted by the mix's cells"}
+
+
+def run_reference_mix(args):
+    """The mix's reference arm: `mix_sample` on every usable host core (one hall and one cavity of
+    128³ per thread, at most 8 pairs), weighted by the mix's cells, the median of `steps` samples."""
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    copies = max(1, min(ncpu, 8))
+    hall_cells, cav_cells = args.n ** 3, args.grids * args.cavity_n ** 3
+    runs = [mix_sample(hall_cells, cav_cells, 128, 8, copies) for _ in range(args.steps)]
+    value = statistics.median(r[0] for r in runs)
+    line = {
+        "metric": MIX_METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded speed blocks, inclusions and noise; Ricker and dipole sources)", "impl": "reference",
+        "config": {"workload": f"{args.n}^3 speed-block hall + {args.grids} dielectric cavities of {args.cavity_n}^3, "
+                               "audited Simulation::advance steps", "copies": copies},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": copies, "kind": "port",
+                         "sample": f"{copies} independent pairs of a 128^3 speed-block hall and a 128^3 dielectric "
+                                   f"cavity, one pair per thread, 8 audited steps of each per bench step "
+                                   f"({runs[0][1] * 1e9:.1f} and {runs[0][2] * 1e9:.1f} ns of wall clock per "
+                                   "node- and cell-update), weighted by the mix's cells; the Rust reference cannot be "
+                                   "built here (no cargo), so this is the oracle's C++ restatement of its loops"},
+        "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_mix(args):
@@ -1308,9 +1359,7 @@ def main():
         args.cpu_sample_steps = 16 if args.workload == "hall" else 8
     if args.workload == "mix":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "workload": "mix",
-                              "unavailable": "the reference arm times the headline hall and the ensemble; "
-                                             "the mix's parts are timed per cell in the hall and cavity arms"}))
+            run_reference_mix(args)
         else:
             run_mix(args)
         return

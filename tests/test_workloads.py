@@ -63,3 +63,12 @@ def test_cavity_sample_holds_its_audit():
     assert rate > 0.0 and secs > 0.0
     out = bench.cpu_baseline_cavity(16, 5)
     assert out["cores"] == 1 and out["kind"] == "port" and out["value"] > 0.0
+
+
+def test_mix_sample_holds_its_audit():
+    """The mix's CPU baseline and reference arm (bench.py): the oracle's audited speed-block hall and
+    dielectric cavity, independent pairs one per thread, weighted by the mix's cells."""
+    import bench
+
+    value, t_hall, t_cav = bench.mix_sample(1024 ** 3, 64 * 128 ** 3, n_sample=16, sample_steps=3, copies=2)
+    assert value > 0.0 and t_hall > 0.0 and t_cav > 0.0
