@@ -37,16 +37,15 @@ METRIC = "Gcell-updates/s (acoustic hall 256^3, FP32 fields + FP64 audit)"
 UNIT = "Gcell-updates/s"
 BYTES_F32 = 32  # per node-update: p, vx, vy, vz, read and written once
 BYTES_F64 = 64
-# dram__bytes_read.sum + dram__bytes_write.sum of one hall_tma_step launch at 256³ (270.4 MB read
-# + 219.5 MB written), from the ncu capture summarised in profiles/hall_tma_step_f32_256.md.
+# DRAM traffic per launch, dram__bytes_read.sum + dram__bytes_write.sum, as one ncu capture of the
+# kernel measured it (ncu cannot run inside the timed process; the capture's command is the bench's
+# own, on one GPU). The hall kernel at 256³: 270.4 MB read + 219.5 MB written.
 HALL_F32_TRAFFIC = 489971968
-# dram__bytes_read.sum + dram__bytes_write.sum of one yee_tma_step launch at 256³ cells (432.4 MB
-# read + 366.6 MB written, profiles/yee_tma_step_f32_256.md), per cell; a launch at another size
-# moves that many bytes per cell (the kernel reads and writes each cell's six values once)
+# The Yee kernel, per cell: 432.4 MB read + 366.6 MB written at 256³ cells. A launch at another
+# size moves that many bytes per cell (it reads and writes each cell's six values once).
 YEE_F32_TRAFFIC_PER_CELL = (432385024 + 366586112) / 256 ** 3
-# dram__bytes_read.sum + dram__bytes_write.sum of one ens_tma_step launch over the 512-grid heat
-# ensemble (1.149 GB read + 785.9 MB written for 187,991,031 cells,
-# profiles/ens_tma_step_f32_ensemble512.md), per cell
+# The ensemble brick kernel over the 512-block heat ensemble, per cell: 1.149 GB read + 785.9 MB
+# written for 187,991,031 cells.
 ENS_F32_TRAFFIC_PER_CELL = (1149139000 + 785889024) / 187991031
 
 

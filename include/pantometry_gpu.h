@@ -2,7 +2,7 @@
  * pantometry_gpu.h — the C ABI of the B200-native stepping path.
  *
  * One library, libpantometry_b200.so, holds sm_100a CUDA kernels and a C++ host runtime for
- * three of pantometry's `Domain` implementations:
+ * six of pantometry's `Domain` implementations, and an ensemble of many `Solid3D` blocks:
  *
  *   pm_heat    ~ Solid3D  (crates/pantometry-thermal/src/solid.rs)
  *   pm_hall    ~ Hall     (crates/pantometry-acoustic/src/hall.rs)
@@ -45,7 +45,9 @@ typedef enum pm_status {
     PM_NO_DEVICE = 1,      /* no CUDA device, or the library's kernels cannot run on it */
     PM_UNSUPPORTED = 2,    /* a feature the kernels do not implement (e.g. phase change) */
     PM_VIOLATION = 3,      /* a step was refused or an audit failed; the pm_violation is filled */
-    PM_DEVICE_TIMEOUT = 4, /* reserved: a device-side wait gave up (no kernel here waits) */
+    PM_DEVICE_TIMEOUT = 4, /* a bounded wait inside a kernel ran out (the TMA-staged kernels wait on
+                            * their own copies); the call stopped, and the fields of the step that
+                            * gave up are incomplete: restore a checkpoint before going on */
     PM_BAD_ARG = 5,
     PM_CUDA_ERROR = 6,
     PM_OUT_OF_MEMORY = 7
@@ -414,8 +416,11 @@ void pm_ensemble_destroy(pm_ensemble* e);
  * cudaMalloc, no cudaFree, no allocating library call.
  *   Fields are in the reference's index order, nx*ny*nz nodes and (nx-1)*ny*nz, nx*(ny-1)*nz,
  *   nx*ny*(nz-1) faces, as `Hall` lays them out (hall.rs:67-77); the old state is read from
- *   p0/vx0/vy0/vz0 and the new one written to p1/vx1/vy1/vz1 (distinct buffers). first_step != 0
- *   gives the velocities the half step the leapfrog opens with (hall.rs:427-430). *invariant
+ *   p0/vx0/vy0/vz0 and the new one written to p1/vx1/vy1/vz1; an output that is also an input or
+ *   another output is refused with PM_BAD_ARG. first_step != 0 gives the velocities the half step
+ *   the leapfrog opens with (hall.rs:427-430). dt must be positive: pm_hall_step, like
+ *   `Hall::step` (hall.rs:421-423), treats a non-positive dt as a step that changes nothing, but
+ *   this entry point has no state of its own to leave unchanged and returns PM_BAD_ARG. *invariant
  *   receives `invariant_si` of the new state (hall.rs:334-384); the startup offset and the audit
  *   stay with the caller.
  *   The first call on a device looks up the scratch array's device address (cudaGetSymbolAddress,

@@ -20,17 +20,8 @@ cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s) {
 
 template <>
 cudaError_t launch_hall<float>(const HallArgs<float>& a, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
-        cudaFuncSetAttribute(hall_step<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
-        attr = true;
-    }
-    if (a.block_scale)
-        hall_step<float, true><<<a.nblocks, tile_block(), hall_smem_bytes<float>(), s>>>(a);
-    else
-        hall_step<float, false><<<a.nblocks, tile_block(), hall_smem_bytes<float>(), s>>>(a);
-    return cudaGetLastError();
+    const int smem = (int)hall_smem_bytes<float>();
+    return launch_smem(a.block_scale ? hall_step<float, true> : hall_step<float, false>, a.nblocks, tile_block(), smem, s, a);
 }
 template <>
 cudaError_t launch_hall_measure<float>(const HallMeasureArgs<float>& a, cudaStream_t s) {
@@ -49,23 +40,10 @@ cudaError_t launch_yee_e<float>(const YeeEArgs<float>& a, cudaStream_t s) {
 }
 template <>
 cudaError_t launch_yee_step<float>(const YeeStepArgs<float>& a, cudaStream_t s) {
-    static bool attr = false;
     const int smem = (int)yee_smem_bytes<float>();
-    if (!attr) {
-        cudaFuncSetAttribute(yee_step<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_step<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_step<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_step<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
-    if (a.uniform) {
-        if (a.solid) yee_step<float, true, true><<<a.nblocks, tile_block(), smem, s>>>(a);
-        else yee_step<float, true, false><<<a.nblocks, tile_block(), smem, s>>>(a);
-    } else {
-        if (a.solid) yee_step<float, false, true><<<a.nblocks, tile_block(), smem, s>>>(a);
-        else yee_step<float, false, false><<<a.nblocks, tile_block(), smem, s>>>(a);
-    }
-    return cudaGetLastError();
+    auto k = a.uniform ? (a.solid ? yee_step<float, true, true> : yee_step<float, true, false>)
+                       : (a.solid ? yee_step<float, false, true> : yee_step<float, false, false>);
+    return launch_smem(k, a.nblocks, tile_block(), smem, s, a);
 }
 template <>
 cudaError_t launch_yee_measure<float>(const YeeHArgs<float>& a, double* out2, cudaStream_t s) {
@@ -105,30 +83,23 @@ cudaError_t launch_ens<float>(const EnsArgs<float>& a, bool measure, unsigned nb
 
 cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s) {
     constexpr int P = kHallTmaPlanes, S = kHallTmaStages;
-    static bool attr = false;
     const int smem = (int)hall_tma_smem_bytes();
-    if (!attr) {
-        cudaFuncSetAttribute(hall_tma_step<P, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(hall_tma_step<P, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
-    if (a.block_scale)
-        hall_tma_step<P, S, true><<<a.nblocks, tile_block(), smem, s>>>(a, m);
-    else
-        hall_tma_step<P, S, false><<<a.nblocks, tile_block(), smem, s>>>(a, m);
-    return cudaGetLastError();
+    return launch_smem(a.block_scale ? hall_tma_step<P, S, true> : hall_tma_step<P, S, false>, a.nblocks, tile_block(), smem,
+                       s, a, m);
 }
 
 bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+    // looked up once per process (the driver's entry point is the same for every device); a
+    // function-local static is initialised exactly once even when threads race to it
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         cudaDriverEntryPointQueryResult q;
         void* fn = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return false;
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
     const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
     const cuuint32_t box[3] = {bx, by, bz};
@@ -140,25 +111,11 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
 
 cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
     constexpr int S = kYeeTmaStages, PU = kYeeTmaPlanesUniform, PM = kYeeTmaPlanesMedia;
-    static bool attr = false;
     const bool media = !a.uniform;
     const int smem = (int)yee_tma_smem_bytes(media);
-    if (!attr) {
-        const int s0 = (int)yee_tma_smem_bytes(false), s1 = (int)yee_tma_smem_bytes(true);
-        cudaFuncSetAttribute(yee_tma_step<PU, S, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
-        cudaFuncSetAttribute(yee_tma_step<PU, S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s0);
-        cudaFuncSetAttribute(yee_tma_step<PM, S, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
-        cudaFuncSetAttribute(yee_tma_step<PM, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
-        attr = true;
-    }
-    if (a.solid) {
-        if (media) yee_tma_step<PM, S, true, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-        else yee_tma_step<PU, S, true, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-    } else {
-        if (media) yee_tma_step<PM, S, false, true><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-        else yee_tma_step<PU, S, false, false><<<a.nblocks, tile_block(), smem, s>>>(a, L, m);
-    }
-    return cudaGetLastError();
+    auto k = a.solid ? (media ? yee_tma_step<PM, S, true, true> : yee_tma_step<PU, S, true, false>)
+                     : (media ? yee_tma_step<PM, S, false, true> : yee_tma_step<PU, S, false, false>);
+    return launch_smem(k, a.nblocks, tile_block(), smem, s, a, L, m);
 }
 
 cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,
@@ -178,14 +135,8 @@ cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool d
 }
 
 cudaError_t launch_ens_tma(const EnsTmaArgs& t, unsigned nblocks, cudaStream_t s) {
-    static bool attr = false;
     const int smem = (int)ens_tma_smem_bytes();
-    if (!attr) {
-        cudaFuncSetAttribute(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
-    ens_tma_step<kEnsTmaPlanes, kEnsTmaStages><<<nblocks, kEnsConsumers + 32, smem, s>>>(t);
-    return cudaGetLastError();
+    return launch_smem(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, nblocks, kEnsConsumers + 32, smem, s, t);
 }
 
 cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, int nx, int ny, int nz, int pitch,
@@ -245,38 +196,40 @@ int occupancy_f32(KernelId id) {
         case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step<false>, 256, 0); break;
         case kHeatF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_step, 256, 0); break;
         case kHallF32:
-            cudaFuncSetAttribute(hall_step<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<float>());
+            e = allow_smem(hall_step<float, false>, (int)hall_smem_bytes<float>());
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<float, false>, 256, hall_smem_bytes<float>());
             break;
         case kYeeHF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<float>, 256, 0); break;
         case kYeeEF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<float>, 256, 0); break;
         case kYeeStepF32:
-            cudaFuncSetAttribute(yee_step<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<float>());
+            e = allow_smem(yee_step<float, false, true>, (int)yee_smem_bytes<float>());
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<float, false, true>, 256, yee_smem_bytes<float>());
             break;
         case kEnsF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false>, 256, 0); break;
         case kEnsF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<float, false, true>, 256, 0); break;
         case kEnsTma:
-            cudaFuncSetAttribute(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ens_tma_smem_bytes());
+            e = allow_smem(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, (int)ens_tma_smem_bytes());
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>,
                                                               kEnsConsumers + 32, ens_tma_smem_bytes());
             break;
         case kYeeTma:
-            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes(false));
+            e = allow_smem(yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>, (int)yee_tma_smem_bytes(false));
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>,
                                                               256, yee_tma_smem_bytes(false));
             break;
         case kYeeTmaMedia:
-            cudaFuncSetAttribute(yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_tma_smem_bytes(true));
+            e = allow_smem(yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>, (int)yee_tma_smem_bytes(true));
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>,
                                                               256, yee_tma_smem_bytes(true));
             break;
         case kHallTma:
-            cudaFuncSetAttribute(hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_tma_smem_bytes());
+            e = allow_smem(hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>, (int)hall_tma_smem_bytes());
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>, 256,
                                                               hall_tma_smem_bytes());
             break;

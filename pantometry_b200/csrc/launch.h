@@ -43,8 +43,24 @@ inline unsigned grid_for(const Tiles& t, unsigned resident) {
     return (unsigned)(t.ntiles < (long long)resident ? t.ntiles : (long long)resident);
 }
 
+// Opt `kernel` in to `bytes` of dynamic shared memory on the current device. The attribute
+// belongs to the function on one device, so the opt-in is recorded per (kernel, device) and made
+// once for each, under a lock (handles on several devices and several host threads share it).
+cudaError_t allow_smem_fn(const void* kernel, int bytes);
+template <typename K>
+inline cudaError_t allow_smem(K* kernel, int bytes) {
+    return allow_smem_fn(reinterpret_cast<const void*>(kernel), bytes);
+}
+// Launch `kernel` with `smem` bytes of dynamic shared memory, opting it in first on this device.
+template <typename... P, typename... A>
+inline cudaError_t launch_smem(void (*kernel)(P...), dim3 grid, dim3 block, int smem, cudaStream_t s, const A&... args) {
+    if (cudaError_t e = allow_smem(kernel, smem); e != cudaSuccess) return e;
+    kernel<<<grid, block, smem, s>>>(args...);
+    return cudaGetLastError();
+}
+
 // Resident blocks per SM of each step kernel at 256 threads (cudaOccupancyMaxActiveBlocksPer-
-// Multiprocessor, asked once per process), so a persistent grid is exactly one full wave.
+// Multiprocessor, asked once per kernel and device), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
     kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kKernelCount

@@ -73,6 +73,14 @@ extern "C" pm_status pm_hall_step_f32_noalloc(int nx, int ny, int nz, double dx,
                                               float* vz1, void* stream, double* invariant) {
     if (!p0 || !vx0 || !vy0 || !vz0 || !p1 || !vx1 || !vy1 || !vz1)
         return fail(PM_BAD_ARG, "noalloc: null field pointer");
+    {
+        // the kernel reads old values of neighbouring nodes while it writes the new ones, so
+        // every output must be a buffer of its own, apart from every input and other output
+        const void* all[8] = {p0, vx0, vy0, vz0, p1, vx1, vy1, vz1};
+        for (int o = 4; o < 8; ++o)
+            for (int q = 0; q < o; ++q)
+                if (all[o] == all[q]) return fail(PM_BAD_ARG, "noalloc: an output buffer is also an input or another output");
+    }
     if (nx < 2 || ny < 1 || nz < 1) return fail(PM_BAD_ARG, "noalloc: a hall has at least 2 x 1 x 1 nodes");
     if ((unsigned long long)nx * ny * nz >= (1ull << 32)) return fail(PM_BAD_ARG, "noalloc: grid above 2^32 nodes");
     if (!(dx > 0.0) || !(density > 0.0) || !(speed > 0.0) || !(dt > 0.0))

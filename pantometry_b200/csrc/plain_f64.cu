@@ -36,17 +36,8 @@ cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, cud
 
 template <>
 cudaError_t launch_hall<double>(const HallArgs<double>& a, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(hall_step<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
-        cudaFuncSetAttribute(hall_step<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
-        attr = true;
-    }
-    if (a.block_scale)
-        hall_step<double, true><<<a.nblocks, tile_block(), hall_smem_bytes<double>(), s>>>(a);
-    else
-        hall_step<double, false><<<a.nblocks, tile_block(), hall_smem_bytes<double>(), s>>>(a);
-    return cudaGetLastError();
+    const int smem = (int)hall_smem_bytes<double>();
+    return launch_smem(a.block_scale ? hall_step<double, true> : hall_step<double, false>, a.nblocks, tile_block(), smem, s, a);
 }
 template <>
 cudaError_t launch_hall_measure<double>(const HallMeasureArgs<double>& a, cudaStream_t s) {
@@ -65,23 +56,10 @@ cudaError_t launch_yee_e<double>(const YeeEArgs<double>& a, cudaStream_t s) {
 }
 template <>
 cudaError_t launch_yee_step<double>(const YeeStepArgs<double>& a, cudaStream_t s) {
-    static bool attr = false;
     const int smem = (int)yee_smem_bytes<double>();
-    if (!attr) {
-        cudaFuncSetAttribute(yee_step<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_step<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_step<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(yee_step<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
-    if (a.uniform) {
-        if (a.solid) yee_step<double, true, true><<<a.nblocks, tile_block(), smem, s>>>(a);
-        else yee_step<double, true, false><<<a.nblocks, tile_block(), smem, s>>>(a);
-    } else {
-        if (a.solid) yee_step<double, false, true><<<a.nblocks, tile_block(), smem, s>>>(a);
-        else yee_step<double, false, false><<<a.nblocks, tile_block(), smem, s>>>(a);
-    }
-    return cudaGetLastError();
+    auto k = a.uniform ? (a.solid ? yee_step<double, true, true> : yee_step<double, true, false>)
+                       : (a.solid ? yee_step<double, false, true> : yee_step<double, false, false>);
+    return launch_smem(k, a.nblocks, tile_block(), smem, s, a);
 }
 template <>
 cudaError_t launch_yee_measure<double>(const YeeHArgs<double>& a, double* out2, cudaStream_t s) {
@@ -151,13 +129,15 @@ int occupancy_f64(KernelId id) {
         case kHeatPlain: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_step, 256, 0); break;
         case kHeatPlainPair: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_step, 256, 0); break;
         case kHallF64:
-            cudaFuncSetAttribute(hall_step<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hall_smem_bytes<double>());
+            e = allow_smem(hall_step<double, false>, (int)hall_smem_bytes<double>());
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_step<double, false>, 256, hall_smem_bytes<double>());
             break;
         case kYeeHF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_h<double>, 256, 0); break;
         case kYeeEF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_e<double>, 256, 0); break;
         case kYeeStepF64:
-            cudaFuncSetAttribute(yee_step<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yee_smem_bytes<double>());
+            e = allow_smem(yee_step<double, false, true>, (int)yee_smem_bytes<double>());
+            if (e != cudaSuccess) break;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_step<double, false, true>, 256, yee_smem_bytes<double>());
             break;
         case kEnsF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_step<double, false>, 256, 0); break;

@@ -1,7 +1,10 @@
 // Host runtime: the Handle base (stream, graphs, device state, audit readout) and the C ABI's
 // status and error functions. The three domains live in heat.cu, hall.cu and cavity.cu.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <new>
+#include <utility>
 
 #include "runtime.h"
 
@@ -12,15 +15,40 @@ static thread_local std::string g_error;
 int occupancy_f64(KernelId id);
 int occupancy_f32(KernelId id);
 
+namespace {
+std::mutex g_attr_mutex;
+std::map<std::pair<const void*, int>, int> g_smem_opt_in;  // (kernel, device) -> bytes allowed
+std::map<std::pair<int, int>, int> g_occupancy;             // (kernel id, device) -> blocks per SM
+}  // namespace
+
+cudaError_t allow_smem_fn(const void* kernel, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    auto it = g_smem_opt_in.find({kernel, dev});
+    if (it != g_smem_opt_in.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) g_smem_opt_in[{kernel, dev}] = bytes;
+    return e;
+}
+
 int blocks_per_sm(KernelId id) {
-    static int cache[kKernelCount] = {0};
     if (id < 0 || id >= kKernelCount) return 1;
-    if (cache[id] == 0) {
-        int n = occupancy_f64(id);
-        if (n < 0) n = occupancy_f32(id);
-        cache[id] = n < 1 ? 1 : n;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+    {
+        std::lock_guard<std::mutex> lock(g_attr_mutex);
+        auto it = g_occupancy.find({(int)id, dev});
+        if (it != g_occupancy.end()) return it->second;
     }
-    return cache[id];
+    // asked outside the lock: the occupancy queries take it themselves for the opt-in
+    int n = occupancy_f64(id);
+    if (n < 0) n = occupancy_f32(id);
+    if (n < 1) n = 1;
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    g_occupancy[{(int)id, dev}] = n;
+    return n;
 }
 
 void set_error(const std::string& msg) { g_error = msg; }

@@ -61,3 +61,22 @@ def test_entry_build_in_a_fresh_interpreter():
     r = subprocess.run([sys.executable, "-c", "import __graft_entry__ as g; g.build()"], cwd=ROOT,
                        capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c", "-std=c11"), ("c++", "-std=c++11"), ("c++", "-std=c++17")])
+def test_header_compiles_as_c_and_cpp(tmp_path, lang, std):
+    """A Rust `bindgen`, a C host or a C++ host each include the header on its own: it must
+    compile alone, warning-free, in C and in C++."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / ("use." + ("c" if lang == "c" else "cpp"))
+    src.write_text('#include "pantometry_gpu.h"\n'
+                   "int main(void) { pm_violation v; pm_ledger l; (void)v; (void)l;\n"
+                   "  return (int)sizeof(pm_status_string(PM_OK)) - (int)sizeof(const char*); }\n")
+    r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-I", os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -58,16 +58,59 @@ def test_noalloc_hall_step_matches_the_handle_two_calls_in_a_row():
 
 def test_noalloc_refuses_sizes_beyond_its_limits():
     """Refusals happen on the host, before anything reaches the GPU: a grid of 2^32 nodes or more
-    (the kernel's 32-bit node index) and a step past the Courant limit."""
+    (the kernel's 32-bit node index), a step past the Courant limit, a non-positive step, and an
+    output buffer that is also an input or another output (the kernel reads neighbours' old
+    values while it writes new ones)."""
     import torch
 
     from pantometry_b200 import _native as N
 
     lib = N.load()
-    t = torch.zeros(8, device="cuda")
-    ptrs = [C.c_void_p(t.data_ptr())] * 8
+    bufs = [torch.zeros(8, device="cuda") for _ in range(8)]
+    ptrs = [C.c_void_p(t.data_ptr()) for t in bufs]
     inv = C.c_double(0.0)
     st = lib.pm_hall_step_f32_noalloc(2048, 2048, 1024, 1.0, 1.0, 1.0, 0.1, 1, *ptrs, None, C.byref(inv))
     assert st == N.PM_BAD_ARG and b"2^32" in lib.pm_last_error()
     st = lib.pm_hall_step_f32_noalloc(4, 2, 1, 1.0, 1.0, 1.0, 10.0, 1, *ptrs, None, C.byref(inv))
     assert st == N.PM_VIOLATION and b"Courant" in lib.pm_last_error()
+    st = lib.pm_hall_step_f32_noalloc(4, 2, 1, 1.0, 1.0, 1.0, 0.0, 1, *ptrs, None, C.byref(inv))
+    assert st == N.PM_BAD_ARG and b"dt" in lib.pm_last_error()
+    for out, same in ((4, 0), (5, 1), (7, 3), (6, 5)):
+        aliased = list(ptrs)
+        aliased[out] = ptrs[same]
+        st = lib.pm_hall_step_f32_noalloc(4, 2, 1, 1.0, 1.0, 1.0, 0.1, 1, *aliased, None, C.byref(inv))
+        assert st == N.PM_BAD_ARG and b"output buffer" in lib.pm_last_error(), (out, same)
+
+
+def test_noalloc_on_a_second_device_after_the_first():
+    """The array exists once per GPU that loads the library; a call on the second device after one
+    on the first looks up that device's own copy and gives the same fields."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one CUDA device: the second-device case needs two")
+    from pantometry_b200 import _native as N
+    from pantometry_b200 import workloads as W
+
+    cfg = W.acoustic_hall(24, steps=2, source=False)
+    lib = N.load()
+    results = []
+    for d in (0, 1):
+        with torch.cuda.device(d):
+            dev = torch.device("cuda", d)
+            nx = ny = nz = 24
+            p = torch.tensor(cfg["pressure"], dtype=torch.float64, device=dev).float()
+            state = [p, torch.zeros((nx - 1) * ny * nz, device=dev), torch.zeros(nx * (ny - 1) * nz, device=dev),
+                     torch.zeros(nx * ny * (nz - 1), device=dev)]
+            out = [torch.empty_like(t) for t in state]
+            inv = C.c_double(0.0)
+            torch.cuda.synchronize(dev)
+            st = lib.pm_hall_step_f32_noalloc(nx, ny, nz, cfg["size"][0] / (nx - 1), cfg["speed"], cfg["density"], cfg["dt"], 1,
+                                              *[C.c_void_p(t.data_ptr()) for t in state],
+                                              *[C.c_void_p(t.data_ptr()) for t in out],
+                                              C.c_void_p(torch.cuda.current_stream(dev).cuda_stream), C.byref(inv))
+            assert st == N.PM_OK, lib.pm_last_error().decode()
+            results.append(([t.cpu() for t in out], inv.value))
+    for a, b in zip(results[0][0], results[1][0]):
+        assert torch.equal(a, b)
+    assert results[0][1] == results[1][1]
