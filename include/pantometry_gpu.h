@@ -333,7 +333,13 @@ pm_status pm_cavity_upload(pm_cavity* c, const double* ex, const double* ey, con
 pm_status pm_cavity_download(pm_cavity* c, double* ex, double* ey, double* ez, double* hx,
                              double* hy, double* hz);
 /* Extension (not in the reference): a soft current density current[s] (A/m^2) on the Ez edge
- * with flat index `edge`, applied in step s's electric update; its work is kept in the ledger. */
+ * with flat index `edge`, applied in step s's electric update; its work is kept in the ledger.
+ * An FP32 cavity keeps the six components of a 5^3 box of lattice nodes around the edge in f64
+ * (the source's near field, where the pulse moves energy in and out many times over the net work;
+ * f32 storage there leaves the books a few 1e-6 of the injected energy off the f64 run), when the
+ * box and the edges along its high sides lie a node or more inside the walls, and the cavity is
+ * on the padded FP32 layout (one medium, or per-cell epsilon without conductivity or per-cell mu)
+ * and not both lossy and obstructed. Elsewhere the FP32 form keeps the whole field in f32. */
 pm_status pm_cavity_set_source(pm_cavity* c, long long edge, const double* current, size_t n);
 /* Cavity::courant_limit (cavity.rs:1035-1037). */
 pm_status pm_cavity_courant_limit(pm_cavity* c, double* seconds);
@@ -344,6 +350,10 @@ pm_status pm_cavity_step(pm_cavity* c, double dt, long long nsteps, pm_violation
 pm_status pm_cavity_ledger(pm_cavity* c, pm_ledger* out);
 /* Cavity::electric_energy / magnetic_energy (cavity.rs:824-847, 919-940), on the device. */
 pm_status pm_cavity_energies(pm_cavity* c, double* electric, double* magnetic);
+/* Domain::checkpoint / restore (cavity.rs:1566-1590): the fields, `started` and `dissipated`. With
+ * a source set (the extension) the checkpoint also keeps the source's clock and its work books, so
+ * steps retried after a restore drive the same samples of the current; an FP32 cavity keeps the f64
+ * values of its source's near field with them. */
 pm_status pm_cavity_checkpoint(pm_cavity* c);
 pm_status pm_cavity_restore(pm_cavity* c);
 pm_status pm_cavity_set_stream(pm_cavity* c, void* stream);

@@ -49,6 +49,10 @@ struct Cavity : Handle {
     DBuf sf[6];
     bool s_started = false;
     double s_dissipated = 0.0;
+    // the source extension's clock (which sample of the current comes next) and its work books,
+    // so that steps retried after a restore drive the same pulse
+    long long s_steps = 0;
+    double s_work = 0.0, s_work_booked = 0.0;
     // FP32 cavities of one medium keep all six components on the padded lattice (row pitch L)
     // and step with the TMA-staged kernel (yee_tma.cuh); maps[par] describe parity par's fields
     bool tma = false;
@@ -59,6 +63,16 @@ struct Cavity : Handle {
     bool has_prev = false;   // a step has run (cavity.rs:1087)
     bool use_stale = false;  // the next step's history is `stale`
     DBuf stale[3];
+    // The source's near field in f64 (yee_near.cuh): the six components of a box of
+    // kNearWidth³ lattice nodes around the source edge, one set per parity. Kept when the cavity
+    // is TMA-staged FP32 with a source and the box, with the ring of edges on its high sides,
+    // lies one node or more inside the walls (near_w = kNearWidth); otherwise near_w = 0.
+    static constexpr int kNearWidth = 5;
+    int near_x0 = 0, near_y0 = 0, near_z0 = 0, near_w = 0;
+    DBuf dnear[2];
+    bool near_dirty = true;  // the stored field changed outside a step: seed the box from it
+    DBuf snear;              // the box of the checkpoint
+    bool s_near = false;
 
     size_t count(int q) const {
         switch (q) {
@@ -292,6 +306,7 @@ struct Cavity : Handle {
 
     pm_status put(int q, const double* src_host) {
         const size_t n = count(q);
+        near_dirty = true;
         if (tma) {  // into the padded lattice, padding zero
             PM_CUDA(cudaMemsetAsync(f[parity][q].p, 0, lattice() * 4, stream()));
             if (!src_host) return PM_OK;
@@ -359,6 +374,7 @@ struct Cavity : Handle {
         parity = home;
         if (s != PM_OK) return s;
         if (writes) {
+            near_dirty = true;
             for (int q = 0; q < 6; ++q) {
                 int ex, ey, ez;
                 extents(q, ex, ey, ez);
@@ -423,9 +439,23 @@ struct Cavity : Handle {
     // One step from `par`, its walls included.
     cudaError_t step_once(int par, double h, bool prev, bool stale_history, cudaStream_t s) const {
         cudaError_t e;
-        if (precision == PM_PLAIN_F64) e = launch_yee_step<double>(sargs<double>(par, h), s);
-        else if (tma) e = launch_yee_tma(targs(par, h), L, maps[par], s);
-        else e = launch_yee_step<float>(sargs<float>(par, h), s);
+        if (precision == PM_PLAIN_F64) {
+            e = launch_yee_step<double>(sargs<double>(par, h), s);
+        } else if (tma) {
+            YeeStepArgs<float> t = targs(par, h);
+            if (near_on()) {
+                // the box's terms and the source are the box kernel's; it closes the books
+                const YeeNearArgs n = nargs(par, h, t);
+                t.nb_x0 = near_x0; t.nb_y0 = near_y0; t.nb_z0 = near_z0; t.nb_w = near_w;
+                t.src_i = t.src_j = t.src_k = -1;
+                e = launch_yee_tma(t, L, maps[par], s);
+                if (e == cudaSuccess) e = launch_yee_near(n, any_solid, s);
+            } else {
+                e = launch_yee_tma(t, L, maps[par], s);
+            }
+        } else {
+            e = launch_yee_step<float>(sargs<float>(par, h), s);
+        }
         if (e != cudaSuccess || !open_or_magnetic()) return e;
         return precision == PM_PLAIN_F64 ? walls<double>(par, prev, stale_history, h, s) : walls<float>(par, prev, stale_history, h, s);
     }
@@ -443,6 +473,78 @@ struct Cavity : Handle {
                 !hall_tma_map(&maps[q].hz, f[q][5].p, d0, d1, d2, 36, 9, P))
                 return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a cavity field");
         }
+        return PM_OK;
+    }
+
+    bool lossy_now() const { return uniform ? sig_u != 0.0 : !lossless; }
+    // The near-field box is stepped: TMA-staged FP32, a source, a box inside the walls. A lossy
+    // cavity with obstacles keeps the plain FP32 form: the Joule term of an edge is booked before
+    // the obstacles zero it, and the ring's correction could not see that value.
+    bool near_on() const {
+        return tma && precision == PM_FIELDS_F32 && src >= 0 && near_w > 0 && !(any_solid && lossy_now());
+    }
+    // Place the box around the source edge's node, or turn it off where it would not fit.
+    pm_status place_near() {
+        near_w = 0;
+        near_dirty = true;
+        if (src < 0) return PM_OK;
+        const int w = kNearWidth, r = w / 2;
+        const int si = (int)(src % (nx + 1)), sj = (int)((src / (nx + 1)) % (ny + 1));
+        const int sk = (int)(src / ((long long)(nx + 1) * (ny + 1)));
+        const int x0 = si - r, y0 = sj - r, z0 = sk - r;
+        // the box and the ring on its high sides at nodes 1 .. n−1: every component exists at
+        // each of their nodes and every edge is interior
+        if (x0 < 1 || y0 < 1 || z0 < 1 || x0 + w > nx - 1 || y0 + w > ny - 1 || z0 + w > nz - 1) return PM_OK;
+        const size_t bytes = 6 * (size_t)w * w * w * sizeof(double);
+        for (int par = 0; par < 2; ++par)
+            if (dnear[par].bytes < bytes) PM_CUDA(dnear[par].alloc(bytes));
+        near_x0 = x0; near_y0 = y0; near_z0 = z0; near_w = w;
+        return PM_OK;
+    }
+    // Arguments of the box's kernel for the step from `par` with the TMA step's arguments `t`.
+    YeeNearArgs nargs(int par, double h, const YeeStepArgs<float>& t) const {
+        YeeNearArgs n{};
+        for (int q = 0; q < 6; ++q) {
+            n.old[q] = f[par][q].as<float>();
+            n.neu[q] = f[par ^ 1][q].as<float>();
+        }
+        n.nold = dnear[par].as<double>();
+        n.nneu = dnear[par ^ 1].as<double>();
+        n.x0 = near_x0; n.y0 = near_y0; n.z0 = near_z0; n.w = near_w;
+        n.L = L; n.ny1 = (unsigned)ny + 1;
+        n.nx = nx; n.ny = ny; n.nz = nz;
+        n.ch = t.g / t.mu_u;  // cavity.rs:1355 in f64
+        if (uniform) {
+            const double half = sig_u * h / (2.0 * eps_u);  // cavity.rs:1391-1397
+            n.decay = (1.0 - half) / (1.0 + half);
+            n.gain = (h / (eps_u * dx)) / (1.0 + half);
+        } else {
+            n.decay = 1.0;  // lossless mixed ε: each edge's own gain
+            n.gain = 0.0;
+            n.media = 1;
+            for (int q = 0; q < 3; ++q) n.cgain[q] = dgain[q].as<float>();
+        }
+        n.chf = t.ch; n.gainf = t.gain[0]; n.decf = t.decay[0];
+        n.lossy = t.sigma_u[0] != 0.0 ? 1 : 0;
+        n.sig0 = t.sigma_u[0];
+        n.solid = t.solid;
+        n.src_i = t.src_i; n.src_j = t.src_j; n.src_k = t.src_k;
+        n.current = t.current; n.ncurrent = t.ncurrent;
+        n.eps_src = t.eps_src; n.sig_src = t.sig_src;
+        n.dt = h; n.volume = t.volume; n.g = t.g; n.eps_u = t.eps_u; n.mu_u = t.mu_u;
+        n.st = t.st;
+        return n;
+    }
+    // The box's f64 values from the stored field of the present parity.
+    pm_status seed_near() {
+        if (!near_on()) return PM_OK;
+        YeeNearArgs n{};
+        for (int q = 0; q < 6; ++q) n.neu[q] = f[parity][q].as<float>();
+        n.nneu = dnear[parity].as<double>();
+        n.x0 = near_x0; n.y0 = near_y0; n.z0 = near_z0; n.w = near_w;
+        n.L = L; n.ny1 = (unsigned)ny + 1;
+        PM_CUDA(launch_yee_near_seed(n, stream()));
+        near_dirty = false;
         return PM_OK;
     }
 
@@ -819,6 +921,8 @@ pm_status pm_cavity_set_source(pm_cavity* cp, long long edge, const double* cur,
         PM_CUDA(c->put_sync(c->current.p, cur, n * 8));
     }
     c->drop_graphs();
+    pm_status ps = c->place_near();
+    if (ps != PM_OK) return ps;
     return c->reset_ledger();
 }
 
@@ -861,6 +965,7 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
         if (s != PM_OK) return s;
         c->started = true;
     }
+    if (c->near_dirty && (s = c->seed_near()) != PM_OK) return s;
     long long remaining = nsteps;
     if (!c->has_prev || c->use_stale) {
         // the first step after creation holds open walls at zero; the first after E was rewritten
@@ -908,10 +1013,22 @@ pm_status pm_cavity_checkpoint(pm_cavity* cp) {
         if (!c->sf[q].p || c->sf[q].bytes < bytes) PM_CUDA(c->sf[q].alloc(bytes));
         PM_CUDA(cudaMemcpyAsync(c->sf[q].p, c->f[c->parity][q].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
     }
+    c->s_near = false;
+    if (c->near_on()) {  // the box's f64 values are part of the state
+        pm_status ns = c->near_dirty ? c->seed_near() : PM_OK;
+        if (ns != PM_OK) return ns;
+        const size_t bytes = c->dnear[c->parity].bytes;
+        if (c->snear.bytes < bytes) PM_CUDA(c->snear.alloc(bytes));
+        PM_CUDA(cudaMemcpyAsync(c->snear.p, c->dnear[c->parity].p, bytes, cudaMemcpyDeviceToDevice, c->stream()));
+        c->s_near = true;
+    }
     pm_status s = c->read_state();
     if (s != PM_OK) return s;
     c->s_started = c->started;
     c->s_dissipated = c->host_state->dissipated;
+    c->s_steps = c->host_state->steps;
+    c->s_work = c->host_state->work;
+    c->s_work_booked = c->host_state->work_booked;
     c->has_saved = true;
     return PM_OK;
 }
@@ -924,10 +1041,20 @@ pm_status pm_cavity_restore(pm_cavity* cp) {
     if (hs != PM_OK) return hs;
     for (int q = 0; q < 6; ++q)
         PM_CUDA(cudaMemcpyAsync(c->f[c->parity][q].p, c->sf[q].p, c->dcount(q) * c->esize(), cudaMemcpyDeviceToDevice, c->stream()));
+    c->near_dirty = true;
+    if (c->s_near && c->near_on() && c->snear.bytes == c->dnear[c->parity].bytes) {
+        PM_CUDA(cudaMemcpyAsync(c->dnear[c->parity].p, c->snear.p, c->snear.bytes, cudaMemcpyDeviceToDevice, c->stream()));
+        c->near_dirty = false;
+    }
     pm_status s = c->read_state();
     if (s != PM_OK) return s;
     c->started = c->s_started;
     c->host_state->dissipated = c->s_dissipated;
+    if (c->src >= 0) {
+        c->host_state->steps = c->s_steps;
+        c->host_state->work = c->s_work;
+        c->host_state->work_booked = c->s_work_booked;
+    }
     if ((s = c->write_state()) != PM_OK) return s;
     c->has_saved = false;  // cavity.rs:1580 takes the checkpoint
     return c->reset_ledger();

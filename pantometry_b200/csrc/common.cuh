@@ -58,7 +58,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // Why the run stopped, in DevState::violated.
 // kDeviceTimeout: a bounded wait inside a kernel ran out (the kernel gave up and returned).
-enum : int { kRunning = 0, kAuditFailed = 1, kStartupFailed = 2, kDeviceTimeout = 3 };
+// kRefused: a step was refused before anything moved (a state-dependent stability limit, checked
+// on the device at the start of each step; the v_* fields hold the refusal's numbers).
+enum : int { kRunning = 0, kAuditFailed = 1, kStartupFailed = 2, kDeviceTimeout = 3, kRefused = 4 };
 
 // One per handle, in device memory. Written only by the last block of a step kernel (and by
 // the host between calls), read by every block of the next kernel: stream order is the only
@@ -80,6 +82,14 @@ struct DevState {
     // Cavity books (cavity.rs:161-162) and the source extension
     double invariant, dissipated, work;
     double work_booked;  // cavity source work already in the ledger: through the previous step
+    // an FP32 cavity whose source's near field is kept in f64: the step kernel's four sums over
+    // every node outside that box, handed to the kernel that steps the box and closes the books
+    double near_acc[4];
+    // Solid3D with radiating films: `worst_rate_now` of the present state (solid.rs:1148-1185),
+    // and the max over boundary cells the step kernel gathers for the next state (the bits of a
+    // non-negative double, so an integer atomicMax orders them)
+    double rate_now;
+    unsigned long long rate_bits;
     unsigned int counter;  // arrival ticket for the last-block reduction; always 0 between kernels
     unsigned int pad;
 };

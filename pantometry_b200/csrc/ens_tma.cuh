@@ -8,6 +8,19 @@
 // heat_f32_step's, the per-brick FP64 partials and the per-block ticket reduction are ens_step's.
 // Every wait on a stage's mbarrier is bounded; a wait that runs out stops the kernel with
 // kDeviceTimeout in every block's books.
+//
+// Order of the walk. Bricks differ in cost (blocks of 16 to 128 cells per axis), so a fixed share
+// per CTA (brick c, c + gridDim, ...) lets the CTAs drift apart, and the bricks running at one time
+// stop being neighbours: the halo rows and planes one brick reads from its neighbours are then
+// gone from L2 by the time the neighbour runs. The producers therefore take bricks in list order
+// from one atomic counter, so the bricks in flight are always a contiguous run of the list and a
+// brick's x, y and z neighbours run beside it. Which CTA takes which brick changes nothing in the
+// results: every partial is stored by brick and warp, and each block's are summed in fixed order.
+//
+// No barrier spans the consumer warps. Each warp waits for its stage, computes its row of the
+// brick, hands the slot back, and at the end of a brick stores its own two partials and takes a
+// ticket of its block; the warp holding the block's last ticket sums the block's partials in a
+// fixed order and runs its ledger and audit.
 #pragma once
 
 #include "ensemble_kernels.cuh"
@@ -57,7 +70,12 @@ struct EnsTmaArgs {
     EnsArgs<float> e;
     const CUtensorMap* maps;    // per block: the old field's map (this launch's parity)
     const EnsBrickInfo* infos;  // per brick
+    // work[0]: the next brick of the walk; work[1]: CTAs done. Zero at every launch's start: the
+    // last CTA to finish puts both back to zero.
+    unsigned* work;
 };
+// Partials per brick: two for each consumer warp (Σ deviation of the new state, Σ heat shed).
+constexpr int kEnsTmaPartialsPerBrick = 2 * 8;
 
 __device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -67,46 +85,17 @@ __device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigne
 __device__ __forceinline__ void mbar_arrive(unsigned bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-// The 256 consumer threads only (named barrier 1): a barrier, and a barrier that ANDs a predicate.
 constexpr int kEnsConsumers = 256;
-__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
-__device__ __forceinline__ bool consumers_and(bool p) {
-    unsigned r;
-    asm volatile("{\n .reg .pred a, b;\n setp.ne.u32 a, %1, 0;\n bar.red.and.pred b, 1, 256, a;\n selp.u32 %0, 1, 0, b;\n}\n"
-                 : "=r"(r)
-                 : "r"((unsigned)p)
-                 : "memory");
-    return r != 0;
-}
-// block_sum over the consumers (result in consumer thread 0).
-template <int NV>
-__device__ __forceinline__ void consumers_sum(double (&v)[NV], double* smem, int tid) {
-    const int lane = tid & 31, warp = tid >> 5;
-    warp_sum<NV>(v);
-    if (lane == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) smem[warp * NV + q] = v[q];
-    }
-    consumers_sync();
-    if (warp == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) v[q] = lane < kEnsConsumers / 32 ? smem[lane * NV + q] : 0.0;
-        warp_sum<NV>(v);
-    }
-    consumers_sync();
-}
 
-// Warps 0-7 consume (the cells of a 32 × 8 brick column each); warp 8 produces: it walks the
-// bricks (blockIdx.x, blockIdx.x + gridDim.x, ...), the next brick's entry fetched a brick ahead,
-// and for every stage issues the brick's record and the tile, S − 1 stages ahead. Slots are handed
-// back and forth with a full and an empty mbarrier each; every wait is bounded.
+// Warps 0-7 consume (the cells of a 32 × 8 brick column each); warp 8 produces: it takes the
+// bricks of the walk from the shared counter, one brick ahead, and for every stage issues the
+// brick's record and the tile, S − 1 stages ahead. Slots are handed back and forth with a full and
+// an empty mbarrier each; every wait is bounded.
 template <int P, int S>
 static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOCKS) ens_tma_step(const EnsTmaArgs t) {
     using St = EnsTmaStage<P>;
     const EnsArgs<float>& a = t.e;
     extern __shared__ __align__(128) unsigned char ens_tma_smem[];
-    __shared__ double red[32 * 2];
-    __shared__ int last;
     __shared__ EnsBrickInfo info[S];
     __shared__ unsigned stage_brick[S];
     __shared__ int stage_kb[S], stage_z1[S];  // stage_z1 < 0: the walk is over
@@ -134,10 +123,11 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
     __syncthreads();
     if (warp == kEnsConsumers / 32) {  // the producer
         if (lane != 0) return;
-        unsigned b = blockIdx.x;
+        unsigned b = atomicAdd(&t.work[0], 1u);
         EnsBrick br{}, nbr{};
         if (b < a.nbricks) br = a.bricks[b];
-        if (b + gridDim.x < a.nbricks) nbr = a.bricks[b + gridDim.x];
+        unsigned nb = b < a.nbricks ? atomicAdd(&t.work[0], 1u) : a.nbricks;
+        if (nb < a.nbricks) nbr = a.bricks[nb];
         int kb = br.z0;
         int q = 0;
         bool ok = true;
@@ -161,11 +151,12 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
             tma_load_3d(ring_base + slot * (unsigned)sizeof(St), t.maps + br.grid, (int)br.x0 - 4, (int)br.y0 - 1, kb - 1,
                         full);
             kb += P;
-            if (kb >= br.z1) {  // to the next brick, and fetch the one after it
-                b += gridDim.x;
+            if (kb >= br.z1) {  // to the next brick, and take the one after it
+                b = nb;
                 br = nbr;
                 kb = br.z0;
-                if (b + gridDim.x < a.nbricks) nbr = a.bricks[b + gridDim.x];
+                nb = b < a.nbricks ? atomicAdd(&t.work[0], 1u) : a.nbricks;
+                if (nb < a.nbricks) nbr = a.bricks[nb];
             }
         }
         if (!ok) {
@@ -173,16 +164,24 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
         }
         // the last use of each slot: its copies land before this thread (and the block) is done
         for (int u = (q >= S ? q - S + 1 : 0); u < q; ++u) mbar_wait(full_base + 8 * (u % S), (unsigned)((u / S) & 1));
+        // this CTA takes no more bricks; the last CTA to get here zeroes the counters for the next
+        // launch (every other CTA's last take precedes its arrival here)
+        __threadfence();
+        if (atomicAdd(&t.work[1], 1u) == gridDim.x - 1) {
+            t.work[0] = 0u;
+            t.work[1] = 0u;
+            __threadfence();
+        }
         return;
     }
     const int tx = lane, ty = warp;
-    double acc[2] = {0.0, 0.0};  // the brick's Σ deviation of the new state, Σ heat shed
+    double acc[2] = {0.0, 0.0};  // this warp's row of the brick: Σ deviation of the new state, Σ heat shed
     int slot = 0;
     unsigned phase = 0;  // of the slot's full barrier: flips each time the ring wraps
     for (;; slot = slot + 1 == S ? 0 : slot + 1, phase ^= slot == 0 ? 1u : 0u) {
         const bool got = mbar_wait(full_base + 8 * slot, phase);
-        if (!consumers_and(got)) {
-            if (tid == 0)
+        if (__any_sync(0xffffffffu, !got)) {  // this warp stops; the others and the producer run out too
+            if (lane == 0)
                 for (unsigned g = 0; g < a.ngrids; ++g) a.states[g].violated = kDeviceTimeout;
             return;
         }
@@ -294,32 +293,35 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
             }
         }
         const bool brick_done = kb + P >= z1;
+        const unsigned nbricks_of_block = a.grids[gi].nbricks;
         // this warp is done with the slot (the tile and the record)
         __syncwarp();
         if (lane == 0) mbar_arrive(empty_base + 8 * slot);
         if (brick_done && !hold) {
-            // the brick's partials, then the block's ticket; the last brick of the block reduces
-            // the block's partials in fixed order, then its ledger and audit
+            // this warp's partials, then its ticket of the block; the warp with the block's last
+            // ticket sums the block's partials in fixed order, then runs its ledger and audit
             const EnsGrid& g = a.grids[gi];
             DevState* st = a.states + gi;
-            consumers_sum<2>(acc, red, tid);
-            if (tid == 0) {
-                a.partials[2 * (size_t)brick] = acc[0];
-                a.partials[2 * (size_t)brick + 1] = acc[1];
+            warp_sum<2>(acc);
+            unsigned ticket = 0;
+            if (lane == 0) {
+                const size_t at = ((size_t)brick * 8 + (size_t)warp) * 2;
+                a.partials[at] = acc[0];
+                a.partials[at + 1] = acc[1];
                 __threadfence();
-                const unsigned ticket = atomicAdd(&st->counter, 1u);
-                last = ticket == g.nbricks - 1 ? 1 : 0;
+                ticket = atomicAdd(&st->counter, 1u);
             }
-            consumers_sync();
-            if (last) {
+            ticket = __shfl_sync(0xffffffffu, ticket, 0);
+            if (ticket == nbricks_of_block * 8 - 1) {
                 __threadfence();
                 double v[2] = {0.0, 0.0};
-                for (unsigned q = tid; q < g.nbricks; q += kEnsConsumers) {
-                    v[0] += __ldcg(&a.partials[2 * (size_t)(g.first_brick + q)]);
-                    v[1] += __ldcg(&a.partials[2 * (size_t)(g.first_brick + q) + 1]);
+                const size_t first = (size_t)g.first_brick * 8, count = (size_t)g.nbricks * 8;
+                for (size_t q = lane; q < count; q += 32) {
+                    v[0] += __ldcg(&a.partials[(first + q) * 2]);
+                    v[1] += __ldcg(&a.partials[(first + q) * 2 + 1]);
                 }
-                consumers_sum<2>(v, red, tid);
-                if (tid == 0) {
+                warp_sum<2>(v);
+                if (lane == 0) {
                     st->counter = 0u;
                     const double stored = g.capacity * v[0];
                     st->lost += g.capacity * v[1];

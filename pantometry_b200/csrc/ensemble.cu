@@ -154,6 +154,7 @@ struct Ensemble : Handle {
     bool tma = false;
     std::vector<CUtensorMap> maps;
     DBuf dmaps, dinfos;
+    DBuf dwork;  // the TMA walk's two counters (next brick, CTAs done), zero between launches
     int shape = 0;
     long long generation = 0;  // bumped when the brick list changes (the graph cache key)
     DBuf field[2], stage, dgrids, dbricks, dstates, bpartials, saved, saved_states;
@@ -208,7 +209,14 @@ struct Ensemble : Handle {
         drop_graphs();
         PM_CUDA(cudaStreamSynchronize(stream()));
         if (dbricks.bytes < bricks.size() * sizeof(EnsBrick)) PM_CUDA(dbricks.alloc(bricks.size() * sizeof(EnsBrick)));
-        if (bpartials.bytes < bricks.size() * 2 * sizeof(double)) PM_CUDA(bpartials.alloc(bricks.size() * 2 * sizeof(double)));
+        // two partials per brick, or two per consumer warp of a brick on the TMA path
+        const size_t per_brick = tma ? (size_t)kEnsTmaPartialsPerBrick : 2;
+        if (bpartials.bytes < bricks.size() * per_brick * sizeof(double))
+            PM_CUDA(bpartials.alloc(bricks.size() * per_brick * sizeof(double)));
+        if (tma && !dwork.p) {
+            PM_CUDA(dwork.alloc(2 * sizeof(unsigned)));
+            PM_CUDA(cudaMemsetAsync(dwork.p, 0, 2 * sizeof(unsigned), stream()));
+        }
         PM_CUDA(put_sync(dbricks.p, bricks.data(), bricks.size() * sizeof(EnsBrick)));
         PM_CUDA(put_sync(dgrids.p, grids.data(), grids.size() * sizeof(EnsGrid)));
         shape = sh;
@@ -240,6 +248,7 @@ struct Ensemble : Handle {
             t.e = args<float>(par);
             t.maps = dmaps.as<CUtensorMap>() + (size_t)par * grids.size();
             t.infos = dinfos.as<EnsBrickInfo>();
+            t.work = dwork.as<unsigned>();
             const unsigned w = wave_of(kEnsTma);
             return launch_ens_tma(t, std::min<unsigned>(w, (unsigned)std::max<size_t>(bricks.size(), 1)), s);
         }

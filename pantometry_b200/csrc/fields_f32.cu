@@ -118,6 +118,16 @@ cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMap
     return launch_smem(k, a.nblocks, tile_block(), smem, s, a, L, m);
 }
 
+cudaError_t launch_yee_near(const YeeNearArgs& a, bool solid, cudaStream_t s) {
+    if (solid) yee_near_step<true><<<1, 256, 0, s>>>(a);
+    else yee_near_step<false><<<1, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_yee_near_seed(const YeeNearArgs& a, cudaStream_t s) {
+    yee_near_seed<<<1, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,
                                 unsigned L, unsigned ny1, int to_padded, cudaStream_t s) {
     if (src_f64 && !dst_f64)

@@ -156,6 +156,54 @@ struct Heat : Handle {
         if (nowhere) worst_rate = NAN;
     }
 
+    // Radiating films: the step limit follows the state (solid.rs:1148-1185).
+    bool radiating() const { return films.exposed && any_radiative_film(); }
+
+    // solid.rs:1269-1288 `loss_conductance_at` at temperature `at`, summed from −0.0 (Rust's
+    // `Sum for f64`), radiating term included.
+    double loss_conductance_at(double at, int i, int j, int k, size_t c) const {
+        double total = -0.0;
+        const double eps = mat_eps(mat_of(c));
+        for (int f = 0; f < 6; ++f) {
+            if (!((films.exposed >> f) & 1)) continue;
+            bool holds = f == 0 ? i == 0 : f == 1 ? i + 1 == nx : f == 2 ? j == 0 : f == 3 ? j + 1 == ny : f == 4 ? k == 0 : k + 1 == nz;
+            if (!holds) continue;
+            const double share = films.share[f];
+            const double hot = rust_max(at, films.ambient[f]);
+            const double h = film_conv[f] + 4.0 * eps * kStefanBoltzmann * (hot * (hot * hot));  // powi(3)
+            total += host_series_with_half_cell(h * share, mat_k(mat_of(c)), share, dx);
+        }
+        return total;
+    }
+    // solid.rs:1148-1185 over a state `t` (kelvin, reference order).
+    double worst_rate_of(const std::vector<double>& t) const {
+        if (films.exposed == 0 || std::isnan(worst_rate)) return worst_rate;
+        double worst = worst_rate;
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    if (!(i == 0 || i + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz)) continue;
+                    const size_t c = i + (size_t)nx * (j + (size_t)ny * k);
+                    const double loss = loss_conductance_at(t[c], i, j, k, c);
+                    if (loss == 0.0) continue;
+                    worst = rust_max(worst, mob_at(c) * (face_sum_at(i, j, k) + loss / dx));
+                }
+        return worst;
+    }
+    // The rate of the present state into the device books, where the films radiate: the step
+    // kernels keep it from then on, step by step.
+    pm_status refresh_rate() {
+        if (precision != PM_PLAIN_F64 || !radiating()) return PM_OK;
+        std::vector<double> t(n());
+        PM_CUDA(cudaMemcpyAsync(t.data(), field[parity].p, n() * 8, cudaMemcpyDeviceToHost, stream()));
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        pm_status s = read_state();
+        if (s != PM_OK) return s;
+        host_state->rate_now = worst_rate_of(t);
+        host_state->rate_bits = 0ull;
+        return write_state();
+    }
+
     bool any_radiative_film() const {
         for (int f = 0; f < 6; ++f)
             if (((films.exposed >> f) & 1)) {
@@ -309,6 +357,8 @@ struct Heat : Handle {
         a.dts = dt; a.dx = dx; a.reference = reference;
         a.films = films;
         a.pairs = uniform && nx % 2 == 0 && wide ? 1 : 0;
+        a.radiating = radiating() ? 1 : 0;
+        a.static_rate = worst_rate;
         const unsigned w = wave_of(a.pairs ? kHeatPlainPair : kHeatPlain);
         const int tx = a.pairs ? nx / 2 : nx;  // the threads along a row
         a.tiles = make_tiles(tx, ny, nz, choose_zc(tx, ny, nz, w));
@@ -364,7 +414,9 @@ struct Heat : Handle {
         m.partials = partials.as<double>();
         m.nblocks = kMeasureBlocks;
         PM_CUDA(precision == PM_PLAIN_F64 ? launch_heat_measure_plain(m, stream()) : launch_heat_measure_f32(m, stream()));
-        return read_state();
+        pm_status s = read_state();
+        if (s != PM_OK) return s;
+        return refresh_rate();
     }
 };
 
@@ -388,6 +440,7 @@ pm_status pm_heat_create(const pm_heat_desc* d, pm_heat** out) {
     Heat* h = new (std::nothrow) Heat();
     if (!h) return fail(PM_OUT_OF_MEMORY, "host allocation");
     h->name = d->name ? d->name : "block";
+    h->refusal_site = h->name + " (explicit 3D conduction)";
     h->nx = std::max(d->nx, 1); h->ny = std::max(d->ny, 1); h->nz = std::max(d->nz, 1);
     h->dx = d->dx;
     h->reference = d->initial_kelvin;
@@ -440,7 +493,9 @@ pm_status pm_heat_losing_from(pm_heat* hp, int face, double ambient, double conv
     h->films.share[face] = area / (double)std::max<size_t>(h->cells_on(face), 1);  // solid.rs:1203
     h->resolve();
     h->drop_graphs();
-    return h->upload_films_f32();
+    pm_status s = h->upload_films_f32();
+    if (s != PM_OK) return s;
+    return h->refresh_rate();
 }
 
 pm_status pm_heat_upload(pm_heat* hp, const double* kelvin, size_t n) {
@@ -477,9 +532,16 @@ pm_status pm_heat_max_stable_dt(pm_heat* hp, double* seconds) {
     Heat* h = reinterpret_cast<Heat*>(hp);
     HEAT_GUARD(h);
     if (!seconds) return fail(PM_BAD_ARG, "null output");
-    if (h->films.exposed && h->any_radiative_film())
-        return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) make the step limit state-dependent; not on the GPU path");
-    double rate = h->worst_rate_now();
+    double rate;
+    if (h->radiating()) {
+        if (h->precision != PM_PLAIN_F64)
+            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) are on the plain f64 form only");
+        pm_status s = h->read_state();  // the rate the last step (or the last change of state) left
+        if (s != PM_OK) return s;
+        rate = h->host_state->rate_now;
+    } else {
+        rate = h->worst_rate_now();
+    }
     *seconds = std::isnan(rate) ? std::numeric_limits<double>::infinity() : 1.0 / rate;  // solid.rs:1709-1715
     return PM_OK;
 }
@@ -496,10 +558,20 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
     HEAT_GUARD(h);
     if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
     if (nsteps == 0) return PM_OK;
-    if (h->films.exposed && h->any_radiative_film())
-        return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) make the step limit state-dependent; not on the GPU path");
+    double rate;
+    if (h->radiating()) {
+        // the limit follows the state: the first step is checked here against the present
+        // state's rate, every later one on the device against the rate its own state gives
+        if (h->precision != PM_PLAIN_F64)
+            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) are on the plain f64 form only");
+        pm_status rs = h->read_state();
+        if (rs != PM_OK) return rs;
+        rate = h->host_state->rate_now;
+    } else {
+        rate = h->worst_rate_now();
+    }
     // solid.rs:1718-1738: the stability refusal, before anything moves.
-    const double ratio = dt * h->worst_rate_now();
+    const double ratio = dt * rate;
     if (std::isnan(ratio)) {
         const double inf = std::numeric_limits<double>::infinity();
         fill_violation(out, "substance has no diffusivity", h->name, inf, inf, inf, 0.0, 1);

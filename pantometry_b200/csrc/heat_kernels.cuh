@@ -27,6 +27,7 @@ __device__ __forceinline__ double powi4(double x) {
     double s = x * x;
     return s * s;
 }
+__device__ __forceinline__ double powi3(double x) { return x * (x * x); }
 
 // solid.rs:110-122
 __device__ __forceinline__ double series_with_half_cell(double film, double conductivity, double area,
@@ -76,6 +77,11 @@ struct HeatPlainArgs {
     double dts, dx, reference;
     HeatFilms films;
     int pairs;  // uniform blocks with rows of an even number of cells: heat_plain_pair_step
+    // Radiating films (some exposed cell with emissivity > 0): the step limit depends on the
+    // state, so each step checks dt against the rate its own state gives (solid.rs:1718-1738) and
+    // gathers the rate of the state it leaves. static_rate: `worst_rate` of `resolve`.
+    int radiating;
+    double static_rate;
     Tiles tiles;
     DevState* st;
     double* partials;
@@ -113,6 +119,94 @@ __device__ __forceinline__ double film_flux(const HeatPlainArgs& a, int i, int j
     return out;
 }
 
+// solid.rs:1269-1288 `loss_conductance_at`: the films' tangent conductance at temperature `at`,
+// h + 4εσ·max(T, T∞)³ per exposed face with the half cell in series, summed from −0.0 as Rust's
+// `Sum for f64` does.
+__device__ __forceinline__ double loss_conductance(const HeatPlainArgs& a, int i, int j, int k, size_t c, double at) {
+    double emissivity, conductivity;
+    if (a.uniform) {
+        emissivity = a.eps_cell;
+        conductivity = a.k_cell;
+    } else {
+        uint32_t m = a.which[c];
+        emissivity = a.mat_eps[m];
+        conductivity = a.mat_k[m];
+    }
+    double total = -0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        if (!((a.films.exposed >> f) & 1)) continue;
+        if (!face_holds(f, i, j, k, a.nx, a.ny, a.nz)) continue;
+        const double share = a.films.share[f];
+        const double hot = fmax(at, a.films.ambient[f]);
+        const double h = a.films.convection[f] + 4.0 * emissivity * kStefanBoltzmann * powi3(hot);
+        total += series_with_half_cell(h * share, conductivity, share, a.dx);
+    }
+    return total;
+}
+
+// One boundary cell's term of `worst_rate_now` (solid.rs:1172-1183) at its new temperature, or
+// −1 where it has no film: mobility·(face_sum + loss/dx), face_sum summed as `resolve` sums it
+// (solid.rs:757-762).
+__device__ __forceinline__ double heat_cell_rate(const HeatPlainArgs& a, int i, int j, int k, size_t c, double t) {
+    const double loss = loss_conductance(a, i, j, k, c, t);
+    if (loss == 0.0) return -1.0;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    double face_sum, mob;
+    if (a.uniform) {
+        const double kf = a.kface;
+        face_sum = ((((((i > 0 && i < nx) ? kf : 0.0) + ((i + 1 < nx) ? kf : 0.0)) + ((j > 0 && j < ny) ? kf : 0.0)) +
+                     ((j + 1 < ny) ? kf : 0.0)) + ((k > 0 && k < nz) ? kf : 0.0)) + ((k + 1 < nz) ? kf : 0.0);
+        mob = a.mobility;
+    } else {
+        const size_t plane = (size_t)nx * ny;
+        const size_t xr = (size_t)(nx + 1) * ((size_t)j + (size_t)ny * k);
+        const size_t yr = (size_t)nx * ((size_t)j + (size_t)(ny + 1) * k);
+        face_sum = ((((a.kx[i + xr] + a.kx[i + 1 + xr]) + a.ky[i + yr]) + a.ky[i + nx + yr]) + a.kz[c]) + a.kz[c + plane];
+        mob = a.mob[c];
+    }
+    return mob * (face_sum + loss / a.dx);
+}
+
+// The refusal a radiating block's step makes before anything moves (solid.rs:1718-1738), against
+// the rate of the state the step starts from. Every block reads the same rate and takes the same
+// decision; block 0 records it.
+__device__ __forceinline__ bool heat_refused(const HeatPlainArgs& a) {
+    if (!a.radiating) return false;
+    DevState* st = a.st;
+    const double ratio = a.dts * st->rate_now;
+    if (!(ratio > 1.0 + 6e-12)) return false;
+    if (blockIdx.x == 0 && linear_tid() == 0) {
+        constexpr double fourier = 1.0 / 6.0;  // solid.rs:84
+        st->violated = kRefused;
+        st->violation_step = st->steps + 1;
+        st->v_before = fourier;
+        st->v_after = ratio * fourier;
+        st->v_scale = fourier;
+        st->v_tol = 1e-12;
+    }
+    return true;
+}
+
+// The block's largest boundary-cell rate into the launch's max, before the block's ticket: a
+// warp tree, then the warps' values, then one integer atomicMax on the bits (every candidate is
+// a non-negative double or −1, which is left out).
+__device__ __forceinline__ void heat_rate_publish(const HeatPlainArgs& a, double r) {
+    __shared__ double wmax[32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, off));
+    const int tid = linear_tid(), lane = tid & 31, warp = tid >> 5;
+    const int nwarps = (blockDim.x * blockDim.y * blockDim.z) >> 5;
+    if (lane == 0) wmax[warp] = r;
+    __syncthreads();
+    if (tid == 0) {
+        double m = -1.0;
+        for (int w = 0; w < nwarps; ++w) m = fmax(m, wmax[w]);
+        if (m >= 0.0) atomicMax(&a.st->rate_bits, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+}
+
 // Decode tile t of a tiling into the thread's column (i, j) and plane range [k0, k1).
 __device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i, int& j, int& k0, int& k1) {
     const int tx = (int)(t % T.ntx);
@@ -139,6 +233,10 @@ __device__ __forceinline__ void heat_plain_books(const HeatPlainArgs& a, double 
         st->part[1] = st->lost;
         st->part[2] = -st->supplied;
         audit_and_commit(st, total, scale);
+        if (a.radiating) {  // worst_rate_now of the state this step leaves (solid.rs:1148-1185)
+            const unsigned long long bits = atomicExch(&st->rate_bits, 0ull);
+            st->rate_now = bits ? fmax(a.static_rate, __longlong_as_double((long long)bits)) : a.static_rate;
+        }
     }
 }
 
@@ -149,10 +247,11 @@ __device__ __forceinline__ void heat_plain_books(const HeatPlainArgs& a, double 
 #define PM_HEAT_PLAIN_MIN_BLOCKS 4
 #endif
 static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_plain_step(HeatPlainArgs a) {
-    if (a.st->violated) return;
+    if (a.st->violated || heat_refused(a)) return;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
     double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
+    double rate = -1.0;          // radiating films: the largest boundary-cell rate of the new state
     for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
         int i, j, k0, k1;
         tile_column(a.tiles, t, i, j, k0, k1);
@@ -189,10 +288,13 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
             a.tnew[c] = nt;
             acc[0] += capc * (nt - a.reference);                  // solid.rs:1583-1590
             if (shed != 0.0) acc[1] += a.dts * mob * shed * capc;  // solid.rs:1821-1823
+            if (a.radiating && (i == 0 || i + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz))
+                rate = fmax(rate, heat_cell_rate(a, i, j, k, c, nt));
             below = here;
             here = above;
         }
     }
+    if (a.radiating) heat_rate_publish(a, rate);
     heat_plain_books(a, acc);
 }
 
@@ -209,12 +311,13 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
 #define PM_HEAT_PAIR_MIN_BLOCKS 4
 #endif
 static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_step(HeatPlainArgs a) {
-    if (a.st->violated) return;
+    if (a.st->violated || heat_refused(a)) return;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
     const double2 zero = make_double2(0.0, 0.0);
     const double kf = a.kface;
     double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
+    double rate = -1.0;          // radiating films: the largest boundary-cell rate of the new state
     for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
         int q, j, k0, k1;
         tile_column(a.tiles, t, q, j, k0, k1);  // q: the pair's place along the row
@@ -249,12 +352,15 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plai
                 nt[e] = t0 + a.dts * a.mobility * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
                 acc[0] += a.capacity * (nt[e] - a.reference);     // solid.rs:1583-1590
                 if (shed != 0.0) acc[1] += a.dts * a.mobility * shed * a.capacity;  // solid.rs:1821-1823
+                if (a.radiating && (i + e == 0 || i + e + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz))
+                    rate = fmax(rate, heat_cell_rate(a, i + e, j, k, c + e, nt[e]));
             }
             *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);
             below = here;
             here = above;
         }
     }
+    if (a.radiating) heat_rate_publish(a, rate);
     heat_plain_books(a, acc);
 }
 

@@ -13,6 +13,7 @@
 #include "yee_tma.cuh"
 #include "room_kernels.cuh"
 #include "ens_tma.cuh"
+#include "yee_near.cuh"
 
 namespace pm {
 
@@ -102,6 +103,10 @@ inline size_t yee_tma_smem_bytes(bool media = false) {
     return media ? yee_tma_smem_bytes_for<kYeeTmaPlanesMedia, true>(kYeeTmaStages)
                  : yee_tma_smem_bytes_for<kYeeTmaPlanesUniform, false>(kYeeTmaStages);
 }
+// The FP32 cavity's near-field box in f64 after the TMA step (yee_near.cuh), and its seeding from
+// the stored field.
+cudaError_t launch_yee_near(const YeeNearArgs& a, bool solid, cudaStream_t s);
+cudaError_t launch_yee_near_seed(const YeeNearArgs& a, cudaStream_t s);
 // One component between the reference layout and the padded lattice (see yee_relayout);
 // src_f64 / dst_f64 select double or float for each side.
 cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool dst_f64, int ex, int ey, int ez,

@@ -152,6 +152,7 @@ pm_status Handle::begin_call() {
     host_state->violation_step = 0;
     host_state->tol = tolerance;
     host_state->counter = 0u;
+    host_state->rate_bits = 0ull;
     call_parity = parity;
     return write_state();
 }
@@ -167,6 +168,12 @@ pm_status Handle::finish_call(long long steps_before, pm_violation* out, const s
     if (host_state->violated == kDeviceTimeout)
         return fail(PM_DEVICE_TIMEOUT, "a bounded wait inside a " + name + " kernel ran out; the call stopped");
     const long long at = host_state->violation_step - steps_before;
+    if (host_state->violated == kRefused) {  // solid.rs:1718-1738, decided on the device
+        fill_violation(out, "Fourier number", refusal_site, host_state->v_before, host_state->v_after, host_state->v_scale,
+                       host_state->v_tol, at);
+        set_error("Fourier number past the explicit limit");
+        return PM_VIOLATION;
+    }
     if (host_state->violated == kStartupFailed)
         fill_violation(out, "energy", startup_site, host_state->v_before, host_state->v_after, host_state->v_scale,
                        host_state->v_tol, at);

@@ -62,6 +62,7 @@ struct Handle {
     DBuf partials;   // per-block partial sums
     DevState* host_state = nullptr;  // pinned mirror
     double tolerance = -1.0;         // no audit: plain `Domain::step`; set one to audit every step
+    std::string refusal_site;        // where a step refused on the device (kRefused) is reported
     unsigned resident = 148 * kBlocksPerSM;  // upper bound of any persistent grid (partials sizing)
     unsigned sm_count = 148;
     unsigned wave_of(KernelId id) const { return sm_count * (unsigned)blocks_per_sm(id); }

@@ -378,6 +378,10 @@ struct YeeStepArgs {
     const Real* __restrict__ cdecay[3];
     const Real* __restrict__ cch[3];
     int lossless, mu_var;
+    // FP32 TMA form only: a box of nb_w³ lattice nodes from (nb_x0, nb_y0, nb_z0) whose six
+    // components are stepped in f64 by yee_near_step after this kernel; the kernel leaves the
+    // box's energy terms to it and hands it its sums instead of closing the books. nb_w = 0: none.
+    int nb_x0, nb_y0, nb_z0, nb_w;
 };
 
 // The per-edge and per-face coefficients of one dt for a cavity of mixed media, exactly the values

@@ -1,0 +1,227 @@
+// The near field of an FP32 cavity's soft current, kept in f64.
+//
+// Why. A soft current drives the field at its edge up and down with every cycle of the pulse, and
+// what flows in and out of the edge and its neighbours is many times the net work the source does.
+// Stored in f32, those values are rounded on every step while that flow passes through them, and
+// the ledger (invariant − work) ends a few 1e-6 of the injected energy away from the f64 run's. A
+// numpy emulation of the scheme shows where it comes from: with the six components of a 5³ box of
+// lattice nodes around the source kept in f64 (every stencil reading the stored values), the same
+// run ends 1e-9 away, against 2e-6 with the whole field in f32.
+//
+// The rule, in one line: inside the box every value is f64, outside it f32, and every stencil reads
+// what is stored. yee_tma_step steps every node in f32 from the stored values (the box's f32
+// roundings included) but leaves the box's energy terms out and the source to this kernel, and
+// hands over its four sums. This kernel (one block, after it, before the walls) then
+//   A. forms H⁺ of the box's faces in f64 from the box's f64 H and E (f32 values outside),
+//   B. forms Eⁿ⁺¹ of the box's edges in f64 from those H⁺ (f32 H⁺ outside), with the source,
+//   C. forms again, in f32, the edges just outside the box whose curl reads a box face, so they
+//      read the f32 rounding of the box's f64 H⁺ (the value stored there) and not the f32 value
+//      yee_tma_step formed,
+//   D. adds the box's energy terms, Joule loss and source work in f64 and closes the books with
+//      yee_tma_close, as yee_tma_step does for a cavity without a box.
+// The box and the ring of C lie inside the walls (one node from them at least), so every
+// component exists at every node they hold, every edge is interior and no wall kernel touches it.
+//
+// The arithmetic of A and B is cavity.rs:1346-1452 with the uniform medium's f64 coefficients (or
+// each edge's own f32 gain with MEDIA, the coefficient the update and the energy weight use), the
+// soft current as in yee_tma_step.
+#pragma once
+
+#include "yee_tma.cuh"
+
+namespace pm {
+
+struct YeeNearArgs {
+    const float* old[6];    // ex ey ez hx hy hz at step n, padded lattice
+    float* neu[6];          // at n + 1, already stepped by yee_tma_step
+    const double* nold;     // the box's f64 values at step n: [q][lk][lj][li], w³ per component
+    double* nneu;           // at n + 1
+    int x0, y0, z0, w;      // the box: w³ lattice nodes from (x0, y0, z0)
+    unsigned L, ny1;        // lattice row pitch and rows per plane
+    int nx, ny, nz;
+    double ch, gain, decay;  // f64 coefficients of one medium: g/μ, edge gain and decay
+    float chf, gainf, decf;  // the f32 ones yee_tma_step used (the ring's edges)
+    const float* cgain[3];   // MEDIA: per-edge gains on the padded lattice
+    int media, lossy;
+    double sig0;
+    const uint8_t* solid;
+    int src_i, src_j, src_k;
+    const double* current;
+    long long ncurrent;
+    double eps_src, sig_src, dt, volume, g, eps_u, mu_u;
+    DevState* st;
+};
+
+__device__ __forceinline__ bool near_in(const YeeNearArgs& a, int i, int j, int k) {
+    return (unsigned)(i - a.x0) < (unsigned)a.w && (unsigned)(j - a.y0) < (unsigned)a.w &&
+           (unsigned)(k - a.z0) < (unsigned)a.w;
+}
+__device__ __forceinline__ size_t near_lat(const YeeNearArgs& a, int i, int j, int k) {
+    return (size_t)i + (size_t)a.L * ((size_t)j + (size_t)a.ny1 * (size_t)k);
+}
+__device__ __forceinline__ size_t near_box(const YeeNearArgs& a, int q, int i, int j, int k) {
+    const size_t w = (size_t)a.w;
+    return (size_t)q * w * w * w + (size_t)(i - a.x0) + w * ((size_t)(j - a.y0) + w * (size_t)(k - a.z0));
+}
+// The stored value of component q at node (i, j, k): f64 in the box, f32 outside.
+__device__ __forceinline__ double near_get(const YeeNearArgs& a, const double* box, const float* const* lat, int q,
+                                           int i, int j, int k) {
+    return near_in(a, i, j, k) ? box[near_box(a, q, i, j, k)] : (double)lat[q][near_lat(a, i, j, k)];
+}
+
+// Seed the box's f64 values from the stored f32 field (after the state was set from outside a step).
+static __global__ void yee_near_seed(YeeNearArgs a) {
+    const int w = a.w, w3 = w * w * w;
+    for (int r = threadIdx.x; r < 6 * w3; r += blockDim.x) {
+        const int q = r / w3, l = r - q * w3;
+        const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
+        a.nneu[r] = (double)a.neu[q][near_lat(a, i, j, k)];
+    }
+}
+
+template <bool SOLID>
+static __global__ void __launch_bounds__(256) yee_near_step(YeeNearArgs a) {
+    DevState* st = a.st;
+    if (st->violated) return;
+    const int w = a.w, w3 = w * w * w;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const long long step = st->steps;
+    const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const float* const* lat_old = a.old;
+    const float* const* lat_neu = const_cast<const float* const*>(a.neu);
+
+    // A. H⁺ on the box's faces (cavity.rs:1346-1379), and the box's energy terms: ½ε|Eⁿ|² with
+    // the half weights of node-centred boundary samples (cavity.rs:766-772), ½μ H⁻·H⁺
+    for (int l = threadIdx.x; l < w3; l += blockDim.x) {
+        const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
+        const double hi = (i == 0 || i == nx) ? 0.5 : 1.0, hj = (j == 0 || j == ny) ? 0.5 : 1.0,
+                     hk = (k == 0 || k == nz) ? 0.5 : 1.0;
+        const double ex0 = a.nold[near_box(a, 0, i, j, k)], ey0 = a.nold[near_box(a, 1, i, j, k)],
+                     ez0 = a.nold[near_box(a, 2, i, j, k)];
+        const double wx = a.nold[near_box(a, 3, i, j, k)], wy = a.nold[near_box(a, 4, i, j, k)],
+                     wz = a.nold[near_box(a, 5, i, j, k)];
+        const double hxn = wx - a.ch * ((near_get(a, a.nold, lat_old, 2, i, j + 1, k) - ez0) -
+                                        (near_get(a, a.nold, lat_old, 1, i, j, k + 1) - ey0));
+        const double hyn = wy - a.ch * ((near_get(a, a.nold, lat_old, 0, i, j, k + 1) - ex0) -
+                                        (near_get(a, a.nold, lat_old, 2, i + 1, j, k) - ez0));
+        const double hzn = wz - a.ch * ((near_get(a, a.nold, lat_old, 1, i + 1, j, k) - ey0) -
+                                        (near_get(a, a.nold, lat_old, 0, i, j + 1, k) - ex0));
+        const size_t n = near_lat(a, i, j, k);
+        a.nneu[near_box(a, 3, i, j, k)] = hxn;
+        a.nneu[near_box(a, 4, i, j, k)] = hyn;
+        a.nneu[near_box(a, 5, i, j, k)] = hzn;
+        a.neu[3][n] = (float)hxn;
+        a.neu[4][n] = (float)hyn;
+        a.neu[5][n] = (float)hzn;
+        acc[1] += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
+        if (a.media)  // weighted by 1/g, the ε the update uses
+            acc[0] += (hj * hk) * (ex0 * ex0) / (double)a.cgain[0][n] + (hi * hk) * (ey0 * ey0) / (double)a.cgain[1][n] +
+                      (hi * hj) * (ez0 * ez0) / (double)a.cgain[2][n];
+        else
+            acc[0] += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+    }
+    __syncthreads();  // the box's H⁺, in both stores, before any edge reads it
+
+    // B. Eⁿ⁺¹ on the box's edges (cavity.rs:1383-1452), the soft current, Joule loss
+    for (int l = threadIdx.x; l < w3; l += blockDim.x) {
+        const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
+        const size_t n = near_lat(a, i, j, k);
+        auto hp = [&](int q, int ii, int jj, int kk) { return near_get(a, a.nneu, lat_neu, q, ii, jj, kk); };
+        const double cex = (hp(5, i, j, k) - hp(5, i, j - 1, k)) - (hp(4, i, j, k) - hp(4, i, j, k - 1));
+        const double cey = (hp(3, i, j, k) - hp(3, i, j, k - 1)) - (hp(5, i, j, k) - hp(5, i - 1, j, k));
+        const double cez = (hp(4, i, j, k) - hp(4, i - 1, j, k)) - (hp(3, i, j, k) - hp(3, i, j - 1, k));
+        const double ex0 = a.nold[near_box(a, 0, i, j, k)], ey0 = a.nold[near_box(a, 1, i, j, k)],
+                     ez0 = a.nold[near_box(a, 2, i, j, k)];
+        double gx = a.gain, gy = a.gain, gz = a.gain;
+        if (a.media) {
+            gx = (double)a.cgain[0][n];
+            gy = (double)a.cgain[1][n];
+            gz = (double)a.cgain[2][n];
+        }
+        double vx = a.decay * ex0 + gx * cex;
+        double vy = a.decay * ey0 + gy * cey;
+        double vz = a.decay * ez0 + gz * cez;
+        if (i == a.src_i && j == a.src_j && k == a.src_k) {
+            // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
+            const double e = a.eps_src, ss = a.sig_src;
+            vz = vz - (a.dt / e) / (1.0 + (ss * a.dt / (2.0 * e))) * jsrc;
+            acc[3] += -(a.dt * a.volume) * jsrc * (0.5 * (ez0 + vz));
+        }
+        const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
+        const bool lx = iy && iz, ly = ix && iz, lz = ix && iy;
+        vx = lx ? vx : 0.0;
+        vy = ly ? vy : 0.0;
+        vz = lz ? vz : 0.0;
+        if (a.lossy) {
+            const double mx = 0.5 * (ex0 + vx), my = 0.5 * (ey0 + vy), mz = 0.5 * (ez0 + vz);
+            acc[2] += lx ? a.sig0 * mx * mx * a.dt * a.volume : 0.0;
+            acc[2] += ly ? a.sig0 * my * my * a.dt * a.volume : 0.0;
+            acc[2] += lz ? a.sig0 * mz * mz * a.dt * a.volume : 0.0;
+        }
+        if constexpr (SOLID) {
+            if (touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) vx = 0.0;
+            if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) vy = 0.0;
+            if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) vz = 0.0;
+        }
+        a.nneu[near_box(a, 0, i, j, k)] = vx;
+        a.nneu[near_box(a, 1, i, j, k)] = vy;
+        a.nneu[near_box(a, 2, i, j, k)] = vz;
+        a.neu[0][n] = (float)vx;
+        a.neu[1][n] = (float)vy;
+        a.neu[2][n] = (float)vz;
+    }
+
+    // C. The edges just outside the box whose curl reads a box face: the nodes of the (w+1)³ cube
+    // that are not in the box, on its high sides. Each is formed again in f32 from the stored H⁺
+    // (the box's own faces now hold the roundings of their f64 values), as yee_tma_step forms it;
+    // with a lossy medium the Joule term yee_tma_step booked for it is replaced by this value's.
+    const int w1 = w + 1, ring = w1 * w1 * w1;
+    for (int l = threadIdx.x; l < ring; l += blockDim.x) {
+        const int i = a.x0 + l % w1, j = a.y0 + (l / w1) % w1, k = a.z0 + l / (w1 * w1);
+        if (near_in(a, i, j, k)) continue;
+        const size_t n = near_lat(a, i, j, k);
+        auto h = [&](int q, int ii, int jj, int kk) { return lat_neu[q][near_lat(a, ii, jj, kk)]; };
+        const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
+        for (int q = 0; q < 3; ++q) {
+            // which faces the curl of component q reads besides the node's own: x reads j−1 and
+            // k−1, y reads k−1 and i−1, z reads i−1 and j−1
+            const bool reads = q == 0   ? (near_in(a, i, j - 1, k) || near_in(a, i, j, k - 1))
+                               : q == 1 ? (near_in(a, i, j, k - 1) || near_in(a, i - 1, j, k))
+                                        : (near_in(a, i - 1, j, k) || near_in(a, i, j - 1, k));
+            if (!reads) continue;
+            const float before = a.old[q][n];
+            float curl;
+            if (q == 0) curl = (h(5, i, j, k) - h(5, i, j - 1, k)) - (h(4, i, j, k) - h(4, i, j, k - 1));
+            else if (q == 1) curl = (h(3, i, j, k) - h(3, i, j, k - 1)) - (h(5, i, j, k) - h(5, i - 1, j, k));
+            else curl = (h(4, i, j, k) - h(4, i - 1, j, k)) - (h(3, i, j, k) - h(3, i, j - 1, k));
+            const float gq = a.media ? a.cgain[q][n] : a.gainf;
+            float v = a.decf * before + gq * curl;
+            const bool interior = q == 0 ? (iy && iz) : q == 1 ? (ix && iz) : (ix && iy);
+            v = interior ? v : 0.0f;
+            if (a.lossy && interior) {
+                const double mold = 0.5 * ((double)before + (double)a.neu[q][n]);
+                const double mnew = 0.5 * ((double)before + (double)v);
+                acc[2] += a.sig0 * mnew * mnew * a.dt * a.volume - a.sig0 * mold * mold * a.dt * a.volume;
+            }
+            if constexpr (SOLID) {
+                const bool hit = q == 0   ? touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)
+                                 : q == 1 ? touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)
+                                          : touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k);
+                if (hit) v = 0.0f;
+            }
+            a.neu[q][n] = v;
+        }
+    }
+
+    // D. the box's sums in a fixed order, added to yee_tma_step's, and the books
+    __shared__ double red[32 * 4];
+    block_sum<4>(acc, red);
+    if (threadIdx.x == 0) {
+        double total[4];
+        for (int q = 0; q < 4; ++q) total[q] = st->near_acc[q] + acc[q];
+        yee_tma_close(st, total, a.media != 0, a.g, a.eps_u, a.mu_u, a.volume, a.src_i >= 0);
+    }
+}
+
+}  // namespace pm

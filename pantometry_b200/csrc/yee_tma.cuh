@@ -104,6 +104,29 @@ __device__ __forceinline__ void yee_tma_issue(const YeeMaps& m, unsigned stage, 
     }
 }
 
+// The books of one FP32 cavity step from its four sums (Σ w|Eⁿ|² or, with MEDIA, Σ w|Eⁿ|²/g;
+// Σ w H⁺·H⁻; Joule loss; source work): the invariant, the running books, the ledger
+// (cavity.rs:1520-1524) and the audit. Run by one thread.
+__device__ __forceinline__ void yee_tma_close(DevState* st, const double (&acc)[4], bool media, double g, double eps_u,
+                                              double mu_u, double v, bool with_source) {
+    // cavity.rs:846; with MEDIA the terms are already weighted by 1/g = ε Δx/Δt
+    const double electric = media ? 0.5 * (g * acc[0]) * v : 0.5 * (eps_u * acc[0]) * v;
+    const double paired = 0.5 * v * (mu_u * acc[1]);  // cavity.rs:885-904
+    st->invariant = electric + paired;
+    st->has_invariant = 1;
+    st->dissipated += fmax(acc[2], 0.0);
+    st->work_booked = st->work;
+    st->work += acc[3];
+    double total = 0.0, scale = 0.0;
+    ledger_add(total, scale, st->invariant);
+    ledger_add(total, scale, st->dissipated);
+    if (with_source) ledger_add(total, scale, -st->work_booked);
+    st->part[0] = st->invariant;
+    st->part[1] = st->dissipated;
+    st->part[2] = -st->work_booked;
+    audit_and_commit(st, total, scale);
+}
+
 template <int P, int S, bool SOLID, bool MEDIA>
 static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m) {
@@ -178,6 +201,8 @@ static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeSte
         const bool in_x = i <= nx, in_y = j <= ny;
         // node-centred half weights of the boundary samples (cavity.rs:766-772)
         const float hi = (i == 0 || i == nx) ? 0.5f : 1.0f, hj = (j == 0 || j == ny) ? 0.5f : 1.0f;
+        // the column crosses the f64 near-field box (nb_w = 0: no box, never)
+        const bool box_xy = (unsigned)(i - a.nb_x0) < (unsigned)a.nb_w && (unsigned)(j - a.nb_y0) < (unsigned)a.nb_w;
         float es = 0.0f, ms = 0.0f;  // this stage's w|E|² and w H⁺·H⁻ of the thread's cells
 #pragma unroll 1
         for (int h = 0; h < P; ++h) {
@@ -186,6 +211,8 @@ static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeSte
             const bool compute = k >= cc.k0;  // else the plane below the chunk: H⁺ only
             const bool zin = k < nz;
             const float hk = (k == 0 || k == nz) ? 0.5f : 1.0f;
+            // a node of the near-field box: its energy terms are the box kernel's, in f64
+            const bool inbox = box_xy && (unsigned)(k - a.nb_z0) < (unsigned)a.nb_w;
             const unsigned n = (unsigned)i + L * ((unsigned)j + ny1 * (unsigned)k);
             // the gains of the thread's own edges; at a position the component does not have (the
             // padding, or the fill outside the lattice) the uniform gain, never read as a value
@@ -214,12 +241,14 @@ static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeSte
                 // mask is needed: at a lattice position a component does not have, its old value
                 // (padding, or the fill outside the lattice) is exactly zero, so its E term and
                 // its H⁻·H⁺ term are zero.
-                ms += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
-                if constexpr (MEDIA)  // 1/g to within 2 ulp: the terms are f32 roundings already
-                    es += __fdividef((hj * hk) * (ex0 * ex0), gx) + __fdividef((hi * hk) * (ey0 * ey0), gy) +
-                          __fdividef((hi * hj) * (ez0 * ez0), gz);
-                else
-                    es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+                if (!inbox) {
+                    ms += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
+                    if constexpr (MEDIA)  // 1/g to within 2 ulp: the terms are f32 roundings already
+                        es += __fdividef((hj * hk) * (ex0 * ex0), gx) + __fdividef((hi * hk) * (ey0 * ey0), gy) +
+                              __fdividef((hi * hj) * (ez0 * ez0), gz);
+                    else
+                        es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+                }
                 // halo faces, one line per warp so the barrier waits on no warp doing twice the
                 // work: the y0 − 1 row of hx (warp 7) and of hz (warp 6), the x0 − 1 column of hz
                 // (warp 5, rows y0 − 1 .. y0 + 7) and of hy (warp 4, rows y0 .. y0 + 7)
@@ -256,7 +285,7 @@ static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeSte
                 vx = lx ? vx : 0.0f;
                 vy = ly ? vy : 0.0f;
                 vz = lz ? vz : 0.0f;
-                if (lossy) {
+                if (lossy && !inbox) {
                     const double mx = 0.5 * ((double)ex0 + (double)vx), my = 0.5 * ((double)ey0 + (double)vy),
                                  mz = 0.5 * ((double)ez0 + (double)vz);
                     acc[2] += (lx && i < nx && in_y) ? sig0 * mx * mx * dt * a.volume : 0.0;
@@ -291,23 +320,11 @@ static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeSte
         return;
     }
     if (finish_blocks<4>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
-        const double v = a.volume;
-        // cavity.rs:846; with MEDIA the terms are already weighted by 1/g = ε Δx/Δt
-        const double electric = MEDIA ? 0.5 * (a.g * acc[0]) * v : 0.5 * (a.eps_u * acc[0]) * v;
-        const double paired = 0.5 * v * (a.mu_u * acc[1]);     // cavity.rs:885-904
-        st->invariant = electric + paired;
-        st->has_invariant = 1;
-        st->dissipated += fmax(acc[2], 0.0);
-        st->work_booked = st->work;
-        st->work += acc[3];
-        double total = 0.0, scale = 0.0;
-        ledger_add(total, scale, st->invariant);
-        ledger_add(total, scale, st->dissipated);
-        if (a.src_i >= 0) ledger_add(total, scale, -st->work_booked);
-        st->part[0] = st->invariant;
-        st->part[1] = st->dissipated;
-        st->part[2] = -st->work_booked;
-        audit_and_commit(st, total, scale);
+        if (a.nb_w > 0) {  // the near-field box kernel adds its terms and closes the books
+            for (int q = 0; q < 4; ++q) st->near_acc[q] = acc[q];
+        } else {
+            yee_tma_close(st, acc, MEDIA, a.g, a.eps_u, a.mu_u, a.volume, a.src_i >= 0);
+        }
     }
 }
 

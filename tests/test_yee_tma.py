@@ -145,25 +145,79 @@ def test_yee_upload_starts_fresh_books(precision):
             assert np.abs(fo[k] - runs[1][0][k]).max() <= 1e-4 * scale[k[0]], k
 
 
-def test_yee_f32_books_hold_after_the_source():
-    """The FP32 cavity's books against the soft current: f32 storage rounds the field at the source
-    edge and its neighbours while the pulse pumps energy in and out there, which leaves the ledger a
-    few 1e-6 of the injected energy off (an f32 emulation of the scheme gives the same; f32
-    coefficients alone give 2e-8). Once the pulse has passed the books must hold: no drift."""
-    from pantometry_b200 import workloads as W
-    from pantometry_b200.domains import Cavity
+def _ledger_gap(runs, dt, calls, every):
+    """Step the FP32 and f64 cavities side by side `every` steps at a time and return the worst
+    |L32 − L64| / scale64 over the comparisons (scale: the f64 ledger's largest entry then)."""
+    worst = 0.0
+    for _ in range(calls):
+        for c in runs.values():
+            assert c.step(dt, every) is None
+        a, b = runs["f32"].ledger(), runs["f64"].ledger()
+        worst = max(worst, abs(a["total"] - b["total"]) / b["scale"])
+    return worst
 
-    n = 48
-    cfg = W.yee_cavity(n, steps=1600)
-    g = Cavity((n, n, n), cfg["dx"], precision="f32")
-    g.set_source(cfg["edge"], cfg["current"])
-    g.set_tolerance(1e-5)
-    assert g.step(cfg["dt"], 300) is None  # the pulse is over by about step 180
-    a = g.ledger()
-    assert g.step(cfg["dt"], 1200) is None
-    b = g.ledger()
-    assert abs(a["total"]) < 5e-5 * a["scale"]
-    assert abs(b["total"] - a["total"]) < 2e-7 * b["scale"]
+
+def test_yee_f32_ledger_within_1e6_of_f64_over_10000_steps():
+    """The FP32 cavity driven by the soft dipole current. The source's near field (a 5³ box of
+    lattice nodes around the source edge) is kept in f64 by the box kernel, so the ledger stays
+    within 1e-6 of the f64 run's, compared every 10 steps over 10 000 steps and audited at 1e-6
+    every step. With the whole field in f32 the same run ends a few 1e-6 away."""
+    from pantometry_b200 import workloads as W
+
+    n = 64
+    cfg = W.yee_cavity(n, steps=10000)
+    runs = {p: W.build_cavity(cfg, precision=p) for p in ("f32", "f64")}
+    runs["f32"].set_tolerance(1e-6)
+    assert _ledger_gap(runs, cfg["dt"], 1000, 10) <= 1e-6
+
+
+def test_yee_f32_dielectric_source_ledger_within_1e6_of_f64():
+    """The same with per-cell ε (ε_r in [1, 4] in 10% of the cells): the box's edges use their own
+    f32 gains, as the update does, and weigh their energy by them."""
+    from pantometry_b200 import workloads as W
+
+    cfg = W.dielectric_cavities(count=1, n=40, steps=3000)
+    runs = {p: W.build_dielectric_cavity(cfg, 0, precision=p) for p in ("f32", "f64")}
+    runs["f32"].set_tolerance(1e-6)
+    assert _ledger_gap(runs, cfg["dt"], 300, 10) <= 1e-6
+
+
+def test_yee_f32_near_field_checkpoint_restore_is_exact():
+    """The box's f64 values and the source's clock are part of the state: a checkpoint taken during
+    the pulse and restored gives the same fields and books bit for bit on the second run."""
+    from pantometry_b200 import workloads as W
+
+    cfg = W.yee_cavity(32, steps=400)
+    g = W.build_cavity(cfg, precision="f32")
+    assert g.step(cfg["dt"], 70) is None
+    g.checkpoint()
+    runs = []
+    for _ in range(2):
+        assert g.step(cfg["dt"], 90) is None  # a graph of 64 steps and single launches
+        runs.append((g.fields(), g.ledger()))
+        g.restore()
+        g.checkpoint()
+    (fa, la), (fb, lb) = runs
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
+    assert la["total"] == lb["total"] and la["parts"] == lb["parts"]
+
+
+def test_yee_f32_source_near_a_wall_keeps_the_plain_form():
+    """A source too close to a wall for the box (it must lie a node inside the walls with the ring
+    of edges on its high sides) steps in plain FP32 and still matches the oracle."""
+    counts, dx = (12, 10, 9), 1e-3
+    nx, ny, nz = counts
+    edge = 2 + (nx + 1) * (5 + (ny + 1) * 4)  # Ez at node (2, 5, 4): the box would reach node 0
+    o0 = oracle.Yee(counts, dx)
+    dt = 0.9 * o0.courant_limit()
+    t = (np.arange(200) + 0.5) * dt
+    cur = 1e6 * np.exp(-((t - 40 * dt) / (10 * dt)) ** 2) * np.sin(2 * math.pi * t / (20 * dt))
+    o, g = cavity_pair(counts, dx, source=(edge, cur), precision="f32")
+    assert o.advance(dt, 200, tol=1e-9) is None
+    g.set_tolerance(1e-4)
+    assert g.step(dt, 200) is None
+    assert field_err(o.fields(), g.fields()) < 1e-4
 
 
 def test_yee_f32_invariant_against_f64_over_2000_steps():
