@@ -8,9 +8,10 @@ audited at the scene's conservation tolerance (`audit_with`,
 crates/pantometry-core/src/conserved.rs:323-363).
 
 A scene is a dict with the keys of the reference's scene files (`schedule`, `duration_s`, `frames`,
-`conservation_tolerance`, `domains`) holding one domain of kind "block", "hall", "room" or
-"cavity", with the keys the world reads for it (lib.rs:1405-1430, 1786-1812, 1876-1960,
-2192-2350). `build` makes the GPU domain, with the initial fields generated here on the host;
+`conservation_tolerance`, `domains`) holding one domain of kind "block" (of the catalogue's
+aluminium and borosilicate, with regions and a hot spot), "hall", "room" (released in a mode or
+from a pulse) or "cavity", with the keys the world reads for it (lib.rs:1405-1433, 1786-1812,
+1876-1960, 2192-2350). `build` makes the GPU domain, with the initial fields generated here on the host;
 `run` runs any domain object with `step`, `ledger` and `max_stable_dt` (or `courant_limit`).
 """
 from __future__ import annotations
@@ -21,8 +22,12 @@ import numpy as np
 
 from .domains import Cavity, Hall, Room, Solid3D
 
-# substance.rs:362-373 (`Substance::aluminium_6061`; g/cm³ × 1e3, units lib.rs:751-753)
+# substance.rs:362-373 (`Substance::aluminium_6061`; g/cm³ × 1e3, units lib.rs:751-753) and
+# substance.rs:336-347 (`Substance::borosilicate_crown`), the catalogue names a scene gives them
+# (substance.rs:318-319)
 ALUMINIUM_6061 = dict(density=2.70 * 1e3, conductivity=167.0, specific_heat=896.0, emissivity=0.09)
+BOROSILICATE_CROWN = dict(density=2.51 * 1e3, conductivity=1.114, specific_heat=858.0, emissivity=0.90)
+MATERIALS = {"aluminium": ALUMINIUM_6061, "borosilicate": BOROSILICATE_CROWN}
 AIR = dict(speed=343.0, density=1.204)  # hall.rs:139-152, room.rs:122-138
 
 
@@ -64,6 +69,50 @@ def room_mode_profile(cells, dx, mode, amplitude):
     return (amplitude * px[None, :] * py[:, None]).reshape(-1)
 
 
+def room_pulse_profile(cells, dx, x_m, y_m, radius_m, amplitude):
+    """A room released from a Gaussian pulse (lib.rs:1424-1433): a·exp(−|r − c|²/R²) at the nodes
+    (`Room::released_from` samples x = i·dx, y = j·dx, room.rs:140-147)."""
+    nx, ny = cells
+    r = max(radius_m, 1e-9)
+    x = np.arange(nx) * dx - x_m
+    y = np.arange(ny) * dx - y_m
+    d2 = x[None, :] * x[None, :] + y[:, None] * y[:, None]
+    return (amplitude * np.exp(-d2 / (r * r))).reshape(-1)
+
+
+def room_release(cells, dx, rel):
+    """The pressure a room is released with: a mode or a pulse (lib.rs:1418-1433)."""
+    if rel.get("as") == "mode":
+        return room_mode_profile(cells, dx, (rel["nx"], rel["ny"]), rel["amplitude_pa"])
+    if rel.get("as") == "pulse":
+        return room_pulse_profile(cells, dx, rel["x_m"], rel["y_m"], rel["radius_m"], rel["amplitude_pa"])
+    raise ValueError(f"room release {rel.get('as')!r}")
+
+
+def block_layout(d):
+    """A block's bulk material, its regions' fills in order (later wins where they overlap) and its
+    initial kelvin per cell (x fastest): the world's block construction (lib.rs:2192-2350) for
+    regions of catalogue materials, region temperatures and a hot spot."""
+    counts = tuple(d["cells"])
+    bulk = MATERIALS[d.get("material", "aluminium")]
+    k, j, i = np.indices(counts[::-1]).reshape(3, -1)
+    t = np.full(int(np.prod(counts)), celsius(d["initial_c"]))
+    fills = []
+    for r in d.get("regions", []):
+        if r["material"] not in MATERIALS:
+            raise ValueError(f"region material {r['material']!r}: the catalogue's aluminium and borosilicate only")
+        lo, hi = r["from"], r["to"]
+        inside = (i >= lo[0]) & (i < hi[0]) & (j >= lo[1]) & (j < hi[1]) & (k >= lo[2]) & (k < hi[2])
+        fills.append((inside.astype(np.uint8), MATERIALS[r["material"]]))
+        if r.get("initial_c") is not None:
+            t[inside] = celsius(r["initial_c"])
+    spot = d.get("hot_spot")
+    if spot:
+        si, sj, sk = spot["at"]
+        t[si + counts[0] * (sj + counts[1] * sk)] = celsius(d["initial_c"] + spot["above_k"])
+    return bulk, fills, t
+
+
 def window(scene):
     return scene["duration_s"] / scene["frames"]
 
@@ -77,19 +126,16 @@ def build(scene, precision="f64", device=0):
     d = scene["domains"][0]
     kind = d["kind"]
     if kind == "block":  # lib.rs:2192-2350
-        if d.get("material", "aluminium") != "aluminium":
-            raise ValueError("blocks of aluminium (the world's default material) only")
-        m = ALUMINIUM_6061
+        if d.get("cooling") or d.get("parts"):
+            raise ValueError("blocks without cooling films or voxelised parts only")
+        m, fills, t = block_layout(d)
         counts = tuple(d["cells"])
         dom = Solid3D(counts, d["cell_mm"] * 1e-3, m["density"], m["conductivity"], m["specific_heat"],
                       celsius(d["initial_c"]), emissivity=m["emissivity"], precision=precision, name=d["name"],
                       device=device)
-        spot = d.get("hot_spot")
-        if spot:
-            t = np.full(dom.n, celsius(d["initial_c"]))
-            i, j, k = spot["at"]
-            t[i + counts[0] * (j + counts[1] * k)] = celsius(d["initial_c"] + spot["above_k"])
-            dom.cells = t
+        for mask, sub in fills:
+            dom.fill(mask, sub["density"], sub["conductivity"], sub["specific_heat"], sub["emissivity"])
+        dom.cells = t
         return dom
     if kind == "hall":  # lib.rs:1786-1812
         dom = Hall(d["width_m"], d["height_m"], d["depth_m"], d["nodes_across"], AIR["speed"], AIR["density"],
@@ -98,11 +144,9 @@ def build(scene, precision="f64", device=0):
         return dom
     if kind == "room":  # lib.rs:1405-1430
         rel = d["release"]
-        if rel.get("as") != "mode":
-            raise ValueError("rooms released in a mode only")
         dom = Room(d["width_m"], d["height_m"], d["cells_across"], 1.0, AIR["density"], AIR["speed"],
                    precision=precision, name=d["name"], device=device)
-        dom.release(room_mode_profile(dom.cells, dom.dx, (rel["nx"], rel["ny"]), rel["amplitude_pa"]))
+        dom.release(room_release(dom.cells, dom.dx, rel))
         return dom
     if kind == "cavity":  # lib.rs:1876-1960, 3144-3149
         if d.get("medium", "vacuum") != "vacuum":

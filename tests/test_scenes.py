@@ -2,49 +2,36 @@
 (crates/pantometry-world/src/lib.rs:3204-3215) under the multirate schedule, through
 `pantometry_b200.scenes`.
 
-The scenes are the reference's own, their parameters restated below from
-crates/pantometry-world/scenes/{15,16,27,01}-*.json. The oracle's domains must hold each scene's
-conservation tolerance across every window; the GPU's plain f64 domains must reproduce the oracle's
-frames (the same substeps, the same ledgers to 1e-12, the final state bit for bit); the FP32 forms
-must hold the scenes whose tolerance is an FP32 one (1e-6).
+The scenes are the reference's own files, read into tests/golden/scenes.json by
+tests/golden/make_scenes.py (each entry names the file it came from). The oracle's domains must
+hold each scene's conservation tolerance across every window; the GPU's plain f64 domains must
+reproduce the oracle's frames (the same substeps, the same ledgers to 1e-12, the final state bit
+for bit); the FP32 forms must hold the scenes whose tolerance is an FP32 one (1e-6).
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
 import oracle
 from pantometry_b200 import scenes as S
 
-SCENES = {
-    # scenes/15-a-hot-spot-in-a-block.json
-    "block": {"schedule": "multirate", "duration_s": 0.006, "frames": 11, "conservation_tolerance": 1e-9,
-              "domains": [{"kind": "block", "name": "block", "cells": [9, 9, 9], "cell_mm": 1.0, "initial_c": 20.0,
-                           "hot_spot": {"at": [4, 4, 4], "above_k": 60.0}}]},
-    # scenes/16-a-room-with-a-ceiling.json
-    "hall": {"schedule": "multirate", "duration_s": 0.02, "frames": 11, "conservation_tolerance": 1e-6,
-             "domains": [{"kind": "hall", "name": "hall", "width_m": 4.4, "height_m": 3.1, "depth_m": 2.4,
-                          "nodes_across": 23, "mode": [1, 1, 1], "amplitude_pa": 1.0}]},
-    # scenes/27-a-cavity-ringing-at-its-own-frequency.json
-    "cavity": {"schedule": "multirate", "duration_s": 4e-09, "frames": 200, "conservation_tolerance": 1e-06,
-               "domains": [{"kind": "cavity", "name": "resonator", "cells": [24, 4, 24], "cell_mm": 5.0,
-                            "medium": "vacuum", "mode": [1, 1], "amplitude_v_per_m": 1000.0}]},
-    # scenes/01-room-mode.json
-    "room": {"schedule": "multirate", "duration_s": 0.02, "frames": 11, "conservation_tolerance": 1e-6,
-             "domains": [{"kind": "room", "name": "room", "width_m": 4.4, "height_m": 3.1, "cells_across": 81,
-                          "release": {"as": "mode", "nx": 1, "ny": 1, "amplitude_pa": 1.0}}]},
-}
+with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scenes.json")) as _f:
+    SCENES = {k: v["scene"] for k, v in json.load(_f).items()}
+ACOUSTIC_FP32 = [k for k, v in SCENES.items() if v["domains"][0]["kind"] in ("hall", "room", "cavity")]
 
 
 def oracle_domain(scene):
     """The same domain built from the oracle's restatements, released with the same host fields."""
     d = scene["domains"][0]
     if d["kind"] == "block":
-        m = S.ALUMINIUM_6061
+        m, fills, t = S.block_layout(d)
         counts = tuple(d["cells"])
         o = oracle.Heat(counts, d["cell_mm"] * 1e-3, m["density"], m["conductivity"], m["specific_heat"],
                         S.celsius(d["initial_c"]), emissivity=m["emissivity"])
-        t = np.full(int(np.prod(counts)), S.celsius(d["initial_c"]))
-        i, j, k = d["hot_spot"]["at"]
-        t[i + counts[0] * (j + counts[1] * k)] = S.celsius(d["initial_c"] + d["hot_spot"]["above_k"])
+        for mask, sub in fills:
+            o.fill(mask, sub["density"], sub["conductivity"], sub["specific_heat"], sub["emissivity"])
         o.cells = t
         return o
     if d["kind"] == "hall":
@@ -52,14 +39,21 @@ def oracle_domain(scene):
         o.release(S.hall_mode_profile(o.nodes, o.dx, d["mode"], d["amplitude_pa"]))
         return o
     if d["kind"] == "room":
-        rel = d["release"]
         o = oracle.Room(d["width_m"], d["height_m"], d["cells_across"], 1.0, S.AIR["density"], S.AIR["speed"])
-        o.release(S.room_mode_profile(o.cells, o.dx, (rel["nx"], rel["ny"]), rel["amplitude_pa"]))
+        o.release(S.room_release(o.cells, o.dx, d["release"]))
         return o
     o = oracle.Yee(tuple(d["cells"]), d["cell_mm"] * 1e-3)
     steps = max(int(np.ceil(S.window(scene) / o.courant_limit())), 1)
     o.release_mode(tuple(d["mode"]), d["amplitude_v_per_m"], S.window(scene) / steps)
     return o
+
+
+def test_the_fixture_holds_the_reference_files():
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scenes.json")) as f:
+        entries = json.load(f)
+    for k, v in entries.items():
+        assert v["source"].startswith("crates/pantometry-world/scenes/") and v["source"].endswith(".json"), k
+        assert len(v["scene"]["domains"]) == 1, k
 
 
 def test_substeps_follow_the_reference_rule():
@@ -88,7 +82,7 @@ def test_the_scenes_on_the_gpu_match_the_oracle(name):
     assert got["substeps"] == want["substeps"]
     for fg, fo in zip(got["frames"], want["frames"]):
         assert abs(fg["total"] - fo["total"]) <= 1e-12 * max(fo["scale"], 1e-300)
-    if name == "block":
+    if SCENES[name]["domains"][0]["kind"] == "block":
         assert np.array_equal(g.cells.view(np.uint64), o.cells.view(np.uint64))
     else:
         fg, fo = g.fields(), o.fields()
@@ -97,7 +91,7 @@ def test_the_scenes_on_the_gpu_match_the_oracle(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["hall", "cavity", "room"])
+@pytest.mark.parametrize("name", ACOUSTIC_FP32)
 def test_the_scenes_hold_in_fp32(name):
     scene = SCENES[name]
     out = S.run(scene, S.build(scene, precision="f32"))
