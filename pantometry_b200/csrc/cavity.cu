@@ -393,6 +393,18 @@ struct Cavity : Handle {
             if (boundary[w] != 0) return true;
         return false;
     }
+    // Obstacles with magnetic or open walls: the reference applies the walls, keeps E as Mur's
+    // history, and only then zeroes the obstacles' edges (cavity.rs:1497-1499, 1159-1163). The
+    // step kernels then leave those edges alone, the walls run, E is copied to `stale` (the history
+    // lives there from then on) and yee_enforce_solid zeroes the edges.
+    bool solid_after_walls() const { return any_solid && open_or_magnetic(); }
+    pm_status ensure_stale() {
+        for (int q = 0; q < 3; ++q) {
+            const size_t bytes = dcount(q) * esize();
+            if (stale[q].bytes < bytes) PM_CUDA(stale[q].alloc(bytes));
+        }
+        return PM_OK;
+    }
     // Before E is rewritten between steps: keep the history the next step's open walls need.
     pm_status keep_history() {
         if (!has_prev || use_stale) return PM_OK;
@@ -407,7 +419,7 @@ struct Cavity : Handle {
     // The walls after the step from `par` into `par ^ 1` (cavity.rs:1074-1164): magnetic mirrors,
     // then open walls by Mur (or held at zero before any history exists), one wall at a time.
     template <typename Real>
-    cudaError_t walls(int par, bool prev, bool stale_history, double dt, cudaStream_t s) const {
+    YeeWallArgs<Real> wall_args(int par, bool stale_history) const {
         YeeWallArgs<Real> a{};
         for (int q = 0; q < 3; ++q) {
             a.e[q] = f[par ^ 1][q].as<Real>();
@@ -418,6 +430,21 @@ struct Cavity : Handle {
             a.ry[q] = tma ? (unsigned)(ny + 1) : (unsigned)ey;
         }
         a.nx = nx; a.ny = ny; a.nz = nz;
+        return a;
+    }
+    // After the walls of the step from `par`: E (before the obstacles are zeroed) becomes Mur's
+    // history, then the obstacles' edges are zeroed.
+    template <typename Real>
+    cudaError_t solid_after(int par, cudaStream_t s) const {
+        for (int q = 0; q < 3; ++q) {
+            cudaError_t e = cudaMemcpyAsync(stale[q].p, f[par ^ 1][q].p, dcount(q) * esize(), cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return e;
+        }
+        return launch_yee_enforce_solid<Real>(wall_args<Real>(par, false), dsolid.as<uint8_t>(), s);
+    }
+    template <typename Real>
+    cudaError_t walls(int par, bool prev, bool stale_history, double dt, cudaStream_t s) const {
+        YeeWallArgs<Real> a = wall_args<Real>(par, stale_history);
         const double c_dt = wave_speed() * dt;
         a.k = (Real)((c_dt - dx) / (c_dt + dx));  // cavity.rs:1075-1078
         for (int w = 0; w < 6; ++w) {
@@ -439,25 +466,34 @@ struct Cavity : Handle {
     // One step from `par`, its walls included.
     cudaError_t step_once(int par, double h, bool prev, bool stale_history, cudaStream_t s) const {
         cudaError_t e;
+        const bool after = solid_after_walls();  // the obstacles' edges are zeroed after the walls
         if (precision == PM_PLAIN_F64) {
-            e = launch_yee_step<double>(sargs<double>(par, h), s);
+            YeeStepArgs<double> a = sargs<double>(par, h);
+            if (after) a.solid = nullptr;
+            e = launch_yee_step<double>(a, s);
         } else if (tma) {
             YeeStepArgs<float> t = targs(par, h);
+            if (after) t.solid = nullptr;
             if (near_on()) {
                 // the box's terms and the source are the box kernel's; it closes the books
                 const YeeNearArgs n = nargs(par, h, t);
                 t.nb_x0 = near_x0; t.nb_y0 = near_y0; t.nb_z0 = near_z0; t.nb_w = near_w;
                 t.src_i = t.src_j = t.src_k = -1;
                 e = launch_yee_tma(t, L, maps[par], s);
-                if (e == cudaSuccess) e = launch_yee_near(n, any_solid, s);
+                if (e == cudaSuccess) e = launch_yee_near(n, any_solid && !after, s);
             } else {
                 e = launch_yee_tma(t, L, maps[par], s);
             }
         } else {
-            e = launch_yee_step<float>(sargs<float>(par, h), s);
+            YeeStepArgs<float> a = sargs<float>(par, h);
+            if (after) a.solid = nullptr;
+            e = launch_yee_step<float>(a, s);
         }
         if (e != cudaSuccess || !open_or_magnetic()) return e;
-        return precision == PM_PLAIN_F64 ? walls<double>(par, prev, stale_history, h, s) : walls<float>(par, prev, stale_history, h, s);
+        if (after) stale_history = prev;  // the history lives in `stale` once a step has run
+        e = precision == PM_PLAIN_F64 ? walls<double>(par, prev, stale_history, h, s) : walls<float>(par, prev, stale_history, h, s);
+        if (e != cudaSuccess || !after) return e;
+        return precision == PM_PLAIN_F64 ? solid_after<double>(par, s) : solid_after<float>(par, s);
     }
 
     // Tensor maps of both parities' six components over the padded lattice.
@@ -946,9 +982,18 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
     CAV_GUARD(c);
     if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
     if (nsteps == 0) return PM_OK;
-    if (c->open_or_magnetic() && c->any_solid)
-        return fail(PM_UNSUPPORTED, "obstacles together with magnetic or open walls are not on the GPU path (the reference zeroes "
-                                    "obstacle edges after the walls)");
+    if (c->solid_after_walls()) {
+        pm_status es = c->ensure_stale();
+        if (es != PM_OK) return es;
+        if (c->has_prev && !c->use_stale) {
+            // the history the last step left, now kept in `stale` (stepped before these walls were
+            // set: the field after its step, the obstacles' edges already zeroed)
+            for (int q = 0; q < 3; ++q)
+                PM_CUDA(cudaMemcpyAsync(c->stale[q].p, c->f[c->parity][q].p, c->dcount(q) * c->esize(), cudaMemcpyDeviceToDevice,
+                                        c->stream()));
+            c->use_stale = true;
+        }
+    }
     // cavity.rs:1469-1480
     const double h = dt, limit = c->courant_limit();
     if (h > limit) {
@@ -973,7 +1018,7 @@ pm_status pm_cavity_step(pm_cavity* cp, double dt, long long nsteps, pm_violatio
         PM_CUDA(c->step_once(c->parity, h, c->has_prev, c->use_stale, c->stream()));
         c->parity ^= 1;
         c->has_prev = true;
-        c->use_stale = false;
+        c->use_stale = c->solid_after_walls();  // there the history stays in `stale`
         remaining -= 1;
     }
     s = c->run_steps(remaining, dt, true, [c, h](int par, cudaStream_t st) { return c->step_once(par, h, true, false, st); });

@@ -156,6 +156,11 @@ cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, i
 }
 
 template <>
+cudaError_t launch_yee_enforce_solid<float>(const YeeWallArgs<float>& a, const uint8_t* solid, cudaStream_t s) {
+    yee_enforce_solid<float><<<kMeasureBlocks, 256, 0, s>>>(a, solid);
+    return cudaGetLastError();
+}
+template <>
 cudaError_t launch_yee_walls<float>(const YeeWallArgs<float>& a, cudaStream_t s) {
     yee_walls<float><<<kMeasureBlocks, 256, 0, s>>>(a);
     return cudaGetLastError();

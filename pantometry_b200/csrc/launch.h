@@ -88,6 +88,8 @@ template <typename Real> cudaError_t launch_yee_e(const YeeEArgs<Real>& a, cudaS
 template <typename Real> cudaError_t launch_yee_step(const YeeStepArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_measure(const YeeHArgs<Real>& a, double* out2, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_walls(const YeeWallArgs<Real>& a, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_yee_enforce_solid(const YeeWallArgs<Real>& a, const uint8_t* solid, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_coefs(const YeeCoefArgs<Real>& a, cudaStream_t s);
 // The FP32 Hall step staged by TMA (padded face layout, nx a multiple of 4).
 cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s);

@@ -79,6 +79,11 @@ cudaError_t launch_ens<double>(const EnsArgs<double>& a, bool measure, unsigned 
 }
 
 template <>
+cudaError_t launch_yee_enforce_solid<double>(const YeeWallArgs<double>& a, const uint8_t* solid, cudaStream_t s) {
+    yee_enforce_solid<double><<<kMeasureBlocks, 256, 0, s>>>(a, solid);
+    return cudaGetLastError();
+}
+template <>
 cudaError_t launch_yee_walls<double>(const YeeWallArgs<double>& a, cudaStream_t s) {
     yee_walls<double><<<kMeasureBlocks, 256, 0, s>>>(a);
     return cudaGetLastError();

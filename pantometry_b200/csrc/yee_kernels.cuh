@@ -805,6 +805,29 @@ struct YeeWallArgs {
     Real k;             // Mur's coefficient (cΔt − Δ)/(cΔt + Δ)
 };
 
+// cavity.rs:304-331 `enforce_solid` as a pass of its own: the twelve edges of every solid cell to
+// zero. Run after the walls when a cavity has both obstacles and magnetic or open walls, since the
+// reference applies its walls (and takes Mur's history) before it zeroes the obstacles' edges
+// (cavity.rs:1497-1499); the step kernels then leave those edges to this pass. Neighbouring solid
+// cells share edges and write the same zero.
+template <typename Real>
+static __global__ void yee_enforce_solid(YeeWallArgs<Real> a, const uint8_t* __restrict__ solid) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const size_t cells = (size_t)nx * ny * nz;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+        if (!solid[c]) continue;
+        const size_t i = c % (size_t)nx, r = c / (size_t)nx;
+        const size_t j = r % (size_t)ny, k = r / (size_t)ny;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const size_t u = q & 1, v = q >> 1;
+            a.e[0][i + a.rx[0] * ((j + u) + a.ry[0] * (k + v))] = Real(0);
+            a.e[1][(i + u) + a.rx[1] * (j + a.ry[1] * (k + v))] = Real(0);
+            a.e[2][(i + u) + a.rx[2] * ((j + v) + a.ry[2] * k)] = Real(0);
+        }
+    }
+}
+
 template <typename Real>
 static __global__ void yee_walls(YeeWallArgs<Real> a) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, w = a.wall;

@@ -5,7 +5,8 @@ held at zero, magnetic walls mirrored from one cell in, open walls by Mur's firs
 from the previous step's E (or held at zero before any step has run). Mur's history is what the
 last step left, also after E was rewritten between steps (a second release), as in the reference.
 Plain f64 is compared bit for bit; FP32 (both the padded TMA form and the per-cell-media form)
-within the f32 bounds of the other tests.
+within the f32 bounds of the other tests. With obstacles the walls come before the obstacles'
+edges are zeroed, as in the reference.
 """
 import numpy as np
 import pytest
@@ -87,13 +88,52 @@ def test_walls_f32(media):
     assert e_h_err(o.fields(), g.fields()) < 1e-4
 
 
-def test_obstacles_with_open_walls_are_refused():
-    from pantometry_b200._native import NativeError
-
-    counts = (8, 8, 8)
+@pytest.mark.parametrize("walls", [MIXED, OPEN], ids=["mixed", "open"])
+def test_obstacles_with_magnetic_and_open_walls_bitexact(walls):
+    """Obstacles beside magnetic and open walls: the reference applies the walls, keeps E as Mur's
+    history and only then zeroes the obstacles' edges (cavity.rs:1497-1499), so an obstacle edge on
+    a wall's inner plane feeds Mur's update before it is zeroed. Solid cells touch the x, y and z
+    walls' inner planes; plain f64 bit for bit through a release between runs, FP32 within bounds."""
+    counts = (12, 10, 9)
     solid = np.zeros(counts[::-1], dtype=np.uint8)
-    solid[3, 3, 3] = 1
-    _, g = cavity_pair(counts, 1e-3, solid=solid.reshape(-1))
-    g.set_boundary(5, 2)
-    with pytest.raises(NativeError, match="obstacles"):
-        g.step(0.5 * g.courant_limit(), 1)
+    solid[0:2, 3:5, 1:3] = 1      # against the z-low wall and the x-low wall's inner planes
+    solid[4:6, 8:10, 9:11] = 1    # against the y-high and x-high walls
+    solid[7:9, 0:2, 5:7] = 1      # against the z-high and y-low walls
+    dt = None
+    for precision in ("f64", "f32"):
+        o, g = cavity_pair(counts, 1e-3, solid=solid.reshape(-1), precision=precision)
+        with_walls(o, g, walls)
+        dt = 0.9 * o.courant_limit()
+        o.release_mode((1, 1), 1.0, dt)
+        g.release_mode((1, 1), 1.0, dt)
+        assert o.step(dt, 70) is None and g.step(dt, 70) is None  # a graph of 64 steps and single launches
+        if precision == "f64":
+            fo, fg = o.fields(), g.fields()
+            for k in fo:
+                assert_bitexact(k, fg[k], fo[k])
+            o.release_mode((2, 1), 0.5, dt)
+            g.release_mode((2, 1), 0.5, dt)
+            assert o.step(dt, 40) is None and g.step(dt, 40) is None
+            fo, fg = o.fields(), g.fields()
+            for k in fo:
+                assert_bitexact(k, fg[k], fo[k])
+        else:
+            assert e_h_err(o.fields(), g.fields()) < 1e-4
+
+
+def test_walls_set_after_obstructed_steps():
+    """Open walls set on an obstructed cavity that has already stepped: the history is the field
+    the last step left (its obstacles' edges already zeroed), and the runs go on together."""
+    counts = (10, 9, 8)
+    solid = np.zeros(counts[::-1], dtype=np.uint8)
+    solid[3:5, 3:5, 3:5] = 1
+    o, g = cavity_pair(counts, 1e-3, solid=solid.reshape(-1))
+    dt = 0.9 * o.courant_limit()
+    o.release_mode((1, 1), 1.0, dt)
+    g.release_mode((1, 1), 1.0, dt)
+    assert o.step(dt, 10) is None and g.step(dt, 10) is None
+    with_walls(o, g, OPEN)
+    assert o.step(dt, 30) is None and g.step(dt, 30) is None
+    fo, fg = o.fields(), g.fields()
+    for k in fo:
+        assert_bitexact(k, fg[k], fo[k])
