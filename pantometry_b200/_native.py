@@ -172,6 +172,7 @@ SIGNATURES = {
     "pm_heat_restore": (_st, [_p]),
     "pm_heat_set_cells_per_thread": (_st, [_p, _i]),
     "pm_heat_set_stream": (_st, [_p, _p]),
+    "pm_heat_set_wait_budget": (_st, [_p, C.c_uint]),
     "pm_heat_destroy": (None, [_p]),
     # Hall
     "pm_hall_create": (_st, [C.POINTER(HallDesc), C.POINTER(_p)]),

@@ -191,6 +191,29 @@ __device__ __forceinline__ void audit_and_commit(DevState* st, double total, dou
     st->scale = scale;
 }
 
+// A barrier across every block of a cooperative launch (all co-resident), bounded. `count` is zero
+// at the launch's start (the host clears it) and barrier b of the launch completes when it reaches
+// (b + 1)·gridDim.x. Each block's thread 0 arrives once; the others wait at __syncthreads. The
+// wait polls at most `budget` times, about 100 ns apart, after a first look; a wait that runs out
+// returns false in every thread of the block, and the caller stops with kDeviceTimeout.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target, unsigned budget) {
+    __shared__ int passed;
+    __syncthreads();
+    if (linear_tid() == 0) {
+        __threadfence();  // this block's writes before its arrival
+        atomicAdd(count, 1u);
+        bool ok = *(volatile unsigned*)count >= target;
+        for (unsigned it = 0; !ok && it < budget; ++it) {
+            __nanosleep(100);
+            ok = *(volatile unsigned*)count >= target;
+        }
+        __threadfence();  // the other blocks' writes after the wait
+        passed = ok ? 1 : 0;
+    }
+    __syncthreads();
+    return passed != 0;
+}
+
 // `Ledger::add` (conserved.rs:86-90) into an entry that starts at zero.
 __device__ __forceinline__ void ledger_add(double& total, double& scale, double x) {
     total += x;

@@ -13,6 +13,14 @@ cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_heat_f32_steps(const HeatF32Args& a, const HeatPersist& p, cudaStream_t s) {
+    HeatF32Args aa = a;
+    HeatPersist pp = p;
+    void* args[2] = {&aa, &pp};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_f32_quad_steps), dim3(a.nblocks), tile_block(),
+                                       args, 0, s);
+}
+
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s) {
     heat_measure<<<a.nblocks, 256, 0, s>>>(a);
     return cudaGetLastError();
@@ -210,6 +218,7 @@ int occupancy_f32(KernelId id) {
     switch (id) {
         case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step<false>, 256, 0); break;
         case kHeatF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_step, 256, 0); break;
+        case kHeatF32QuadSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_steps, 256, 0); break;
         case kHallF32:
             e = allow_smem(hall_step<float, false>, (int)hall_smem_bytes<float>());
             if (e != cudaSuccess) break;

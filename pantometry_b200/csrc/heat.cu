@@ -54,6 +54,11 @@ struct Heat : Handle {
     bool wide = true;
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
+    // the persistent many-step path of small plain f64 blocks (heat_plain_pair_steps)
+    DBuf dbarrier;
+    unsigned wait_budget = 1u << 24;  // polls per grid-barrier wait, about 100 ns apart
+    static constexpr size_t kPersistMaxCells = size_t(1) << 22;
+    static constexpr int kPersistChunk = 1024;  // steps per cooperative launch
     double saved_lost = 0.0, saved_supplied = 0.0;
 
     size_t n() const { return (size_t)nx * ny * nz; }
@@ -402,6 +407,46 @@ struct Heat : Handle {
         return a;
     }
 
+    // Small uniform plain f64 blocks in the pair form, films that do not radiate, more than one
+    // step: every step of a launch-bound block in one cooperative launch per kPersistChunk steps.
+    bool persistent(long long nsteps) const {
+        const int width = precision == PM_PLAIN_F64 ? 2 : 4;  // the pair and the quad forms
+        if (!uniform || !wide || nx % width != 0 || radiating() || nsteps < 2) return false;
+        if (n() > kPersistMaxCells) return false;
+        int coop = 0;
+        return cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop;
+    }
+    pm_status run_persistent(long long nsteps, double dt) {
+        if (!dbarrier.p) PM_CUDA(dbarrier.alloc(sizeof(unsigned)));
+        const bool plain = precision == PM_PLAIN_F64;
+        // a grid of co-resident blocks, tiles made as small as that grid takes
+        const unsigned wave = wave_of(plain ? kHeatPlainSteps : kHeatF32QuadSteps);
+        const int tx = nx / (plain ? 2 : 4);
+        int zc = 1;
+        while (zc < nz && make_tiles(tx, ny, nz, zc).ntiles > (long long)wave) zc *= 2;
+        const Tiles tiles = make_tiles(tx, ny, nz, zc);
+        int par = parity;
+        for (long long done = 0; done < nsteps;) {
+            const int chunk = (int)std::min<long long>(kPersistChunk, nsteps - done);
+            PM_CUDA(cudaMemsetAsync(dbarrier.p, 0, sizeof(unsigned), stream()));
+            const HeatPersist p{dbarrier.as<unsigned>(), chunk, wait_budget};
+            if (plain) {
+                HeatPlainArgs a = plain_args(par, dt);
+                a.tiles = tiles;
+                a.nblocks = grid_for(tiles, wave);
+                PM_CUDA(launch_heat_plain_steps(a, p, stream()));
+            } else {
+                HeatF32Args a = f32_args(par, dt);
+                a.tiles = tiles;
+                a.nblocks = grid_for(tiles, wave);
+                PM_CUDA(launch_heat_f32_steps(a, p, stream()));
+            }
+            par ^= chunk & 1;
+            done += chunk;
+        }
+        return PM_OK;
+    }
+
     pm_status measure() {  // the opening ledger of the present state
         HeatMeasureArgs m{};
         if (precision == PM_PLAIN_F64) m.t64 = field[parity].as<double>();
@@ -587,10 +632,14 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
     pm_status s = h->begin_call();
     if (s != PM_OK) return s;
     const long long before = h->host_state->steps;
-    if (h->precision == PM_PLAIN_F64) {
+    if (h->precision == PM_PLAIN_F64 && h->persistent(nsteps)) {
+        s = h->run_persistent(nsteps, dt);
+    } else if (h->precision == PM_PLAIN_F64) {
         s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {
             return launch_heat_plain(h->plain_args(par, dt), st);
         });
+    } else if (h->persistent(nsteps)) {
+        s = h->run_persistent(nsteps, dt);
     } else {
         if ((s = h->prepare_f32(dt)) != PM_OK) return s;
         s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {
@@ -675,6 +724,13 @@ pm_status pm_heat_set_cells_per_thread(pm_heat* hp, int cells) {
         h->drop_graphs();  // the captured launches hold the old tiling
         h->wide = cells != 1;
     }
+    return PM_OK;
+}
+
+pm_status pm_heat_set_wait_budget(pm_heat* hp, unsigned polls) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    h->wait_budget = polls;
     return PM_OK;
 }
 

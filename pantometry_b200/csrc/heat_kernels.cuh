@@ -310,58 +310,158 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
 #ifndef PM_HEAT_PAIR_MIN_BLOCKS
 #define PM_HEAT_PAIR_MIN_BLOCKS 4
 #endif
-static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_step(HeatPlainArgs a) {
-    if (a.st->violated || heat_refused(a)) return;
+// A load of the old field: through L1 within one launch (its inputs never change while it runs), or
+// from L2 alone (`ld.global.cg`) in the many-step kernel, where a buffer read two steps ago has since
+// been rewritten by other blocks and a line kept in this SM's L1 would be stale.
+template <bool CG>
+__device__ __forceinline__ double2 heat_ld2(const double* p) {
+    if constexpr (CG) return __ldcg(reinterpret_cast<const double2*>(p));
+    else return *reinterpret_cast<const double2*>(p);
+}
+template <bool CG>
+__device__ __forceinline__ double heat_ld(const double* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
+}
+
+// One tile of the pair form for one step, from `told` into `tnew`: the arithmetic both the one-step
+// kernel and the persistent many-step kernel run, so they agree bit for bit.
+template <bool CG>
+__device__ __forceinline__ void heat_pair_tile(const HeatPlainArgs& a, long long t, const double* told, double* tnew,
+                                               double (&acc)[2], double& rate) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
     const double2 zero = make_double2(0.0, 0.0);
     const double kf = a.kface;
+    int q, j, k0, k1;
+    tile_column(a.tiles, t, q, j, k0, k1);  // q: the pair's place along the row
+    const int i = 2 * q;
+    if (i >= nx || j >= ny) return;
+    const size_t c0 = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+    const double* p = told + c0;
+    double* o = tnew + c0;
+    const bool xl = i > 0, xh = i + 2 < nx, yl = j > 0, yh = j + 1 < ny;
+    double2 below = k0 > 0 ? heat_ld2<CG>(p - plane) : zero;
+    double2 here = heat_ld2<CG>(p);
+    size_t c = c0;
+    for (int k = k0; k < k1; ++k, p += plane, o += plane, c += plane) {
+        const double2 above = k + 1 < nz ? heat_ld2<CG>(p + plane) : zero;
+        const double2 ym = yl ? heat_ld2<CG>(p - nx) : zero;
+        const double2 yp = yh ? heat_ld2<CG>(p + nx) : zero;
+        const double xm = xl ? heat_ld<CG>(p - 1) : 0.0, xp = xh ? heat_ld<CG>(p + 2) : 0.0;
+        const double hv[2] = {here.x, here.y}, bv[2] = {below.x, below.y}, av[2] = {above.x, above.y};
+        const double mv[2] = {ym.x, ym.y}, pv[2] = {yp.x, yp.y};
+        double nt[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const double t0 = hv[e];
+            double flux = 0.0;
+            if (e > 0 || xl) flux += kf * ((e == 0 ? xm : hv[0]) - t0);
+            if (e < 1 || xh) flux += kf * ((e == 1 ? xp : hv[1]) - t0);
+            if (yl) flux += kf * (mv[e] - t0);
+            if (yh) flux += kf * (pv[e] - t0);
+            if (k > 0) flux += kf * (bv[e] - t0);
+            if (k + 1 < nz) flux += kf * (av[e] - t0);
+            const double shed = a.films.exposed ? film_flux(a, i + e, j, k, c + e, t0) : 0.0;
+            nt[e] = t0 + a.dts * a.mobility * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
+            acc[0] += a.capacity * (nt[e] - a.reference);     // solid.rs:1583-1590
+            if (shed != 0.0) acc[1] += a.dts * a.mobility * shed * a.capacity;  // solid.rs:1821-1823
+            if (a.radiating && (i + e == 0 || i + e + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz))
+                rate = fmax(rate, heat_cell_rate(a, i + e, j, k, c + e, nt[e]));
+        }
+        *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);
+        below = here;
+        here = above;
+    }
+}
+
+static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_step(HeatPlainArgs a) {
+    if (a.st->violated || heat_refused(a)) return;
     double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
     double rate = -1.0;          // radiating films: the largest boundary-cell rate of the new state
-    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
-        int q, j, k0, k1;
-        tile_column(a.tiles, t, q, j, k0, k1);  // q: the pair's place along the row
-        const int i = 2 * q;
-        if (i >= nx || j >= ny) continue;
-        const size_t c0 = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
-        const double* p = a.told + c0;
-        double* o = a.tnew + c0;
-        const bool xl = i > 0, xh = i + 2 < nx, yl = j > 0, yh = j + 1 < ny;
-        double2 below = k0 > 0 ? *reinterpret_cast<const double2*>(p - plane) : zero;
-        double2 here = *reinterpret_cast<const double2*>(p);
-        size_t c = c0;
-        for (int k = k0; k < k1; ++k, p += plane, o += plane, c += plane) {
-            const double2 above = k + 1 < nz ? *reinterpret_cast<const double2*>(p + plane) : zero;
-            const double2 ym = yl ? *reinterpret_cast<const double2*>(p - nx) : zero;
-            const double2 yp = yh ? *reinterpret_cast<const double2*>(p + nx) : zero;
-            const double xm = xl ? p[-1] : 0.0, xp = xh ? p[2] : 0.0;
-            const double hv[2] = {here.x, here.y}, bv[2] = {below.x, below.y}, av[2] = {above.x, above.y};
-            const double mv[2] = {ym.x, ym.y}, pv[2] = {yp.x, yp.y};
-            double nt[2];
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const double t0 = hv[e];
-                double flux = 0.0;
-                if (e > 0 || xl) flux += kf * ((e == 0 ? xm : hv[0]) - t0);
-                if (e < 1 || xh) flux += kf * ((e == 1 ? xp : hv[1]) - t0);
-                if (yl) flux += kf * (mv[e] - t0);
-                if (yh) flux += kf * (pv[e] - t0);
-                if (k > 0) flux += kf * (bv[e] - t0);
-                if (k + 1 < nz) flux += kf * (av[e] - t0);
-                const double shed = a.films.exposed ? film_flux(a, i + e, j, k, c + e, t0) : 0.0;
-                nt[e] = t0 + a.dts * a.mobility * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
-                acc[0] += a.capacity * (nt[e] - a.reference);     // solid.rs:1583-1590
-                if (shed != 0.0) acc[1] += a.dts * a.mobility * shed * a.capacity;  // solid.rs:1821-1823
-                if (a.radiating && (i + e == 0 || i + e + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz))
-                    rate = fmax(rate, heat_cell_rate(a, i + e, j, k, c + e, nt[e]));
-            }
-            *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);
-            below = here;
-            here = above;
-        }
-    }
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_pair_tile<false>(a, t, a.told, a.tnew, acc, rate);
     if (a.radiating) heat_rate_publish(a, rate);
     heat_plain_books(a, acc);
+}
+
+// Many steps of a small block in one cooperative launch (every block co-resident), for blocks whose
+// step is far shorter than a kernel launch (a 64³ block in plain f64 holds 2 MiB and sweeps from L2
+// in about a microsecond). Each step: the pair form's tiles, this block's two partials, one bounded
+// grid barrier, then every block sums all blocks' partials in the same fixed order and runs the
+// ledger and the audit on its own copy of the books (audit_and_commit, the one-step kernels'
+// arithmetic), so every block reaches the same verdict without a second barrier. The partials are
+// double-buffered by step parity: a block writes a step's partials only after the barrier that
+// every block passes after reading the ones two steps back. Block 0 writes the books back at the
+// end. Films must not radiate (the limit is the host's, checked once for the call).
+struct HeatPersist {
+    unsigned* barrier;  // arrivals, zero at launch
+    int nsteps;
+    unsigned budget;    // polls per barrier wait before giving up
+};
+
+static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_steps(HeatPlainArgs a, HeatPersist p) {
+    __shared__ DevState books;
+    __shared__ double red[32 * 2];
+    __shared__ int stop;
+    const int tid = linear_tid();
+    if (tid == 0) {
+        books = *a.st;
+        stop = books.violated;
+    }
+    __syncthreads();
+    if (stop) return;
+    const double* told = a.told;
+    double* tnew = a.tnew;
+    bool timed_out = false;
+    for (int s = 0; s < p.nsteps; ++s) {
+        double acc[2] = {0.0, 0.0};
+        double rate = -1.0;
+        for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_pair_tile<true>(a, t, told, tnew, acc, rate);
+        block_sum<2>(acc, red);
+        double* part = a.partials + (size_t)(s & 1) * 2 * gridDim.x;
+        if (tid == 0) {
+            part[2 * (size_t)blockIdx.x] = acc[0];
+            part[2 * (size_t)blockIdx.x + 1] = acc[1];
+        }
+        if (!grid_barrier(p.barrier, (unsigned)(s + 1) * gridDim.x, p.budget)) {
+            timed_out = true;
+            break;
+        }
+        double v[2] = {0.0, 0.0};
+        for (unsigned b = tid; b < gridDim.x; b += blockDim.x * blockDim.y) {
+            v[0] += __ldcg(&part[2 * (size_t)b]);
+            v[1] += __ldcg(&part[2 * (size_t)b + 1]);
+        }
+        block_sum<2>(v, red);
+        if (tid == 0) {
+            books.lost += v[1];
+            double total = 0.0, scale = 0.0;
+            ledger_add(total, scale, v[0]);
+            ledger_add(total, scale, books.lost);
+            ledger_add(total, scale, -books.supplied);
+            books.part[0] = v[0];
+            books.part[1] = books.lost;
+            books.part[2] = -books.supplied;
+            audit_and_commit(&books, total, scale);
+            stop = books.violated;
+        }
+        __syncthreads();
+        if (stop) break;
+        const double* next = tnew;
+        tnew = const_cast<double*>(told);
+        told = next;
+    }
+    if (timed_out) {
+        if (tid == 0) atomicExch(&a.st->violated, kDeviceTimeout);
+        return;
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+        DevState* st = a.st;
+        const int seen = atomicAdd(&st->violated, 0);  // a block that gave up has already said so
+        books.counter = 0u;
+        *st = books;
+        if (seen == kDeviceTimeout) st->violated = kDeviceTimeout;
+    }
 }
 
 struct HeatF32Args {
@@ -494,65 +594,149 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
 // (the sums from +0 with the neighbours present, the films as the fused b·(here + off) + shed,
 // then here + (a·sum − shed) as a fused multiply-add and an add), so the fields agree with it bit
 // for bit; only the order of the FP64 sums within a block differs.
-static __global__ void __launch_bounds__(256) heat_f32_quad_step(HeatF32Args a) {
-    if (a.st->violated) return;
+template <bool CG>
+__device__ __forceinline__ float4 heat_ld4(const float* p) {
+    if constexpr (CG) return __ldcg(reinterpret_cast<const float4*>(p));
+    else return __ldg(reinterpret_cast<const float4*>(p));
+}
+template <bool CG>
+__device__ __forceinline__ float heat_ldf(const float* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return __ldg(p);
+}
+
+// One tile of the quad form for one step, from `dold` into `dnew` (loads as heat_ld2 describes):
+// the arithmetic of the one-step and the many-step kernels.
+template <bool CG>
+__device__ __forceinline__ void heat_quad_tile(const HeatF32Args& a, long long t, const float* dold, float* dnew,
+                                               double (&acc)[2]) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    double acc[2] = {0.0, 0.0};
-    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
-        int q, j, k0, k1;
-        tile_column(a.tiles, t, q, j, k0, k1);  // q: the quad's place along the row
-        const int i = 4 * q;
-        if (i >= nx || j >= ny) continue;
-        const size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
-        const float* p = a.dold + c;
-        float* o = a.dnew + c;
-        const bool xl = i > 0, xh = i + 4 < nx, yl = j > 0, yh = j + 1 < ny;
-        float4 below = k0 > 0 ? __ldg(reinterpret_cast<const float4*>(p - plane)) : zero;
-        float4 here = __ldg(reinterpret_cast<const float4*>(p));
-        double col_shed = 0.0;
-        for (int k = k0; k < k1; ++k, p += plane, o += plane) {
-            const bool zl = k > 0, zh = k + 1 < nz;
-            const float4 above = zh ? __ldg(reinterpret_cast<const float4*>(p + plane)) : zero;
-            const float4 ym = yl ? __ldg(reinterpret_cast<const float4*>(p - nx)) : zero;
-            const float4 yp = yh ? __ldg(reinterpret_cast<const float4*>(p + nx)) : zero;
-            const float xm = xl ? __ldg(p - 1) : 0.0f, xp = xh ? __ldg(p + 4) : 0.0f;
-            const float hv[4] = {here.x, here.y, here.z, here.w}, bv[4] = {below.x, below.y, below.z, below.w};
-            const float av[4] = {above.x, above.y, above.z, above.w};
-            const float mv[4] = {ym.x, ym.y, ym.z, ym.w}, pv[4] = {yp.x, yp.y, yp.z, yp.w};
-            float nd[4];
+    int q, j, k0, k1;
+    tile_column(a.tiles, t, q, j, k0, k1);  // q: the quad's place along the row
+    const int i = 4 * q;
+    if (i >= nx || j >= ny) return;
+    const size_t c = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
+    const float* p = dold + c;
+    float* o = dnew + c;
+    const bool xl = i > 0, xh = i + 4 < nx, yl = j > 0, yh = j + 1 < ny;
+    float4 below = k0 > 0 ? heat_ld4<CG>(p - plane) : zero;
+    float4 here = heat_ld4<CG>(p);
+    double col_shed = 0.0;
+    for (int k = k0; k < k1; ++k, p += plane, o += plane) {
+        const bool zl = k > 0, zh = k + 1 < nz;
+        const float4 above = zh ? heat_ld4<CG>(p + plane) : zero;
+        const float4 ym = yl ? heat_ld4<CG>(p - nx) : zero;
+        const float4 yp = yh ? heat_ld4<CG>(p + nx) : zero;
+        const float xm = xl ? heat_ldf<CG>(p - 1) : 0.0f, xp = xh ? heat_ldf<CG>(p + 4) : 0.0f;
+        const float hv[4] = {here.x, here.y, here.z, here.w}, bv[4] = {below.x, below.y, below.z, below.w};
+        const float av[4] = {above.x, above.y, above.z, above.w};
+        const float mv[4] = {ym.x, ym.y, ym.z, ym.w}, pv[4] = {yp.x, yp.y, yp.z, yp.w};
+        float nd[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const float h = hv[e];
-                const bool l = e > 0 || xl, r = e < 3 || xh;  // the cell's x neighbours are in the block
-                float s = 0.0f;
-                if (l) s += (e == 0 ? xm : hv[e - 1]) - h;
-                if (r) s += (e == 3 ? xp : hv[e + 1]) - h;
-                if (yl) s += mv[e] - h;
-                if (yh) s += pv[e] - h;
-                if (zl) s += bv[e] - h;
-                if (zh) s += av[e] - h;
-                float shed = 0.0f;
-                if (a.exposed && (!(l && r && yl && yh) || !zl || !zh)) {
-                    if (((a.exposed >> 0) & 1) && !l) shed = __fmaf_rn(a.b[0], h + a.off[0], shed);
-                    if (((a.exposed >> 1) & 1) && !r) shed = __fmaf_rn(a.b[1], h + a.off[1], shed);
-                    if (((a.exposed >> 2) & 1) && !yl) shed = __fmaf_rn(a.b[2], h + a.off[2], shed);
-                    if (((a.exposed >> 3) & 1) && !yh) shed = __fmaf_rn(a.b[3], h + a.off[3], shed);
-                    if (((a.exposed >> 4) & 1) && !zl) shed = __fmaf_rn(a.b[4], h + a.off[4], shed);
-                    if (((a.exposed >> 5) & 1) && !zh) shed = __fmaf_rn(a.b[5], h + a.off[5], shed);
-                    col_shed += (double)shed;
-                }
-                nd[e] = __fadd_rn(h, __fmaf_rn(a.a, s, -shed));
-                acc[0] += (double)nd[e];
+        for (int e = 0; e < 4; ++e) {
+            const float h = hv[e];
+            const bool l = e > 0 || xl, r = e < 3 || xh;  // the cell's x neighbours are in the block
+            float s = 0.0f;
+            if (l) s += (e == 0 ? xm : hv[e - 1]) - h;
+            if (r) s += (e == 3 ? xp : hv[e + 1]) - h;
+            if (yl) s += mv[e] - h;
+            if (yh) s += pv[e] - h;
+            if (zl) s += bv[e] - h;
+            if (zh) s += av[e] - h;
+            float shed = 0.0f;
+            if (a.exposed && (!(l && r && yl && yh) || !zl || !zh)) {
+                if (((a.exposed >> 0) & 1) && !l) shed = __fmaf_rn(a.b[0], h + a.off[0], shed);
+                if (((a.exposed >> 1) & 1) && !r) shed = __fmaf_rn(a.b[1], h + a.off[1], shed);
+                if (((a.exposed >> 2) & 1) && !yl) shed = __fmaf_rn(a.b[2], h + a.off[2], shed);
+                if (((a.exposed >> 3) & 1) && !yh) shed = __fmaf_rn(a.b[3], h + a.off[3], shed);
+                if (((a.exposed >> 4) & 1) && !zl) shed = __fmaf_rn(a.b[4], h + a.off[4], shed);
+                if (((a.exposed >> 5) & 1) && !zh) shed = __fmaf_rn(a.b[5], h + a.off[5], shed);
+                col_shed += (double)shed;
             }
-            *reinterpret_cast<float4*>(o) = make_float4(nd[0], nd[1], nd[2], nd[3]);
-            below = here;
-            here = above;
+            nd[e] = __fadd_rn(h, __fmaf_rn(a.a, s, -shed));
+            acc[0] += (double)nd[e];
         }
-        acc[1] += col_shed;
+        *reinterpret_cast<float4*>(o) = make_float4(nd[0], nd[1], nd[2], nd[3]);
+        below = here;
+        here = above;
     }
+    acc[1] += col_shed;
+}
+
+static __global__ void __launch_bounds__(256) heat_f32_quad_step(HeatF32Args a) {
+    if (a.st->violated) return;
+    double acc[2] = {0.0, 0.0};
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_quad_tile<false>(a, t, a.dold, a.dnew, acc);
     heat_f32_books(a, acc, false);
+}
+
+// The quad form's many-step kernel, as heat_plain_pair_steps (one bounded grid barrier per step,
+// every block auditing its own copy of the books, block 0 writing them back).
+static __global__ void __launch_bounds__(256) heat_f32_quad_steps(HeatF32Args a, HeatPersist p) {
+    __shared__ DevState books;
+    __shared__ double red[32 * 2];
+    __shared__ int stop;
+    const int tid = linear_tid();
+    if (tid == 0) {
+        books = *a.st;
+        stop = books.violated;
+    }
+    __syncthreads();
+    if (stop) return;
+    const float* dold = a.dold;
+    float* dnew = a.dnew;
+    bool timed_out = false;
+    for (int s = 0; s < p.nsteps; ++s) {
+        double acc[2] = {0.0, 0.0};
+        for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_quad_tile<true>(a, t, dold, dnew, acc);
+        block_sum<2>(acc, red);
+        double* part = a.partials + (size_t)(s & 1) * 2 * gridDim.x;
+        if (tid == 0) {
+            part[2 * (size_t)blockIdx.x] = acc[0];
+            part[2 * (size_t)blockIdx.x + 1] = acc[1];
+        }
+        if (!grid_barrier(p.barrier, (unsigned)(s + 1) * gridDim.x, p.budget)) {
+            timed_out = true;
+            break;
+        }
+        double v[2] = {0.0, 0.0};
+        for (unsigned b = tid; b < gridDim.x; b += blockDim.x * blockDim.y) {
+            v[0] += __ldcg(&part[2 * (size_t)b]);
+            v[1] += __ldcg(&part[2 * (size_t)b + 1]);
+        }
+        block_sum<2>(v, red);
+        if (tid == 0) {
+            const double stored = a.capacity * v[0];
+            books.lost += a.capacity * v[1];
+            double total = 0.0, scale = 0.0;
+            ledger_add(total, scale, stored);
+            ledger_add(total, scale, books.lost);
+            ledger_add(total, scale, -books.supplied);
+            books.part[0] = stored;
+            books.part[1] = books.lost;
+            books.part[2] = -books.supplied;
+            audit_and_commit(&books, total, scale);
+            stop = books.violated;
+        }
+        __syncthreads();
+        if (stop) break;
+        const float* next = dnew;
+        dnew = const_cast<float*>(dold);
+        dold = next;
+    }
+    if (timed_out) {
+        if (tid == 0) atomicExch(&a.st->violated, kDeviceTimeout);
+        return;
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+        DevState* st = a.st;
+        const int seen = atomicAdd(&st->violated, 0);  // a block that gave up has already said so
+        books.counter = 0u;
+        *st = books;
+        if (seen == kDeviceTimeout) st->violated = kDeviceTimeout;
+    }
 }
 
 // The opening ledger of a freshly uploaded block: stored heat only (lost and supplied are zero

@@ -64,7 +64,7 @@ inline cudaError_t launch_smem(void (*kernel)(P...), dim3 grid, dim3 block, int 
 // Multiprocessor, asked once per kernel and device), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps, kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -74,8 +74,12 @@ template <typename Real>
 inline size_t hall_smem_bytes() { return sizeof(HallStage<Real>) * HallDepth<Real>::stages; }
 
 cudaError_t launch_heat_plain(const HeatPlainArgs& a, cudaStream_t s);
+// Many plain f64 pair-form steps of a small block in one cooperative launch (heat_plain_pair_steps).
+cudaError_t launch_heat_plain_steps(const HeatPlainArgs& a, const HeatPersist& p, cudaStream_t s);
 cudaError_t launch_heat_measure_plain(const HeatMeasureArgs& a, cudaStream_t s);
 cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s);
+// Many FP32 quad-form steps of a small block in one cooperative launch (heat_f32_quad_steps).
+cudaError_t launch_heat_f32_steps(const HeatF32Args& a, const HeatPersist& p, cudaStream_t s);
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s);
 cudaError_t launch_heat_convert(const double* t, float* d, double t0, size_t n, int to_dev, double* tout,
                                 cudaStream_t s);

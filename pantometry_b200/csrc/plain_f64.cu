@@ -12,6 +12,14 @@ cudaError_t launch_heat_plain(const HeatPlainArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_heat_plain_steps(const HeatPlainArgs& a, const HeatPersist& p, cudaStream_t s) {
+    HeatPlainArgs aa = a;
+    HeatPersist pp = p;
+    void* args[2] = {&aa, &pp};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_plain_pair_steps), dim3(a.nblocks), tile_block(),
+                                       args, 0, s);
+}
+
 cudaError_t launch_heat_measure_plain(const HeatMeasureArgs& a, cudaStream_t s) {
     heat_measure<<<a.nblocks, 256, 0, s>>>(a);
     return cudaGetLastError();
@@ -133,6 +141,7 @@ int occupancy_f64(KernelId id) {
     switch (id) {
         case kHeatPlain: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_step, 256, 0); break;
         case kHeatPlainPair: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_step, 256, 0); break;
+        case kHeatPlainSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_steps, 256, 0); break;
         case kHallF64:
             e = allow_smem(hall_step<double, false>, (int)hall_smem_bytes<double>());
             if (e != cudaSuccess) break;

@@ -121,6 +121,11 @@ class Solid3D(_Domain):
         N.check(self._lib.pm_heat_losing_from(self._h, f, ambient, convection, area))
         return self
 
+    def set_wait_budget(self, polls):
+        """Polls per grid-wide wait of the many-step path (small plain f64 blocks); 0 makes every
+        wait that is not already over give up at once (the call returns PM_DEVICE_TIMEOUT)."""
+        N.check(self._lib.pm_heat_set_wait_budget(self._h, int(polls)))
+
     def set_cells_per_thread(self, cells):
         """Cells of a row per thread: 1, or the precision's wide form (the default where the block
         is one material and its rows allow): 2 for plain f64, 4 for FP32. The fields agree bit for
