@@ -154,6 +154,8 @@ def run_ours(args):
         hall = W.build_hall(cfg, precision=precision, device=local)
         hall.set_stream(stream.cuda_stream)
         hall.set_tolerance(1e-6 if precision == "f32" else 1e-9)
+        if precision == "f32":
+            tiles.append(hall.autotune(trial_steps=16))  # the tile shape, timed on this grid
         for _ in range(w):
             hall.release(cfg["pressure"])
             v = hall.step(cfg["dt"], T)
@@ -175,6 +177,7 @@ def run_ours(args):
 
     # FP32 chosen form (the headline) and the plain f64 form, device-resident; each handle ends
     # holding one whole run of the workload
+    tiles = []
     h32, ms32, clk = timed_runs("f32", args.steps, args.warmup)
     led32 = h32.ledger()
     p32 = h32.fields()["p"]
@@ -244,7 +247,8 @@ def run_ours(args):
         "gpu_launches": args.steps * T,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": HALL_F32_TRAFFIC,
-                     "kernel": "hall_tma_step (FP32, TMA-staged)", "bytes_per_launch": BYTES_F32 * nodes,
+                     "kernel": f"hall_tma_step (FP32, TMA-staged, {tiles[0][0]} planes x {tiles[0][1]} stages, autotuned)",
+                     "bytes_per_launch": BYTES_F32 * nodes,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "plain_f64": {"value": round(plain, 3), "unit": UNIT, "ms_per_step": round(ms64 / plain_steps, 3),
                       "roofline_frac": round(BYTES_F64 * nodes / (per_launch64 * 1e-3) / 1e9 / peak, 4),

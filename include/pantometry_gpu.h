@@ -186,6 +186,15 @@ pm_status pm_hall_ledger(pm_hall* h, pm_ledger* out);
 pm_status pm_hall_download(pm_hall* h, double* p, double* p_prev, double* vx, double* vy, double* vz);
 pm_status pm_hall_checkpoint(pm_hall* h);
 pm_status pm_hall_restore(pm_hall* h);
+/* No counterpart in the reference. FP32 halls on the TMA-staged kernel (x extent a multiple of 4)
+ * step in one of several tile shapes, planes per stage x stages in the ring (8x2, 6x2, 4x3, 4x2),
+ * all computing every node with the same expressions (the fields agree bit for bit). Autotune times
+ * `trial_steps` steps of each from the present state (into the buffer the next step writes, so the
+ * state is untouched), keeps the fastest and puts the books and the source's clock back as they
+ * were; a grid shape timed once on a device is not timed again in the process. Planes and stages are 0 where the hall does not use that kernel. */
+pm_status pm_hall_autotune(pm_hall* h, int trial_steps, int* planes, int* stages);
+pm_status pm_hall_set_tile(pm_hall* h, int planes, int stages);
+pm_status pm_hall_tile(pm_hall* h, int* planes, int* stages);
 pm_status pm_hall_set_stream(pm_hall* h, void* stream);
 void pm_hall_destroy(pm_hall* h);
 
@@ -363,6 +372,16 @@ pm_status pm_cavity_energies(pm_cavity* c, double* electric, double* magnetic);
  * values of its source's near field with them. */
 pm_status pm_cavity_checkpoint(pm_cavity* c);
 pm_status pm_cavity_restore(pm_cavity* c);
+/* No counterpart in the reference. FP32 cavities on the TMA-staged kernel step in one of several
+ * tile shapes, planes per stage x stages (one medium: 3x2, 4x2, 3x3; per-cell epsilon: 4x2, 3x2),
+ * all computing every edge and face with the same expressions (the fields agree bit for bit).
+ * Autotune times `trial_steps` steps of each from the present state (into the buffer the next step
+ * writes), keeps the fastest and puts the books and the source's clock back; a grid shape timed once
+ * on a device is not timed again in the process. Planes and stages are 0 where the cavity does not
+ * use that kernel. A change of media (pm_cavity_fill_cells) goes back to the new form's shape 0. */
+pm_status pm_cavity_autotune(pm_cavity* c, int trial_steps, int* planes, int* stages);
+pm_status pm_cavity_set_tile(pm_cavity* c, int planes, int stages);
+pm_status pm_cavity_tile(pm_cavity* c, int* planes, int* stages);
 pm_status pm_cavity_set_stream(pm_cavity* c, void* stream);
 void pm_cavity_destroy(pm_cavity* c);
 

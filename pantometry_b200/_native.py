@@ -187,6 +187,9 @@ SIGNATURES = {
     "pm_hall_download": (_st, [_p, _dp, _dp, _dp, _dp, _dp]),
     "pm_hall_checkpoint": (_st, [_p]),
     "pm_hall_restore": (_st, [_p]),
+    "pm_hall_autotune": (_st, [_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pm_hall_set_tile": (_st, [_p, C.c_int, C.c_int]),
+    "pm_hall_tile": (_st, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pm_hall_set_stream": (_st, [_p, _p]),
     "pm_hall_destroy": (None, [_p]),
     "pm_room_create": (_st, [C.POINTER(RoomDesc), C.POINTER(_p)]),
@@ -243,6 +246,9 @@ SIGNATURES = {
     "pm_cavity_energies": (_st, [_p, _dp, _dp]),
     "pm_cavity_checkpoint": (_st, [_p]),
     "pm_cavity_restore": (_st, [_p]),
+    "pm_cavity_autotune": (_st, [_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pm_cavity_set_tile": (_st, [_p, C.c_int, C.c_int]),
+    "pm_cavity_tile": (_st, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pm_cavity_set_stream": (_st, [_p, _p]),
     "pm_cavity_destroy": (None, [_p]),
     # Ensembles

@@ -1,5 +1,8 @@
 // pm_cavity: the device form of `Cavity` (crates/pantometry-em/src/cavity.rs).
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <limits>
 #include <new>
 
@@ -58,6 +61,7 @@ struct Cavity : Handle {
     bool tma = false;
     unsigned L = 0;
     YeeMaps maps[2];
+    int yshape = 0;  // the TMA kernel's tile shape, an index of the present form's shape list
     // Mur's history (cavity.rs:141): E after the last step's walls. Normally the old buffer of the
     // ping-pong pair; after something rewrote E between steps it is a snapshot taken before that.
     bool has_prev = false;   // a step has run (cavity.rs:1087)
@@ -479,10 +483,10 @@ struct Cavity : Handle {
                 const YeeNearArgs n = nargs(par, h, t);
                 t.nb_x0 = near_x0; t.nb_y0 = near_y0; t.nb_z0 = near_z0; t.nb_w = near_w;
                 t.src_i = t.src_j = t.src_k = -1;
-                e = launch_yee_tma(t, L, maps[par], s);
+                e = launch_yee_tma(t, L, maps[par], yshape, s);
                 if (e == cudaSuccess) e = launch_yee_near(n, any_solid && !after, s);
             } else {
-                e = launch_yee_tma(t, L, maps[par], s);
+                e = launch_yee_tma(t, L, maps[par], yshape, s);
             }
         } else {
             YeeStepArgs<float> a = sargs<float>(par, h);
@@ -498,7 +502,7 @@ struct Cavity : Handle {
 
     // Tensor maps of both parities' six components over the padded lattice.
     pm_status build_maps() {
-        const unsigned P = (unsigned)yee_tma_planes(!uniform);
+        const unsigned P = (unsigned)yee_tma_shape(!uniform, yshape).planes;
         for (int q = 0; q < 2; ++q) {
             const int d0 = (int)L, d1 = ny + 1, d2 = nz + 1;
             if (!hall_tma_map(&maps[q].ex, f[q][0].p, d0, d1, d2, 36, 10, P + 1) ||
@@ -584,6 +588,78 @@ struct Cavity : Handle {
         return PM_OK;
     }
 
+    // The mixed-ε form's gain boxes, the tile's own edges, 32 × 8 × P (both parities share the arrays).
+    pm_status build_gain_maps() {
+        if (uniform || !tma) return PM_OK;
+        const unsigned P = (unsigned)yee_tma_shape(true, yshape).planes;
+        for (int par = 0; par < 2; ++par)
+            for (int q = 0; q < 3; ++q) {
+                CUtensorMap* m = q == 0 ? &maps[par].gx : q == 1 ? &maps[par].gy : &maps[par].gz;
+                if (!hall_tma_map(m, dgain[q].p, (int)L, ny + 1, nz + 1, 32, 8, P))
+                    return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a cavity gain array");
+            }
+        return PM_OK;
+    }
+    pm_status set_shape(int sh) {
+        if (sh < 0 || sh >= yee_tma_shape_count(!uniform)) return fail(PM_BAD_ARG, "cavity tile shape");
+        if (!tma || sh == yshape) return PM_OK;
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        yshape = sh;
+        drop_graphs();
+        pm_status s = build_maps();
+        if (s != PM_OK) return s;
+        return build_gain_maps();
+    }
+    // Time `trial` steps of every tile shape of the present form on the present state and keep the
+    // fastest. Each trial step reads the present parity and writes the other one (free between
+    // steps), so the fields are never touched; the books (the source's clock among them) are put back
+    // after each trial. A grid shape timed once on a device is not timed again in the process.
+    pm_status autotune(int trial) {
+        if (!tma) return PM_OK;
+        static std::mutex cache_mutex;
+        static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
+        const auto key = std::make_tuple(nx, ny, nz, uniform ? 1 : 0, any_solid ? 1 : 0, device);
+        {
+            std::lock_guard<std::mutex> lock(cache_mutex);
+            auto it = cache.find(key);
+            if (it != cache.end()) return set_shape(it->second);
+        }
+        pm_status s = read_state();
+        if (s != PM_OK) return s;
+        const DevState books = *host_state;
+        const double dt = 0.9 * courant_limit();
+        if ((s = prepare_coefs(dt)) != PM_OK) return s;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        PM_CUDA(cudaEventCreate(&e0));
+        PM_CUDA(cudaEventCreate(&e1));
+        int best = yshape;
+        float best_ms = 0.0f;
+        for (int sh = 0; sh < yee_tma_shape_count(!uniform) && s == PM_OK; ++sh) {
+            if ((s = set_shape(sh)) != PM_OK) break;
+            host_state->tol = -1.0;  // no audit while timing
+            if ((s = write_state()) != PM_OK) break;
+            for (int q = 0; q < 2 + trial; ++q) {
+                if (q == 2) PM_CUDA(cudaEventRecord(e0, stream()));
+                PM_CUDA(launch_yee_tma(targs(parity, dt), L, maps[parity], yshape, stream()));
+            }
+            PM_CUDA(cudaEventRecord(e1, stream()));
+            PM_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            PM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (sh == 0 || ms < best_ms) { best = sh; best_ms = ms; }
+            *host_state = books;
+            s = write_state();
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (s != PM_OK) return s;
+        {
+            std::lock_guard<std::mutex> lock(cache_mutex);
+            cache[key] = best;
+        }
+        return set_shape(best);
+    }
+
     // The padded cavity back to the reference layout (before media with conductivity or per-cell
     // μ, which only the cp.async kernel reads). The state goes through the host once; a
     // checkpoint taken in the other layout is dropped.
@@ -608,8 +684,8 @@ struct Cavity : Handle {
     // P·m − 1 planes, so a chunk and the plane below it fill whole stages).
     YeeStepArgs<float> targs(int par, double dt) const {
         YeeStepArgs<float> a = sargs<float>(par, dt);
-        const unsigned w = wave_of(uniform ? kYeeTma : kYeeTmaMedia);
-        const int P = yee_tma_planes(!uniform);
+        const unsigned w = wave_of(yee_tma_kernel_id(!uniform, yshape));
+        const int P = yee_tma_shape(!uniform, yshape).planes;
         const int X = nx + 1, Y = ny + 1, Z = nz + 1;
         int best = 2 * P - 1;
         double best_score = -1.0;
@@ -686,16 +762,10 @@ struct Cavity : Handle {
             else dch[q].release();
         }
         if (tma) {
-            // the mixed-ε form stages more planes: the field boxes again, then the gains' boxes,
-            // the tile's own edges, 32 × 8 × P (both parities share the arrays)
+            yshape = 0;  // the mixed-ε form's own shape list
             pm_status ms = build_maps();
             if (ms != PM_OK) return ms;
-            for (int par = 0; par < 2; ++par)
-                for (int q = 0; q < 3; ++q) {
-                    CUtensorMap* m = q == 0 ? &maps[par].gx : q == 1 ? &maps[par].gy : &maps[par].gz;
-                    if (!hall_tma_map(m, dgain[q].p, (int)L, ny + 1, nz + 1, 32, 8, kYeeTmaPlanesMedia))
-                        return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a cavity gain array");
-                }
+            if ((ms = build_gain_maps()) != PM_OK) return ms;
         }
         coef_dt = NAN;
         return PM_OK;
@@ -1103,6 +1173,35 @@ pm_status pm_cavity_restore(pm_cavity* cp) {
     if ((s = c->write_state()) != PM_OK) return s;
     c->has_saved = false;  // cavity.rs:1580 takes the checkpoint
     return c->reset_ledger();
+}
+
+pm_status pm_cavity_autotune(pm_cavity* cp, int trial_steps, int* planes, int* stages) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (trial_steps < 1) return fail(PM_BAD_ARG, "autotune: at least one trial step");
+    pm_status s = c->autotune(trial_steps);
+    if (s != PM_OK) return s;
+    return pm_cavity_tile(cp, planes, stages);
+}
+
+pm_status pm_cavity_set_tile(pm_cavity* cp, int planes, int stages) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (!c->tma) return fail(PM_UNSUPPORTED, "tile shapes are those of the TMA-staged FP32 kernel");
+    for (int q = 0; q < yee_tma_shape_count(!c->uniform); ++q) {
+        const YeeTmaShape sh = yee_tma_shape(!c->uniform, q);
+        if (sh.planes == planes && sh.stages == stages) return c->set_shape(q);
+    }
+    return fail(PM_BAD_ARG, c->uniform ? "cavity tile: planes x stages of 3x2, 4x2 or 3x3" : "cavity tile: planes x stages of 4x2 or 3x2");
+}
+
+pm_status pm_cavity_tile(pm_cavity* cp, int* planes, int* stages) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    const YeeTmaShape sh = yee_tma_shape(!c->uniform, c->yshape);
+    if (planes) *planes = c->tma ? sh.planes : 0;
+    if (stages) *stages = c->tma ? sh.stages : 0;
+    return PM_OK;
 }
 
 pm_status pm_cavity_set_stream(pm_cavity* cp, void* stream) {

@@ -89,11 +89,31 @@ cudaError_t launch_ens<float>(const EnsArgs<float>& a, bool measure, unsigned nb
     return cudaGetLastError();
 }
 
-cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s) {
-    constexpr int P = kHallTmaPlanes, S = kHallTmaStages;
-    const int smem = (int)hall_tma_smem_bytes();
-    return launch_smem(a.block_scale ? hall_tma_step<P, S, true> : hall_tma_step<P, S, false>, a.nblocks, tile_block(), smem,
-                       s, a, m);
+template <int P, int S, int MINB>
+static cudaError_t launch_hall_tma_shape(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s) {
+    const int smem = (int)hall_tma_smem_bytes_for<P, S>();
+    return launch_smem(a.block_scale ? hall_tma_step<P, S, true, MINB> : hall_tma_step<P, S, false, MINB>, a.nblocks,
+                       tile_block(), smem, s, a, m);
+}
+cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, int shape, cudaStream_t s) {
+    static_assert(kHallTmaShapes[0].planes == 8 && kHallTmaShapes[1].planes == 6 && kHallTmaShapes[2].planes == 4 &&
+                      kHallTmaShapes[3].planes == 4,
+                  "the dispatch below instantiates kHallTmaShapes in order");
+    switch (shape) {
+        case 1: return launch_hall_tma_shape<6, 2, 3>(a, m, s);
+        case 2: return launch_hall_tma_shape<4, 3, 3>(a, m, s);
+        case 3: return launch_hall_tma_shape<4, 2, 4>(a, m, s);
+        default: return launch_hall_tma_shape<8, 2, 2>(a, m, s);
+    }
+}
+template <int P, int S, int MINB>
+static int hall_tma_occupancy() {
+    int n = 0;
+    if (allow_smem(hall_tma_step<P, S, false, MINB>, (int)hall_tma_smem_bytes_for<P, S>()) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_tma_step<P, S, false, MINB>, 256,
+                                                      hall_tma_smem_bytes_for<P, S>()) != cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
 }
 
 bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz) {
@@ -117,13 +137,32 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
-    constexpr int S = kYeeTmaStages, PU = kYeeTmaPlanesUniform, PM = kYeeTmaPlanesMedia;
-    const bool media = !a.uniform;
-    const int smem = (int)yee_tma_smem_bytes(media);
-    auto k = a.solid ? (media ? yee_tma_step<PM, S, true, true> : yee_tma_step<PU, S, true, false>)
-                     : (media ? yee_tma_step<PM, S, false, true> : yee_tma_step<PU, S, false, false>);
+template <int P, int S, bool MEDIA, int MINB>
+static cudaError_t launch_yee_tma_shape(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
+    const int smem = (int)yee_tma_smem_bytes_for<P, MEDIA>(S);
+    auto k = a.solid ? yee_tma_step<P, S, true, MEDIA, MINB> : yee_tma_step<P, S, false, MEDIA, MINB>;
     return launch_smem(k, a.nblocks, tile_block(), smem, s, a, L, m);
+}
+cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s) {
+    static_assert(kYeeTmaUniformShapes[0].planes == 3 && kYeeTmaUniformShapes[1].planes == 4 &&
+                      kYeeTmaUniformShapes[2].stages == 3 && kYeeTmaMediaShapes[0].planes == 4 &&
+                      kYeeTmaMediaShapes[1].planes == 3,
+                  "the dispatch below instantiates the shape lists in order");
+    if (!a.uniform) return shape == 1 ? launch_yee_tma_shape<3, 2, true, 3>(a, L, m, s) : launch_yee_tma_shape<4, 2, true, 2>(a, L, m, s);
+    switch (shape) {
+        case 1: return launch_yee_tma_shape<4, 2, false, 2>(a, L, m, s);
+        case 2: return launch_yee_tma_shape<3, 3, false, 2>(a, L, m, s);
+        default: return launch_yee_tma_shape<3, 2, false, 3>(a, L, m, s);
+    }
+}
+template <int P, int S, bool MEDIA, int MINB>
+static int yee_tma_occupancy() {
+    int n = 0;
+    const size_t smem = yee_tma_smem_bytes_for<P, MEDIA>(S);
+    if (allow_smem(yee_tma_step<P, S, false, MEDIA, MINB>, (int)smem) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<P, S, false, MEDIA, MINB>, 256, smem) != cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
 }
 
 cudaError_t launch_yee_near(const YeeNearArgs& a, bool solid, cudaStream_t s) {
@@ -239,24 +278,15 @@ int occupancy_f32(KernelId id) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>,
                                                               kEnsConsumers + 32, ens_tma_smem_bytes());
             break;
-        case kYeeTma:
-            e = allow_smem(yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>, (int)yee_tma_smem_bytes(false));
-            if (e != cudaSuccess) break;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanesUniform, kYeeTmaStages, false, false>,
-                                                              256, yee_tma_smem_bytes(false));
-            break;
-        case kYeeTmaMedia:
-            e = allow_smem(yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>, (int)yee_tma_smem_bytes(true));
-            if (e != cudaSuccess) break;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<kYeeTmaPlanesMedia, kYeeTmaStages, false, true>,
-                                                              256, yee_tma_smem_bytes(true));
-            break;
-        case kHallTma:
-            e = allow_smem(hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>, (int)hall_tma_smem_bytes());
-            if (e != cudaSuccess) break;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hall_tma_step<kHallTmaPlanes, kHallTmaStages, false>, 256,
-                                                              hall_tma_smem_bytes());
-            break;
+        case kYeeTma: return yee_tma_occupancy<3, 2, false, 3>();
+        case kYeeTmaShape1: return yee_tma_occupancy<4, 2, false, 2>();
+        case kYeeTmaShape2: return yee_tma_occupancy<3, 3, false, 2>();
+        case kYeeTmaMedia: return yee_tma_occupancy<4, 2, true, 2>();
+        case kYeeTmaMediaShape1: return yee_tma_occupancy<3, 2, true, 3>();
+        case kHallTma: return hall_tma_occupancy<8, 2, 2>();
+        case kHallTmaShape1: return hall_tma_occupancy<6, 2, 3>();
+        case kHallTmaShape2: return hall_tma_occupancy<4, 3, 3>();
+        case kHallTmaShape3: return hall_tma_occupancy<4, 2, 4>();
         case kRoomF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, room_step<float>, 256, 0); break;
         case kTubeF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tube_step<float>, 256, 0); break;
         case kBarF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bar_step<float>, 256, 0); break;

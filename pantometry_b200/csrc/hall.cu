@@ -1,5 +1,8 @@
 // pm_hall: the device form of `Hall` (crates/pantometry-acoustic/src/hall.rs).
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <limits>
 #include <new>
 
@@ -31,6 +34,7 @@ struct Hall : Handle {
     // and step with the TMA-staged kernel (hall_tma.cuh); maps[par] describe the fields of parity par
     bool tma = false;
     HallMaps maps[2];
+    int tshape = 0;  // the TMA kernel's tile shape, an index of kHallTmaShapes
 
     size_t nodes() const { return (size_t)nx * ny * nz; }
     size_t nvx() const { return (size_t)(nx - 1) * ny * nz; }
@@ -71,8 +75,8 @@ struct Hall : Handle {
         a.nwave = nwave;
         a.wsrc = wsrc;
         a.starting = starting ? 1 : 0;
-        const unsigned w = wave_of(sizeof(Real) == 8 ? kHallF64 : (tma ? kHallTma : kHallF32));
-        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w, (sizeof(Real) == 4 && tma) ? kHallTmaPlanes : 4));
+        const unsigned w = wave_of(sizeof(Real) == 8 ? kHallF64 : (tma ? hall_tma_kernel_id(tshape) : kHallF32));
+        a.tiles = make_tiles(nx, ny, nz, choose_zc(nx, ny, nz, w, (sizeof(Real) == 4 && tma) ? kHallTmaShapes[tshape].planes : 4));
         a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
         a.partials = partials.as<double>();
@@ -81,7 +85,7 @@ struct Hall : Handle {
 
     cudaError_t launch(int par, double h, bool starting, cudaStream_t s) const {
         if (precision == PM_PLAIN_F64) return launch_hall<double>(args<double>(par, h, starting), s);
-        if (tma) return launch_hall_tma(args<float>(par, h, starting), maps[par], s);
+        if (tma) return launch_hall_tma(args<float>(par, h, starting), maps[par], tshape, s);
         return launch_hall<float>(args<float>(par, h, starting), s);
     }
     pm_status launch_one(int par, double h, bool starting, cudaStream_t s) const {
@@ -91,7 +95,7 @@ struct Hall : Handle {
 
     // Tensor maps of both parities' fields, with the boxes hall_tma_step loads.
     pm_status build_maps() {
-        constexpr unsigned P = kHallTmaPlanes;
+        const unsigned P = (unsigned)kHallTmaShapes[tshape].planes;
         for (int q = 0; q < 2; ++q) {
             if (!hall_tma_map(&maps[q].p, p[q].p, nx, ny, nz, 40, 10, P + 2) ||
                 !hall_tma_map(&maps[q].vx, vx[q].p, nx, ny, nz, 36, 8, P) ||
@@ -100,6 +104,66 @@ struct Hall : Handle {
                 return fail(PM_CUDA_ERROR, "cuTensorMapEncodeTiled refused a hall field");
         }
         return PM_OK;
+    }
+
+    // Time `trial` steps of every TMA tile shape on the present state and keep the fastest. Each
+    // trial step reads the present parity and writes the other one, which is free between steps,
+    // so the fields are never touched; the books (the source's clock among them) are put back after
+    // each trial. A grid shape (nx, ny, nz, with or without speed blocks) timed once on a device is
+    // not timed again in the process.
+    pm_status autotune(int trial) {
+        if (!tma) return PM_OK;
+        static std::mutex cache_mutex;
+        static std::map<std::tuple<int, int, int, int, int>, int> cache;
+        const auto key = std::make_tuple(nx, ny, nz, block > 0 ? 1 : 0, device);
+        {
+            std::lock_guard<std::mutex> lock(cache_mutex);
+            auto it = cache.find(key);
+            if (it != cache.end()) return set_shape(it->second);
+        }
+        pm_status s = read_state();
+        if (s != PM_OK) return s;
+        const DevState books = *host_state;
+        const double c = block > 0 ? max_speed : speed;
+        const double dt = 0.5 * dx / (c * std::sqrt(3.0));
+        if ((s = upload_block_scale(dt)) != PM_OK) return s;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        PM_CUDA(cudaEventCreate(&e0));
+        PM_CUDA(cudaEventCreate(&e1));
+        int best = tshape;
+        float best_ms = 0.0f;
+        for (int sh = 0; sh < kHallTmaShapeCount && s == PM_OK; ++sh) {
+            if ((s = set_shape(sh)) != PM_OK) break;
+            host_state->tol = -1.0;  // no audit while timing
+            if ((s = write_state()) != PM_OK) break;
+            for (int q = 0; q < 2 + trial; ++q) {
+                if (q == 2) PM_CUDA(cudaEventRecord(e0, stream()));
+                PM_CUDA(launch(parity, dt, false, stream()));
+            }
+            PM_CUDA(cudaEventRecord(e1, stream()));
+            PM_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            PM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (sh == 0 || ms < best_ms) { best = sh; best_ms = ms; }
+            *host_state = books;
+            s = write_state();
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (s != PM_OK) return s;
+        {
+            std::lock_guard<std::mutex> lock(cache_mutex);
+            cache[key] = best;
+        }
+        return set_shape(best);
+    }
+    pm_status set_shape(int sh) {
+        if (sh < 0 || sh >= kHallTmaShapeCount) return fail(PM_BAD_ARG, "hall tile shape");
+        if (!tma || sh == tshape) return PM_OK;
+        PM_CUDA(cudaStreamSynchronize(stream()));
+        tshape = sh;
+        drop_graphs();
+        return build_maps();
     }
 
     // The ledger of the state in host_state: the energy, then the source's injected work as an
@@ -481,6 +545,34 @@ pm_status pm_hall_restore(pm_hall* hp) {
     st->prev_total = st->total;
     st->prev_scale = st->scale;
     return h->write_state();
+}
+
+pm_status pm_hall_autotune(pm_hall* hp, int trial_steps, int* planes, int* stages) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (trial_steps < 1) return fail(PM_BAD_ARG, "autotune: at least one trial step");
+    pm_status s = h->autotune(trial_steps);
+    if (s != PM_OK) return s;
+    if (planes) *planes = h->tma ? kHallTmaShapes[h->tshape].planes : 0;
+    if (stages) *stages = h->tma ? kHallTmaShapes[h->tshape].stages : 0;
+    return PM_OK;
+}
+
+pm_status pm_hall_set_tile(pm_hall* hp, int planes, int stages) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (!h->tma) return fail(PM_UNSUPPORTED, "tile shapes are those of the TMA-staged FP32 kernel (x extent a multiple of 4)");
+    for (int q = 0; q < kHallTmaShapeCount; ++q)
+        if (kHallTmaShapes[q].planes == planes && kHallTmaShapes[q].stages == stages) return h->set_shape(q);
+    return fail(PM_BAD_ARG, "hall tile: planes x stages of 8x2, 6x2, 4x3 or 4x2");
+}
+
+pm_status pm_hall_tile(pm_hall* hp, int* planes, int* stages) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    if (planes) *planes = h->tma ? kHallTmaShapes[h->tshape].planes : 0;
+    if (stages) *stages = h->tma ? kHallTmaShapes[h->tshape].stages : 0;
+    return PM_OK;
 }
 
 pm_status pm_hall_set_stream(pm_hall* hp, void* stream) {

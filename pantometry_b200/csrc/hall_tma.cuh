@@ -43,21 +43,19 @@ struct HallTmaStage {
     float vz[P + 1][8][32];
 };
 
-// Planes per stage, stages in the ring and resident blocks per SM: 8 planes in each of 2 stages
-// (87 KB of shared memory, two blocks per SM) measured fastest on B200 at 256³ among 2-8 planes
-// and 2-5 stages, and against three blocks per SM (6 planes × 2 stages: 166 Gcell/s; 4 × 3: 141;
-// this one: 176).
-#ifndef PM_HALL_TMA_PLANES
-#define PM_HALL_TMA_PLANES 8
-#endif
-#ifndef PM_HALL_TMA_STAGES
-#define PM_HALL_TMA_STAGES 2
-#endif
-#ifndef PM_HALL_TMA_MIN_BLOCKS
-#define PM_HALL_TMA_MIN_BLOCKS 2
-#endif
-constexpr int kHallTmaPlanes = PM_HALL_TMA_PLANES;
-constexpr int kHallTmaStages = PM_HALL_TMA_STAGES;
+// The tile shapes a hall can step with: planes per stage, stages in the ring, resident blocks per
+// SM the kernel is held to. Shape 0 (8 planes in each of 2 stages, 87 KB of shared memory, two
+// blocks per SM) measured fastest on B200 at 256³ among 2-8 planes and 2-5 stages in hand sweeps
+// (176 Gcell/s, against 166 for 6 × 2 at three blocks and 141 for 4 × 3); the others are the
+// runners-up, which pm_hall_autotune times on a hall's own grid. Every shape computes each node
+// with the same expressions, so they agree bit for bit.
+struct HallTmaShape {
+    int planes, stages, min_blocks;
+};
+constexpr HallTmaShape kHallTmaShapes[] = {{8, 2, 2}, {6, 2, 3}, {4, 3, 3}, {4, 2, 4}};
+constexpr int kHallTmaShapeCount = sizeof(kHallTmaShapes) / sizeof(kHallTmaShapes[0]);
+constexpr int kHallTmaPlanes = kHallTmaShapes[0].planes;
+constexpr int kHallTmaStages = kHallTmaShapes[0].stages;
 constexpr unsigned kMbarSpinLimit = 1u << 22;  // try_wait rounds before a wait gives up
 
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
@@ -115,8 +113,8 @@ __device__ __forceinline__ void hall_tma_issue(const HallMaps& m, unsigned stage
     tma_load_3d(stage + off(&z->vz[0][0][0]), &m.vz, c.x0, c.y0, c.k - 1, bar);
 }
 
-template <int P, int S, bool HET>
-static __global__ void __launch_bounds__(256, PM_HALL_TMA_MIN_BLOCKS) hall_tma_step(HallArgs<float> a, const __grid_constant__ HallMaps m) {
+template <int P, int S, bool HET, int MINB>
+static __global__ void __launch_bounds__(256, MINB) hall_tma_step(HallArgs<float> a, const __grid_constant__ HallMaps m) {
     DevState* st = a.st;
     if (st->violated) return;
     using St = HallTmaStage<P>;

@@ -64,7 +64,10 @@ inline cudaError_t launch_smem(void (*kernel)(P...), dim3 grid, dim3 block, int 
 // Multiprocessor, asked once per kernel and device), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps, kKernelCount
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps,
+    kHallTmaShape1, kHallTmaShape2, kHallTmaShape3,  // kHallTma is shape 0
+    kYeeTmaShape1, kYeeTmaShape2, kYeeTmaMediaShape1,  // kYeeTma and kYeeTmaMedia are shape 0 of each form
+    kKernelCount
 };
 int blocks_per_sm(KernelId id);
 
@@ -95,19 +98,38 @@ template <typename Real> cudaError_t launch_yee_walls(const YeeWallArgs<Real>& a
 template <typename Real>
 cudaError_t launch_yee_enforce_solid(const YeeWallArgs<Real>& a, const uint8_t* solid, cudaStream_t s);
 template <typename Real> cudaError_t launch_yee_coefs(const YeeCoefArgs<Real>& a, cudaStream_t s);
-// The FP32 Hall step staged by TMA (padded face layout, nx a multiple of 4).
-cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, cudaStream_t s);
-inline size_t hall_tma_smem_bytes() {
-    return sizeof(HallTmaStage<kHallTmaPlanes>) * kHallTmaStages + 8 * kHallTmaStages;
+// The FP32 Hall step staged by TMA (padded face layout, nx a multiple of 4), in tile shape `shape`
+// (an index of kHallTmaShapes).
+cudaError_t launch_hall_tma(const HallArgs<float>& a, const HallMaps& m, int shape, cudaStream_t s);
+template <int P, int S>
+inline size_t hall_tma_smem_bytes_for() {
+    return sizeof(HallTmaStage<P>) * S + 8 * S;
+}
+inline size_t hall_tma_smem_bytes(int shape = 0) {
+    switch (shape) {
+        case 1: return hall_tma_smem_bytes_for<6, 2>();
+        case 2: return hall_tma_smem_bytes_for<4, 3>();
+        case 3: return hall_tma_smem_bytes_for<4, 2>();
+        default: return hall_tma_smem_bytes_for<8, 2>();
+    }
+}
+inline KernelId hall_tma_kernel_id(int shape) {
+    return shape == 1 ? kHallTmaShape1 : shape == 2 ? kHallTmaShape2 : shape == 3 ? kHallTmaShape3 : kHallTma;
 }
 // Encode the tensor map of one f32 field of an nx × ny × nz hall (row pitch nx·4 bytes) with the
 // given box; false if the driver refuses it.
 bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz);
 // The FP32 uniform-medium cavity step staged by TMA (padded lattice of row pitch L).
-cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s);
-inline size_t yee_tma_smem_bytes(bool media = false) {
-    return media ? yee_tma_smem_bytes_for<kYeeTmaPlanesMedia, true>(kYeeTmaStages)
-                 : yee_tma_smem_bytes_for<kYeeTmaPlanesUniform, false>(kYeeTmaStages);
+// `shape` indexes the form's list (kYeeTmaUniformShapes, or kYeeTmaMediaShapes when !a.uniform).
+cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s);
+inline size_t yee_tma_smem_bytes(bool media = false, int shape = 0) {
+    const YeeTmaShape sh = yee_tma_shape(media, shape);
+    if (media) return sh.planes == 4 ? yee_tma_smem_bytes_for<4, true>(sh.stages) : yee_tma_smem_bytes_for<3, true>(sh.stages);
+    return sh.planes == 4 ? yee_tma_smem_bytes_for<4, false>(sh.stages) : yee_tma_smem_bytes_for<3, false>(sh.stages);
+}
+inline KernelId yee_tma_kernel_id(bool media, int shape) {
+    if (media) return shape == 1 ? kYeeTmaMediaShape1 : kYeeTmaMedia;
+    return shape == 1 ? kYeeTmaShape1 : shape == 2 ? kYeeTmaShape2 : kYeeTma;
 }
 // The FP32 cavity's near-field box in f64 after the TMA step (yee_near.cuh), and its seeding from
 // the stored field.

@@ -36,13 +36,24 @@ struct YeeMaps {
     CUtensorMap gx, gy, gz;  // per-edge gains of a cavity of mixed ε (MEDIA)
 };
 
-// Planes per stage and resident blocks per SM of each form, both with 2 stages in the ring: one
-// medium 3 planes at three blocks per SM (61 KB of shared memory a block), mixed ε 4 planes at two
-// (95 KB with its gain boxes). Measured on B200 at 384³: one medium 100 Gcell/s at 3 planes and
-// three blocks against 95 at 4 planes and two; mixed ε 85 at 4 planes and two against 60 at 3.
+// The tile shapes of each form: planes per stage, stages in the ring, resident blocks per SM the
+// kernel is held to. Shape 0 of each is the one hand sweeps chose on B200 at 384³: one medium 3
+// planes × 2 stages at three blocks per SM (61 KB of shared memory a block, 100 Gcell/s against 95
+// for 4 × 2 at two), mixed ε 4 × 2 at two (95 KB with its gain boxes, 85 against 60 for 3 × 2 at
+// three). The others are the runners-up, which pm_cavity_autotune times on a cavity's own grid.
+// Every shape computes each edge and face with the same expressions, so they agree bit for bit.
+struct YeeTmaShape {
+    int planes, stages, min_blocks;
+};
+constexpr YeeTmaShape kYeeTmaUniformShapes[] = {{3, 2, 3}, {4, 2, 2}, {3, 3, 2}};
+constexpr YeeTmaShape kYeeTmaMediaShapes[] = {{4, 2, 2}, {3, 2, 3}};
+constexpr int kYeeTmaUniformShapeCount = 3, kYeeTmaMediaShapeCount = 2;
+inline constexpr YeeTmaShape yee_tma_shape(bool media, int shape) {
+    return media ? kYeeTmaMediaShapes[shape] : kYeeTmaUniformShapes[shape];
+}
+inline constexpr int yee_tma_shape_count(bool media) { return media ? kYeeTmaMediaShapeCount : kYeeTmaUniformShapeCount; }
 constexpr int kYeeTmaStages = 2;
 constexpr int kYeeTmaPlanesUniform = 3, kYeeTmaPlanesMedia = 4;
-constexpr int yee_tma_planes(bool media) { return media ? kYeeTmaPlanesMedia : kYeeTmaPlanesUniform; }
 
 constexpr unsigned round128(unsigned b) { return (b + 127u) & ~127u; }
 
@@ -127,8 +138,8 @@ __device__ __forceinline__ void yee_tma_close(DevState* st, const double (&acc)[
     audit_and_commit(st, total, scale);
 }
 
-template <int P, int S, bool SOLID, bool MEDIA>
-static __global__ void __launch_bounds__(256, MEDIA ? 2 : 3) yee_tma_step(YeeStepArgs<float> a, unsigned L,
+template <int P, int S, bool SOLID, bool MEDIA, int MINB>
+static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m) {
     DevState* st = a.st;
     if (st->violated) return;

@@ -263,6 +263,22 @@ class Hall(_Domain):
         N.check(self._lib.pm_hall_download(self._h, _ptr(out), None, None, None, None))
         return out
 
+    def autotune(self, trial_steps=8):
+        """Time every tile shape of the TMA-staged FP32 kernel on the present state and keep the
+        fastest (the state and books are put back). Returns (planes, stages); (0, 0) where the hall
+        does not use that kernel."""
+        pl, st = C.c_int(), C.c_int()
+        N.check(self._lib.pm_hall_autotune(self._h, int(trial_steps), C.byref(pl), C.byref(st)))
+        return pl.value, st.value
+
+    def set_tile(self, planes, stages):
+        N.check(self._lib.pm_hall_set_tile(self._h, int(planes), int(stages)))
+
+    def tile(self):
+        pl, st = C.c_int(), C.c_int()
+        N.check(self._lib.pm_hall_tile(self._h, C.byref(pl), C.byref(st)))
+        return pl.value, st.value
+
     def fields(self):
         nx, ny, nz = self.nodes
         out = {
@@ -440,6 +456,22 @@ class Cavity(_Domain):
     def set_source(self, edge, current):
         w = _f64(current)
         N.check(self._lib.pm_cavity_set_source(self._h, int(edge), _ptr(w), w.size))
+
+    def autotune(self, trial_steps=8):
+        """Time every tile shape of the TMA-staged FP32 kernel on the present state and keep the
+        fastest (the state and books are put back). Returns (planes, stages); (0, 0) where the
+        cavity does not use that kernel."""
+        pl, st = C.c_int(), C.c_int()
+        N.check(self._lib.pm_cavity_autotune(self._h, int(trial_steps), C.byref(pl), C.byref(st)))
+        return pl.value, st.value
+
+    def set_tile(self, planes, stages):
+        N.check(self._lib.pm_cavity_set_tile(self._h, int(planes), int(stages)))
+
+    def tile(self):
+        pl, st = C.c_int(), C.c_int()
+        N.check(self._lib.pm_cavity_tile(self._h, C.byref(pl), C.byref(st)))
+        return pl.value, st.value
 
     def courant_limit(self):
         out = C.c_double()

@@ -85,3 +85,55 @@ def test_hall_tma_thin_halls():
                 continue
             scale = max(np.abs(fo[k]).max(), 1e-30)
             assert np.abs(fg[k] - fo[k]).max() <= 1e-4 * max(scale, 2.0), (dims, k)
+
+
+SHAPES = [(8, 2), (6, 2), (4, 3), (4, 2)]  # planes per stage × stages of the TMA kernel
+
+
+@pytest.mark.parametrize("speed_blocks", [False, True], ids=["one-medium", "speed-blocks"])
+def test_hall_tma_every_tile_shape_agrees_bit_for_bit(speed_blocks):
+    """Every tile shape computes each node with the same expressions; only the staging differs. A
+    hall with noise and the point source (and with speed blocks: the heterogeneous form) gives the
+    same FP32 fields and books under every shape, over 70 steps (a 64-step graph and single ones),
+    in chunks that exercise partial stages (28 planes)."""
+    from pantometry_b200 import workloads as W
+
+    cfg = W.acoustic_hall(28, steps=80)
+    runs = []
+    for shape in SHAPES:
+        h = W.build_hall(cfg, precision="f32")
+        if speed_blocks:
+            h.set_speed_blocks(8, np.linspace(300.0, 343.0, 64))
+        h.set_tile(*shape)
+        assert h.tile() == shape
+        h.set_tolerance(1e-6)
+        assert h.step(cfg["dt"], 70) is None
+        runs.append((h.fields(), h.ledger()))
+    (f0, l0) = runs[0]
+    for f, l in runs[1:]:
+        for k in f0:
+            assert np.array_equal(f[k].view(np.uint64), f0[k].view(np.uint64)), k
+        assert l["total"] == l0["total"] or abs(l["total"] - l0["total"]) <= 1e-12 * l0["scale"]
+
+
+def test_hall_autotune_keeps_state_books_and_source_clock():
+    from pantometry_b200 import workloads as W
+
+    cfg = W.acoustic_hall(36, steps=200)
+    a = W.build_hall(cfg, precision="f32")
+    b = W.build_hall(cfg, precision="f32")
+    for h in (a, b):
+        assert h.step(cfg["dt"], 30) is None
+    shape = a.autotune(trial_steps=4)
+    assert shape in SHAPES and a.tile() == shape
+    b.set_tile(*shape)
+    fa, fb = a.fields(), b.fields()
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
+    la, lb = a.ledger(), b.ledger()
+    assert la["steps"] == lb["steps"] == 30 and la["total"] == lb["total"]
+    for h in (a, b):
+        assert h.step(cfg["dt"], 40) is None  # the source goes on from its 31st sample in both
+    fa, fb = a.fields(), b.fields()
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k

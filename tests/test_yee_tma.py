@@ -234,3 +234,51 @@ def test_yee_f32_invariant_against_f64_over_2000_steps():
         assert g.step(dt, 2000) is None
         runs[prec] = g.ledger()
     assert abs(runs["f32"]["total"] - runs["f64"]["total"]) < 1e-6 * runs["f64"]["scale"]
+
+
+@pytest.mark.parametrize("media", [False, True], ids=["one-medium", "dielectric"])
+def test_yee_tma_every_tile_shape_agrees_bit_for_bit(media):
+    """Every tile shape of a form computes each edge and face with the same expressions: the same
+    FP32 fields under every shape, with the source's near field in f64, over 70 steps (a 64-step
+    graph and single launches) of a cavity whose planes do not fill whole stages."""
+    from pantometry_b200 import workloads as W
+
+    n = 30
+    shapes = [(4, 2), (3, 2)] if media else [(3, 2), (4, 2), (3, 3)]
+    if media:
+        cfg = W.dielectric_cavities(count=1, n=n, steps=100)
+    else:
+        cfg = W.yee_cavity(n, steps=100)
+    runs = []
+    for shape in shapes:
+        c = W.build_dielectric_cavity(cfg, 0, precision="f32") if media else W.build_cavity(cfg, precision="f32")
+        c.set_tile(*shape)
+        assert c.tile() == shape
+        c.set_tolerance(1e-6)
+        assert c.step(cfg["dt"], 70) is None
+        runs.append((c.fields(), c.ledger()))
+    f0, l0 = runs[0]
+    for f, l in runs[1:]:
+        for k in f0:
+            assert np.array_equal(f[k].view(np.uint64), f0[k].view(np.uint64)), k
+        assert abs(l["total"] - l0["total"]) <= 1e-12 * l0["scale"]
+
+
+def test_yee_autotune_keeps_state_books_and_source_clock():
+    from pantometry_b200 import workloads as W
+
+    cfg = W.yee_cavity(32, steps=200)
+    a = W.build_cavity(cfg, precision="f32")
+    b = W.build_cavity(cfg, precision="f32")
+    for c in (a, b):
+        assert c.step(cfg["dt"], 30) is None
+    shape = a.autotune(trial_steps=4)
+    assert shape in [(3, 2), (4, 2), (3, 3)] and a.tile() == shape
+    b.set_tile(*shape)
+    la, lb = a.ledger(), b.ledger()
+    assert la["steps"] == lb["steps"] == 30 and la["total"] == lb["total"]
+    for c in (a, b):
+        assert c.step(cfg["dt"], 40) is None
+    fa, fb = a.fields(), b.fields()
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
