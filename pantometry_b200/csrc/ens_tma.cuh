@@ -209,7 +209,6 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                     // a whole stage of interior cells: no film, no bound, the planes below and
                     // above carried in registers; the general form's arithmetic without its zeros
                     float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
-                    float stage_sum = 0.0f;  // the stage's new deviations, summed in f32, then into FP64
 #pragma unroll
                     for (int h = 0; h < P; ++h) {
                         const float above = s.t[h + 2][ty + 1][tx + 4];
@@ -219,11 +218,10 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                         const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
                         *out = nd;
                         out += plane;
-                        stage_sum += nd;
+                        acc[0] += (double)nd;
                         below = here;
                         here = above;
                     }
-                    acc[0] += (double)stage_sum;
                 } else {
                     // The general form, taken by the whole warp: its row (y) and each plane (z) are
                     // the same for every lane, so those tests are uniform, and a lane on an x face
@@ -240,8 +238,7 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                     const bool faces = ey0 || ey1 || ez0 || (ez1 && zlast < hn);
                     // the x faces' film coefficients, used by every cell of the stage, in registers
                     const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
-                    // the stage's new deviations and shed heat, summed in f32, then into FP64
-                    float stage_sum = 0.0f, col_shed = 0.0f;
+                    double col_shed = 0.0;
                     auto run = [&](auto faces_tag, auto full_tag) {
                         constexpr bool FACES = decltype(faces_tag)::value, FULL = decltype(full_tag)::value;
                         float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
@@ -274,12 +271,12 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                                     if (ez0 && h == 0) shed = __fmaf_rn(m.b[4], here + m.off[4], shed);
                                     if (ez1 && !zh) shed = __fmaf_rn(m.b[5], here + m.off[5], shed);
                                 }
-                                col_shed += shed;
+                                col_shed += (double)shed;
                             }
                             const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
                             *out = nd;
                             out += plane;
-                            stage_sum += nd;
+                            acc[0] += (double)nd;
                             below = here;
                             here = above;
                         }
@@ -291,8 +288,7 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                         if (hn == P) run(Flag<false>{}, Flag<true>{});
                         else run(Flag<false>{}, Flag<false>{});
                     }
-                    acc[0] += (double)stage_sum;
-                    acc[1] += (double)col_shed;
+                    acc[1] += col_shed;
                 }
             }
         }
@@ -311,12 +307,16 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                 const size_t at = ((size_t)brick * 8 + (size_t)warp) * 2;
                 a.partials[at] = acc[0];
                 a.partials[at + 1] = acc[1];
-                __threadfence();
-                ticket = atomicAdd(&st->counter, 1u);
+                // the ticket in acquire-release order: this lane's partials are visible to whoever
+                // takes a later ticket, and it sees those of every earlier one, without a full fence
+                // in every warp of every brick
+                asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(ticket) : "l"(&st->counter) : "memory");
             }
+            __syncwarp();  // the other lanes' reads below come after lane 0's acquire
             ticket = __shfl_sync(0xffffffffu, ticket, 0);
             if (ticket == g.nbricks * 8 - 1) {
-                __threadfence();
+                // the last ticket: every other warp's partials, acquired
+                asm volatile("fence.acq_rel.gpu;" ::: "memory");
                 double v[2] = {0.0, 0.0};
                 const size_t first = (size_t)g.first_brick * 8, count = (size_t)g.nbricks * 8;
                 for (size_t q = lane; q < count; q += 32) {

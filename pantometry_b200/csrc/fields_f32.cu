@@ -166,8 +166,8 @@ static int yee_tma_occupancy() {
 }
 
 cudaError_t launch_yee_near(const YeeNearArgs& a, bool solid, cudaStream_t s) {
-    if (solid) yee_near_step<true><<<1, 256, 0, s>>>(a);
-    else yee_near_step<false><<<1, 256, 0, s>>>(a);
+    if (solid) yee_near_step<true><<<1, kNearThreads, 0, s>>>(a);
+    else yee_near_step<false><<<1, kNearThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_yee_near_seed(const YeeNearArgs& a, cudaStream_t s) {

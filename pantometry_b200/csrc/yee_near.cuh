@@ -63,10 +63,35 @@ __device__ __forceinline__ size_t near_box(const YeeNearArgs& a, int q, int i, i
     const size_t w = (size_t)a.w;
     return (size_t)q * w * w * w + (size_t)(i - a.x0) + w * ((size_t)(j - a.y0) + w * (size_t)(k - a.z0));
 }
+// Component q's pointer of a lattice set, chosen by a switch: indexing the parameter block's array
+// with a runtime index would copy the whole block to local memory.
+__device__ __forceinline__ const float* near_comp(const float* const (&lat)[6], int q) {
+    switch (q) {
+        case 0: return lat[0];
+        case 1: return lat[1];
+        case 2: return lat[2];
+        case 3: return lat[3];
+        case 4: return lat[4];
+        default: return lat[5];
+    }
+}
+__device__ __forceinline__ float* near_comp(float* const (&lat)[6], int q) {
+    switch (q) {
+        case 0: return lat[0];
+        case 1: return lat[1];
+        case 2: return lat[2];
+        case 3: return lat[3];
+        case 4: return lat[4];
+        default: return lat[5];
+    }
+}
+__device__ __forceinline__ const float* near_comp(const float* const (&lat)[3], int q) {
+    return q == 0 ? lat[0] : q == 1 ? lat[1] : lat[2];
+}
 // The stored value of component q at node (i, j, k): f64 in the box, f32 outside.
-__device__ __forceinline__ double near_get(const YeeNearArgs& a, const double* box, const float* const* lat, int q,
-                                           int i, int j, int k) {
-    return near_in(a, i, j, k) ? box[near_box(a, q, i, j, k)] : (double)lat[q][near_lat(a, i, j, k)];
+__device__ __forceinline__ double near_get(const YeeNearArgs& a, const double* box, const float* lat_q, int q, int i,
+                                           int j, int k) {
+    return near_in(a, i, j, k) ? box[near_box(a, q, i, j, k)] : (double)lat_q[near_lat(a, i, j, k)];
 }
 
 // Seed the box's f64 values from the stored f32 field (after the state was set from outside a step).
@@ -75,12 +100,15 @@ static __global__ void yee_near_seed(YeeNearArgs a) {
     for (int r = threadIdx.x; r < 6 * w3; r += blockDim.x) {
         const int q = r / w3, l = r - q * w3;
         const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
-        a.nneu[r] = (double)a.neu[q][near_lat(a, i, j, k)];
+        a.nneu[r] = (double)near_comp(a.neu, q)[near_lat(a, i, j, k)];
     }
 }
 
+// One work item per (component, node): 3 × w³ in phases A and B, 3 × (w+1)³ in phase C.
+constexpr int kNearThreads = 384;
+
 template <bool SOLID>
-static __global__ void __launch_bounds__(256) yee_near_step(YeeNearArgs a) {
+static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs a) {
     DevState* st = a.st;
     if (st->violated) return;
     const int w = a.w, w3 = w * w * w;
@@ -88,88 +116,78 @@ static __global__ void __launch_bounds__(256) yee_near_step(YeeNearArgs a) {
     const long long step = st->steps;
     const double jsrc = (a.src_i >= 0 && step < a.ncurrent) ? a.current[step] : 0.0;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const float* const* lat_old = a.old;
-    const float* const* lat_neu = const_cast<const float* const*>(a.neu);
 
-    // A. H⁺ on the box's faces (cavity.rs:1346-1379), and the box's energy terms: ½ε|Eⁿ|² with
-    // the half weights of node-centred boundary samples (cavity.rs:766-772), ½μ H⁻·H⁺
-    for (int l = threadIdx.x; l < w3; l += blockDim.x) {
+    // A. H⁺ of face component q at each box node (cavity.rs:1346-1379) with its term of ½μ H⁻·H⁺,
+    // and the ½ε|Eⁿ|² term of edge component q there (half weights of node-centred boundary
+    // samples, cavity.rs:766-772)
+    for (int r = threadIdx.x; r < 3 * w3; r += blockDim.x) {
+        const int q = r / w3, l = r - q * w3;
         const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
         const double hi = (i == 0 || i == nx) ? 0.5 : 1.0, hj = (j == 0 || j == ny) ? 0.5 : 1.0,
                      hk = (k == 0 || k == nz) ? 0.5 : 1.0;
-        const double ex0 = a.nold[near_box(a, 0, i, j, k)], ey0 = a.nold[near_box(a, 1, i, j, k)],
-                     ez0 = a.nold[near_box(a, 2, i, j, k)];
-        const double wx = a.nold[near_box(a, 3, i, j, k)], wy = a.nold[near_box(a, 4, i, j, k)],
-                     wz = a.nold[near_box(a, 5, i, j, k)];
-        const double hxn = wx - a.ch * ((near_get(a, a.nold, lat_old, 2, i, j + 1, k) - ez0) -
-                                        (near_get(a, a.nold, lat_old, 1, i, j, k + 1) - ey0));
-        const double hyn = wy - a.ch * ((near_get(a, a.nold, lat_old, 0, i, j, k + 1) - ex0) -
-                                        (near_get(a, a.nold, lat_old, 2, i + 1, j, k) - ez0));
-        const double hzn = wz - a.ch * ((near_get(a, a.nold, lat_old, 1, i + 1, j, k) - ey0) -
-                                        (near_get(a, a.nold, lat_old, 0, i, j + 1, k) - ex0));
+        const double was = a.nold[near_box(a, 3 + q, i, j, k)];
+        double curl, wh;
+        if (q == 0) {  // hx: (ez(j+1) − ez) − (ey(k+1) − ey)
+            curl = (near_get(a, a.nold, a.old[2], 2, i, j + 1, k) - a.nold[near_box(a, 2, i, j, k)]) -
+                   (near_get(a, a.nold, a.old[1], 1, i, j, k + 1) - a.nold[near_box(a, 1, i, j, k)]);
+            wh = hi;
+        } else if (q == 1) {  // hy: (ex(k+1) − ex) − (ez(i+1) − ez)
+            curl = (near_get(a, a.nold, a.old[0], 0, i, j, k + 1) - a.nold[near_box(a, 0, i, j, k)]) -
+                   (near_get(a, a.nold, a.old[2], 2, i + 1, j, k) - a.nold[near_box(a, 2, i, j, k)]);
+            wh = hj;
+        } else {  // hz: (ey(i+1) − ey) − (ex(j+1) − ex)
+            curl = (near_get(a, a.nold, a.old[1], 1, i + 1, j, k) - a.nold[near_box(a, 1, i, j, k)]) -
+                   (near_get(a, a.nold, a.old[0], 0, i, j + 1, k) - a.nold[near_box(a, 0, i, j, k)]);
+            wh = hk;
+        }
+        const double hn = was - a.ch * curl;
         const size_t n = near_lat(a, i, j, k);
-        a.nneu[near_box(a, 3, i, j, k)] = hxn;
-        a.nneu[near_box(a, 4, i, j, k)] = hyn;
-        a.nneu[near_box(a, 5, i, j, k)] = hzn;
-        a.neu[3][n] = (float)hxn;
-        a.neu[4][n] = (float)hyn;
-        a.neu[5][n] = (float)hzn;
-        acc[1] += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
+        a.nneu[near_box(a, 3 + q, i, j, k)] = hn;
+        near_comp(a.neu, 3 + q)[n] = (float)hn;
+        acc[1] += wh * (hn * was);
+        const double e0 = a.nold[near_box(a, q, i, j, k)];
+        const double we = q == 0 ? hj * hk : q == 1 ? hi * hk : hi * hj;
         if (a.media)  // weighted by 1/g, the ε the update uses
-            acc[0] += (hj * hk) * (ex0 * ex0) / (double)a.cgain[0][n] + (hi * hk) * (ey0 * ey0) / (double)a.cgain[1][n] +
-                      (hi * hj) * (ez0 * ez0) / (double)a.cgain[2][n];
+            acc[0] += we * (e0 * e0) / (double)near_comp(a.cgain, q)[n];
         else
-            acc[0] += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+            acc[0] += we * (e0 * e0);
     }
     __syncthreads();  // the box's H⁺, in both stores, before any edge reads it
 
-    // B. Eⁿ⁺¹ on the box's edges (cavity.rs:1383-1452), the soft current, Joule loss
-    for (int l = threadIdx.x; l < w3; l += blockDim.x) {
+    // B. Eⁿ⁺¹ of edge component q at each box node (cavity.rs:1383-1452), the soft current, Joule loss
+    for (int r = threadIdx.x; r < 3 * w3; r += blockDim.x) {
+        const int q = r / w3, l = r - q * w3;
         const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
         const size_t n = near_lat(a, i, j, k);
-        auto hp = [&](int q, int ii, int jj, int kk) { return near_get(a, a.nneu, lat_neu, q, ii, jj, kk); };
-        const double cex = (hp(5, i, j, k) - hp(5, i, j - 1, k)) - (hp(4, i, j, k) - hp(4, i, j, k - 1));
-        const double cey = (hp(3, i, j, k) - hp(3, i, j, k - 1)) - (hp(5, i, j, k) - hp(5, i - 1, j, k));
-        const double cez = (hp(4, i, j, k) - hp(4, i - 1, j, k)) - (hp(3, i, j, k) - hp(3, i, j - 1, k));
-        const double ex0 = a.nold[near_box(a, 0, i, j, k)], ey0 = a.nold[near_box(a, 1, i, j, k)],
-                     ez0 = a.nold[near_box(a, 2, i, j, k)];
-        double gx = a.gain, gy = a.gain, gz = a.gain;
-        if (a.media) {
-            gx = (double)a.cgain[0][n];
-            gy = (double)a.cgain[1][n];
-            gz = (double)a.cgain[2][n];
-        }
-        double vx = a.decay * ex0 + gx * cex;
-        double vy = a.decay * ey0 + gy * cey;
-        double vz = a.decay * ez0 + gz * cez;
-        if (i == a.src_i && j == a.src_j && k == a.src_k) {
+        auto hp = [&](int c, int ii, int jj, int kk) { return near_get(a, a.nneu, near_comp(a.neu, c), c, ii, jj, kk); };
+        double curl;
+        if (q == 0) curl = (hp(5, i, j, k) - hp(5, i, j - 1, k)) - (hp(4, i, j, k) - hp(4, i, j, k - 1));
+        else if (q == 1) curl = (hp(3, i, j, k) - hp(3, i, j, k - 1)) - (hp(5, i, j, k) - hp(5, i - 1, j, k));
+        else curl = (hp(4, i, j, k) - hp(4, i - 1, j, k)) - (hp(3, i, j, k) - hp(3, i, j - 1, k));
+        const double e0 = a.nold[near_box(a, q, i, j, k)];
+        const double g = a.media ? (double)near_comp(a.cgain, q)[n] : a.gain;
+        double v = a.decay * e0 + g * curl;
+        if (q == 2 && i == a.src_i && j == a.src_j && k == a.src_k) {
             // soft current: ε dE/dt = ∇×H − J, with the σ term's semi-implicit divisor
             const double e = a.eps_src, ss = a.sig_src;
-            vz = vz - (a.dt / e) / (1.0 + (ss * a.dt / (2.0 * e))) * jsrc;
-            acc[3] += -(a.dt * a.volume) * jsrc * (0.5 * (ez0 + vz));
+            v = v - (a.dt / e) / (1.0 + (ss * a.dt / (2.0 * e))) * jsrc;
+            acc[3] += -(a.dt * a.volume) * jsrc * (0.5 * (e0 + v));
         }
         const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
-        const bool lx = iy && iz, ly = ix && iz, lz = ix && iy;
-        vx = lx ? vx : 0.0;
-        vy = ly ? vy : 0.0;
-        vz = lz ? vz : 0.0;
-        if (a.lossy) {
-            const double mx = 0.5 * (ex0 + vx), my = 0.5 * (ey0 + vy), mz = 0.5 * (ez0 + vz);
-            acc[2] += lx ? a.sig0 * mx * mx * a.dt * a.volume : 0.0;
-            acc[2] += ly ? a.sig0 * my * my * a.dt * a.volume : 0.0;
-            acc[2] += lz ? a.sig0 * mz * mz * a.dt * a.volume : 0.0;
+        const bool interior = q == 0 ? (iy && iz) : q == 1 ? (ix && iz) : (ix && iy);
+        v = interior ? v : 0.0;
+        if (a.lossy && interior) {
+            const double m = 0.5 * (e0 + v);
+            acc[2] += a.sig0 * m * m * a.dt * a.volume;
         }
         if constexpr (SOLID) {
-            if (touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)) vx = 0.0;
-            if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) vy = 0.0;
-            if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) vz = 0.0;
+            const bool hit = q == 0   ? touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)
+                             : q == 1 ? touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)
+                                      : touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k);
+            if (hit) v = 0.0;
         }
-        a.nneu[near_box(a, 0, i, j, k)] = vx;
-        a.nneu[near_box(a, 1, i, j, k)] = vy;
-        a.nneu[near_box(a, 2, i, j, k)] = vz;
-        a.neu[0][n] = (float)vx;
-        a.neu[1][n] = (float)vy;
-        a.neu[2][n] = (float)vz;
+        a.nneu[near_box(a, q, i, j, k)] = v;
+        near_comp(a.neu, q)[n] = (float)v;
     }
 
     // C. The edges just outside the box whose curl reads a box face: the nodes of the (w+1)³ cube
@@ -177,41 +195,41 @@ static __global__ void __launch_bounds__(256) yee_near_step(YeeNearArgs a) {
     // (the box's own faces now hold the roundings of their f64 values), as yee_tma_step forms it;
     // with a lossy medium the Joule term yee_tma_step booked for it is replaced by this value's.
     const int w1 = w + 1, ring = w1 * w1 * w1;
-    for (int l = threadIdx.x; l < ring; l += blockDim.x) {
+    for (int r = threadIdx.x; r < 3 * ring; r += blockDim.x) {
+        const int q = r / ring, l = r - q * ring;
         const int i = a.x0 + l % w1, j = a.y0 + (l / w1) % w1, k = a.z0 + l / (w1 * w1);
         if (near_in(a, i, j, k)) continue;
+        // which faces the curl of component q reads besides the node's own: x reads j−1 and
+        // k−1, y reads k−1 and i−1, z reads i−1 and j−1
+        const bool reads = q == 0   ? (near_in(a, i, j - 1, k) || near_in(a, i, j, k - 1))
+                           : q == 1 ? (near_in(a, i, j, k - 1) || near_in(a, i - 1, j, k))
+                                    : (near_in(a, i - 1, j, k) || near_in(a, i, j - 1, k));
+        if (!reads) continue;
         const size_t n = near_lat(a, i, j, k);
-        auto h = [&](int q, int ii, int jj, int kk) { return lat_neu[q][near_lat(a, ii, jj, kk)]; };
+        auto h = [&](int c, int ii, int jj, int kk) { return near_comp(a.neu, c)[near_lat(a, ii, jj, kk)]; };
+        const float before = near_comp(a.old, q)[n];
+        float curl;
+        if (q == 0) curl = (h(5, i, j, k) - h(5, i, j - 1, k)) - (h(4, i, j, k) - h(4, i, j, k - 1));
+        else if (q == 1) curl = (h(3, i, j, k) - h(3, i, j, k - 1)) - (h(5, i, j, k) - h(5, i - 1, j, k));
+        else curl = (h(4, i, j, k) - h(4, i - 1, j, k)) - (h(3, i, j, k) - h(3, i, j - 1, k));
+        const float gq = a.media ? near_comp(a.cgain, q)[n] : a.gainf;
+        float v = a.decf * before + gq * curl;
         const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
-        for (int q = 0; q < 3; ++q) {
-            // which faces the curl of component q reads besides the node's own: x reads j−1 and
-            // k−1, y reads k−1 and i−1, z reads i−1 and j−1
-            const bool reads = q == 0   ? (near_in(a, i, j - 1, k) || near_in(a, i, j, k - 1))
-                               : q == 1 ? (near_in(a, i, j, k - 1) || near_in(a, i - 1, j, k))
-                                        : (near_in(a, i - 1, j, k) || near_in(a, i, j - 1, k));
-            if (!reads) continue;
-            const float before = a.old[q][n];
-            float curl;
-            if (q == 0) curl = (h(5, i, j, k) - h(5, i, j - 1, k)) - (h(4, i, j, k) - h(4, i, j, k - 1));
-            else if (q == 1) curl = (h(3, i, j, k) - h(3, i, j, k - 1)) - (h(5, i, j, k) - h(5, i - 1, j, k));
-            else curl = (h(4, i, j, k) - h(4, i - 1, j, k)) - (h(3, i, j, k) - h(3, i, j - 1, k));
-            const float gq = a.media ? a.cgain[q][n] : a.gainf;
-            float v = a.decf * before + gq * curl;
-            const bool interior = q == 0 ? (iy && iz) : q == 1 ? (ix && iz) : (ix && iy);
-            v = interior ? v : 0.0f;
-            if (a.lossy && interior) {
-                const double mold = 0.5 * ((double)before + (double)a.neu[q][n]);
-                const double mnew = 0.5 * ((double)before + (double)v);
-                acc[2] += a.sig0 * mnew * mnew * a.dt * a.volume - a.sig0 * mold * mold * a.dt * a.volume;
-            }
-            if constexpr (SOLID) {
-                const bool hit = q == 0   ? touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)
-                                 : q == 1 ? touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)
-                                          : touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k);
-                if (hit) v = 0.0f;
-            }
-            a.neu[q][n] = v;
+        const bool interior = q == 0 ? (iy && iz) : q == 1 ? (ix && iz) : (ix && iy);
+        v = interior ? v : 0.0f;
+        float* out = near_comp(a.neu, q);
+        if (a.lossy && interior) {
+            const double mold = 0.5 * ((double)before + (double)out[n]);
+            const double mnew = 0.5 * ((double)before + (double)v);
+            acc[2] += a.sig0 * mnew * mnew * a.dt * a.volume - a.sig0 * mold * mold * a.dt * a.volume;
         }
+        if constexpr (SOLID) {
+            const bool hit = q == 0   ? touches_solid(a.solid, nx, ny, nz, i, i, j - 1, j, k - 1, k)
+                             : q == 1 ? touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)
+                                      : touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k);
+            if (hit) v = 0.0f;
+        }
+        out[n] = v;
     }
 
     // D. the box's sums in a fixed order, added to yee_tma_step's, and the books
