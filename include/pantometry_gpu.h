@@ -116,6 +116,22 @@ pm_status pm_heat_fill(pm_heat* h, const pm_substance* substance, const uint8_t*
  * `area` is the whole face's area; convection may be +inf (a Dirichlet face). */
 pm_status pm_heat_losing_from(pm_heat* h, int face, double ambient_kelvin,
                               double convection_w_per_m2_k, double area);
+/* Solid3D::empty (solid.rs:986-1005): cells with mask[c] != 0 become void. A void cell holds no
+ * heat, conducts nothing, takes no share of absorbed heat and generates nothing; its value in the
+ * downloaded field is a placeholder that never changes (solid.rs:1324-1335 reads it as NaN). Two
+ * solid cells facing each other along a grid line across a run of void radiate to each other,
+ * σA(T1^4 - T2^4)/(1/e1 + 1/e2 - 1) (solid.rs:786-838, 1866-1878); the limit then follows the
+ * state, and a block with such gaps steps on the plain f64 form only. */
+pm_status pm_heat_empty(pm_heat* h, const uint8_t* mask, size_t n);
+/* Solid3D::dissipating (solid.rs:1045-1085): `watts` in total, spread evenly over the solid cells
+ * with mask[c] != 0, replacing what they generated before; selecting no solid cell does nothing. */
+pm_status pm_heat_dissipating(pm_heat* h, double watts, const uint8_t* mask, size_t n);
+/* Solid3D::generated_power and generated_energy (solid.rs:1118-1126); either may be NULL. */
+pm_status pm_heat_generated(pm_heat* h, double* watts, double* joules);
+/* The gap pairs (first cell, second cell, coefficient in W/K^4) in the order the step applies
+ * them; *count is the number of pairs, of which the first `capacity` are written. */
+pm_status pm_heat_gaps(pm_heat* h, long long* a, long long* b, double* coefficient, size_t capacity,
+                       size_t* count);
 /* Solid3D::set_temperature over every cell (solid.rs:1346-1361), kelvin, index x + nx(y + ny z). */
 pm_status pm_heat_upload(pm_heat* h, const double* kelvin, size_t n);
 pm_status pm_heat_download(pm_heat* h, double* kelvin, size_t n);

@@ -94,6 +94,11 @@ def _declare(L):
         "or_heat_free": (None, [p]),
         "or_heat_losing_from": (None, [p, i, d, d, d]),
         "or_heat_fill": (None, [p, d, d, d, d, i, C.c_void_p]),
+        "or_heat_empty": (None, [p, C.c_void_p]),
+        "or_heat_dissipating": (None, [p, d, C.c_void_p]),
+        "or_heat_generated_power": (d, [p]),
+        "or_heat_generated_energy": (d, [p]),
+        "or_heat_gaps": (C.c_longlong, [p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]),
         "or_heat_set_cells": (None, [p, dp]),
         "or_heat_get_cells": (None, [p, dp]),
         "or_heat_get_coefficients": (None, [p, dp, dp, dp, dp, dp]),
@@ -231,6 +236,36 @@ class Heat(_Box):
         lib().or_heat_fill(self._h, density, conductivity, specific_heat, emissivity, int(thermal),
                            m.ctypes.data_as(C.c_void_p))
         return self
+
+    def empty(self, mask):
+        """solid.rs:986-1005: the cells the mask selects become void."""
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        assert m.size == self.n
+        lib().or_heat_empty(self._h, m.ctypes.data_as(C.c_void_p))
+        return self
+
+    def dissipating(self, watts, mask):
+        """solid.rs:1045-1085: `watts` spread over the solid cells the mask selects."""
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        assert m.size == self.n
+        lib().or_heat_dissipating(self._h, watts, m.ctypes.data_as(C.c_void_p))
+        return self
+
+    def generated_power(self):
+        return lib().or_heat_generated_power(self._h)
+
+    def generated_energy(self):
+        return lib().or_heat_generated_energy(self._h)
+
+    def gaps(self):
+        """The gap pairs (a, b, coefficient) in the order the step applies them."""
+        count = lib().or_heat_gaps(self._h, None, None, None, 0)
+        a = np.zeros(count, dtype=np.int64)
+        b = np.zeros(count, dtype=np.int64)
+        g = np.zeros(count)
+        lib().or_heat_gaps(self._h, a.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p),
+                           g.ctypes.data_as(C.c_void_p), count)
+        return a, b, g
 
     @property
     def cells(self):

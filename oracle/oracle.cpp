@@ -145,6 +145,12 @@ struct Heat {
     std::vector<uint32_t> which;
     std::vector<double> cells, saved;
     std::vector<double> kx, ky, kz, mobility, capacity, face_sum;
+    // solid.rs:238-266: void cells, the gap pairs across them (a, b, σA/(1/ε₁+1/ε₂−1)) and the
+    // watts each cell generates
+    std::vector<uint8_t> vd;
+    struct Gap { size_t a, b; double coefficient; };
+    std::vector<Gap> gaps;
+    std::vector<double> source;
     double worst_rate = 0.0;
     bool exposed[6] = {false, false, false, false, false, false};
     Env env[6];
@@ -193,13 +199,16 @@ struct Heat {
         return m.thermal ? m.emissivity : 0.0;
     }
 
-    // solid.rs:588-784, one-phase, no void: face conductivities, capacity, mobility, face_sum,
-    // worst_rate.
+    // solid.rs:588-784, one-phase: face conductivities, capacity, mobility, face_sum, worst_rate,
+    // then the gaps (solid.rs:783).
     void resolve() {
         double volume = dx * dx * dx;
         size_t N = n();
+        if (vd.size() != N) vd.assign(N, 0);
+        if (source.size() != N) source.assign(N, 0.0);
         std::vector<double> kmix(N), cmix(N);
         for (size_t c = 0; c < N; ++c) {
+            if (vd[c]) { kmix[c] = 0.0; cmix[c] = 0.0; continue; }  // solid.rs:689-694
             const Material& m = mats[which[c]];
             double k = m.thermal ? m.conductivity : NAN;
             // `heat_capacity(volume)` = (density * volume) * specific_heat (substance.rs:219-239)
@@ -238,7 +247,7 @@ struct Heat {
                     size_t c = i + (size_t)nx * (j + (size_t)ny * k);
                     double cap = cmix[c];
                     capacity[c] = cap;
-                    mobility[c] = dx / cap;
+                    mobility[c] = vd[c] ? 0.0 : dx / cap;  // solid.rs:753-756
                     double sum = kx[i + (size_t)(nx + 1) * (j + (size_t)ny * k)] +
                                  kx[i + 1 + (size_t)(nx + 1) * (j + (size_t)ny * k)] +
                                  ky[i + (size_t)nx * (j + (size_t)(ny + 1) * k)] +
@@ -253,7 +262,60 @@ struct Heat {
                         worst_rate = rmax(worst_rate, rate);
                 }
         if (nowhere) worst_rate = NAN;
+        find_gaps();
     }
+
+    // solid.rs:786-838 `find_gaps`: along every row, then every column, then every pillar, a run
+    // of void with solid at both ends pairs the two end cells.
+    void find_gaps() {
+        gaps.clear();
+        bool any = false;
+        for (uint8_t v : vd) any = any || v;
+        if (!any) return;
+        const double area = dx * dx;
+        auto walk = [&](size_t first, size_t stride, int len) {
+            bool have_last = false, void_between = false;
+            size_t last = 0;
+            for (int q = 0; q < len; ++q) {
+                const size_t c = first + stride * (size_t)q;
+                if (vd[c]) { void_between = have_last; continue; }
+                if (have_last && void_between) {
+                    const double ea = mat_emissivity(last), eb = mat_emissivity(c);
+                    if (ea > 0.0 && eb > 0.0) {
+                        const double resistance = 1.0 / ea + 1.0 / eb - 1.0;
+                        if (resistance > 0.0) gaps.push_back(Gap{last, c, STEFAN_BOLTZMANN * area / resistance});
+                    }
+                }
+                last = c;
+                have_last = true;
+                void_between = false;
+            }
+        };
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j) walk((size_t)nx * (j + (size_t)ny * k), 1, nx);
+        for (int k = 0; k < nz; ++k)
+            for (int i = 0; i < nx; ++i) walk(i + (size_t)nx * ny * k, (size_t)nx, ny);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) walk(i + (size_t)nx * j, (size_t)nx * ny, nz);
+    }
+
+    // solid.rs:1045-1085 `dissipating`: `watts` spread evenly over the solid cells the mask
+    // selects, replacing what they generated before.
+    void dissipating(double watts, const uint8_t* mask) {
+        std::vector<size_t> chosen;
+        for (size_t c = 0; c < n(); ++c)
+            if (!vd[c] && mask[c]) chosen.push_back(c);
+        if (chosen.empty()) return;
+        const double each = watts / (double)chosen.size();
+        for (size_t c : chosen) source[c] = each;
+        resolve();
+    }
+    bool supplies() const {  // solid.rs:1110-1112
+        for (double w : source) if (w != 0.0) return true;
+        return false;
+    }
+    // solid.rs:1324-1335 `temperature_at`: not a number where there is nothing.
+    double temperature_at(size_t c) const { return vd[c] ? NAN : cells[c]; }
 
     // solid.rs:1269-1288
     double loss_conductance_at(double at, int i, int j, int k, size_t c) const {
@@ -269,17 +331,23 @@ struct Heat {
         return total;
     }
 
-    // solid.rs:1148-1185 (no gaps)
+    // solid.rs:1148-1185
     double worst_rate_now() const {
         bool any = false;
         for (int f = 0; f < 6; ++f) any = any || exposed[f];
-        if (!any || std::isnan(worst_rate)) return worst_rate;
+        if ((!any && gaps.empty()) || std::isnan(worst_rate)) return worst_rate;
         double worst = worst_rate;
+        for (const Gap& g : gaps) {
+            const double hotter = rmax(cells[g.a], cells[g.b]);
+            const double cond = 4.0 * g.coefficient * powi3(hotter);
+            for (size_t c : {g.a, g.b})
+                if (capacity[c] > 0.0) worst = rmax(worst, cond / capacity[c]);
+        }
         for (int k = 0; k < nz; ++k)
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < nx; ++i) {
                     size_t c = i + (size_t)nx * (j + (size_t)ny * k);
-                    double loss = loss_conductance_at(cells[c], i, j, k, c);
+                    double loss = loss_conductance_at(temperature_at(c), i, j, k, c);
                     if (loss == 0.0) continue;
                     worst = rmax(worst, mobility[c] * (face_sum[c] + loss / dx));
                 }
@@ -359,6 +427,23 @@ struct Heat {
                     cells[c] += dts * mobility[c] * (flux - shed);  // add_kelvin, latent <= 0
                     if (shed != 0.0) lost += dts * mobility[c] * shed * capacity[c];
                 }
+        // solid.rs:1854-1864: heat that has a place, after the sweep
+        if (supplies()) {
+            for (size_t c = 0; c < n(); ++c) {
+                if (source[c] == 0.0 || vd[c]) continue;
+                const double joules = source[c] * dts;
+                cells[c] += joules / capacity[c];
+                supplied += joules;
+            }
+        }
+        // solid.rs:1866-1878: what the gaps carry, read off `old`, in the pairs' order
+        for (const Gap& g : gaps) {
+            const double watts = g.coefficient * (powi4(old[g.a]) - powi4(old[g.b]));
+            if (watts == 0.0) continue;
+            const double joules = watts * dts;
+            cells[g.a] += -joules / capacity[g.a];
+            cells[g.b] += joules / capacity[g.b];
+        }
         return true;
     }
 
@@ -369,7 +454,8 @@ struct Heat {
         double cap_sum = -0.0;
         for (double c : capacity) cap_sum += c;
         double rise = gained / cap_sum;
-        for (size_t c = 0; c < n(); ++c) cells[c] += rise;
+        for (size_t c = 0; c < n(); ++c)
+            if (!vd[c]) cells[c] += rise;  // void takes no share (solid.rs:1756-1764)
     }
 };
 
@@ -1323,6 +1409,31 @@ void or_heat_fill(void* p, double density, double conductivity, double specific_
     for (size_t c = 0; c < h->n(); ++c)
         if (mask[c]) h->which[c] = (uint32_t)id;
     h->resolve();
+}
+// solid.rs:986-1005 `empty`: cells where mask != 0 become void.
+void or_heat_empty(void* p, const uint8_t* mask) {
+    Heat* h = (Heat*)p;
+    for (size_t c = 0; c < h->n(); ++c)
+        if (mask[c]) h->vd[c] = 1;
+    h->resolve();
+}
+void or_heat_dissipating(void* p, double watts, const uint8_t* mask) { ((Heat*)p)->dissipating(watts, mask); }
+// solid.rs:1118-1126: watts summed over the cells, and the joules generated over the run
+double or_heat_generated_power(void* p) {
+    double s = -0.0;
+    for (double w : ((Heat*)p)->source) s += w;
+    return s;
+}
+double or_heat_generated_energy(void* p) { return ((Heat*)p)->supplied; }
+// The gap pairs in the reference's order: up to `cap` of them into a, b, coefficient; the count.
+long long or_heat_gaps(void* p, long long* a, long long* b, double* coefficient, long long cap) {
+    Heat* h = (Heat*)p;
+    for (size_t q = 0; q < h->gaps.size() && (long long)q < cap; ++q) {
+        a[q] = (long long)h->gaps[q].a;
+        b[q] = (long long)h->gaps[q].b;
+        coefficient[q] = h->gaps[q].coefficient;
+    }
+    return (long long)h->gaps.size();
 }
 void or_heat_set_cells(void* p, const double* t) { Heat* h = (Heat*)p; std::memcpy(h->cells.data(), t, h->n() * 8); }
 void or_heat_get_cells(void* p, double* t) { Heat* h = (Heat*)p; std::memcpy(t, h->cells.data(), h->n() * 8); }

@@ -161,6 +161,10 @@ SIGNATURES = {
     "pm_heat_create": (_st, [C.POINTER(HeatDesc), C.POINTER(_p)]),
     "pm_heat_fill": (_st, [_p, C.POINTER(Substance), _p, _sz]),
     "pm_heat_losing_from": (_st, [_p, _i, _d, _d, _d]),
+    "pm_heat_empty": (_st, [_p, _p, _sz]),
+    "pm_heat_dissipating": (_st, [_p, _d, _p, _sz]),
+    "pm_heat_generated": (_st, [_p, _dp, _dp]),
+    "pm_heat_gaps": (_st, [_p, _p, _p, _p, _sz, C.POINTER(_sz)]),
     "pm_heat_upload": (_st, [_p, _dp, _sz]),
     "pm_heat_download": (_st, [_p, _dp, _sz]),
     "pm_heat_max_stable_dt": (_st, [_p, _dp]),

@@ -32,6 +32,12 @@ struct Heat : Handle {
     double dx = 0.0, reference = 0.0;
     std::vector<pm_substance> mats;
     std::vector<uint32_t> which;  // empty while the block is one material
+    // solid.rs:238-266: void cells (empty while there are none), the watts each cell generates
+    // (empty while nothing does) and the gap pairs across the void, in the order they were found
+    std::vector<uint8_t> vd;
+    std::vector<double> source;
+    struct Gap { size_t a, b; double coefficient; };
+    std::vector<Gap> gaps;
     HeatFilms films{};
     double film_conv[6] = {0, 0, 0, 0, 0, 0};
     // `resolve` products (solid.rs:588-784)
@@ -43,6 +49,7 @@ struct Heat : Handle {
     // device buffers
     DBuf field[2];  // f64 kelvin (plain) or f32 deviations
     DBuf dkx, dky, dkz, dmob, dcap, dwhich, dmatk, dmateps;
+    DBuf dsrc, dvoid, dgap_of, dgaps;  // watts per cell (zero on void), void flags, the gap table
     // the FP32 form of a filled block: face conductivities and film conductances in f32, and
     // dt·mobility per cell for the step size m_dt
     DBuf dkx32, dky32, dkz32, dm32, dfilm32;
@@ -67,9 +74,11 @@ struct Heat : Handle {
     double mat_k(uint32_t m) const { return mats[m].thermal ? mats[m].conductivity : std::numeric_limits<double>::infinity(); }
     double mat_eps(uint32_t m) const { return mats[m].thermal ? mats[m].emissivity : 0.0; }
     uint32_t mat_of(size_t c) const { return which.empty() ? 0u : which[c]; }
+    bool is_void(size_t c) const { return !vd.empty() && vd[c]; }
 
-    // Per-cell (k, C) of a one-phase block (solid.rs:600-702 with φ = 0).
+    // Per-cell (k, C) of a one-phase block (solid.rs:600-702 with φ = 0); nothing for void.
     void cell_props(size_t c, double& k, double& C) const {
+        if (is_void(c)) { k = 0.0; C = 0.0; return; }
         const pm_substance& s = mats[mat_of(c)];
         const double volume = dx * dx * dx;
         const double ks = s.thermal ? s.conductivity : NAN;
@@ -97,9 +106,10 @@ struct Heat : Handle {
     }
     double mob_at(size_t c) const { return uniform ? mobility : mob[c]; }
 
-    // solid.rs:588-784 for a one-phase block with no void.
+    // solid.rs:588-784 for a one-phase block; a block with void or a source is a filled one.
     void resolve() {
-        uniform = mats.size() == 1;
+        uniform = mats.size() == 1 && vd.empty() && source.empty();
+        gaps.clear();
         const size_t N = n();
         if (uniform) {
             double k, C;
@@ -152,17 +162,52 @@ struct Heat : Handle {
                 for (int i = 0; i < nx; ++i) {
                     size_t c = i + (size_t)nx * (j + (size_t)ny * k);
                     cap[c] = cm[c];
-                    mob[c] = dx / cm[c];
+                    mob[c] = is_void(c) ? 0.0 : dx / cm[c];  // solid.rs:753-756
                     cap_sum += cm[c];
                     double rate = mob[c] * face_sum_at(i, j, k);
                     if (std::isnan(rate)) nowhere = true;
                     else worst_rate = rust_max(worst_rate, rate);
                 }
         if (nowhere) worst_rate = NAN;
+        find_gaps();
+    }
+
+    // solid.rs:786-838 `find_gaps`: along every row, then every column, then every pillar, a run
+    // of void with solid at both ends pairs its two end cells, with the parallel-plate series.
+    void find_gaps() {
+        gaps.clear();
+        if (vd.empty()) return;
+        const double area = dx * dx;
+        auto walk = [&](size_t first, size_t stride, int len) {
+            bool have_last = false, void_between = false;
+            size_t last = 0;
+            for (int q = 0; q < len; ++q) {
+                const size_t c = first + stride * (size_t)q;
+                if (vd[c]) { void_between = have_last; continue; }
+                if (have_last && void_between) {
+                    const double ea = mat_eps(mat_of(last)), eb = mat_eps(mat_of(c));
+                    if (ea > 0.0 && eb > 0.0) {
+                        const double resistance = 1.0 / ea + 1.0 / eb - 1.0;
+                        if (resistance > 0.0) gaps.push_back(Gap{last, c, kStefanBoltzmann * area / resistance});
+                    }
+                }
+                last = c;
+                have_last = true;
+                void_between = false;
+            }
+        };
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j) walk((size_t)nx * (j + (size_t)ny * k), 1, nx);
+        for (int k = 0; k < nz; ++k)
+            for (int i = 0; i < nx; ++i) walk(i + (size_t)nx * ny * k, (size_t)nx, ny);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) walk(i + (size_t)nx * j, (size_t)nx * ny, nz);
     }
 
     // Radiating films: the step limit follows the state (solid.rs:1148-1185).
     bool radiating() const { return films.exposed && any_radiative_film(); }
+    // Radiating films or radiative gaps: the limit follows the state.
+    bool state_dependent() const { return radiating() || !gaps.empty(); }
 
     // solid.rs:1269-1288 `loss_conductance_at` at temperature `at`, summed from −0.0 (Rust's
     // `Sum for f64`), radiating term included.
@@ -180,16 +225,24 @@ struct Heat : Handle {
         }
         return total;
     }
-    // solid.rs:1148-1185 over a state `t` (kelvin, reference order).
+    // solid.rs:1148-1185 over a state `t` (kelvin, reference order); a void cell's temperature is
+    // not a number (solid.rs:1324-1335).
     double worst_rate_of(const std::vector<double>& t) const {
-        if (films.exposed == 0 || std::isnan(worst_rate)) return worst_rate;
+        if ((films.exposed == 0 && gaps.empty()) || std::isnan(worst_rate)) return worst_rate;
         double worst = worst_rate;
+        for (const Gap& g : gaps) {
+            const double hotter = rust_max(t[g.a], t[g.b]);
+            const double cond = 4.0 * g.coefficient * (hotter * (hotter * hotter));  // powi(3)
+            for (size_t c : {g.a, g.b})
+                if (cap[c] > 0.0) worst = rust_max(worst, cond / cap[c]);
+        }
+        if (films.exposed == 0) return worst;
         for (int k = 0; k < nz; ++k)
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < nx; ++i) {
                     if (!(i == 0 || i + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz)) continue;
                     const size_t c = i + (size_t)nx * (j + (size_t)ny * k);
-                    const double loss = loss_conductance_at(t[c], i, j, k, c);
+                    const double loss = loss_conductance_at(is_void(c) ? NAN : t[c], i, j, k, c);
                     if (loss == 0.0) continue;
                     worst = rust_max(worst, mob_at(c) * (face_sum_at(i, j, k) + loss / dx));
                 }
@@ -198,7 +251,7 @@ struct Heat : Handle {
     // The rate of the present state into the device books, where the films radiate: the step
     // kernels keep it from then on, step by step.
     pm_status refresh_rate() {
-        if (precision != PM_PLAIN_F64 || !radiating()) return PM_OK;
+        if (precision != PM_PLAIN_F64 || !state_dependent()) return PM_OK;
         std::vector<double> t(n());
         PM_CUDA(cudaMemcpyAsync(t.data(), field[parity].p, n() * 8, cudaMemcpyDeviceToHost, stream()));
         PM_CUDA(cudaStreamSynchronize(stream()));
@@ -284,6 +337,7 @@ struct Heat : Handle {
         if ((s = put32(dky32, ky)) != PM_OK) return s;
         if ((s = put32(dkz32, kz)) != PM_OK) return s;
         if ((s = put_buf(dcap, cap.data(), cap.size() * 8)) != PM_OK) return s;
+        if ((s = upload_places()) != PM_OK) return s;
         m_dt = NAN;
         return upload_films_f32();
     }
@@ -343,6 +397,43 @@ struct Heat : Handle {
         for (uint32_t m = 0; m < mats.size(); ++m) { mk[m] = mat_k(m); me[m] = mat_eps(m); }
         if ((s = put(dmatk, mk.data(), mk.size() * 8)) != PM_OK) return s;
         if ((s = put(dmateps, me.data(), me.size() * 8)) != PM_OK) return s;
+        if ((s = upload_places()) != PM_OK) return s;
+        // The gap table: per cell its entries in the pairs' order, which is the order the step adds
+        // them (solid.rs:1866-1878 walks the pairs; each touches two cells).
+        if (!gaps.empty()) {
+            std::vector<std::vector<std::pair<size_t, int>>> per(n());  // (pair, this cell is its first)
+            for (size_t q = 0; q < gaps.size(); ++q) {
+                per[gaps[q].a].push_back({q, 1});
+                per[gaps[q].b].push_back({q, 0});
+            }
+            std::vector<int> first(n(), -1);
+            std::vector<HeatGapEntry> table;
+            for (size_t c = 0; c < n(); ++c) {
+                if (per[c].empty()) continue;
+                first[c] = (int)table.size();
+                for (size_t e = 0; e < per[c].size(); ++e) {
+                    const Gap& g = gaps[per[c][e].first];
+                    const int lower = per[c][e].second;
+                    table.push_back(HeatGapEntry{(long long)(lower ? g.b : g.a), g.coefficient, lower,
+                                                 e + 1 == per[c].size() ? 1 : 0});
+                }
+            }
+            if ((s = put(dgap_of, first.data(), first.size() * 4)) != PM_OK) return s;
+            if ((s = put(dgaps, table.data(), table.size() * sizeof(HeatGapEntry))) != PM_OK) return s;
+        }
+        return PM_OK;
+    }
+
+    // The sources (zeroed on void, where the step skips them: solid.rs:1857) and the void flags.
+    pm_status upload_places() {
+        pm_status s;
+        if (!source.empty()) {
+            std::vector<double> w(source);
+            for (size_t c = 0; c < n(); ++c)
+                if (is_void(c)) w[c] = 0.0;
+            if ((s = put_buf(dsrc, w.data(), w.size() * 8)) != PM_OK) return s;
+        }
+        if (!vd.empty() && (s = put_buf(dvoid, vd.data(), vd.size())) != PM_OK) return s;
         return PM_OK;
     }
 
@@ -355,6 +446,8 @@ struct Heat : Handle {
             a.kx = dkx.as<double>(); a.ky = dky.as<double>(); a.kz = dkz.as<double>();
             a.mob = dmob.as<double>(); a.cap = dcap.as<double>();
             a.which = dwhich.as<uint32_t>(); a.mat_k = dmatk.as<double>(); a.mat_eps = dmateps.as<double>();
+            a.src = source.empty() ? nullptr : dsrc.as<double>();
+            if (!gaps.empty()) { a.gap_of = dgap_of.as<int>(); a.gaps = dgaps.as<HeatGapEntry>(); }
         }
         a.kface = kface; a.mobility = mobility; a.capacity = capacity;
         a.k_cell = mat_k(0); a.eps_cell = mat_eps(0);
@@ -362,7 +455,7 @@ struct Heat : Handle {
         a.dts = dt; a.dx = dx; a.reference = reference;
         a.films = films;
         a.pairs = uniform && nx % 2 == 0 && wide ? 1 : 0;
-        a.radiating = radiating() ? 1 : 0;
+        a.radiating = state_dependent() ? 1 : 0;
         a.static_rate = worst_rate;
         const unsigned w = wave_of(a.pairs ? kHeatPlainPair : kHeatPlain);
         const int tx = a.pairs ? nx / 2 : nx;  // the threads along a row
@@ -396,7 +489,9 @@ struct Heat : Handle {
             a.kx = dkx32.as<float>(); a.ky = dky32.as<float>(); a.kz = dkz32.as<float>();
             a.m = dm32.as<float>(); a.cap = dcap.as<double>();
             for (int f = 0; f < 6; ++f) a.film[f] = dfilm32.as<float>() + film_off[f];
+            a.src = source.empty() ? nullptr : dsrc.as<double>();
         }
+        a.dts = dt;
         a.quads = uniform && nx % 4 == 0 && wide ? 1 : 0;
         const unsigned w = wave_of(a.quads ? kHeatF32Quad : kHeatF32);
         const int tx = a.quads ? nx / 4 : nx;  // the threads along a row
@@ -411,7 +506,7 @@ struct Heat : Handle {
     // step: every step of a launch-bound block in one cooperative launch per kPersistChunk steps.
     bool persistent(long long nsteps) const {
         const int width = precision == PM_PLAIN_F64 ? 2 : 4;  // the pair and the quad forms
-        if (!uniform || !wide || nx % width != 0 || radiating() || nsteps < 2) return false;
+        if (!uniform || !wide || nx % width != 0 || state_dependent() || nsteps < 2) return false;
         if (n() > kPersistMaxCells) return false;
         int coop = 0;
         return cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop;
@@ -527,6 +622,69 @@ pm_status pm_heat_fill(pm_heat* hp, const pm_substance* sub, const uint8_t* mask
     return h->measure();
 }
 
+pm_status pm_heat_empty(pm_heat* hp, const uint8_t* mask, size_t n) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!mask || n != h->n()) return fail(PM_BAD_ARG, "empty: a mask of one byte per cell");
+    // solid.rs:986-1005: the cells the mask selects become nothing
+    if (h->vd.empty()) h->vd.assign(h->n(), 0);
+    for (size_t c = 0; c < n; ++c)
+        if (mask[c]) h->vd[c] = 1;
+    h->resolve();
+    pm_status s = h->upload_coefficients();
+    if (s != PM_OK) return s;
+    return h->measure();
+}
+
+pm_status pm_heat_dissipating(pm_heat* hp, double watts, const uint8_t* mask, size_t n) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!mask || n != h->n()) return fail(PM_BAD_ARG, "dissipating: a mask of one byte per cell");
+    // solid.rs:1045-1085: the watts spread evenly over the solid cells selected; none selected
+    // generates nothing and is not an error
+    size_t chosen = 0;
+    for (size_t c = 0; c < n; ++c)
+        if (!h->is_void(c) && mask[c]) ++chosen;
+    if (chosen == 0) return PM_OK;
+    const double each = watts / (double)chosen;
+    if (h->source.empty()) h->source.assign(h->n(), 0.0);
+    for (size_t c = 0; c < n; ++c)
+        if (!h->is_void(c) && mask[c]) h->source[c] = each;
+    h->resolve();
+    pm_status s = h->upload_coefficients();
+    if (s != PM_OK) return s;
+    return h->measure();
+}
+
+pm_status pm_heat_generated(pm_heat* hp, double* watts, double* joules) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (watts) {  // solid.rs:1118-1121: summed over the cells
+        double sum = -0.0;
+        for (double w : h->source) sum += w;
+        *watts = sum;
+    }
+    if (joules) {  // solid.rs:1123-1126: what the steps generated
+        pm_status s = h->read_state();
+        if (s != PM_OK) return s;
+        *joules = h->host_state->supplied;
+    }
+    return PM_OK;
+}
+
+pm_status pm_heat_gaps(pm_heat* hp, long long* a, long long* b, double* coefficient, size_t capacity, size_t* count) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!count) return fail(PM_BAD_ARG, "null count");
+    *count = h->gaps.size();
+    for (size_t q = 0; q < h->gaps.size() && q < capacity; ++q) {
+        if (a) a[q] = (long long)h->gaps[q].a;
+        if (b) b[q] = (long long)h->gaps[q].b;
+        if (coefficient) coefficient[q] = h->gaps[q].coefficient;
+    }
+    return PM_OK;
+}
+
 pm_status pm_heat_losing_from(pm_heat* hp, int face, double ambient, double convection, double area) {
     Heat* h = reinterpret_cast<Heat*>(hp);
     HEAT_GUARD(h);
@@ -578,9 +736,9 @@ pm_status pm_heat_max_stable_dt(pm_heat* hp, double* seconds) {
     HEAT_GUARD(h);
     if (!seconds) return fail(PM_BAD_ARG, "null output");
     double rate;
-    if (h->radiating()) {
+    if (h->state_dependent()) {
         if (h->precision != PM_PLAIN_F64)
-            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) are on the plain f64 form only");
+            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) and radiative gaps are on the plain f64 form only");
         pm_status s = h->read_state();  // the rate the last step (or the last change of state) left
         if (s != PM_OK) return s;
         rate = h->host_state->rate_now;
@@ -604,11 +762,11 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
     if (nsteps < 0) return fail(PM_BAD_ARG, "nsteps must be >= 0");
     if (nsteps == 0) return PM_OK;
     double rate;
-    if (h->radiating()) {
+    if (h->state_dependent()) {
         // the limit follows the state: the first step is checked here against the present
         // state's rate, every later one on the device against the rate its own state gives
         if (h->precision != PM_PLAIN_F64)
-            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) are on the plain f64 form only");
+            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) and radiative gaps are on the plain f64 form only");
         pm_status rs = h->read_state();
         if (rs != PM_OK) return rs;
         rate = h->host_state->rate_now;
@@ -672,7 +830,7 @@ pm_status pm_heat_absorb(pm_heat* hp, double joules) {
     const double rise = joules / h->cap_sum;  // solid.rs:1755
     PM_CUDA(launch_heat_rise(h->precision == PM_PLAIN_F64 ? h->field[h->parity].as<double>() : nullptr,
                              h->precision == PM_PLAIN_F64 ? nullptr : h->field[h->parity].as<float>(), rise, h->n(),
-                             h->stream()));
+                             h->vd.empty() ? nullptr : h->dvoid.as<uint8_t>(), h->stream()));
     // absorbed heat is bus traffic, not a change of the domain's own books: re-measure stored
     pm_status s = h->read_state();
     if (s != PM_OK) return s;

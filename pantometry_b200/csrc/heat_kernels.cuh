@@ -57,6 +57,16 @@ struct HeatFilms {
     double share[6];  // area / cells_on(face), computed on the host as the reference does
 };
 
+// One cell's side of a radiative gap: a pair of solid cells facing each other along a grid line
+// across a run of void (solid.rs:786-838), in the order the pairs were found, which is the order
+// the step applies them (solid.rs:1866-1878).
+struct HeatGapEntry {
+    long long partner;   // the cell across the void
+    double coefficient;  // σA/(1/ε₁ + 1/ε₂ − 1)
+    int lower;           // 1: this cell is the pair's first cell, the one the exchange is taken from
+    int last;            // 1: the cell's last entry
+};
+
 struct HeatPlainArgs {
     const double* __restrict__ told;
     double* __restrict__ tnew;
@@ -70,6 +80,11 @@ struct HeatPlainArgs {
     const uint32_t* __restrict__ which;  // per-cell material, for the film (general mode)
     const double* __restrict__ mat_k;    // per-material conductivity (+inf: `thermal: None`)
     const double* __restrict__ mat_eps;  // per-material emissivity
+    // Heat that has a place (null where nothing generates): watts per cell, zero on void
+    // (solid.rs:1045-1085); the gaps (null without any): per cell the first of its entries or −1
+    const double* __restrict__ src;
+    const int* __restrict__ gap_of;
+    const HeatGapEntry* __restrict__ gaps;
     // Uniform blocks: the single values every interior face and cell holds.
     double kface, mobility, capacity, k_cell, eps_cell;
     int uniform;
@@ -77,9 +92,10 @@ struct HeatPlainArgs {
     double dts, dx, reference;
     HeatFilms films;
     int pairs;  // uniform blocks with rows of an even number of cells: heat_plain_pair_step
-    // Radiating films (some exposed cell with emissivity > 0): the step limit depends on the
-    // state, so each step checks dt against the rate its own state gives (solid.rs:1718-1738) and
-    // gathers the rate of the state it leaves. static_rate: `worst_rate` of `resolve`.
+    // Radiating films (some exposed cell with emissivity > 0) or radiative gaps: the step limit
+    // depends on the state, so each step checks dt against the rate its own state gives
+    // (solid.rs:1718-1738) and gathers the rate of the state it leaves. static_rate: `worst_rate`
+    // of `resolve`.
     int radiating;
     double static_rate;
     Tiles tiles;
@@ -207,6 +223,35 @@ __device__ __forceinline__ void heat_rate_publish(const HeatPlainArgs& a, double
     __syncthreads();
 }
 
+// A gap cell's exchanges after the sweep and the source (solid.rs:1866-1878): each pair's watts
+// read off the old state, the cell's share added in the pairs' order. Where the limit follows the
+// state, the pairs' terms of `worst_rate_now` (solid.rs:1159-1171) at the cell's new temperature:
+// each side offers 4σA·T³/(...)/C of both cells at its own T, and since every operation there is
+// monotone in T the larger side's offers are the reference's value at the hotter of the two.
+__device__ __forceinline__ double heat_gap_cell(const HeatPlainArgs& a, int g, double here, double capc, double nt,
+                                                double& rate) {
+    for (int e = g;; ++e) {
+        const HeatGapEntry x = a.gaps[e];
+        const double other = a.told[x.partner];
+        const double ta = x.lower ? here : other, tb = x.lower ? other : here;
+        const double watts = x.coefficient * (powi4(ta) - powi4(tb));
+        if (watts != 0.0) {
+            const double joules = watts * a.dts;
+            nt += x.lower ? -joules / capc : joules / capc;
+        }
+        if (x.last) break;
+    }
+    if (a.radiating) {
+        for (int e = g;; ++e) {
+            const HeatGapEntry x = a.gaps[e];
+            const double cond = 4.0 * x.coefficient * powi3(nt);
+            rate = fmax(rate, fmax(cond / capc, cond / a.cap[x.partner]));
+            if (x.last) break;
+        }
+    }
+    return nt;
+}
+
 // Decode tile t of a tiling into the thread's column (i, j) and plane range [k0, k1).
 __device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i, int& j, int& k0, int& k1) {
     const int tx = (int)(t % T.ntx);
@@ -221,10 +266,13 @@ __device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i,
 
 // The books of a plain step, after its cells: the blocks' partials reduced in fixed order by the
 // last block to finish, then the ledger and the audit.
-__device__ __forceinline__ void heat_plain_books(const HeatPlainArgs& a, double (&acc)[2]) {
-    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+// acc: stored heat, heat shed, and (filled blocks) heat generated.
+template <int NV>
+__device__ __forceinline__ void heat_plain_books(const HeatPlainArgs& a, double (&acc)[NV]) {
+    if (finish_blocks<NV>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;
         st->lost += acc[1];
+        if constexpr (NV > 2) st->supplied += acc[2];
         double total = 0.0, scale = 0.0;
         ledger_add(total, scale, acc[0]);
         ledger_add(total, scale, st->lost);
@@ -250,8 +298,8 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
     if (a.st->violated || heat_refused(a)) return;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
-    double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
-    double rate = -1.0;          // radiating films: the largest boundary-cell rate of the new state
+    double acc[3] = {0.0, 0.0, 0.0};  // stored heat of the new state, heat shed and generated this step
+    double rate = -1.0;  // a state-dependent limit: the largest rate of the new state
     for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
         int i, j, k0, k1;
         tile_column(a.tiles, t, i, j, k0, k1);
@@ -284,7 +332,19 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
             const double shed = a.films.exposed ? film_flux(a, i, j, k, c, t0) : 0.0;
             const double mob = a.uniform ? a.mobility : a.mob[c];
             const double capc = a.uniform ? a.capacity : a.cap[c];
-            const double nt = t0 + a.dts * mob * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
+            double nt = t0 + a.dts * mob * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
+            if (a.src) {  // solid.rs:1854-1864, after the sweep
+                const double w = a.src[c];
+                if (w != 0.0) {
+                    const double joules = w * a.dts;
+                    nt += joules / capc;
+                    acc[2] += joules;
+                }
+            }
+            if (a.gap_of) {
+                const int g = a.gap_of[c];
+                if (g >= 0) nt = heat_gap_cell(a, g, t0, capc, nt, rate);
+            }
             a.tnew[c] = nt;
             acc[0] += capc * (nt - a.reference);                  // solid.rs:1583-1590
             if (shed != 0.0) acc[1] += a.dts * mob * shed * capc;  // solid.rs:1821-1823
@@ -378,7 +438,7 @@ __device__ __forceinline__ void heat_pair_tile(const HeatPlainArgs& a, long long
 static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_step(HeatPlainArgs a) {
     if (a.st->violated || heat_refused(a)) return;
     double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
-    double rate = -1.0;          // radiating films: the largest boundary-cell rate of the new state
+    double rate = -1.0;  // a state-dependent limit: the largest rate of the new state
     for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_pair_tile<false>(a, t, a.told, a.tnew, acc, rate);
     if (a.radiating) heat_rate_publish(a, rate);
     heat_plain_books(a, acc);
@@ -482,6 +542,8 @@ struct HeatF32Args {
     const float* __restrict__ m;
     const double* __restrict__ cap;
     const float* film[6];
+    double dts;                       // the step, for the sources
+    const double* __restrict__ src;   // filled blocks that generate: watts per cell, zero on void
     int quads;  // uniform blocks with rows of a multiple of 4: heat_f32_quad_step, tiles of quads
     Tiles tiles;
     DevState* st;
@@ -491,11 +553,14 @@ struct HeatF32Args {
 
 // The books of an FP32 step, after its cells: the block's partials reduced in fixed order by the
 // last block to finish, then the ledger and the audit.
-__device__ __forceinline__ void heat_f32_books(const HeatF32Args& a, double (&acc)[2], bool filled) {
-    if (finish_blocks<2>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
+// acc: stored heat, heat shed, and (filled blocks) heat generated.
+template <int NV>
+__device__ __forceinline__ void heat_f32_books(const HeatF32Args& a, double (&acc)[NV], bool filled) {
+    if (finish_blocks<NV>(acc, a.partials, a.nblocks, &a.st->counter) && linear_tid() == 0) {
         DevState* st = a.st;
         const double stored = filled ? acc[0] : a.capacity * acc[0];
         st->lost += filled ? acc[1] : a.capacity * acc[1];
+        if constexpr (NV > 2) st->supplied += acc[2];
         double total = 0.0, scale = 0.0;
         ledger_add(total, scale, stored);
         ledger_add(total, scale, st->lost);
@@ -513,7 +578,7 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
     if (a.st->violated) return;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
-    double acc[2] = {0.0, 0.0};
+    double acc[FILLED ? 3 : 2] = {};
     for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) {
         int i, j, k0, k1;
         tile_column(a.tiles, t, i, j, k0, k1);
@@ -572,6 +637,14 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
                 const float mc = __ldg(a.m + c);
                 nd = here + mc * (s - shed);
                 const double capc = __ldg(a.cap + c);
+                if (a.src) {  // solid.rs:1854-1864, after the sweep: the joules in FP64, the rise in f32
+                    const double w = __ldg(a.src + c);
+                    if (w != 0.0) {
+                        const double joules = w * a.dts;
+                        nd += (float)(joules / capc);
+                        acc[FILLED ? 2 : 0] += joules;
+                    }
+                }
                 acc[0] += capc * (double)nd;
                 if (shed != 0.0f) acc[1] += capc * (double)(mc * shed);
             } else {
@@ -788,14 +861,15 @@ static __global__ void heat_from_deviation(const float* __restrict__ d, double* 
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
         t[c] = t0 + (double)d[c];
 }
-// solid.rs:1752-1765 + 1620-1635: a uniform rise over every cell.
-static __global__ void heat_add_rise64(double* __restrict__ t, double rise, size_t n) {
+// solid.rs:1752-1765 + 1620-1635: a uniform rise over every cell but the void ones (`vd`, null
+// where there is none).
+static __global__ void heat_add_rise64(double* __restrict__ t, double rise, size_t n, const uint8_t* __restrict__ vd) {
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
-        t[c] += rise;
+        if (!vd || !vd[c]) t[c] += rise;
 }
-static __global__ void heat_add_rise32(float* __restrict__ d, float rise, size_t n) {
+static __global__ void heat_add_rise32(float* __restrict__ d, float rise, size_t n, const uint8_t* __restrict__ vd) {
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
-        d[c] += rise;
+        if (!vd || !vd[c]) d[c] += rise;
 }
 
 // ---------------------------------------------------------------------------------------------

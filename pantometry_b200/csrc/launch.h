@@ -86,7 +86,7 @@ cudaError_t launch_heat_f32_steps(const HeatF32Args& a, const HeatPersist& p, cu
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s);
 cudaError_t launch_heat_convert(const double* t, float* d, double t0, size_t n, int to_dev, double* tout,
                                 cudaStream_t s);
-cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, cudaStream_t s);
+cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, const uint8_t* vd, cudaStream_t s);
 
 template <typename Real> cudaError_t launch_hall(const HallArgs<Real>& a, cudaStream_t s);
 template <typename Real> cudaError_t launch_hall_measure(const HallMeasureArgs<Real>& a, cudaStream_t s);

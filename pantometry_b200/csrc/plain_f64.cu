@@ -34,11 +34,11 @@ cudaError_t launch_heat_convert(const double* t, float* d, double t0, size_t n, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, cudaStream_t s) {
+cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, const uint8_t* vd, cudaStream_t s) {
     if (t64)
-        heat_add_rise64<<<kMeasureBlocks, 256, 0, s>>>(t64, rise, n);
+        heat_add_rise64<<<kMeasureBlocks, 256, 0, s>>>(t64, rise, n, vd);
     else
-        heat_add_rise32<<<kMeasureBlocks, 256, 0, s>>>(d32, (float)rise, n);
+        heat_add_rise32<<<kMeasureBlocks, 256, 0, s>>>(d32, (float)rise, n, vd);
     return cudaGetLastError();
 }
 

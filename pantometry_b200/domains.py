@@ -138,6 +138,40 @@ class Solid3D(_Domain):
         N.check(self._lib.pm_heat_fill(self._h, C.byref(s), m.ctypes.data_as(C.c_void_p), m.size))
         return self
 
+    def empty(self, mask):
+        """`Solid3D::empty` (solid.rs:986-1005): the cells the mask selects become void."""
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        N.check(self._lib.pm_heat_empty(self._h, m.ctypes.data_as(C.c_void_p), m.size))
+        return self
+
+    def dissipating(self, watts, mask):
+        """`Solid3D::dissipating` (solid.rs:1045-1085): `watts` spread over the solid cells the mask
+        selects."""
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        N.check(self._lib.pm_heat_dissipating(self._h, float(watts), m.ctypes.data_as(C.c_void_p), m.size))
+        return self
+
+    def generated_power(self):
+        w = C.c_double()
+        N.check(self._lib.pm_heat_generated(self._h, C.byref(w), None))
+        return w.value
+
+    def generated_energy(self):
+        j = C.c_double()
+        N.check(self._lib.pm_heat_generated(self._h, None, C.byref(j)))
+        return j.value
+
+    def gaps(self):
+        """The gap pairs (a, b, coefficient) in the order the step applies them."""
+        count = C.c_size_t()
+        N.check(self._lib.pm_heat_gaps(self._h, None, None, None, 0, C.byref(count)))
+        a = np.zeros(count.value, dtype=np.int64)
+        b = np.zeros(count.value, dtype=np.int64)
+        g = np.zeros(count.value)
+        N.check(self._lib.pm_heat_gaps(self._h, a.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p),
+                                       g.ctypes.data_as(C.c_void_p), count.value, C.byref(count)))
+        return a, b, g
+
     @property
     def cells(self):
         out = np.empty(self.n, dtype=np.float64)
