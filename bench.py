@@ -258,6 +258,7 @@ def run_ours(args):
     }
     if not args.no_side_records:
         line["cavity"] = cavity_record(local, stream, peak)
+        line["ensemble"] = ensemble_record(local, stream, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, sample_steps=args.cpu_sample_steps, threads=1)
     if rank == 0:
@@ -657,6 +658,74 @@ def cpu_baseline_heat(cfg, sample_steps):
 
 
 CAV_METRIC = "Gcell-updates/s (Yee cavity 384^3, FP32 fields + FP64 audit)"
+
+
+def ensemble_record(local, stream, peak, timesteps=2000, steps=2):
+    """The heat ensemble (512 uneven blocks of 16..128 cells per axis, Dirichlet 300 K films, dt at
+    0.9 of each block's own limit, FP64 books and audit per block every timestep) as an object of the
+    default line: the FP32 form (brick shape autotuned) over `steps` runs of `timesteps` timesteps and
+    the plain f64 form over one, device-resident, CUDA events on the ensemble's stream; the FP32
+    fields and books against the f64 run's after one run from the same start."""
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import workloads as W
+    from pantometry_b200.domains import Ensemble
+
+    cfg = W.heat_ensemble(count=512, steps=timesteps)
+    grids = W.ensemble_grids(cfg)
+    cells = np.concatenate([W.ensemble_cells(g) for g in cfg["grids"]])
+    total = int(cells.size)
+
+    def run(precision, k, tol, tune):
+        e = Ensemble(grids, precision=precision, device=local)
+        e.set_stream(stream.cuda_stream)
+        e.upload(cells)
+        shape = e.autotune(trial_steps=tune)
+        e.upload(cells)
+        e.set_tolerance(tol)
+        assert e.step(64) is None  # warm-up: graphs captured
+        e.upload(cells)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for q in range(k):
+            v = e.step(timesteps)
+            assert v is None, v
+        end.record(stream)
+        torch.cuda.synchronize()
+        return e, start.elapsed_time(end), shape
+
+    e32, ms32, shape32 = run("f32", steps, 1e-6, 10)
+    e64, ms64, shape64 = run("f64", 1, 1e-9, 5)
+    # both hold one run from the same start after their first timed run; the FP32 one has run more
+    e32.upload(cells)
+    assert e32.step(timesteps) is None
+    d32, d64 = e32.download(), e64.download()
+    l32, l64 = e32.ledgers(), e64.ledgers()
+    ledger_err = max(abs(a["total"] - b["total"]) / max(abs(b["total"]), b["scale"], 1e-300) for a, b in zip(l32, l64))
+    field_err = float(np.abs(d32 - d64).max())
+    del e32, e64
+    value = total * timesteps * steps / (ms32 * 1e-3) / 1e9
+    plain = total * timesteps / (ms64 * 1e-3) / 1e9
+    achieved = 8 * total / (ms32 / (steps * timesteps) * 1e-3) / 1e9
+    tma = tuple(shape32[:2]) == (32, 8)
+    return {
+        "workload": f"heat ensemble: 512 grids, 16..128 cells per axis, {total} cells, {timesteps} timesteps per run, "
+                    "Dirichlet 300 K faces, dt 0.9 x each grid's limit, FP64 audit per grid every timestep",
+        "value": round(value, 3), "unit": UNIT, "timed_runs": steps, "ms_per_run": round(ms32 / steps, 3),
+        "brick_f32": list(shape32), "brick_f64": list(shape64),
+        "plain_f64": {"value": round(plain, 3), "ms_per_run": round(ms64, 3),
+                      "roofline_frac": round(16 * total / (ms64 / timesteps * 1e-3) / 1e9 / peak, 4)},
+        "fp32_over_f64": round(value / plain, 3),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4),
+                     "kernel": "ens_tma_step (FP32, TMA-staged)" if tma else "ens_step<float>",
+                     "bytes_per_timestep": 8 * total,
+                     "traffic": round(ENS_F32_TRAFFIC_PER_CELL * total) if tma else None,
+                     "traffic_source": "ncu capture of the 512-grid ensemble, per cell"},
+        "error_vs_f64": {"max_abs_kelvin": field_err, "ledger_rel_max_over_grids": ledger_err, "after_timesteps": timesteps},
+    }
 
 
 def cavity_record(local, stream, peak, n=384, timed_steps=2000, compare_steps=10000, every=10):

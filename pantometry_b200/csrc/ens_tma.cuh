@@ -222,6 +222,41 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
                         below = here;
                         here = above;
                     }
+                } else if (yl && yh && hn == P && kb > 0 && kb + P < nz) {
+                    // a whole stage of a brick on an x face, inside in y and z: the general form's
+                    // sums and x films term for term, the x faces' terms taken by select, so the
+                    // stage stays one straight run of planes
+                    const int exposed = m.exposed;
+                    const bool fx0 = ((exposed >> 0) & 1) && !xl, fx1 = ((exposed >> 1) & 1) && !xh;
+                    const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
+                    double col_shed = 0.0;
+                    float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
+#pragma unroll
+                    for (int h = 0; h < P; ++h) {
+                        const float above = s.t[h + 2][ty + 1][tx + 4];
+                        const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+                        const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
+                        float sum = 0.0f;
+                        sum += xl ? xm - here : 0.0f;
+                        sum += xh ? xp - here : 0.0f;
+                        sum += ym - here;
+                        sum += yp - here;
+                        sum += below - here;
+                        sum += above - here;
+                        float shed = 0.0f;
+                        const float v0 = __fmaf_rn(b0, here + o0, shed);
+                        shed = fx0 ? v0 : shed;
+                        const float v1 = __fmaf_rn(b1, here + o1, shed);
+                        shed = fx1 ? v1 : shed;
+                        if (exposed) col_shed += (double)shed;
+                        const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
+                        *out = nd;
+                        out += plane;
+                        acc[0] += (double)nd;
+                        below = here;
+                        here = above;
+                    }
+                    acc[1] += col_shed;
                 } else {
                     // The general form, taken by the whole warp: its row (y) and each plane (z) are
                     // the same for every lane, so those tests are uniform, and a lane on an x face

@@ -107,10 +107,12 @@ struct Hall : Handle {
     }
 
     // Time `trial` steps of every TMA tile shape on the present state and keep the fastest. Each
-    // trial step reads the present parity and writes the other one, which is free between steps,
-    // so the fields are never touched; the books (the source's clock among them) are put back after
-    // each trial. A grid shape (nx, ny, nz, with or without speed blocks) timed once on a device is
-    // not timed again in the process.
+    // trial step reads the present parity and writes the other one. The other parity's velocities
+    // are free between steps; its pressure is the previous pressure the invariant reads (hall.rs
+    // keeps `p_prev`), so it is copied aside first (on the device where there is room, else on the
+    // host) and put back after the trials, as are the books (the source's clock among them). A grid
+    // shape (nx, ny, nz, with or without speed blocks) timed once on a device is not timed again in
+    // the process.
     pm_status autotune(int trial) {
         if (!tma) return PM_OK;
         static std::mutex cache_mutex;
@@ -124,6 +126,17 @@ struct Hall : Handle {
         pm_status s = read_state();
         if (s != PM_OK) return s;
         const DevState books = *host_state;
+        const size_t pbytes = nodes() * esize();
+        DBuf aside;
+        std::vector<unsigned char> aside_host;
+        if (aside.alloc(pbytes) == cudaSuccess) {
+            PM_CUDA(cudaMemcpyAsync(aside.p, p[parity ^ 1].p, pbytes, cudaMemcpyDeviceToDevice, stream()));
+        } else {
+            cudaGetLastError();  // the refused allocation is not an error of the stream
+            aside_host.resize(pbytes);
+            PM_CUDA(cudaMemcpyAsync(aside_host.data(), p[parity ^ 1].p, pbytes, cudaMemcpyDeviceToHost, stream()));
+            PM_CUDA(cudaStreamSynchronize(stream()));
+        }
         const double c = block > 0 ? max_speed : speed;
         const double dt = 0.5 * dx / (c * std::sqrt(3.0));
         if ((s = upload_block_scale(dt)) != PM_OK) return s;
@@ -151,6 +164,9 @@ struct Hall : Handle {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (s != PM_OK) return s;
+        PM_CUDA(cudaMemcpyAsync(p[parity ^ 1].p, aside.p ? aside.p : (void*)aside_host.data(), pbytes,
+                                aside.p ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream()));
+        PM_CUDA(cudaStreamSynchronize(stream()));
         {
             std::lock_guard<std::mutex> lock(cache_mutex);
             cache[key] = best;
