@@ -159,8 +159,9 @@ pm_status pm_heat_set_cells_per_thread(pm_heat* h, int cells);
 /* Run subsequent work on `stream` (a cudaStream_t); NULL restores the handle's own stream. */
 /* No counterpart in the reference. Small uniform blocks (up to 2^22 cells, rows of an even number of
  * cells in plain f64 or a multiple of 4 in FP32, films that do not radiate) take many steps of one
- * call in one cooperative launch, one grid-wide wait per step. Each wait is bounded: `polls` checks about 100 ns apart (default
- * 2^24, over a second); a wait that runs out stops the call with PM_DEVICE_TIMEOUT and leaves the
+ * call in one cooperative launch, one grid-wide wait per step. Each wait is bounded: `polls` looks at the
+ * arrivals, each a few hundred ns apart (default 2^24, over a second); a wait that runs out stops the
+ * call with PM_DEVICE_TIMEOUT and leaves the
  * fields of the step in progress incomplete. 0 makes every wait that is not already over give up at
  * once, which exercises that path without a fault. */
 pm_status pm_heat_set_wait_budget(pm_heat* h, unsigned polls);

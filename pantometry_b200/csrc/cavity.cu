@@ -479,12 +479,11 @@ struct Cavity : Handle {
             YeeStepArgs<float> t = targs(par, h);
             if (after) t.solid = nullptr;
             if (near_on()) {
-                // the box's terms and the source are the box kernel's; it closes the books
+                // the box's terms and the source are the step's last block's; it closes the books
                 const YeeNearArgs n = nargs(par, h, t);
                 t.nb_x0 = near_x0; t.nb_y0 = near_y0; t.nb_z0 = near_z0; t.nb_w = near_w;
                 t.src_i = t.src_j = t.src_k = -1;
-                e = launch_yee_tma(t, L, maps[par], yshape, s);
-                if (e == cudaSuccess) e = launch_yee_near(n, any_solid && !after, s);
+                e = launch_yee_tma(t, L, maps[par], yshape, s, n);
             } else {
                 e = launch_yee_tma(t, L, maps[par], yshape, s);
             }

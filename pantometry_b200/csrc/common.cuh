@@ -23,13 +23,15 @@ struct Tiles {
     int nx, ny, nz, zc;
     int ntx, nty, ntz;
     long long ntiles;
+    int rows;  // rows of a tile: the block's y extent (8 but in the many-step heat kernels)
 };
 
-__host__ __device__ inline Tiles make_tiles(int nx, int ny, int nz, int zc) {
+__host__ __device__ inline Tiles make_tiles(int nx, int ny, int nz, int zc, int rows = 8) {
     Tiles t;
     t.nx = nx; t.ny = ny; t.nz = nz; t.zc = zc;
+    t.rows = rows;
     t.ntx = (nx + 31) / 32;
-    t.nty = (ny + 7) / 8;
+    t.nty = (ny + rows - 1) / rows;
     t.ntz = (nz + zc - 1) / zc;
     t.ntiles = (long long)t.ntx * t.nty * t.ntz;
     return t;
@@ -82,9 +84,6 @@ struct DevState {
     // Cavity books (cavity.rs:161-162) and the source extension
     double invariant, dissipated, work;
     double work_booked;  // cavity source work already in the ledger: through the previous step
-    // an FP32 cavity whose source's near field is kept in f64: the step kernel's four sums over
-    // every node outside that box, handed to the kernel that steps the box and closes the books
-    double near_acc[4];
     // Solid3D with radiating films: `worst_rate_now` of the present state (solid.rs:1148-1185),
     // and the max over boundary cells the step kernel gathers for the next state (the bits of a
     // non-negative double, so an integer atomicMax orders them)
@@ -191,23 +190,37 @@ __device__ __forceinline__ void audit_and_commit(DevState* st, double total, dou
     st->scale = scale;
 }
 
-// A barrier across every block of a cooperative launch (all co-resident), bounded. `count` is zero
-// at the launch's start (the host clears it) and barrier b of the launch completes when it reaches
-// (b + 1)·gridDim.x. Each block's thread 0 arrives once; the others wait at __syncthreads. The
-// wait polls at most `budget` times, about 100 ns apart, after a first look; a wait that runs out
-// returns false in every thread of the block, and the caller stops with kDeviceTimeout.
-__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target, unsigned budget) {
+// The many-step kernels' grid-wide wait: arrival counters 128 bytes apart (so the blocks' arrivals do
+// not queue on one address), then a word of their own for the books' verdict.
+constexpr int kWaitCounters = 8;
+constexpr int kWaitWords = 32 * kWaitCounters + 32;
+
+// Arrive at the grid's n-th wait and wait until every block has arrived n times, polling at most
+// `budget` times after the first look (false: the wait ran out). The arrival is a release, so what
+// the block wrote before it is seen by every block after its own wait, which ends with an acquire.
+__device__ __forceinline__ bool grid_wait(unsigned* base, unsigned n, unsigned budget) {
     __shared__ int passed;
     __syncthreads();
     if (linear_tid() == 0) {
-        __threadfence();  // this block's writes before its arrival
-        atomicAdd(count, 1u);
-        bool ok = *(volatile unsigned*)count >= target;
-        for (unsigned it = 0; !ok && it < budget; ++it) {
-            __nanosleep(100);
-            ok = *(volatile unsigned*)count >= target;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(base + 32 * (blockIdx.x % kWaitCounters)) : "memory");
+        const unsigned target = n * gridDim.x;
+        bool ok = false;
+        for (unsigned it = 0;; ++it) {
+            unsigned v[kWaitCounters];
+#pragma unroll
+            for (int r = 0; r < kWaitCounters; ++r)
+                asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v[r]) : "l"(base + 32 * r) : "memory");
+            unsigned sum = 0;
+#pragma unroll
+            for (int r = 0; r < kWaitCounters; ++r) sum += v[r];
+            if (sum >= target) {
+                ok = true;
+                break;
+            }
+            if (it >= budget) break;
+            __nanosleep(32);
         }
-        __threadfence();  // the other blocks' writes after the wait
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         passed = ok ? 1 : 0;
     }
     __syncthreads();

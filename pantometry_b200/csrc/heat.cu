@@ -454,6 +454,15 @@ struct Heat : Handle {
         a.nx = nx; a.ny = ny; a.nz = nz;
         a.dts = dt; a.dx = dx; a.reference = reference;
         a.films = films;
+        a.films.dirichlet = 0;
+        if (uniform) {  // solid.rs:1192-1219 at h = +inf: the film's series with the half cell, per face
+            for (int f = 0; f < 6; ++f) {
+                if (!((films.exposed >> f) & 1) || !(films.convection[f] == std::numeric_limits<double>::infinity())) continue;
+                a.films.dirichlet |= 1 << f;
+                a.films.g_inf[f] = host_series_with_half_cell(std::numeric_limits<double>::infinity(), mat_k(0),
+                                                              films.share[f], dx);
+            }
+        }
         a.pairs = uniform && nx % 2 == 0 && wide ? 1 : 0;
         a.radiating = state_dependent() ? 1 : 0;
         a.static_rate = worst_rate;
@@ -512,28 +521,35 @@ struct Heat : Handle {
         return cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop;
     }
     pm_status run_persistent(long long nsteps, double dt) {
-        if (!dbarrier.p) PM_CUDA(dbarrier.alloc(sizeof(unsigned)));
+        const size_t wait_bytes = kWaitWords * sizeof(unsigned);
+        if (!dbarrier.p) PM_CUDA(dbarrier.alloc(wait_bytes));
         const bool plain = precision == PM_PLAIN_F64;
-        // a grid of co-resident blocks, tiles made as small as that grid takes
-        const unsigned wave = wave_of(plain ? kHeatPlainSteps : kHeatF32QuadSteps);
+        // Blocks of 1024 threads (tiles of 32 rows) where the block has the rows for them, so that
+        // fewer blocks meet at each step's wait; a grid of co-resident blocks, one of them keeping the
+        // books, and tiles made as small as the others take.
+        const int rows = ny >= 32 ? 32 : 8;
+        const unsigned wave = wave_of(plain ? (rows == 32 ? kHeatPlainSteps32 : kHeatPlainSteps)
+                                            : (rows == 32 ? kHeatF32QuadSteps32 : kHeatF32QuadSteps));
+        if (wave < 2) return fail(PM_UNSUPPORTED, "the many-step heat kernel needs two co-resident blocks");
         const int tx = nx / (plain ? 2 : 4);
         int zc = 1;
-        while (zc < nz && make_tiles(tx, ny, nz, zc).ntiles > (long long)wave) zc *= 2;
-        const Tiles tiles = make_tiles(tx, ny, nz, zc);
+        while (zc < nz && make_tiles(tx, ny, nz, zc, rows).ntiles > (long long)(wave - 1)) zc *= 2;
+        const Tiles tiles = make_tiles(tx, ny, nz, zc, rows);
+        const unsigned nblocks = 1u + (unsigned)std::min<long long>(tiles.ntiles, (long long)(wave - 1));
         int par = parity;
         for (long long done = 0; done < nsteps;) {
             const int chunk = (int)std::min<long long>(kPersistChunk, nsteps - done);
-            PM_CUDA(cudaMemsetAsync(dbarrier.p, 0, sizeof(unsigned), stream()));
+            PM_CUDA(cudaMemsetAsync(dbarrier.p, 0, wait_bytes, stream()));
             const HeatPersist p{dbarrier.as<unsigned>(), chunk, wait_budget};
             if (plain) {
                 HeatPlainArgs a = plain_args(par, dt);
                 a.tiles = tiles;
-                a.nblocks = grid_for(tiles, wave);
+                a.nblocks = nblocks;
                 PM_CUDA(launch_heat_plain_steps(a, p, stream()));
             } else {
                 HeatF32Args a = f32_args(par, dt);
                 a.tiles = tiles;
-                a.nblocks = grid_for(tiles, wave);
+                a.nblocks = nblocks;
                 PM_CUDA(launch_heat_f32_steps(a, p, stream()));
             }
             par ^= chunk & 1;

@@ -55,6 +55,10 @@ struct HeatFilms {
     double ambient[6];
     double convection[6];
     double share[6];  // area / cells_on(face), computed on the host as the reference does
+    // Faces with h = +inf on a block of one material: bit f set, and g_inf[f] the film's series
+    // with the half cell there, which is the same for every cell of the face (see film_flux).
+    int dirichlet;
+    double g_inf[6];
 };
 
 // One cell's side of a radiative gap: a pair of solid cells facing each other along a grid line
@@ -125,11 +129,19 @@ __device__ __forceinline__ double film_flux(const HeatPlainArgs& a, int i, int j
         double ambient = a.films.ambient[f];
         double gap = here - ambient;
         if (gap == 0.0) continue;
-        // crates/pantometry-thermal/src/lib.rs:104-110 `Environment::loss_from`, area = share
-        double convective = a.films.convection[f] * share * (here - ambient);
-        double radiative = emissivity * kStefanBoltzmann * share * (powi4(here) - powi4(ambient));
-        double bare = convective + radiative;
-        double g = series_with_half_cell(bare / gap, conductivity, share, a.dx);
+        double g;
+        if ((a.films.dirichlet >> f) & 1) {
+            // h = +inf: the convective term is ±inf with the gap's sign and the radiative one finite,
+            // so bare / gap is +inf for every finite nonzero gap, and series_with_half_cell(+inf, k,
+            // share, dx) is the face's constant, formed once on the host by the same expression
+            g = a.films.g_inf[f];
+        } else {
+            // crates/pantometry-thermal/src/lib.rs:104-110 `Environment::loss_from`, area = share
+            double convective = a.films.convection[f] * share * (here - ambient);
+            double radiative = emissivity * kStefanBoltzmann * share * (powi4(here) - powi4(ambient));
+            double bare = convective + radiative;
+            g = series_with_half_cell(bare / gap, conductivity, share, a.dx);
+        }
         out += g * gap / a.dx;
     }
     return out;
@@ -259,7 +271,7 @@ __device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i,
     const int ty = (int)(r % T.nty);
     const int tz = (int)(r / T.nty);
     i = tx * 32 + threadIdx.x;
-    j = ty * 8 + threadIdx.y;
+    j = ty * T.rows + threadIdx.y;
     k0 = tz * T.zc;
     k1 = min(T.nz, k0 + T.zc);
 }
@@ -444,84 +456,108 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plai
     heat_plain_books(a, acc);
 }
 
-// Many steps of a small block in one cooperative launch (every block co-resident), for blocks whose
-// step is far shorter than a kernel launch (a 64³ block in plain f64 holds 2 MiB and sweeps from L2
-// in about a microsecond). Each step: the pair form's tiles, this block's two partials, one bounded
-// grid barrier, then every block sums all blocks' partials in the same fixed order and runs the
-// ledger and the audit on its own copy of the books (audit_and_commit, the one-step kernels'
-// arithmetic), so every block reaches the same verdict without a second barrier. The partials are
-// double-buffered by step parity: a block writes a step's partials only after the barrier that
-// every block passes after reading the ones two steps back. Block 0 writes the books back at the
-// end. Films must not radiate (the limit is the host's, checked once for the call).
 struct HeatPersist {
-    unsigned* barrier;  // arrivals, zero at launch
+    unsigned* barrier;  // kWaitWords words, zero at launch: the grid wait's counters, then the verdict
     int nsteps;
-    unsigned budget;    // polls per barrier wait before giving up
+    unsigned budget;    // polls per grid wait before giving up
 };
 
-static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plain_pair_steps(HeatPlainArgs a, HeatPersist p) {
+// The many-step kernels of small uniform blocks: every step of a call in one cooperative launch.
+// Block 0 keeps the books and takes no cells; blocks 1.. take the tiles. In step s the workers step
+// their tiles and store their partials (two sets, by the step's parity) while block 0 sums step
+// s−1's in a fixed order, audits them and, if the audit failed, sets the verdict word; then every
+// block arrives at the grid's s-th wait and, once through it, reads the verdict. A failed audit of
+// step s−1 ends the call with step s−1's state, which is intact: step s wrote the other buffer. After
+// the last wait block 0 audits the last step and writes the books back. So the books' arithmetic
+// never sits between the steps, and only block 0 reads the partials.
+template <typename Args, typename StepTiles>
+__device__ __forceinline__ void heat_persist(const Args& a, const HeatPersist& p, double cap_scale,
+                                             StepTiles step_tiles) {
     __shared__ DevState books;
     __shared__ double red[32 * 2];
     __shared__ int stop;
     const int tid = linear_tid();
+    const int nthreads = blockDim.x * blockDim.y;
+    const bool keeper = blockIdx.x == 0;
+    const unsigned workers = gridDim.x - 1;
+    unsigned* verdict = p.barrier + 32 * kWaitCounters;
     if (tid == 0) {
-        books = *a.st;
-        stop = books.violated;
+        stop = a.st->violated;
+        if (keeper) books = *a.st;
     }
     __syncthreads();
     if (stop) return;
-    const double* told = a.told;
-    double* tnew = a.tnew;
-    bool timed_out = false;
-    for (int s = 0; s < p.nsteps; ++s) {
-        double acc[2] = {0.0, 0.0};
-        double rate = -1.0;
-        for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_pair_tile<true>(a, t, told, tnew, acc, rate);
-        block_sum<2>(acc, red);
-        double* part = a.partials + (size_t)(s & 1) * 2 * gridDim.x;
-        if (tid == 0) {
-            part[2 * (size_t)blockIdx.x] = acc[0];
-            part[2 * (size_t)blockIdx.x + 1] = acc[1];
-        }
-        if (!grid_barrier(p.barrier, (unsigned)(s + 1) * gridDim.x, p.budget)) {
-            timed_out = true;
-            break;
-        }
+    auto audit = [&](int s) {  // block 0: step s's partials into the books
+        const double* part = a.partials + (size_t)(s & 1) * 2 * workers;
         double v[2] = {0.0, 0.0};
-        for (unsigned b = tid; b < gridDim.x; b += blockDim.x * blockDim.y) {
+        for (unsigned b = tid; b < workers; b += nthreads) {
             v[0] += __ldcg(&part[2 * (size_t)b]);
             v[1] += __ldcg(&part[2 * (size_t)b + 1]);
         }
         block_sum<2>(v, red);
         if (tid == 0) {
-            books.lost += v[1];
+            const double stored = cap_scale * v[0];
+            books.lost += cap_scale * v[1];
             double total = 0.0, scale = 0.0;
-            ledger_add(total, scale, v[0]);
+            ledger_add(total, scale, stored);
             ledger_add(total, scale, books.lost);
             ledger_add(total, scale, -books.supplied);
-            books.part[0] = v[0];
+            books.part[0] = stored;
             books.part[1] = books.lost;
             books.part[2] = -books.supplied;
             audit_and_commit(&books, total, scale);
-            stop = books.violated;
+            if (books.violated) *(volatile unsigned*)verdict = 1u;
         }
+    };
+    bool timed_out = false;
+    int s = 0;
+    for (; s < p.nsteps; ++s) {
+        if (!keeper) {
+            double acc[2] = {0.0, 0.0};
+            step_tiles(s, (long long)blockIdx.x - 1, (long long)workers, acc);
+            block_sum<2>(acc, red);
+            if (tid == 0) {
+                double* part = a.partials + (size_t)(s & 1) * 2 * workers;
+                part[2 * (size_t)(blockIdx.x - 1)] = acc[0];
+                part[2 * (size_t)(blockIdx.x - 1) + 1] = acc[1];
+            }
+        } else if (s > 0) {
+            audit(s - 1);
+        }
+        if (!grid_wait(p.barrier, (unsigned)(s + 1), p.budget)) {
+            timed_out = true;
+            break;
+        }
+        if (tid == 0) stop = (int)*(volatile unsigned*)verdict;
         __syncthreads();
         if (stop) break;
-        const double* next = tnew;
-        tnew = const_cast<double*>(told);
-        told = next;
     }
     if (timed_out) {
         if (tid == 0) atomicExch(&a.st->violated, kDeviceTimeout);
         return;
     }
-    if (blockIdx.x == 0 && tid == 0) {
+    if (!keeper) return;
+    if (!stop) audit(p.nsteps - 1);
+    if (tid == 0) {
         DevState* st = a.st;
         const int seen = atomicAdd(&st->violated, 0);  // a block that gave up has already said so
         books.counter = 0u;
         *st = books;
         if (seen == kDeviceTimeout) st->violated = kDeviceTimeout;
     }
+}
+
+// The pair form's many-step kernel: blocks of 32 × ROWS threads (8 rows: four blocks per SM; 32 rows:
+// one block of 1024 per SM, so a 64³ block is 128 workers and the keeper).
+template <int ROWS>
+static __global__ void __launch_bounds__(32 * ROWS, ROWS == 8 ? PM_HEAT_PAIR_MIN_BLOCKS : 1)
+    heat_plain_pair_steps(HeatPlainArgs a, HeatPersist p) {
+    heat_persist(a, p, 1.0, [&](int s, long long first, long long stride, double (&acc)[2]) {
+        const double* told = (s & 1) ? a.tnew : a.told;
+        double* tnew = const_cast<double*>((s & 1) ? a.told : a.tnew);
+        double rate = -1.0;
+        for (long long t = first; t < a.tiles.ntiles; t += stride) heat_pair_tile<true>(a, t, told, tnew, acc, rate);
+    });
 }
 
 struct HeatF32Args {
@@ -745,71 +781,14 @@ static __global__ void __launch_bounds__(256) heat_f32_quad_step(HeatF32Args a) 
     heat_f32_books(a, acc, false);
 }
 
-// The quad form's many-step kernel, as heat_plain_pair_steps (one bounded grid barrier per step,
-// every block auditing its own copy of the books, block 0 writing them back).
-static __global__ void __launch_bounds__(256) heat_f32_quad_steps(HeatF32Args a, HeatPersist p) {
-    __shared__ DevState books;
-    __shared__ double red[32 * 2];
-    __shared__ int stop;
-    const int tid = linear_tid();
-    if (tid == 0) {
-        books = *a.st;
-        stop = books.violated;
-    }
-    __syncthreads();
-    if (stop) return;
-    const float* dold = a.dold;
-    float* dnew = a.dnew;
-    bool timed_out = false;
-    for (int s = 0; s < p.nsteps; ++s) {
-        double acc[2] = {0.0, 0.0};
-        for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_quad_tile<true>(a, t, dold, dnew, acc);
-        block_sum<2>(acc, red);
-        double* part = a.partials + (size_t)(s & 1) * 2 * gridDim.x;
-        if (tid == 0) {
-            part[2 * (size_t)blockIdx.x] = acc[0];
-            part[2 * (size_t)blockIdx.x + 1] = acc[1];
-        }
-        if (!grid_barrier(p.barrier, (unsigned)(s + 1) * gridDim.x, p.budget)) {
-            timed_out = true;
-            break;
-        }
-        double v[2] = {0.0, 0.0};
-        for (unsigned b = tid; b < gridDim.x; b += blockDim.x * blockDim.y) {
-            v[0] += __ldcg(&part[2 * (size_t)b]);
-            v[1] += __ldcg(&part[2 * (size_t)b + 1]);
-        }
-        block_sum<2>(v, red);
-        if (tid == 0) {
-            const double stored = a.capacity * v[0];
-            books.lost += a.capacity * v[1];
-            double total = 0.0, scale = 0.0;
-            ledger_add(total, scale, stored);
-            ledger_add(total, scale, books.lost);
-            ledger_add(total, scale, -books.supplied);
-            books.part[0] = stored;
-            books.part[1] = books.lost;
-            books.part[2] = -books.supplied;
-            audit_and_commit(&books, total, scale);
-            stop = books.violated;
-        }
-        __syncthreads();
-        if (stop) break;
-        const float* next = dnew;
-        dnew = const_cast<float*>(dold);
-        dold = next;
-    }
-    if (timed_out) {
-        if (tid == 0) atomicExch(&a.st->violated, kDeviceTimeout);
-        return;
-    }
-    if (blockIdx.x == 0 && tid == 0) {
-        DevState* st = a.st;
-        const int seen = atomicAdd(&st->violated, 0);  // a block that gave up has already said so
-        books.counter = 0u;
-        *st = books;
-        if (seen == kDeviceTimeout) st->violated = kDeviceTimeout;
-    }
+// The quad form's many-step kernel, as heat_plain_pair_steps.
+template <int ROWS>
+static __global__ void __launch_bounds__(32 * ROWS, ROWS == 8 ? 3 : 1) heat_f32_quad_steps(HeatF32Args a, HeatPersist p) {
+    heat_persist(a, p, a.capacity, [&](int s, long long first, long long stride, double (&acc)[2]) {
+        const float* dold = (s & 1) ? a.dnew : a.dold;
+        float* dnew = const_cast<float*>((s & 1) ? a.dold : a.dnew);
+        for (long long t = first; t < a.tiles.ntiles; t += stride) heat_quad_tile<true>(a, t, dold, dnew, acc);
+    });
 }
 
 // The opening ledger of a freshly uploaded block: stored heat only (lost and supplied are zero

@@ -64,7 +64,7 @@ inline cudaError_t launch_smem(void (*kernel)(P...), dim3 grid, dim3 block, int 
 // Multiprocessor, asked once per kernel and device), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps,
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps, kHeatPlainSteps32, kHeatF32QuadSteps32,
     kHallTmaShape1, kHallTmaShape2, kHallTmaShape3,  // kHallTma is shape 0
     kYeeTmaShape1, kYeeTmaShape2, kYeeTmaMediaShape1,  // kYeeTma and kYeeTmaMedia are shape 0 of each form
     kKernelCount
@@ -121,7 +121,9 @@ inline KernelId hall_tma_kernel_id(int shape) {
 bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned bx, unsigned by, unsigned bz);
 // The FP32 uniform-medium cavity step staged by TMA (padded lattice of row pitch L).
 // `shape` indexes the form's list (kYeeTmaUniformShapes, or kYeeTmaMediaShapes when !a.uniform).
-cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s);
+// `n`: the near-field box the last block steps (n.w = 0 with none; then it is not read).
+cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s,
+                           const YeeNearArgs& n = YeeNearArgs{});
 inline size_t yee_tma_smem_bytes(bool media = false, int shape = 0) {
     const YeeTmaShape sh = yee_tma_shape(media, shape);
     if (media) return sh.planes == 4 ? yee_tma_smem_bytes_for<4, true>(sh.stages) : yee_tma_smem_bytes_for<3, true>(sh.stages);
@@ -133,7 +135,6 @@ inline KernelId yee_tma_kernel_id(bool media, int shape) {
 }
 // The FP32 cavity's near-field box in f64 after the TMA step (yee_near.cuh), and its seeding from
 // the stored field.
-cudaError_t launch_yee_near(const YeeNearArgs& a, bool solid, cudaStream_t s);
 cudaError_t launch_yee_near_seed(const YeeNearArgs& a, cudaStream_t s);
 // One component between the reference layout and the padded lattice (see yee_relayout);
 // src_f64 / dst_f64 select double or float for each side.

@@ -16,7 +16,11 @@ cudaError_t launch_heat_plain_steps(const HeatPlainArgs& a, const HeatPersist& p
     HeatPlainArgs aa = a;
     HeatPersist pp = p;
     void* args[2] = {&aa, &pp};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_plain_pair_steps), dim3(a.nblocks), tile_block(),
+    // the tiling's rows are the block's y extent: 8 (256 threads) or 32 (1024)
+    if (a.tiles.rows == 32)
+        return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_plain_pair_steps<32>), dim3(a.nblocks),
+                                           dim3(32, 32), args, 0, s);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_plain_pair_steps<8>), dim3(a.nblocks), tile_block(),
                                        args, 0, s);
 }
 
@@ -141,7 +145,8 @@ int occupancy_f64(KernelId id) {
     switch (id) {
         case kHeatPlain: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_step, 256, 0); break;
         case kHeatPlainPair: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_step, 256, 0); break;
-        case kHeatPlainSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_steps, 256, 0); break;
+        case kHeatPlainSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_steps<8>, 256, 0); break;
+        case kHeatPlainSteps32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_steps<32>, 1024, 0); break;
         case kHallF64:
             e = allow_smem(hall_step<double, false>, (int)hall_smem_bytes<double>());
             if (e != cudaSuccess) break;

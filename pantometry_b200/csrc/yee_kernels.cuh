@@ -379,8 +379,8 @@ struct YeeStepArgs {
     const Real* __restrict__ cch[3];
     int lossless, mu_var;
     // FP32 TMA form only: a box of nb_w³ lattice nodes from (nb_x0, nb_y0, nb_z0) whose six
-    // components are stepped in f64 by yee_near_step after this kernel; the kernel leaves the
-    // box's energy terms to it and hands it its sums instead of closing the books. nb_w = 0: none.
+    // components the kernel's last block steps again in f64 (yee_near_body) once the grid's cells
+    // are in; the box's energy terms are left to it, and it closes the books. nb_w = 0: none.
     int nb_x0, nb_y0, nb_z0, nb_w;
 };
 

@@ -10,8 +10,9 @@
 //
 // The rule, in one line: inside the box every value is f64, outside it f32, and every stencil reads
 // what is stored. yee_tma_step steps every node in f32 from the stored values (the box's f32
-// roundings included) but leaves the box's energy terms out and the source to this kernel, and
-// hands over its four sums. This kernel (one block, after it, before the walls) then
+// roundings included) but leaves the box's energy terms and the source out; its last block, once
+// every other block's cells and sums are in, runs yee_near_body with the grid's four sums (before
+// the walls, which run after the step). yee_near_body then
 //   A. forms H⁺ of the box's faces in f64 from the box's f64 H and E (f32 values outside),
 //   B. forms Eⁿ⁺¹ of the box's edges in f64 from those H⁺ (f32 H⁺ outside), with the source,
 //   C. forms again, in f32, the edges just outside the box whose curl reads a box face, so they
@@ -30,27 +31,6 @@
 #include "yee_tma.cuh"
 
 namespace pm {
-
-struct YeeNearArgs {
-    const float* old[6];    // ex ey ez hx hy hz at step n, padded lattice
-    float* neu[6];          // at n + 1, already stepped by yee_tma_step
-    const double* nold;     // the box's f64 values at step n: [q][lk][lj][li], w³ per component
-    double* nneu;           // at n + 1
-    int x0, y0, z0, w;      // the box: w³ lattice nodes from (x0, y0, z0)
-    unsigned L, ny1;        // lattice row pitch and rows per plane
-    int nx, ny, nz;
-    double ch, gain, decay;  // f64 coefficients of one medium: g/μ, edge gain and decay
-    float chf, gainf, decf;  // the f32 ones yee_tma_step used (the ring's edges)
-    const float* cgain[3];   // MEDIA: per-edge gains on the padded lattice
-    int media, lossy;
-    double sig0;
-    const uint8_t* solid;
-    int src_i, src_j, src_k;
-    const double* current;
-    long long ncurrent;
-    double eps_src, sig_src, dt, volume, g, eps_u, mu_u;
-    DevState* st;
-};
 
 __device__ __forceinline__ bool near_in(const YeeNearArgs& a, int i, int j, int k) {
     return (unsigned)(i - a.x0) < (unsigned)a.w && (unsigned)(j - a.y0) < (unsigned)a.w &&
@@ -104,13 +84,16 @@ static __global__ void yee_near_seed(YeeNearArgs a) {
     }
 }
 
-// One work item per (component, node): 3 × w³ in phases A and B, 3 × (w+1)³ in phase C.
-constexpr int kNearThreads = 384;
+// A load of the new field, written by the other blocks of the step: from L2, past this SM's L1.
+__device__ __forceinline__ float near_ld_new(const float* p) { return __ldcg(p); }
 
+// Run by the whole last block of yee_tma_step, once every other block's cells are in, with the
+// grid's four sums (valid in thread 0): one work item per (component, node), 3 × w³ in phases A
+// and B, 3 × (w+1)³ in phase C, strided over the block's threads.
 template <bool SOLID>
-static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs a) {
+__device__ void yee_near_body(const YeeNearArgs& a, const double (&tma)[4]) {
     DevState* st = a.st;
-    if (st->violated) return;
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z, tid0 = linear_tid();
     const int w = a.w, w3 = w * w * w;
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const long long step = st->steps;
@@ -120,7 +103,7 @@ static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs
     // A. H⁺ of face component q at each box node (cavity.rs:1346-1379) with its term of ½μ H⁻·H⁺,
     // and the ½ε|Eⁿ|² term of edge component q there (half weights of node-centred boundary
     // samples, cavity.rs:766-772)
-    for (int r = threadIdx.x; r < 3 * w3; r += blockDim.x) {
+    for (int r = tid0; r < 3 * w3; r += nthreads) {
         const int q = r / w3, l = r - q * w3;
         const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
         const double hi = (i == 0 || i == nx) ? 0.5 : 1.0, hj = (j == 0 || j == ny) ? 0.5 : 1.0,
@@ -155,11 +138,14 @@ static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs
     __syncthreads();  // the box's H⁺, in both stores, before any edge reads it
 
     // B. Eⁿ⁺¹ of edge component q at each box node (cavity.rs:1383-1452), the soft current, Joule loss
-    for (int r = threadIdx.x; r < 3 * w3; r += blockDim.x) {
+    for (int r = tid0; r < 3 * w3; r += nthreads) {
         const int q = r / w3, l = r - q * w3;
         const int i = a.x0 + l % w, j = a.y0 + (l / w) % w, k = a.z0 + l / (w * w);
         const size_t n = near_lat(a, i, j, k);
-        auto hp = [&](int c, int ii, int jj, int kk) { return near_get(a, a.nneu, near_comp(a.neu, c), c, ii, jj, kk); };
+        auto hp = [&](int c, int ii, int jj, int kk) {
+            return near_in(a, ii, jj, kk) ? a.nneu[near_box(a, c, ii, jj, kk)]
+                                          : (double)near_ld_new(near_comp(a.neu, c) + near_lat(a, ii, jj, kk));
+        };
         double curl;
         if (q == 0) curl = (hp(5, i, j, k) - hp(5, i, j - 1, k)) - (hp(4, i, j, k) - hp(4, i, j, k - 1));
         else if (q == 1) curl = (hp(3, i, j, k) - hp(3, i, j, k - 1)) - (hp(5, i, j, k) - hp(5, i - 1, j, k));
@@ -195,7 +181,7 @@ static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs
     // (the box's own faces now hold the roundings of their f64 values), as yee_tma_step forms it;
     // with a lossy medium the Joule term yee_tma_step booked for it is replaced by this value's.
     const int w1 = w + 1, ring = w1 * w1 * w1;
-    for (int r = threadIdx.x; r < 3 * ring; r += blockDim.x) {
+    for (int r = tid0; r < 3 * ring; r += nthreads) {
         const int q = r / ring, l = r - q * ring;
         const int i = a.x0 + l % w1, j = a.y0 + (l / w1) % w1, k = a.z0 + l / (w1 * w1);
         if (near_in(a, i, j, k)) continue;
@@ -206,7 +192,7 @@ static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs
                                     : (near_in(a, i - 1, j, k) || near_in(a, i, j - 1, k));
         if (!reads) continue;
         const size_t n = near_lat(a, i, j, k);
-        auto h = [&](int c, int ii, int jj, int kk) { return near_comp(a.neu, c)[near_lat(a, ii, jj, kk)]; };
+        auto h = [&](int c, int ii, int jj, int kk) { return near_ld_new(near_comp(a.neu, c) + near_lat(a, ii, jj, kk)); };
         const float before = near_comp(a.old, q)[n];
         float curl;
         if (q == 0) curl = (h(5, i, j, k) - h(5, i, j - 1, k)) - (h(4, i, j, k) - h(4, i, j, k - 1));
@@ -219,7 +205,7 @@ static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs
         v = interior ? v : 0.0f;
         float* out = near_comp(a.neu, q);
         if (a.lossy && interior) {
-            const double mold = 0.5 * ((double)before + (double)out[n]);
+            const double mold = 0.5 * ((double)before + (double)near_ld_new(out + n));
             const double mnew = 0.5 * ((double)before + (double)v);
             acc[2] += a.sig0 * mnew * mnew * a.dt * a.volume - a.sig0 * mold * mold * a.dt * a.volume;
         }
@@ -235,9 +221,9 @@ static __global__ void __launch_bounds__(kNearThreads) yee_near_step(YeeNearArgs
     // D. the box's sums in a fixed order, added to yee_tma_step's, and the books
     __shared__ double red[32 * 4];
     block_sum<4>(acc, red);
-    if (threadIdx.x == 0) {
+    if (tid0 == 0) {
         double total[4];
-        for (int q = 0; q < 4; ++q) total[q] = st->near_acc[q] + acc[q];
+        for (int q = 0; q < 4; ++q) total[q] = tma[q] + acc[q];
         yee_tma_close(st, total, a.media != 0, a.g, a.eps_u, a.mu_u, a.volume, a.src_i >= 0);
     }
 }

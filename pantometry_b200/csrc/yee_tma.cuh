@@ -138,9 +138,35 @@ __device__ __forceinline__ void yee_tma_close(DevState* st, const double (&acc)[
     audit_and_commit(st, total, scale);
 }
 
+// The near field of a soft current, kept in f64 (yee_near.cuh): its arguments, and the last
+// block's work on it after the grid's sums are in.
+struct YeeNearArgs {
+    const float* old[6];    // ex ey ez hx hy hz at step n, padded lattice
+    float* neu[6];          // at n + 1, already stepped by yee_tma_step
+    const double* nold;     // the box's f64 values at step n: [q][lk][lj][li], w³ per component
+    double* nneu;           // at n + 1
+    int x0, y0, z0, w;      // the box: w³ lattice nodes from (x0, y0, z0)
+    unsigned L, ny1;        // lattice row pitch and rows per plane
+    int nx, ny, nz;
+    double ch, gain, decay;  // f64 coefficients of one medium: g/μ, edge gain and decay
+    float chf, gainf, decf;  // the f32 ones yee_tma_step used (the ring's edges)
+    const float* cgain[3];   // MEDIA: per-edge gains on the padded lattice
+    int media, lossy;
+    double sig0;
+    const uint8_t* solid;
+    int src_i, src_j, src_k;
+    const double* current;
+    long long ncurrent;
+    double eps_src, sig_src, dt, volume, g, eps_u, mu_u;
+    DevState* st;
+};
+template <bool SOLID>
+__device__ void yee_near_body(const YeeNearArgs& a, const double (&tma)[4]);
+
 template <int P, int S, bool SOLID, bool MEDIA, int MINB>
 static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<float> a, unsigned L,
-                                                             const __grid_constant__ YeeMaps m) {
+                                                             const __grid_constant__ YeeMaps m,
+                                                             const __grid_constant__ YeeNearArgs nr) {
     DevState* st = a.st;
     if (st->violated) return;
     using Lay = YeeTmaLayout<P, MEDIA>;
@@ -330,12 +356,13 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
         }
         return;
     }
-    if (finish_blocks<4>(acc, a.partials, a.nblocks, &st->counter) && linear_tid() == 0) {
-        if (a.nb_w > 0) {  // the near-field box kernel adds its terms and closes the books
-            for (int q = 0; q < 4; ++q) st->near_acc[q] = acc[q];
-        } else {
+    if (finish_blocks<4>(acc, a.partials, a.nblocks, &st->counter)) {
+        // the last block: with a near-field box it steps the box, adds the box's terms and closes the
+        // books (every other block's cells are in by now: each published its sums after them)
+        if (a.nb_w > 0)
+            yee_near_body<SOLID>(nr, acc);
+        else if (linear_tid() == 0)
             yee_tma_close(st, acc, MEDIA, a.g, a.eps_u, a.mu_u, a.volume, a.src_i >= 0);
-        }
     }
 }
 

@@ -2,7 +2,8 @@
 
 A 64³ block is launch-bound: its state (2 MiB) sweeps from L2 in about a microsecond, far below a
 kernel launch. Calls of two or more steps on a small uniform block take every step in one launch
-with one bounded grid-wide wait per step, each block auditing its own copy of the books. These tests
+with one bounded grid-wide wait per step; one block keeps the books, auditing each step while the
+others take the next (a failed audit ends the call with that step's state). These tests
 check that path against the one-step kernels (a call of one step never takes it): the same fields
 bit for bit, the same books, the same step when an audit fails, and a wait that runs out (its
 budget set to zero) ending the call with PM_DEVICE_TIMEOUT while the handle stays usable.
