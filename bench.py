@@ -474,7 +474,7 @@ def run_ensemble(args):
                    "grids_per_s": round(len(all_grids) * args.steps / (ms32 * 1e-3), 3)},
         "e2e": {"value": round(total_cells * T * args.steps / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
                 "h2d_bytes_per_step": local_cells * 8, "d2h_bytes_per_step": len(grids) * 56},
-        "gpu_launches": args.steps * T,
+        "gpu_launches": args.steps * T * (2 if tma else 1),  # the TMA step and its books kernel
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": round(ENS_F32_TRAFFIC_PER_CELL * local_cells) if tma else None,
@@ -743,9 +743,13 @@ def cavity_record(local, stream, peak, n=384, timed_steps=2000, compare_steps=10
     cells = n ** 3
     dt = cfg["dt"]
 
+    tiles = {}
+
     def timed(precision, tol):
         c = W.build_cavity(cfg, precision=precision, device=local)
         c.set_stream(stream.cuda_stream)
+        if precision == "f32":  # the TMA kernel's tile shape, timed on this grid
+            tiles[precision] = list(c.autotune(trial_steps=8))
         c.set_tolerance(tol)
         assert c.step(dt, 128) is None
         torch.cuda.synchronize()
@@ -783,7 +787,7 @@ def cavity_record(local, stream, peak, n=384, timed_steps=2000, compare_steps=10
         "workload": f"yee_cavity {n}^3 cells, vacuum, conducting walls, Courant 0.99/sqrt(3), soft z-current at the "
                     f"centre Ez edge (its 5^3 near field in f64), FP64 audit every timestep",
         "value": round(value, 3), "unit": UNIT, "timed_timesteps": timed_steps,
-        "ms_per_timestep": round(ms32 / timed_steps, 4),
+        "ms_per_timestep": round(ms32 / timed_steps, 4), "tile_planes_stages": tiles.get("f32"),
         "plain_f64": {"value": round(plain, 3), "ms_per_timestep": round(ms64 / timed_steps, 4),
                       "roofline_frac": round(96 * cells / (ms64 / timed_steps * 1e-3) / 1e9 / peak, 4)},
         "fp32_over_f64": round(value / plain, 3),

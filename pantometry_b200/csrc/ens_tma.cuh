@@ -18,9 +18,8 @@
 // results: every partial is stored by brick and warp, and each block's are summed in fixed order.
 //
 // No barrier spans the consumer warps. Each warp waits for its stage, computes its row of the
-// brick, hands the slot back, and at the end of a brick stores its own two partials and takes a
-// ticket of its block; the warp holding the block's last ticket sums the block's partials in a
-// fixed order and runs its ledger and audit.
+// brick, hands the slot back, and at the end of a brick stores its own two partials; after the step
+// ens_tma_books sums each block's partials in a fixed order and runs its ledger and audit.
 #pragma once
 
 #include "ensemble_kernels.cuh"
@@ -332,49 +331,48 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
         __syncwarp();
         if (lane == 0) mbar_arrive(empty_base + 8 * slot);
         if (brick_done && !hold) {
-            // this warp's partials, then its ticket of the block; the warp with the block's last
-            // ticket sums the block's partials in fixed order, then runs its ledger and audit
-            const EnsGrid& g = a.grids[gi];
-            DevState* st = a.states + gi;
+            // this warp's two partials of the brick, stored by brick and warp; ens_tma_books sums
+            // them per block once the step is done (no ordering inside this kernel, so no warp waits
+            // for its field stores to land)
             warp_sum<2>(acc);
-            unsigned ticket = 0;
             if (lane == 0) {
                 const size_t at = ((size_t)brick * 8 + (size_t)warp) * 2;
                 a.partials[at] = acc[0];
                 a.partials[at + 1] = acc[1];
-                // the ticket in acquire-release order: this lane's partials are visible to whoever
-                // takes a later ticket, and it sees those of every earlier one, without a full fence
-                // in every warp of every brick
-                asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(ticket) : "l"(&st->counter) : "memory");
-            }
-            __syncwarp();  // the other lanes' reads below come after lane 0's acquire
-            ticket = __shfl_sync(0xffffffffu, ticket, 0);
-            if (ticket == g.nbricks * 8 - 1) {
-                // the last ticket: every other warp's partials, acquired
-                asm volatile("fence.acq_rel.gpu;" ::: "memory");
-                double v[2] = {0.0, 0.0};
-                const size_t first = (size_t)g.first_brick * 8, count = (size_t)g.nbricks * 8;
-                for (size_t q = lane; q < count; q += 32) {
-                    v[0] += __ldcg(&a.partials[(first + q) * 2]);
-                    v[1] += __ldcg(&a.partials[(first + q) * 2 + 1]);
-                }
-                warp_sum<2>(v);
-                if (lane == 0) {
-                    st->counter = 0u;
-                    const double stored = g.capacity * v[0];
-                    st->lost += g.capacity * v[1];
-                    double total = 0.0, scale = 0.0;
-                    ledger_add(total, scale, stored);
-                    ledger_add(total, scale, st->lost);
-                    ledger_add(total, scale, -st->supplied);
-                    st->part[0] = stored;
-                    st->part[1] = st->lost;
-                    st->part[2] = -st->supplied;
-                    audit_and_commit(st, total, scale);
-                }
             }
         }
         if (brick_done) acc[0] = acc[1] = 0.0;
+    }
+}
+
+// The books of every block after ens_tma_step: one warp per block sums its bricks' partials in a
+// fixed order (lane-strided, then the warp's tree), then runs its ledger and audit. A block held at
+// the step's start (violated) was copied, not stepped, and is left alone.
+static __global__ void __launch_bounds__(256) ens_tma_books(const EnsArgs<float> a) {
+    const int lane = threadIdx.x & 31;
+    const unsigned gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (gi >= a.ngrids) return;
+    DevState* st = a.states + gi;
+    if (st->violated) return;
+    const EnsGrid& g = a.grids[gi];
+    double v[2] = {0.0, 0.0};
+    const size_t first = (size_t)g.first_brick * 8, count = (size_t)g.nbricks * 8;
+    for (size_t q = lane; q < count; q += 32) {
+        v[0] += a.partials[(first + q) * 2];
+        v[1] += a.partials[(first + q) * 2 + 1];
+    }
+    warp_sum<2>(v);
+    if (lane == 0) {
+        const double stored = g.capacity * v[0];
+        st->lost += g.capacity * v[1];
+        double total = 0.0, scale = 0.0;
+        ledger_add(total, scale, stored);
+        ledger_add(total, scale, st->lost);
+        ledger_add(total, scale, -st->supplied);
+        st->part[0] = stored;
+        st->part[1] = st->lost;
+        st->part[2] = -st->supplied;
+        audit_and_commit(st, total, scale);
     }
 }
 

@@ -357,6 +357,8 @@ pm_status pm_ensemble_create(const pm_ensemble_grid* grids, int count, int preci
             const double gf = q.exposed ? ens_series_with_half_cell(d.convection_w_per_m2_k * u.share[f], u.k_cell, u.share[f], d.dx) : 0.0;
             q.b[f] = (float)(dm * gf / d.dx);
             q.off[f] = 0.0f;  // the films' ambient is the block's own T0
+            if (d.convection_w_per_m2_k == std::numeric_limits<double>::infinity())
+                q.g_inf[f] = ens_series_with_half_cell(d.convection_w_per_m2_k, u.k_cell, u.share[f], d.dx);
         }
     }
     e->dcells = offset;

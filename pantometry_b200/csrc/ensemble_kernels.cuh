@@ -44,6 +44,9 @@ struct EnsGrid {
     float b[6];   // dt · mobility · g_f / dx per film face
     float off[6]; // T0 − ambient per film face
     float pad;
+    // h = +inf: per face the film's series with the half cell, the same for every cell of the face
+    // (bare / gap is +inf for every finite nonzero gap; see film_flux)
+    double g_inf[6];
 };
 
 struct EnsBrick {
@@ -77,11 +80,16 @@ __device__ __forceinline__ double ens_film_flux(const EnsGrid& g, int i, int j, 
         const double ambient = g.ambient[f];
         const double gap = here - ambient;
         if (gap == 0.0) continue;
-        // crates/pantometry-thermal/src/lib.rs:104-110 `Environment::loss_from`, area = share
-        const double convective = g.convection[f] * share * (here - ambient);
-        const double radiative = g.eps_cell * kStefanBoltzmann * share * (powi4(here) - powi4(ambient));
-        const double bare = convective + radiative;
-        const double cond = series_with_half_cell(bare / gap, g.k_cell, share, g.dx);
+        double cond;
+        if (isinf(g.convection[f]) && g.convection[f] > 0.0) {
+            cond = g.g_inf[f];
+        } else {
+            // crates/pantometry-thermal/src/lib.rs:104-110 `Environment::loss_from`, area = share
+            const double convective = g.convection[f] * share * (here - ambient);
+            const double radiative = g.eps_cell * kStefanBoltzmann * share * (powi4(here) - powi4(ambient));
+            const double bare = convective + radiative;
+            cond = series_with_half_cell(bare / gap, g.k_cell, share, g.dx);
+        }
         out += cond * gap / g.dx;
     }
     return out;

@@ -17,7 +17,11 @@ cudaError_t launch_heat_f32_steps(const HeatF32Args& a, const HeatPersist& p, cu
     HeatF32Args aa = a;
     HeatPersist pp = p;
     void* args[2] = {&aa, &pp};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_f32_quad_steps), dim3(a.nblocks), tile_block(),
+    // the tiling's rows are the block's y extent: 8 (256 threads) or 32 (1024)
+    if (a.tiles.rows == 32)
+        return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_f32_quad_steps<32>), dim3(a.nblocks),
+                                           dim3(32, 32), args, 0, s);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(heat_f32_quad_steps<8>), dim3(a.nblocks), tile_block(),
                                        args, 0, s);
 }
 
@@ -138,21 +142,23 @@ bool hall_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz, unsigned
 }
 
 template <int P, int S, bool MEDIA, int MINB>
-static cudaError_t launch_yee_tma_shape(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, cudaStream_t s) {
+static cudaError_t launch_yee_tma_shape(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, const YeeNearArgs& n,
+                                       cudaStream_t s) {
     const int smem = (int)yee_tma_smem_bytes_for<P, MEDIA>(S);
     auto k = a.solid ? yee_tma_step<P, S, true, MEDIA, MINB> : yee_tma_step<P, S, false, MEDIA, MINB>;
-    return launch_smem(k, a.nblocks, tile_block(), smem, s, a, L, m);
+    return launch_smem(k, a.nblocks, tile_block(), smem, s, a, L, m, n);
 }
-cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s) {
+cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s,
+                           const YeeNearArgs& n) {
     static_assert(kYeeTmaUniformShapes[0].planes == 3 && kYeeTmaUniformShapes[1].planes == 4 &&
                       kYeeTmaUniformShapes[2].stages == 3 && kYeeTmaMediaShapes[0].planes == 4 &&
                       kYeeTmaMediaShapes[1].planes == 3,
                   "the dispatch below instantiates the shape lists in order");
-    if (!a.uniform) return shape == 1 ? launch_yee_tma_shape<3, 2, true, 3>(a, L, m, s) : launch_yee_tma_shape<4, 2, true, 2>(a, L, m, s);
+    if (!a.uniform) return shape == 1 ? launch_yee_tma_shape<3, 2, true, 3>(a, L, m, n, s) : launch_yee_tma_shape<4, 2, true, 2>(a, L, m, n, s);
     switch (shape) {
-        case 1: return launch_yee_tma_shape<4, 2, false, 2>(a, L, m, s);
-        case 2: return launch_yee_tma_shape<3, 3, false, 2>(a, L, m, s);
-        default: return launch_yee_tma_shape<3, 2, false, 3>(a, L, m, s);
+        case 1: return launch_yee_tma_shape<4, 2, false, 2>(a, L, m, n, s);
+        case 2: return launch_yee_tma_shape<3, 3, false, 2>(a, L, m, n, s);
+        default: return launch_yee_tma_shape<3, 2, false, 3>(a, L, m, n, s);
     }
 }
 template <int P, int S, bool MEDIA, int MINB>
@@ -165,11 +171,6 @@ static int yee_tma_occupancy() {
     return n > 0 ? n : 1;
 }
 
-cudaError_t launch_yee_near(const YeeNearArgs& a, bool solid, cudaStream_t s) {
-    if (solid) yee_near_step<true><<<1, kNearThreads, 0, s>>>(a);
-    else yee_near_step<false><<<1, kNearThreads, 0, s>>>(a);
-    return cudaGetLastError();
-}
 cudaError_t launch_yee_near_seed(const YeeNearArgs& a, cudaStream_t s) {
     yee_near_seed<<<1, 256, 0, s>>>(a);
     return cudaGetLastError();
@@ -193,7 +194,10 @@ cudaError_t launch_yee_relayout(const void* src, bool src_f64, void* dst, bool d
 
 cudaError_t launch_ens_tma(const EnsTmaArgs& t, unsigned nblocks, cudaStream_t s) {
     const int smem = (int)ens_tma_smem_bytes();
-    return launch_smem(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, nblocks, kEnsConsumers + 32, smem, s, t);
+    cudaError_t e = launch_smem(ens_tma_step<kEnsTmaPlanes, kEnsTmaStages>, nblocks, kEnsConsumers + 32, smem, s, t);
+    if (e != cudaSuccess) return e;
+    ens_tma_books<<<(t.e.ngrids + 7) / 8, 256, 0, s>>>(t.e);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, int nx, int ny, int nz, int pitch,
@@ -257,7 +261,8 @@ int occupancy_f32(KernelId id) {
     switch (id) {
         case kHeatF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_step<false>, 256, 0); break;
         case kHeatF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_step, 256, 0); break;
-        case kHeatF32QuadSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_steps, 256, 0); break;
+        case kHeatF32QuadSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_steps<8>, 256, 0); break;
+        case kHeatF32QuadSteps32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_steps<32>, 1024, 0); break;
         case kHallF32:
             e = allow_smem(hall_step<float, false>, (int)hall_smem_bytes<float>());
             if (e != cudaSuccess) break;
