@@ -86,6 +86,149 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar) {
 }
 constexpr int kEnsConsumers = 256;
 
+// One warp's row of one stage: the cells (i, j, kb .. kb + hn − 1) of a block of m.nx × m.ny × m.nz
+// cells, read from the stage tile `s` (x0−4 .. x0+35, y0−1 .. y0+8, kb−1 .. kb+P, the block's own
+// tile at x0, y0) and written through `out`, one plane apart. The per-cell arithmetic of
+// heat_f32_step in the same order and roundings, shared by the ensemble's TMA kernel and the single
+// block's (heat_tma_step), so all three agree bit for bit.
+template <int P>
+__device__ __forceinline__ void tma_stage_row(const EnsTmaStage<P>& s, const EnsBrickInfo& m, int x0, int tx, int ty,
+                                              int i, int j, int kb, int hn, float* __restrict__ out, size_t plane,
+                                              double (&acc)[2]) {
+    const int nx = m.nx, ny = m.ny, nz = m.nz;
+    const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
+    const bool xedge = x0 == 0 || x0 + 32 >= nx;  // the brick holds an x face
+    const float ga = m.a;
+    if (!xedge && yl && yh && hn == P && kb > 0 && kb + P < nz) {
+        // a whole stage of interior cells: no film, no bound, the planes below and
+        // above carried in registers; the general form's arithmetic without its zeros
+        float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
+#pragma unroll
+        for (int h = 0; h < P; ++h) {
+            const float above = s.t[h + 2][ty + 1][tx + 4];
+            const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+            const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
+            const float sum = (((((xm - here) + (xp - here)) + (ym - here)) + (yp - here)) + (below - here)) + (above - here);
+            const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
+            *out = nd;
+            out += plane;
+            acc[0] += (double)nd;
+            below = here;
+            here = above;
+        }
+    } else if (yl && yh) {
+        // a stage of a row inside the block in y (a brick on an x face, a stage holding a
+        // z face, or a partial stage): the general form's sums and films term for term,
+        // the x faces' taken by select per lane and the z faces' per plane, so the stage
+        // stays one straight run of planes. Adding +0 for an absent neighbour is adding
+        // nothing, since a sum that starts at +0 is never −0 here.
+        const int exposed = m.exposed;
+        const bool fx0 = ((exposed >> 0) & 1) && !xl, fx1 = ((exposed >> 1) & 1) && !xh;
+        const bool fz0 = ((exposed >> 4) & 1) && kb == 0, fz1 = (exposed >> 5) & 1;
+        const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
+        const int zlast = nz - 1 - kb;  // the stage's plane on the z+ face, if below hn
+        double col_shed = 0.0;
+        float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
+#pragma unroll
+        for (int h = 0; h < P; ++h) {
+            if (h >= hn) break;
+            const bool zl = h > 0 || kb > 0, zh = h < zlast;
+            const float above = s.t[h + 2][ty + 1][tx + 4];
+            const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+            const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
+            float sum = 0.0f;
+            sum += xl ? xm - here : 0.0f;
+            sum += xh ? xp - here : 0.0f;
+            sum += ym - here;
+            sum += yp - here;
+            sum += zl ? below - here : 0.0f;
+            sum += zh ? above - here : 0.0f;
+            float shed = 0.0f;
+            const float v0 = __fmaf_rn(b0, here + o0, shed);
+            shed = fx0 ? v0 : shed;
+            const float v1 = __fmaf_rn(b1, here + o1, shed);
+            shed = fx1 ? v1 : shed;
+            if (h == 0 && fz0) shed = __fmaf_rn(m.b[4], here + m.off[4], shed);
+            if (fz1 && !zh) shed = __fmaf_rn(m.b[5], here + m.off[5], shed);
+            if (exposed) col_shed += (double)shed;
+            const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
+            *out = nd;
+            out += plane;
+            acc[0] += (double)nd;
+            below = here;
+            here = above;
+        }
+        acc[1] += col_shed;
+    } else {
+        // The general form, taken by the whole warp: its row (y) and each plane (z) are
+        // the same for every lane, so those tests are uniform, and a lane on an x face
+        // selects its terms rather than diverging. The sums start at +0 and so are never
+        // −0, which makes adding +0 for an absent neighbour or film exact; the film terms
+        // are the fused b·(here + off) + shed that the plain `shed += ...` contracts to.
+        const int exposed = m.exposed;
+        const bool ex0 = xedge && ((exposed >> 0) & 1), ex1 = xedge && ((exposed >> 1) & 1);
+        const bool ey0 = ((exposed >> 2) & 1) && !yl, ey1 = ((exposed >> 3) & 1) && !yh;
+        const bool ez0 = ((exposed >> 4) & 1) && kb == 0;  // plane 0 of the stage is the z− face
+        const bool ez1 = (exposed >> 5) & 1;
+        const int zlast = nz - 1 - kb;  // the stage's plane on the z+ face, if below P
+        // the y and z films are taken only by stages on a face row or a face plane
+        const bool faces = ey0 || ey1 || ez0 || (ez1 && zlast < hn);
+        // the x faces' film coefficients, used by every cell of the stage, in registers
+        const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
+        double col_shed = 0.0;
+        auto run = [&](auto faces_tag, auto full_tag) {
+            constexpr bool FACES = decltype(faces_tag)::value, FULL = decltype(full_tag)::value;
+            float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
+#pragma unroll
+            for (int h = 0; h < P; ++h) {
+                if (!FULL && h >= hn) break;
+                const bool zl = h > 0 || kb > 0, zh = h < zlast;
+                const float above = s.t[h + 2][ty + 1][tx + 4];
+                const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+                float sum = 0.0f;  // the neighbours present, in the reference's order
+                sum += xl ? xm - here : 0.0f;
+                sum += xh ? xp - here : 0.0f;
+                if (yl) sum += s.t[h + 1][ty][tx + 4] - here;
+                if (yh) sum += s.t[h + 1][ty + 2][tx + 4] - here;
+                if (zl) sum += below - here;
+                if (zh) sum += above - here;
+                float shed = 0.0f;
+                if (exposed) {
+                    if (ex0) {
+                        const float v = __fmaf_rn(b0, here + o0, shed);
+                        shed = xl ? shed : v;
+                    }
+                    if (ex1) {
+                        const float v = __fmaf_rn(b1, here + o1, shed);
+                        shed = xh ? shed : v;
+                    }
+                    if constexpr (FACES) {
+                        if (ey0) shed = __fmaf_rn(m.b[2], here + m.off[2], shed);
+                        if (ey1) shed = __fmaf_rn(m.b[3], here + m.off[3], shed);
+                        if (ez0 && h == 0) shed = __fmaf_rn(m.b[4], here + m.off[4], shed);
+                        if (ez1 && !zh) shed = __fmaf_rn(m.b[5], here + m.off[5], shed);
+                    }
+                    col_shed += (double)shed;
+                }
+                const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
+                *out = nd;
+                out += plane;
+                acc[0] += (double)nd;
+                below = here;
+                here = above;
+            }
+        };
+        if (faces) {
+            if (hn == P) run(Flag<true>{}, Flag<true>{});
+            else run(Flag<true>{}, Flag<false>{});
+        } else {
+            if (hn == P) run(Flag<false>{}, Flag<true>{});
+            else run(Flag<false>{}, Flag<false>{});
+        }
+        acc[1] += col_shed;
+    }
+}
+
 // Warps 0-7 consume (the cells of a 32 × 8 brick column each); warp 8 produces: it takes the
 // bricks of the walk from the shared counter, one brick ahead, and for every stage issues the
 // brick's record and the tile, S − 1 stages ahead. Slots are handed back and forth with a full and
@@ -190,7 +333,7 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
         const St& s = ring[slot];
         const int kb = stage_kb[slot];
         const unsigned brick = stage_brick[slot], gi = m.grid;
-        const int nx = m.nx, ny = m.ny, nz = m.nz, pitch = m.pitch;
+        const int nx = m.nx, ny = m.ny, pitch = m.pitch;
         const bool hold = (holdmask[gi >> 5] >> (gi & 31)) & 1u;
         const int i = m.x0 + tx, j = m.y0 + ty;
         if (i < nx && j < ny) {
@@ -201,129 +344,7 @@ static __global__ void __launch_bounds__(kEnsConsumers + 32, PM_ENS_TMA_MIN_BLOC
             if (hold) {
                 for (int h = 0; h < hn; ++h, out += plane) *out = s.t[h + 1][ty + 1][tx + 4];
             } else {
-                const bool xl = i > 0, xh = i + 1 < nx, yl = j > 0, yh = j + 1 < ny;
-                const bool xedge = m.x0 == 0 || m.x0 + 32 >= nx;  // the brick holds an x face
-                const float ga = m.a;
-                if (!xedge && yl && yh && hn == P && kb > 0 && kb + P < nz) {
-                    // a whole stage of interior cells: no film, no bound, the planes below and
-                    // above carried in registers; the general form's arithmetic without its zeros
-                    float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
-#pragma unroll
-                    for (int h = 0; h < P; ++h) {
-                        const float above = s.t[h + 2][ty + 1][tx + 4];
-                        const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
-                        const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
-                        const float sum = (((((xm - here) + (xp - here)) + (ym - here)) + (yp - here)) + (below - here)) + (above - here);
-                        const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -0.0f));
-                        *out = nd;
-                        out += plane;
-                        acc[0] += (double)nd;
-                        below = here;
-                        here = above;
-                    }
-                } else if (yl && yh && hn == P && kb > 0 && kb + P < nz) {
-                    // a whole stage of a brick on an x face, inside in y and z: the general form's
-                    // sums and x films term for term, the x faces' terms taken by select, so the
-                    // stage stays one straight run of planes
-                    const int exposed = m.exposed;
-                    const bool fx0 = ((exposed >> 0) & 1) && !xl, fx1 = ((exposed >> 1) & 1) && !xh;
-                    const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
-                    double col_shed = 0.0;
-                    float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
-#pragma unroll
-                    for (int h = 0; h < P; ++h) {
-                        const float above = s.t[h + 2][ty + 1][tx + 4];
-                        const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
-                        const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
-                        float sum = 0.0f;
-                        sum += xl ? xm - here : 0.0f;
-                        sum += xh ? xp - here : 0.0f;
-                        sum += ym - here;
-                        sum += yp - here;
-                        sum += below - here;
-                        sum += above - here;
-                        float shed = 0.0f;
-                        const float v0 = __fmaf_rn(b0, here + o0, shed);
-                        shed = fx0 ? v0 : shed;
-                        const float v1 = __fmaf_rn(b1, here + o1, shed);
-                        shed = fx1 ? v1 : shed;
-                        if (exposed) col_shed += (double)shed;
-                        const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
-                        *out = nd;
-                        out += plane;
-                        acc[0] += (double)nd;
-                        below = here;
-                        here = above;
-                    }
-                    acc[1] += col_shed;
-                } else {
-                    // The general form, taken by the whole warp: its row (y) and each plane (z) are
-                    // the same for every lane, so those tests are uniform, and a lane on an x face
-                    // selects its terms rather than diverging. The sums start at +0 and so are never
-                    // −0, which makes adding +0 for an absent neighbour or film exact; the film terms
-                    // are the fused b·(here + off) + shed that the plain `shed += ...` contracts to.
-                    const int exposed = m.exposed;
-                    const bool ex0 = xedge && ((exposed >> 0) & 1), ex1 = xedge && ((exposed >> 1) & 1);
-                    const bool ey0 = ((exposed >> 2) & 1) && !yl, ey1 = ((exposed >> 3) & 1) && !yh;
-                    const bool ez0 = ((exposed >> 4) & 1) && kb == 0;  // plane 0 of the stage is the z− face
-                    const bool ez1 = (exposed >> 5) & 1;
-                    const int zlast = nz - 1 - kb;  // the stage's plane on the z+ face, if below P
-                    // the y and z films are taken only by stages on a face row or a face plane
-                    const bool faces = ey0 || ey1 || ez0 || (ez1 && zlast < hn);
-                    // the x faces' film coefficients, used by every cell of the stage, in registers
-                    const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
-                    double col_shed = 0.0;
-                    auto run = [&](auto faces_tag, auto full_tag) {
-                        constexpr bool FACES = decltype(faces_tag)::value, FULL = decltype(full_tag)::value;
-                        float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
-#pragma unroll
-                        for (int h = 0; h < P; ++h) {
-                            if (!FULL && h >= hn) break;
-                            const bool zl = h > 0 || kb > 0, zh = h < zlast;
-                            const float above = s.t[h + 2][ty + 1][tx + 4];
-                            const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
-                            float sum = 0.0f;  // the neighbours present, in the reference's order
-                            sum += xl ? xm - here : 0.0f;
-                            sum += xh ? xp - here : 0.0f;
-                            if (yl) sum += s.t[h + 1][ty][tx + 4] - here;
-                            if (yh) sum += s.t[h + 1][ty + 2][tx + 4] - here;
-                            if (zl) sum += below - here;
-                            if (zh) sum += above - here;
-                            float shed = 0.0f;
-                            if (exposed) {
-                                if (ex0) {
-                                    const float v = __fmaf_rn(b0, here + o0, shed);
-                                    shed = xl ? shed : v;
-                                }
-                                if (ex1) {
-                                    const float v = __fmaf_rn(b1, here + o1, shed);
-                                    shed = xh ? shed : v;
-                                }
-                                if constexpr (FACES) {
-                                    if (ey0) shed = __fmaf_rn(m.b[2], here + m.off[2], shed);
-                                    if (ey1) shed = __fmaf_rn(m.b[3], here + m.off[3], shed);
-                                    if (ez0 && h == 0) shed = __fmaf_rn(m.b[4], here + m.off[4], shed);
-                                    if (ez1 && !zh) shed = __fmaf_rn(m.b[5], here + m.off[5], shed);
-                                }
-                                col_shed += (double)shed;
-                            }
-                            const float nd = __fadd_rn(here, __fmaf_rn(ga, sum, -shed));
-                            *out = nd;
-                            out += plane;
-                            acc[0] += (double)nd;
-                            below = here;
-                            here = above;
-                        }
-                    };
-                    if (faces) {
-                        if (hn == P) run(Flag<true>{}, Flag<true>{});
-                        else run(Flag<true>{}, Flag<false>{});
-                    } else {
-                        if (hn == P) run(Flag<false>{}, Flag<true>{});
-                        else run(Flag<false>{}, Flag<false>{});
-                    }
-                    acc[1] += col_shed;
-                }
+                tma_stage_row<P>(s, m, m.x0, tx, ty, i, j, kb, hn, out, plane, acc);
             }
         }
         const bool brick_done = kb + P >= z1;

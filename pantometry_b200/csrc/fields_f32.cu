@@ -200,6 +200,14 @@ cudaError_t launch_ens_tma(const EnsTmaArgs& t, unsigned nblocks, cudaStream_t s
     return cudaGetLastError();
 }
 
+cudaError_t launch_heat_tma(const HeatTmaArgs& a, const CUtensorMap& map, cudaStream_t s) {
+    return launch_smem(heat_tma_step<kEnsTmaPlanes, kEnsTmaStages>, a.nblocks, kEnsConsumers + 32,
+                       (int)ens_tma_smem_bytes(), s, a, map);
+}
+bool heat_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz) {
+    return hall_tma_map(map, base, nx, ny, nz, 40, 10, kEnsTmaPlanes + 2);
+}
+
 cudaError_t launch_ens_relayout(const double* kelvin, float* dev, double* out, int nx, int ny, int nz, int pitch,
                                 double t0, int to_dev, cudaStream_t s) {
     ens_relayout<<<kMeasureBlocks, 256, 0, s>>>(kelvin, dev, out, nx, ny, nz, pitch, t0, to_dev);
@@ -263,6 +271,12 @@ int occupancy_f32(KernelId id) {
         case kHeatF32Quad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_step, 256, 0); break;
         case kHeatF32QuadSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_steps<8>, 256, 0); break;
         case kHeatF32QuadSteps32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_f32_quad_steps<32>, 1024, 0); break;
+        case kHeatTma:
+            e = allow_smem(heat_tma_step<kEnsTmaPlanes, kEnsTmaStages>, (int)ens_tma_smem_bytes());
+            if (e != cudaSuccess) break;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_tma_step<kEnsTmaPlanes, kEnsTmaStages>,
+                                                              kEnsConsumers + 32, ens_tma_smem_bytes());
+            break;
         case kHallF32:
             e = allow_smem(hall_step<float, false>, (int)hall_smem_bytes<float>());
             if (e != cudaSuccess) break;

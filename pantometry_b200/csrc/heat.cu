@@ -61,6 +61,10 @@ struct Heat : Handle {
     bool wide = true;
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
+    // the TMA-staged FP32 form of a uniform block whose rows hold a multiple of 4 cells: the tensor
+    // maps of the two parities' deviations (heat_tma_step)
+    CUtensorMap tmaps[2];
+    bool tma_maps = false;
     // the persistent many-step path of small plain f64 blocks (heat_plain_pair_steps)
     DBuf dbarrier;
     unsigned wait_budget = 1u << 24;  // polls per grid-barrier wait, about 100 ns apart
@@ -475,6 +479,27 @@ struct Heat : Handle {
         return a;
     }
 
+    bool tma_form() const { return precision == PM_FIELDS_F32 && uniform && wide && nx % 4 == 0 && tma_maps; }
+    HeatTmaArgs tma_args(int par, double dt) const {
+        const HeatF32Args f = f32_args(par, dt);
+        HeatTmaArgs a{};
+        a.dnew = field[par ^ 1].as<float>();
+        a.nx = nx; a.ny = ny; a.nz = nz;
+        a.ntx = (unsigned)((nx + 31) / 32);
+        a.nty = (unsigned)((ny + 7) / 8);
+        a.ntz = (unsigned)((nz + kEnsTmaPlanes - 1) / kEnsTmaPlanes);
+        a.cell.nx = nx; a.cell.ny = ny; a.cell.nz = nz; a.cell.pitch = nx;
+        a.cell.exposed = f.exposed;
+        a.cell.a = f.a;
+        for (int q = 0; q < 6; ++q) { a.cell.b[q] = f.b[q]; a.cell.off[q] = f.off[q]; }
+        a.capacity = capacity;
+        a.st = state.as<DevState>();
+        a.partials = partials.as<double>();
+        const unsigned long long items = (unsigned long long)a.ntx * a.nty * a.ntz;
+        a.nblocks = (unsigned)std::min<unsigned long long>(items, wave_of(kHeatTma));
+        return a;
+    }
+
     HeatF32Args f32_args(int par, double dt) const {
         HeatF32Args a{};
         a.dold = field[par].as<float>();
@@ -609,6 +634,10 @@ pm_status pm_heat_create(const pm_heat_desc* d, pm_heat** out) {
         cudaError_t e = f.alloc(h->n() * h->esize());
         if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaMalloc field"); }
     }
+    // TMA maps of the FP32 deviations, where the rows hold a multiple of 4 cells (16-byte rows)
+    if (h->precision == PM_FIELDS_F32 && h->nx % 4 == 0 && (size_t)h->nx * h->ny * h->nz < (size_t(1) << 31))
+        h->tma_maps = heat_tma_map(&h->tmaps[0], h->field[0].p, h->nx, h->ny, h->nz) &&
+                      heat_tma_map(&h->tmaps[1], h->field[1].p, h->nx, h->ny, h->nz);
     // Solid3D::new starts every cell at `initial`.
     std::vector<double> t(h->n(), d->initial_kelvin);
     *out = reinterpret_cast<pm_heat*>(h);
@@ -814,6 +843,10 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
         });
     } else if (h->persistent(nsteps)) {
         s = h->run_persistent(nsteps, dt);
+    } else if (h->tma_form()) {
+        s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {
+            return launch_heat_tma(h->tma_args(par, dt), h->tmaps[par], st);
+        });
     } else {
         if ((s = h->prepare_f32(dt)) != PM_OK) return s;
         s = h->run_steps(nsteps, dt, true, [h, dt](int par, cudaStream_t st) {

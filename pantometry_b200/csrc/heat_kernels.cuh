@@ -265,11 +265,22 @@ __device__ __forceinline__ double heat_gap_cell(const HeatPlainArgs& a, int g, d
 }
 
 // Decode tile t of a tiling into the thread's column (i, j) and plane range [k0, k1).
+// In 32-bit arithmetic where the tiling allows (a 64-bit division is a long software sequence, and the
+// many-step kernels decode a tile every step).
 __device__ __forceinline__ void tile_column(const Tiles& T, long long t, int& i, int& j, int& k0, int& k1) {
-    const int tx = (int)(t % T.ntx);
-    const long long r = t / T.ntx;
-    const int ty = (int)(r % T.nty);
-    const int tz = (int)(r / T.nty);
+    int tx, ty, tz;
+    if (T.ntiles <= 0x7fffffffLL) {
+        const unsigned u = (unsigned)t, ntx = (unsigned)T.ntx, nty = (unsigned)T.nty;
+        const unsigned r = u / ntx;
+        tx = (int)(u - r * ntx);
+        ty = (int)(r % nty);
+        tz = (int)(r / nty);
+    } else {
+        tx = (int)(t % T.ntx);
+        const long long r = t / T.ntx;
+        ty = (int)(r % T.nty);
+        tz = (int)(r / T.nty);
+    }
     i = tx * 32 + threadIdx.x;
     j = ty * T.rows + threadIdx.y;
     k0 = tz * T.zc;
@@ -341,7 +352,8 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
                 if (k > 0) flux += a.kz[c] * (below - t0);
                 if (k + 1 < nz) flux += a.kz[c + plane] * (above - t0);
             }
-            const double shed = a.films.exposed ? film_flux(a, i, j, k, c, t0) : 0.0;
+            const bool face = i == 0 || i + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz;
+            const double shed = (a.films.exposed && face) ? film_flux(a, i, j, k, c, t0) : 0.0;
             const double mob = a.uniform ? a.mobility : a.mob[c];
             const double capc = a.uniform ? a.capacity : a.cap[c];
             double nt = t0 + a.dts * mob * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
@@ -360,8 +372,7 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PLAIN_MIN_BLOCKS) heat_pla
             a.tnew[c] = nt;
             acc[0] += capc * (nt - a.reference);                  // solid.rs:1583-1590
             if (shed != 0.0) acc[1] += a.dts * mob * shed * capc;  // solid.rs:1821-1823
-            if (a.radiating && (i == 0 || i + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz))
-                rate = fmax(rate, heat_cell_rate(a, i, j, k, c, nt));
+            if (a.radiating && face) rate = fmax(rate, heat_cell_rate(a, i, j, k, c, nt));
             below = here;
             here = above;
         }
@@ -434,11 +445,13 @@ __device__ __forceinline__ void heat_pair_tile(const HeatPlainArgs& a, long long
             if (yh) flux += kf * (pv[e] - t0);
             if (k > 0) flux += kf * (bv[e] - t0);
             if (k + 1 < nz) flux += kf * (av[e] - t0);
-            const double shed = a.films.exposed ? film_flux(a, i + e, j, k, c + e, t0) : 0.0;
+            // only a cell on a face can have a film: film_flux is +0 everywhere else
+            const bool face = i + e == 0 || i + e + 1 == nx || !yl || !yh || k == 0 || k + 1 == nz;
+            const double shed = (a.films.exposed && face) ? film_flux(a, i + e, j, k, c + e, t0) : 0.0;
             nt[e] = t0 + a.dts * a.mobility * (flux - shed);  // add_kelvin, latent <= 0 (solid.rs:1620-1635)
             acc[0] += a.capacity * (nt[e] - a.reference);     // solid.rs:1583-1590
             if (shed != 0.0) acc[1] += a.dts * a.mobility * shed * a.capacity;  // solid.rs:1821-1823
-            if (a.radiating && (i + e == 0 || i + e + 1 == nx || j == 0 || j + 1 == ny || k == 0 || k + 1 == nz))
+            if (a.radiating && face)
                 rate = fmax(rate, heat_cell_rate(a, i + e, j, k, c + e, nt[e]));
         }
         *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);

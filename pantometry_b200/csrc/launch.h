@@ -14,6 +14,7 @@
 #include "room_kernels.cuh"
 #include "ens_tma.cuh"
 #include "yee_near.cuh"
+#include "heat_tma.cuh"
 
 namespace pm {
 
@@ -64,7 +65,7 @@ inline cudaError_t launch_smem(void (*kernel)(P...), dim3 grid, dim3 block, int 
 // Multiprocessor, asked once per kernel and device), so a persistent grid is exactly one full wave.
 enum KernelId : int {
     kHeatPlain = 0, kHeatF32, kHallF64, kHallF32, kYeeHF64, kYeeHF32, kYeeEF64, kYeeEF32, kYeeStepF64, kYeeStepF32,
-    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps, kHeatPlainSteps32, kHeatF32QuadSteps32,
+    kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps, kHeatPlainSteps32, kHeatF32QuadSteps32, kHeatTma,
     kHallTmaShape1, kHallTmaShape2, kHallTmaShape3,  // kHallTma is shape 0
     kYeeTmaShape1, kYeeTmaShape2, kYeeTmaMediaShape1,  // kYeeTma and kYeeTmaMedia are shape 0 of each form
     kKernelCount
@@ -83,6 +84,10 @@ cudaError_t launch_heat_measure_plain(const HeatMeasureArgs& a, cudaStream_t s);
 cudaError_t launch_heat_f32(const HeatF32Args& a, cudaStream_t s);
 // Many FP32 quad-form steps of a small block in one cooperative launch (heat_f32_quad_steps).
 cudaError_t launch_heat_f32_steps(const HeatF32Args& a, const HeatPersist& p, cudaStream_t s);
+// One FP32 step of a uniform block whose rows hold a multiple of 4 cells, staged by TMA
+// (heat_tma_step) from the old deviations `map` describes (heat_tma_map).
+cudaError_t launch_heat_tma(const HeatTmaArgs& a, const CUtensorMap& map, cudaStream_t s);
+bool heat_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz);
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s);
 cudaError_t launch_heat_convert(const double* t, float* d, double t0, size_t n, int to_dev, double* tout,
                                 cudaStream_t s);
