@@ -399,6 +399,14 @@ pm_status pm_cavity_restore(pm_cavity* c);
 pm_status pm_cavity_autotune(pm_cavity* c, int trial_steps, int* planes, int* stages);
 pm_status pm_cavity_set_tile(pm_cavity* c, int planes, int stages);
 pm_status pm_cavity_tile(pm_cavity* c, int* planes, int* stages);
+/* No counterpart in the reference. On the TMA-staged FP32 kernel, when nx is a multiple of 32 and
+ * ny of 8, the tiles cover the first nx columns and ny rows of the node lattice and a wall pass in
+ * the same launch steps the last column (x = nx) and row (y = ny), whose edges are all wall edges:
+ * no tile then runs for one column or row alone. The fields are the same bit for bit either way.
+ * On by default; set_wall_split(c, 0) makes the tiles cover the whole lattice. wall_split reports
+ * whether the present cavity steps split (0 where it does not use that kernel or does not split). */
+pm_status pm_cavity_set_wall_split(pm_cavity* c, int on);
+pm_status pm_cavity_wall_split(pm_cavity* c, int* on);
 pm_status pm_cavity_set_stream(pm_cavity* c, void* stream);
 void pm_cavity_destroy(pm_cavity* c);
 

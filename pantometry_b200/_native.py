@@ -253,6 +253,8 @@ SIGNATURES = {
     "pm_cavity_autotune": (_st, [_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pm_cavity_set_tile": (_st, [_p, C.c_int, C.c_int]),
     "pm_cavity_tile": (_st, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pm_cavity_set_wall_split": (_st, [_p, C.c_int]),
+    "pm_cavity_wall_split": (_st, [_p, C.POINTER(C.c_int)]),
     "pm_cavity_set_stream": (_st, [_p, _p]),
     "pm_cavity_destroy": (None, [_p]),
     # Ensembles

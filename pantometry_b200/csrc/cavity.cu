@@ -62,6 +62,7 @@ struct Cavity : Handle {
     unsigned L = 0;
     YeeMaps maps[2];
     int yshape = 0;  // the TMA kernel's tile shape, an index of the present form's shape list
+    bool wall_split_on = true;  // the TMA kernel's last column and row by its wall pass, where they split off
     // Mur's history (cavity.rs:141): E after the last step's walls. Normally the old buffer of the
     // ping-pong pair; after something rewrote E between steps it is a snapshot taken before that.
     bool has_prev = false;   // a step has run (cavity.rs:1087)
@@ -685,7 +686,11 @@ struct Cavity : Handle {
         YeeStepArgs<float> a = sargs<float>(par, dt);
         const unsigned w = wave_of(yee_tma_kernel_id(!uniform, yshape));
         const int P = yee_tma_shape(!uniform, yshape).planes;
-        const int X = nx + 1, Y = ny + 1, Z = nz + 1;
+        // the wall pass takes the last column and row when the tiles then cover the rest exactly;
+        // a source on one of those edges stays with the tiles, which book its work
+        const bool src_on_wall = a.src_i >= 0 && (a.src_i == nx || a.src_j == ny);
+        a.wall_split = (wall_split_on && nx % 32 == 0 && ny % 8 == 0 && !src_on_wall) ? 1 : 0;
+        const int X = a.wall_split ? nx : nx + 1, Y = a.wall_split ? ny : ny + 1, Z = nz + 1;
         int best = 2 * P - 1;
         double best_score = -1.0;
         for (int mlt : {2, 4, 8, 16}) {
@@ -1200,6 +1205,23 @@ pm_status pm_cavity_tile(pm_cavity* cp, int* planes, int* stages) {
     const YeeTmaShape sh = yee_tma_shape(!c->uniform, c->yshape);
     if (planes) *planes = c->tma ? sh.planes : 0;
     if (stages) *stages = c->tma ? sh.stages : 0;
+    return PM_OK;
+}
+
+pm_status pm_cavity_set_wall_split(pm_cavity* cp, int on) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (c->wall_split_on == (on != 0)) return PM_OK;
+    PM_CUDA(cudaStreamSynchronize(c->stream()));
+    c->wall_split_on = on != 0;
+    c->drop_graphs();
+    return PM_OK;
+}
+
+pm_status pm_cavity_wall_split(pm_cavity* cp, int* on) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    if (on) *on = (c->tma && c->targs(c->parity, c->courant_limit()).wall_split) ? 1 : 0;
     return PM_OK;
 }
 

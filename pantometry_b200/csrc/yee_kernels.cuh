@@ -382,6 +382,9 @@ struct YeeStepArgs {
     // components the kernel's last block steps again in f64 (yee_near_body) once the grid's cells
     // are in; the box's energy terms are left to it, and it closes the books. nb_w = 0: none.
     int nb_x0, nb_y0, nb_z0, nb_w;
+    // FP32 TMA form only: the tiles cover [0, nx) × [0, ny) of the lattice and the last column and
+    // row are stepped by the wall pass (yee_tma_wall_pass). 0: the tiles cover the whole lattice.
+    int wall_split;
 };
 
 // The per-edge and per-face coefficients of one dt for a cavity of mixed media, exactly the values

@@ -163,6 +163,70 @@ struct YeeNearArgs {
 template <bool SOLID>
 __device__ void yee_near_body(const YeeNearArgs& a, const double (&tma)[4]);
 
+// One face of H⁺ (cavity.rs:1346-1379): was − (g/μ)·((a₁ − a₀) − (b₁ − b₀)). The tiles and the
+// wall pass below form every face through this one expression, so the two agree bit for bit.
+__device__ __forceinline__ float yee_face_f32(float was, float ch, float a1, float a0, float b1, float b0) {
+    return was - ch * ((a1 - a0) - (b1 - b0));
+}
+
+// The lattice's last column (i = nx, every j and k) and last row (j = ny, i < nx), when the tiles
+// cover only [0, nx) × [0, ny) (a.wall_split: nx a multiple of 32 and ny of 8, so that no tile is
+// there for one column or row alone). Every edge on these nodes is tangential to the x = nx or
+// y = ny wall, so the step writes 0 to each (cavity.rs:1239-1293; open and magnetic walls are the
+// wall kernel's, after the step), and the one face that moves is hx on x = nx and hy on y = ny.
+// Each value and energy term is the one a tile would have formed there: neighbours beyond the
+// lattice read 0, as the tensor maps' fill does, and a component's absent positions hold the
+// padding's 0. The node is taken from the thread's index, `nthreads` apart.
+template <bool MEDIA>
+__device__ __forceinline__ void yee_tma_wall_pass(const YeeStepArgs<float>& a, unsigned L, long long first,
+                                                  long long nthreads, float& es, float& ms) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const unsigned ny1 = (unsigned)ny + 1;
+    const size_t plane = (size_t)L * ny1;
+    const long long ncol = (long long)(ny + 1) * (nz + 1), nall = ncol + (long long)nx * (nz + 1);
+    const float ch = a.ch, gain0 = a.gain[0];
+    for (long long r = first; r < nall; r += nthreads) {
+        int i, j, k;
+        if (r < ncol) {
+            i = nx;
+            j = (int)(r % (ny + 1));
+            k = (int)(r / (ny + 1));
+        } else {
+            const long long q = r - ncol;
+            i = (int)(q % nx);
+            j = ny;
+            k = (int)(q / nx);
+        }
+        const size_t n = (size_t)i + L * ((size_t)j + (size_t)ny1 * (size_t)k);
+        const bool zin = k < nz;
+        const float hi = (i == 0 || i == nx) ? 0.5f : 1.0f, hj = (j == 0 || j == ny) ? 0.5f : 1.0f,
+                    hk = (k == 0 || k == nz) ? 0.5f : 1.0f;
+        const float ex0 = a.old[0][n], ey0 = a.old[1][n], ez0 = a.old[2][n];
+        if (i == nx) {
+            const float wx = a.old[3][n];
+            const float hxn = yee_face_f32(wx, ch, j < ny ? a.old[2][n + L] : 0.0f, ez0, zin ? a.old[1][n + plane] : 0.0f, ey0);
+            if (j < ny && zin) a.neu[3][n] = hxn;
+            ms += hi * (hxn * wx);
+            if (j < ny) a.neu[1][n] = 0.0f;
+        } else {
+            const float wy = a.old[4][n];
+            const float hyn = yee_face_f32(wy, ch, zin ? a.old[0][n + plane] : 0.0f, ex0, a.old[2][n + 1], ez0);
+            if (zin) a.neu[4][n] = hyn;
+            ms += hj * (hyn * wy);
+            a.neu[0][n] = 0.0f;
+        }
+        if (zin) a.neu[2][n] = 0.0f;
+        if constexpr (MEDIA) {
+            const float gx = i < nx ? a.cgain[0][n] : gain0, gy = j < ny ? a.cgain[1][n] : gain0,
+                        gz = zin ? a.cgain[2][n] : gain0;
+            es += __fdividef((hj * hk) * (ex0 * ex0), gx) + __fdividef((hi * hk) * (ey0 * ey0), gy) +
+                  __fdividef((hi * hj) * (ez0 * ez0), gz);
+        } else {
+            es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+        }
+    }
+}
+
 template <int P, int S, bool SOLID, bool MEDIA, int MINB>
 static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m,
@@ -264,9 +328,9 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
             const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
             const float wx = HX[h][ty + 1][tx], wy = HY[h][ty][tx + 4], wz = HZ[h][ty + 1][tx + 4];
             const float ex0 = EX[h][ty + 1][tx + 4], ey0 = EY[h][ty + 1][tx + 4], ez0 = EZ[h][ty + 1][tx + 4];
-            const float hxn = wx - ch * ((EZ[h][ty + 2][tx + 4] - ez0) - (EY[h + 1][ty + 1][tx + 4] - ey0));
-            const float hyn = wy - ch * ((EX[h + 1][ty + 1][tx + 4] - ex0) - (EZ[h][ty + 1][tx + 5] - ez0));
-            const float hzn = wz - ch * ((EY[h][ty + 1][tx + 5] - ey0) - (EX[h][ty + 2][tx + 4] - ex0));
+            const float hxn = yee_face_f32(wx, ch, EZ[h][ty + 2][tx + 4], ez0, EY[h + 1][ty + 1][tx + 4], ey0);
+            const float hyn = yee_face_f32(wy, ch, EX[h + 1][ty + 1][tx + 4], ex0, EZ[h][ty + 1][tx + 5], ez0);
+            const float hzn = yee_face_f32(wz, ch, EY[h][ty + 1][tx + 5], ey0, EX[h][ty + 2][tx + 4], ex0);
             hq->hx[ty + 1][tx] = hxn;
             hq->hy[ty][tx + 1] = hyn;
             hq->hz[ty + 1][tx + 1] = hzn;
@@ -290,15 +354,15 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
                 // work: the y0 − 1 row of hx (warp 7) and of hz (warp 6), the x0 − 1 column of hz
                 // (warp 5, rows y0 − 1 .. y0 + 7) and of hy (warp 4, rows y0 .. y0 + 7)
                 if (ty == 7) {
-                    hq->hx[0][tx] = HX[h][0][tx] - ch * ((EZ[h][1][tx + 4] - EZ[h][0][tx + 4]) - (EY[h + 1][0][tx + 4] - EY[h][0][tx + 4]));
+                    hq->hx[0][tx] = yee_face_f32(HX[h][0][tx], ch, EZ[h][1][tx + 4], EZ[h][0][tx + 4], EY[h + 1][0][tx + 4], EY[h][0][tx + 4]);
                 } else if (ty == 6) {
-                    hq->hz[0][tx + 1] = HZ[h][0][tx + 4] - ch * ((EY[h][0][tx + 5] - EY[h][0][tx + 4]) - (EX[h][1][tx + 4] - EX[h][0][tx + 4]));
+                    hq->hz[0][tx + 1] = yee_face_f32(HZ[h][0][tx + 4], ch, EY[h][0][tx + 5], EY[h][0][tx + 4], EX[h][1][tx + 4], EX[h][0][tx + 4]);
                 } else if (ty == 5 && tx < 9) {
                     const int r = tx;
-                    hq->hz[r][0] = HZ[h][r][3] - ch * ((EY[h][r][4] - EY[h][r][3]) - (EX[h][r + 1][3] - EX[h][r][3]));
+                    hq->hz[r][0] = yee_face_f32(HZ[h][r][3], ch, EY[h][r][4], EY[h][r][3], EX[h][r + 1][3], EX[h][r][3]);
                 } else if (ty == 4 && tx >= 1 && tx < 9) {
                     const int r = tx;
-                    hq->hy[r - 1][0] = HY[h][r - 1][3] - ch * ((EX[h + 1][r][3] - EX[h][r][3]) - (EZ[h][r][4] - EZ[h][r][3]));
+                    hq->hy[r - 1][0] = yee_face_f32(HY[h][r - 1][3], ch, EX[h + 1][r][3], EX[h][r][3], EZ[h][r][4], EZ[h][r][3]);
                 }
             }
             __syncthreads();
@@ -346,6 +410,12 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
         acc[1] += (double)ms;
         yee_tma_next(cc, T, P);
         ++it;
+    }
+    if (a.wall_split && !timed_out) {
+        float es = 0.0f, ms = 0.0f;
+        yee_tma_wall_pass<MEDIA>(a, L, (long long)blockIdx.x * 256 + tid, (long long)gridDim.x * 256, es, ms);
+        acc[0] += (double)es;
+        acc[1] += (double)ms;
     }
     if (timed_out) {
         // stop every later kernel of the call, and let the copies still in flight land before

@@ -507,6 +507,16 @@ class Cavity(_Domain):
         N.check(self._lib.pm_cavity_tile(self._h, C.byref(pl), C.byref(st)))
         return pl.value, st.value
 
+    def set_wall_split(self, on):
+        """Step the lattice's last column and row by the TMA kernel's wall pass (where nx is a
+        multiple of 32 and ny of 8), or by whole tiles; the fields agree bit for bit."""
+        N.check(self._lib.pm_cavity_set_wall_split(self._h, 1 if on else 0))
+
+    def wall_split(self):
+        on = C.c_int()
+        N.check(self._lib.pm_cavity_wall_split(self._h, C.byref(on)))
+        return bool(on.value)
+
     def courant_limit(self):
         out = C.c_double()
         N.check(self._lib.pm_cavity_courant_limit(self._h, C.byref(out)))

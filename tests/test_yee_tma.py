@@ -285,3 +285,67 @@ def test_yee_autotune_keeps_state_books_and_source_clock():
     fa, fb = a.fields(), b.fields()
     for k in fa:
         assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
+
+
+def _split_runs(make, steps, dt):
+    runs = []
+    for split in (True, False):
+        c = make()
+        c.set_wall_split(split)
+        assert c.step(dt, steps) is None  # a 64-step graph and single launches
+        assert c.wall_split() == split
+        runs.append((c.fields(), c.ledger()))
+    (fa, la), (fb, lb) = runs
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
+    # the books are FP64 sums taken in another order
+    assert abs(la["total"] - lb["total"]) <= 1e-9 * lb["scale"]
+
+
+@pytest.mark.parametrize("media", [False, True], ids=["one-medium", "dielectric"])
+def test_yee_wall_pass_agrees_with_whole_tiles(media):
+    """nx a multiple of 32 and ny of 8: the TMA kernel's wall pass steps the lattice's last column
+    and row, and the fields equal those of tiles over the whole lattice bit for bit, with the
+    dipole's near field in f64."""
+    from pantometry_b200 import workloads as W
+
+    n = 32
+    if media:
+        cfg = W.dielectric_cavities(count=1, n=n, steps=100)
+        make = lambda: W.build_dielectric_cavity(cfg, 0, precision="f32")  # noqa: E731
+    else:
+        cfg = W.yee_cavity(n, steps=100)
+        make = lambda: W.build_cavity(cfg, precision="f32")  # noqa: E731
+    _split_runs(make, 70, cfg["dt"])
+
+
+def test_yee_wall_pass_with_open_and_magnetic_walls_loss_and_obstacles():
+    """A lossy 64×40×20 cavity released in a mode, with an open x wall and a magnetic y wall (which
+    leave the wall edges of the last column and row non-zero) and obstacles: the wall pass and
+    whole tiles agree bit for bit."""
+    from pantometry_b200.domains import Cavity
+
+    counts, dx = (64, 40, 20), 1e-3
+    nx, ny, nz = counts
+    dt = 0.9 * Cavity(counts, dx, precision="f32").courant_limit()
+    solid = np.zeros((nz, ny, nx), dtype=np.uint8)
+    solid[4:9, 30:39, 50:63] = 1
+
+    def make():
+        c = Cavity(counts, dx, sigma=2e-3, precision="f32")
+        c.release_mode((1, 2), 1.0, dt)
+        c.obstruct(solid)
+        c.set_boundary("XHigh", "open")
+        c.set_boundary("YHigh", "magnetic")
+        return c
+
+    _split_runs(make, 70, dt)
+
+
+def test_yee_wall_pass_only_where_the_tiles_fit():
+    from pantometry_b200.domains import Cavity
+
+    assert Cavity((32, 16, 9), 1e-3, precision="f32").wall_split()
+    assert not Cavity((30, 16, 9), 1e-3, precision="f32").wall_split()
+    assert not Cavity((32, 12, 9), 1e-3, precision="f32").wall_split()
+    assert not Cavity((32, 16, 9), 1e-3, precision="f64").wall_split()
