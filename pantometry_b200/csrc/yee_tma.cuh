@@ -304,8 +304,11 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
         const float hi = (i == 0 || i == nx) ? 0.5f : 1.0f, hj = (j == 0 || j == ny) ? 0.5f : 1.0f;
         // the column crosses the f64 near-field box (nb_w = 0: no box, never)
         const bool box_xy = (unsigned)(i - a.nb_x0) < (unsigned)a.nb_w && (unsigned)(j - a.nb_y0) < (unsigned)a.nb_w;
-        float es = 0.0f, ms = 0.0f;  // this stage's w|E|² and w H⁺·H⁻ of the thread's cells
-#pragma unroll 1
+        // this stage's energy products of the thread's cells per component, the z weight in each:
+        // Σ hk ex², Σ hk ey², Σ ez² (with MEDIA each over its gain), Σ hx⁺hx⁻, Σ hy⁺hy⁻, Σ hk hz⁺hz⁻;
+        // the x and y weights are applied once a stage
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
         for (int h = 0; h < P; ++h) {
             const int k = cc.kb + h;
             if (k >= cc.k1) break;
@@ -343,12 +346,18 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
                 // (padding, or the fill outside the lattice) is exactly zero, so its E term and
                 // its H⁻·H⁺ term are zero.
                 if (!inbox) {
-                    ms += hi * (hxn * wx) + hj * (hyn * wy) + hk * (hzn * wz);
-                    if constexpr (MEDIA)  // 1/g to within 2 ulp: the terms are f32 roundings already
-                        es += __fdividef((hj * hk) * (ex0 * ex0), gx) + __fdividef((hi * hk) * (ey0 * ey0), gy) +
-                              __fdividef((hi * hj) * (ez0 * ez0), gz);
-                    else
-                        es += (hj * hk) * (ex0 * ex0) + (hi * hk) * (ey0 * ey0) + (hi * hj) * (ez0 * ez0);
+                    mx = fmaf(hxn, wx, mx);
+                    my = fmaf(hyn, wy, my);
+                    mz = fmaf(hk * hzn, wz, mz);
+                    if constexpr (MEDIA) {  // 1/g to within 2 ulp: the terms are f32 roundings already
+                        sx += __fdividef((hk * ex0) * ex0, gx);
+                        sy += __fdividef((hk * ey0) * ey0, gy);
+                        sz += __fdividef(ez0 * ez0, gz);
+                    } else {
+                        sx = fmaf(hk * ex0, ex0, sx);
+                        sy = fmaf(hk * ey0, ey0, sy);
+                        sz = fmaf(ez0, ez0, sz);
+                    }
                 }
                 // halo faces, one line per warp so the barrier waits on no warp doing twice the
                 // work: the y0 − 1 row of hx (warp 7) and of hz (warp 6), the x0 − 1 column of hz
@@ -370,8 +379,8 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
             // conducting walls 0 (cavity.rs:1239-1293), edges touching a solid cell 0 (cavity.rs:304-331)
             if (compute) {
                 const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
-                const float cex = (hq->hz[ty + 1][tx + 1] - hq->hz[ty][tx + 1]) - (hyn - hy_below);
-                const float cey = (hxn - hx_below) - (hq->hz[ty + 1][tx + 1] - hq->hz[ty + 1][tx]);
+                const float cex = (hzn - hq->hz[ty][tx + 1]) - (hyn - hy_below);  // own H⁺ from registers
+                const float cey = (hxn - hx_below) - (hzn - hq->hz[ty + 1][tx]);
                 const float cez = (hyn - hq->hy[ty][tx]) - (hxn - hq->hx[ty][tx]);
                 float vx = dec0 * ex0 + gx * cex;
                 float vy = dec0 * ey0 + gy * cey;
@@ -406,8 +415,8 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
             hy_below = hyn;
             hpar ^= 1;
         }
-        acc[0] += (double)es;
-        acc[1] += (double)ms;
+        acc[0] += (double)(hj * sx + hi * sy + (hi * hj) * sz);
+        acc[1] += (double)(hi * mx + hj * my + mz);
         yee_tma_next(cc, T, P);
         ++it;
     }

@@ -287,7 +287,7 @@ def test_yee_autotune_keeps_state_books_and_source_clock():
         assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
 
 
-def _split_runs(make, steps, dt):
+def _split_runs(make, steps, dt, books=1e-9):
     runs = []
     for split in (True, False):
         c = make()
@@ -298,8 +298,8 @@ def _split_runs(make, steps, dt):
     (fa, la), (fb, lb) = runs
     for k in fa:
         assert np.array_equal(fa[k].view(np.uint64), fb[k].view(np.uint64)), k
-    # the books are FP64 sums taken in another order
-    assert abs(la["total"] - lb["total"]) <= 1e-9 * lb["scale"]
+    # the books: f32 stage sums of the same terms grouped another way, then FP64
+    assert abs(la["total"] - lb["total"]) <= books * lb["scale"]
 
 
 @pytest.mark.parametrize("media", [False, True], ids=["one-medium", "dielectric"])
@@ -339,7 +339,9 @@ def test_yee_wall_pass_with_open_and_magnetic_walls_loss_and_obstacles():
         c.set_boundary("YHigh", "magnetic")
         return c
 
-    _split_runs(make, 70, dt)
+    # this cavity's FP32 books hold about 1e-7 of the f64 run's; the two groupings of the f32
+    # stage sums differ by a few 1e-9
+    _split_runs(make, 70, dt, books=2e-8)
 
 
 def test_yee_wall_pass_only_where_the_tiles_fit():
