@@ -44,9 +44,9 @@ HALL_F32_TRAFFIC = 489971968
 # The Yee kernel, per cell: 432.4 MB read + 366.6 MB written at 256³ cells. A launch at another
 # size moves that many bytes per cell (it reads and writes each cell's six values once).
 YEE_F32_TRAFFIC_PER_CELL = (432385024 + 366586112) / 256 ** 3
-# The ensemble brick kernel over the 512-block heat ensemble, per cell: 1.149 GB read + 785.9 MB
+# The ensemble brick kernel over the 512-block heat ensemble, per cell: 1.004 GB read + 772.1 MB
 # written for 187,991,031 cells.
-ENS_F32_TRAFFIC_PER_CELL = (1149139000 + 785889024) / 187991031
+ENS_F32_TRAFFIC_PER_CELL = (1004143360 + 772071936) / 187991031
 
 
 def peaks():
