@@ -27,14 +27,18 @@
 
 namespace pm {
 
+// Planes per stage, stages in the ring, blocks per SM. Measured on B200 over the 512-grid ensemble:
+// 16 × 2 at three blocks per SM 405 Gcell/s, 16 × 3 at two 398, 8 × 3 at four 371-378, 12 × 4 at
+// two 378, 24 × 2 at two 379, 32 × 2 at two 328, 4 × 6 at three 307. A deeper stage reads its
+// two halo planes over more planes of its own.
 #ifndef PM_ENS_TMA_PLANES
-#define PM_ENS_TMA_PLANES 8
+#define PM_ENS_TMA_PLANES 16
 #endif
 #ifndef PM_ENS_TMA_STAGES
-#define PM_ENS_TMA_STAGES 3
+#define PM_ENS_TMA_STAGES 2
 #endif
 #ifndef PM_ENS_TMA_MIN_BLOCKS
-#define PM_ENS_TMA_MIN_BLOCKS 4
+#define PM_ENS_TMA_MIN_BLOCKS 3
 #endif
 constexpr int kEnsTmaPlanes = PM_ENS_TMA_PLANES;
 constexpr int kEnsTmaStages = PM_ENS_TMA_STAGES;
@@ -116,16 +120,20 @@ __device__ __forceinline__ void tma_stage_row(const EnsTmaStage<P>& s, const Ens
             below = here;
             here = above;
         }
-    } else if (yl && yh) {
+    } else if (yl && yh && nx > 1) {
         // a stage of a row inside the block in y (a brick on an x face, a stage holding a
-        // z face, or a partial stage): the general form's sums and films term for term,
-        // the x faces' taken by select per lane and the z faces' per plane, so the stage
-        // stays one straight run of planes. Adding +0 for an absent neighbour is adding
-        // nothing, since a sum that starts at +0 is never −0 here.
+        // z face, or a partial stage): the general form's sums and films term for term, so
+        // the stage stays one straight run of planes. Adding +0 for an absent neighbour is
+        // adding nothing, since a sum that starts at +0 is never −0 here. An absent x
+        // neighbour is read at the cell itself, so its term is here − here = +0 with no
+        // select; a lane lies on one x face at most (the block is two cells wide or more),
+        // and its film b·(here + off) + 0 takes that face's coefficients, or 0 · (here + 0)
+        // + 0 = +0 off the faces.
         const int exposed = m.exposed;
         const bool fx0 = ((exposed >> 0) & 1) && !xl, fx1 = ((exposed >> 1) & 1) && !xh;
         const bool fz0 = ((exposed >> 4) & 1) && kb == 0, fz1 = (exposed >> 5) & 1;
-        const float b0 = m.b[0], o0 = m.off[0], b1 = m.b[1], o1 = m.off[1];
+        const float bx = fx0 ? m.b[0] : fx1 ? m.b[1] : 0.0f, ox = fx0 ? m.off[0] : fx1 ? m.off[1] : 0.0f;
+        const int xmi = xl ? tx + 3 : tx + 4, xpi = xh ? tx + 5 : tx + 4;
         const int zlast = nz - 1 - kb;  // the stage's plane on the z+ face, if below hn
         double col_shed = 0.0;
         float below = s.t[0][ty + 1][tx + 4], here = s.t[1][ty + 1][tx + 4];
@@ -134,20 +142,16 @@ __device__ __forceinline__ void tma_stage_row(const EnsTmaStage<P>& s, const Ens
             if (h >= hn) break;
             const bool zl = h > 0 || kb > 0, zh = h < zlast;
             const float above = s.t[h + 2][ty + 1][tx + 4];
-            const float xm = s.t[h + 1][ty + 1][tx + 3], xp = s.t[h + 1][ty + 1][tx + 5];
+            const float xm = s.t[h + 1][ty + 1][xmi], xp = s.t[h + 1][ty + 1][xpi];
             const float ym = s.t[h + 1][ty][tx + 4], yp = s.t[h + 1][ty + 2][tx + 4];
             float sum = 0.0f;
-            sum += xl ? xm - here : 0.0f;
-            sum += xh ? xp - here : 0.0f;
+            sum += xm - here;
+            sum += xp - here;
             sum += ym - here;
             sum += yp - here;
             sum += zl ? below - here : 0.0f;
             sum += zh ? above - here : 0.0f;
-            float shed = 0.0f;
-            const float v0 = __fmaf_rn(b0, here + o0, shed);
-            shed = fx0 ? v0 : shed;
-            const float v1 = __fmaf_rn(b1, here + o1, shed);
-            shed = fx1 ? v1 : shed;
+            float shed = __fmaf_rn(bx, here + ox, 0.0f);
             if (h == 0 && fz0) shed = __fmaf_rn(m.b[4], here + m.off[4], shed);
             if (fz1 && !zh) shed = __fmaf_rn(m.b[5], here + m.off[5], shed);
             if (exposed) col_shed += (double)shed;
