@@ -559,8 +559,10 @@ def run_heat(args):
 
     b64, dt, ms64, clk = timed("f64", args.steps, args.warmup, 1e-9)
     field64, led64 = b64.cells, b64.ledger()
+    kernel64, launches64 = b64.step_kernel(T)  # what each bench step ran, as the library reports it
     del b64
     b32, _, ms32, _ = timed("f32", args.steps, args.warmup, 1e-6)
+    kernel32, launches32 = b32.step_kernel(T)
     del b32
     # FP32 against f64 after the same steps from the same start
     a32, _, _, _ = timed("f32", 0, args.warmup + args.steps, 1e-6)
@@ -597,7 +599,6 @@ def run_heat(args):
     peak, peak_kind = peaks()
     value = world * cells * T * args.steps / (ms64 * 1e-3) / 1e9
     fp32 = world * cells * T * args.steps / (ms32 * 1e-3) / 1e9
-    quads = n % 4 == 0
     line = {
         "metric": HEAT_METRIC.replace("64^3", f"{n}^3"), "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms64 / args.steps, 3),
@@ -610,15 +611,15 @@ def run_heat(args):
                          "outside the timed events"},
         "e2e": {"value": round(world * cells * T * args.steps / (e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
                 "h2d_bytes_per_step": 8 * cells, "d2h_bytes_per_step": 64},
-        "gpu_launches": args.steps * T,
+        "gpu_launches": args.steps * launches64,
         "roofline": {"bound": "hbm", "achieved": round(16 * cells * T * args.steps / (ms64 * 1e-3) / 1e9, 1),
                      "peak": peak, "unit": "GB/s",
                      "frac": round(16 * cells * T * args.steps / (ms64 * 1e-3) / 1e9 / peak, 4), "traffic": None,
-                     "kernel": "heat_plain_step (f64)", "bytes_per_launch": 16 * cells,
+                     "kernel": f"{kernel64} (f64)", "bytes_per_step": 16 * cells,
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "note": "L2-resident within a bench step at 64^3" if 16 * cells < 126e6 else "state larger than L2"},
         "fp32": {"value": round(fp32, 3), "unit": UNIT, "ms_per_step": round(ms32 / args.steps, 3),
-                 "kernel": "heat_f32_quad_step (four cells per thread)" if quads else "heat_f32_step",
+                 "kernel": kernel32, "gpu_launches": args.steps * launches32,
                  "roofline_frac": round(8 * cells * T * args.steps / (ms32 * 1e-3) / 1e9 / peak, 4),
                  "fp32_over_f64": round(fp32 / value, 3)},
         "error_vs_f64": {"max_abs_kelvin": field_err, "ledger_rel": ledger_err,

@@ -150,6 +150,11 @@ pm_status pm_heat_absorb(pm_heat* h, double joules);
 /* Domain::checkpoint / restore (solid.rs:1935-1950). */
 pm_status pm_heat_checkpoint(pm_heat* h);
 pm_status pm_heat_restore(pm_heat* h);
+/* No counterpart in the reference. The kernel a call of pm_heat_step for `nsteps` steps would run
+ * on the present block (its name, at most cap - 1 bytes and a terminating 0, into `name`) and how
+ * many launches of it the call makes: one a step, or one per 1024 steps for the many-step
+ * cooperative kernels of small uniform blocks. Nothing runs. */
+pm_status pm_heat_step_kernel(pm_heat* h, long long nsteps, char* name, int cap, long long* launches);
 /* Cells of a row per thread (no reference counterpart: a launch shape, like the ensemble's brick
  * shape). The default is the precision's wide form where the block is one material and its rows
  * allow: 2 adjacent cells per thread in the plain f64 form (rows of an even number of cells), 4 in

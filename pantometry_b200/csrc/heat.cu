@@ -480,6 +480,7 @@ struct Heat : Handle {
     }
 
     bool tma_form() const { return precision == PM_FIELDS_F32 && uniform && wide && nx % 4 == 0 && tma_maps; }
+
     HeatTmaArgs tma_args(int par, double dt) const {
         const HeatF32Args f = f32_args(par, dt);
         HeatTmaArgs a{};
@@ -638,6 +639,7 @@ pm_status pm_heat_create(const pm_heat_desc* d, pm_heat** out) {
     if (h->precision == PM_FIELDS_F32 && h->nx % 4 == 0 && (size_t)h->nx * h->ny * h->nz < (size_t(1) << 31))
         h->tma_maps = heat_tma_map(&h->tmaps[0], h->field[0].p, h->nx, h->ny, h->nz) &&
                       heat_tma_map(&h->tmaps[1], h->field[1].p, h->nx, h->ny, h->nz);
+
     // Solid3D::new starts every cell at `initial`.
     std::vector<double> t(h->n(), d->initial_kelvin);
     *out = reinterpret_cast<pm_heat*>(h);
@@ -918,6 +920,32 @@ pm_status pm_heat_restore(pm_heat* hp) {
     s = h->write_state();
     if (s != PM_OK) return s;
     return h->measure();
+}
+
+pm_status pm_heat_step_kernel(pm_heat* hp, long long nsteps, char* name, int cap, long long* launches) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    if (!name || cap < 1) return fail(PM_BAD_ARG, "step_kernel: a name buffer of one byte or more");
+    const bool plain = h->precision == PM_PLAIN_F64;
+    const bool filled = !h->uniform;
+    std::string k;
+    long long n = nsteps > 0 ? nsteps : 0;  // one launch a step, replayed from a graph or not
+    if (nsteps < 1) {
+        k = "none";
+    } else if (h->persistent(nsteps)) {
+        k = plain ? "heat_plain_pair_steps (cooperative, many steps a launch)"
+                  : "heat_f32_quad_steps (cooperative, many steps a launch)";
+        n = (nsteps + Heat::kPersistChunk - 1) / Heat::kPersistChunk;
+    } else if (plain) {
+        k = (!filled && h->nx % 2 == 0 && h->wide) ? "heat_plain_pair_step" : "heat_plain_step";
+    } else if (h->tma_form()) {
+        k = "heat_tma_step (TMA-staged)";
+    } else {
+        k = filled ? "heat_f32_step<filled>" : (h->nx % 4 == 0 && h->wide) ? "heat_f32_quad_step" : "heat_f32_step";
+    }
+    std::snprintf(name, (size_t)cap, "%s", k.c_str());
+    if (launches) *launches = n;
+    return PM_OK;
 }
 
 pm_status pm_heat_set_cells_per_thread(pm_heat* hp, int cells) {

@@ -126,6 +126,13 @@ class Solid3D(_Domain):
         wait that is not already over give up at once (the call returns PM_DEVICE_TIMEOUT)."""
         N.check(self._lib.pm_heat_set_wait_budget(self._h, int(polls)))
 
+    def step_kernel(self, nsteps):
+        """The kernel a step call of `nsteps` steps would run on this block, and its launches."""
+        buf = C.create_string_buffer(96)
+        n = C.c_longlong()
+        N.check(self._lib.pm_heat_step_kernel(self._h, int(nsteps), buf, 96, C.byref(n)))
+        return buf.value.decode(), n.value
+
     def set_cells_per_thread(self, cells):
         """Cells of a row per thread: 1, or the precision's wide form (the default where the block
         is one material and its rows allow): 2 for plain f64, 4 for FP32. The fields agree bit for

@@ -67,3 +67,21 @@ def test_cells_per_thread_is_one_or_the_width():
         g.set_cells_per_thread(4)
     g.set_cells_per_thread(1)
     g.set_cells_per_thread(2)
+
+
+def test_step_kernel_names_each_form():
+    """pm_heat_step_kernel names the kernel a call would run and its launches, running nothing."""
+    from helpers import dirichlet_films
+
+    counts, dx = (64, 20, 17), 1e-3
+    _, g = heat_pair(counts, dx, ALUMINIUM, 300.0, dirichlet_films(counts, dx, 300.0))
+    assert g.step_kernel(1) == ("heat_plain_pair_step", 1)
+    name, launches = g.step_kernel(2500)  # a small block: many steps a cooperative launch
+    assert name.startswith("heat_plain_pair_steps") and launches == 3
+    g.set_cells_per_thread(1)
+    assert g.step_kernel(1) == ("heat_plain_step", 1)
+    _, h = heat_pair((63, 20, 17), dx, ALUMINIUM, 300.0)
+    assert h.step_kernel(5) == ("heat_plain_step", 5)  # odd rows: one cell per thread
+    _, f = heat_pair(counts, dx, ALUMINIUM, 300.0, precision="f32")
+    assert f.step_kernel(1) == ("heat_tma_step (TMA-staged)", 1)
+    assert f.step_kernel(0) == ("none", 0)
