@@ -41,9 +41,10 @@ BYTES_F64 = 64
 # kernel measured it (ncu cannot run inside the timed process; the capture's command is the bench's
 # own, on one GPU). The hall kernel at 256³: 270.4 MB read + 219.5 MB written.
 HALL_F32_TRAFFIC = 489971968
-# The Yee kernel, per cell: 432.4 MB read + 366.6 MB written at 256³ cells. A launch at another
-# size moves that many bytes per cell (it reads and writes each cell's six values once).
-YEE_F32_TRAFFIC_PER_CELL = (432385024 + 366586112) / 256 ** 3
+# The Yee kernel, per cell: 463.1 MB read + 385.7 MB written at 256³ cells. A launch at another
+# size moves about that many bytes per cell (it reads and writes each cell's six values once; the
+# wall column and row are a smaller share of a larger cavity).
+YEE_F32_TRAFFIC_PER_CELL = (463146240 + 385735424) / 256 ** 3
 # The ensemble brick kernel over the 512-block heat ensemble, per cell: 1.004 GB read + 772.1 MB
 # written for 187,991,031 cells.
 ENS_F32_TRAFFIC_PER_CELL = (1004143360 + 772071936) / 187991031
