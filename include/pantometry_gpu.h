@@ -156,10 +156,10 @@ pm_status pm_heat_restore(pm_heat* h);
  * cooperative kernels of small uniform blocks. Nothing runs. */
 pm_status pm_heat_step_kernel(pm_heat* h, long long nsteps, char* name, int cap, long long* launches);
 /* Cells of a row per thread (no reference counterpart: a launch shape, like the ensemble's brick
- * shape). The default is the precision's wide form where the block is one material and its rows
- * allow: 2 adjacent cells per thread in the plain f64 form (rows of an even number of cells), 4 in
- * the FP32 form (rows of a multiple of 4). 1 takes one cell per thread; the other accepted value
- * is the precision's width (2 or 4). The fields are the same bit for bit either way. */
+ * shape). The default is the precision's widest form where the block is one material and its rows
+ * allow: in plain f64, 4 adjacent cells per thread on rows of a multiple of 4 cells, else 2 on rows
+ * of an even number; in FP32, 4 on rows of a multiple of 4. 1 takes one cell per thread; plain f64
+ * also takes 2 or 4, FP32 4. The fields are the same bit for bit either way. */
 pm_status pm_heat_set_cells_per_thread(pm_heat* h, int cells);
 /* Run subsequent work on `stream` (a cudaStream_t); NULL restores the handle's own stream. */
 /* No counterpart in the reference. Small uniform blocks (up to 2^22 cells, rows of an even number of

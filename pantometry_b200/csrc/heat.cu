@@ -59,6 +59,7 @@ struct Heat : Handle {
     // in the plain form (heat_plain_pair_step, even rows), four in the FP32 form
     // (heat_f32_quad_step, rows of a multiple of 4); false: one cell per thread throughout
     bool wide = true;
+    bool quads64 = true;  // plain f64, rows of a multiple of 4: four cells a thread (else two)
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
     // the TMA-staged FP32 form of a uniform block whose rows hold a multiple of 4 cells: the tensor
@@ -467,11 +468,12 @@ struct Heat : Handle {
                                                               films.share[f], dx);
             }
         }
-        a.pairs = uniform && nx % 2 == 0 && wide ? 1 : 0;
+        a.quads = uniform && nx % 4 == 0 && wide && quads64 ? 1 : 0;
+        a.pairs = !a.quads && uniform && nx % 2 == 0 && wide ? 1 : 0;
         a.radiating = state_dependent() ? 1 : 0;
         a.static_rate = worst_rate;
-        const unsigned w = wave_of(a.pairs ? kHeatPlainPair : kHeatPlain);
-        const int tx = a.pairs ? nx / 2 : nx;  // the threads along a row
+        const unsigned w = wave_of(a.quads ? kHeatPlainQuad : a.pairs ? kHeatPlainPair : kHeatPlain);
+        const int tx = a.quads ? nx / 4 : a.pairs ? nx / 2 : nx;  // the threads along a row
         a.tiles = make_tiles(tx, ny, nz, choose_zc(tx, ny, nz, w));
         a.nblocks = grid_for(a.tiles, w);
         a.st = state.as<DevState>();
@@ -937,7 +939,9 @@ pm_status pm_heat_step_kernel(pm_heat* hp, long long nsteps, char* name, int cap
                   : "heat_f32_quad_steps (cooperative, many steps a launch)";
         n = (nsteps + Heat::kPersistChunk - 1) / Heat::kPersistChunk;
     } else if (plain) {
-        k = (!filled && h->nx % 2 == 0 && h->wide) ? "heat_plain_pair_step" : "heat_plain_step";
+        k = (!filled && h->nx % 4 == 0 && h->wide && h->quads64) ? "heat_plain_quad_step"
+            : (!filled && h->nx % 2 == 0 && h->wide)               ? "heat_plain_pair_step"
+                                                                    : "heat_plain_step";
     } else if (h->tma_form()) {
         k = "heat_tma_step (TMA-staged)";
     } else {
@@ -951,13 +955,15 @@ pm_status pm_heat_step_kernel(pm_heat* hp, long long nsteps, char* name, int cap
 pm_status pm_heat_set_cells_per_thread(pm_heat* hp, int cells) {
     Heat* h = reinterpret_cast<Heat*>(hp);
     HEAT_GUARD(h);
-    const int width = h->precision == PM_PLAIN_F64 ? 2 : 4;
-    if (cells != 1 && cells != width)
-        return fail(PM_BAD_ARG, width == 2 ? "cells per thread (plain f64): 1 or 2" : "cells per thread (FP32): 1 or 4");
-    if ((cells != 1) != h->wide) {
+    const bool plain = h->precision == PM_PLAIN_F64;
+    if (plain ? (cells != 1 && cells != 2 && cells != 4) : (cells != 1 && cells != 4))
+        return fail(PM_BAD_ARG, plain ? "cells per thread (plain f64): 1, 2 or 4" : "cells per thread (FP32): 1 or 4");
+    const bool wide = cells != 1, quads64 = plain ? cells == 4 : h->quads64;
+    if (wide != h->wide || quads64 != h->quads64) {
         PM_CUDA(cudaStreamSynchronize(h->stream()));
         h->drop_graphs();  // the captured launches hold the old tiling
-        h->wide = cells != 1;
+        h->wide = wide;
+        h->quads64 = quads64;
     }
     return PM_OK;
 }

@@ -96,6 +96,7 @@ struct HeatPlainArgs {
     double dts, dx, reference;
     HeatFilms films;
     int pairs;  // uniform blocks with rows of an even number of cells: heat_plain_pair_step
+    int quads;  // rows of a multiple of 4 cells, four a thread: heat_plain_quad_step (pairs is 0)
     // Radiating films (some exposed cell with emissivity > 0) or radiative gaps: the step limit
     // depends on the state, so each step checks dt against the rate its own state gives
     // (solid.rs:1718-1738) and gathers the rate of the state it leaves. static_rate: `worst_rate`
@@ -407,40 +408,49 @@ __device__ __forceinline__ double heat_ld(const double* p) {
     else return *p;
 }
 
-// One tile of the pair form for one step, from `told` into `tnew`: the arithmetic both the one-step
-// kernel and the persistent many-step kernel run, so they agree bit for bit.
-template <bool CG>
+// One tile of the wide form for one step, from `told` into `tnew`: W adjacent cells of a row per
+// thread (W = 2, the pair form, or 4), the arithmetic the one-step kernels and the persistent
+// many-step kernel run, so they agree bit for bit. Each row of W cells comes in 16-byte loads.
+template <bool CG, int W = 2>
 __device__ __forceinline__ void heat_pair_tile(const HeatPlainArgs& a, long long t, const double* told, double* tnew,
                                                double (&acc)[2], double& rate) {
+    static_assert(W == 2 || W == 4, "two or four cells of a row per thread");
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
-    const double2 zero = make_double2(0.0, 0.0);
     const double kf = a.kface;
     int q, j, k0, k1;
-    tile_column(a.tiles, t, q, j, k0, k1);  // q: the pair's place along the row
-    const int i = 2 * q;
+    tile_column(a.tiles, t, q, j, k0, k1);  // q: the group's place along the row
+    const int i = W * q;
     if (i >= nx || j >= ny) return;
     const size_t c0 = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k0);
     const double* p = told + c0;
     double* o = tnew + c0;
-    const bool xl = i > 0, xh = i + 2 < nx, yl = j > 0, yh = j + 1 < ny;
-    double2 below = k0 > 0 ? heat_ld2<CG>(p - plane) : zero;
-    double2 here = heat_ld2<CG>(p);
+    const bool xl = i > 0, xh = i + W < nx, yl = j > 0, yh = j + 1 < ny;
+    auto row = [&](double (&v)[W], const double* at, bool present) {
+#pragma unroll
+        for (int w = 0; w < W / 2; ++w) {
+            const double2 d = present ? heat_ld2<CG>(at + 2 * w) : make_double2(0.0, 0.0);
+            v[2 * w] = d.x;
+            v[2 * w + 1] = d.y;
+        }
+    };
+    double bv[W], hv[W];
+    row(bv, p - plane, k0 > 0);
+    row(hv, p, true);
     size_t c = c0;
     for (int k = k0; k < k1; ++k, p += plane, o += plane, c += plane) {
-        const double2 above = k + 1 < nz ? heat_ld2<CG>(p + plane) : zero;
-        const double2 ym = yl ? heat_ld2<CG>(p - nx) : zero;
-        const double2 yp = yh ? heat_ld2<CG>(p + nx) : zero;
-        const double xm = xl ? heat_ld<CG>(p - 1) : 0.0, xp = xh ? heat_ld<CG>(p + 2) : 0.0;
-        const double hv[2] = {here.x, here.y}, bv[2] = {below.x, below.y}, av[2] = {above.x, above.y};
-        const double mv[2] = {ym.x, ym.y}, pv[2] = {yp.x, yp.y};
-        double nt[2];
+        double av[W], mv[W], pv[W];
+        row(av, p + plane, k + 1 < nz);
+        row(mv, p - nx, yl);
+        row(pv, p + nx, yh);
+        const double xm = xl ? heat_ld<CG>(p - 1) : 0.0, xp = xh ? heat_ld<CG>(p + W) : 0.0;
+        double nt[W];
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
+        for (int e = 0; e < W; ++e) {
             const double t0 = hv[e];
             double flux = 0.0;
-            if (e > 0 || xl) flux += kf * ((e == 0 ? xm : hv[0]) - t0);
-            if (e < 1 || xh) flux += kf * ((e == 1 ? xp : hv[1]) - t0);
+            if (e > 0 || xl) flux += kf * ((e == 0 ? xm : hv[e > 0 ? e - 1 : 0]) - t0);
+            if (e < W - 1 || xh) flux += kf * ((e == W - 1 ? xp : hv[e + 1 < W ? e + 1 : W - 1]) - t0);
             if (yl) flux += kf * (mv[e] - t0);
             if (yh) flux += kf * (pv[e] - t0);
             if (k > 0) flux += kf * (bv[e] - t0);
@@ -454,9 +464,13 @@ __device__ __forceinline__ void heat_pair_tile(const HeatPlainArgs& a, long long
             if (a.radiating && face)
                 rate = fmax(rate, heat_cell_rate(a, i + e, j, k, c + e, nt[e]));
         }
-        *reinterpret_cast<double2*>(o) = make_double2(nt[0], nt[1]);
-        below = here;
-        here = above;
+#pragma unroll
+        for (int w = 0; w < W / 2; ++w) reinterpret_cast<double2*>(o)[w] = make_double2(nt[2 * w], nt[2 * w + 1]);
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+            bv[e] = hv[e];
+            hv[e] = av[e];
+        }
     }
 }
 
@@ -465,6 +479,23 @@ static __global__ void __launch_bounds__(256, PM_HEAT_PAIR_MIN_BLOCKS) heat_plai
     double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
     double rate = -1.0;  // a state-dependent limit: the largest rate of the new state
     for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x) heat_pair_tile<false>(a, t, a.told, a.tnew, acc, rate);
+    if (a.radiating) heat_rate_publish(a, rate);
+    heat_plain_books(a, acc);
+}
+
+// Four cells of a row per thread (rows of a multiple of 4 cells): four independent FP64 chains a
+// thread, where the reference's sequential flux sum makes each cell one chain. Measured on a 256³
+// block: 170 Gcell/s at two blocks of 256 per SM (no bound on registers), 159 at three (80
+// registers, a few bytes spilled), against the pair form's 161.
+#ifndef PM_HEAT_QUAD64_MIN_BLOCKS
+#define PM_HEAT_QUAD64_MIN_BLOCKS 2
+#endif
+static __global__ void __launch_bounds__(256, PM_HEAT_QUAD64_MIN_BLOCKS) heat_plain_quad_step(HeatPlainArgs a) {
+    if (a.st->violated || heat_refused(a)) return;
+    double acc[2] = {0.0, 0.0};  // stored heat of the new state, heat shed this step
+    double rate = -1.0;  // a state-dependent limit: the largest rate of the new state
+    for (long long t = blockIdx.x; t < a.tiles.ntiles; t += gridDim.x)
+        heat_pair_tile<false, 4>(a, t, a.told, a.tnew, acc, rate);
     if (a.radiating) heat_rate_publish(a, rate);
     heat_plain_books(a, acc);
 }

@@ -68,6 +68,7 @@ enum KernelId : int {
     kEnsF64, kEnsF32, kHallTma, kYeeTma, kYeeTmaMedia, kEnsTma, kRoomF64, kRoomF32, kTubeF64, kTubeF32, kBarF64, kBarF32, kHeatF32Quad, kEnsF32Quad, kHeatPlainPair, kEnsF64Pair, kHeatPlainSteps, kHeatF32QuadSteps, kHeatPlainSteps32, kHeatF32QuadSteps32, kHeatTma,
     kHallTmaShape1, kHallTmaShape2, kHallTmaShape3,  // kHallTma is shape 0
     kYeeTmaShape1, kYeeTmaShape2, kYeeTmaMediaShape1,  // kYeeTma and kYeeTmaMedia are shape 0 of each form
+    kHeatPlainQuad,
     kKernelCount
 };
 int blocks_per_sm(KernelId id);

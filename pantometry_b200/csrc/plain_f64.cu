@@ -7,7 +7,8 @@
 namespace pm {
 
 cudaError_t launch_heat_plain(const HeatPlainArgs& a, cudaStream_t s) {
-    if (a.pairs) heat_plain_pair_step<<<a.nblocks, tile_block(), 0, s>>>(a);
+    if (a.quads) heat_plain_quad_step<<<a.nblocks, tile_block(), 0, s>>>(a);
+    else if (a.pairs) heat_plain_pair_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     else heat_plain_step<<<a.nblocks, tile_block(), 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -145,6 +146,7 @@ int occupancy_f64(KernelId id) {
     switch (id) {
         case kHeatPlain: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_step, 256, 0); break;
         case kHeatPlainPair: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_step, 256, 0); break;
+        case kHeatPlainQuad: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_quad_step, 256, 0); break;
         case kHeatPlainSteps: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_steps<8>, 256, 0); break;
         case kHeatPlainSteps32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, heat_plain_pair_steps<32>, 1024, 0); break;
         case kHallF64:

@@ -134,9 +134,9 @@ class Solid3D(_Domain):
         return buf.value.decode(), n.value
 
     def set_cells_per_thread(self, cells):
-        """Cells of a row per thread: 1, or the precision's wide form (the default where the block
-        is one material and its rows allow): 2 for plain f64, 4 for FP32. The fields agree bit for
-        bit."""
+        """Cells of a row per thread: 1, or a wide form (the default where the block is one material
+        and its rows allow): 2 or 4 for plain f64 (4 by default on rows of a multiple of 4), 4 for
+        FP32. The fields agree bit for bit."""
         N.check(self._lib.pm_heat_set_cells_per_thread(self._h, int(cells)))
 
     def fill(self, mask, density, conductivity, specific_heat, emissivity=0.0, thermal=True):

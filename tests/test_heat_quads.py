@@ -56,7 +56,7 @@ def test_wide_and_single_cells_agree(counts, kind, precision):
         assert np.abs(wide - o.cells).max() < 1e-4  # kelvin, on a 30 K spread
 
 
-def test_cells_per_thread_is_one_or_the_width():
+def test_cells_per_thread_is_one_or_a_width_of_the_form():
     _, g = heat_pair((8, 4, 4), 1e-3, ALUMINIUM, 300.0, precision="f32")
     with pytest.raises(Exception):
         g.set_cells_per_thread(2)
@@ -64,9 +64,10 @@ def test_cells_per_thread_is_one_or_the_width():
     g.set_cells_per_thread(4)
     _, g = heat_pair((8, 4, 4), 1e-3, ALUMINIUM, 300.0, precision="f64")
     with pytest.raises(Exception):
-        g.set_cells_per_thread(4)
+        g.set_cells_per_thread(3)
     g.set_cells_per_thread(1)
     g.set_cells_per_thread(2)
+    g.set_cells_per_thread(4)
 
 
 def test_step_kernel_names_each_form():
@@ -75,9 +76,11 @@ def test_step_kernel_names_each_form():
 
     counts, dx = (64, 20, 17), 1e-3
     _, g = heat_pair(counts, dx, ALUMINIUM, 300.0, dirichlet_films(counts, dx, 300.0))
-    assert g.step_kernel(1) == ("heat_plain_pair_step", 1)
+    assert g.step_kernel(1) == ("heat_plain_quad_step", 1)
     name, launches = g.step_kernel(2500)  # a small block: many steps a cooperative launch
     assert name.startswith("heat_plain_pair_steps") and launches == 3
+    g.set_cells_per_thread(2)
+    assert g.step_kernel(1) == ("heat_plain_pair_step", 1)
     g.set_cells_per_thread(1)
     assert g.step_kernel(1) == ("heat_plain_step", 1)
     _, h = heat_pair((63, 20, 17), dx, ALUMINIUM, 300.0)
@@ -85,3 +88,44 @@ def test_step_kernel_names_each_form():
     _, f = heat_pair(counts, dx, ALUMINIUM, 300.0, precision="f32")
     assert f.step_kernel(1) == ("heat_tma_step (TMA-staged)", 1)
     assert f.step_kernel(0) == ("none", 0)
+
+
+@pytest.mark.parametrize("counts", [(64, 20, 17), (100, 9, 33), (8, 8, 8), (4, 3, 5)])
+@pytest.mark.parametrize("kind", ["insulated", "dirichlet", "finite"])
+def test_plain_four_two_and_one_cells_agree_with_the_oracle(counts, kind):
+    """Four cells of a row per thread in plain f64 (heat_plain_quad_step), one step a call (a call of
+    more steps on a block this small takes the many-step cooperative kernel): bit for bit with the
+    pair and one-cell forms and the oracle, books within 1e-12 of the oracle's scale."""
+    dx = 1e-3
+    cells = 300.0 + 30.0 * np.random.default_rng(sum(counts) + 1).random(int(np.prod(counts)))
+    films = films_of(kind, counts, dx)
+    runs = []
+    for per_thread in (4, 2, 1):
+        o, g = heat_pair(counts, dx, ALUMINIUM, 300.0, films, cells)
+        g.set_cells_per_thread(per_thread)
+        g.set_tolerance(1e-9)
+        dt = 0.9 * g.max_stable_dt()
+        for _ in range(20):
+            assert g.step(dt, 1) is None
+        runs.append((g.cells, g.ledger()))
+    assert o.step(dt, 20) is None
+    lo = o.ledger()
+    for cells_now, led in runs:
+        assert np.array_equal(cells_now.view(np.uint64), o.cells.view(np.uint64))
+        assert abs(led["total"] - lo["total"]) <= 1e-12 * max(lo["scale"], 1e-300)
+
+
+def test_plain_four_cells_many_steps_past_the_cooperative_size():
+    """256 × 128 × 129 cells (just over 2^22): a call of 70 steps runs heat_plain_quad_step (a
+    64-step graph and six single launches), bit for bit with the oracle."""
+    counts, dx = (256, 128, 129), 1e-3
+    cells = 300.0 + 30.0 * np.random.default_rng(3).random(int(np.prod(counts)))
+    o, g = heat_pair(counts, dx, ALUMINIUM, 300.0, films_of("dirichlet", counts, dx), cells)
+    assert g.step_kernel(70) == ("heat_plain_quad_step", 70)
+    g.set_tolerance(1e-9)
+    dt = 0.9 * g.max_stable_dt()
+    assert g.step(dt, 70) is None
+    assert o.step(dt, 70) is None
+    assert np.array_equal(g.cells.view(np.uint64), o.cells.view(np.uint64))
+    lg, lo = g.ledger(), o.ledger()
+    assert abs(lg["total"] - lo["total"]) <= 1e-12 * max(lo["scale"], 1e-300)
