@@ -135,6 +135,14 @@ pm_status pm_heat_gaps(pm_heat* h, long long* a, long long* b, double* coefficie
 /* Solid3D::set_temperature over every cell (solid.rs:1346-1361), kelvin, index x + nx(y + ny z). */
 pm_status pm_heat_upload(pm_heat* h, const double* kelvin, size_t n);
 pm_status pm_heat_download(pm_heat* h, double* kelvin, size_t n);
+/* Solid3D as a field (solid.rs:2028-2104): kelvin, trilinear between cell centres, clamped at the
+ * faces, NaN in a void cell, the weights renormalised over the solid corners.
+ * scene::capture's sampling (crates/pantometry-scene/src/lib.rs:347-420), run on the device over the
+ * resident field: `samples[0] * samples[1] * samples[2]` points from `lo` to `hi` (metres, the
+ * domain's own coordinates), x fastest, i / (n - 1) of the way along an axis of n > 1 samples and
+ * the middle of an axis of one; `out` (host, n values) receives `ScalarField::at` at each point. */
+pm_status pm_heat_sample(pm_heat* h, const double lo[3], const double hi[3], const int samples[3], double* out,
+                         size_t n);
 /* Domain::max_stable_dt (solid.rs:1709-1715). */
 pm_status pm_heat_max_stable_dt(pm_heat* h, double* seconds);
 /* Relative tolerance of the per-step audit (`Simulation::advance`, sim.rs:947-965, and
@@ -206,6 +214,13 @@ pm_status pm_hall_step(pm_hall* h, double dt, long long nsteps, pm_violation* ou
 pm_status pm_hall_ledger(pm_hall* h, pm_ledger* out);
 /* Any pointer may be NULL. p_prev is `pressure_prev`. */
 pm_status pm_hall_download(pm_hall* h, double* p, double* p_prev, double* vx, double* vy, double* vz);
+/* Hall as a field (hall.rs:585-613): pascals, trilinear between nodes, clamped at the surfaces.
+ * scene::capture's sampling (crates/pantometry-scene/src/lib.rs:347-420), run on the device over the
+ * resident field: `samples[0] * samples[1] * samples[2]` points from `lo` to `hi` (metres, the
+ * domain's own coordinates), x fastest, i / (n - 1) of the way along an axis of n > 1 samples and
+ * the middle of an axis of one; `out` (host, n values) receives `ScalarField::at` at each point. */
+pm_status pm_hall_sample(pm_hall* h, const double lo[3], const double hi[3], const int samples[3], double* out,
+                         size_t n);
 pm_status pm_hall_checkpoint(pm_hall* h);
 pm_status pm_hall_restore(pm_hall* h);
 /* No counterpart in the reference. FP32 halls on the TMA-staged kernel (x extent a multiple of 4)
@@ -388,6 +403,14 @@ pm_status pm_cavity_step(pm_cavity* c, double dt, long long nsteps, pm_violation
 pm_status pm_cavity_ledger(pm_cavity* c, pm_ledger* out);
 /* Cavity::electric_energy / magnetic_energy (cavity.rs:824-847, 919-940), on the device. */
 pm_status pm_cavity_energies(pm_cavity* c, double* electric, double* magnetic);
+/* Cavity as a field (cavity.rs:191-206, 735-742): |E| in V/m of the edges of the cell a point falls
+ * in, nearest cell, clamped.
+ * scene::capture's sampling (crates/pantometry-scene/src/lib.rs:347-420), run on the device over the
+ * resident field: `samples[0] * samples[1] * samples[2]` points from `lo` to `hi` (metres, the
+ * domain's own coordinates), x fastest, i / (n - 1) of the way along an axis of n > 1 samples and
+ * the middle of an axis of one; `out` (host, n values) receives `ScalarField::at` at each point. */
+pm_status pm_cavity_sample(pm_cavity* c, const double lo[3], const double hi[3], const int samples[3], double* out,
+                           size_t n);
 /* Domain::checkpoint / restore (cavity.rs:1566-1590): the fields, `started` and `dissipated`. With
  * a source set (the extension) the checkpoint also keeps the source's clock and its work books, so
  * steps retried after a restore drive the same samples of the current; an FP32 cavity keeps the f64

@@ -95,6 +95,9 @@ def _declare(L):
         "or_heat_losing_from": (None, [p, i, d, d, d]),
         "or_heat_fill": (None, [p, d, d, d, d, i, C.c_void_p]),
         "or_heat_empty": (None, [p, C.c_void_p]),
+        "or_heat_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
+        "or_hall_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
+        "or_yee_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_heat_dissipating": (None, [p, d, C.c_void_p]),
         "or_heat_generated_power": (d, [p]),
         "or_heat_generated_energy": (d, [p]),
@@ -203,6 +206,17 @@ class _Box:
         fn(self._h, *[C.byref(v) for v in vals])
         return [v.value for v in vals]
 
+    _sampler = None
+
+    def sample(self, lo, hi, samples):
+        """scene::capture's sampling of this domain's field over an extent (crates/pantometry-
+        scene/src/lib.rs:391-420): samples = (nx, ny, nz) points from lo to hi (metres), x fastest."""
+        n = (C.c_int * 3)(*[int(v) for v in samples])
+        lo3, hi3 = (C.c_double * 3)(*map(float, lo)), (C.c_double * 3)(*map(float, hi))
+        out = np.empty(int(np.prod([int(v) for v in samples])), dtype=np.float64)
+        getattr(lib(), self._sampler)(self._h, lo3, hi3, n, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
 
 # --------------------------------------------------------------------------------------------
 # Solid3D
@@ -212,6 +226,8 @@ FACES = ("XMin", "XMax", "YMin", "YMax", "ZMin", "ZMax")
 
 class Heat(_Box):
     """`Solid3D` restated: `new`, `losing_from`, `fill`, `step`, `ledger`, `Simulation::advance`."""
+
+    _sampler = "or_heat_sample"
 
     def __init__(self, counts, dx, density, conductivity, specific_heat, initial, emissivity=0.0,
                  thermal=True, name="block"):
@@ -328,6 +344,8 @@ class Heat(_Box):
 # --------------------------------------------------------------------------------------------
 class Hall(_Box):
     """`Hall` restated: `new`, `released_from`, `released_in_mode`, `step`, `ledger`."""
+
+    _sampler = "or_hall_sample"
 
     def __init__(self, width, height, depth, across, speed, density, name="hall"):
         L = lib()
@@ -603,6 +621,8 @@ WALL_KINDS = {"conducting": 0, "magnetic": 1, "open": 2}
 
 class Yee(_Box):
     """`Cavity` restated: `new`, `fill` (per cell), `obstruct`, `release_mode`, `step`, `ledger`."""
+
+    _sampler = "or_yee_sample"
 
     def __init__(self, counts, dx, eps_r=1.0, mu_r=1.0, sigma=0.0, name="cavity"):
         L = lib()

@@ -1989,4 +1989,126 @@ void or_yee_inject_divergence(void* p, int i, int j, int k, double amount) {  //
     c->hx[at] += amount;
 }
 
+
+}  // extern "C"
+
+// ---- scene::capture's field sampling (crates/pantometry-scene/src/lib.rs:347-420): the extent's
+// sample grid, x fastest; along an axis of n > 1 samples the point i / (n − 1) of the way from min
+// to max, of one sample the middle (lib.rs:398-406); each point is `lo + (hi − lo) · f` per
+// component, then the domain's own `ScalarField::at` there.
+static double or_along(int i, int n) { return n > 1 ? (double)i / (double)(n - 1) : 0.5; }
+template <typename At>
+static void or_sample_grid(const double* lo, const double* hi, const int* n, double* out, At at) {
+    size_t r = 0;
+    for (int k = 0; k < n[2]; ++k)
+        for (int j = 0; j < n[1]; ++j)
+            for (int i = 0; i < n[0]; ++i) {
+                const double f[3] = {or_along(i, n[0]), or_along(j, n[1]), or_along(k, n[2])};
+                double q[3];
+                for (int a = 0; a < 3; ++a) q[a] = lo[a] + (hi[a] - lo[a]) * f[a];
+                out[r++] = at(q);
+            }
+}
+
+extern "C" {
+
+// Solid3D::at (solid.rs:2045-2104): trilinear between cell centres, clamped at the faces, NaN in
+// a void cell, the weights renormalised over the solid corners.
+void or_heat_sample(void* p, const double* lo, const double* hi, const int* n, double* out) {
+    Heat* h = (Heat*)p;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    auto is_void = [&](size_t c) { return !h->vd.empty() && h->vd[c] != 0; };
+    or_sample_grid(lo, hi, n, out, [&](const double* pt) {
+        const double q[3] = {pt[0] / h->dx - 0.5, pt[1] / h->dx - 0.5, pt[2] / h->dx - 0.5};
+        if (std::isnan(q[0]) || std::isnan(q[1]) || std::isnan(q[2])) return std::nan("");
+        auto axis = [](double v, int cnt, int& i, double& f) {
+            const int last = cnt > 0 ? cnt - 1 : 0;
+            if (v <= 0.0) { i = 0; f = 0.0; return; }
+            if (v >= (double)last) { i = last; f = 0.0; return; }
+            const double fl = std::floor(v);
+            i = (int)fl;
+            f = v - fl;
+        };
+        int i, j, k;
+        double fx, fy, fz;
+        axis(q[0], nx, i, fx);
+        axis(q[1], ny, j, fy);
+        axis(q[2], nz, k, fz);
+        auto nearest = [](double v, int cnt) {
+            double r = std::round(v);
+            if (r < 0.0) r = 0.0;
+            const int last = cnt > 0 ? cnt - 1 : 0;
+            return std::min((int)r, last);
+        };
+        if (is_void((size_t)nearest(q[0], nx) + (size_t)nx * ((size_t)nearest(q[1], ny) + (size_t)ny * nearest(q[2], nz))))
+            return std::nan("");
+        const int i1 = std::min(i + 1, nx - 1), j1 = std::min(j + 1, ny - 1), k1 = std::min(k + 1, nz - 1);
+        const int ai[2] = {i, i1}, bj[2] = {j, j1}, ck[2] = {k, k1};
+        const double wa[2] = {1.0 - fx, fx}, wb[2] = {1.0 - fy, fy}, wc[2] = {1.0 - fz, fz};
+        double sum = 0.0, weight = 0.0;
+        for (int x = 0; x < 2; ++x)
+            for (int y = 0; y < 2; ++y)
+                for (int z = 0; z < 2; ++z) {
+                    const double w = wa[x] * wb[y] * wc[z];
+                    const size_t at = (size_t)ai[x] + (size_t)nx * ((size_t)bj[y] + (size_t)ny * ck[z]);
+                    if (w > 0.0 && !is_void(at)) {
+                        sum += w * h->cells[at];
+                        weight += w;
+                    }
+                }
+        return weight > 0.0 ? sum / weight : std::nan("");
+    });
+}
+
+// Hall::at (hall.rs:591-613) with clamp_index (hall.rs:684-694): trilinear between nodes, clamped
+// at the surfaces; a NaN point reads node 0.
+void or_hall_sample(void* p, const double* lo, const double* hi, const int* n, double* out) {
+    Hall* h = (Hall*)p;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    or_sample_grid(lo, hi, n, out, [&](const double* pt) {
+        const double q[3] = {pt[0] / h->dx, pt[1] / h->dx, pt[2] / h->dx};
+        if (std::isnan(q[0]) || std::isnan(q[1]) || std::isnan(q[2])) return h->p[0];
+        auto clamp_index = [](double v, int cnt, int& i, double& f) {
+            if (std::isnan(v) || v <= 0.0) { i = 0; f = 0.0; return; }
+            const double last = (double)(cnt - 1);
+            if (v >= last) { i = cnt - 1; f = 0.0; return; }
+            const double fl = std::floor(v);
+            i = (int)fl;
+            f = v - fl;
+        };
+        int i, j, k;
+        double fx, fy, fz;
+        clamp_index(q[0], nx, i, fx);
+        clamp_index(q[1], ny, j, fy);
+        clamp_index(q[2], nz, k, fz);
+        const int i1 = std::min(i + 1, nx - 1), j1 = std::min(j + 1, ny - 1), k1 = std::min(k + 1, nz - 1);
+        auto g = [&](int a, int b, int c) { return h->p[h->at(a, b, c)]; };
+        auto lerp = [](double a, double b, double t) { return a * (1.0 - t) + b * t; };
+        const double z0 = lerp(lerp(g(i, j, k), g(i1, j, k), fx), lerp(g(i, j1, k), g(i1, j1, k), fx), fy);
+        const double z1 = lerp(lerp(g(i, j, k1), g(i1, j, k1), fx), lerp(g(i, j1, k1), g(i1, j1, k1), fx), fy);
+        return lerp(z0, z1, fz);
+    });
+}
+
+// Cavity::at (cavity.rs:197-206) over electric_at (cavity.rs:735-742): |E| of the edges of the cell
+// the point falls in, nearest cell, clamped; NaN for a NaN point.
+void or_yee_sample(void* p, const double* lo, const double* hi, const int* n, double* out) {
+    Cavity* c = (Cavity*)p;
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    or_sample_grid(lo, hi, n, out, [&](const double* pt) {
+        const double q[3] = {pt[0] / c->dx, pt[1] / c->dx, pt[2] / c->dx};
+        if (std::isnan(q[0]) || std::isnan(q[1]) || std::isnan(q[2])) return std::nan("");
+        auto pick = [](double v, int cnt) {
+            double f = std::floor(v);
+            if (f < 0.0) f = 0.0;
+            return std::min((int)f, cnt > 0 ? cnt - 1 : 0);
+        };
+        const int i = pick(q[0], nx), j = pick(q[1], ny), k = pick(q[2], nz);
+        const double x = c->ex[c->iex(std::min(i, nx - 1), std::min(j, ny), std::min(k, nz))];
+        const double y = c->ey[c->iey(std::min(i, nx), std::min(j, ny - 1), std::min(k, nz))];
+        const double z = c->ez[c->iez(std::min(i, nx), std::min(j, ny), std::min(k, nz - 1))];
+        return std::sqrt((x * x + y * y) + z * z);  // DVec3::length: the dot product, then sqrt
+    });
+}
+
 }  // extern "C"

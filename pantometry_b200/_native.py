@@ -174,6 +174,9 @@ SIGNATURES = {
     "pm_heat_absorb": (_st, [_p, _d]),
     "pm_heat_checkpoint": (_st, [_p]),
     "pm_heat_restore": (_st, [_p]),
+    "pm_heat_sample": (_st, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t]),
+    "pm_hall_sample": (_st, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t]),
+    "pm_cavity_sample": (_st, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t]),
     "pm_heat_step_kernel": (_st, [_p, C.c_longlong, C.c_char_p, C.c_int, C.POINTER(C.c_longlong)]),
     "pm_heat_set_cells_per_thread": (_st, [_p, _i]),
     "pm_heat_set_stream": (_st, [_p, _p]),

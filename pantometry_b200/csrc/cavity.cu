@@ -1118,6 +1118,27 @@ pm_status pm_cavity_ledger(pm_cavity* cp, pm_ledger* out) {
     return PM_OK;
 }
 
+pm_status pm_cavity_sample(pm_cavity* cp, const double* lo, const double* hi, const int* samples, double* out,
+                           size_t n) {
+    Cavity* c = reinterpret_cast<Cavity*>(cp);
+    CAV_GUARD(c);
+    SampleGrid g{};
+    pm_status s = sample_grid_of(lo, hi, samples, out, n, g);
+    if (s != PM_OK) return s;
+    g.dx = c->dx;
+    g.nx = c->nx; g.ny = c->ny; g.nz = c->nz;
+    const unsigned nx = (unsigned)c->nx, ny = (unsigned)c->ny;
+    // each E component's row pitch and rows per plane: its own extents, or the padded lattice
+    const uint3 rx = c->tma ? make_uint3(c->L, c->L, c->L) : make_uint3(nx, nx + 1, nx + 1);
+    const uint3 ry = c->tma ? make_uint3(ny + 1, ny + 1, ny + 1) : make_uint3(ny + 1, ny, ny + 1);
+    const DBuf* f = c->f[c->parity];
+    return run_sample(c, out, n, [&](double* dev, cudaStream_t st) {
+        return c->precision == PM_PLAIN_F64
+                   ? launch_yee_sample<double>(g, f[0].as<double>(), f[1].as<double>(), f[2].as<double>(), rx, ry, dev, st)
+                   : launch_yee_sample<float>(g, f[0].as<float>(), f[1].as<float>(), f[2].as<float>(), rx, ry, dev, st);
+    });
+}
+
 pm_status pm_cavity_energies(pm_cavity* cp, double* electric, double* magnetic) {
     Cavity* c = reinterpret_cast<Cavity*>(cp);
     CAV_GUARD(c);

@@ -509,6 +509,20 @@ pm_status pm_hall_ledger(pm_hall* hp, pm_ledger* out) {
     return PM_OK;
 }
 
+pm_status pm_hall_sample(pm_hall* hp, const double* lo, const double* hi, const int* samples, double* out, size_t n) {
+    Hall* h = reinterpret_cast<Hall*>(hp);
+    HALL_GUARD(h);
+    SampleGrid g{};
+    pm_status s = sample_grid_of(lo, hi, samples, out, n, g);
+    if (s != PM_OK) return s;
+    g.dx = h->dx;
+    g.nx = h->nx; g.ny = h->ny; g.nz = h->nz;
+    return run_sample(h, out, n, [&](double* dev, cudaStream_t st) {
+        return h->precision == PM_PLAIN_F64 ? launch_hall_sample<double>(g, h->p[h->parity].as<double>(), dev, st)
+                                            : launch_hall_sample<float>(g, h->p[h->parity].as<float>(), dev, st);
+    });
+}
+
 pm_status pm_hall_download(pm_hall* hp, double* pr, double* pp, double* vx, double* vy, double* vz) {
     Hall* h = reinterpret_cast<Hall*>(hp);
     HALL_GUARD(h);

@@ -780,6 +780,22 @@ pm_status pm_heat_download(pm_heat* hp, double* kelvin, size_t n) {
     return PM_OK;
 }
 
+pm_status pm_heat_sample(pm_heat* hp, const double* lo, const double* hi, const int* samples, double* out, size_t n) {
+    Heat* h = reinterpret_cast<Heat*>(hp);
+    HEAT_GUARD(h);
+    SampleGrid g{};
+    pm_status s = sample_grid_of(lo, hi, samples, out, n, g);
+    if (s != PM_OK) return s;
+    g.dx = h->dx;
+    g.nx = h->nx; g.ny = h->ny; g.nz = h->nz;
+    const uint8_t* vd = h->vd.empty() ? nullptr : h->dvoid.as<uint8_t>();
+    return run_sample(h, out, n, [&](double* dev, cudaStream_t st) {
+        return h->precision == PM_PLAIN_F64
+                   ? launch_heat_sample<double>(g, h->field[h->parity].as<double>(), 0.0, vd, dev, st)
+                   : launch_heat_sample<float>(g, h->field[h->parity].as<float>(), h->reference, vd, dev, st);
+    });
+}
+
 pm_status pm_heat_max_stable_dt(pm_heat* hp, double* seconds) {
     Heat* h = reinterpret_cast<Heat*>(hp);
     HEAT_GUARD(h);

@@ -15,6 +15,7 @@
 #include "ens_tma.cuh"
 #include "yee_near.cuh"
 #include "heat_tma.cuh"
+#include "sample_kernels.cuh"
 
 namespace pm {
 
@@ -90,6 +91,16 @@ cudaError_t launch_heat_f32_steps(const HeatF32Args& a, const HeatPersist& p, cu
 cudaError_t launch_heat_tma(const HeatTmaArgs& a, const CUtensorMap& map, cudaStream_t s);
 bool heat_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz);
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s);
+// scene::capture's sampling of a field over an extent's grid (sample_kernels.cuh), into `out` on
+// the device: Solid3D (kelvin, or FP32 deviations with t0 added), Hall pressure, Cavity |E|.
+template <typename Real>
+cudaError_t launch_heat_sample(const SampleGrid& g, const Real* cells, double t0, const uint8_t* vd, double* out,
+                               cudaStream_t s);
+template <typename Real>
+cudaError_t launch_hall_sample(const SampleGrid& g, const Real* p, double* out, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_yee_sample(const SampleGrid& g, const Real* ex, const Real* ey, const Real* ez, uint3 rx, uint3 ry,
+                              double* out, cudaStream_t s);
 cudaError_t launch_heat_convert(const double* t, float* d, double t0, size_t n, int to_dev, double* tout,
                                 cudaStream_t s);
 cudaError_t launch_heat_rise(double* t64, float* d32, double rise, size_t n, const uint8_t* vd, cudaStream_t s);

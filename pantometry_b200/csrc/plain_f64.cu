@@ -140,6 +140,36 @@ cudaError_t launch_bar_deposit<double>(double* t, const double* per_cell, double
     return cudaGetLastError();
 }
 
+static unsigned sample_blocks(const SampleGrid& g) {
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    return (unsigned)std::max<long long>(1, std::min<long long>((total + 255) / 256, 592));
+}
+template <typename Real>
+cudaError_t launch_heat_sample(const SampleGrid& g, const Real* cells, double t0, const uint8_t* vd, double* out,
+                               cudaStream_t s) {
+    heat_sample<Real><<<sample_blocks(g), 256, 0, s>>>(g, cells, t0, vd, out);
+    return cudaGetLastError();
+}
+template <typename Real>
+cudaError_t launch_hall_sample(const SampleGrid& g, const Real* p, double* out, cudaStream_t s) {
+    hall_sample<Real><<<sample_blocks(g), 256, 0, s>>>(g, p, out);
+    return cudaGetLastError();
+}
+template <typename Real>
+cudaError_t launch_yee_sample(const SampleGrid& g, const Real* ex, const Real* ey, const Real* ez, uint3 rx, uint3 ry,
+                              double* out, cudaStream_t s) {
+    yee_sample<Real><<<sample_blocks(g), 256, 0, s>>>(g, ex, ey, ez, rx, ry, out);
+    return cudaGetLastError();
+}
+template cudaError_t launch_heat_sample<double>(const SampleGrid&, const double*, double, const uint8_t*, double*, cudaStream_t);
+template cudaError_t launch_heat_sample<float>(const SampleGrid&, const float*, double, const uint8_t*, double*, cudaStream_t);
+template cudaError_t launch_hall_sample<double>(const SampleGrid&, const double*, double*, cudaStream_t);
+template cudaError_t launch_hall_sample<float>(const SampleGrid&, const float*, double*, cudaStream_t);
+template cudaError_t launch_yee_sample<double>(const SampleGrid&, const double*, const double*, const double*, uint3, uint3,
+                                               double*, cudaStream_t);
+template cudaError_t launch_yee_sample<float>(const SampleGrid&, const float*, const float*, const float*, uint3, uint3,
+                                              double*, cudaStream_t);
+
 int occupancy_f64(KernelId id) {
     int n = 0;
     cudaError_t e = cudaSuccess;

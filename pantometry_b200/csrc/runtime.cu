@@ -51,6 +51,21 @@ int blocks_per_sm(KernelId id) {
     return n;
 }
 
+pm_status sample_grid_of(const double* lo, const double* hi, const int* samples, const double* out, size_t n,
+                         SampleGrid& g) {
+    if (!lo || !hi || !samples || !out) return fail(PM_BAD_ARG, "sample: lo, hi, samples and out are required");
+    size_t count = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (samples[a] < 1) return fail(PM_BAD_ARG, "sample: at least one sample along each axis");
+        count *= (size_t)samples[a];
+        g.lo[a] = lo[a];
+        g.hi[a] = hi[a];
+        g.n[a] = samples[a];
+    }
+    if (count != n) return fail(PM_BAD_ARG, "sample: out holds one value per sample point");
+    return PM_OK;
+}
+
 void set_error(const std::string& msg) { g_error = msg; }
 
 pm_status fail(pm_status s, const std::string& msg) {

@@ -51,6 +51,19 @@ struct DBuf {
 
 // What every handle carries: its device, its stream, its device state and partials, and the
 // cached graphs of G steps (one per ping-pong parity, rebuilt when the step size changes).
+// The sample grid of a pm_*_sample call: lo, hi in metres, samples per axis, `n` values in `out`.
+pm_status sample_grid_of(const double* lo, const double* hi, const int* samples, const double* out, size_t n,
+                         SampleGrid& g);
+// Run `launch` into the handle's sample buffer, then copy the n samples to `out` (host).
+template <typename H, typename F>
+pm_status run_sample(H* h, double* out, size_t n, F launch) {
+    if (!h->sampled.p || h->sampled.bytes < n * 8) PM_CUDA(h->sampled.alloc(n * 8));
+    PM_CUDA(launch(h->sampled.template as<double>(), h->stream()));
+    PM_CUDA(cudaMemcpyAsync(out, h->sampled.p, n * 8, cudaMemcpyDeviceToHost, h->stream()));
+    PM_CUDA(cudaStreamSynchronize(h->stream()));
+    return PM_OK;
+}
+
 struct Handle {
     int device = 0;
     std::string name;
@@ -60,6 +73,7 @@ struct Handle {
     cudaStream_t capture = nullptr;
     DBuf state;      // DevState
     DBuf partials;   // per-block partial sums
+    DBuf sampled;    // the samples of the last pm_*_sample call
     DevState* host_state = nullptr;  // pinned mirror
     double tolerance = -1.0;         // no audit: plain `Domain::step`; set one to audit every step
     std::string refusal_site;        // where a step refused on the device (kRefused) is reported

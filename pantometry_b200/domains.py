@@ -64,7 +64,10 @@ class _Domain:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            getattr(N.load(), self._destroy)(h)
+            try:
+                getattr(N.load(), self._destroy)(h)
+            except (TypeError, AttributeError):  # the interpreter is shutting down: the process frees it
+                pass
             self._h = None
 
     def close(self):
@@ -91,7 +94,23 @@ class _Domain:
         N.check(getattr(self._lib, self._prefix + "restore")(self._h))
 
 
-class Solid3D(_Domain):
+class _Field:
+    """A domain that is a field: scene::capture's sampling of it (crates/pantometry-scene/src/lib.rs:
+    347-420), run on the device over the resident state."""
+
+    def sample(self, lo, hi, samples):
+        """`ScalarField::at` at samples = (nx, ny, nz) points from lo to hi (metres), x fastest:
+        a flat array of nx·ny·nz values, i / (n − 1) of the way along an axis of n > 1 samples and
+        the middle of an axis of one."""
+        n = (C.c_int * 3)(*[int(v) for v in samples])
+        lo3, hi3 = (C.c_double * 3)(*map(float, lo)), (C.c_double * 3)(*map(float, hi))
+        out = np.empty(int(n[0]) * int(n[1]) * int(n[2]), dtype=np.float64)
+        fn = getattr(self._lib, self._prefix + "sample")
+        N.check(fn(self._h, lo3, hi3, n, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
+
+
+class Solid3D(_Domain, _Field):
     """`Solid3D` (crates/pantometry-thermal/src/solid.rs) on the GPU."""
 
     _destroy = "pm_heat_destroy"
@@ -248,7 +267,7 @@ class Bar(_Domain):
         return out.value
 
 
-class Hall(_Domain):
+class Hall(_Domain, _Field):
     """`Hall` (crates/pantometry-acoustic/src/hall.rs) on the GPU."""
 
     _destroy = "pm_hall_destroy"
@@ -427,7 +446,7 @@ class Tube(_Domain):
         return out
 
 
-class Cavity(_Domain):
+class Cavity(_Domain, _Field):
     """`Cavity` (crates/pantometry-em/src/cavity.rs) on the GPU."""
 
     _destroy = "pm_cavity_destroy"

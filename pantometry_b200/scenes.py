@@ -186,3 +186,29 @@ def run(scene, domain):
         substeps.append(n)
         frames.append({"t": t, "total": led["total"], "scale": led["scale"]})
     return {"frames": frames, "substeps": substeps, "violation": None}
+
+
+# ScalarField::unit of each field domain (solid.rs:2030-2032, hall.rs:586-588, cavity.rs:191-193)
+UNITS = {Solid3D: "K", Hall: "Pa", Cavity: "V/m"}
+
+
+def capture(domains, placed, time_s=0.0):
+    """`scene::capture` (crates/pantometry-scene/src/lib.rs:347-372) over domains on the device.
+
+    `domains` maps names to domains; `placed` maps names to placements, each with an optional
+    "extent": {"min": (x, y, z), "max": (x, y, z), "samples": (nx, ny, nz)} in metres. Every domain
+    that is a field and was placed with an extent becomes a panel: its `ScalarField::at` at each
+    point of the extent's sample grid, sampled on the device from the resident state (only the
+    samples cross to the host). A field placed with no extent is not drawn (lib.rs:343-345), as
+    the reference leaves it. Scalar readings and body sets are outside this path.
+    """
+    panels = []
+    for name, domain in domains.items():
+        extent = (placed.get(name) or {}).get("extent")
+        unit = next((u for cls, u in UNITS.items() if isinstance(domain, cls)), None)
+        if extent is None or unit is None:
+            continue
+        samples = tuple(int(v) for v in extent["samples"])
+        values = domain.sample(extent["min"], extent["max"], samples)
+        panels.append({"name": name, "unit": unit, "grid": samples, "values": values})
+    return {"time_s": float(time_s), "panels": panels}

@@ -1,0 +1,193 @@
+"""scene::capture's field sampling (crates/pantometry-scene/src/lib.rs:347-420): each domain's
+`ScalarField::at` over an extent's sample grid. The oracle's samplers are pinned by the properties
+the reference states for them (a sample on a cell centre or node is that value exactly, void reads
+NaN, points outside are clamped, one sample along an axis is its middle); the device samplers are
+bit for bit with the oracle in f64 and within f32 rounding in FP32, on the resident fields.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import heat_pair
+
+
+def heat_oracle(counts=(6, 5, 4), dx=1e-3, void=None, seed=1):
+    o = oracle.Heat(counts, dx, 1000.0, 100.0, 1000.0, 300.0)
+    if void is not None:
+        o.empty(void)
+    cells = 300.0 + 40.0 * np.random.default_rng(seed).random(int(np.prod(counts)))
+    o.cells = cells
+    return o, cells
+
+
+def test_heat_samples_on_cell_centres_are_the_cells():
+    """solid.rs:2041-2043: a sample at a cell centre is that cell exactly; a grid laid over the centres
+    lands on them to the rounding of lo + (hi − lo)·f."""
+    o, cells = heat_oracle()
+    got = o.sample((0.5e-3, 0.5e-3, 0.5e-3), (5.5e-3, 4.5e-3, 3.5e-3), (6, 5, 4))
+    assert np.allclose(got, cells, rtol=1e-12, atol=0)
+    one = o.sample((2.5e-3, 1.5e-3, 0.5e-3), (2.5e-3, 1.5e-3, 0.5e-3), (1, 1, 1))[0]
+    assert one == cells[2 + 6 * 1]  # exactly on a centre: that cell, bit for bit
+
+
+def test_heat_samples_clamp_outside_and_blend_between():
+    o, cells = heat_oracle()
+    nx, ny, nz = 6, 5, 4
+    c = cells.reshape(nz, ny, nx)
+    # far outside every face: the corner cells, clamped rather than extrapolated
+    got = o.sample((-1.0, -1.0, -1.0), (1.0, 1.0, 1.0), (2, 2, 2))
+    assert got[0] == c[0, 0, 0] and got[-1] == c[-1, -1, -1]
+    # halfway between two cell centres along x: the mean of the two
+    mid = o.sample((1.0e-3, 0.5e-3, 0.5e-3), (1.0e-3, 0.5e-3, 0.5e-3), (1, 1, 1))[0]
+    assert mid == pytest.approx(0.5 * (c[0, 0, 0] + c[0, 0, 1]), rel=1e-15)
+
+
+def test_heat_samples_in_void_are_nan_and_neighbours_renormalise():
+    """solid.rs:2034-2044, 2069-2079: a sample in a void cell is NaN; one leaning on a void
+    neighbour takes the solid corners' values alone."""
+    counts = (6, 5, 4)
+    void = np.zeros(counts[::-1], dtype=np.uint8)
+    void[:, :, 3] = 1  # the x = 3 column of cells
+    o, cells = heat_oracle(counts, void=void.reshape(-1))
+    c = cells.reshape(4, 5, 6)
+    assert math.isnan(o.sample((3.5e-3, 2.5e-3, 1.5e-3), (3.5e-3, 2.5e-3, 1.5e-3), (1, 1, 1))[0])
+    # a quarter of the way from cell 2 towards void cell 3: cell 2 alone
+    v = o.sample((2.75e-3, 2.5e-3, 1.5e-3), (2.75e-3, 2.5e-3, 1.5e-3), (1, 1, 1))[0]
+    assert v == c[1, 2, 2]
+
+
+def test_one_sample_along_an_axis_is_its_middle():
+    """lib.rs:398-406: a single sample along an axis is taken at the middle of the extent."""
+    o, cells = heat_oracle()
+    a = o.sample((0.5e-3, 0.5e-3, 0.0), (0.5e-3, 0.5e-3, 3.0e-3), (1, 1, 1))[0]
+    b = o.sample((0.5e-3, 0.5e-3, 1.5e-3), (0.5e-3, 0.5e-3, 1.5e-3), (1, 1, 1))[0]
+    assert a == b
+
+
+def test_hall_samples_on_nodes_are_the_pressures_and_blend_linearly():
+    h = oracle.Hall(0.01, 0.008, 0.006, 6, 343.0, 1.2)
+    nx, ny, nz = h.nodes
+    dx = 0.01 / (nx - 1)
+    pr = np.random.default_rng(2).uniform(-1.0, 1.0, nx * ny * nz)
+    h.release(pr)
+    got = h.sample((0.0, 0.0, 0.0), ((nx - 1) * dx, (ny - 1) * dx, (nz - 1) * dx), (nx, ny, nz))
+    assert np.allclose(got, pr, rtol=0, atol=1e-15)
+    g = pr.reshape(nz, ny, nx)
+    mid = h.sample((0.5 * dx, 0.0, 0.0), (0.5 * dx, 0.0, 0.0), (1, 1, 1))[0]
+    assert mid == pytest.approx(0.5 * (g[0, 0, 0] + g[0, 0, 1]), rel=1e-14)
+
+
+def test_cavity_samples_are_the_length_of_the_cells_edges():
+    """cavity.rs:197-206, 735-742: |E| from the cell's own x, y and z edges, nearest cell."""
+    y = oracle.Yee((5, 4, 3), 1e-3)
+    dt = 0.9 * y.courant_limit()
+    y.release_mode((1, 1), 1.0, dt)
+    f = y.fields()
+    nx, ny, nz = 5, 4, 3
+    got = y.sample((0.5e-3, 0.5e-3, 0.5e-3), (4.5e-3, 3.5e-3, 2.5e-3), (nx, ny, nz))
+    ex = f["ex"].reshape(nz + 1, ny + 1, nx)
+    ey = f["ey"].reshape(nz + 1, ny, nx + 1)
+    ez = f["ez"].reshape(nz, ny + 1, nx + 1)
+    want = np.array([math.sqrt((ex[k, j, i] ** 2 + ey[k, j, i] ** 2) + ez[k, j, i] ** 2)
+                     for k in range(nz) for j in range(ny) for i in range(nx)])
+    assert np.array_equal(got, want)
+
+
+EXTENTS = [((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (7, 5, 3)), ((-2e-3, 1e-4, 3e-4), (9e-3, 7.3e-3, 2e-3), (13, 1, 9)),
+           ((1.7e-3, 2.2e-3, 0.9e-3), (1.7e-3, 2.2e-3, 0.9e-3), (1, 1, 1))]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_heat_device_samples_match_the_oracle(precision):
+    counts, dx = (16, 12, 10), 1e-3
+    void = np.zeros(counts[::-1], dtype=np.uint8)
+    void[3:6, 4:8, 7:11] = 1
+    cells = 300.0 + 40.0 * np.random.default_rng(5).random(int(np.prod(counts)))
+    o, g = heat_pair(counts, dx, dict(density=1000.0, conductivity=100.0, specific_heat=1000.0), 300.0,
+                     cells=cells, precision=precision)
+    o.empty(void.reshape(-1))
+    g.empty(void.reshape(-1))
+    o.cells = cells
+    g.cells = cells
+    for lo, hi, n in EXTENTS + [((0.5e-3, 0.5e-3, 0.5e-3), (15.5e-3, 11.5e-3, 9.5e-3), counts)]:
+        want, got = o.sample(lo, hi, n), g.sample(lo, hi, n)
+        assert np.array_equal(np.isnan(got), np.isnan(want))
+        if precision == "f64":
+            assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        else:
+            ok = ~np.isnan(want)
+            assert np.abs(got[ok] - want[ok]).max() < 1e-4  # kelvin: f32 deviations of ~40 K
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_hall_device_samples_match_the_oracle(precision):
+    from pantometry_b200.domains import Hall
+
+    n = 12
+    w = 0.011
+    o = oracle.Hall(w, 0.008, 0.006, n, 343.0, 1.2)
+    g = Hall(w, 0.008, 0.006, n, 343.0, 1.2, precision=precision)
+    pr = np.random.default_rng(3).uniform(-1.0, 1.0, int(np.prod(o.nodes)))
+    o.release(pr)
+    g.release(pr)
+    for lo, hi, cnt in EXTENTS:
+        want, got = o.sample(lo, hi, cnt), g.sample(lo, hi, cnt)
+        if precision == "f64":
+            assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        else:
+            assert np.abs(got - want).max() < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("counts,precision", [((10, 8, 6), "f64"), ((10, 8, 6), "f32"), ((32, 16, 9), "f32")])
+def test_cavity_device_samples_match_the_oracle(counts, precision):
+    """The f64 form on the reference layout, the FP32 form on the padded lattice (and with the wall
+    split where nx is a multiple of 32), after 30 steps of a released mode."""
+    from pantometry_b200.domains import Cavity
+
+    dx = 1e-3
+    o = oracle.Yee(counts, dx)
+    g = Cavity(counts, dx, precision=precision)
+    dt = 0.9 * o.courant_limit()
+    o.release_mode((1, 1), 1.0, dt)
+    g.release_mode((1, 1), 1.0, dt)
+    assert o.step(dt, 30) is None and g.step(dt, 30) is None
+    nx, ny, nz = counts
+    for lo, hi, cnt in EXTENTS + [((0.5e-3, 0.5e-3, 0.5e-3), ((nx - 0.5) * dx, (ny - 0.5) * dx, (nz - 0.5) * dx), counts)]:
+        want, got = o.sample(lo, hi, cnt), g.sample(lo, hi, cnt)
+        if precision == "f64":
+            assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        else:
+            assert np.abs(got - want).max() <= 1e-5 * max(np.abs(want).max(), 1e-30)
+
+
+@pytest.mark.gpu
+def test_sample_refuses_a_mismatched_buffer():
+    from pantometry_b200._native import NativeError
+    from pantometry_b200.domains import Cavity
+
+    g = Cavity((4, 4, 4), 1e-3)
+    with pytest.raises(NativeError):
+        g.sample((0, 0, 0), (1, 1, 1), (0, 2, 2))
+
+
+@pytest.mark.gpu
+def test_capture_draws_placed_fields_only():
+    """scene::capture: a placed field becomes a panel of its samples; a field with no extent is not
+    drawn (lib.rs:343-345)."""
+    from pantometry_b200 import scenes
+    from pantometry_b200.domains import Cavity, Hall
+
+    hall = Hall(0.01, 0.008, 0.006, 6, 343.0, 1.2)
+    cav = Cavity((6, 5, 4), 1e-3)
+    extent = {"min": (0.0, 0.0, 0.0), "max": (0.004, 0.003, 0.002), "samples": (5, 4, 3)}
+    frame = scenes.capture({"hall": hall, "cavity": cav}, {"hall": {"extent": extent}, "cavity": {}}, 0.25)
+    assert frame["time_s"] == 0.25
+    assert [p["name"] for p in frame["panels"]] == ["hall"]
+    panel = frame["panels"][0]
+    assert panel["unit"] == "Pa" and panel["grid"] == (5, 4, 3) and panel["values"].shape == (60,)
+    assert np.array_equal(panel["values"], hall.sample(extent["min"], extent["max"], extent["samples"]))
