@@ -196,15 +196,21 @@ constexpr int kWaitCounters = 8;
 constexpr int kWaitWords = 32 * kWaitCounters + 32;
 
 // Arrive at the grid's n-th wait and wait until every block has arrived n times, polling at most
-// `budget` times after the first look (false: the wait ran out). The arrival is a release, so what
-// the block wrote before it is seen by every block after its own wait, which ends with an acquire.
-__device__ __forceinline__ bool grid_wait(unsigned* base, unsigned n, unsigned budget) {
+// `budget` times after the first look. The arrival is a release, so what the block wrote before it
+// is seen by every block after its own wait, which ends with an acquire. A block may add
+// kWaitStop to its arrival to say the grid is to stop after this wait: every block sees it in the
+// sum it polls, with no further read. Returns 0 when the wait ran out, 1 when every block has
+// arrived, 2 when every block has arrived and one said stop.
+constexpr unsigned kWaitStop = 1u << 30;
+__device__ __forceinline__ int grid_wait(unsigned* base, unsigned n, unsigned budget, bool stop_after = false) {
     __shared__ int passed;
     __syncthreads();
     if (linear_tid() == 0) {
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(base + 32 * (blockIdx.x % kWaitCounters)) : "memory");
+        const unsigned arrive = stop_after ? 1u + kWaitStop : 1u;
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(base + 32 * (blockIdx.x % kWaitCounters)), "r"(arrive)
+                     : "memory");
         const unsigned target = n * gridDim.x;
-        bool ok = false;
+        int ok = 0;
         for (unsigned it = 0;; ++it) {
             unsigned v[kWaitCounters];
 #pragma unroll
@@ -213,18 +219,18 @@ __device__ __forceinline__ bool grid_wait(unsigned* base, unsigned n, unsigned b
             unsigned sum = 0;
 #pragma unroll
             for (int r = 0; r < kWaitCounters; ++r) sum += v[r];
-            if (sum >= target) {
-                ok = true;
+            if (sum % kWaitStop >= target) {
+                ok = sum >= kWaitStop ? 2 : 1;
                 break;
             }
             if (it >= budget) break;
             __nanosleep(32);
         }
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
-        passed = ok ? 1 : 0;
+        passed = ok;
     }
     __syncthreads();
-    return passed != 0;
+    return passed;
 }
 
 // `Ledger::add` (conserved.rs:86-90) into an entry that starts at zero.

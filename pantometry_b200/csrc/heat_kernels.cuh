@@ -501,7 +501,7 @@ static __global__ void __launch_bounds__(256, PM_HEAT_QUAD64_MIN_BLOCKS) heat_pl
 }
 
 struct HeatPersist {
-    unsigned* barrier;  // kWaitWords words, zero at launch: the grid wait's counters, then the verdict
+    unsigned* barrier;  // kWaitWords words, zero at launch: the grid wait's counters
     int nsteps;
     unsigned budget;    // polls per grid wait before giving up
 };
@@ -509,11 +509,12 @@ struct HeatPersist {
 // The many-step kernels of small uniform blocks: every step of a call in one cooperative launch.
 // Block 0 keeps the books and takes no cells; blocks 1.. take the tiles. In step s the workers step
 // their tiles and store their partials (two sets, by the step's parity) while block 0 sums step
-// s−1's in a fixed order, audits them and, if the audit failed, sets the verdict word; then every
-// block arrives at the grid's s-th wait and, once through it, reads the verdict. A failed audit of
-// step s−1 ends the call with step s−1's state, which is intact: step s wrote the other buffer. After
-// the last wait block 0 audits the last step and writes the books back. So the books' arithmetic
-// never sits between the steps, and only block 0 reads the partials.
+// s−1's in a fixed order and audits them; then every block arrives at the grid's s-th wait, block 0
+// adding the stop mark to its arrival if the audit failed, and every block learns of it from the
+// sum it polls. A failed audit of step s−1 ends the call with step s−1's state, which is intact:
+// step s wrote the other buffer. After the last wait block 0 audits the last step and writes the
+// books back. So the books' arithmetic never sits between the steps, and only block 0 reads the
+// partials.
 template <typename Args, typename StepTiles>
 __device__ __forceinline__ void heat_persist(const Args& a, const HeatPersist& p, double cap_scale,
                                              StepTiles step_tiles) {
@@ -524,7 +525,6 @@ __device__ __forceinline__ void heat_persist(const Args& a, const HeatPersist& p
     const int nthreads = blockDim.x * blockDim.y;
     const bool keeper = blockIdx.x == 0;
     const unsigned workers = gridDim.x - 1;
-    unsigned* verdict = p.barrier + 32 * kWaitCounters;
     if (tid == 0) {
         stop = a.st->violated;
         if (keeper) books = *a.st;
@@ -550,7 +550,7 @@ __device__ __forceinline__ void heat_persist(const Args& a, const HeatPersist& p
             books.part[1] = books.lost;
             books.part[2] = -books.supplied;
             audit_and_commit(&books, total, scale);
-            if (books.violated) *(volatile unsigned*)verdict = 1u;
+            stop = books.violated ? 1 : 0;
         }
     };
     bool timed_out = false;
@@ -566,15 +566,17 @@ __device__ __forceinline__ void heat_persist(const Args& a, const HeatPersist& p
                 part[2 * (size_t)(blockIdx.x - 1) + 1] = acc[1];
             }
         } else if (s > 0) {
-            audit(s - 1);
+            audit(s - 1);  // sets `stop` in block 0 when the audit failed (read after the wait's barrier)
         }
-        if (!grid_wait(p.barrier, (unsigned)(s + 1), p.budget)) {
+        const int w = grid_wait(p.barrier, (unsigned)(s + 1), p.budget, keeper && stop);
+        if (w == 0) {
             timed_out = true;
             break;
         }
-        if (tid == 0) stop = (int)*(volatile unsigned*)verdict;
-        __syncthreads();
-        if (stop) break;
+        if (w == 2) {
+            stop = 1;
+            break;
+        }
     }
     if (timed_out) {
         if (tid == 0) atomicExch(&a.st->violated, kDeviceTimeout);
