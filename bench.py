@@ -260,6 +260,7 @@ def run_ours(args):
     if not args.no_side_records:
         line["cavity"] = cavity_record(local, stream, peak)
         line["ensemble"] = ensemble_record(local, stream, peak)
+        line["heat_block"] = heat_block_record(local, stream, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n, sample_steps=args.cpu_sample_steps, threads=1)
     if rank == 0:
@@ -660,6 +661,64 @@ def cpu_baseline_heat(cfg, sample_steps):
 
 
 CAV_METRIC = "Gcell-updates/s (Yee cavity 384^3, FP32 fields + FP64 audit)"
+
+
+def heat_block_record(local, stream, peak, n=64, timesteps=1000, steps=5, warmup=3):
+    """The heat block of config 1 (n³ cells, Dirichlet 300 K faces, a 50 K Gaussian hot spot at a
+    seed-jittered point, dt at 0.9 of the limit) as an object of the default line: the plain f64 form
+    the configuration names and the FP32 form, each `steps` calls of `timesteps` audited timesteps
+    after `warmup` calls, L2 flushed before each call outside the events (the 64³ state fits in L2);
+    the FP32 field and books against the f64 run's after the same calls from the same start."""
+    import numpy as np
+    import torch
+
+    from pantometry_b200 import workloads as W
+
+    cfg = W.heat_block(n, steps=timesteps)
+    cells = n ** 3
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device=local)  # 256 MB, twice the L2
+
+    def run(precision, tol):
+        b = W.build_heat(cfg, precision=precision, device=local)
+        b.set_stream(stream.cuda_stream)
+        b.set_tolerance(tol)
+        dt = cfg["dt_fraction"] * b.max_stable_dt()
+        for _ in range(warmup):
+            assert b.step(dt, timesteps) is None
+        ms = 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            v = b.step(dt, timesteps)
+            assert v is None, v
+            end.record(stream)
+            torch.cuda.synchronize()
+            ms += start.elapsed_time(end)
+        return b, ms
+
+    b64, ms64 = run("f64", 1e-9)
+    b32, ms32 = run("f32", 1e-6)
+    kernel64, launches64 = b64.step_kernel(timesteps)
+    kernel32, _ = b32.step_kernel(timesteps)
+    l64, l32 = b64.ledger(), b32.ledger()
+    field_err = float(np.abs(b32.cells - b64.cells).max())
+    ledger_err = abs(l32["total"] - l64["total"]) / max(abs(l64["total"]), l64["scale"], 1e-300)
+    del b64, b32, flush
+    us64, us32 = ms64 * 1e3 / (steps * timesteps), ms32 * 1e3 / (steps * timesteps)
+    return {
+        "workload": f"heat_block {n}^3 cells, diffusivity 1e-4 m^2/s, dx 1 mm, dt 0.9 x the limit, Dirichlet 300 K "
+                    f"faces, {timesteps} audited timesteps per call, L2 flushed before each call",
+        "value": round(cells * timesteps * steps / (ms64 * 1e-3) / 1e9, 3), "unit": UNIT, "dtype": "f64",
+        "us_per_timestep": round(us64, 3), "grids_per_s": round(1e6 / us64, 1), "timed_calls": steps,
+        "kernel": kernel64, "gpu_launches": steps * launches64,
+        "fp32": {"value": round(cells * timesteps * steps / (ms32 * 1e-3) / 1e9, 3), "us_per_timestep": round(us32, 3),
+                 "kernel": kernel32},
+        "error_vs_f64": {"max_abs_kelvin": field_err, "ledger_rel": ledger_err,
+                         "after_timesteps": timesteps * (warmup + steps)},
+        "note": "state 4.2 MB (f64, both parities): L2-resident within a call, bound by the per-step grid wait",
+    }
 
 
 def ensemble_record(local, stream, peak, timesteps=2000, steps=2):
@@ -1499,7 +1558,7 @@ def main():
                     help="audited steps per CPU sample (hall 16, ensemble 8): about 10 s of one core")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-side-records", action="store_true",
-                    help="hall: leave out the cavity and ensemble objects of the default line")
+                    help="hall: leave out the cavity, ensemble and heat-block objects of the default line")
     args = ap.parse_args()
     if args.n is None:
         args.n = {"cavity": 384, "mix": 1024, "heat": 64}.get(args.workload, 256)
