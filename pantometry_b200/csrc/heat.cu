@@ -260,9 +260,15 @@ struct Heat : Handle {
     // The rate of the present state into the device books, where the films radiate: the step
     // kernels keep it from then on, step by step.
     pm_status refresh_rate() {
-        if (precision != PM_PLAIN_F64 || !state_dependent()) return PM_OK;
+        if (!state_dependent() || (precision != PM_PLAIN_F64 && !radiating_f32())) return PM_OK;
         std::vector<double> t(n());
-        PM_CUDA(cudaMemcpyAsync(t.data(), field[parity].p, n() * 8, cudaMemcpyDeviceToHost, stream()));
+        if (precision == PM_PLAIN_F64) {
+            PM_CUDA(cudaMemcpyAsync(t.data(), field[parity].p, n() * 8, cudaMemcpyDeviceToHost, stream()));
+        } else {  // the kelvin the FP32 deviations hold
+            if (!stage.p || stage.bytes < n() * 8) PM_CUDA(stage.alloc(n() * 8));
+            PM_CUDA(launch_heat_convert(nullptr, field[parity].as<float>(), reference, n(), 0, stage.as<double>(), stream()));
+            PM_CUDA(cudaMemcpyAsync(t.data(), stage.p, n() * 8, cudaMemcpyDeviceToHost, stream()));
+        }
         PM_CUDA(cudaStreamSynchronize(stream()));
         pm_status s = read_state();
         if (s != PM_OK) return s;
@@ -485,7 +491,12 @@ struct Heat : Handle {
         return a;
     }
 
-    bool tma_form() const { return precision == PM_FIELDS_F32 && uniform && wide && nx % 4 == 0 && tma_maps; }
+    bool tma_form() const {
+        return precision == PM_FIELDS_F32 && uniform && wide && nx % 4 == 0 && tma_maps && !state_dependent();
+    }
+    // FP32 blocks of one material whose films radiate and that leave no gaps: the one-cell FP32
+    // kernel, its limit following the state as the plain form's does
+    bool radiating_f32() const { return precision == PM_FIELDS_F32 && uniform && gaps.empty() && radiating(); }
 
     HeatTmaArgs tma_args(int par, double dt) const {
         const HeatF32Args f = f32_args(par, dt);
@@ -533,7 +544,12 @@ struct Heat : Handle {
             a.src = source.empty() ? nullptr : dsrc.as<double>();
         }
         a.dts = dt;
-        a.quads = uniform && nx % 4 == 0 && wide ? 1 : 0;
+        a.quads = uniform && nx % 4 == 0 && wide && !state_dependent() ? 1 : 0;
+        if (radiating_f32()) {  // the one-cell kernel, its face cells through the plain form's films
+            a.radiating = 1;
+            a.t0 = reference;
+            a.rad = plain_args(par, dt);
+        }
         const unsigned w = wave_of(a.quads ? kHeatF32Quad : kHeatF32);
         const int tx = a.quads ? nx / 4 : nx;  // the threads along a row
         a.tiles = make_tiles(tx, ny, nz, choose_zc(tx, ny, nz, w));
@@ -807,8 +823,8 @@ pm_status pm_heat_max_stable_dt(pm_heat* hp, double* seconds) {
     if (!seconds) return fail(PM_BAD_ARG, "null output");
     double rate;
     if (h->state_dependent()) {
-        if (h->precision != PM_PLAIN_F64)
-            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) and radiative gaps are on the plain f64 form only");
+        if (h->precision != PM_PLAIN_F64 && !h->radiating_f32())
+            return fail(PM_UNSUPPORTED, "radiative gaps, and radiating films on blocks of several materials, are on the plain f64 form only");
         pm_status s = h->read_state();  // the rate the last step (or the last change of state) left
         if (s != PM_OK) return s;
         rate = h->host_state->rate_now;
@@ -835,8 +851,8 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
     if (h->state_dependent()) {
         // the limit follows the state: the first step is checked here against the present
         // state's rate, every later one on the device against the rate its own state gives
-        if (h->precision != PM_PLAIN_F64)
-            return fail(PM_UNSUPPORTED, "radiating films (emissivity > 0) and radiative gaps are on the plain f64 form only");
+        if (h->precision != PM_PLAIN_F64 && !h->radiating_f32())
+            return fail(PM_UNSUPPORTED, "radiative gaps, and radiating films on blocks of several materials, are on the plain f64 form only");
         pm_status rs = h->read_state();
         if (rs != PM_OK) return rs;
         rate = h->host_state->rate_now;
@@ -966,7 +982,9 @@ pm_status pm_heat_step_kernel(pm_heat* hp, long long nsteps, char* name, int cap
     } else if (h->tma_form()) {
         k = "heat_tma_step (TMA-staged)";
     } else {
-        k = filled ? "heat_f32_step<filled>" : (h->nx % 4 == 0 && h->wide) ? "heat_f32_quad_step" : "heat_f32_step";
+        k = filled ? "heat_f32_step<filled>"
+            : (h->nx % 4 == 0 && h->wide && !h->state_dependent()) ? "heat_f32_quad_step"
+                                                                   : "heat_f32_step";
     }
     std::snprintf(name, (size_t)cap, "%s", k.c_str());
     if (launches) *launches = n;

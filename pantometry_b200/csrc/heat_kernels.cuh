@@ -631,6 +631,12 @@ struct HeatF32Args {
     DevState* st;
     double* partials;
     unsigned nblocks;
+    // Uniform blocks whose films radiate (heat_f32_step only): each face cell's film is the plain
+    // form's film_flux at its kelvin T0 + deviation, and its new rate joins the state's limit, both
+    // through `rad` (the plain form's film, conductance and limit parameters; no field is read)
+    int radiating;
+    double t0;
+    HeatPlainArgs rad;
 };
 
 // The books of an FP32 step, after its cells: the block's partials reduced in fixed order by the
@@ -651,13 +657,18 @@ __device__ __forceinline__ void heat_f32_books(const HeatF32Args& a, double (&ac
         st->part[1] = st->lost;
         st->part[2] = -st->supplied;
         audit_and_commit(st, total, scale);
+        if (a.radiating) {  // worst_rate_now of the state this step leaves (solid.rs:1148-1185)
+            const unsigned long long bits = atomicExch(&st->rate_bits, 0ull);
+            st->rate_now = bits ? fmax(a.rad.static_rate, __longlong_as_double((long long)bits)) : a.rad.static_rate;
+        }
     }
 }
 
 // Chosen form, z-marching like the plain form; neighbours in the plane come from L1/L2.
 template <bool FILLED>
 static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
-    if (a.st->violated) return;
+    if (a.st->violated || (a.radiating && heat_refused(a.rad))) return;
+    double rate = -1.0;  // radiating films: the largest rate of the new state
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const size_t plane = (size_t)nx * ny;
     double acc[FILLED ? 3 : 2] = {};
@@ -703,6 +714,10 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
                     if (((a.exposed >> 3) & 1) && !yh) shed += __ldg(a.film[3] + py) * (here + a.off[3]);
                     if (((a.exposed >> 4) & 1) && k == 0) shed += __ldg(a.film[4] + pz) * (here + a.off[4]);
                     if (((a.exposed >> 5) & 1) && k + 1 == nz) shed += __ldg(a.film[5] + pz) * (here + a.off[5]);
+                } else if (a.radiating) {
+                    // solid.rs:1192-1219 at the cell's kelvin, as dt · mobility · flux
+                    shed = (float)(a.rad.dts * a.rad.mobility * film_flux(a.rad, i, j, k, c, a.t0 + (double)here));
+                    col_shed += (double)shed;
                 } else {
                     if (((a.exposed >> 0) & 1) && !xl) shed += a.b[0] * (here + a.off[0]);
                     if (((a.exposed >> 1) & 1) && !xh) shed += a.b[1] * (here + a.off[1]);
@@ -732,6 +747,8 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
             } else {
                 nd = here + (a.a * s - shed);
                 acc[0] += (double)nd;
+                if (a.radiating && (edge_xy || k == 0 || k + 1 == nz))
+                    rate = fmax(rate, heat_cell_rate(a.rad, i, j, k, c, a.t0 + (double)nd));
             }
             a.dnew[c] = nd;
             below = here;
@@ -739,6 +756,7 @@ static __global__ void __launch_bounds__(256) heat_f32_step(HeatF32Args a) {
         }
         acc[1] += col_shed;
     }
+    if (a.radiating) heat_rate_publish(a.rad, rate);
     heat_f32_books(a, acc, FILLED);
 }
 

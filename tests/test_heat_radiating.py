@@ -1,4 +1,5 @@
-"""Radiating films (emissivity > 0) on the plain f64 path.
+"""Radiating films (emissivity > 0) on the plain f64 path, and on the FP32 form for blocks of one
+material.
 
 With ε > 0 a film's conductance depends on the temperature of the cell it cools: `film_flux` adds
 εσ·share·(T⁴ − T∞⁴) (solid.rs:1192-1219), and `worst_rate_now` takes each boundary cell's tangent
@@ -141,11 +142,55 @@ def test_radiating_refusal_falls_on_the_reference_step(calls):
 
 
 @pytest.mark.gpu
-def test_radiating_films_on_the_fp32_form_are_refused():
+def test_radiating_fp32_copper_cube_tracks_the_oracle_and_counts_every_joule():
+    """The FP32 form of the cooling cube (one material, no gaps): the one-cell FP32 kernel with each
+    face cell's film at its kelvin, 20 000 steps at 0.4 of the limit, within f32 rounding of the
+    oracle, the books holding what the film took."""
+    o, g = copper_cube_pair()
+    _, f = copper_cube_pair(precision="f32")
+    assert f.step_kernel(64)[0] == "heat_f32_step"
+    assert abs(f.max_stable_dt() - o.max_stable_dt()) <= 1e-6 * o.max_stable_dt()
+    dt = 0.4 * o.max_stable_dt()
+    f.set_tolerance(1e-6)
+    opening = f.ledger()["total"]
+    assert o.step(dt, 20000) is None
+    assert f.step(dt, 20000) is None
+    assert np.abs(f.cells - o.cells).max() < 1e-3  # kelvin, from 573 K down by tens of kelvin
+    lf, lo = f.ledger(), o.ledger()
+    assert lf["parts"][1] > 0.0 and abs(lf["parts"][1] - lo["lost"]) <= 1e-4 * lo["lost"]
+    # the books: every step audited at 1e-6; over 20 000 steps the f32 rounding of each cell's
+    # deviation (tens of kelvin, 27 cells) leaves the total a few 1e-5 of the scale from the opening
+    assert abs(lf["total"] - opening) <= 1e-4 * lf["scale"]
+    assert abs(f.max_stable_dt() - o.max_stable_dt()) <= 1e-6 * o.max_stable_dt()
+
+
+@pytest.mark.gpu
+def test_radiating_fp32_limit_follows_the_state_and_refuses_on_the_reference_step():
+    o, g = slab_pair(precision="f32")
+    assert abs(g.max_stable_dt() - o.max_stable_dt()) <= 1e-6 * o.max_stable_dt()
+    dt = 0.5 * o.max_stable_dt()
+    for _ in range(3):
+        assert o.step(dt, 5) is None
+        assert g.step(dt, 5) is None
+        assert np.abs(g.cells - o.cells).max() < 1e-3
+        assert abs(g.max_stable_dt() - o.max_stable_dt()) <= 1e-6 * o.max_stable_dt()
+    # at 0.95 of the opening limit the state's own limit overtakes the step on the fourth step
+    o, g = slab_pair(precision="f32")
+    dt = 0.95 * o.max_stable_dt()
+    v = g.step(dt, 100)
+    assert v is not None and v["quantity"] == "Fourier number" and v["step"] == 4
+    assert g.ledger()["steps"] == 3
+
+
+@pytest.mark.gpu
+def test_radiating_fp32_refusals_that_remain():
+    """Blocks of several materials with radiating films stay on the plain f64 form."""
     from pantometry_b200._native import NativeError
 
-    _, g = copper_cube_pair(precision="f32")
-    with pytest.raises(NativeError, match="plain f64"):
-        g.max_stable_dt()
+    counts, dx = (6, 5, 5), 5e-2
+    mask = np.zeros(int(np.prod(counts)), dtype=np.uint8)
+    mask[:30] = 1
+    _, g = heat_pair(counts, dx, CERAMIC, 300.0, films=[(0, 300.0, 10.0, 0.0625)], precision="f32",
+                     fill=(mask, COPPER))
     with pytest.raises(NativeError, match="plain f64"):
         g.step(1e-3, 1)
