@@ -145,7 +145,8 @@ template <int P, int S, bool MEDIA, int MINB>
 static cudaError_t launch_yee_tma_shape(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, const YeeNearArgs& n,
                                        cudaStream_t s) {
     const int smem = (int)yee_tma_smem_bytes_for<P, MEDIA>(S);
-    auto k = a.solid ? yee_tma_step<P, S, true, MEDIA, MINB> : yee_tma_step<P, S, false, MEDIA, MINB>;
+    auto k = a.solid ? (a.wall_split ? yee_tma_step<P, S, true, MEDIA, MINB, true> : yee_tma_step<P, S, true, MEDIA, MINB, false>)
+                     : (a.wall_split ? yee_tma_step<P, S, false, MEDIA, MINB, true> : yee_tma_step<P, S, false, MEDIA, MINB, false>);
     return launch_smem(k, a.nblocks, tile_block(), smem, s, a, L, m, n);
 }
 cudaError_t launch_yee_tma(const YeeStepArgs<float>& a, unsigned L, const YeeMaps& m, int shape, cudaStream_t s,
@@ -165,8 +166,8 @@ template <int P, int S, bool MEDIA, int MINB>
 static int yee_tma_occupancy() {
     int n = 0;
     const size_t smem = yee_tma_smem_bytes_for<P, MEDIA>(S);
-    if (allow_smem(yee_tma_step<P, S, false, MEDIA, MINB>, (int)smem) != cudaSuccess) return 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<P, S, false, MEDIA, MINB>, 256, smem) != cudaSuccess)
+    if (allow_smem(yee_tma_step<P, S, false, MEDIA, MINB, false>, (int)smem) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, yee_tma_step<P, S, false, MEDIA, MINB, false>, 256, smem) != cudaSuccess)
         return 1;
     return n > 0 ? n : 1;
 }

@@ -227,7 +227,7 @@ __device__ __forceinline__ void yee_tma_wall_pass(const YeeStepArgs<float>& a, u
     }
 }
 
-template <int P, int S, bool SOLID, bool MEDIA, int MINB>
+template <int P, int S, bool SOLID, bool MEDIA, int MINB, bool SPLIT>
 static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<float> a, unsigned L,
                                                              const __grid_constant__ YeeMaps m,
                                                              const __grid_constant__ YeeNearArgs nr) {
@@ -299,9 +299,11 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
         const float(*GY)[8][32] = reinterpret_cast<const float(*)[8][32]>(sb + Lay::GY);
         const float(*GZ)[8][32] = reinterpret_cast<const float(*)[8][32]>(sb + Lay::GZ);
         const int i = cc.x0 + tx, j = cc.y0 + ty;
-        const bool in_x = i <= nx, in_y = j <= ny;
+        // whether the lattice position lies in each component's extent along x and y; with the wall
+        // split (SPLIT: a.wall_split) the tiles hold i < nx and j < ny only, so every test is true
+        const bool in_x = SPLIT || i <= nx, in_y = SPLIT || j <= ny, bx = SPLIT || i < nx, by = SPLIT || j < ny;
         // node-centred half weights of the boundary samples (cavity.rs:766-772)
-        const float hi = (i == 0 || i == nx) ? 0.5f : 1.0f, hj = (j == 0 || j == ny) ? 0.5f : 1.0f;
+        const float hi = (i == 0 || (!SPLIT && i == nx)) ? 0.5f : 1.0f, hj = (j == 0 || (!SPLIT && j == ny)) ? 0.5f : 1.0f;
         // the column crosses the f64 near-field box (nb_w = 0: no box, never)
         const bool box_xy = (unsigned)(i - a.nb_x0) < (unsigned)a.nb_w && (unsigned)(j - a.nb_y0) < (unsigned)a.nb_w;
         // this stage's energy products of the thread's cells per component, the z weight in each:
@@ -322,13 +324,13 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
             // padding, or the fill outside the lattice) the uniform gain, never read as a value
             float gx = gain0, gy = gain0, gz = gain0;
             if constexpr (MEDIA) {
-                gx = (i < nx && in_y) ? GX[h][ty][tx] : gain0;
-                gy = (in_x && j < ny) ? GY[h][ty][tx] : gain0;
+                gx = (bx && in_y) ? GX[h][ty][tx] : gain0;
+                gy = (in_x && by) ? GY[h][ty][tx] : gain0;
                 gz = (in_x && in_y && zin) ? GZ[h][ty][tx] : gain0;
             }
             YeeHp<float>* hq = hp + hpar;
             // ---- 1. H⁺ (cavity.rs:1346-1379) on own faces
-            const bool fx = in_x && j < ny && zin, fy = i < nx && in_y && zin, fz = i < nx && j < ny;
+            const bool fx = in_x && by && zin, fy = bx && in_y && zin, fz = bx && by;
             const float wx = HX[h][ty + 1][tx], wy = HY[h][ty][tx + 4], wz = HZ[h][ty + 1][tx + 4];
             const float ex0 = EX[h][ty + 1][tx + 4], ey0 = EY[h][ty + 1][tx + 4], ez0 = EZ[h][ty + 1][tx + 4];
             const float hxn = yee_face_f32(wx, ch, EZ[h][ty + 2][tx + 4], ez0, EY[h + 1][ty + 1][tx + 4], ey0);
@@ -378,7 +380,7 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
             // ---- 2. Eⁿ⁺¹ on own edges (cavity.rs:1383-1452): interior by the semi-implicit update,
             // conducting walls 0 (cavity.rs:1239-1293), edges touching a solid cell 0 (cavity.rs:304-331)
             if (compute) {
-                const bool ix = i >= 1 && i < nx, iy = j >= 1 && j < ny, iz = k >= 1 && k < nz;
+                const bool ix = i >= 1 && bx, iy = j >= 1 && by, iz = k >= 1 && k < nz;
                 const float cex = (hzn - hq->hz[ty][tx + 1]) - (hyn - hy_below);  // own H⁺ from registers
                 const float cey = (hxn - hx_below) - (hzn - hq->hz[ty + 1][tx]);
                 const float cez = (hyn - hq->hy[ty][tx]) - (hxn - hq->hx[ty][tx]);
@@ -398,8 +400,8 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
                 if (lossy && !inbox) {
                     const double mx = 0.5 * ((double)ex0 + (double)vx), my = 0.5 * ((double)ey0 + (double)vy),
                                  mz = 0.5 * ((double)ez0 + (double)vz);
-                    acc[2] += (lx && i < nx && in_y) ? sig0 * mx * mx * dt * a.volume : 0.0;
-                    acc[2] += (ly && in_x && j < ny) ? sig0 * my * my * dt * a.volume : 0.0;
+                    acc[2] += (lx && bx && in_y) ? sig0 * mx * mx * dt * a.volume : 0.0;
+                    acc[2] += (ly && in_x && by) ? sig0 * my * my * dt * a.volume : 0.0;
                     acc[2] += (lz && in_x && in_y && zin) ? sig0 * mz * mz * dt * a.volume : 0.0;
                 }
                 if constexpr (SOLID) {
@@ -407,8 +409,8 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
                     if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j, j, k - 1, k)) vy = 0.0f;
                     if (touches_solid(a.solid, nx, ny, nz, i - 1, i, j - 1, j, k, k)) vz = 0.0f;
                 }
-                if (i < nx && in_y) a.neu[0][n] = vx;
-                if (in_x && j < ny) a.neu[1][n] = vy;
+                if (bx && in_y) a.neu[0][n] = vx;
+                if (in_x && by) a.neu[1][n] = vy;
                 if (in_x && in_y && zin) a.neu[2][n] = vz;
             }
             hx_below = hxn;
@@ -420,7 +422,7 @@ static __global__ void __launch_bounds__(256, MINB) yee_tma_step(YeeStepArgs<flo
         yee_tma_next(cc, T, P);
         ++it;
     }
-    if (a.wall_split && !timed_out) {
+    if (SPLIT && !timed_out) {
         float es = 0.0f, ms = 0.0f;
         yee_tma_wall_pass<MEDIA>(a, L, (long long)blockIdx.x * 256 + tid, (long long)gridDim.x * 256, es, ms);
         acc[0] += (double)es;
