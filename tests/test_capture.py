@@ -191,3 +191,82 @@ def test_capture_draws_placed_fields_only():
     panel = frame["panels"][0]
     assert panel["unit"] == "Pa" and panel["grid"] == (5, 4, 3) and panel["values"].shape == (60,)
     assert np.array_equal(panel["values"], hall.sample(extent["min"], extent["max"], extent["samples"]))
+
+
+def _py_heat_at(cells, void, counts, dx, p):
+    """solid.rs:2045-2104 restated line by line in Python, for the oracle's sampler to be checked."""
+    nx, ny, nz = counts
+    q = [p[a] / dx - 0.5 for a in range(3)]
+    if any(math.isnan(v) for v in q):
+        return math.nan
+
+    def axis(v, n):
+        last = max(n - 1, 0)
+        if v <= 0.0:
+            return 0, 0.0
+        if v >= last:
+            return last, 0.0
+        i = math.floor(v)
+        return int(i), v - i
+
+    (i, fx), (j, fy), (k, fz) = axis(q[0], nx), axis(q[1], ny), axis(q[2], nz)
+
+    def nearest(v, n):  # f64::round: half away from zero
+        r = math.floor(abs(v) + 0.5) * (1 if v >= 0 else -1)
+        return min(int(max(r, 0.0)), max(n - 1, 0))
+
+    if void[nearest(q[0], nx) + nx * (nearest(q[1], ny) + ny * nearest(q[2], nz))]:
+        return math.nan
+    i1, j1, k1 = min(i + 1, nx - 1), min(j + 1, ny - 1), min(k + 1, nz - 1)
+    s = w_sum = 0.0
+    for a, wa in ((i, 1.0 - fx), (i1, fx)):
+        for b, wb in ((j, 1.0 - fy), (j1, fy)):
+            for c, wc in ((k, 1.0 - fz), (k1, fz)):
+                w = wa * wb * wc
+                at = a + nx * (b + ny * c)
+                if w > 0.0 and not void[at]:
+                    s += w * cells[at]
+                    w_sum += w
+    return s / w_sum if w_sum > 0.0 else math.nan
+
+
+def test_oracle_heat_sampler_against_a_python_restatement():
+    counts, dx = (7, 6, 5), 1e-3
+    void = np.zeros(int(np.prod(counts)), dtype=np.uint8)
+    void[np.random.default_rng(9).random(void.size) < 0.2] = 1
+    o, cells = heat_oracle(counts, dx, void=void)
+    rng = np.random.default_rng(11)
+    for _ in range(60):
+        p = rng.uniform(-1e-3, 8e-3, 3)
+        got = o.sample(p, p, (1, 1, 1))[0]
+        want = _py_heat_at(cells, void, counts, dx, p)
+        assert (math.isnan(got) and math.isnan(want)) or got == want, (p, got, want)
+
+
+def test_oracle_hall_sampler_against_a_python_restatement():
+    h = oracle.Hall(0.01, 0.008, 0.006, 7, 343.0, 1.2)
+    nx, ny, nz = h.nodes
+    dx = 0.01 / (nx - 1)
+    pr = np.random.default_rng(4).uniform(-1.0, 1.0, nx * ny * nz)
+    h.release(pr)
+
+    def clamp(v, n):
+        if math.isnan(v) or v <= 0.0:
+            return 0, 0.0
+        if v >= n - 1:
+            return n - 1, 0.0
+        i = math.floor(v)
+        return int(i), v - i
+
+    def lerp(a, b, t):
+        return a * (1.0 - t) + b * t
+
+    rng = np.random.default_rng(12)
+    for _ in range(60):
+        p = rng.uniform(-2e-3, 0.012, 3)
+        (i, fx), (j, fy), (k, fz) = clamp(p[0] / dx, nx), clamp(p[1] / dx, ny), clamp(p[2] / dx, nz)
+        i1, j1, k1 = min(i + 1, nx - 1), min(j + 1, ny - 1), min(k + 1, nz - 1)
+        g = lambda a, b, c: pr[a + nx * (b + ny * c)]  # noqa: E731
+        z0 = lerp(lerp(g(i, j, k), g(i1, j, k), fx), lerp(g(i, j1, k), g(i1, j1, k), fx), fy)
+        z1 = lerp(lerp(g(i, j, k1), g(i1, j, k1), fx), lerp(g(i, j1, k1), g(i1, j1, k1), fx), fy)
+        assert h.sample(p, p, (1, 1, 1))[0] == lerp(z0, z1, fz)
