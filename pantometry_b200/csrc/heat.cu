@@ -71,10 +71,6 @@ struct Heat : Handle {
     unsigned wait_budget = 1u << 24;  // polls per grid-barrier wait, about 100 ns apart
     static constexpr size_t kPersistMaxCells = size_t(1) << 22;
     static constexpr int kPersistChunk = 1024;  // steps per cooperative launch
-#ifndef PM_PERSIST_MAX_WORKERS
-#define PM_PERSIST_MAX_WORKERS 1000000
-#endif
-    static constexpr long long kPersistMaxWorkers = PM_PERSIST_MAX_WORKERS;  // blocks with tiles, at most
     double saved_lost = 0.0, saved_supplied = 0.0;
 
     size_t n() const { return (size_t)nx * ny * nz; }
@@ -581,8 +577,7 @@ struct Heat : Handle {
         if (wave < 2) return fail(PM_UNSUPPORTED, "the many-step heat kernel needs two co-resident blocks");
         const int tx = nx / (plain ? 2 : 4);
         int zc = 1;
-        const long long cap = std::min<long long>(wave - 1, kPersistMaxWorkers);
-        while (zc < nz && make_tiles(tx, ny, nz, zc, rows).ntiles > cap) zc *= 2;
+        while (zc < nz && make_tiles(tx, ny, nz, zc, rows).ntiles > (long long)(wave - 1)) zc *= 2;
         const Tiles tiles = make_tiles(tx, ny, nz, zc, rows);
         const unsigned nblocks = 1u + (unsigned)std::min<long long>(tiles.ntiles, (long long)(wave - 1));
         int par = parity;
