@@ -265,6 +265,12 @@ pm_status pm_room_step(pm_room* r, double dt, long long nsteps, pm_violation* ou
 pm_status pm_room_ledger(pm_room* r, pm_ledger* out);
 /* Any pointer may be NULL: p (nx ny), p_prev (nx ny), vx ((nx-1) ny), vy (nx (ny-1)). */
 pm_status pm_room_download(pm_room* r, double* p, double* p_prev, double* vx, double* vy);
+/* ScalarField::at (room.rs:587-601), the view scene::capture (crates/pantometry-scene/src/lib.rs:
+ * 347-420) takes of a room: pressure bilinear between the nodes round each point's (x, y), clamped
+ * at the walls, a NaN coordinate reading node 0 along its axis, z not read. Points as for
+ * pm_hall_sample. */
+pm_status pm_room_sample(pm_room* r, const double lo[3], const double hi[3], const int samples[3], double* out,
+                         size_t n);
 /* Domain::checkpoint / restore (room.rs:484-505). */
 pm_status pm_room_checkpoint(pm_room* r);
 pm_status pm_room_restore(pm_room* r);
@@ -331,6 +337,11 @@ pm_status pm_bar_create(const pm_bar_desc* desc, pm_bar** out);
 /* Set / read every cell's temperature (kelvin). An upload re-takes the books from the new state. */
 pm_status pm_bar_upload(pm_bar* b, const double* kelvin, size_t n);
 pm_status pm_bar_download(pm_bar* b, double* kelvin, size_t n);
+/* ScalarField::at (lib.rs:736-751), the view scene::capture takes of a bar: kelvin linear between
+ * cell centres along x, the end cell's value beyond either centre and for a NaN x, y and z not
+ * read. Points as for pm_hall_sample. */
+pm_status pm_bar_sample(pm_bar* b, const double lo[3], const double hi[3], const int samples[3], double* out,
+                        size_t n);
 /* The heat the next step takes from the bus, handed in by the caller (lib.rs:590-606): lumped
  * joules into the first cell (`take_share` of HEAT), joules per cell (a flux over `exposing`'s
  * faces). Both are booked as taken from the bus. */

@@ -98,6 +98,8 @@ def _declare(L):
         "or_heat_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_hall_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_yee_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
+        "or_room_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
+        "or_bar_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_heat_dissipating": (None, [p, d, C.c_void_p]),
         "or_heat_generated_power": (d, [p]),
         "or_heat_generated_energy": (d, [p]),
@@ -422,6 +424,8 @@ class Room(_Box):
     """`Room` restated (crates/pantometry-acoustic/src/room.rs): `new`, `released_from`, `step`,
     `ledger`, `checkpoint`/`restore`. Pressure row-major (i + nx·j); vx (nx−1)·ny, vy nx·(ny−1)."""
 
+    _sampler = "or_room_sample"
+
     def __init__(self, width, height, across, depth=1.0, density=1.204, speed=343.0, name="room"):
         L = lib()
         self._h = L.or_room_new(name.encode(), width, height, across, depth, density, speed)
@@ -552,6 +556,8 @@ class Bar(_Box):
     """`Bar1D` restated (crates/pantometry-thermal/src/lib.rs:425-660): insulated explicit
     conduction; the heat a step takes from the bus is handed in first (`absorb`: lumped, into
     the first cell; `deposit`: per cell)."""
+
+    _sampler = "or_bar_sample"
 
     def __init__(self, cells, dx, area, density, conductivity, specific_heat, initial, thermal=True, name="bar"):
         L = lib()

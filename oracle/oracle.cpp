@@ -2090,6 +2090,49 @@ void or_hall_sample(void* p, const double* lo, const double* hi, const int* n, d
     });
 }
 
+// Room::at (room.rs:587-601) with its clamp_index (room.rs:739-749): bilinear between the four nodes
+// round (x, y), clamped at the walls; each coordinate is clamped on its own, a NaN one to node 0.
+void or_room_sample(void* p, const double* lo, const double* hi, const int* n, double* out) {
+    Room* r = (Room*)p;
+    const int nx = r->nx, ny = r->ny;
+    or_sample_grid(lo, hi, n, out, [&](const double* pt) {
+        auto clamp_index = [](double q, int cnt, int& i, double& f) {
+            if (std::isnan(q) || q <= 0.0) { i = 0; f = 0.0; return; }
+            const double last = (double)(cnt - 1);
+            if (q >= last) { i = cnt - 1; f = 0.0; return; }
+            const double fl = std::floor(q);
+            i = (int)fl;
+            f = q - fl;
+        };
+        int i, j;
+        double fx, fy;
+        clamp_index(pt[0] / r->dx, nx, i, fx);
+        clamp_index(pt[1] / r->dx, ny, j, fy);
+        const int i1 = std::min(i + 1, nx - 1), j1 = std::min(j + 1, ny - 1);
+        const double p00 = r->p[(size_t)j * nx + i], p10 = r->p[(size_t)j * nx + i1];
+        const double p01 = r->p[(size_t)j1 * nx + i], p11 = r->p[(size_t)j1 * nx + i1];
+        const double bottom = p00 * (1.0 - fx) + p10 * fx;
+        const double top = p01 * (1.0 - fx) + p11 * fx;
+        return bottom * (1.0 - fy) + top * fy;
+    });
+}
+
+// Bar1D::at (crates/pantometry-thermal/src/lib.rs:736-751): linear between cell centres along x;
+// the end cell's value beyond either centre and for a NaN x.
+void or_bar_sample(void* p, const double* lo, const double* hi, const int* n, double* out) {
+    Bar* b = (Bar*)p;
+    const int last = (int)b->cells.size() - 1;
+    or_sample_grid(lo, hi, n, out, [&](const double* pt) {
+        const double u = pt[0] / b->dx - 0.5;
+        if (std::isnan(u) || u <= 0.0) return b->cells[0];
+        if (u >= (double)last) return b->cells[last];
+        const double fl = std::floor(u);
+        const int i = (int)fl;
+        const double f = u - fl;
+        return b->cells[i] * (1.0 - f) + b->cells[i + 1] * f;
+    });
+}
+
 // Cavity::at (cavity.rs:197-206) over electric_at (cavity.rs:735-742): |E| of the edges of the cell
 // the point falls in, nearest cell, clamped; NaN for a NaN point.
 void or_yee_sample(void* p, const double* lo, const double* hi, const int* n, double* out) {

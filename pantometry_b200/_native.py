@@ -208,6 +208,7 @@ SIGNATURES = {
     "pm_room_step": (_st, [_p, _d, _ll, _vp]),
     "pm_room_ledger": (_st, [_p, _lp]),
     "pm_room_download": (_st, [_p, _dp, _dp, _dp, _dp]),
+    "pm_room_sample": (_st, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t]),
     "pm_room_checkpoint": (_st, [_p]),
     "pm_room_restore": (_st, [_p]),
     "pm_room_set_stream": (_st, [_p, _p]),
@@ -228,6 +229,7 @@ SIGNATURES = {
     "pm_bar_create": (_st, [C.POINTER(BarDesc), C.POINTER(_p)]),
     "pm_bar_upload": (_st, [_p, _dp, _sz]),
     "pm_bar_download": (_st, [_p, _dp, _sz]),
+    "pm_bar_sample": (_st, [_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t]),
     "pm_bar_absorb": (_st, [_p, _d]),
     "pm_bar_deposit": (_st, [_p, _dp, _sz]),
     "pm_bar_max_stable_dt": (_st, [_p, _dp]),

@@ -145,6 +145,21 @@ pm_status pm_bar_download(pm_bar* bp, double* kelvin, size_t n) {
     return PM_OK;
 }
 
+pm_status pm_bar_sample(pm_bar* bp, const double* lo, const double* hi, const int* samples, double* out, size_t n) {
+    Bar* b = reinterpret_cast<Bar*>(bp);
+    BAR_GUARD(b);
+    SampleGrid g{};
+    pm_status s = sample_grid_of(lo, hi, samples, out, n, g);
+    if (s != PM_OK) return s;
+    g.dx = b->dx;
+    g.nx = b->n; g.ny = 1; g.nz = 1;
+    return run_sample(b, out, n, [&](double* dev, cudaStream_t st) {
+        return b->precision == PM_PLAIN_F64
+                   ? launch_bar_sample<double>(g, b->field[b->parity].as<double>(), 0.0, dev, st)
+                   : launch_bar_sample<float>(g, b->field[b->parity].as<float>(), b->reference, dev, st);
+    });
+}
+
 pm_status pm_bar_absorb(pm_bar* bp, double joules) {
     Bar* b = reinterpret_cast<Bar*>(bp);
     BAR_GUARD(b);

@@ -92,12 +92,17 @@ cudaError_t launch_heat_tma(const HeatTmaArgs& a, const CUtensorMap& map, cudaSt
 bool heat_tma_map(CUtensorMap* map, void* base, int nx, int ny, int nz);
 cudaError_t launch_heat_measure_f32(const HeatMeasureArgs& a, cudaStream_t s);
 // scene::capture's sampling of a field over an extent's grid (sample_kernels.cuh), into `out` on
-// the device: Solid3D (kelvin, or FP32 deviations with t0 added), Hall pressure, Cavity |E|.
+// the device: Solid3D and Bar1D (kelvin, or FP32 deviations with t0 added), Hall and Room
+// pressure, Cavity |E|.
 template <typename Real>
 cudaError_t launch_heat_sample(const SampleGrid& g, const Real* cells, double t0, const uint8_t* vd, double* out,
                                cudaStream_t s);
 template <typename Real>
 cudaError_t launch_hall_sample(const SampleGrid& g, const Real* p, double* out, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_room_sample(const SampleGrid& g, const Real* p, double* out, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_bar_sample(const SampleGrid& g, const Real* cells, double t0, double* out, cudaStream_t s);
 template <typename Real>
 cudaError_t launch_yee_sample(const SampleGrid& g, const Real* ex, const Real* ey, const Real* ez, uint3 rx, uint3 ry,
                               double* out, cudaStream_t s);

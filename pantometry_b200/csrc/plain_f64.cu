@@ -161,10 +161,24 @@ cudaError_t launch_yee_sample(const SampleGrid& g, const Real* ex, const Real* e
     yee_sample<Real><<<sample_blocks(g), 256, 0, s>>>(g, ex, ey, ez, rx, ry, out);
     return cudaGetLastError();
 }
+template <typename Real>
+cudaError_t launch_room_sample(const SampleGrid& g, const Real* p, double* out, cudaStream_t s) {
+    room_sample<Real><<<sample_blocks(g), 256, 0, s>>>(g, p, out);
+    return cudaGetLastError();
+}
+template <typename Real>
+cudaError_t launch_bar_sample(const SampleGrid& g, const Real* cells, double t0, double* out, cudaStream_t s) {
+    bar_sample<Real><<<sample_blocks(g), 256, 0, s>>>(g, cells, t0, out);
+    return cudaGetLastError();
+}
 template cudaError_t launch_heat_sample<double>(const SampleGrid&, const double*, double, const uint8_t*, double*, cudaStream_t);
 template cudaError_t launch_heat_sample<float>(const SampleGrid&, const float*, double, const uint8_t*, double*, cudaStream_t);
 template cudaError_t launch_hall_sample<double>(const SampleGrid&, const double*, double*, cudaStream_t);
 template cudaError_t launch_hall_sample<float>(const SampleGrid&, const float*, double*, cudaStream_t);
+template cudaError_t launch_room_sample<double>(const SampleGrid&, const double*, double*, cudaStream_t);
+template cudaError_t launch_room_sample<float>(const SampleGrid&, const float*, double*, cudaStream_t);
+template cudaError_t launch_bar_sample<double>(const SampleGrid&, const double*, double, double*, cudaStream_t);
+template cudaError_t launch_bar_sample<float>(const SampleGrid&, const float*, double, double*, cudaStream_t);
 template cudaError_t launch_yee_sample<double>(const SampleGrid&, const double*, const double*, const double*, uint3, uint3,
                                                double*, cudaStream_t);
 template cudaError_t launch_yee_sample<float>(const SampleGrid&, const float*, const float*, const float*, uint3, uint3,

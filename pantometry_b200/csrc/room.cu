@@ -261,6 +261,20 @@ pm_status pm_room_download(pm_room* rp, double* pr, double* pp, double* vx, doub
     return r->get(r->vy[par], vy, r->nvy());
 }
 
+pm_status pm_room_sample(pm_room* rp, const double* lo, const double* hi, const int* samples, double* out, size_t n) {
+    Room* r = reinterpret_cast<Room*>(rp);
+    ROOM_GUARD(r);
+    SampleGrid g{};
+    pm_status s = sample_grid_of(lo, hi, samples, out, n, g);
+    if (s != PM_OK) return s;
+    g.dx = r->dx;
+    g.nx = r->nx; g.ny = r->ny; g.nz = 1;
+    return run_sample(r, out, n, [&](double* dev, cudaStream_t st) {
+        return r->precision == PM_PLAIN_F64 ? launch_room_sample<double>(g, r->p[r->parity].as<double>(), dev, st)
+                                            : launch_room_sample<float>(g, r->p[r->parity].as<float>(), dev, st);
+    });
+}
+
 pm_status pm_room_checkpoint(pm_room* rp) {
     Room* r = reinterpret_cast<Room*>(rp);
     ROOM_GUARD(r);

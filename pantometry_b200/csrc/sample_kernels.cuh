@@ -120,6 +120,63 @@ static __global__ void hall_sample(const SampleGrid g, const Real* __restrict__ 
     }
 }
 
+// Room::at (room.rs:587-601) with its clamp_index (room.rs:739-749): bilinear between the four nodes
+// round the point's (x, y), clamped at the walls, a NaN coordinate reading node 0 along its axis;
+// z is not read. Pressure sits at i + nx·j.
+__device__ __forceinline__ void clamp_node(double q, int n, int& i, double& f) {
+    if (isnan(q) || q <= 0.0) { i = 0; f = 0.0; }
+    else if (q >= (double)(n - 1)) { i = n - 1; f = 0.0; }
+    else { const double fl = floor(q); i = (int)fl; f = q - fl; }
+}
+
+template <typename Real>
+static __global__ void room_sample(const SampleGrid g, const Real* __restrict__ p, double* __restrict__ out) {
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    const int nx = g.nx, ny = g.ny;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < total; r += (long long)gridDim.x * blockDim.x) {
+        double pt[3];
+        sample_point(g, r, pt);
+        int i, j;
+        double fx, fy;
+        clamp_node(pt[0] / g.dx, nx, i, fx);
+        clamp_node(pt[1] / g.dx, ny, j, fy);
+        const int i1 = min(i + 1, nx - 1), j1 = min(j + 1, ny - 1);
+        const double p00 = (double)p[(size_t)j * nx + i], p10 = (double)p[(size_t)j * nx + i1];
+        const double p01 = (double)p[(size_t)j1 * nx + i], p11 = (double)p[(size_t)j1 * nx + i1];
+        const double bottom = p00 * (1.0 - fx) + p10 * fx;
+        const double top = p01 * (1.0 - fx) + p11 * fx;
+        out[r] = bottom * (1.0 - fy) + top * fy;
+    }
+}
+
+// Bar1D::at (crates/pantometry-thermal/src/lib.rs:736-751): linear between cell centres along x,
+// the end cell's value beyond either centre and for a NaN x; y and z are not read. The FP32 form
+// adds `t0` to its stored deviations; the f64 form reads kelvin as stored.
+template <typename Real>
+static __global__ void bar_sample(const SampleGrid g, const Real* __restrict__ cells, double t0, double* __restrict__ out) {
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    const int last = g.nx - 1;
+    auto kelvin = [&](int c) {
+        const double v = (double)cells[c];
+        return sizeof(Real) == 8 ? v : v + t0;
+    };
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < total; r += (long long)gridDim.x * blockDim.x) {
+        double pt[3];
+        sample_point(g, r, pt);
+        const double u = pt[0] / g.dx - 0.5;
+        if (isnan(u) || u <= 0.0) {
+            out[r] = kelvin(0);
+        } else if (u >= (double)last) {
+            out[r] = kelvin(last);
+        } else {
+            const double fl = floor(u);
+            const int i = (int)fl;
+            const double f = u - fl;
+            out[r] = kelvin(i) * (1.0 - f) + kelvin(i + 1) * f;
+        }
+    }
+}
+
 // Cavity::at (cavity.rs:197-206) over electric_at (cavity.rs:735-742): |E| of the edges of the cell
 // the point falls in (nearest cell, clamped), NaN for a NaN point. Component q of E sits at
 // i + rx[q]·(j + ry[q]·k): the reference layout's extents, or the padded lattice's pitch.

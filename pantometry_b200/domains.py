@@ -218,7 +218,7 @@ class Solid3D(_Domain, _Field):
         N.check(self._lib.pm_heat_absorb(self._h, float(joules)))
 
 
-class Bar(_Domain):
+class Bar(_Domain, _Field):
     """`Bar1D` (crates/pantometry-thermal/src/lib.rs:425-660) on the GPU: insulated conduction along a
     bar. `absorb` (lumped, into the first cell) and `deposit` (per cell) hand it the heat its next
     step takes from the bus."""
@@ -349,7 +349,7 @@ class Hall(_Domain, _Field):
         return out
 
 
-class Room(_Domain):
+class Room(_Domain, _Field):
     """`Room` (crates/pantometry-acoustic/src/room.rs) on the GPU: the two-dimensional hall."""
 
     _destroy = "pm_room_destroy"

@@ -20,7 +20,7 @@ import math
 
 import numpy as np
 
-from .domains import Cavity, Hall, Room, Solid3D
+from .domains import Bar, Cavity, Hall, Room, Solid3D
 
 # substance.rs:362-373 (`Substance::aluminium_6061`; g/cm³ × 1e3, units lib.rs:751-753) and
 # substance.rs:336-347 (`Substance::borosilicate_crown`), the catalogue names a scene gives them
@@ -189,7 +189,7 @@ def run(scene, domain):
 
 
 # ScalarField::unit of each field domain (solid.rs:2030-2032, hall.rs:586-588, cavity.rs:191-193)
-UNITS = {Solid3D: "K", Hall: "Pa", Cavity: "V/m"}
+UNITS = {Solid3D: "K", Bar: "K", Hall: "Pa", Room: "Pa", Cavity: "V/m"}
 
 
 def capture(domains, placed, time_s=0.0):

@@ -270,3 +270,160 @@ def test_oracle_hall_sampler_against_a_python_restatement():
         z0 = lerp(lerp(g(i, j, k), g(i1, j, k), fx), lerp(g(i, j1, k), g(i1, j1, k), fx), fy)
         z1 = lerp(lerp(g(i, j, k1), g(i1, j, k1), fx), lerp(g(i, j1, k1), g(i1, j1, k1), fx), fy)
         assert h.sample(p, p, (1, 1, 1))[0] == lerp(z0, z1, fz)
+
+
+def room_oracle(seed=6):
+    r = oracle.Room(0.011, 0.007, 12)
+    pr = np.random.default_rng(seed).uniform(-1.0, 1.0, r.n)
+    r.release(pr)
+    return r, pr
+
+
+def test_room_samples_on_nodes_are_the_pressures_and_ignore_depth():
+    """room.rs:587-601: a sample on a node is that node's pressure, halfway between two nodes the mean
+    of the two; z is not read; each NaN coordinate is clamped to node 0 along its own axis."""
+    r, pr = room_oracle()
+    nx, ny = r.cells
+    dx = r.dx
+    got = r.sample((0.0, 0.0, 0.3), ((nx - 1) * dx, (ny - 1) * dx, 0.3), (nx, ny, 1))
+    assert np.allclose(got, pr, rtol=0, atol=1e-14)  # lo + (hi − lo)·f lands on a node to its rounding
+    g = pr.reshape(ny, nx)
+    assert r.sample((dx * 2, dx * 3, -5.0), (dx * 2, dx * 3, -5.0), (1, 1, 1))[0] == g[3, 2]
+    mid = r.sample((1.5 * dx, 0.0, 0.0), (1.5 * dx, 0.0, 0.0), (1, 1, 1))[0]
+    assert mid == pytest.approx(0.5 * (g[0, 1] + g[0, 2]), rel=1e-14)
+    nan_x = r.sample((math.nan, 4 * dx, 0.0), (math.nan, 4 * dx, 0.0), (1, 1, 1))[0]
+    assert nan_x == g[4, 0]
+    # beyond the walls: the corner nodes, clamped rather than extrapolated
+    out = r.sample((-1.0, -1.0, 0.0), (1.0, 1.0, 0.0), (2, 2, 1))
+    assert out[0] == g[0, 0] and out[-1] == g[-1, -1]
+
+
+def bar_oracle(cells=9, seed=7):
+    b = oracle.Bar(cells, 1e-3, 1e-4, 2700.0, 167.0, 896.0, 300.0)
+    t = 300.0 + 30.0 * np.random.default_rng(seed).random(b.n)
+    b.cells = t
+    return b, t
+
+
+def test_bar_samples_on_centres_and_beyond_the_ends():
+    """lib.rs:736-751: cell centres at (i + ½)·dx read the cells, between two centres the blend,
+    beyond either end centre and at a NaN x the end cell; y and z are not read."""
+    b, t = bar_oracle()
+    n = b.n
+    got = b.sample((0.5e-3, 7.0, -3.0), ((n - 0.5) * 1e-3, 7.0, -3.0), (n, 1, 1))
+    assert np.allclose(got, t, rtol=1e-15, atol=0)
+    assert b.sample((0.0, 0, 0), (0.0, 0, 0), (1, 1, 1))[0] == t[0]
+    assert b.sample((1.0, 0, 0), (1.0, 0, 0), (1, 1, 1))[0] == t[-1]
+    assert b.sample((math.nan, 0, 0), (math.nan, 0, 0), (1, 1, 1))[0] == t[0]
+    mid = b.sample((2.0e-3, 0, 0), (2.0e-3, 0, 0), (1, 1, 1))[0]
+    assert mid == pytest.approx(0.5 * (t[1] + t[2]), rel=1e-15)
+
+
+def test_oracle_room_and_bar_samplers_against_a_python_restatement():
+    r, pr = room_oracle(8)
+    nx, ny = r.cells
+    dx = r.dx
+
+    def clamp(v, n):  # room.rs:739-749
+        if math.isnan(v) or v <= 0.0:
+            return 0, 0.0
+        if v >= n - 1:
+            return n - 1, 0.0
+        i = math.floor(v)
+        return int(i), v - i
+
+    rng = np.random.default_rng(13)
+    for _ in range(60):
+        p = rng.uniform(-2e-3, 0.013, 3)
+        if rng.random() < 0.1:
+            p[rng.integers(0, 2)] = math.nan
+        (i, fx), (j, fy) = clamp(p[0] / dx, nx), clamp(p[1] / dx, ny)
+        i1, j1 = min(i + 1, nx - 1), min(j + 1, ny - 1)
+        bottom = pr[j * nx + i] * (1.0 - fx) + pr[j * nx + i1] * fx
+        top = pr[j1 * nx + i] * (1.0 - fx) + pr[j1 * nx + i1] * fx
+        assert r.sample(p, p, (1, 1, 1))[0] == bottom * (1.0 - fy) + top * fy
+
+    b, t = bar_oracle(11, 9)
+    last = b.n - 1
+    for _ in range(60):
+        x = rng.uniform(-2e-3, 0.013)
+        u = x / 1e-3 - 0.5
+        if u <= 0.0:
+            want = t[0]
+        elif u >= last:
+            want = t[last]
+        else:
+            i = math.floor(u)
+            f = u - i
+            want = t[int(i)] * (1.0 - f) + t[int(i) + 1] * f
+        assert b.sample((x, 0, 0), (x, 0, 0), (1, 1, 1))[0] == want
+
+
+NAN_EXTENT = ((math.nan, 1e-3, 0.0), (math.nan, 5e-3, 1e-3), (1, 4, 2))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_room_device_samples_match_the_oracle(precision):
+    """After 25 steps of a released (1, 1) mode (white noise would trip the startup check,
+    room.rs:460-475). The f64 form is stepped beside the oracle; the FP32 form's own pressures are
+    handed to the oracle, so both forms' samples are bit for bit."""
+    from pantometry_b200.domains import Room
+
+    o = oracle.Room(0.011, 0.007, 12)
+    g = Room(0.011, 0.007, 12, precision=precision)
+    pr = o.mode_profile(1, 1, 1.0)
+    o.release(pr)
+    g.release(pr)
+    dt = 0.9 * o.max_stable_dt()
+    assert g.step(dt, 25) is None
+    if precision == "f64":
+        assert o.step(dt, 25) is None
+    else:
+        o.release(g.fields()["p"])
+    for lo, hi, cnt in EXTENTS + [NAN_EXTENT]:
+        want, got = o.sample(lo, hi, cnt), g.sample(lo, hi, cnt)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_bar_device_samples_match_the_oracle(precision):
+    from pantometry_b200.domains import Bar
+
+    sub = (2700.0, 167.0, 896.0)
+    o = oracle.Bar(40, 1e-3, 1e-4, *sub, 300.0)
+    g = Bar(40, 1e-3, 1e-4, *sub, 300.0, precision=precision)
+    t = 300.0 + 30.0 * np.random.default_rng(7).random(40)
+    o.cells = t
+    g.cells = t
+    dt = 0.9 * o.max_stable_dt()
+    assert g.step(dt, 25) is None
+    if precision == "f64":
+        assert o.step(dt, 25) is None
+    else:
+        o.cells = g.cells  # kelvin as the FP32 form reads it: T_ref + deviation
+    for lo, hi, cnt in EXTENTS + [NAN_EXTENT, ((0.5e-3, 0, 0), (39.5e-3, 0, 0), (40, 1, 1))]:
+        want, got = o.sample(lo, hi, cnt), g.sample(lo, hi, cnt)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.gpu
+def test_capture_labels_every_field_kind():
+    """Each field kind is drawn with the unit its ScalarField::unit gives (solid.rs, lib.rs:732-734,
+    hall.rs:586-588, room.rs:583-585, cavity.rs)."""
+    from pantometry_b200 import scenes
+    from pantometry_b200.domains import Bar, Cavity, Hall, Room, Solid3D
+
+    doms = {"block": Solid3D((4, 4, 4), 1e-3, 1000.0, 100.0, 1000.0, 300.0),
+            "bar": Bar(8, 1e-3, 1e-4, 2700.0, 167.0, 896.0, 310.0),
+            "hall": Hall(0.01, 0.008, 0.006, 6, 343.0, 1.2),
+            "room": Room(0.011, 0.007, 12),
+            "cavity": Cavity((4, 4, 4), 1e-3)}
+    extent = {"min": (0.0, 0.0, 0.0), "max": (0.004, 0.003, 0.002), "samples": (3, 2, 2)}
+    frame = scenes.capture(doms, {k: {"extent": extent} for k in doms})
+    units = {p["name"]: p["unit"] for p in frame["panels"]}
+    assert units == {"block": "K", "bar": "K", "hall": "Pa", "room": "Pa", "cavity": "V/m"}
+    for p in frame["panels"]:
+        want = doms[p["name"]].sample(extent["min"], extent["max"], extent["samples"])
+        assert np.array_equal(p["values"], want)
