@@ -27,6 +27,7 @@ startup order (hall_closed_forms.rs:132-181), the Cavity divergence identity
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -98,6 +99,9 @@ def _declare(L):
         "or_heat_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_hall_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_yee_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
+        "or_yee_cutoff_frequency": (C.c_double, [p, C.c_int, C.c_int]),
+        "or_yee_launch_along_z": (None, [p, dp, dp]),
+        "or_yee_impress": (None, [p, C.c_int, dp]),
         "or_room_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_bar_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_heat_dissipating": (None, [p, d, C.c_void_p]),
@@ -623,6 +627,9 @@ class Bar(_Box):
 # Cavity
 # --------------------------------------------------------------------------------------------
 WALL_KINDS = {"conducting": 0, "magnetic": 1, "open": 2}
+# crates/pantometry-em/src/lib.rs:67-69: the permittivity (F/m) and permeability (H/m) of free space
+EPSILON_0 = 8.854_187_812_8e-12
+MU_0 = 1.256_637_062_12e-6
 
 
 class Yee(_Box):
@@ -635,6 +642,8 @@ class Yee(_Box):
         self._h = L.or_yee_new(name.encode(), counts[0], counts[1], counts[2], dx, eps_r, mu_r, sigma)
         self.counts = tuple(max(1, c) for c in counts)
         self.dx = dx
+        # Medium::wave_speed (crates/pantometry-em/src/lib.rs:67-69, 104-112): 1/√(εμ)
+        self.wave_speed = 1.0 / math.sqrt((EPSILON_0 * eps_r) * (MU_0 * mu_r))
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -656,6 +665,34 @@ class Yee(_Box):
     def obstruct(self, solid):
         m = np.ascontiguousarray(solid, dtype=np.uint8).reshape(-1)
         lib().or_yee_obstruct(self._h, m.ctypes.data_as(C.c_void_p))
+
+    def cutoff_frequency(self, mode):
+        """`Cavity::cutoff_frequency` (cavity.rs:559-563): the (m, n) mode's cutoff of the cross-section."""
+        return lib().or_yee_cutoff_frequency(self._h, int(mode[0]), int(mode[1]))
+
+    def launch_along_z(self, dt, envelope):
+        """`Cavity::launch_along_z` (cavity.rs:488-521): `envelope(x, y, z)`, over numpy arrays of
+        positions in metres, sets Ey at its edges and (as −envelope/η, z moved on by c·dt/2) Hx at its
+        faces; the conducting walls are then cleared and the leapfrog counts as begun."""
+        nx, ny, nz = self.counts
+        x = np.arange(nx + 1, dtype=np.float64) * self.dx
+        y = (np.arange(ny, dtype=np.float64) + 0.5) * self.dx
+        ze = np.arange(nz + 1, dtype=np.float64) * self.dx
+        zh = (np.arange(nz, dtype=np.float64) + 0.5) * self.dx + self.wave_speed * dt / 2.0
+        ey = np.ascontiguousarray(envelope(x[None, None, :], y[None, :, None], ze[:, None, None]) *
+                                  np.ones((nz + 1, ny, nx + 1)), dtype=np.float64)
+        hx = np.ascontiguousarray(envelope(x[None, None, :], y[None, :, None], zh[:, None, None]) *
+                                  np.ones((nz, ny, nx + 1)), dtype=np.float64)
+        lib().or_yee_launch_along_z(self._h, _dp(ey), _dp(hx))
+
+    def impress(self, plane, add):
+        """`Cavity::impress` (cavity.rs:537-548): `add(x, y)` over numpy arrays of positions, added to
+        Ey on the plane z = min(plane, nz)·dx, the conducting walls cleared after."""
+        nx, ny, _ = self.counts
+        x = np.arange(nx + 1, dtype=np.float64) * self.dx
+        y = (np.arange(ny, dtype=np.float64) + 0.5) * self.dx
+        a = np.ascontiguousarray(add(x[None, :], y[:, None]) * np.ones((ny, nx + 1)), dtype=np.float64)
+        lib().or_yee_impress(self._h, int(plane), _dp(a))
 
     def set_boundary(self, wall, kind):
         lib().or_yee_set_boundary(self._h, wall, WALL_KINDS[kind] if isinstance(kind, str) else kind)

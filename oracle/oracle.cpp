@@ -1258,6 +1258,33 @@ struct Cavity {
 
     double courant_limit() const { return COURANT_3D * dx / medium.wave_speed(); }
 
+    // cavity.rs:559-563 with size() (639-647): f_c = (c/2)·√((m/a)² + (n/b)²), a = nx·dx, b = ny·dx
+    double cutoff_frequency(int m, int n) const {
+        const double a = (double)m / ((double)nx * dx), b = (double)n / ((double)ny * dx);
+        return 0.5 * medium.wave_speed() * std::sqrt(a * a + b * b);
+    }
+
+    // cavity.rs:488-521: Ey from the envelope at its edges (i·dx, (j+½)·dx, k·dx), Hx = −envelope/η
+    // at its faces with z moved on by c·dt/2 (the caller evaluates the envelope at both sets of
+    // points, in the layouts of ey and hx), then the conducting walls' tangential E cleared; the
+    // next step starts the leapfrog as already begun.
+    void launch_along_z(const double* ey_env, const double* hx_env) {
+        const double eta = std::sqrt(medium.permeability() / medium.permittivity());
+        for (size_t c = 0; c < ey.size(); ++c) ey[c] = ey_env[c];
+        for (size_t c = 0; c < hx.size(); ++c) hx[c] = -hx_env[c] / eta;
+        enforce_walls_where(CONDUCTING);
+        started = true;
+    }
+
+    // cavity.rs:537-548: a soft source, `add` (at (i·dx, (j+½)·dx), i fastest over nx+1, then j over
+    // ny) added to Ey on the plane k = min(plane, nz), then the conducting walls' tangential E cleared.
+    void impress(int plane, const double* add) {
+        const int k = std::min(plane, nz);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i <= nx; ++i) ey[iey(i, j, k)] += add[i + (size_t)(nx + 1) * j];
+        enforce_walls_where(CONDUCTING);
+    }
+
     // cavity.rs:675-732
     void release_mode(int mm, int pm, double amplitude, double dt) {
         double m = (double)std::max(mm, 1), pp = (double)std::max(pm, 1);
@@ -1905,6 +1932,11 @@ void or_yee_obstruct(void* p, const uint8_t* solid) {
     c->enforce_solid();
 }
 void or_yee_set_boundary(void* p, int wall, int kind) { ((Cavity*)p)->boundary[wall] = kind; }
+double or_yee_cutoff_frequency(void* p, int m, int n) { return ((Cavity*)p)->cutoff_frequency(m, n); }
+void or_yee_launch_along_z(void* p, const double* ey_env, const double* hx_env) {
+    ((Cavity*)p)->launch_along_z(ey_env, hx_env);
+}
+void or_yee_impress(void* p, int plane, const double* add) { ((Cavity*)p)->impress(plane, add); }
 void or_yee_release_mode(void* p, int m, int pm, double amplitude, double dt) { ((Cavity*)p)->release_mode(m, pm, amplitude, dt); }
 void or_yee_set_source(void* p, long long edge, const double* current, long long n) {
     Cavity* c = (Cavity*)p;

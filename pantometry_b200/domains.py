@@ -9,6 +9,7 @@ order (x fastest). Everything runs on the GPU; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -17,6 +18,9 @@ from . import _native as N
 FACES = ("XMin", "XMax", "YMin", "YMax", "ZMin", "ZMax")
 WALLS = ("XLow", "XHigh", "YLow", "YHigh", "ZLow", "ZHigh")
 BOUNDARY_KINDS = {"conducting": 0, "magnetic": 1, "open": 2}
+# crates/pantometry-em/src/lib.rs:67-69: the permittivity (F/m) and permeability (H/m) of free space
+EPSILON_0 = 8.854_187_812_8e-12
+MU_0 = 1.256_637_062_12e-6
 
 
 def _f64(a, n=None):
@@ -468,6 +472,11 @@ class Cavity(_Domain, _Field):
         self.counts = (d.nx, d.ny, d.nz)
         self.dx = dx
         self.precision = d.precision
+        self._walls = [BOUNDARY_KINDS["conducting"]] * 6  # cavity.rs:230: conducting walls by default
+        # Medium::permittivity / permeability / wave_speed (crates/pantometry-em/src/lib.rs:67-69,
+        # 104-112), of the medium the cavity was made of
+        self._eps, self._mu = EPSILON_0 * eps_r, MU_0 * mu_r
+        self.wave_speed = 1.0 / math.sqrt(self._eps * self._mu)
 
     def shapes(self):
         nx, ny, nz = self.counts
@@ -489,6 +498,50 @@ class Cavity(_Domain, _Field):
         w = WALLS.index(wall) if isinstance(wall, str) else int(wall)
         k = BOUNDARY_KINDS[kind] if isinstance(kind, str) else int(kind)
         N.check(self._lib.pm_cavity_set_boundary(self._h, w, k))
+        self._walls[w] = k
+
+    def cutoff_frequency(self, mode):
+        """`Cavity::cutoff_frequency` (cavity.rs:559-563, size() 639-647): the (m, n) mode's cutoff,
+        (c/2)·√((m/a)² + (n/b)²) over the cross-section a = nx·dx, b = ny·dx, in hertz."""
+        a = float(mode[0]) / (self.counts[0] * self.dx)
+        b = float(mode[1]) / (self.counts[1] * self.dx)
+        return 0.5 * self.wave_speed * math.sqrt(a * a + b * b)
+
+    def launch_along_z(self, dt, envelope):
+        """`Cavity::launch_along_z` (cavity.rs:488-521): `envelope(x, y, z)`, over numpy arrays of
+        positions in metres, sets Ey at its edges (i·dx, (j+½)·dx, k·dx) and Hx = −envelope/η at its
+        faces with z moved on by c·dt/2; the conducting walls' tangential E is cleared
+        (`enforce_walls_where`, cavity.rs:1239-1293) and the next step continues the leapfrog rather
+        than starting it. Built on the host and uploaded; the other components are kept."""
+        nx, ny, nz = self.counts
+        f = self.fields()
+        x = np.arange(nx + 1, dtype=np.float64) * self.dx
+        y = (np.arange(ny, dtype=np.float64) + 0.5) * self.dx
+        ze = np.arange(nz + 1, dtype=np.float64) * self.dx
+        zh = (np.arange(nz, dtype=np.float64) + 0.5) * self.dx + self.wave_speed * dt / 2.0
+        eta = math.sqrt(self._mu / self._eps)
+        ey = envelope(x[None, None, :], y[None, :, None], ze[:, None, None]) * np.ones((nz + 1, ny, nx + 1))
+        hx = -(envelope(x[None, None, :], y[None, :, None], zh[:, None, None]) * np.ones((nz, ny, nx + 1))) / eta
+        ex = f["ex"].reshape(nz + 1, ny + 1, nx)
+        ez = f["ez"].reshape(nz, ny + 1, nx + 1)
+        for w, kind in enumerate(self._walls):
+            if kind != BOUNDARY_KINDS["conducting"]:
+                continue
+            if w < 2:
+                edge = 0 if w == 0 else nx
+                ey[:, :, edge] = 0.0
+                ez[:, :, edge] = 0.0
+            elif w < 4:
+                edge = 0 if w == 2 else ny
+                ex[:, edge, :] = 0.0
+                ez[:, edge, :] = 0.0
+            else:
+                edge = 0 if w == 4 else nz
+                ex[edge, :, :] = 0.0
+                ey[edge, :, :] = 0.0
+        f["ey"], f["hx"] = ey.reshape(-1), hx.reshape(-1)
+        self.set_fields(f, started=True)
+        return self
 
     def release_mode(self, mode, amplitude, dt):
         N.check(self._lib.pm_cavity_release_mode(self._h, int(mode[0]), int(mode[1]), float(amplitude), float(dt)))
