@@ -427,3 +427,73 @@ def test_capture_labels_every_field_kind():
     for p in frame["panels"]:
         want = doms[p["name"]].sample(extent["min"], extent["max"], extent["samples"])
         assert np.array_equal(p["values"], want)
+
+
+# nothing_is_not_a_temperature.rs: Substance::copper (substance.rs:462-471), 10 mm cells at 20 °C
+COPPER = dict(density=8.96e3, conductivity=401.0, specific_heat=385.0, emissivity=0.04)
+C20, C300 = 20.0 + 273.15, 300.0 + 273.15
+
+
+def copper_block(counts, make=None, precision="f64"):
+    s = COPPER
+    if make is None:
+        return oracle.Heat(counts, 10e-3, s["density"], s["conductivity"], s["specific_heat"], C20,
+                           emissivity=s["emissivity"])
+    return make(counts, 10e-3, s["density"], s["conductivity"], s["specific_heat"], C20,
+                emissivity=s["emissivity"], precision=precision)
+
+
+def gapped_bar(make=None, precision="f64"):
+    """nothing_is_not_a_temperature.rs:20-32: four cells along x, the first at 300 °C, the middle two
+    emptied."""
+    b = copper_block((4, 1, 1), make, precision)
+    b.cells = np.array([C300, C20, C20, C20])
+    b.empty(np.array([0, 1, 1, 0], dtype=np.uint8))
+    return b
+
+
+def at_mm(block, mm):
+    p = (mm * 1e-3, 5e-3, 5e-3)
+    return block.sample(p, p, (1, 1, 1))[0]
+
+
+def check_void_readings(block, tol):
+    # nothing_is_not_a_temperature.rs:34-60: exact on the metal, no value in the gap
+    assert abs(at_mm(block, 5.0) - C300) < tol
+    assert abs(at_mm(block, 35.0) - C20) < tol
+    for mm in (15.0, 20.0, 25.0):
+        assert math.isnan(at_mm(block, mm)), mm
+    # :62-83: a sample straddling the boundary belongs to the cell it is in
+    assert math.isfinite(at_mm(block, 9.0))
+    assert math.isnan(at_mm(block, 11.0))
+    face = at_mm(block, 10.0)
+    assert math.isnan(face) or abs(face - C300) < tol
+
+
+def check_unmasked_block_interpolates(block, tol):
+    """nothing_is_not_a_temperature.rs:85-125: a 2×2×2 block with nothing masked is plain trilinear."""
+    cell = lambda i, j, k: 100.0 * (i + 2 * j + 4 * k) + 273.15  # noqa: E731
+    block.cells = np.array([cell(i, j, k) for k in range(2) for j in range(2) for i in range(2)])
+    fx, fy, fz = 0.3, 0.6, 0.8
+    mm = lambda f: (5.0 + 10.0 * f) * 1e-3  # noqa: E731
+    p = (mm(fx), mm(fy), mm(fz))
+    got = block.sample(p, p, (1, 1, 1))[0]
+    lerp = lambda lo, hi, t: lo * (1.0 - t) + hi * t  # noqa: E731
+    z0 = lerp(lerp(cell(0, 0, 0), cell(1, 0, 0), fx), lerp(cell(0, 1, 0), cell(1, 1, 0), fx), fy)
+    z1 = lerp(lerp(cell(0, 0, 1), cell(1, 0, 1), fx), lerp(cell(0, 1, 1), cell(1, 1, 1), fx), fy)
+    assert abs(got - lerp(z0, z1, fz)) < tol
+
+
+def test_oracle_void_readings_restate_the_reference():
+    check_void_readings(gapped_bar(), 1e-12)
+    check_unmasked_block_interpolates(copper_block((2, 2, 2)), 1e-9)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_device_void_readings_restate_the_reference(precision):
+    from pantometry_b200.domains import Solid3D
+
+    tol = 1e-12 if precision == "f64" else 1e-4  # FP32: kelvin from f32 deviations
+    check_void_readings(gapped_bar(Solid3D, precision), tol)
+    check_unmasked_block_interpolates(copper_block((2, 2, 2), Solid3D, precision), max(tol, 1e-9))
