@@ -153,7 +153,9 @@ pm_status pm_heat_set_tolerance(pm_heat* h, double tolerance);
 pm_status pm_heat_step(pm_heat* h, double dt, long long nsteps, pm_violation* out);
 /* Domain::ledger (solid.rs:1904-1927), as of the last step. */
 pm_status pm_heat_ledger(pm_heat* h, pm_ledger* out);
-/* Placeless heat off the bus, spread to a uniform rise (solid.rs:1752-1765). */
+/* Placeless heat off the bus (solid.rs:1752-1765): held until the next pm_heat_step, whose first
+ * step takes it after its stability refusal (checked against the state before the rise) as a
+ * uniform rise over the solid cells. A refused step leaves it held. */
 pm_status pm_heat_absorb(pm_heat* h, double joules);
 /* Domain::checkpoint / restore (solid.rs:1935-1950). */
 pm_status pm_heat_checkpoint(pm_heat* h);

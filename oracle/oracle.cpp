@@ -404,6 +404,7 @@ struct Heat {
                           STABLE_FOURIER_3D, ratio * STABLE_FOURIER_3D, STABLE_FOURIER_3D, 1e-12);
             return false;
         }
+        take_pending();
         bool any = false;
         for (int f = 0; f < 6; ++f) any = any || exposed[f];
         std::vector<double> old = cells;
@@ -447,8 +448,16 @@ struct Heat {
         return true;
     }
 
-    // solid.rs:1368-1375 `deposit` and the bus share at 1752-1765 both go through add_kelvin.
-    void absorb(double gained) {
+    // Placeless heat handed in for the next step, as the bus's HEAT channel holds it: the step takes
+    // it after its stability refusal (solid.rs:1718-1765), so a refused step leaves it pending.
+    double pending = 0.0;
+    void absorb(double gained) { pending += gained; }
+
+    // solid.rs:1752-1765: the bus share, spread to a uniform rise through add_kelvin (as `deposit`,
+    // 1368-1375, is).
+    void take_pending() {
+        const double gained = pending;
+        pending = 0.0;
         if (gained == 0.0) return;
         absorbed += gained;
         double cap_sum = -0.0;

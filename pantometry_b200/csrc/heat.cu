@@ -60,6 +60,7 @@ struct Heat : Handle {
     // (heat_f32_quad_step, rows of a multiple of 4); false: one cell per thread throughout
     bool wide = true;
     bool quads64 = true;  // plain f64, rows of a multiple of 4: four cells a thread (else two)
+    double pending = 0.0; // placeless heat handed in for the next step (pm_heat_absorb)
     DBuf saved;
     DBuf stage;     // f64 staging for uploads/downloads of the f32 form
     // the TMA-staged FP32 form of a uniform block whose rows hold a multiple of 4 cells: the tensor
@@ -602,6 +603,30 @@ struct Heat : Handle {
         return PM_OK;
     }
 
+    // solid.rs:1752-1765: the first step of a call takes the placeless heat handed in since the last
+    // one, after its stability refusal, as a uniform rise over the solid cells. It is bus traffic,
+    // not a change of the domain's own books, so the stored heat is re-measured and lost and
+    // supplied kept; and since the refusal was made against the state before the rise, the rate
+    // that state gave stays the one the step's own check reads.
+    pm_status take_pending() {
+        const double joules = pending;
+        if (joules == 0.0) return PM_OK;
+        pending = 0.0;
+        const double rise = joules / cap_sum;  // solid.rs:1755
+        PM_CUDA(launch_heat_rise(precision == PM_PLAIN_F64 ? field[parity].as<double>() : nullptr,
+                                 precision == PM_PLAIN_F64 ? nullptr : field[parity].as<float>(), rise, n(),
+                                 vd.empty() ? nullptr : dvoid.as<uint8_t>(), stream()));
+        pm_status s = read_state();
+        if (s != PM_OK) return s;
+        const double lost = host_state->lost, supplied = host_state->supplied, rate = host_state->rate_now;
+        s = measure();
+        if (s != PM_OK) return s;
+        host_state->lost = lost;
+        host_state->supplied = supplied;
+        host_state->rate_now = rate;
+        return write_state();
+    }
+
     pm_status measure() {  // the opening ledger of the present state
         HeatMeasureArgs m{};
         if (precision == PM_PLAIN_F64) m.t64 = field[parity].as<double>();
@@ -868,7 +893,9 @@ pm_status pm_heat_step(pm_heat* hp, double dt, long long nsteps, pm_violation* o
         set_error("Fourier number past the explicit limit");
         return PM_VIOLATION;
     }
-    pm_status s = h->begin_call();
+    pm_status s = h->take_pending();
+    if (s != PM_OK) return s;
+    s = h->begin_call();
     if (s != PM_OK) return s;
     const long long before = h->host_state->steps;
     if (h->precision == PM_PLAIN_F64 && h->persistent(nsteps)) {
@@ -911,20 +938,8 @@ pm_status pm_heat_ledger(pm_heat* hp, pm_ledger* out) {
 pm_status pm_heat_absorb(pm_heat* hp, double joules) {
     Heat* h = reinterpret_cast<Heat*>(hp);
     HEAT_GUARD(h);
-    if (joules == 0.0) return PM_OK;
-    const double rise = joules / h->cap_sum;  // solid.rs:1755
-    PM_CUDA(launch_heat_rise(h->precision == PM_PLAIN_F64 ? h->field[h->parity].as<double>() : nullptr,
-                             h->precision == PM_PLAIN_F64 ? nullptr : h->field[h->parity].as<float>(), rise, h->n(),
-                             h->vd.empty() ? nullptr : h->dvoid.as<uint8_t>(), h->stream()));
-    // absorbed heat is bus traffic, not a change of the domain's own books: re-measure stored
-    pm_status s = h->read_state();
-    if (s != PM_OK) return s;
-    double lost = h->host_state->lost, supplied = h->host_state->supplied;
-    s = h->measure();
-    if (s != PM_OK) return s;
-    h->host_state->lost = lost;
-    h->host_state->supplied = supplied;
-    return h->write_state();
+    h->pending += joules;  // held, as the bus holds it, until the next step takes it
+    return PM_OK;
 }
 
 pm_status pm_heat_checkpoint(pm_heat* hp) {
