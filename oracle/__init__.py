@@ -100,6 +100,7 @@ def _declare(L):
         "or_hall_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_yee_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
         "or_yee_cutoff_frequency": (C.c_double, [p, C.c_int, C.c_int]),
+        "or_yee_mur_coefficient": (C.c_double, [p, C.c_double]),
         "or_yee_launch_along_z": (None, [p, dp, dp]),
         "or_yee_impress": (None, [p, C.c_int, dp]),
         "or_room_sample": (None, [p, dp, dp, C.POINTER(C.c_int), dp]),
@@ -665,6 +666,10 @@ class Yee(_Box):
     def obstruct(self, solid):
         m = np.ascontiguousarray(solid, dtype=np.uint8).reshape(-1)
         lib().or_yee_obstruct(self._h, m.ctypes.data_as(C.c_void_p))
+
+    def mur_coefficient(self, dt):
+        """`Cavity::mur_coefficient` (cavity.rs:588-591): (c·dt − dx)/(c·dt + dx)."""
+        return lib().or_yee_mur_coefficient(self._h, float(dt))
 
     def cutoff_frequency(self, mode):
         """`Cavity::cutoff_frequency` (cavity.rs:559-563): the (m, n) mode's cutoff of the cross-section."""

@@ -1092,10 +1092,15 @@ struct Cavity {
         }
     }
 
+    // cavity.rs:588-591: Mur's coefficient (c·dt − dx)/(c·dt + dx)
+    double mur_coefficient(double dt) const {
+        const double c_dt = medium.wave_speed() * dt;
+        return (c_dt - dx) / (c_dt + dx);
+    }
+
     // cavity.rs:1074-1164
     void apply_boundaries(double dt) {
-        double c_dt = medium.wave_speed() * dt;
-        double kk = (c_dt - dx) / (c_dt + dx);
+        double kk = mur_coefficient(dt);
         bool prev = has_prev;
         has_prev = false;
         enforce_walls_where(CONDUCTING);
@@ -1941,6 +1946,7 @@ void or_yee_obstruct(void* p, const uint8_t* solid) {
     c->enforce_solid();
 }
 void or_yee_set_boundary(void* p, int wall, int kind) { ((Cavity*)p)->boundary[wall] = kind; }
+double or_yee_mur_coefficient(void* p, double dt) { return ((Cavity*)p)->mur_coefficient(dt); }
 double or_yee_cutoff_frequency(void* p, int m, int n) { return ((Cavity*)p)->cutoff_frequency(m, n); }
 void or_yee_launch_along_z(void* p, const double* ey_env, const double* hx_env) {
     ((Cavity*)p)->launch_along_z(ey_env, hx_env);
