@@ -5,7 +5,11 @@ on the oracle (the eigen-decay, axis, conservation and limit tests are restated 
   * a hot spot spreads the same way along all six arms, to 1e-12 of its rise, and the diagonal sits
     between the air and an arm (:296-339);
   * a block one cell thick is a bar: its mode's amplification is 1 + F·λ with λ = −4 sin²(π/2n),
-    and 30 steps give the amplitude to 1e-12 (:341-371).
+    and 30 steps give the amplitude to 1e-12 (:341-371);
+  * the field reads each cell back at its centre and stays inside the block's range outside it
+    (:373-416);
+  * at the reported limit the sharpest mode is marginal and oscillatory (amplification in
+    [−1, −0.5)) and holds over 60 steps; at three times it diverges and is refused (:503-541).
 The device's placeless heat, deposits and plain stencil are checked against the oracle bit for bit
 elsewhere (`test_layered_wall.py`, `test_voids_gaps_sources.py`, `test_gpu_parity.py`).
 """
@@ -64,3 +68,30 @@ def test_one_cell_thick_reduces_to_a_bar():  # :341-371
     assert abs(b.mode_amplification((1, 0, 0), dt) - per_step) < 1e-15
     assert b.step(dt, 30) is None
     assert abs(b.mode_amplitude((1, 0, 0)) - 5.0 * per_step ** 30) < 1e-12 * 5.0
+
+
+def test_the_field_reads_back_the_cells_and_clamps_at_the_faces():  # :373-416
+    b = block((5, 4, 3), 2.0)
+    b.release_mode((1, 1, 1), C20, 10.0)
+    t = b.cells
+    dx = 2e-3
+    got = b.sample((0.5 * dx, 0.5 * dx, 0.5 * dx), (4.5 * dx, 3.5 * dx, 2.5 * dx), (5, 4, 3))
+    assert np.abs(got - t).max() < 1e-9  # each cell centre reads its cell
+    for p in ((-1.0, 0.0, 0.0), (0.0, -1.0, 0.0), (0.0, 0.0, -1.0), (1.0, 1.0, 1.0)):
+        v = b.sample(p, p, (1, 1, 1))[0]
+        assert t.min() - 1e-9 <= v <= t.max() + 1e-9
+
+
+def test_the_limit_is_where_the_sharpest_mode_stops_growing():  # :503-541
+    n = 5
+    sharpest = (n - 1, n - 1, n - 1)
+    b = block((n, n, n), 2.0)
+    b.release_mode(sharpest, C20, 1.0)
+    limit = b.max_stable_dt()
+    assert b.step(limit, 60) is None
+    assert abs(b.mode_amplitude(sharpest)) <= 1.0 + 1e-9
+    per_step = block((n, n, n), 2.0).mode_amplification(sharpest, limit)
+    assert -1.0 <= per_step < -0.5  # marginal and oscillatory
+    runaway = block((n, n, n), 2.0).mode_amplification(sharpest, 3.0 * limit)
+    assert abs(runaway) > 1.0 and abs(runaway) ** 60 > 1e6
+    assert block((n, n, n), 2.0).step(3.0 * limit)["quantity"] == "Fourier number"
